@@ -1,0 +1,258 @@
+/*
+ * ORACLE — test infrastructure only (see tgap_oracle.h).
+ *
+ * Restatement of the GAP prediction layer and of the dynamics arithmetic:
+ *   get_soap_energy_and_forces   src/gap/gap.f90:39-244
+ *   get_gap_soap                 src/gap/gap_interface.f90:41-433 (subset, renumber, scatter)
+ *   velocity_verlet              src/md/md_utils.f90:486-532
+ *   monte_carlo_move             src/mc/mc_utils.f90:172-180 (+ min(1,p) of :255)
+ */
+#include "tgap_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+static double ipow(double x, int n)
+{
+    double r = 1.0;
+    for (int i = 0; i < n; ++i) r *= x;
+    return r;
+}
+
+void orc_get_soap_energy_and_forces(int n_soap, int n_sites, int n_sparse, const double *soap,
+                                    const double *soap_der, const double *alphas, double delta,
+                                    double zeta0, double e0, const double *Qs,
+                                    const int *n_neigh, const int *neighbors_list,
+                                    const double *xyz, int do_forces, int n_sites0,
+                                    double *energies, double *forces, double *virial)
+{
+    /* gap.f90:99-105: integer zeta if within 1e-5 */
+    int is_int = fabs(zeta0 - (double)(int)zeta0) < 1.0e-5;
+    int zi = (int)zeta0;
+    double zeta = is_int ? (double)zi : zeta0;
+    double *K = (double *)malloc(sizeof(double) * (size_t)n_sites * (size_t)n_sparse);
+    /* gap.f90:123 K = soap^T Qs; K(i,s) stored K[i*n_sparse + s] */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_sites; ++i)
+        for (int s = 0; s < n_sparse; ++s) {
+            const double *a = soap + (size_t)i * n_soap, *b = Qs + (size_t)s * n_soap;
+            double acc = 0.0;
+            for (int d = 0; d < n_soap; ++d) acc += a[d] * b[d];
+            K[(size_t)i * n_sparse + s] = acc;
+        }
+    /* gap.f90:128-135 */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_sites; ++i) {
+        double e = 0.0;
+        for (int s = 0; s < n_sparse; ++s) {
+            double k = K[(size_t)i * n_sparse + s];
+            e += (is_int ? ipow(k, zi) : pow(k, zeta)) * alphas[s];
+        }
+        energies[i] = delta * delta * e + e0;
+    }
+    if (!do_forces) {
+        free(K);
+        return;
+    }
+    /* gap.f90:153-171 Qss = -zeta delta^2 (K^(zeta-1) o alpha) Qs^T */
+    double *Qss = (double *)malloc(sizeof(double) * (size_t)n_sites * (size_t)n_soap);
+    double pref = -zeta * delta * delta;
+#pragma omp parallel
+    {
+        double *kd = (double *)malloc(sizeof(double) * (size_t)n_sparse);
+#pragma omp for schedule(static)
+        for (int i = 0; i < n_sites; ++i) {
+            for (int s = 0; s < n_sparse; ++s) {
+                double k = K[(size_t)i * n_sparse + s];
+                kd[s] = (is_int ? ipow(k, zi - 1) : pow(k, zeta - 1.0)) * alphas[s];
+            }
+            double *out = Qss + (size_t)i * n_soap;
+            for (int d = 0; d < n_soap; ++d) out[d] = 0.0;
+            for (int s = 0; s < n_sparse; ++s) {
+                double w = pref * kd[s];
+                const double *b = Qs + (size_t)s * n_soap;
+                for (int d = 0; d < n_soap; ++d) out[d] += w * b[d];
+            }
+        }
+        free(kd);
+    }
+    /* gap.f90:187-209 pair loop */
+    for (int x = 0; x < 9; ++x) virial[x] = 0.0;
+    for (int x = 0; x < 3 * n_sites0; ++x) forces[x] = 0.0;
+    int64_t l = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        const double *qs = Qss + (size_t)i * n_soap;
+        for (int j = 0; j < n_neigh[i]; ++j, ++l) {
+            int j2 = (neighbors_list[l] - 1) % n_sites0;
+            double f[3];
+            for (int k = 0; k < 3; ++k) {
+                double acc = 0.0;
+                const double *der = soap_der + (size_t)l * n_soap * 3;
+                for (int d = 0; d < n_soap; ++d) acc += qs[d] * der[3 * d + k];
+                f[k] = acc;
+                forces[3 * j2 + k] += f[k];
+            }
+            const double *r = xyz + 3 * l;
+            for (int k1 = 0; k1 < 3; ++k1)
+                for (int k2 = 0; k2 < 3; ++k2)
+                    virial[k1 + 3 * k2] += 0.5 * (f[k1] * r[k2] + f[k2] * r[k1]);
+        }
+    }
+    free(Qss);
+    free(K);
+}
+
+int orc_get_gap_soap(const orc_soap_hypers *h, int n_total_sites, int n_sites0,
+                     const int *n_neigh0, const int *neighbors_list0, const double *rjs0,
+                     const double *thetas0, const double *phis0, const double *xyz0,
+                     const int *species_supercell, int central_species, int n_sparse,
+                     const double *alphas, const double *Qs, double delta, double zeta,
+                     int do_forces, double *energies0, double *forces0, double *virial)
+{
+    const int ns = h->n_species;
+    double rcut_max = 0.0;
+    for (int s = 0; s < ns; ++s)
+        if (h->rcut_hard[s] > rcut_max) rcut_max = h->rcut_hard[s];
+    /* gap_interface.f90:184-212: count kept sites and pairs */
+    int n_sites = 0;
+    int64_t n_pairs = 0, k = 0;
+    unsigned char *seen = (unsigned char *)calloc((size_t)n_total_sites, 1);
+    for (int i = 0; i < n_sites0; ++i) {
+        int sp_i = species_supercell[(neighbors_list0[k] - 1) % n_total_sites];
+        if (sp_i == central_species || central_species == 0) {
+            ++n_sites;
+            for (int j = 0; j < n_neigh0[i]; ++j, ++k) {
+                int j2 = (neighbors_list0[k] - 1) % n_total_sites;
+                if (rjs0[k] < rcut_max && species_supercell[j2] > 0) {
+                    ++n_pairs;
+                    seen[j2] = 1;
+                }
+            }
+        } else {
+            k += n_neigh0[i];
+        }
+    }
+    int n_all = 0;
+    for (int i = 0; i < n_total_sites; ++i) n_all += seen[i];
+    /* gap_interface.f90:215-289: build the subset and renumber */
+    int *n_neigh = (int *)malloc(sizeof(int) * (size_t)(n_sites > 0 ? n_sites : 1));
+    int *nl = (int *)malloc(sizeof(int) * (size_t)(n_pairs > 0 ? n_pairs : 1));
+    double *rjs = (double *)malloc(sizeof(double) * (size_t)(n_pairs > 0 ? n_pairs : 1));
+    double *th = (double *)malloc(sizeof(double) * (size_t)(n_pairs > 0 ? n_pairs : 1));
+    double *ph = (double *)malloc(sizeof(double) * (size_t)(n_pairs > 0 ? n_pairs : 1));
+    double *xyz = (double *)malloc(sizeof(double) * 3 * (size_t)(n_pairs > 0 ? n_pairs : 1));
+    unsigned char *mask = (unsigned char *)calloc((size_t)(n_pairs > 0 ? n_pairs : 1) * ns, 1);
+    int *in_to_out = (int *)calloc((size_t)(n_all > 0 ? n_all : 1), sizeof(int));
+    int *out_to_in = (int *)calloc((size_t)n_total_sites, sizeof(int));
+    int i2 = 0;
+    k = 0;
+    for (int i = 0; i < n_sites0; ++i) {
+        int j = (neighbors_list0[k] - 1) % n_total_sites;
+        int sp_i = species_supercell[j];
+        if (sp_i == central_species || central_species == 0) {
+            in_to_out[i2] = j + 1;
+            out_to_in[j] = i2 + 1;
+            ++i2;
+        }
+        k += n_neigh0[i];
+    }
+    k = 0;
+    i2 = 0;
+    int i4 = 0;
+    int64_t k2 = 0;
+    for (int i = 0; i < n_sites0; ++i) {
+        int sp_i = species_supercell[(neighbors_list0[k] - 1) % n_total_sites];
+        if (sp_i == central_species || central_species == 0) {
+            ++i2;
+            int jj = 0;
+            for (int j = 1; j <= n_neigh0[i]; ++j, ++k) {
+                int j3 = (neighbors_list0[k] - 1) % n_total_sites;
+                if (rjs0[k] < rcut_max && species_supercell[j3] > 0) {
+                    ++jj;
+                    rjs[k2] = rjs0[k];
+                    ph[k2] = phis0[k];
+                    th[k2] = thetas0[k];
+                    xyz[3 * k2] = xyz0[3 * k];
+                    xyz[3 * k2 + 1] = xyz0[3 * k + 1];
+                    xyz[3 * k2 + 2] = xyz0[3 * k + 2];
+                    mask[k2 + (int64_t)(species_supercell[j3] - 1) * n_pairs] = 1;
+                    if (j > 1 && out_to_in[j3] == 0) {
+                        ++i4;
+                        in_to_out[n_sites + i4 - 1] = j3 + 1;
+                        out_to_in[j3] = n_sites + i4;
+                        nl[k2] = out_to_in[j3];
+                    } else if (j > 1) {
+                        nl[k2] = out_to_in[j3];
+                    } else {
+                        nl[k2] = i2;
+                    }
+                    ++k2;
+                }
+            }
+            n_neigh[i2 - 1] = jj;
+        } else {
+            k += n_neigh0[i];
+        }
+    }
+    int D = orc_soap_dim(h);
+    int rc = 0;
+    double *soap = (double *)calloc((size_t)D * (size_t)(n_sites > 0 ? n_sites : 1), sizeof(double));
+    double *der = NULL;
+    if (do_forces) der = (double *)calloc((size_t)D * 3 * (size_t)(n_pairs > 0 ? n_pairs : 1), sizeof(double));
+    for (int x = 0; x < 9; ++x) virial[x] = 0.0;
+    if (n_sites > 0) {
+        rc = orc_get_soap(h, n_sites, n_neigh, (int)n_pairs, mask, rjs, th, ph, soap, der);
+        if (rc == 0) {
+            double *en = (double *)calloc((size_t)n_sites, sizeof(double));
+            double *fo = (double *)calloc((size_t)3 * (size_t)n_all, sizeof(double));
+            orc_get_soap_energy_and_forces(D, n_sites, n_sparse, soap, der, alphas, delta, zeta, 0.0,
+                                           Qs, n_neigh, nl, xyz, do_forces, n_all, en, fo, virial);
+            for (int i = 0; i < n_sites; ++i) energies0[in_to_out[i] - 1] = en[i];
+            if (do_forces)
+                for (int i = 0; i < n_all; ++i)
+                    for (int x = 0; x < 3; ++x) forces0[3 * (in_to_out[i] - 1) + x] = fo[3 * i + x];
+            free(en);
+            free(fo);
+        }
+    }
+    free(soap);
+    free(der);
+    free(seen);
+    free(n_neigh);
+    free(nl);
+    free(rjs);
+    free(th);
+    free(ph);
+    free(xyz);
+    free(mask);
+    free(in_to_out);
+    free(out_to_in);
+    return rc;
+}
+
+void orc_velocity_verlet(int n_sites, double *positions, double *positions_prev,
+                         double *velocities, const double *forces, double *forces_prev,
+                         const double *masses, double dt, double *dt_prev, int first_step)
+{
+    if (!first_step)
+        for (int i = 0; i < n_sites; ++i)
+            for (int j = 0; j < 3; ++j)
+                velocities[3 * i + j] = velocities[3 * i + j] +
+                                        0.5 * (forces[3 * i + j] + forces_prev[3 * i + j]) /
+                                            masses[i] * *dt_prev;
+    memcpy(positions_prev, positions, sizeof(double) * 3 * (size_t)n_sites);
+    memcpy(forces_prev, forces, sizeof(double) * 3 * (size_t)n_sites);
+    for (int i = 0; i < n_sites; ++i)
+        for (int j = 0; j < 3; ++j)
+            positions[3 * i + j] = positions[3 * i + j] + velocities[3 * i + j] * dt +
+                                   0.5 * forces[3 * i + j] / masses[i] * (dt * dt);
+    *dt_prev = dt;
+}
+
+double orc_mc_move_acceptance(double e_new, double e_prev, double temp)
+{
+    const double kB = (double)(float)8.617333262e-5;
+    double p = exp(-(e_new - e_prev) / (kB * temp));
+    return p < 1.0 ? p : 1.0;
+}
