@@ -1,0 +1,469 @@
+"""Headline benchmark of the SOAP/GAP energy-and-force path on B200.
+
+Workload (the reference's NVE MD configuration): 4,096 carbon atoms at 2.5 g/cm^3 in a cubic
+periodic box (seeded rejection sampling, 1.2 A minimum distance), Maxwell-Boltzmann velocities
+at 3000 K, velocity-Verlet NVE with dt = 1 fs, neighbor list rebuilt every 10 steps with a
+0.3 A skin; SOAP poly3 n_max = l_max = 8, rcut 3.7/3.2 A, sigma 0.5 A; synthetic GAP with
+2,000 sparse points (normalised SOAP vectors of random atoms from 10 further seeded boxes),
+zeta = 4, delta = 1 eV, alphas ~ N(0, 1e-6).
+
+A step is one MD step (geometry refresh or rebuild, descriptor, GAP contraction, adjoint force
+back-scatter, integrator). `value` is atom-steps/s of the mixed-precision path (FP32 descriptor,
+bf16x3 tcgen05 GEMMs, FP64 accumulation), device-timed with CUDA events per step, L2 flushed
+(256 MB write) between timed steps. The plain FP64 path is measured the same way and reported
+beside it. `e2e` drives the same MD through the host-buffer C ABI call (positions in, energies/
+forces/virial out every step, integrator on the host). N > 1 GPUs run independent replicas.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+METRIC = "atom-steps/s & MC moves/s: mixed/surrogate vs plain FP64, 1 B200, at stated RMSE"
+WORKLOAD = ("NVE velocity-Verlet MD, 4096 C atoms, 2.5 g/cm3, dt 1 fs, rebuild every 10 steps, "
+            "skin 0.3 A, SOAP n_max=l_max=8 rcut 3.7/3.2, GAP 2000 sparse zeta=4")
+N_ATOMS = 4096
+N_SPARSE = 2000
+DT = 1.0
+REBUILD = 10
+SKIN = 0.3
+
+
+def _load_package():
+    import importlib.util
+    if "turbogap_b200" in sys.modules:
+        return sys.modules["turbogap_b200"]
+    pkg_dir = os.path.join(ROOT, "turbogap_2.0_b200")
+    spec = importlib.util.spec_from_file_location(
+        "turbogap_b200", os.path.join(pkg_dir, "__init__.py"), submodule_search_locations=[pkg_dir])
+    mod = importlib.util.module_from_spec(spec)
+    sys.modules["turbogap_b200"] = mod
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def _workload(tg, seed):
+    pos, box, sp, masses = tg.synth.random_packing(N_ATOMS, 2.5, 1.2, seed=seed)
+    vel = tg.synth.maxwell_boltzmann(masses, 3000.0, seed=seed + 1)
+    return pos, box, sp, masses, vel
+
+
+def _pool_structures(tg, seed):
+    return [tg.synth.random_packing(N_ATOMS, 2.5, 1.2, seed=seed + 100 + k)[:3] for k in range(10)]
+
+
+def _peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return dict(hbm=p["hbm_gbs"], bf16=p["bf16_tflops"], bf16_sus=p["bf16_tflops_sustained"], src="measured")
+    except Exception:
+        return dict(hbm=6650.0, bf16=1590.0, bf16_sus=1400.0, src="fallback")
+
+
+# ----------------------------------------------------------------------------- clocks
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return dict(sm_mhz=None, sm_max_mhz=None, reasons=["nvidia-smi unavailable"])
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return dict(sm_mhz=float(np.median(sm)) if sm else None, sm_max_mhz=smax, reasons=sorted(reasons),
+                    samples=len(sm))
+
+
+# ----------------------------------------------------------------------------- reference arm
+
+def _oracle_md_steps(orc, hyp, model, pos, box, sp, masses, vel, steps, budget_s, warmup):
+    """velocity_verlet MD of the oracle (FP64 CPU restatement), list rebuilt every REBUILD steps
+    at rcut + skin, geometry refreshed every step. Returns (steps done, seconds)."""
+    H = orc.Hypers(hyp)
+    n = len(pos)
+    x = pos.copy()
+    v = vel.copy()
+    xp = np.zeros_like(x)
+    fp = np.zeros_like(x)
+    mm = masses * 103.6426965268
+    dtp = DT
+    nb = None
+    done = 0
+    t0 = None
+    for k in range(warmup + steps):
+        if k == warmup:
+            t0 = time.perf_counter()
+        if k % REBUILD == 0 or nb is None:
+            nb = orc.build_neighbors(x, n, *box, 3.7 + SKIN, sp, False)
+        else:
+            nb.update(orc.neighbor_geometry(x, n, *box, nb["n_neigh"], nb["neighbors_list"], sp))
+        _, f, _ = orc.get_gap_soap(H, n, nb, sp, 0, model["alphas"], model["Qs"], model["delta"], model["zeta"])
+        dtp = orc.velocity_verlet(x, xp, v, f, fp, mm, DT, dtp, k == 0)
+        if k >= warmup:
+            done += 1
+            if time.perf_counter() - t0 > budget_s:
+                break
+    return done, time.perf_counter() - t0
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    tg = _load_package()
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import helpers
+    import oracle_lib as orc
+    hyp = tg.synth.carbon_hypers()
+    pool = [helpers.oracle_descriptors(hyp, p, b, s) for p, b, s in _pool_structures(tg, 1000)]
+    model = tg.synth.gap_model(np.concatenate(pool), N_SPARSE, seed=7)
+    pos, box, sp, masses, vel = _workload(tg, 0)
+    steps, secs = _oracle_md_steps(orc, hyp, model, pos, box, sp, masses, vel, args.steps, 100.0,
+                                   min(args.warmup, 1))
+    value = N_ATOMS * steps / secs
+    cores = orc.num_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": args.gpus,
+        "steps": steps, "warmup": min(args.warmup, 1), "ms_per_step": 1e3 * secs / max(steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": WORKLOAD},
+        "cpu_baseline": {"value": value, "unit": "atom-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"{steps} MD steps of the 4096-atom box (oracle restatement, not TurboGAP; "
+                                   f"the Fortran reference cannot be compiled here)"},
+        "e2e": {"value": value, "unit": "atom-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# ----------------------------------------------------------------------------- our arm
+
+def _timed_md(tg, torch, ctx, stream, flush, system, model, masses, vel, precision, steps, warmup):
+    md = tg.MD(ctx, system, [model], masses, DT, rebuild_every=REBUILD, precision=precision, use_graph=True)
+    md.set_velocities(vel)
+    with torch.cuda.stream(stream):
+        md.run(warmup)
+        ctx.synchronize()
+        st0 = md.state()
+        l0 = ctx.kernel_launches
+        starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+        for k in range(steps):
+            flush.zero_()
+            starts[k].record(stream)
+            md.run(1)
+            ends[k].record(stream)
+        stream.synchronize()
+    ms = sum(s.elapsed_time(e) for s, e in zip(starts, ends))
+    launches = ctx.kernel_launches - l0
+    st1 = md.state()
+    md.close()
+    return ms, launches, st0, st1
+
+
+def _stage_profile(tg, ctx, system, model, masses, vel, precision, steps=20):
+    """Per-kernel device time from CUDA events around every stage (eager steps, no graph)."""
+    from turbogap_b200 import native
+    import ctypes as C
+    L = native.lib()
+    md = tg.MD(ctx, system, [model], masses, DT, rebuild_every=REBUILD, precision=precision, use_graph=False)
+    md.set_velocities(vel)
+    md.run(2)
+    ctx.synchronize()
+    L.tgap_timing_reset(ctx.h)
+    L.tgap_timing_enable(ctx.h, 1)
+    md.run(steps)
+    L.tgap_timing_enable(ctx.h, 0)
+    cap = 64
+    names = C.create_string_buffer(32 * cap)
+    tot = np.zeros(cap)
+    cnt = np.zeros(cap, np.int64)
+    n = C.c_int(0)
+    L.tgap_timing_report(ctx.h, cap, names, native.ptr(tot), native.ptr(cnt), C.byref(n))
+    out = {}
+    for i in range(n.value):
+        nm = names.raw[32 * i:32 * (i + 1)].split(b"\0")[0].decode()
+        if cnt[i]:
+            out[nm] = dict(total_ms=float(tot[i]), launches=int(cnt[i]), avg_us=1e3 * tot[i] / cnt[i])
+    L.tgap_timing_reset(ctx.h)
+    md.close()
+    return out
+
+
+def _roofline(stages, n_rows, dim, dim_pad, n_sparse, n_sparse_pad, n_pairs, peaks):
+    """Roofline of the dominant kernel: algorithmic work per launch / measured launch time."""
+    if not stages:
+        return None
+    total = sum(v["total_ms"] for v in stages.values())
+    name, st = max(stages.items(), key=lambda kv: kv[1]["total_ms"])
+    t = st["avg_us"] * 1e-6
+    traffic = _ncu_traffic(name)
+    nlm, nmax = 81, 8
+    if name.startswith("gemm_bf16x3"):
+        flops = 2.0 * n_rows * dim * n_sparse
+        ach = flops / t / 1e12
+        return dict(kernel=name, bound="tensor", achieved=ach, peak=peaks["bf16_sus"], unit="TFLOP/s",
+                    frac=ach / peaks["bf16_sus"], traffic=traffic, share=st["total_ms"] / total,
+                    executed_tflops=3.0 * 2.0 * n_rows * dim_pad * n_sparse_pad / t / 1e12,
+                    peak_source=peaks["src"] + " sustained bf16")
+    if name.startswith("soap_forward"):
+        # reads the pair list (xyz, r, species: 36 B/pair), writes c, q (+bf16 split), |p|
+        byts = 36.0 * n_pairs + n_rows * (4.0 * nmax * nlm + 8.0 * dim_pad + 4.0)
+    elif name.startswith("soap_backward"):
+        # reads pairs (+ neighbor index), c, q, g; scatters 3 FP64 forces per pair
+        byts = 40.0 * n_pairs + 24.0 * n_pairs + n_rows * (4.0 * nmax * nlm + 8.0 * dim_pad + 4.0)
+    else:
+        byts = 48.0 * n_pairs
+    ach = byts / t / 1e9
+    return dict(kernel=name, bound="hbm", achieved=ach, peak=peaks["hbm"], unit="GB/s", frac=ach / peaks["hbm"],
+                traffic=traffic, share=st["total_ms"] / total, peak_source=peaks["src"] + " HBM copy")
+
+
+def _ncu_traffic(kernel):
+    """dram bytes per launch of `kernel` from the committed ncu summary, if present."""
+    path = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        parts = line.split()
+        if len(parts) >= 2 and parts[0] == kernel:
+            try:
+                return float(parts[1])
+            except ValueError:
+                return None
+    return None
+
+
+def _e2e(tg, ctx, system, model, masses, vel, pos0, precision, steps):
+    """MD driven through the host-buffer C ABI call (calculate_gap_soap surface): positions
+    host->device, energies/forces/virial device->host every step, integrator on the host."""
+    from turbogap_b200 import native
+    import ctypes as C
+    L = native.lib()
+    n = len(masses)
+    x = np.ascontiguousarray(pos0.copy())
+    v = vel.copy()
+    mm = (masses * 103.6426965268)[:, None]
+    e = np.zeros(n)
+    f = np.zeros((n, 3))
+    fp = np.zeros((n, 3))
+    vir = np.zeros(9)
+    arr = (C.c_void_p * 1)(model.h.value)
+
+    def force(k):
+        st = L.tgap_calculate_gap_soap(ctx.h, system.h, 1, arr, int(precision), native.ptr(x), int(k % REBUILD == 0),
+                                       native.ptr(e), native.ptr(f), native.ptr(vir))
+        native.check(st, ctx.h, "tgap_calculate_gap_soap")
+
+    for k in range(3):  # warm-up
+        force(k)
+    x[:] = pos0
+    t0 = time.perf_counter()
+    for k in range(steps):
+        force(k)
+        if k > 0:
+            v += 0.5 * (f + fp) / mm * DT
+        fp[:] = f
+        x += v * DT + 0.5 * f / mm * DT * DT
+    secs = time.perf_counter() - t0
+    return dict(value=n * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=8 * 3 * n,
+                d2h_bytes_per_step=8 * (4 * n + 9), steps=steps, precision="mixed" if precision else "fp64")
+
+
+def _cpu_baseline(tg, pos, box, sp, masses, vel, model_np):
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as orc
+    hyp = tg.synth.carbon_hypers()
+    steps, secs = _oracle_md_steps(orc, hyp, model_np, pos, box, sp, masses, vel, 1000, 20.0, 0)
+    return dict(value=N_ATOMS * steps / secs, unit="atom-steps/s", cores=orc.num_threads(), kind="port",
+                sample=f"{steps} MD steps of the same 4096-atom box (FP64 oracle restatement with OpenMP, "
+                       f"materialised dq/dr as in the reference; not TurboGAP itself)")
+
+
+def run_ours(args):
+    import torch
+    tg = _load_package()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    seed = 17 * rank
+    pos, box, sp, masses, vel = _workload(tg, seed)
+    ctx = tg.Context(local)
+    stream = torch.cuda.Stream()
+    ctx.set_stream(stream.cuda_stream)
+    hyp = tg.synth.carbon_hypers()
+    # sparse set: descriptors of 10 further seeded boxes, computed on the device (FP64)
+    pool = []
+    dummy = tg.Model(ctx, hyp, np.zeros((1, tg.synth.soap_dim(hyp))), np.zeros(1))
+    for p, b, s in _pool_structures(tg, 1000 + seed):
+        sysp = tg.System(ctx, [(p, b, s)], 3.7)
+        q = torch.zeros((len(s), dummy.dim), dtype=torch.float64, device="cuda")
+        import ctypes as C
+        from turbogap_b200 import native
+        nr = C.c_int(0)
+        torch.cuda.synchronize()
+        native.check(native.lib().tgap_descriptors(ctx.h, sysp.h, dummy.h, 0, C.c_void_p(q.data_ptr()), C.byref(nr)),
+                     ctx.h, "descriptors")
+        ctx.synchronize()
+        pool.append(q.cpu().numpy())
+        sysp.close()
+    dummy.close()
+    model_np = tg.synth.gap_model(np.concatenate(pool), N_SPARSE, seed=7)
+    model = tg.Model(ctx, hyp, model_np["Qs"], model_np["alphas"], model_np["delta"], model_np["zeta"])
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + SKIN)
+    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+
+    # accuracy: single point, mixed vs FP64
+    e64 = torch.zeros(N_ATOMS, dtype=torch.float64, device="cuda")
+    f64 = torch.zeros(3 * N_ATOMS, dtype=torch.float64, device="cuda")
+    v64 = torch.zeros(9, dtype=torch.float64, device="cuda")
+    e32, f32, v32 = torch.zeros_like(e64), torch.zeros_like(f64), torch.zeros_like(v64)
+    torch.cuda.synchronize()
+    system.compute_device([model], tg.TGAP_FP64, e64.data_ptr(), f64.data_ptr(), v64.data_ptr())
+    system.compute_device([model], tg.TGAP_MIXED, e32.data_ptr(), f32.data_ptr(), v32.data_ptr())
+    ctx.synchronize()
+    e_rmse = float(torch.sqrt(torch.mean((e32 - e64) ** 2)))
+    f_rmse = float(torch.sqrt(torch.mean((f32 - f64) ** 2)))
+    n_pairs = system.n_pairs
+
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    ms64, _, _, _ = _timed_md(tg, torch, ctx, stream, flush, system, model, masses, vel, tg.TGAP_FP64,
+                              args.steps, args.warmup)
+    system.set_positions(pos)
+    system.update(True)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ms, launches, st0, st1 = _timed_md(tg, torch, ctx, stream, flush, system, model, masses, vel, tg.TGAP_MIXED,
+                                       args.steps, args.warmup)
+    clk = clocks.stop()
+    torch.cuda.synchronize()
+    if dist:
+        t = torch.tensor([ms, ms64], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms, ms64 = float(t[0]), float(t[1])
+    drift = ((st1["e_pot"] + st1["e_kin"]) - (st0["e_pot"] + st0["e_kin"])) / N_ATOMS
+    value = world * N_ATOMS * args.steps / (ms * 1e-3)
+    value64 = world * N_ATOMS * args.steps / (ms64 * 1e-3)
+
+    # per-kernel times (mixed) and roofline of the dominant kernel
+    system.set_positions(pos)
+    system.update(True)
+    stages = _stage_profile(tg, ctx, system, model, masses, vel, tg.TGAP_MIXED)
+    peaks = _peaks()
+    dim = tg.synth.soap_dim(hyp)
+    roof = _roofline(stages, N_ATOMS, dim, (dim + 127) // 128 * 128, N_SPARSE, (N_SPARSE + 127) // 128 * 128,
+                     n_pairs, peaks)
+    system.set_positions(pos)
+    system.update(True)
+    e2e = _e2e(tg, ctx, system, model, masses, vel, pos, tg.TGAP_MIXED, min(args.steps, 50))
+    if dist:
+        t = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MIN)
+        e2e["value"] = float(t[0]) * world
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = _cpu_baseline(tg, pos, box, sp, masses, vel, model_np)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32 descriptor + bf16x3 tensor-core GEMM, f64 accumulation",
+            "data": "synthetic (seeded random packing, synthetic GAP model)",
+            "config": {"workload": WORKLOAD, "n_atoms": N_ATOMS, "n_sparse": N_SPARSE, "pairs_in_list": n_pairs,
+                       "l2": "flushed between timed steps (256 MB device write, untimed)",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "plain_fp64": {"value": value64, "unit": "atom-steps/s", "ms_per_step": ms64 / args.steps},
+            "speedup_mixed_vs_fp64": value / value64,
+            "accuracy_vs_fp64": {"energy_rmse_meV_per_atom": 1e3 * e_rmse, "force_rmse_meV_per_A": 1e3 * f_rmse},
+            "energy_drift_meV_per_atom": 1e3 * drift,
+            "roofline": roof,
+            "stages_us_per_step": {k: v["total_ms"] * 1e3 / 20 for k, v in stages.items()},
+            "cpu_baseline": cpu,
+            "e2e": e2e,
+            "gpu_launches": launches,
+            "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    model.close()
+    system.close()
+    ctx.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,235 @@
+/*
+ * tgap.h — C ABI of the B200 (sm_100a) SOAP/GAP energy-and-force path.
+ *
+ * Drop-in boundary for the TurboGAP `predict` / `md` / `mc` hot path. The first group of
+ * entry points mirrors, argument for argument, the Fortran routines a TurboGAP build calls
+ * (the Fortran side binds them with ISO_C_BINDING; see fortran/tgap_iface.f90 in the package):
+ *
+ *   tgap_build_neighbors            build_neighbors_list   src/neighbors/neighbors_interface.f90:144
+ *   tgap_number_of_unit_cells       number_of_unit_cells_for_given_cutoff  neighbors_interface.f90:655
+ *   tgap_get_soap                   soap_turbo get_soap    (call site src/gap/gap_interface.f90:301-306)
+ *   tgap_get_soap_energy_and_forces get_soap_energy_and_forces  src/gap/gap.f90:39
+ *   tgap_get_gap_soap               get_gap_soap           src/gap/gap_interface.f90:41
+ *
+ * These take HOST arrays in Fortran layout (column-major, first index fastest, neighbor ids
+ * 1-based supercell indices, self first in every site's neighbor block) and copy to and
+ * from the device inside the call.
+ *
+ * The second group keeps models, structures and MD state resident in HBM (device-pointer
+ * interface, no host copies) for the MD/MC drivers and batched evaluation.
+ *
+ * Conventions: every entry point returns a tgap_status (0 = success) and never aborts.
+ * Output capacities are passed in; a too-small capacity returns TGAP_ERR_CAPACITY and
+ * writes the required size (mirrors the grow-on-demand of check_extend_neighbor_list,
+ * neighbors_interface.f90:526-540). A context owns its device buffers and one CUDA stream;
+ * calls on one context are not thread-safe.
+ */
+#ifndef TGAP_H
+#define TGAP_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    TGAP_OK = 0,
+    TGAP_ERR_ARGUMENT = 1,     /* bad size, null pointer, inconsistent dimensions */
+    TGAP_ERR_CUDA = 2,         /* a CUDA runtime call failed (message: tgap_last_error) */
+    TGAP_ERR_CAPACITY = 3,     /* output capacity too small; required size written back */
+    TGAP_ERR_HYPERS = 4,       /* unsupported descriptor hyperparameters */
+    TGAP_ERR_TIMEOUT = 5,      /* a bounded device wait gave up */
+    TGAP_ERR_UNSUPPORTED = 6,  /* valid in the reference, not implemented on this path */
+    TGAP_ERR_NOMEM = 7,        /* device allocation failed */
+    TGAP_ERR_NUMERIC = 8       /* non-finite input or result detected */
+} tgap_status;
+
+typedef enum { TGAP_FP64 = 0, TGAP_MIXED = 1 } tgap_precision;
+
+typedef struct tgap_context tgap_context;
+
+/* ------------------------------------------------------------------ context */
+
+int tgap_create(int device, tgap_context **ctx);
+int tgap_destroy(tgap_context *ctx);
+/* Use an external stream (cudaStream_t) for all later work; NULL restores the own stream. */
+int tgap_set_stream(tgap_context *ctx, void *stream);
+int tgap_synchronize(tgap_context *ctx);
+const char *tgap_last_error(const tgap_context *ctx);
+const char *tgap_version(void);
+/* Number of kernels this library launched on ctx since creation (instrumentation). */
+int64_t tgap_kernel_launches(const tgap_context *ctx);
+/* Stage timing (the tracing counterpart of the reference's time_start/time_end,
+ * src/utils/timing.f90:117-131): when enabled, CUDA events bracket every kernel stage on the
+ * context stream (outside graph capture). tgap_timing_report synchronizes and returns up to
+ * `cap` stages: names (32 chars each, NUL padded), total milliseconds and launch counts. */
+int tgap_timing_enable(tgap_context *ctx, int enable);
+int tgap_timing_reset(tgap_context *ctx);
+int tgap_timing_report(tgap_context *ctx, int cap, char *names, double *total_ms,
+                       int64_t *counts, int *n_stages);
+
+/* ------------------------------------------------------------------ reference call surface */
+
+/* neighbors_interface.f90:655-708: replicas per lattice vector so that the cell's planes are
+ * at least 2*rcut apart. Pure host arithmetic. */
+int tgap_number_of_unit_cells(const double a_box[3], const double b_box[3],
+                              const double c_box[3], double rcut, int indices[3]);
+
+/* build_neighbors_list (neighbors_interface.f90:144-524), single rank, all sites owned.
+ *  positions           3 x n_sites_supercell (supercell already replicated, read_xyz.f90:323)
+ *  box_small           any(indices > 1): the brute-force path is used, as in the reference
+ *  rebuild             1: build the list; 0: keep n_neigh/neighbors_list (inputs) and only
+ *                      refresh rjs/xyz/thetas/phis/neighbor_species (:445-510)
+ *  capacity            length of neighbors_list and of the per-pair outputs
+ *  n_atom_pairs        in/out: pairs written (or required, with TGAP_ERR_CAPACITY)
+ * Pair lists are bit-identical to the reference ordering (cell traversal z->y->x with LIFO
+ * cells, or ascending supercell index on the brute-force path). */
+int tgap_build_neighbors(tgap_context *ctx, int n_sites, int n_sites_supercell,
+                         const double *positions, const double a_box[3], const double b_box[3],
+                         const double c_box[3], int box_small, double rcut_max,
+                         const int *species_supercell, int rebuild, int *n_neigh,
+                         int *neighbors_list, double *rjs, double *xyz, double *thetas,
+                         double *phis, int *neighbor_species, int64_t capacity,
+                         int64_t *n_atom_pairs);
+
+/* soap_turbo get_soap, argument order of gap_interface.f90:301-306 (do_timing dropped).
+ *  species              max_species_multiplicity x n_sites (only multiplicity 1 supported)
+ *  mask                 n_atom_pairs x n_species, nonzero = neighbor belongs to the channel
+ *  basis                "poly3" (poly3gauss: TGAP_ERR_UNSUPPORTED)
+ *  scaling_mode         "polynomial"
+ *  compress_soap        must be 0 (compression: TGAP_ERR_UNSUPPORTED)
+ *  soap                 out, n_soap x n_sites (normalised q)
+ *  soap_cart_der        out, 3 x n_soap x n_atom_pairs (dq_i/dr_j; self slot = -sum), or NULL
+ *                       when do_derivatives == 0 */
+int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh, int n_species,
+                  const int *species, const int *species_multiplicity, int n_atom_pairs,
+                  const unsigned char *mask, const double *rjs, const double *thetas,
+                  const double *phis, const int *alpha_max, int l_max,
+                  const double *rcut_hard, const double *rcut_soft, const double *nf,
+                  const double *global_scaling, const double *atom_sigma_r,
+                  const double *atom_sigma_r_scaling, const double *atom_sigma_t,
+                  const double *atom_sigma_t_scaling, const double *amplitude_scaling,
+                  int radial_enhancement, const double *central_weight, const char *basis,
+                  const char *scaling_mode, int do_derivatives, int compress_soap,
+                  int compress_P_nonzero, const int *compress_P_i, const int *compress_P_j,
+                  const double *compress_P_el, double *soap, double *soap_cart_der);
+
+/* get_soap_energy_and_forces (gap.f90:39-244).
+ *  soap (n_soap x n_sites), soap_der (3 x n_soap x n_atom_pairs), Qs (n_soap x n_sparse)
+ *  forces (3 x n_sites0): n_sites0 is the fold modulus of neighbors_list (gap.f90:118,196)
+ *  virial (3 x 3) */
+int tgap_get_soap_energy_and_forces(tgap_context *ctx, int n_soap, int n_sites, int n_sparse,
+                                    const double *soap, const double *soap_der,
+                                    const double *alphas, double delta, double zeta0,
+                                    double e0, const double *Qs, const int *n_neigh,
+                                    const int *neighbors_list, const double *xyz,
+                                    int n_atom_pairs, int do_forces, int n_sites0,
+                                    double *energies, double *forces, double *virial);
+
+/* Descriptor hyperparameters of one soap_turbo model (read_gap.f90:156-432), per species. */
+typedef struct {
+    int n_species;
+    const int *alpha_max;
+    int l_max;
+    const double *rcut_hard, *rcut_soft, *nf, *global_scaling;
+    const double *atom_sigma_r, *atom_sigma_r_scaling, *atom_sigma_t, *atom_sigma_t_scaling;
+    const double *amplitude_scaling, *central_weight;
+    int radial_enhancement;
+} tgap_soap_hypers;
+
+/* get_gap_soap (gap_interface.f90:41-433) for one model on the global neighbor list:
+ * subset (rjs < max rcut_hard, species known), central-species filter, descriptor,
+ * energies/forces/virial, scatter back to global indices.
+ *  species_supercell    species channel 1..n_species per supercell atom (0 = not seen by the
+ *                       model); tgap_assign_species maps character*8 names to it
+ *  energies0 (n_total_sites), forces0 (3 x n_total_sites): overwritten for touched sites
+ *  soap_out             optional (NULL), n_soap x n_sites0 (write_soap, :391-401)
+ *  precision            TGAP_FP64 or TGAP_MIXED
+ * Forces are computed without materialising dq/dr (adjoint back-scatter). */
+int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hypers, int n_total_sites,
+                      int n_sites0, const int *n_neigh0, const int *neighbors_list0,
+                      const double *rjs0, const double *xyz0, const int *species_supercell,
+                      int central_species, int n_sparse, const double *alphas,
+                      const double *Qs, double delta, double zeta, int do_forces,
+                      int precision, double *energies0, double *forces0, double *virial,
+                      double *soap_out);
+
+/* assign_species_multiplicity (soap_turbo; call site gap_interface.f90:175): map Fortran
+ * character*8 species names to channel ids. species_types: n_species x 8 chars, names:
+ * n x 8 chars (blank padded). out: channel 1..n_species, 0 if absent. Duplicated
+ * species_types (multiplicity > 1) returns TGAP_ERR_UNSUPPORTED. */
+int tgap_assign_species(int n_species, const char *species_types, int n, const char *names,
+                        int *out);
+
+/* ------------------------------------------------------------------ resident (device) API */
+
+typedef struct tgap_model tgap_model;
+typedef struct tgap_system tgap_system;
+
+/* One soap_turbo GAP model resident on the device. Qs: n_soap x n_sparse (Fortran layout,
+ * read_gap.f90:810-827). central_species: 0 = all sites. */
+int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
+                      int n_sparse, const double *alphas, const double *Qs, double delta,
+                      double zeta, tgap_model **model);
+int tgap_model_destroy(tgap_model *model);
+int tgap_model_dim(const tgap_model *model);
+
+/* A batch of periodic structures resident on the device. Structure b holds atoms
+ * [offsets[b], offsets[b+1]); boxes: 9 doubles per structure (rows a, b, c); species:
+ * channel ids. Small cells are replicated internally (read_xyz.f90:323-373). */
+int tgap_system_create(tgap_context *ctx, int n_structures, const int *offsets,
+                       const double *positions, const double *boxes, const int *species,
+                       double rcut_max, tgap_system **system);
+int tgap_system_destroy(tgap_system *system);
+int tgap_system_n_atoms(const tgap_system *system);
+/* Device pointer to the 3 x n_atoms positions (read/write, layout as on input). */
+int tgap_system_positions(tgap_system *system, double **d_positions);
+/* Copy host positions (3 x n_atoms) into the resident structure. */
+int tgap_system_set_positions(tgap_system *system, const double *positions);
+/* Rebuild the neighbor lists (or only refresh geometry when rebuild == 0). */
+int tgap_system_update(tgap_system *system, int rebuild);
+int64_t tgap_system_n_pairs(const tgap_system *system);
+
+/* Energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure), device pointers,
+ * summed over models (e0 = 0). Overwrites the outputs. */
+int tgap_compute(tgap_context *ctx, tgap_system *system, int n_models,
+                 tgap_model *const *models, int precision, int do_forces, double *d_energies,
+                 double *d_forces, double *d_virial);
+
+/* calculate_gap_soap (src/gap/calculate_gap_soap.f90:171-481) with HOST buffers: copies
+ * `positions` (3 x n_atoms, NULL = keep the resident ones) to the device, rebuilds the
+ * neighbor list when rebuild != 0 (else refreshes geometry), evaluates all models and copies
+ * energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure) back. */
+int tgap_calculate_gap_soap(tgap_context *ctx, tgap_system *system, int n_models,
+                            tgap_model *const *models, int precision, const double *positions,
+                            int rebuild, double *energies, double *forces, double *virial);
+
+/* Normalised descriptors of every atom seen by the model (rows in site order), device
+ * pointer out (n_sites x n_soap). */
+int tgap_descriptors(tgap_context *ctx, tgap_system *system, const tgap_model *model,
+                     int precision, double *d_soap, int *n_rows);
+
+/* ------------------------------------------------------------------ MD driver */
+
+typedef struct tgap_md tgap_md;
+
+/* NVE velocity Verlet (md_utils.f90:486-532) on one resident structure. masses: amu.
+ * The neighbor list uses rcut_max + skin and is rebuilt every `rebuild_every` steps;
+ * geometry is refreshed every step. use_graph != 0 captures one step in a CUDA graph. */
+int tgap_md_create(tgap_context *ctx, tgap_system *system, int n_models,
+                   tgap_model *const *models, const double *masses_amu, double dt,
+                   int rebuild_every, int precision, int use_graph, tgap_md **md);
+int tgap_md_destroy(tgap_md *md);
+int tgap_md_set_velocities(tgap_md *md, const double *velocities);
+int tgap_md_run(tgap_md *md, int n_steps);
+/* Host copies of the current state; any pointer may be NULL. energies: potential and
+ * kinetic energy (eV) of the last step. */
+int tgap_md_get_state(tgap_md *md, double *positions, double *velocities, double *forces,
+                      double *e_pot, double *e_kin);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,310 @@
+"""Parity of the sm_100a path (through the C ABI) with the CPU oracle.
+
+Bars: neighbor pairs bit-exact (list order, rjs and xyz bits); FP64 energies within
+1e-10 eV/atom, forces within 1e-8 eV/A, virial within 1e-8 eV; descriptors within 1e-12
+(q) and 1e-10 (dq/dr). Mixed precision (FP32 descriptor, bf16x3 tensor-core GEMM) is held to
+energy RMSE <= 0.5 meV/atom and force RMSE <= 5 meV/A against FP64.
+"""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import helpers
+import oracle_lib as orc
+
+pytestmark = pytest.mark.gpu
+
+E_TOL = 1e-10   # eV / atom
+F_TOL = 1e-8    # eV / A
+V_TOL = 1e-8    # eV
+
+
+@pytest.fixture(scope="module")
+def ctx(tg):
+    import torch
+    assert torch.cuda.is_available()
+    c = tg.Context(0)
+    yield c
+    c.close()
+
+
+def _device(n, torch):
+    return torch.zeros(n, dtype=torch.float64, device="cuda")
+
+
+def _compute(tg, ctx, system, models, precision, n, nst=1):
+    import torch
+    e = _device(n, torch)
+    f = _device(3 * n, torch)
+    v = _device(9 * nst, torch)
+    torch.cuda.synchronize()
+    system.compute_device(models, precision, e.data_ptr(), f.data_ptr(), v.data_ptr())
+    ctx.synchronize()
+    return e.cpu().numpy(), f.cpu().numpy().reshape(n, 3), v.cpu().numpy().reshape(nst, 3, 3)
+
+
+# ------------------------------------------------------------------------- neighbors
+
+def _nb_compare(nb_g, nb_o):
+    assert np.array_equal(nb_g["n_neigh"], nb_o["n_neigh"])
+    assert np.array_equal(nb_g["neighbors_list"], nb_o["neighbors_list"])
+    assert np.array_equal(nb_g["rjs"], nb_o["rjs"])  # bit-exact distances
+    assert np.array_equal(nb_g["xyz"], nb_o["xyz"])
+    assert np.array_equal(nb_g["neighbor_species"], nb_o["neighbor_species"])
+    assert np.allclose(nb_g["thetas"], nb_o["thetas"], rtol=0, atol=1e-14)
+    assert np.allclose(nb_g["phis"], nb_o["phis"], rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("case", ["diamond_m2", "packing_m4", "packing_large"])
+def test_neighbors_cell_path_bit_exact(ctx, synth, case):
+    if case == "diamond_m2":
+        pos, box, sp = synth.diamond_supercell(3, seed=7)
+        rc = 3.7
+    elif case == "packing_m4":
+        pos, box, sp, _ = synth.random_packing(500, 2.5, 1.2, seed=8)
+        rc = 4.0
+    else:
+        pos, box, sp, _ = synth.random_packing(4096, 2.5, 1.2, seed=9)
+        rc = 4.0
+    nb_o = orc.build_neighbors(pos, len(pos), *box, rc, sp, False)
+    nb_g = ctx.build_neighbors_list(pos, len(pos), *box, rc, sp, box_small=False)
+    _nb_compare(nb_g, nb_o)
+
+
+@pytest.mark.parametrize("strain", [0.0, 0.04])
+def test_neighbors_brute_force_and_supercell_bit_exact(ctx, synth, strain):
+    pos, box, sp, _ = synth.random_packing(40, 2.0, 1.2, seed=10, strain=strain)
+    idx = orc.number_of_unit_cells(*box, 3.7)
+    pos_sc, sp_sc, a, b, c = orc.set_supercell(pos, sp, idx, *box)
+    small = bool(np.any(idx > 1))
+    nb_o = orc.build_neighbors(pos_sc, len(pos), a, b, c, 3.7, sp_sc, small)
+    nb_g = ctx.build_neighbors_list(pos_sc, len(pos), a, b, c, 3.7, sp_sc, box_small=small)
+    _nb_compare(nb_g, nb_o)
+
+
+def test_neighbors_triclinic_no_replica(ctx, synth):
+    pos, box, sp, _ = synth.random_packing(400, 2.0, 1.2, seed=11, strain=0.05)
+    nb_o = orc.build_neighbors(pos, len(pos), *box, 3.7, sp, False)
+    nb_g = ctx.build_neighbors_list(pos, len(pos), *box, 3.7, sp, box_small=False)
+    _nb_compare(nb_g, nb_o)
+
+
+def test_neighbors_geometry_refresh(ctx, synth):
+    pos, box, sp, _ = synth.random_packing(300, 2.5, 1.2, seed=12)
+    nb = orc.build_neighbors(pos, len(pos), *box, 4.0, sp, False)
+    moved = pos + np.random.default_rng(0).uniform(-0.1, 0.1, pos.shape)
+    geo_o = orc.neighbor_geometry(moved, len(pos), *box, nb["n_neigh"], nb["neighbors_list"], sp)
+    geo_g = ctx.build_neighbors_list(moved, len(pos), *box, 4.0, sp, rebuild=False, n_neigh=nb["n_neigh"],
+                                     neighbors_list=nb["neighbors_list"])
+    assert np.array_equal(geo_g["rjs"], geo_o["rjs"]) and np.array_equal(geo_g["xyz"], geo_o["xyz"])
+
+
+def test_neighbors_capacity_overflow_reports_required_size(ctx, synth, tg):
+    from turbogap_b200 import native
+    pos, box, sp = synth.diamond_supercell(3, noise=0.0)
+    n = len(pos)
+    cap = 10
+    buf_i = np.zeros(cap, np.int32)
+    buf_d = np.zeros(cap)
+    buf_x = np.zeros(3 * cap)
+    nn = np.zeros(n, np.int32)
+    npairs = C.c_int64(0)
+    st = native.lib().tgap_build_neighbors(
+        ctx.h, n, n, native.ptr(np.ascontiguousarray(pos)), native.ptr(box[0].copy()), native.ptr(box[1].copy()),
+        native.ptr(box[2].copy()), 0, 3.7, native.ptr(sp), 1, native.ptr(nn), native.ptr(buf_i), native.ptr(buf_d),
+        native.ptr(buf_x), native.ptr(buf_d), native.ptr(buf_d), native.ptr(buf_i), cap, C.byref(npairs))
+    assert st == 3 and npairs.value == 35 * n
+
+
+# ------------------------------------------------------------------------- descriptor
+
+def _soap_inputs(synth, seed, n_species=1):
+    if n_species == 1:
+        hyp = synth.carbon_hypers()
+        pos, box, sp = synth.diamond_supercell(2, seed=seed)
+    else:
+        hyp = synth.sio2_hypers()
+        pos, box, sp, _ = synth.random_packing(
+            48, 2.2, {("Si", "O"): 1.4, ("O", "O"): 2.2, ("Si", "Si"): 2.5}, {"Si": 1 / 3, "O": 2 / 3}, seed=seed)
+    rc = max(hyp["rcut_hard"])
+    idx = orc.number_of_unit_cells(*box, rc)
+    small = bool(np.any(idx > 1))
+    pos_sc, sp_sc, a, b, c = orc.set_supercell(pos, sp, idx, *box)
+    nb = orc.build_neighbors(pos_sc, len(pos), a, b, c, rc, sp_sc, small)
+    ns = len(hyp["alpha_max"])
+    mask = np.stack([nb["neighbor_species"] == s + 1 for s in range(ns)], axis=1)
+    return hyp, nb, mask
+
+
+@pytest.mark.parametrize("n_species", [1, 2])
+def test_get_soap_matches_oracle(ctx, synth, n_species):
+    hyp, nb, mask = _soap_inputs(synth, 21, n_species)
+    q_o, d_o = orc.get_soap(orc.Hypers(hyp), nb["n_neigh"], mask, nb["rjs"], nb["thetas"], nb["phis"])
+    q_g, d_g = ctx.get_soap(hyp, nb["n_neigh"], mask, nb["rjs"], nb["thetas"], nb["phis"])
+    assert np.max(np.abs(q_g - q_o)) < 1e-12
+    assert np.max(np.abs(d_g - d_o)) < 1e-10
+
+
+def test_get_soap_energy_and_forces_matches_oracle(ctx, synth):
+    hyp, nb, mask = _soap_inputs(synth, 22)
+    H = orc.Hypers(hyp)
+    q, der = orc.get_soap(H, nb["n_neigh"], mask, nb["rjs"], nb["thetas"], nb["phis"])
+    model = synth.gap_model(q, 30, seed=3)
+    n = len(nb["n_neigh"])
+    args = (q, der, model["alphas"], 1.0, 4.0, 0.0, model["Qs"], nb["n_neigh"], nb["neighbors_list"], nb["xyz"])
+    e_o, f_o, v_o = orc.soap_energy_and_forces(*args, n_sites0=n)
+    e_g, f_g, v_g = ctx.get_soap_energy_and_forces(*args, n_sites0=n)
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g - v_o)) < V_TOL
+
+
+# ------------------------------------------------------------------------- GAP
+
+@pytest.fixture(scope="module")
+def carbon(synth):
+    hyp, m = helpers.carbon_model(synth, 200, seed=5)
+    return hyp, m
+
+
+def test_get_gap_soap_fp64_matches_oracle(ctx, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp = synth.diamond_supercell(3, seed=31)
+    n = len(pos)
+    nb = orc.build_neighbors(pos, n, *box, 3.7, sp, False)
+    e_o, f_o, v_o = orc.get_gap_soap(orc.Hypers(hyp), n, nb, sp, 0, m["alphas"], m["Qs"], 1.0, 4.0)
+    e_g, f_g, v_g = ctx.get_gap_soap(hyp, n, nb, sp, 0, m["alphas"], m["Qs"], 1.0, 4.0)
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g - v_o)) < V_TOL
+
+
+def test_resident_compute_fp64_matches_oracle(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(256, 2.5, 1.2, seed=32)
+    e_o, f_o, v_o = helpers.oracle_structure_eval(hyp, [m], pos, box, sp)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7)
+    e_g, f_g, v_g = _compute(tg, ctx, system, [model], tg.TGAP_FP64, len(pos))
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g[0] - v_o)) < V_TOL
+
+
+def test_batched_uneven_triclinic_structures(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    structs = []
+    for k, n in enumerate([32, 77, 150]):
+        pos, box, sp, _ = synth.random_packing(n, 1.5 + k, 1.1, seed=40 + k, strain=0.05)
+        structs.append((pos, box, sp))
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, structs, 3.7)
+    ntot = sum(len(s[2]) for s in structs)
+    e_g, f_g, v_g = _compute(tg, ctx, system, [model], tg.TGAP_FP64, ntot, nst=len(structs))
+    off = 0
+    for b, (pos, box, sp) in enumerate(structs):
+        e_o, f_o, v_o = helpers.oracle_structure_eval(hyp, [m], pos, box, sp)
+        n = len(pos)
+        assert np.max(np.abs(e_g[off:off + n] - e_o)) < E_TOL
+        assert np.max(np.abs(f_g[off:off + n] - f_o)) < F_TOL
+        assert np.max(np.abs(v_g[b] - v_o)) < V_TOL
+        off += n
+
+
+def test_two_species_two_models(ctx, tg, synth):
+    hyp = synth.sio2_hypers()
+    dmin = {("Si", "O"): 1.4, ("O", "O"): 2.2, ("Si", "Si"): 2.5}
+    pool_q = []
+    for k in range(2):
+        p, bx, s, _ = synth.random_packing(48, 2.2, dmin, {"Si": 1 / 3, "O": 2 / 3}, seed=50 + k)
+        pool_q.append((helpers.oracle_descriptors(hyp, p, bx, s, 1), helpers.oracle_descriptors(hyp, p, bx, s, 2)))
+    mSi = synth.gap_model(np.concatenate([a for a, _ in pool_q]), 20, seed=1)
+    mO = synth.gap_model(np.concatenate([b for _, b in pool_q]), 20, seed=2)
+    mSi["central_species"] = 1
+    mO["central_species"] = 2
+    pos, box, sp, _ = synth.random_packing(48, 2.2, dmin, {"Si": 1 / 3, "O": 2 / 3}, seed=55)
+    e_o, f_o, v_o = helpers.oracle_structure_eval(hyp, [mSi, mO], pos, box, sp)
+    models = [tg.Model(ctx, hyp, mm["Qs"], mm["alphas"], 1.0, 4.0, central_species=mm["central_species"])
+              for mm in (mSi, mO)]
+    system = tg.System(ctx, [(pos, box, sp)], 5.0)
+    e_g, f_g, v_g = _compute(tg, ctx, system, models, tg.TGAP_FP64, len(pos))
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g[0] - v_o)) < V_TOL
+
+
+def test_isolated_atom_and_dimer(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    box = np.diag([30.0, 30.0, 30.0])
+    for pos in (np.array([[15.0, 15.0, 15.0]]), np.array([[15.0, 15.0, 15.0], [16.3, 15.2, 14.9]])):
+        sp = np.ones(len(pos), np.int32)
+        e_o, f_o, _ = helpers.oracle_structure_eval(hyp, [m], pos, box, sp)
+        system = tg.System(ctx, [(pos, box, sp)], 3.7)
+        e_g, f_g, _ = _compute(tg, ctx, system, [model], tg.TGAP_FP64, len(pos))
+        assert np.max(np.abs(e_g - e_o)) < E_TOL
+        assert np.max(np.abs(f_g - f_o)) < F_TOL
+        if len(pos) == 2:
+            assert np.allclose(f_g[0], -f_g[1], atol=1e-14)
+
+
+def test_bad_hypers_raise(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    bad = dict(hyp, l_max=20)
+    with pytest.raises(tg.TgapError):
+        tg.Model(ctx, bad, m["Qs"], m["alphas"])
+
+
+# ------------------------------------------------------------------------- mixed precision
+
+def test_mixed_precision_rmse_against_fp64(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(512, 2.5, 1.2, seed=60)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7)
+    e64, f64, v64 = _compute(tg, ctx, system, [model], tg.TGAP_FP64, len(pos))
+    e32, f32, v32 = _compute(tg, ctx, system, [model], tg.TGAP_MIXED, len(pos))
+    e_rmse = np.sqrt(np.mean((e32 - e64) ** 2))
+    f_rmse = np.sqrt(np.mean((f32 - f64) ** 2))
+    assert e_rmse < 0.5e-3 and f_rmse < 5e-3, (e_rmse, f_rmse)
+    # tighter sanity: the split-bf16 GEMM keeps ~16 mantissa bits
+    assert e_rmse < 1e-5 * max(1.0, np.abs(e64).max() * 1e3)
+
+
+def test_mixed_get_gap_soap_matches_resident_mixed(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp = synth.diamond_supercell(3, seed=61)
+    n = len(pos)
+    nb = orc.build_neighbors(pos, n, *box, 3.7, sp, False)
+    e64, f64, _ = ctx.get_gap_soap(hyp, n, nb, sp, 0, m["alphas"], m["Qs"], 1.0, 4.0)
+    e32, f32, _ = ctx.get_gap_soap(hyp, n, nb, sp, 0, m["alphas"], m["Qs"], 1.0, 4.0, precision=tg.TGAP_MIXED)
+    assert np.sqrt(np.mean((e32 - e64) ** 2)) < 0.5e-3
+    assert np.sqrt(np.mean((f32 - f64) ** 2)) < 5e-3
+
+
+# ------------------------------------------------------------------------- MD
+
+def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, masses = synth.random_packing(128, 2.5, 1.2, seed=70)
+    vel = synth.maxwell_boltzmann(masses, 3000.0, seed=1)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=10, use_graph=True)
+    md.set_velocities(vel)
+    steps = 12
+    md.run(steps)
+    st = md.state()
+    # oracle: forces at x(t) then velocity_verlet, list rebuilt every step at the model cutoff
+    x = pos.copy()
+    v = vel.copy()
+    xp = np.zeros_like(x)
+    fp = np.zeros_like(x)
+    mm = masses * synth.AMU_TO_EV_FS2_A2
+    dtp = 1.0
+    for k in range(steps):
+        _, f, _ = helpers.oracle_structure_eval(hyp, [m], x, box, sp)
+        dtp = orc.velocity_verlet(x, xp, v, f, fp, mm, 1.0, dtp, k == 0)
+    assert np.max(np.abs(st["positions"] - x)) < 1e-9
+    assert np.max(np.abs(st["velocities"] - v)) < 1e-9

@@ -1,0 +1,321 @@
+"""Host-side mirror of TurboGAP's SOAP/GAP operator interface, backed by libtgap (sm_100a).
+
+Reference routines and their counterparts here (arrays in numpy row-major form, which is the
+Fortran column-major layout of the reference read with the first index fastest: positions
+(N, 3) == positions(3, N), soap (n_sites, D) == soap(D, n_sites), soap_cart_der (P, D, 3) ==
+soap_cart_der(3, D, P), Qs (n_sparse, D) == Qs(D, n_sparse)):
+
+    build_neighbors_list        src/neighbors/neighbors_interface.f90:144   Context.build_neighbors_list
+    get_soap (soap_turbo)       src/gap/gap_interface.f90:301-306          Context.get_soap
+    get_soap_energy_and_forces  src/gap/gap.f90:39                         Context.get_soap_energy_and_forces
+    get_gap_soap                src/gap/gap_interface.f90:41               Context.get_gap_soap
+    calculate_gap_soap          src/gap/calculate_gap_soap.f90:171         System.compute (all models)
+    velocity_verlet MD step     src/md/md_utils.f90:486                    MD
+
+Errors raise TgapError with the library status (see include/tgap.h), mirroring the points
+where the reference would stop.
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import native as N
+from .native import TGAP_FP64, TGAP_MIXED, TgapError, check, ptr  # noqa: F401
+
+
+def _f64(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class Context:
+    """One device, one stream, reusable device buffers (tgap_context)."""
+
+    def __init__(self, device=0):
+        self._L = N.lib()
+        h = C.c_void_p()
+        st = self._L.tgap_create(int(device), C.byref(h))
+        if st != 0:
+            raise TgapError(st, f"tgap_create(device={device}) failed")
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if getattr(self, "h", None):
+            self._L.tgap_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def synchronize(self):
+        check(self._L.tgap_synchronize(self.h), self.h, "synchronize")
+
+    def set_stream(self, stream_handle):
+        check(self._L.tgap_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
+              self.h, "set_stream")
+
+    @property
+    def kernel_launches(self):
+        return int(self._L.tgap_kernel_launches(self.h))
+
+    # ------------------------------------------------------------ reference call surface
+
+    @staticmethod
+    def number_of_unit_cells(a, b, c, rcut):
+        idx = np.zeros(3, np.int32)
+        check(N.lib().tgap_number_of_unit_cells(ptr(_f64(a)), ptr(_f64(b)), ptr(_f64(c)), float(rcut), ptr(idx)))
+        return idx
+
+    def build_neighbors_list(self, positions, n_sites, a, b, c, rcut_max, species_supercell,
+                             box_small=False, rebuild=True, n_neigh=None, neighbors_list=None,
+                             capacity=None):
+        """build_neighbors_list: positions (N_sc, 3) of the (replicated) supercell."""
+        pos = _f64(positions)
+        nsc = pos.shape[0]
+        sp = _i32(species_supercell)
+        a, b, c = _f64(a), _f64(b), _f64(c)
+        if rebuild:
+            cap = int(capacity) if capacity else 100 * n_sites  # neighbors_interface.f90:283
+            while True:
+                nn = np.zeros(n_sites, np.int32)
+                nl = np.zeros(cap, np.int32)
+                rjs = np.zeros(cap)
+                xyz = np.zeros((cap, 3))
+                th = np.zeros(cap)
+                ph = np.zeros(cap)
+                nsp = np.zeros(cap, np.int32)
+                npairs = C.c_int64(0)
+                st = self._L.tgap_build_neighbors(self.h, n_sites, nsc, ptr(pos), ptr(a), ptr(b), ptr(c),
+                                                  int(box_small), float(rcut_max), ptr(sp), 1, ptr(nn), ptr(nl),
+                                                  ptr(rjs), ptr(xyz), ptr(th), ptr(ph), ptr(nsp), cap,
+                                                  C.byref(npairs))
+                if st == 3:  # TGAP_ERR_CAPACITY: grow and retry (check_extend_neighbor_list)
+                    cap = int(npairs.value)
+                    continue
+                check(st, self.h, "tgap_build_neighbors")
+                P = int(npairs.value)
+                return dict(n_neigh=nn, neighbors_list=nl[:P].copy(), rjs=rjs[:P].copy(), xyz=xyz[:P].copy(),
+                            thetas=th[:P].copy(), phis=ph[:P].copy(), neighbor_species=nsp[:P].copy())
+        nn = _i32(n_neigh)
+        nl = _i32(neighbors_list)
+        P = nl.shape[0]
+        rjs = np.zeros(P); xyz = np.zeros((P, 3)); th = np.zeros(P); ph = np.zeros(P)
+        nsp = np.zeros(P, np.int32)
+        npairs = C.c_int64(P)
+        check(self._L.tgap_build_neighbors(self.h, n_sites, nsc, ptr(pos), ptr(a), ptr(b), ptr(c), int(box_small),
+                                           float(rcut_max), ptr(sp), 0, ptr(nn), ptr(nl), ptr(rjs), ptr(xyz),
+                                           ptr(th), ptr(ph), ptr(nsp), P, C.byref(npairs)),
+              self.h, "tgap_build_neighbors")
+        return dict(n_neigh=nn, neighbors_list=nl, rjs=rjs, xyz=xyz, thetas=th, phis=ph, neighbor_species=nsp)
+
+    def get_soap(self, hypers, n_neigh, mask, rjs, thetas, phis, do_derivatives=True, basis="poly3",
+                 scaling_mode="polynomial"):
+        """soap_turbo get_soap. mask: (P, n_species) bool. Returns soap (n_sites, D) and,
+        when do_derivatives, soap_cart_der (P, D, 3)."""
+        nn = _i32(n_neigh)
+        n_sites = nn.shape[0]
+        rjs = _f64(rjs)
+        P = rjs.shape[0]
+        ns = len(hypers["alpha_max"])
+        m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(P, ns).T)
+        nmax = int(np.sum(hypers["alpha_max"]))
+        D = nmax * (nmax + 1) // 2 * (int(hypers["l_max"]) + 1)
+        soap = np.zeros((n_sites, D))
+        der = np.zeros((P, D, 3)) if do_derivatives else None
+        hv = {k: _f64(np.broadcast_to(np.asarray(hypers[k], float), (ns,))) for k in N.HYPER_KEYS}
+        am = _i32(hypers["alpha_max"])
+        check(self._L.tgap_get_soap(
+            self.h, n_sites, ptr(nn), ns, None, None, P, ptr(m), ptr(rjs), ptr(_f64(thetas)), ptr(_f64(phis)),
+            ptr(am), int(hypers["l_max"]), ptr(hv["rcut_hard"]), ptr(hv["rcut_soft"]), ptr(hv["nf"]),
+            ptr(hv["global_scaling"]), ptr(hv["atom_sigma_r"]), ptr(hv["atom_sigma_r_scaling"]),
+            ptr(hv["atom_sigma_t"]), ptr(hv["atom_sigma_t_scaling"]), ptr(hv["amplitude_scaling"]),
+            int(hypers.get("radial_enhancement", 0)), ptr(hv["central_weight"]), basis.encode(),
+            scaling_mode.encode(), int(do_derivatives), 0, 0, None, None, None, ptr(soap), ptr(der)),
+            self.h, "tgap_get_soap")
+        return soap, der
+
+    def get_soap_energy_and_forces(self, soap, soap_der, alphas, delta, zeta, e0, Qs, n_neigh,
+                                   neighbors_list, xyz, do_forces=True, n_sites0=None):
+        soap = _f64(soap)
+        n_sites, D = soap.shape
+        Qs = _f64(Qs)
+        M = Qs.shape[0]
+        nn = _i32(n_neigh)
+        nl = _i32(neighbors_list)
+        P = nl.shape[0]
+        if n_sites0 is None:
+            n_sites0 = n_sites
+        en = np.zeros(n_sites)
+        fo = np.zeros((n_sites0, 3))
+        vir = np.zeros(9)
+        check(self._L.tgap_get_soap_energy_and_forces(
+            self.h, D, n_sites, M, ptr(soap), ptr(_f64(soap_der)) if do_forces else None, ptr(_f64(alphas)),
+            float(delta), float(zeta), float(e0), ptr(Qs), ptr(nn), ptr(nl), ptr(_f64(xyz)), P, int(do_forces),
+            int(n_sites0), ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_soap_energy_and_forces")
+        return en, fo, vir.reshape(3, 3, order="F")
+
+    def get_gap_soap(self, hypers, n_total_sites, nb, species_supercell, central_species, alphas, Qs, delta,
+                     zeta, do_forces=True, precision=TGAP_FP64, energies0=None, forces0=None, want_soap=False):
+        """get_gap_soap for one model on a global neighbor list `nb` (dict as returned by
+        build_neighbors_list). energies0/forces0 are overwritten for touched sites."""
+        hs, keep = N.make_hypers(hypers)
+        nn = _i32(nb["n_neigh"])
+        n_sites0 = nn.shape[0]
+        en = np.zeros(n_total_sites) if energies0 is None else energies0
+        fo = np.zeros((n_total_sites, 3)) if forces0 is None else forces0
+        vir = np.zeros(9)
+        Qs = _f64(Qs)
+        D = int(sum(hypers["alpha_max"]))
+        D = D * (D + 1) // 2 * (int(hypers["l_max"]) + 1)
+        soap = np.zeros((n_sites0, D)) if want_soap else None
+        check(self._L.tgap_get_gap_soap(
+            self.h, C.byref(hs), int(n_total_sites), n_sites0, ptr(nn), ptr(_i32(nb["neighbors_list"])),
+            ptr(_f64(nb["rjs"])), ptr(_f64(nb["xyz"])), ptr(_i32(species_supercell)), int(central_species),
+            Qs.shape[0], ptr(_f64(alphas)), ptr(Qs), float(delta), float(zeta), int(do_forces), int(precision),
+            ptr(en), ptr(fo), ptr(vir), ptr(soap)), self.h, "tgap_get_gap_soap")
+        del keep
+        out = (en, fo, vir.reshape(3, 3, order="F"))
+        return out + (soap,) if want_soap else out
+
+
+def assign_species(species_types, names):
+    """assign_species_multiplicity: character*8 names -> channel ids (1-based, 0 = absent)."""
+    st = b"".join(s.encode().ljust(8)[:8] for s in species_types)
+    nm = b"".join(s.encode().ljust(8)[:8] for s in names)
+    out = np.zeros(len(names), np.int32)
+    check(N.lib().tgap_assign_species(len(species_types), st, len(names), nm, ptr(out)))
+    return out
+
+
+class Model:
+    """One soap_turbo GAP model resident on the device (tgap_model)."""
+
+    def __init__(self, ctx, hypers, Qs, alphas, delta=1.0, zeta=4.0, central_species=0):
+        self.ctx = ctx
+        self.hypers = dict(hypers)
+        hs, keep = N.make_hypers(hypers)
+        Qs = _f64(Qs)
+        h = C.c_void_p()
+        check(ctx._L.tgap_model_create(ctx.h, C.byref(hs), int(central_species), Qs.shape[0], ptr(_f64(alphas)),
+                                       ptr(Qs), float(delta), float(zeta), C.byref(h)), ctx.h, "tgap_model_create")
+        del keep
+        self.h = h
+        self.dim = int(ctx._L.tgap_model_dim(h))
+        self.n_sparse = Qs.shape[0]
+        self.central_species = central_species
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.tgap_model_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class System:
+    """A batch of periodic structures resident on the device (tgap_system).
+
+    structures: list of (positions (n, 3), box rows (3, 3), species ids (n,))."""
+
+    def __init__(self, ctx, structures, rcut_max):
+        self.ctx = ctx
+        pos = np.concatenate([_f64(s[0]).reshape(-1, 3) for s in structures])
+        boxes = np.concatenate([_f64(s[1]).reshape(9) for s in structures])
+        sp = np.concatenate([_i32(s[2]) for s in structures])
+        offs = np.zeros(len(structures) + 1, np.int32)
+        offs[1:] = np.cumsum([len(s[2]) for s in structures])
+        self.offsets = offs
+        self.n_atoms = int(offs[-1])
+        self.n_structures = len(structures)
+        h = C.c_void_p()
+        check(ctx._L.tgap_system_create(ctx.h, len(structures), ptr(offs), ptr(pos), ptr(boxes), ptr(sp),
+                                        float(rcut_max), C.byref(h)), ctx.h, "tgap_system_create")
+        self.h = h
+
+    @property
+    def n_pairs(self):
+        return int(self.ctx._L.tgap_system_n_pairs(self.h))
+
+    def device_positions(self):
+        p = C.c_void_p()
+        check(self.ctx._L.tgap_system_positions(self.h, C.byref(p)))
+        return p.value
+
+    def set_positions(self, positions):
+        check(self.ctx._L.tgap_system_set_positions(self.h, ptr(_f64(positions))), self.ctx.h, "set_positions")
+
+    def update(self, rebuild=True):
+        check(self.ctx._L.tgap_system_update(self.h, int(rebuild)), self.ctx.h, "tgap_system_update")
+
+    def compute_device(self, models, precision, d_energies, d_forces, d_virial, do_forces=True):
+        """Device-pointer form: outputs are raw device addresses (ints)."""
+        arr = (C.c_void_p * len(models))(*[m.h.value for m in models])
+        check(self.ctx._L.tgap_compute(self.ctx.h, self.h, len(models), arr, int(precision), int(do_forces),
+                                       C.c_void_p(d_energies), C.c_void_p(d_forces) if d_forces else None,
+                                       C.c_void_p(d_virial) if d_virial else None), self.ctx.h, "tgap_compute")
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.tgap_system_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class MD:
+    """NVE velocity-Verlet driver on the device (tgap_md)."""
+
+    def __init__(self, ctx, system, models, masses_amu, dt, rebuild_every=10, precision=TGAP_FP64,
+                 use_graph=True):
+        self.ctx = ctx
+        self.system = system
+        self.models = list(models)
+        arr = (C.c_void_p * len(models))(*[m.h.value for m in models])
+        h = C.c_void_p()
+        check(ctx._L.tgap_md_create(ctx.h, system.h, len(models), arr, ptr(_f64(masses_amu)), float(dt),
+                                    int(rebuild_every), int(precision), int(use_graph), C.byref(h)),
+              ctx.h, "tgap_md_create")
+        self.h = h
+
+    def set_velocities(self, v):
+        check(self.ctx._L.tgap_md_set_velocities(self.h, ptr(_f64(v))), self.ctx.h, "set_velocities")
+
+    def run(self, n_steps):
+        check(self.ctx._L.tgap_md_run(self.h, int(n_steps)), self.ctx.h, "tgap_md_run")
+
+    def state(self):
+        n = self.system.n_atoms
+        pos = np.zeros((n, 3)); vel = np.zeros((n, 3)); f = np.zeros((n, 3))
+        ep = C.c_double(); ek = C.c_double()
+        check(self.ctx._L.tgap_md_get_state(self.h, ptr(pos), ptr(vel), ptr(f), C.byref(ep), C.byref(ek)),
+              self.ctx.h, "md_get_state")
+        return dict(positions=pos, velocities=vel, forces=f, e_pot=ep.value, e_kin=ek.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.tgap_md_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

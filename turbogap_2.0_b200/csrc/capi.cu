@@ -1,0 +1,1185 @@
+// C ABI of libtgap (declarations and reference citations in include/tgap.h).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "gap_kernels.h"
+#include "md_kernels.h"
+#include "neighbors.h"
+#include "soap_kernels.h"
+#include "tgap_internal.h"
+
+using namespace tgap;
+
+// ============================================================================ utilities
+
+namespace tgap {
+
+int DevBuf::ensure(size_t n)
+{
+    if (n <= bytes && ptr) return 0;
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    size_t want = n < 256 ? 256 : n;
+    if (cudaMalloc(&ptr, want) != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return 1;
+    }
+    bytes = want;
+    return 0;
+}
+
+void DevBuf::release()
+{
+    if (ptr) cudaFree(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int HostBuf::ensure(size_t n)
+{
+    if (n <= bytes && ptr) return 0;
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+    if (cudaMallocHost(&ptr, n < 256 ? 256 : n) != cudaSuccess) {
+        cudaGetLastError();
+        ptr = nullptr;
+        return 1;
+    }
+    bytes = n < 256 ? 256 : n;
+    return 0;
+}
+
+void HostBuf::release()
+{
+    if (ptr) cudaFreeHost(ptr);
+    ptr = nullptr;
+    bytes = 0;
+}
+
+int set_error(tgap_context *ctx, int status, const char *fmt, ...)
+{
+    if (ctx) {
+        char buf[512];
+        va_list ap;
+        va_start(ap, fmt);
+        vsnprintf(buf, sizeof(buf), fmt, ap);
+        va_end(ap);
+        ctx->last_error = buf;
+    }
+    return status;
+}
+
+int cuda_check(tgap_context *ctx, cudaError_t e, const char *what)
+{
+    return set_error(ctx, e == cudaErrorMemoryAllocation ? TGAP_ERR_NOMEM : TGAP_ERR_CUDA,
+                     "%s: %s", what, cudaGetErrorString(e));
+}
+
+StageScope::StageScope(tgap_context *ctx, const char *name) : ctx_(ctx)
+{
+    if (!ctx || !ctx->timing) return;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(ctx->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+    int stage = -1;
+    for (size_t i = 0; i < ctx->stage_names.size(); ++i)
+        if (ctx->stage_names[i] == name) stage = (int)i;
+    if (stage < 0) {
+        stage = (int)ctx->stage_names.size();
+        ctx->stage_names.push_back(name);
+        ctx->stage_ms.push_back(0.0);
+        ctx->stage_count.push_back(0);
+    }
+    StageRecord r;
+    r.stage = stage;
+    for (cudaEvent_t *e : {&r.start, &r.stop}) {
+        if (!ctx->event_pool.empty()) {
+            *e = ctx->event_pool.back();
+            ctx->event_pool.pop_back();
+        } else if (cudaEventCreate(e) != cudaSuccess) {
+            return;
+        }
+    }
+    cudaEventRecord(r.start, ctx->stream);
+    rec_ = (int)ctx->pending.size();
+    ctx->pending.push_back(r);
+}
+
+StageScope::~StageScope()
+{
+    if (rec_ >= 0) cudaEventRecord(ctx_->pending[rec_].stop, ctx_->stream);
+}
+
+}  // namespace tgap
+
+template <class T>
+static int upload(tgap_context *ctx, DevBuf &b, const T *h, size_t n)
+{
+    if (b.ensure(sizeof(T) * (n ? n : 1))) return set_error(ctx, TGAP_ERR_NOMEM, "device buffer");
+    if (n) TGAP_CUDA(ctx, cudaMemcpyAsync(b.ptr, h, sizeof(T) * n, cudaMemcpyHostToDevice, ctx->stream));
+    return TGAP_OK;
+}
+
+template <class T>
+static int download(tgap_context *ctx, T *h, const DevBuf &b, size_t n)
+{
+    if (n) TGAP_CUDA(ctx, cudaMemcpyAsync(h, b.ptr, sizeof(T) * n, cudaMemcpyDeviceToHost, ctx->stream));
+    return TGAP_OK;
+}
+
+#define CHECK_RC(x)           \
+    do {                      \
+        int _rc = (x);        \
+        if (_rc) return _rc;  \
+    } while (0)
+
+static int activate(tgap_context *ctx)
+{
+    if (!ctx) return TGAP_ERR_ARGUMENT;
+    TGAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    return TGAP_OK;
+}
+
+// ============================================================================ context
+
+extern "C" const char *tgap_version(void) { return "tgap-b200 0.1 (sm_100a)"; }
+
+extern "C" int tgap_create(int device, tgap_context **out)
+{
+    if (!out) return TGAP_ERR_ARGUMENT;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        return TGAP_ERR_CUDA;
+    }
+    if (device < 0 || device >= n) return TGAP_ERR_ARGUMENT;
+    if (cudaSetDevice(device) != cudaSuccess) return TGAP_ERR_CUDA;
+    auto *ctx = new tgap_context();
+    ctx->device = device;
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return TGAP_ERR_CUDA;
+    }
+    ctx->stream = ctx->own_stream;
+    if (upload_ylm_constants() != 0) {
+        cudaStreamDestroy(ctx->own_stream);
+        delete ctx;
+        return TGAP_ERR_CUDA;
+    }
+    *out = ctx;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_destroy(tgap_context *ctx)
+{
+    if (!ctx) return TGAP_OK;
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &b : ctx->scratch) b.release();
+    for (auto &b : ctx->pinned) b.release();
+    for (auto &r : ctx->pending) {
+        cudaEventDestroy(r.start);
+        cudaEventDestroy(r.stop);
+    }
+    for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
+    if (ctx->d_flag) cudaFree(ctx->d_flag);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
+    delete ctx;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_set_stream(tgap_context *ctx, void *stream)
+{
+    if (!ctx) return TGAP_ERR_ARGUMENT;
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_synchronize(tgap_context *ctx)
+{
+    CHECK_RC(activate(ctx));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+extern "C" const char *tgap_last_error(const tgap_context *ctx)
+{
+    return ctx ? ctx->last_error.c_str() : "null context";
+}
+
+extern "C" int64_t tgap_kernel_launches(const tgap_context *ctx) { return ctx ? ctx->launches : 0; }
+
+static void timing_collect(tgap_context *ctx)
+{
+    if (ctx->pending.empty()) return;
+    cudaStreamSynchronize(ctx->stream);
+    for (auto &r : ctx->pending) {
+        float ms = 0.0f;
+        if (cudaEventElapsedTime(&ms, r.start, r.stop) == cudaSuccess) {
+            ctx->stage_ms[r.stage] += ms;
+            ctx->stage_count[r.stage] += 1;
+        }
+        ctx->event_pool.push_back(r.start);
+        ctx->event_pool.push_back(r.stop);
+    }
+    ctx->pending.clear();
+}
+
+extern "C" int tgap_timing_enable(tgap_context *ctx, int enable)
+{
+    CHECK_RC(activate(ctx));
+    if (!enable) timing_collect(ctx);
+    ctx->timing = enable != 0;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_timing_reset(tgap_context *ctx)
+{
+    CHECK_RC(activate(ctx));
+    timing_collect(ctx);
+    for (auto &v : ctx->stage_ms) v = 0.0;
+    for (auto &c : ctx->stage_count) c = 0;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_timing_report(tgap_context *ctx, int cap, char *names, double *total_ms, int64_t *counts,
+                                  int *n_stages)
+{
+    CHECK_RC(activate(ctx));
+    if (cap < 0 || !n_stages) return TGAP_ERR_ARGUMENT;
+    timing_collect(ctx);
+    const int n = (int)ctx->stage_names.size();
+    *n_stages = n;
+    for (int i = 0; i < n && i < cap; ++i) {
+        if (names) {
+            std::memset(names + 32 * i, 0, 32);
+            std::strncpy(names + 32 * i, ctx->stage_names[i].c_str(), 31);
+        }
+        if (total_ms) total_ms[i] = ctx->stage_ms[i];
+        if (counts) counts[i] = ctx->stage_count[i];
+    }
+    return TGAP_OK;
+}
+
+// ============================================================================ neighbors
+
+extern "C" int tgap_number_of_unit_cells(const double a[3], const double b[3], const double c[3],
+                                         double rcut, int indices[3])
+{
+    // neighbors_interface.f90:655-708 (host arithmetic, no contraction)
+    if (!a || !b || !c || !indices) return TGAP_ERR_ARGUMENT;
+    auto cross = [](const double *x, const double *y, double *z) {
+        z[0] = x[1] * y[2] - x[2] * y[1];
+        z[1] = x[2] * y[0] - x[0] * y[2];
+        z[2] = x[0] * y[1] - x[1] * y[0];
+    };
+    auto dot = [](const double *x, const double *y) {
+        double s = 0.0;
+        s = s + x[0] * y[0];
+        s = s + x[1] * y[1];
+        s = s + x[2] * y[2];
+        return s;
+    };
+    double axb[3], cxa[3], bxc[3];
+    cross(a, b, axb);
+    cross(c, a, cxa);
+    cross(b, c, bxc);
+    double n = std::sqrt(dot(axb, axb));
+    for (double &v : axb) v = v / n;
+    n = std::sqrt(dot(cxa, cxa));
+    for (double &v : cxa) v = v / n;
+    n = std::sqrt(dot(bxc, bxc));
+    for (double &v : bxc) v = v / n;
+    double m[3][3] = {{dot(axb, a), dot(axb, b), dot(axb, c)},
+                      {dot(cxa, a), dot(cxa, b), dot(cxa, c)},
+                      {dot(bxc, a), dot(bxc, b), dot(bxc, c)}};
+    volatile double md = -m[0][2] * m[1][1] * m[2][0];
+    md = md + m[0][1] * m[1][2] * m[2][0];
+    md = md + m[0][2] * m[1][0] * m[2][1];
+    md = md - m[0][0] * m[1][2] * m[2][1];
+    md = md - m[0][1] * m[1][0] * m[2][2];
+    md = md + m[0][0] * m[1][1] * m[2][2];
+    double inv[3][3] = {{m[1][1] * m[2][2] - m[1][2] * m[2][1], m[0][2] * m[2][1] - m[0][1] * m[2][2],
+                         m[0][1] * m[1][2] - m[0][2] * m[1][1]},
+                        {m[1][2] * m[2][0] - m[1][0] * m[2][2], m[0][0] * m[2][2] - m[0][2] * m[2][0],
+                         m[0][2] * m[1][0] - m[0][0] * m[1][2]},
+                        {m[1][0] * m[2][1] - m[1][1] * m[2][0], m[0][1] * m[2][0] - m[0][0] * m[2][1],
+                         m[0][0] * m[1][1] - m[0][1] * m[1][0]}};
+    const double v = 2.0 * rcut;
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        for (int k = 0; k < 3; ++k) s = s + (inv[i][k] / md) * v;
+        double ir = std::fabs(s);
+        indices[i] = (int)ir;
+        if (ir > (double)indices[i]) indices[i] += 1;
+    }
+    return TGAP_OK;
+}
+
+extern "C" int tgap_build_neighbors(tgap_context *ctx, int n_sites, int n_sites_supercell,
+                                    const double *positions, const double a_box[3],
+                                    const double b_box[3], const double c_box[3], int box_small,
+                                    double rcut_max, const int *species_supercell, int rebuild,
+                                    int *n_neigh, int *neighbors_list, double *rjs, double *xyz,
+                                    double *thetas, double *phis, int *neighbor_species,
+                                    int64_t capacity, int64_t *n_atom_pairs)
+{
+    CHECK_RC(activate(ctx));
+    if (n_sites < 0 || n_sites_supercell < n_sites || !positions || !a_box || !b_box || !c_box ||
+        !n_neigh || !neighbors_list || !n_atom_pairs || !(rcut_max > 0))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_build_neighbors: bad arguments");
+    NeighborBatch nb;
+    std::unique_ptr<NeighborBatch, void (*)(NeighborBatch *)> guard(&nb, [](NeighborBatch *p) { p->release_all(); });
+    CHECK_RC(neighbors_setup_supercell(ctx, &nb, n_sites, n_sites_supercell, positions, a_box, b_box,
+                                       c_box, box_small, rcut_max, species_supercell));
+    int64_t P = 0;
+    if (rebuild) {
+        int rc = neighbors_build(ctx, &nb, 1, capacity, &P, true);
+        *n_atom_pairs = P;
+        if (rc == TGAP_ERR_CAPACITY)
+            return set_error(ctx, rc, "neighbor capacity %lld < %lld pairs", (long long)capacity,
+                             (long long)P);
+        if (rc) return rc;
+    } else {
+        // geometry refresh of the caller's list
+        P = 0;
+        for (int i = 0; i < n_sites; ++i) P += n_neigh[i];
+        if (P > capacity) return set_error(ctx, TGAP_ERR_CAPACITY, "capacity");
+        if (nb.ensure_pairs(P)) return set_error(ctx, TGAP_ERR_NOMEM, "pairs");
+        nb.n_pairs = P;
+        CHECK_RC(upload(ctx, nb.n_neigh, n_neigh, (size_t)n_sites));
+        CHECK_RC(upload(ctx, nb.list, neighbors_list, (size_t)P));
+        CHECK_RC(neighbors_set_counts(ctx, &nb));
+        int64_t dummy = 0;
+        CHECK_RC(neighbors_build(ctx, &nb, 0, capacity, &dummy, true));
+        *n_atom_pairs = P;
+    }
+    CHECK_RC(download(ctx, n_neigh, nb.n_neigh, (size_t)n_sites));
+    CHECK_RC(download(ctx, neighbors_list, nb.list, (size_t)P));
+    if (rjs) CHECK_RC(download(ctx, rjs, nb.rjs, (size_t)P));
+    if (xyz) CHECK_RC(download(ctx, xyz, nb.xyz, 3 * (size_t)P));
+    if (thetas) CHECK_RC(download(ctx, thetas, nb.thetas, (size_t)P));
+    if (phis) CHECK_RC(download(ctx, phis, nb.phis, (size_t)P));
+    if (neighbor_species) CHECK_RC(download(ctx, neighbor_species, nb.nspecies, (size_t)P));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+// ============================================================================ descriptor
+
+static int hypers_from_args(int n_species, const int *alpha_max, int l_max, const double *rcut_hard,
+                            const double *rcut_soft, const double *nf, const double *global_scaling,
+                            const double *atom_sigma_r, const double *atom_sigma_r_scaling,
+                            const double *atom_sigma_t, const double *atom_sigma_t_scaling,
+                            const double *amplitude_scaling, int radial_enhancement,
+                            const double *central_weight, tgap_soap_hypers *h)
+{
+    if (!alpha_max || !rcut_hard || !rcut_soft || !nf || !global_scaling || !atom_sigma_r ||
+        !atom_sigma_r_scaling || !atom_sigma_t || !atom_sigma_t_scaling || !amplitude_scaling ||
+        !central_weight)
+        return TGAP_ERR_ARGUMENT;
+    h->n_species = n_species;
+    h->alpha_max = alpha_max;
+    h->l_max = l_max;
+    h->rcut_hard = rcut_hard;
+    h->rcut_soft = rcut_soft;
+    h->nf = nf;
+    h->global_scaling = global_scaling;
+    h->atom_sigma_r = atom_sigma_r;
+    h->atom_sigma_r_scaling = atom_sigma_r_scaling;
+    h->atom_sigma_t = atom_sigma_t;
+    h->atom_sigma_t_scaling = atom_sigma_t_scaling;
+    h->amplitude_scaling = amplitude_scaling;
+    h->central_weight = central_weight;
+    h->radial_enhancement = radial_enhancement;
+    return TGAP_OK;
+}
+
+static int prepare_soap(tgap_context *ctx, const tgap_soap_hypers *h, DeviceSoap *ds)
+{
+    SoapParams p;
+    std::string why;
+    int rc = make_soap_params(h, &p, &why);
+    if (rc) return set_error(ctx, rc, "descriptor hypers: %s", why.c_str());
+    SoapTables t;
+    build_soap_tables(p, &t);
+    return upload_soap(ctx, p, t, ds);
+}
+
+static void release_soap(DeviceSoap *ds)
+{
+    ds->xq.release();
+    ds->tq.release();
+    ds->central.release();
+    ds->xq32.release();
+    ds->tq32.release();
+    ds->central32.release();
+}
+
+extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh, int n_species,
+                             const int *species, const int *species_multiplicity, int n_atom_pairs,
+                             const unsigned char *mask, const double *rjs, const double *thetas,
+                             const double *phis, const int *alpha_max, int l_max,
+                             const double *rcut_hard, const double *rcut_soft, const double *nf,
+                             const double *global_scaling, const double *atom_sigma_r,
+                             const double *atom_sigma_r_scaling, const double *atom_sigma_t,
+                             const double *atom_sigma_t_scaling, const double *amplitude_scaling,
+                             int radial_enhancement, const double *central_weight, const char *basis,
+                             const char *scaling_mode, int do_derivatives, int compress_soap,
+                             int compress_P_nonzero, const int *compress_P_i, const int *compress_P_j,
+                             const double *compress_P_el, double *soap, double *soap_cart_der)
+{
+    CHECK_RC(activate(ctx));
+    (void)species;
+    (void)compress_P_nonzero;
+    (void)compress_P_i;
+    (void)compress_P_j;
+    (void)compress_P_el;
+    if (n_sites < 0 || n_atom_pairs < n_sites || !n_neigh || !mask || !rjs || !thetas || !phis || !soap)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_soap: bad arguments");
+    if (basis && std::strncmp(basis, "poly3", 5) == 0 && std::strncmp(basis, "poly3gauss", 10) == 0)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED, "basis poly3gauss is not implemented");
+    if (basis && std::strncmp(basis, "poly3", 5) != 0)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED, "basis must be poly3");
+    if (scaling_mode && std::strncmp(scaling_mode, "polynomial", 10) != 0)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED, "scaling_mode must be polynomial");
+    if (compress_soap) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "SOAP compression is not implemented");
+    if (species_multiplicity)
+        for (int i = 0; i < n_sites; ++i)
+            if (species_multiplicity[i] > 1)
+                return set_error(ctx, TGAP_ERR_UNSUPPORTED, "species multiplicity > 1");
+    tgap_soap_hypers h;
+    if (hypers_from_args(n_species, alpha_max, l_max, rcut_hard, rcut_soft, nf, global_scaling,
+                         atom_sigma_r, atom_sigma_r_scaling, atom_sigma_t, atom_sigma_t_scaling,
+                         amplitude_scaling, radial_enhancement, central_weight, &h))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_soap: null hyperparameter array");
+    DeviceSoap ds;
+    std::unique_ptr<DeviceSoap, void (*)(DeviceSoap *)> g0(&ds, release_soap);
+    CHECK_RC(prepare_soap(ctx, &h, &ds));
+    const SoapParams &P = ds.p;
+    // pair arrays: xyz from (r, theta, phi), species channel from the mask
+    const size_t np = (size_t)n_atom_pairs;
+    std::vector<double> hxyz(3 * np);
+    std::vector<int> hsp(np, 0);
+    std::vector<int64_t> hstart(n_sites + 1, 0);
+    for (int i = 0; i < n_sites; ++i) hstart[i + 1] = hstart[i] + n_neigh[i];
+    if (hstart[n_sites] != n_atom_pairs)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "sum(n_neigh) != n_atom_pairs");
+    for (size_t k = 0; k < np; ++k) {
+        const double r = rjs[k], st = std::sin(thetas[k]);
+        hxyz[3 * k] = r * st * std::cos(phis[k]);
+        hxyz[3 * k + 1] = r * st * std::sin(phis[k]);
+        hxyz[3 * k + 2] = r * std::cos(thetas[k]);
+        for (int s = 0; s < n_species; ++s)
+            if (mask[k + np * s]) {
+                hsp[k] = s + 1;
+                break;
+            }
+    }
+    DevBuf *S = ctx->scratch;
+    CHECK_RC(upload(ctx, S[0], hstart.data(), hstart.size()));
+    CHECK_RC(upload(ctx, S[1], hxyz.data(), hxyz.size()));
+    CHECK_RC(upload(ctx, S[2], rjs, np));
+    CHECK_RC(upload(ctx, S[3], hsp.data(), np));
+    const int nlm = (P.l_max + 1) * (P.l_max + 1);
+    if (S[4].ensure(sizeof(double) * (size_t)n_sites * P.n_max * nlm + 8) ||
+        S[5].ensure(sizeof(double) * (size_t)n_sites * P.dim + 8) ||
+        S[6].ensure(sizeof(double) * (size_t)n_sites + 8))
+        return set_error(ctx, TGAP_ERR_NOMEM, "descriptor workspace");
+    PairView pv{S[0].as<int64_t>(), S[1].as<double>(), S[2].as<double>(), S[3].as<int>(), nullptr};
+    SoapOut o;
+    o.c = S[4].ptr;
+    o.q = S[5].ptr;
+    o.norm = S[6].ptr;
+    o.q_ld = P.dim;
+    CHECK_RC(soap_forward(ctx, ds, pv, nullptr, n_sites, TGAP_FP64, o));
+    CHECK_RC(download(ctx, soap, S[5], (size_t)n_sites * P.dim));
+    if (do_derivatives && soap_cart_der) {
+        if (S[7].ensure(sizeof(double) * 3 * (size_t)P.dim * np + 8))
+            return set_error(ctx, TGAP_ERR_NOMEM, "soap_cart_der (%zu bytes)",
+                             sizeof(double) * 3 * (size_t)P.dim * np);
+        CHECK_RC(tgap::soap_cart_der(ctx, ds, pv, nullptr, n_sites, o, S[7].as<double>()));
+        CHECK_RC(download(ctx, soap_cart_der, S[7], 3 * (size_t)P.dim * np));
+    }
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_get_soap_energy_and_forces(tgap_context *ctx, int n_soap, int n_sites,
+                                               int n_sparse, const double *soap,
+                                               const double *soap_der, const double *alphas,
+                                               double delta, double zeta0, double e0,
+                                               const double *Qs, const int *n_neigh,
+                                               const int *neighbors_list, const double *xyz,
+                                               int n_atom_pairs, int do_forces, int n_sites0,
+                                               double *energies, double *forces, double *virial)
+{
+    CHECK_RC(activate(ctx));
+    if (n_soap <= 0 || n_sites < 0 || n_sparse <= 0 || !soap || !alphas || !Qs || !energies ||
+        (do_forces && (!soap_der || !n_neigh || !neighbors_list || !xyz || !forces || !virial ||
+                       n_sites0 <= 0)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_soap_energy_and_forces: bad arguments");
+    DeviceModel m;
+    m.n_sparse = n_sparse;
+    m.dim = n_soap;
+    m.delta = delta;
+    m.zeta = zeta0;
+    DevBuf *S = ctx->scratch;
+    CHECK_RC(upload(ctx, m.Qs, Qs, (size_t)n_sparse * n_soap));
+    CHECK_RC(upload(ctx, m.alphas, alphas, (size_t)n_sparse));
+    if (m.QsT.ensure(sizeof(double) * (size_t)n_sparse * n_soap))
+        return set_error(ctx, TGAP_ERR_NOMEM, "Qs transpose");
+    CHECK_RC(transpose_f64(ctx, n_sparse, n_soap, m.Qs.as<double>(), m.QsT.as<double>()));
+    CHECK_RC(upload(ctx, S[0], soap, (size_t)n_sites * n_soap));
+    if (S[1].ensure(sizeof(double) * (size_t)(n_sites + 1))) return TGAP_ERR_NOMEM;
+    GapWork w;
+    int rc = gap_energy_grad_f64(ctx, m, S[0].as<double>(), n_soap, n_sites, e0, do_forces, &w, nullptr,
+                                 S[1].as<double>(), nullptr);
+    if (!rc) rc = download(ctx, energies, S[1], (size_t)n_sites);
+    if (!rc && do_forces) {
+        std::vector<int64_t> hstart(n_sites + 1, 0);
+        for (int i = 0; i < n_sites; ++i) hstart[i + 1] = hstart[i] + n_neigh[i];
+        const size_t P = (size_t)hstart[n_sites];
+        if ((int64_t)P != (int64_t)n_atom_pairs) rc = set_error(ctx, TGAP_ERR_ARGUMENT, "sum(n_neigh) != n_atom_pairs");
+        if (!rc) rc = upload(ctx, S[2], hstart.data(), hstart.size());
+        if (!rc) rc = upload(ctx, S[3], neighbors_list, P);
+        if (!rc) rc = upload(ctx, S[4], soap_der, 3 * P * (size_t)n_soap);
+        if (!rc) rc = upload(ctx, S[5], xyz, 3 * P);
+        if (!rc && (S[6].ensure(sizeof(double) * 3 * (size_t)n_sites0) || S[7].ensure(sizeof(double) * 9)))
+            rc = TGAP_ERR_NOMEM;
+        if (!rc) {
+            cudaMemsetAsync(S[6].ptr, 0, sizeof(double) * 3 * (size_t)n_sites0, ctx->stream);
+            cudaMemsetAsync(S[7].ptr, 0, sizeof(double) * 9, ctx->stream);
+            rc = pair_forces_from_der(ctx, n_sites, S[2].as<int64_t>(), S[3].as<int>(), n_sites0,
+                                      w.g.as<double>(), n_soap, S[4].as<double>(), S[5].as<double>(),
+                                      S[6].as<double>(), S[7].as<double>());
+        }
+        if (!rc) rc = download(ctx, forces, S[6], 3 * (size_t)n_sites0);
+        if (!rc) rc = download(ctx, virial, S[7], 9);
+    }
+    if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? TGAP_OK : TGAP_ERR_CUDA;
+    m.Qs.release();
+    m.QsT.release();
+    m.alphas.release();
+    w.e_part.release();
+    w.G.release();
+    w.g.release();
+    return rc;
+}
+
+extern "C" int tgap_assign_species(int n_species, const char *species_types, int n, const char *names,
+                                   int *out)
+{
+    if (n_species <= 0 || !species_types || n < 0 || (n > 0 && (!names || !out))) return TGAP_ERR_ARGUMENT;
+    auto trimmed = [](const char *p) {
+        std::string s(p, 8);
+        while (!s.empty() && (s.back() == ' ' || s.back() == '\0')) s.pop_back();
+        return s;
+    };
+    for (int a = 0; a < n_species; ++a)
+        for (int b = a + 1; b < n_species; ++b)
+            if (trimmed(species_types + 8 * a) == trimmed(species_types + 8 * b)) return TGAP_ERR_UNSUPPORTED;
+    for (int i = 0; i < n; ++i) {
+        out[i] = 0;
+        std::string nm = trimmed(names + 8 * (size_t)i);
+        for (int s = 0; s < n_species; ++s)
+            if (trimmed(species_types + 8 * s) == nm) {
+                out[i] = s + 1;
+                break;
+            }
+    }
+    return TGAP_OK;
+}
+
+// ============================================================================ resident objects
+
+struct tgap_model {
+    tgap_context *ctx;
+    DeviceSoap soap;
+    DeviceModel gap;
+    int central_species;
+    bool mixed_ready = false;
+};
+
+struct SiteSet {
+    int central_species = -1;
+    int n_rows = 0;
+    DevBuf sites;
+};
+
+struct tgap_system {
+    tgap_context *ctx;
+    NeighborBatch nb;
+    double rcut;
+    std::vector<int> host_species;
+    std::vector<SiteSet> site_sets;
+    DevBuf c, q, norm, q_hi, q_lo, e_rows;
+    GapWork gw;
+    DevBuf scratch_forces;
+    int generation = 0;  // bumps when a device buffer is reallocated (graph re-capture)
+};
+
+extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
+                                 int n_sparse, const double *alphas, const double *Qs, double delta,
+                                 double zeta, tgap_model **out)
+{
+    CHECK_RC(activate(ctx));
+    if (!hypers || n_sparse <= 0 || !alphas || !Qs || !out)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_model_create: bad arguments");
+    auto *m = new tgap_model();
+    m->ctx = ctx;
+    m->central_species = central_species;
+    int rc = prepare_soap(ctx, hypers, &m->soap);
+    if (!rc) {
+        m->gap.n_sparse = n_sparse;
+        m->gap.dim = m->soap.p.dim;
+        m->gap.delta = delta;
+        m->gap.zeta = zeta;
+        rc = upload(ctx, m->gap.Qs, Qs, (size_t)n_sparse * m->gap.dim);
+    }
+    if (!rc) rc = upload(ctx, m->gap.alphas, alphas, (size_t)n_sparse);
+    if (!rc && m->gap.QsT.ensure(sizeof(double) * (size_t)n_sparse * m->gap.dim)) rc = TGAP_ERR_NOMEM;
+    if (!rc) rc = transpose_f64(ctx, n_sparse, m->gap.dim, m->gap.Qs.as<double>(), m->gap.QsT.as<double>());
+    if (!rc) rc = model_upload_mixed(ctx, &m->gap);
+    if (!rc) m->mixed_ready = true;
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = TGAP_ERR_CUDA;
+    if (rc) {
+        tgap_model_destroy(m);
+        return rc;
+    }
+    *out = m;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_model_destroy(tgap_model *m)
+{
+    if (!m) return TGAP_OK;
+    cudaSetDevice(m->ctx->device);
+    release_soap(&m->soap);
+    DevBuf *bufs[] = {&m->gap.Qs, &m->gap.QsT, &m->gap.alphas, &m->gap.alphas32, &m->gap.Q_hi,
+                      &m->gap.Q_lo, &m->gap.QT_hi, &m->gap.QT_lo};
+    for (DevBuf *b : bufs) b->release();
+    delete m;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_model_dim(const tgap_model *m) { return m ? m->gap.dim : 0; }
+
+extern "C" int tgap_system_create(tgap_context *ctx, int n_structures, const int *offsets,
+                                  const double *positions, const double *boxes, const int *species,
+                                  double rcut_max, tgap_system **out)
+{
+    CHECK_RC(activate(ctx));
+    if (n_structures <= 0 || !offsets || !positions || !boxes || !species || !out || !(rcut_max > 0))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_system_create: bad arguments");
+    auto *s = new tgap_system();
+    s->ctx = ctx;
+    s->rcut = rcut_max;
+    s->host_species.assign(species, species + offsets[n_structures]);
+    int rc = neighbors_setup(ctx, &s->nb, n_structures, offsets, positions, boxes, species, rcut_max,
+                             nullptr);
+    if (!rc) rc = tgap_system_update(s, 1);
+    if (rc) {
+        tgap_system_destroy(s);
+        return rc;
+    }
+    *out = s;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_system_destroy(tgap_system *s)
+{
+    if (!s) return TGAP_OK;
+    cudaSetDevice(s->ctx->device);
+    s->nb.release_all();
+    for (auto &ss : s->site_sets) ss.sites.release();
+    DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces};
+    for (DevBuf *b : bufs) b->release();
+    delete s;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_system_n_atoms(const tgap_system *s) { return s ? s->nb.n_atoms : 0; }
+extern "C" int64_t tgap_system_n_pairs(const tgap_system *s) { return s ? s->nb.n_pairs : 0; }
+
+extern "C" int tgap_system_positions(tgap_system *s, double **d_positions)
+{
+    if (!s || !d_positions) return TGAP_ERR_ARGUMENT;
+    *d_positions = s->nb.positions.as<double>();
+    return TGAP_OK;
+}
+
+extern "C" int tgap_system_set_positions(tgap_system *s, const double *positions)
+{
+    if (!s || !positions) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = s->ctx;
+    CHECK_RC(activate(ctx));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, positions, sizeof(double) * 3 * s->nb.n_atoms,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_system_update(tgap_system *s, int rebuild)
+{
+    if (!s) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = s->ctx;
+    CHECK_RC(activate(ctx));
+    CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
+    void *before = s->nb.list.ptr;
+    int64_t P = 0;
+    CHECK_RC(neighbors_build(ctx, &s->nb, rebuild, -1, &P, false));
+    if (s->nb.list.ptr != before) s->generation++;
+    return TGAP_OK;
+}
+
+static int site_set(tgap_system *s, int central_species, SiteSet **out)
+{
+    for (auto &ss : s->site_sets)
+        if (ss.central_species == central_species) {
+            *out = &ss;
+            return TGAP_OK;
+        }
+    tgap_context *ctx = s->ctx;
+    std::vector<int> rows;
+    for (int i = 0; i < (int)s->host_species.size(); ++i)
+        if (central_species == 0 || s->host_species[i] == central_species) rows.push_back(i);
+    s->site_sets.emplace_back();
+    SiteSet &ss = s->site_sets.back();
+    ss.central_species = central_species;
+    ss.n_rows = (int)rows.size();
+    CHECK_RC(upload(ctx, ss.sites, rows.data(), rows.size()));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *out = &ss;
+    return TGAP_OK;
+}
+
+static int ensure_eval_buffers(tgap_system *s, const tgap_model *m, int n_rows, int precision)
+{
+    const SoapParams &P = m->soap.p;
+    const int nlm = (P.l_max + 1) * (P.l_max + 1);
+    const size_t tsz = precision == TGAP_FP64 ? 8 : 4;
+    const int q_ld = precision == TGAP_FP64 ? P.dim : m->gap.dim_pad;
+    const int rows_pad = (n_rows + 127) / 128 * 128;
+    void *before[5] = {s->c.ptr, s->q.ptr, s->norm.ptr, s->q_hi.ptr, s->q_lo.ptr};
+    if (s->c.ensure(tsz * (size_t)n_rows * P.n_max * nlm) || s->q.ensure(tsz * (size_t)rows_pad * q_ld) ||
+        s->norm.ensure(tsz * (size_t)n_rows))
+        return set_error(s->ctx, TGAP_ERR_NOMEM, "descriptor workspace");
+    if (precision != TGAP_FP64) {
+        if (s->q_hi.ensure(2 * (size_t)rows_pad * q_ld) || s->q_lo.ensure(2 * (size_t)rows_pad * q_ld))
+            return set_error(s->ctx, TGAP_ERR_NOMEM, "descriptor workspace");
+    }
+    void *after[5] = {s->c.ptr, s->q.ptr, s->norm.ptr, s->q_hi.ptr, s->q_lo.ptr};
+    for (int i = 0; i < 5; ++i)
+        if (before[i] != after[i]) s->generation++;
+    // rows past n_rows feed the 128-row GEMM tiles: keep them zero
+    if (precision != TGAP_FP64 && (before[3] != after[3] || before[4] != after[4])) {
+        TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_hi.ptr, 0, s->q_hi.bytes, s->ctx->stream));
+        TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_lo.ptr, 0, s->q_lo.bytes, s->ctx->stream));
+    }
+    return TGAP_OK;
+}
+
+static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m, int precision,
+                         int do_forces, double *d_energies, double *d_forces, double *d_virial)
+{
+    SiteSet *ss = nullptr;
+    CHECK_RC(site_set(s, m->central_species, &ss));
+    const int n_rows = ss->n_rows;
+    if (n_rows == 0) return TGAP_OK;
+    CHECK_RC(ensure_eval_buffers(s, m, n_rows, precision));
+    PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
+                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>()};
+    SoapOut o;
+    o.c = s->c.ptr;
+    o.q = s->q.ptr;
+    o.norm = s->norm.ptr;
+    const int *sites = ss->sites.as<int>();
+    if (precision == TGAP_FP64) {
+        o.q_ld = m->gap.dim;
+        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o));
+        void *gb = s->gw.G.ptr;
+        CHECK_RC(gap_energy_grad_f64(ctx, m->gap, (const double *)o.q, o.q_ld, n_rows, 0.0, do_forces,
+                                     &s->gw, sites, nullptr, d_energies));
+        if (s->gw.G.ptr != gb) s->generation++;
+        if (do_forces)
+            CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o, s->gw.g.ptr, m->gap.dim,
+                                   1, s->nb.site_struct.as<int>(), d_forces, d_virial));
+    } else {
+        if (!m->mixed_ready) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "mixed path not prepared");
+        o.q_ld = m->gap.dim_pad;
+        o.q_hi = s->q_hi.as<__nv_bfloat16>();
+        o.q_lo = s->q_lo.as<__nv_bfloat16>();
+        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o));
+        void *gb = s->gw.G_hi.ptr;
+        CHECK_RC(gap_energy_grad_mixed(ctx, m->gap, o.q_hi, o.q_lo, n_rows, 0.0, do_forces, &s->gw, sites,
+                                       nullptr, d_energies));
+        if (s->gw.G_hi.ptr != gb) s->generation++;
+        if (do_forces)
+            CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o, s->gw.g.ptr,
+                                   m->gap.dim_pad, 0, s->nb.site_struct.as<int>(), d_forces, d_virial));
+    }
+    return TGAP_OK;
+}
+
+extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                            int precision, int do_forces, double *d_energies, double *d_forces,
+                            double *d_virial)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || n_models <= 0 || !models || !d_energies || (do_forces && (!d_forces || !d_virial)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_compute: bad arguments");
+    if (precision != TGAP_FP64 && precision != TGAP_MIXED)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "precision");
+    const int N = s->nb.n_atoms;
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_energies, 0, sizeof(double) * N, ctx->stream));
+    if (do_forces) {
+        TGAP_CUDA(ctx, cudaMemsetAsync(d_forces, 0, sizeof(double) * 3 * N, ctx->stream));
+        TGAP_CUDA(ctx, cudaMemsetAsync(d_virial, 0, sizeof(double) * 9 * s->nb.n_structures, ctx->stream));
+    }
+    for (int i = 0; i < n_models; ++i)
+        CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                                       int precision, const double *positions, int rebuild, double *energies,
+                                       double *forces, double *virial)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || !energies) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad arguments");
+    const int N = s->nb.n_atoms, nst = s->nb.n_structures;
+    const size_t out_bytes = sizeof(double) * ((size_t)N + 3 * (size_t)N + 9 * (size_t)nst);
+    if (ctx->pinned[0].ensure(sizeof(double) * 3 * (size_t)N) || ctx->pinned[1].ensure(out_bytes) ||
+        s->scratch_forces.ensure(out_bytes))
+        return set_error(ctx, TGAP_ERR_NOMEM, "staging buffers");
+    if (positions) {
+        std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
+        TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    }
+    CHECK_RC(tgap_system_update(s, rebuild));
+    double *d_e = s->scratch_forces.as<double>();
+    double *d_f = d_e + N;
+    double *d_v = d_f + 3 * (size_t)N;
+    const int do_forces = forces != nullptr || virial != nullptr;
+    CHECK_RC(tgap_compute(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(ctx->pinned[1].ptr, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    const double *h = ctx->pinned[1].as<double>();
+    std::memcpy(energies, h, sizeof(double) * N);
+    if (forces) std::memcpy(forces, h + N, sizeof(double) * 3 * (size_t)N);
+    if (virial) std::memcpy(virial, h + 4 * (size_t)N, sizeof(double) * 9 * (size_t)nst);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_descriptors(tgap_context *ctx, tgap_system *s, const tgap_model *m, int precision,
+                                double *d_soap, int *n_rows)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || !m || !d_soap || !n_rows) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_descriptors");
+    SiteSet *ss = nullptr;
+    CHECK_RC(site_set(s, m->central_species, &ss));
+    *n_rows = ss->n_rows;
+    if (ss->n_rows == 0) return TGAP_OK;
+    CHECK_RC(ensure_eval_buffers(s, m, ss->n_rows, TGAP_FP64));
+    PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
+                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>()};
+    SoapOut o;
+    o.c = s->c.ptr;
+    o.q = d_soap;
+    o.norm = s->norm.ptr;
+    o.q_ld = m->gap.dim;
+    (void)precision;
+    return soap_forward(ctx, m->soap, pv, ss->sites.as<int>(), ss->n_rows, TGAP_FP64, o);
+}
+
+// ---------------------------------------------------------------------------- get_gap_soap
+
+extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hypers, int n_total_sites,
+                                 int n_sites0, const int *n_neigh0, const int *neighbors_list0,
+                                 const double *rjs0, const double *xyz0, const int *species_supercell,
+                                 int central_species, int n_sparse, const double *alphas, const double *Qs,
+                                 double delta, double zeta, int do_forces, int precision,
+                                 double *energies0, double *forces0, double *virial, double *soap_out)
+{
+    CHECK_RC(activate(ctx));
+    if (!hypers || n_total_sites <= 0 || n_sites0 < 0 || !n_neigh0 || !neighbors_list0 || !rjs0 || !xyz0 ||
+        !species_supercell || !alphas || !Qs || !energies0 || (do_forces && (!forces0 || !virial)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_gap_soap: bad arguments");
+    tgap_model *m = nullptr;
+    CHECK_RC(tgap_model_create(ctx, hypers, central_species, n_sparse, alphas, Qs, delta, zeta, &m));
+    std::unique_ptr<tgap_model, int (*)(tgap_model *)> gm(m, tgap_model_destroy);
+    // host-side pair view of the caller's list (gap_interface.f90:184-289 folds neighbors with
+    // mod(j-1, n_total_sites)+1 and keeps pairs within rcut of known species)
+    std::vector<int64_t> start(n_sites0 + 1, 0);
+    for (int i = 0; i < n_sites0; ++i) start[i + 1] = start[i] + n_neigh0[i];
+    const size_t P = (size_t)start[n_sites0];
+    std::vector<int> sp(P), jat(P), rows;
+    std::vector<unsigned char> seen(n_total_sites, 0);
+    const double rcut_max = m->soap.p.rcut_max;
+    for (int i = 0; i < n_sites0; ++i) {
+        const int self = (neighbors_list0[start[i]] - 1) % n_total_sites;
+        const int si = species_supercell[neighbors_list0[start[i]] - 1];
+        const bool keep = central_species == 0 || si == central_species;
+        if (keep) rows.push_back(i);
+        for (int64_t k = start[i]; k < start[i + 1]; ++k) {
+            const int j = neighbors_list0[k] - 1;
+            sp[k] = species_supercell[j];
+            jat[k] = j % n_total_sites;
+            if (keep && rjs0[k] < rcut_max && sp[k] > 0) seen[jat[k]] = 1;
+        }
+        (void)self;
+    }
+    DevBuf *S = ctx->scratch;
+    CHECK_RC(upload(ctx, S[10], start.data(), start.size()));
+    CHECK_RC(upload(ctx, S[11], xyz0, 3 * P));
+    CHECK_RC(upload(ctx, S[12], rjs0, P));
+    CHECK_RC(upload(ctx, S[13], sp.data(), P));
+    CHECK_RC(upload(ctx, S[14], jat.data(), P));
+    CHECK_RC(upload(ctx, S[15], rows.data(), rows.size()));
+    const int n_rows = (int)rows.size();
+    const SoapParams &Pp = m->soap.p;
+    const int nlm = (Pp.l_max + 1) * (Pp.l_max + 1);
+    const int q_ld = precision == TGAP_FP64 ? Pp.dim : m->gap.dim_pad;
+    const int rows_pad = (n_rows + 127) / 128 * 128;
+    if (S[16].ensure(8 * (size_t)n_rows * Pp.n_max * nlm + 8) || S[17].ensure(8 * (size_t)rows_pad * q_ld + 8) ||
+        S[18].ensure(8 * (size_t)n_rows + 8) || S[19].ensure(8 * (size_t)n_total_sites) ||
+        S[20].ensure(8 * 3 * (size_t)n_total_sites) || S[21].ensure(8 * 9) ||
+        S[22].ensure(2 * (size_t)rows_pad * q_ld + 8) || S[23].ensure(2 * (size_t)rows_pad * q_ld + 8))
+        return set_error(ctx, TGAP_ERR_NOMEM, "get_gap_soap workspace");
+    if (precision != TGAP_FP64) {
+        TGAP_CUDA(ctx, cudaMemsetAsync(S[22].ptr, 0, 2 * (size_t)rows_pad * q_ld, ctx->stream));
+        TGAP_CUDA(ctx, cudaMemsetAsync(S[23].ptr, 0, 2 * (size_t)rows_pad * q_ld, ctx->stream));
+    }
+    PairView pv{S[10].as<int64_t>(), S[11].as<double>(), S[12].as<double>(), S[13].as<int>(), S[14].as<int>()};
+    SoapOut o;
+    o.c = S[16].ptr;
+    o.q = S[17].ptr;
+    o.norm = S[18].ptr;
+    o.q_ld = q_ld;
+    double *d_e = S[19].as<double>(), *d_f = S[20].as<double>(), *d_v = S[21].as<double>();
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, 8 * (size_t)n_total_sites, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_f, 0, 8 * 3 * (size_t)n_total_sites, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_v, 0, 8 * 9, ctx->stream));
+    GapWork w;
+    int rc = TGAP_OK;
+    // the kernels index sites by position in the caller's list; rows map to atoms via jatom of
+    // the self slot, so energies/forces land on folded global indices
+    std::vector<int> row_atom(n_rows);
+    for (int r = 0; r < n_rows; ++r) row_atom[r] = jat[start[rows[r]]];
+    CHECK_RC(upload(ctx, S[9], row_atom.data(), row_atom.size()));
+    if (precision == TGAP_FP64) {
+        rc = soap_forward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_FP64, o);
+        if (!rc) rc = gap_energy_grad_f64(ctx, m->gap, (const double *)o.q, q_ld, n_rows, 0.0, do_forces, &w,
+                                          S[9].as<int>(), nullptr, d_e);
+        if (!rc && do_forces)
+            rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_FP64, o, w.g.ptr, Pp.dim, 1,
+                               nullptr, d_f, d_v);
+    } else {
+        o.q_hi = S[22].as<__nv_bfloat16>();
+        o.q_lo = S[23].as<__nv_bfloat16>();
+        rc = soap_forward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_MIXED, o);
+        if (!rc) rc = gap_energy_grad_mixed(ctx, m->gap, o.q_hi, o.q_lo, n_rows, 0.0, do_forces, &w,
+                                            S[9].as<int>(), nullptr, d_e);
+        if (!rc && do_forces)
+            rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_MIXED, o, w.g.ptr, m->gap.dim_pad,
+                               0, nullptr, d_f, d_v);
+    }
+    std::vector<double> he(n_total_sites), hf(3 * (size_t)n_total_sites);
+    if (!rc) rc = download(ctx, he.data(), S[19], (size_t)n_total_sites);
+    if (!rc && do_forces) rc = download(ctx, hf.data(), S[20], 3 * (size_t)n_total_sites);
+    if (!rc && do_forces) rc = download(ctx, virial, S[21], 9);
+    if (!rc && soap_out && precision == TGAP_FP64) {
+        std::vector<double> q((size_t)n_rows * Pp.dim);
+        rc = download(ctx, q.data(), S[17], q.size());
+        if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = TGAP_ERR_CUDA;
+        for (int r = 0; r < n_rows && !rc; ++r)
+            std::memcpy(soap_out + (size_t)rows[r] * Pp.dim, q.data() + (size_t)r * Pp.dim, 8 * Pp.dim);
+    }
+    if (!rc && cudaStreamSynchronize(ctx->stream) != cudaSuccess) rc = TGAP_ERR_CUDA;
+    if (!rc) {
+        for (int r = 0; r < n_rows; ++r) energies0[row_atom[r]] = he[row_atom[r]];
+        if (do_forces)
+            for (int a = 0; a < n_total_sites; ++a)
+                if (seen[a])
+                    for (int x = 0; x < 3; ++x) forces0[3 * (size_t)a + x] = hf[3 * (size_t)a + x];
+    }
+    DevBuf *wb[] = {&w.e_part, &w.G, &w.g, &w.G_hi, &w.G_lo};
+    for (DevBuf *b : wb) b->release();
+    return rc;
+}
+
+// ============================================================================ MD
+
+struct tgap_md {
+    tgap_context *ctx;
+    tgap_system *sys;
+    std::vector<tgap_model *> models;
+    int precision, rebuild_every, use_graph;
+    double dt, dt_prev = 0.0;
+    int64_t step = 0;
+    bool first = true;
+    DevBuf mass, vel, forces, forces_prev, pos_prev, energies, virial;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int graph_generation = -1;
+    int64_t graph_kernels = 0;
+};
+
+static int md_eval(tgap_md *md)
+{
+    return tgap_compute(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
+                        md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>());
+}
+
+// one step after the first: geometry refresh, forces, velocity Verlet
+static int md_step_body(tgap_md *md)
+{
+    tgap_context *ctx = md->ctx;
+    CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
+    int64_t P = 0;
+    CHECK_RC(neighbors_build(ctx, &md->sys->nb, 0, -1, &P, false));
+    CHECK_RC(md_eval(md));
+    CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
+                             md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),
+                             md->forces_prev.as<double>(), md->mass.as<double>(), md->dt, md->dt, 0));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models, tgap_model *const *models,
+                              const double *masses_amu, double dt, int rebuild_every, int precision,
+                              int use_graph, tgap_md **out)
+{
+    CHECK_RC(activate(ctx));
+    if (!sys || n_models <= 0 || !models || !masses_amu || !(dt > 0) || rebuild_every < 1 || !out)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_md_create: bad arguments");
+    auto *md = new tgap_md();
+    md->ctx = ctx;
+    md->sys = sys;
+    md->models.assign(models, models + n_models);
+    md->precision = precision;
+    md->rebuild_every = rebuild_every;
+    md->use_graph = use_graph;
+    md->dt = dt;
+    const int N = sys->nb.n_atoms;
+    std::vector<double> m(N);
+    for (int i = 0; i < N; ++i) m[i] = masses_amu[i] * 103.6426965268;  // read_files.f90:333
+    int rc = upload(ctx, md->mass, m.data(), (size_t)N);
+    DevBuf *bufs[] = {&md->vel, &md->forces, &md->forces_prev, &md->pos_prev};
+    for (DevBuf *b : bufs)
+        if (!rc && (b->ensure(sizeof(double) * 3 * N) || cudaMemsetAsync(b->ptr, 0, sizeof(double) * 3 * N, ctx->stream)))
+            rc = TGAP_ERR_NOMEM;
+    if (!rc && (md->energies.ensure(sizeof(double) * N) || md->virial.ensure(sizeof(double) * 9 * sys->nb.n_structures)))
+        rc = TGAP_ERR_NOMEM;
+    if (rc) {
+        tgap_md_destroy(md);
+        return rc;
+    }
+    *out = md;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_md_destroy(tgap_md *md)
+{
+    if (!md) return TGAP_OK;
+    cudaSetDevice(md->ctx->device);
+    if (md->exec) cudaGraphExecDestroy(md->exec);
+    if (md->graph) cudaGraphDestroy(md->graph);
+    DevBuf *bufs[] = {&md->mass, &md->vel, &md->forces, &md->forces_prev, &md->pos_prev, &md->energies, &md->virial};
+    for (DevBuf *b : bufs) b->release();
+    delete md;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_md_set_velocities(tgap_md *md, const double *v)
+{
+    if (!md || !v) return TGAP_ERR_ARGUMENT;
+    CHECK_RC(activate(md->ctx));
+    TGAP_CUDA(md->ctx, cudaMemcpyAsync(md->vel.ptr, v, sizeof(double) * 3 * md->sys->nb.n_atoms,
+                                       cudaMemcpyHostToDevice, md->ctx->stream));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_md_run(tgap_md *md, int n_steps)
+{
+    if (!md || n_steps < 0) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = md->ctx;
+    CHECK_RC(activate(ctx));
+    for (int it = 0; it < n_steps; ++it) {
+        const bool rebuild = (md->step % md->rebuild_every) == 0;
+        if (md->first || rebuild) {
+            // eager step: a rebuild needs the pair count on the host, and it sizes every buffer
+            CHECK_RC(tgap_system_update(md->sys, rebuild ? 1 : 0));
+            CHECK_RC(md_eval(md));
+            CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
+                                     md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),
+                                     md->forces_prev.as<double>(), md->mass.as<double>(), md->dt, md->dt,
+                                     md->first ? 1 : 0));
+            md->first = false;
+        } else if (md->use_graph) {
+            if (!md->exec || md->graph_generation != md->sys->generation) {
+                if (md->exec) cudaGraphExecDestroy(md->exec);
+                if (md->graph) cudaGraphDestroy(md->graph);
+                md->exec = nullptr;
+                md->graph = nullptr;
+                TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+                const int64_t launches = ctx->launches;
+                int rc = md_step_body(md);
+                cudaGraph_t g = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+                md->graph_kernels = ctx->launches - launches;
+                ctx->launches = launches;
+                if (rc) {
+                    if (g) cudaGraphDestroy(g);
+                    return rc;
+                }
+                if (ce != cudaSuccess) return cuda_check(ctx, ce, "graph capture");
+                md->graph = g;
+                TGAP_CUDA(ctx, cudaGraphInstantiate(&md->exec, g, 0));
+                md->graph_generation = md->sys->generation;
+            }
+            TGAP_CUDA(ctx, cudaGraphLaunch(md->exec, ctx->stream));
+            ctx->launches += md->graph_kernels;
+        } else {
+            CHECK_RC(md_step_body(md));
+        }
+        ++md->step;
+    }
+    return TGAP_OK;
+}
+
+extern "C" int tgap_md_get_state(tgap_md *md, double *positions, double *velocities, double *forces,
+                                 double *e_pot, double *e_kin)
+{
+    if (!md) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = md->ctx;
+    CHECK_RC(activate(ctx));
+    const int N = md->sys->nb.n_atoms;
+    std::vector<double> v(3 * N), e(N), m(N);
+    if (positions) CHECK_RC(download(ctx, positions, md->sys->nb.positions, 3 * (size_t)N));
+    CHECK_RC(download(ctx, v.data(), md->vel, 3 * (size_t)N));
+    if (forces) CHECK_RC(download(ctx, forces, md->forces, 3 * (size_t)N));
+    CHECK_RC(download(ctx, e.data(), md->energies, (size_t)N));
+    CHECK_RC(download(ctx, m.data(), md->mass, (size_t)N));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (velocities) std::memcpy(velocities, v.data(), sizeof(double) * 3 * N);
+    double ep = 0.0, ek = 0.0;
+    for (int i = 0; i < N; ++i) {
+        ep += e[i];
+        ek += 0.5 * m[i] * (v[3 * i] * v[3 * i] + v[3 * i + 1] * v[3 * i + 1] + v[3 * i + 2] * v[3 * i + 2]);
+    }
+    if (e_pot) *e_pot = ep;
+    if (e_kin) *e_kin = ek;
+    return TGAP_OK;
+}

@@ -1,0 +1,50 @@
+// GAP kernel contraction launchers (gap.cu: FP64; gemm_tc.cu: bf16x3 tensor cores).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "tgap_internal.h"
+
+namespace tgap {
+
+// One soap_turbo GAP model resident on the device.
+struct DeviceModel {
+    int n_sparse = 0, dim = 0;
+    int dim_pad = 0, m_pad = 0;  // padded sizes of the bf16 operands (multiples of 64 / 128)
+    double delta = 1.0, zeta = 4.0;
+    DevBuf Qs;        // double [n_sparse][dim]  (row = sparse point; Fortran Qs(dim, n_sparse))
+    DevBuf QsT;       // double [dim][n_sparse]
+    DevBuf alphas;    // double [n_sparse]
+    DevBuf alphas32;  // float  [m_pad] (zero padded)
+    DevBuf Q_hi, Q_lo;    // bf16 [m_pad][dim_pad]
+    DevBuf QT_hi, QT_lo;  // bf16 [dim_pad][m_pad]
+};
+
+struct GapWork {
+    DevBuf e_part;    // energy partials
+    DevBuf G;         // FP64: [M][n_sparse]
+    DevBuf g;         // dE/dq: double [M][dim] (FP64) or float [M][dim_pad] (mixed)
+    DevBuf G_hi, G_lo;  // mixed: bf16 [m_rows_pad][m_pad]
+};
+
+int dgemm_nt(tgap_context *ctx, int M, int N, int K, const double *A, int lda, const double *B,
+             int ldb, double *C, int ldc, double alpha);
+int transpose_f64(tgap_context *ctx, int R, int C, const double *in, double *out);
+
+// Energies (delta^2 sum alpha K^zeta + e0) added into d_energies[sites[row]] and/or written to
+// d_e_rows; when do_forces, w->g = dE/dq (double, [n_rows][dim]).
+int gap_energy_grad_f64(tgap_context *ctx, const DeviceModel &m, const double *d_q, int q_ld,
+                        int n_rows, double e0, int do_forces, GapWork *w, const int *d_sites,
+                        double *d_e_rows, double *d_energies);
+
+// Mixed path: q given as bf16 hi/lo [rows_pad][dim_pad]; w->g = dE/dq (float [n_rows][dim_pad]).
+int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
+                          const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces,
+                          GapWork *w, const int *d_sites, double *d_e_rows, double *d_energies);
+int model_upload_mixed(tgap_context *ctx, DeviceModel *m);
+
+int pair_forces_from_der(tgap_context *ctx, int n_sites, const int64_t *d_start, const int *d_nl,
+                         int n_sites0, const double *d_g, int D, const double *d_der,
+                         const double *d_xyz, double *d_forces, double *d_virial);
+
+}  // namespace tgap

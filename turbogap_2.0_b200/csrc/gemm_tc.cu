@@ -1,0 +1,480 @@
+// Mixed-precision GAP kernel contraction on the 5th-generation tensor cores (sm_100a).
+//
+// bf16x3 split products: every FP32 operand x is stored as x_hi = bf16(x) and
+// x_lo = bf16(x - x_hi); a product is accumulated as a_hi b_hi + a_hi b_lo + a_lo b_hi in
+// FP32 (the a_lo b_lo term is below the FP32 accumulation error). Two GEMMs per model:
+//
+//   GEMM1  K = q Qs^T       (rows x n_sparse, K-dim = descriptor)   epilogue: K^zeta energy
+//          partials and G = zeta delta^2 alpha o K^(zeta-1), written back as a bf16 split
+//   GEMM2  g = G Qs         (rows x descriptor, K-dim = n_sparse)   epilogue: FP32 store
+//
+// One CTA computes a 128 x BN tile: one thread issues TMA loads (no multicast) into a
+// STAGES-deep ring of 128B-swizzled shared-memory tiles, one thread issues tcgen05.mma
+// (cta_group::1, kind::f16, accumulator in TMEM), and all four warps drain TMEM with
+// tcgen05.ld for the epilogue. Every mbarrier wait is bounded (1 s of globaltimer); on
+// timeout the kernel raises the device error flag, drains its own outstanding copies with a
+// bounded wait, frees TMEM and returns.
+#include <cuda.h>
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstring>
+
+#include "gap_kernels.h"
+
+namespace tgap {
+
+constexpr int kTcThreads = 128;
+constexpr int kBM = 128;
+constexpr int kBK = 64;  // bf16 elements per 128-byte swizzle row
+constexpr uint64_t kWaitNs = 1000000000ull;
+
+// ---------------------------------------------------------------------------- PTX helpers
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p)
+{
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ uint64_t globaltimer()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+// Bounded wait: false after kWaitNs or once *abort is set by another thread of the CTA.
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort)
+{
+    const uint64_t t0 = globaltimer();
+    while (!mbar_try(bar, parity)) {
+        if (*abort) return false;
+        if (globaltimer() - t0 > kWaitNs) return false;
+    }
+    return true;
+}
+
+__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x,
+                                            int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], [%2];"
+        ::"r"(dst), "l"((uint64_t)map), "r"(bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+// K-major operand tile, 128-byte swizzle, 8-row groups 1024 bytes apart (SM100 descriptor:
+// start>>4 [0,14), LBO>>4 [16,30) = 1, SBO>>4 [32,46) = 64, version [46,48) = 1,
+// layout [61,64) = 2 (SWIZZLE_128B)).
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
+{
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)64 << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
+}
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                          uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}"
+        ::"r"(tmem_d), "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_commit(uint32_t bar)
+{
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
+{
+    uint32_t r[16];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
+    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+    for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// ---------------------------------------------------------------------------- epilogues
+
+// GEMM1: per element k = K[row][s]: energy partial alpha_s k^zeta, G = zd2 alpha_s k^(zeta-1).
+struct EpiKernelGap {
+    const float *alphas;       // [m_pad]
+    __nv_bfloat16 *G_hi, *G_lo;  // [rows_pad][ldg]
+    int ldg;
+    double *e_part;            // [n_tiles][rows_pad]
+    int rows_pad;
+    float zd2, zeta;
+    int zeta_int;
+    __device__ __forceinline__ void begin(float &acc) const { acc = 0.0f; }
+    __device__ __forceinline__ void chunk(int row, int col, const float v[16], float &acc) const
+    {
+        __align__(16) __nv_bfloat16 hi[16], lo[16];
+#pragma unroll
+        for (int j = 0; j < 16; ++j) {
+            const float k = v[j], a = alphas[col + j];
+            float kz1;
+            if (zeta_int >= 1) {
+                kz1 = 1.0f;
+                for (int p = 1; p < zeta_int; ++p) kz1 *= k;
+            } else {
+                kz1 = powf(k, zeta - 1.0f);
+            }
+            acc += a * kz1 * k;
+            const float g = zd2 * a * kz1;
+            const __nv_bfloat16 h = __float2bfloat16_rn(g);
+            hi[j] = h;
+            lo[j] = __float2bfloat16_rn(g - __bfloat162float(h));
+        }
+        uint4 *dh = reinterpret_cast<uint4 *>(G_hi + (size_t)row * ldg + col);
+        uint4 *dl = reinterpret_cast<uint4 *>(G_lo + (size_t)row * ldg + col);
+        dh[0] = reinterpret_cast<const uint4 *>(hi)[0];
+        dh[1] = reinterpret_cast<const uint4 *>(hi)[1];
+        dl[0] = reinterpret_cast<const uint4 *>(lo)[0];
+        dl[1] = reinterpret_cast<const uint4 *>(lo)[1];
+    }
+    __device__ __forceinline__ void end(int row, int tile_n, float acc) const
+    {
+        e_part[(size_t)tile_n * rows_pad + row] = (double)acc;
+    }
+};
+
+struct EpiStoreF32 {
+    float *C;
+    int ldc;
+    __device__ __forceinline__ void begin(float &) const {}
+    __device__ __forceinline__ void chunk(int row, int col, const float v[16], float &) const
+    {
+        float4 *d = reinterpret_cast<float4 *>(C + (size_t)row * ldc + col);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) d[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    }
+    __device__ __forceinline__ void end(int, int, float) const {}
+};
+
+// ---------------------------------------------------------------------------- kernel
+
+template <int BN, int STAGES, class Epi>
+__global__ void __launch_bounds__(kTcThreads, 1)
+    k_gemm_bf16x3(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
+                  const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
+                  int num_kb, Epi epi, int *err_flag)
+{
+    constexpr uint32_t A_BYTES = kBM * kBK * 2;
+    constexpr uint32_t B_BYTES = BN * kBK * 2;
+    constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
+    // instruction descriptor: D f32 [4,6)=1, A bf16 [7,10)=1, B bf16 [10,13)=1, K-major A/B,
+    // N>>3 at [17,23), M>>4 at [24,29)
+    constexpr uint32_t IDESC = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(kBM >> 4) << 24);
+
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES], bar_accum;
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ volatile int abort_flag;
+    __shared__ int issued, consumed;
+
+    const uint32_t raw = smem_u32(smem_raw);
+    const uint32_t base = (raw + 1023u) & ~1023u;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_empty[s]), 1);
+        }
+        mbar_init(smem_u32(&bar_accum), 1);
+        abort_flag = 0;
+        issued = 0;
+        consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmA_hi) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmA_lo) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB_hi) : "memory");
+        asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB_lo) : "memory");
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_slot)),
+                     "r"((uint32_t)BN)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_slot;
+
+    if (warp == 0 && lane == 0) {
+        // TMA producer
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (kb >= STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) {
+                abort_flag = 1;
+                break;
+            }
+            const uint32_t st = base + s * STAGE_BYTES;
+            const uint32_t fb = smem_u32(&bar_full[s]);
+            mbar_expect_tx(fb, STAGE_BYTES);
+            tma_load_2d(st, &tmA_hi, fb, kb * kBK, m0);
+            tma_load_2d(st + A_BYTES, &tmA_lo, fb, kb * kBK, m0);
+            tma_load_2d(st + 2 * A_BYTES, &tmB_hi, fb, kb * kBK, n0);
+            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tmB_lo, fb, kb * kBK, n0);
+            issued = kb + 1;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer
+        for (int kb = 0; kb < num_kb; ++kb) {
+            const int s = kb % STAGES;
+            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
+            if (!mbar_wait(smem_u32(&bar_full[s]), ph, &abort_flag)) {
+                abort_flag = 1;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            const uint32_t st = base + s * STAGE_BYTES;
+#pragma unroll
+            for (int k = 0; k < kBK / 16; ++k) {
+                const uint64_t ahi = umma_desc(st + 32 * k);
+                const uint64_t alo = umma_desc(st + A_BYTES + 32 * k);
+                const uint64_t bhi = umma_desc(st + 2 * A_BYTES + 32 * k);
+                const uint64_t blo = umma_desc(st + 2 * A_BYTES + B_BYTES + 32 * k);
+                umma_bf16(tmem, ahi, bhi, IDESC, (kb > 0 || k > 0) ? 1u : 0u);
+                umma_bf16(tmem, ahi, blo, IDESC, 1u);
+                umma_bf16(tmem, alo, bhi, IDESC, 1u);
+            }
+            umma_commit(smem_u32(&bar_empty[s]));
+            consumed = kb + 1;
+        }
+        umma_commit(smem_u32(&bar_accum));
+    }
+    __syncwarp();
+
+    // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w+31
+    const bool ok = mbar_wait(smem_u32(&bar_accum), 0, &abort_flag);
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    __syncwarp();
+    if (ok && !abort_flag) {
+        const int row = m0 + warp * 32 + lane;
+        float acc;
+        epi.begin(acc);
+#pragma unroll 1
+        for (int c = 0; c < BN; c += 16) {
+            float v[16];
+            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
+            epi.chunk(row, n0 + c, v, acc);
+        }
+        epi.end(row, blockIdx.x, acc);
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (abort_flag || !ok) {
+        if (threadIdx.x == 0) {
+            atomicExch(err_flag, 1);
+            // drain this CTA's own copies still in flight (bounded)
+            volatile int dummy = 0;
+            for (int kb = consumed; kb < issued; ++kb)
+                mbar_wait(smem_u32(&bar_full[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &dummy);
+        }
+        __syncthreads();
+    }
+    if (warp == 2) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN)
+                     : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------- host
+
+typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
+                                    const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
+                                    CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static PFN_encodeTiled encode_fn()
+{
+    static PFN_encodeTiled fn = nullptr;
+    if (!fn) {
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = (PFN_encodeTiled)p;
+    }
+    return fn;
+}
+
+// Row-major bf16 matrix [rows][cols] (cols contiguous), box kBK x box_rows, 128B swizzle.
+static int make_map(tgap_context *ctx, CUtensorMap *map, const void *ptr, int rows, int cols, int box_rows)
+{
+    PFN_encodeTiled enc = encode_fn();
+    if (!enc) return set_error(ctx, TGAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
+    if (((uintptr_t)ptr & 15) || (cols * 2) % 16)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tensor map alignment");
+    cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
+    cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
+    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t estr[2] = {1, 1};
+    CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) return set_error(ctx, TGAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
+    return TGAP_OK;
+}
+
+template <int BN, int STAGES, class Epi>
+static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo,
+                       int M, int N, int K, Epi epi)
+{
+    // M, N, K are padded: M % 128 == 0, N % BN == 0, K % 64 == 0 (checked by the caller)
+    CUtensorMap ta_hi, ta_lo, tb_hi, tb_lo;
+    int rc;
+    if ((rc = make_map(ctx, &ta_hi, a_hi, M, K, kBM)) || (rc = make_map(ctx, &ta_lo, a_lo, M, K, kBM)) ||
+        (rc = make_map(ctx, &tb_hi, b_hi, N, K, BN)) || (rc = make_map(ctx, &tb_lo, b_lo, N, K, BN)))
+        return rc;
+    constexpr size_t smem = (size_t)STAGES * (2 * kBM * kBK * 2 + 2 * BN * kBK * 2) + 1024;
+    auto kern = k_gemm_bf16x3<BN, STAGES, Epi>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    if (!ctx->d_flag) {
+        TGAP_CUDA(ctx, cudaMalloc(&ctx->d_flag, sizeof(int)));
+        TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
+    }
+    dim3 grid(N / BN, M / kBM);
+    StageScope sc(ctx, stage);
+    kern<<<grid, kTcThreads, smem, ctx->stream>>>(ta_hi, ta_lo, tb_hi, tb_lo, K / kBK, epi, ctx->d_flag);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+// ---------------------------------------------------------------------------- GAP mixed path
+
+__global__ void k_split_bf16(int R, int C, int ld_in, const double *__restrict__ in, int R_pad, int C_pad,
+                             int transpose, __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo)
+{
+    // out is [R_pad][C_pad] (or [C_pad][R_pad] when transposed), zero padded
+    const size_t total = (size_t)R_pad * C_pad;
+    for (size_t idx = blockIdx.x * (size_t)blockDim.x + threadIdx.x; idx < total; idx += (size_t)gridDim.x * blockDim.x) {
+        const int r = (int)(idx / C_pad), c = (int)(idx % C_pad);
+        const float v = (r < R && c < C) ? (float)in[(size_t)r * ld_in + c] : 0.0f;
+        const __nv_bfloat16 h = __float2bfloat16_rn(v);
+        const __nv_bfloat16 l = __float2bfloat16_rn(v - __bfloat162float(h));
+        const size_t o = transpose ? (size_t)c * R_pad + r : idx;
+        hi[o] = h;
+        lo[o] = l;
+    }
+}
+
+__global__ void k_pad_alphas(int n, int n_pad, const double *__restrict__ a, float *__restrict__ out)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n_pad) out[i] = i < n ? (float)a[i] : 0.0f;
+}
+
+int model_upload_mixed(tgap_context *ctx, DeviceModel *m)
+{
+    m->dim_pad = (m->dim + 127) / 128 * 128;
+    m->m_pad = (m->n_sparse + 127) / 128 * 128;
+    const size_t n = (size_t)m->dim_pad * m->m_pad;
+    if (m->Q_hi.ensure(2 * n) || m->Q_lo.ensure(2 * n) || m->QT_hi.ensure(2 * n) || m->QT_lo.ensure(2 * n) ||
+        m->alphas32.ensure(4 * (size_t)m->m_pad))
+        return set_error(ctx, TGAP_ERR_NOMEM, "mixed model operands");
+    k_split_bf16<<<592, 256, 0, ctx->stream>>>(m->n_sparse, m->dim, m->dim, m->Qs.as<double>(), m->m_pad,
+                                               m->dim_pad, 0, m->Q_hi.as<__nv_bfloat16>(),
+                                               m->Q_lo.as<__nv_bfloat16>());
+    TGAP_LAUNCH_CHECK(ctx);
+    k_split_bf16<<<592, 256, 0, ctx->stream>>>(m->n_sparse, m->dim, m->dim, m->Qs.as<double>(), m->m_pad,
+                                               m->dim_pad, 1, m->QT_hi.as<__nv_bfloat16>(),
+                                               m->QT_lo.as<__nv_bfloat16>());
+    TGAP_LAUNCH_CHECK(ctx);
+    k_pad_alphas<<<(m->m_pad + 255) / 256, 256, 0, ctx->stream>>>(m->n_sparse, m->m_pad, m->alphas.as<double>(),
+                                                                 m->alphas32.as<float>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+__global__ void k_energy_reduce_ld(int M, int n_tiles, int ld, const double *__restrict__ e_part, double d2,
+                                   double e0, const int *__restrict__ sites, double *__restrict__ e_rows,
+                                   double *__restrict__ energies)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= M) return;
+    double s = 0.0;
+    for (int t = 0; t < n_tiles; ++t) s += e_part[(size_t)t * ld + r];
+    const double e = d2 * s + e0;
+    if (e_rows) e_rows[r] = e;
+    if (energies) energies[sites ? sites[r] : r] += e;
+}
+
+int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
+                          const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces, GapWork *w,
+                          const int *d_sites, double *d_e_rows, double *d_energies)
+{
+    if (n_rows <= 0) return TGAP_OK;
+    constexpr int BN1 = 128, BN2 = 64;
+    const int rows_pad = (n_rows + kBM - 1) / kBM * kBM;
+    const int n_tiles = m.m_pad / BN1;
+    if (m.dim_pad % BN2 || m.m_pad % BN1 || m.dim_pad % kBK || m.m_pad % kBK)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "mixed GEMM padding");
+    if (w->e_part.ensure(sizeof(double) * (size_t)n_tiles * rows_pad) ||
+        w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad) ||
+        (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad)))
+        return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
+    const bool zi = std::fabs(m.zeta - (double)(int)m.zeta) < 1.0e-5;  // gap.f90:99-105
+    EpiKernelGap e1;
+    e1.alphas = m.alphas32.as<float>();
+    e1.G_hi = w->G_hi.as<__nv_bfloat16>();
+    e1.G_lo = w->G_lo.as<__nv_bfloat16>();
+    e1.ldg = m.m_pad;
+    e1.e_part = w->e_part.as<double>();
+    e1.rows_pad = rows_pad;
+    e1.zeta_int = zi ? (int)m.zeta : -1;
+    e1.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
+    e1.zd2 = (float)(e1.zeta * m.delta * m.delta);
+    int rc = launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr, rows_pad, m.m_pad,
+                                               m.dim_pad, e1);
+    if (rc) return rc;
+    k_energy_reduce_ld<<<(n_rows + 127) / 128, 128, 0, ctx->stream>>>(n_rows, n_tiles, rows_pad,
+                                                                       w->e_part.as<double>(), m.delta * m.delta,
+                                                                       e0, d_sites, d_e_rows, d_energies);
+    TGAP_LAUNCH_CHECK(ctx);
+    if (!do_forces) return TGAP_OK;
+    EpiStoreF32 e2{w->g.as<float>(), m.dim_pad};
+    return launch_gemm<BN2, 4, EpiStoreF32>(ctx, "gemm_bf16x3_grad", w->G_hi.ptr, w->G_lo.ptr, m.QT_hi.ptr, m.QT_lo.ptr, rows_pad,
+                                            m.dim_pad, m.m_pad, e2);
+}
+
+}  // namespace tgap

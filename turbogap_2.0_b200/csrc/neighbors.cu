@@ -1,0 +1,627 @@
+// Neighbor-list build for batches of periodic structures (sm_100a).
+//
+// Reproduces build_neighbors_list (src/neighbors/neighbors_interface.f90:144-524) pair for
+// pair: self first; orthorhombic boxes that need no replicas use the linked-cell traversal
+// (cell of an atom from the minimum image about the box centre, :311-321; cells visited
+// z -> y -> x over +-1 with the mx/my/mz in {1,2} skips, :352-363; atoms of a cell in
+// decreasing index, the order of the LIFO linked list, :329-330, :365-382); every other box
+// uses the ascending brute-force scan over the supercell (:390-421). Distances follow
+// get_distance (:547-643) operation by operation. This file is compiled with --fmad=false so
+// no multiply-add is contracted and the accept test d < rcut_max sees the same bits as the
+// Fortran arithmetic.
+//
+// One thread owns one central site in both passes (count, then fill at the scanned offset),
+// so the list order inside a site is the sequential order of the reference.
+#include <cub/cub.cuh>
+
+#include "neighbors.h"
+
+namespace tgap {
+
+__device__ __forceinline__ double f_modulo(double a, double p)
+{
+    double r = fmod(a, p);
+    if (r != 0.0 && ((r < 0.0) != (p < 0.0))) r = r + p;
+    return r;
+}
+
+__device__ __forceinline__ int i_modulo(int a, int m)
+{
+    int r = a % m;
+    if (r != 0 && ((r < 0) != (m < 0))) r += m;
+    return r;
+}
+
+__device__ __forceinline__ double dot3(const double *x, const double *y)
+{
+    double s = 0.0;
+    s = s + x[0] * y[0];
+    s = s + x[1] * y[1];
+    s = s + x[2] * y[2];
+    return s;
+}
+
+__device__ void get_distance_dev(const double *pi, const double *pj, const StructDesc &S,
+                                 double dist[3], double *d)
+{
+    if (S.ortho) {
+        const double L[3] = {S.a[0], S.b[1], S.c[2]};
+        double d2 = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            dist[i] = f_modulo(pj[i] - pi[i], L[i]);
+            if (dist[i] > L[i] / 2.0) dist[i] = dist[i] - L[i];
+            d2 = d2 + dist[i] * dist[i];
+        }
+        *d = sqrt(d2);
+        return;
+    }
+    double dv[3] = {pj[0] - pi[0], pj[1] - pi[1], pj[2] - pi[2]};
+    double v[3] = {-1.0 * dot3(dv, S.a), -1.0 * dot3(dv, S.b), -1.0 * dot3(dv, S.c)};
+    int idx[3];
+    for (int i = 0; i < 3; ++i) {
+        double s = 0.0;
+        s = s + S.inv[3 * i + 0] * v[0];
+        s = s + S.inv[3 * i + 1] * v[1];
+        s = s + S.inv[3 * i + 2] * v[2];
+        idx[i] = (int)llround(s);
+    }
+    double res_opt = 1.0e10;
+    double best[3] = {dv[0], dv[1], dv[2]};
+    for (int i = idx[0] - 1; i <= idx[0] + 1; ++i)
+        for (int j = idx[1] - 1; j <= idx[1] + 1; ++j)
+            for (int k = idx[2] - 1; k <= idx[2] + 1; ++k) {
+                double t[3];
+                for (int q = 0; q < 3; ++q)
+                    t[q] = dv[q] + (double)i * S.a[q] + (double)j * S.b[q] + (double)k * S.c[q];
+                double res = dot3(t, t);
+                if (res < res_opt) {
+                    res_opt = res;
+                    best[0] = t[0];
+                    best[1] = t[1];
+                    best[2] = t[2];
+                }
+            }
+    dist[0] = best[0];
+    dist[1] = best[1];
+    dist[2] = best[2];
+    *d = sqrt(dot3(dist, dist));
+}
+
+// Cell coordinates (1-based i2, j2, k2) and the linear cell index of a position.
+__device__ void cell_of(const double *pos, const StructDesc &S, int *i2, int *j2, int *k2,
+                        int *lin)
+{
+    const double tol = 1.0e-10;
+    double centre[3] = {S.a[0] / 2.0, S.b[1] / 2.0, S.c[2] / 2.0};
+    double dist[3], d;
+    get_distance_dev(centre, pos, S, dist, &d);
+    double p[3] = {dist[0] + centre[0], dist[1] + centre[1], dist[2] + centre[2]};
+    int ci = (int)(p[0] / (S.a[0] + tol) * S.mx);
+    int cj = (int)(p[1] / (S.b[1] + tol) * S.my);
+    int ck = (int)(p[2] / (S.c[2] + tol) * S.mz);
+    *i2 = 1 + ci;
+    *j2 = 1 + cj;
+    *k2 = 1 + ck;
+    *lin = i_modulo(ci, S.mx) + i_modulo(cj, S.my) * S.mx + i_modulo(ck, S.mz) * S.my * S.mx;
+}
+
+__global__ void k_cell_count(int n_atoms_total, const int *site_struct, const StructDesc *sd,
+                             const double *pos_sc, int *atom_cell, int *cell_count)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms_total) return;
+    const StructDesc &S = sd[site_struct[g]];
+    if (S.cell_off < 0) return;
+    int local = g - S.atom_off;
+    int i2, j2, k2, lin;
+    cell_of(pos_sc + 3 * (size_t)(S.sc_off + local), S, &i2, &j2, &k2, &lin);
+    atom_cell[g] = S.cell_off + lin;
+    atomicAdd(cell_count + S.cell_off + lin, 1);
+}
+
+__global__ void k_cell_fill(int n_atoms_total, const int *site_struct, const StructDesc *sd,
+                            const int *atom_cell, const int *cell_start, int *cell_cursor,
+                            int *cell_atoms)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms_total) return;
+    const StructDesc &S = sd[site_struct[g]];
+    if (S.cell_off < 0) return;
+    int c = atom_cell[g];
+    int slot = atomicAdd(cell_cursor + c, 1);
+    cell_atoms[cell_start[c] + slot] = g - S.atom_off + 1;  // 1-based local index
+}
+
+// Sort each cell's members in decreasing index (the LIFO order of the linked list).
+__global__ void k_cell_sort(int n_cells, const int *cell_start, int *cell_atoms)
+{
+    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= n_cells) return;
+    int b = cell_start[c], e = cell_start[c + 1];
+    for (int i = b + 1; i < e; ++i) {
+        int v = cell_atoms[i];
+        int j = i - 1;
+        while (j >= b && cell_atoms[j] < v) {
+            cell_atoms[j + 1] = cell_atoms[j];
+            --j;
+        }
+        cell_atoms[j + 1] = v;
+    }
+}
+
+// Pass over one site's candidates in reference order; FILL=false counts, FILL=true writes.
+template <bool FILL>
+__global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const StructDesc *sd,
+                             const double *pos_sc, const int *cell_start, const int *cell_atoms,
+                             int64_t *counts, const int64_t *start, int *list)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms_total) return;
+    const StructDesc S = sd[site_struct[g]];
+    const int i = g - S.atom_off + 1;  // 1-based local site
+    const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
+    const double rc = S.rcut;
+    int64_t w = FILL ? start[g] : 0;
+    int64_t n = 1;
+    if (FILL) list[w++] = i;
+    if (S.cell_off >= 0) {
+        int i2, j2, k2, lin;
+        cell_of(pi, S, &i2, &j2, &k2, &lin);
+        const int mx = S.mx, my = S.my, mz = S.mz;
+        for (int k3 = k2 - 1; k3 <= k2 + 1; ++k3) {
+            if (mz == 1 && k3 != 1) continue;
+            if (mz == 2 && k2 == 1 && k3 == 0) continue;
+            if (mz == 2 && k2 == 2 && k3 == 3) continue;
+            for (int j3 = j2 - 1; j3 <= j2 + 1; ++j3) {
+                if (my == 1 && j3 != 1) continue;
+                if (my == 2 && j2 == 1 && j3 == 0) continue;
+                if (my == 2 && j2 == 2 && j3 == 3) continue;
+                for (int i3 = i2 - 1; i3 <= i2 + 1; ++i3) {
+                    if (mx == 1 && i3 != 1) continue;
+                    if (mx == 2 && i2 == 1 && i3 == 0) continue;
+                    if (mx == 2 && i2 == 2 && i3 == 3) continue;
+                    int c = S.cell_off + i_modulo(i3 - 1, mx) + i_modulo(j3 - 1, my) * mx +
+                            i_modulo(k3 - 1, mz) * mx * my;
+                    for (int t = cell_start[c]; t < cell_start[c + 1]; ++t) {
+                        int k = cell_atoms[t];
+                        if (k == i) continue;
+                        double dist[3], d;
+                        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
+                        if (d < rc) {
+                            if (FILL) list[w++] = k;
+                            ++n;
+                        }
+                    }
+                }
+            }
+        }
+    } else {
+        for (int j = 1; j <= S.n_sc; ++j) {
+            if (j == i) continue;
+            double dist[3], d;
+            get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
+            if (d < rc) {
+                if (FILL) list[w++] = j;
+                ++n;
+            }
+        }
+    }
+    if (!FILL) counts[g] = n;
+}
+
+// Geometry of every pair (neighbors_interface.f90:467-510); angles only when requested.
+__global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const StructDesc *sd,
+                                const double *pos_sc, const int *species_sc, const int64_t *start,
+                                const int *list, double *rjs, double *xyz, double *thetas,
+                                double *phis, int *nspecies, int *jatom)
+{
+    int g = blockIdx.x;
+    if (g >= n_atoms_total) return;
+    const StructDesc &S = sd[site_struct[g]];
+    const int i = g - S.atom_off + 1;
+    const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
+    const int64_t b = start[g], e = start[g + 1];
+    for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+        int j = list[k];
+        if (jatom) jatom[k] = S.atom_off + (j - 1) % S.n;
+        if (nspecies) nspecies[k] = species_sc[S.sc_off + j - 1];
+        if (k == b) {
+            rjs[k] = 0.0;
+            xyz[3 * k] = xyz[3 * k + 1] = xyz[3 * k + 2] = 0.0;
+            if (thetas) thetas[k] = 0.0;
+            if (phis) phis[k] = 0.0;
+            continue;
+        }
+        double dist[3], d;
+        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
+        rjs[k] = d;
+        xyz[3 * k] = dist[0];
+        xyz[3 * k + 1] = dist[1];
+        xyz[3 * k + 2] = dist[2];
+        if (thetas) {
+            if (fabs(dist[2]) >= d)
+                thetas[k] = dist[2] > 0.0 ? 0.0 : acos(-1.0);
+            else
+                thetas[k] = acos(dist[2] / d);
+        }
+        if (phis) phis[k] = atan2(dist[1], dist[0]);
+    }
+}
+
+__global__ void k_start_from_nneigh(int n, const int *n_neigh, int64_t *cnt)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) cnt[g] = n_neigh[g];
+    if (g == n) cnt[g] = 0;
+}
+
+__global__ void k_nneigh_from_counts(int n, const int64_t *cnt, int *n_neigh)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) n_neigh[g] = (int)cnt[g];
+}
+
+static int scan_i64(tgap_context *ctx, DevBuf &tmp, const int64_t *in, int64_t *out, int n)
+{
+    size_t bytes = 0;
+    TGAP_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, ctx->stream));
+    if (tmp.ensure(bytes)) return set_error(ctx, TGAP_ERR_NOMEM, "scan workspace");
+    TGAP_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp.ptr, bytes, in, out, n, ctx->stream));
+    ctx->launches++;
+    return TGAP_OK;
+}
+
+static int scan_i32(tgap_context *ctx, DevBuf &tmp, const int *in, int *out, int n)
+{
+    size_t bytes = 0;
+    TGAP_CUDA(ctx, cub::DeviceScan::ExclusiveSum(nullptr, bytes, in, out, n, ctx->stream));
+    if (tmp.ensure(bytes)) return set_error(ctx, TGAP_ERR_NOMEM, "scan workspace");
+    TGAP_CUDA(ctx, cub::DeviceScan::ExclusiveSum(tmp.ptr, bytes, in, out, n, ctx->stream));
+    ctx->launches++;
+    return TGAP_OK;
+}
+
+// ---------------------------------------------------------------------------- host side
+
+static void host_dot_inverse(const double *a, const double *b, const double *c, double *inv)
+{
+    // neighbors_interface.f90:592-613, same operation order (host code is built without
+    // floating-point contraction).
+    auto dot = [](const double *x, const double *y) {
+        double s = 0.0;
+        s = s + x[0] * y[0];
+        s = s + x[1] * y[1];
+        s = s + x[2] * y[2];
+        return s;
+    };
+    double m[3][3];
+    m[0][0] = dot(a, a);
+    m[0][1] = dot(a, b);
+    m[0][2] = dot(a, c);
+    m[1][0] = m[0][1];
+    m[1][1] = dot(b, b);
+    m[1][2] = dot(b, c);
+    m[2][0] = m[0][2];
+    m[2][1] = m[1][2];
+    m[2][2] = dot(c, c);
+    volatile double md = -(m[0][2] * m[0][2] * m[1][1]);
+    md = md + 2.0 * m[0][1] * m[0][2] * m[1][2];
+    md = md - m[0][0] * (m[1][2] * m[1][2]);
+    md = md - m[0][1] * m[0][1] * m[2][2];
+    md = md + m[0][0] * m[1][1] * m[2][2];
+    double r[3][3];
+    r[0][0] = m[1][1] * m[2][2] - m[1][2] * m[1][2];
+    r[0][1] = m[0][2] * m[1][2] - m[0][1] * m[2][2];
+    r[0][2] = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+    r[1][0] = r[0][1];
+    r[1][1] = m[0][0] * m[2][2] - m[0][2] * m[0][2];
+    r[1][2] = m[0][1] * m[0][2] - m[0][0] * m[1][2];
+    r[2][0] = r[0][2];
+    r[2][1] = r[1][2];
+    r[2][2] = m[0][0] * m[1][1] - m[0][1] * m[0][1];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) inv[3 * i + j] = r[i][j] / md;
+}
+
+int make_struct_desc(const double a[3], const double b[3], const double c[3], int box_small,
+                     double rcut, StructDesc *S)
+{
+    const double d_tol = 1.0e-6;
+    std::memcpy(S->a, a, sizeof(S->a));
+    std::memcpy(S->b, b, sizeof(S->b));
+    std::memcpy(S->c, c, sizeof(S->c));
+    S->ortho = std::fabs(a[1]) < d_tol && std::fabs(a[2]) < d_tol && std::fabs(b[0]) < d_tol &&
+               std::fabs(b[2]) < d_tol && std::fabs(c[0]) < d_tol && std::fabs(c[1]) < d_tol;
+    if (S->ortho) {
+        S->a[1] = S->a[2] = S->b[0] = S->b[2] = S->c[0] = S->c[1] = 0.0;
+    } else {
+        host_dot_inverse(S->a, S->b, S->c, S->inv);
+    }
+    S->rcut = rcut;
+    S->cell_off = -1;
+    S->mx = S->my = S->mz = 0;
+    if (S->ortho && !box_small) {
+        S->mx = (int)(S->a[0] / rcut);
+        S->my = (int)(S->b[1] / rcut);
+        S->mz = (int)(S->c[2] / rcut);
+        if (S->mx < 1 || S->my < 1 || S->mz < 1) return TGAP_ERR_ARGUMENT;
+        S->cell_off = 0;  // set by the caller when batching
+    }
+    return TGAP_OK;
+}
+
+int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
+                    int64_t *n_pairs_out, bool with_angles)
+{
+    const int n = nb->n_atoms;
+    if (n <= 0) {
+        *n_pairs_out = 0;
+        return TGAP_OK;
+    }
+    const int T = 128;
+    const int grid = (n + T - 1) / T;
+    StructDesc *d_sd = nb->d_structs.as<StructDesc>();
+    if (rebuild) {
+        StageScope sc(ctx, "neighbors_rebuild");
+        // cells
+        if (nb->n_cells > 0) {
+            TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_count.ptr, 0, sizeof(int) * (nb->n_cells + 1), ctx->stream));
+            k_cell_count<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd,
+                                                      nb->pos_sc.as<double>(), nb->atom_cell.as<int>(),
+                                                      nb->cell_count.as<int>());
+            TGAP_LAUNCH_CHECK(ctx);
+            int rc = scan_i32(ctx, nb->scan_tmp, nb->cell_count.as<int>(), nb->cell_start.as<int>(),
+                              nb->n_cells + 1);
+            if (rc) return rc;
+            TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_cursor.ptr, 0, sizeof(int) * nb->n_cells, ctx->stream));
+            k_cell_fill<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd,
+                                                     nb->atom_cell.as<int>(), nb->cell_start.as<int>(),
+                                                     nb->cell_cursor.as<int>(), nb->cell_atoms.as<int>());
+            TGAP_LAUNCH_CHECK(ctx);
+            k_cell_sort<<<(nb->n_cells + T - 1) / T, T, 0, ctx->stream>>>(
+                nb->n_cells, nb->cell_start.as<int>(), nb->cell_atoms.as<int>());
+            TGAP_LAUNCH_CHECK(ctx);
+        }
+        k_site_pairs<false><<<grid, T, 0, ctx->stream>>>(
+            n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
+            nb->cell_atoms.as<int>(), nb->counts.as<int64_t>(), nullptr, nullptr);
+        TGAP_LAUNCH_CHECK(ctx);
+        TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
+        int rc = scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
+        if (rc) return rc;
+        int64_t total = 0;
+        TGAP_CUDA(ctx, cudaMemcpyAsync(&total, nb->start.as<int64_t>() + n, sizeof(int64_t),
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+        TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+        *n_pairs_out = total;
+        if (capacity >= 0 && total > capacity) return TGAP_ERR_CAPACITY;
+        if (nb->ensure_pairs(total)) return set_error(ctx, TGAP_ERR_NOMEM, "pair arrays");
+        nb->n_pairs = total;
+        k_nneigh_from_counts<<<grid, T, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->n_neigh.as<int>());
+        TGAP_LAUNCH_CHECK(ctx);
+        k_site_pairs<true><<<grid, T, 0, ctx->stream>>>(
+            n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
+            nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(), nb->list.as<int>());
+        TGAP_LAUNCH_CHECK(ctx);
+    } else {
+        *n_pairs_out = nb->n_pairs;
+    }
+    StageScope sc(ctx, "neighbors_geometry");
+    k_pair_geometry<<<n, 64, 0, ctx->stream>>>(
+        n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->species_sc.as<int>(),
+        nb->start.as<int64_t>(), nb->list.as<int>(), nb->rjs.as<double>(), nb->xyz.as<double>(),
+        with_angles ? nb->thetas.as<double>() : nullptr, with_angles ? nb->phis.as<double>() : nullptr,
+        nb->nspecies.as<int>(), nb->jatom.as<int>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+// Start offsets from a caller-provided n_neigh (geometry-only refresh of a given list).
+int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb)
+{
+    const int n = nb->n_atoms;
+    const int T = 128;
+    k_start_from_nneigh<<<(n + 1 + T - 1) / T, T, 0, ctx->stream>>>(n, nb->n_neigh.as<int>(),
+                                                                       nb->counts.as<int64_t>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
+}
+
+int NeighborBatch::ensure_pairs(int64_t P)
+{
+    size_t p = (size_t)(P > 0 ? P : 1);
+    if (list.ensure(p * sizeof(int))) return 1;
+    if (rjs.ensure(p * sizeof(double))) return 1;
+    if (xyz.ensure(3 * p * sizeof(double))) return 1;
+    if (thetas.ensure(p * sizeof(double))) return 1;
+    if (phis.ensure(p * sizeof(double))) return 1;
+    if (nspecies.ensure(p * sizeof(int))) return 1;
+    if (jatom.ensure(p * sizeof(int))) return 1;
+    return 0;
+}
+
+// Lay out the structures: supercell replication (read_xyz.f90:323-373, replica order
+// a -> b -> c outer, atoms inner), cell grids, per-site structure ids. Host arrays in.
+int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, const int *offsets,
+                    const double *positions, const double *boxes, const int *species,
+                    double rcut, const int *force_small)
+{
+    std::vector<StructDesc> sd(n_structures);
+    std::vector<double> pos_sc;
+    std::vector<int> sp_sc, site_struct;
+    int n_cells = 0, sc_total = 0;
+    for (int b = 0; b < n_structures; ++b) {
+        const int n = offsets[b + 1] - offsets[b];
+        const double *bx = boxes + 9 * b;
+        int idx[3];
+        tgap_number_of_unit_cells(bx, bx + 3, bx + 6, rcut, idx);
+        int small = idx[0] > 1 || idx[1] > 1 || idx[2] > 1;
+        if (force_small && force_small[b]) small = 1;
+        double a[3], bb[3], c[3];
+        for (int q = 0; q < 3; ++q) {
+            a[q] = bx[q];
+            bb[q] = bx[3 + q];
+            c[q] = bx[6 + q];
+        }
+        const int rep = idx[0] * idx[1] * idx[2];
+        StructDesc &S = sd[b];
+        S.atom_off = offsets[b];
+        S.n = n;
+        S.sc_off = sc_total;
+        S.n_sc = n * rep;
+        for (int i2 = 1; i2 <= idx[0]; ++i2)
+            for (int j2 = 1; j2 <= idx[1]; ++j2)
+                for (int k2 = 1; k2 <= idx[2]; ++k2)
+                    for (int i = 0; i < n; ++i) {
+                        const double *p = positions + 3 * (size_t)(offsets[b] + i);
+                        for (int q = 0; q < 3; ++q) {
+                            volatile double v = p[q] + (double)(i2 - 1) * a[q];
+                            v = v + (double)(j2 - 1) * bb[q];
+                            v = v + (double)(k2 - 1) * c[q];
+                            pos_sc.push_back((double)v);
+                        }
+                        sp_sc.push_back(species[offsets[b] + i]);
+                    }
+        for (int q = 0; q < 3; ++q) {
+            a[q] = (double)idx[0] * a[q];
+            bb[q] = (double)idx[1] * bb[q];
+            c[q] = (double)idx[2] * c[q];
+        }
+        for (int q = 0; q < 3; ++q) {
+            S.pa[q] = bx[q];
+            S.pb[q] = bx[3 + q];
+            S.pc[q] = bx[6 + q];
+        }
+        int rc = make_struct_desc(a, bb, c, small, rcut, &S);
+        if (rc) return set_error(ctx, rc, "structure %d: cell smaller than the cutoff", b);
+        S.rep[0] = idx[0];
+        S.rep[1] = idx[1];
+        S.rep[2] = idx[2];
+        if (S.cell_off >= 0) {
+            S.cell_off = n_cells;
+            n_cells += S.mx * S.my * S.mz;
+        }
+        sc_total += S.n_sc;
+        for (int i = 0; i < n; ++i) site_struct.push_back(b);
+    }
+    nb->n_structures = n_structures;
+    nb->n_atoms = offsets[n_structures];
+    nb->n_sc_total = sc_total;
+    nb->n_cells = n_cells;
+    nb->host_structs = sd;
+    size_t N = (size_t)nb->n_atoms;
+    if (nb->d_structs.ensure(sizeof(StructDesc) * n_structures) ||
+        nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)sc_total) ||
+        nb->species_sc.ensure(sizeof(int) * (size_t)sc_total) ||
+        nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
+        nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
+        nb->start.ensure(sizeof(int64_t) * (N + 1)) || nb->n_neigh.ensure(sizeof(int) * N) ||
+        nb->positions.ensure(sizeof(double) * 3 * N))
+        return set_error(ctx, TGAP_ERR_NOMEM, "neighbor set-up");
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->d_structs.ptr, sd.data(), sizeof(StructDesc) * n_structures,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->pos_sc.ptr, pos_sc.data(), sizeof(double) * pos_sc.size(),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->species_sc.ptr, sp_sc.data(), sizeof(int) * sp_sc.size(),
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->site_struct.ptr, site_struct.data(), sizeof(int) * N,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions, sizeof(double) * 3 * N,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+// Replicate the resident positions into the supercell copy (after an MD update).
+__global__ void k_replicate(int n_atoms_total, const int *site_struct, const StructDesc *sd,
+                            const double *pos, double *pos_sc)
+{
+    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= n_atoms_total) return;
+    const StructDesc &S = sd[site_struct[g]];
+    const int i = g - S.atom_off;
+    // lattice vectors of the primitive cell = supercell vectors / replicas
+    int r = 0;
+    for (int i2 = 0; i2 < S.rep[0]; ++i2)
+        for (int j2 = 0; j2 < S.rep[1]; ++j2)
+            for (int k2 = 0; k2 < S.rep[2]; ++k2, ++r) {
+                double *o = pos_sc + 3 * (size_t)(S.sc_off + r * S.n + i);
+                for (int q = 0; q < 3; ++q) {
+                    double v = pos[3 * (size_t)g + q] + (double)i2 * S.pa[q];
+                    v = v + (double)j2 * S.pb[q];
+                    v = v + (double)k2 * S.pc[q];
+                    o[q] = v;
+                }
+            }
+}
+
+int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites, int n_sc,
+                              const double *positions_sc, const double a[3], const double b[3],
+                              const double c[3], int box_small, double rcut,
+                              const int *species_sc)
+{
+    StructDesc S;
+    std::memset(&S, 0, sizeof(S));
+    int rc = make_struct_desc(a, b, c, box_small, rcut, &S);
+    if (rc) return set_error(ctx, rc, "cell smaller than the cutoff on the linked-cell path");
+    S.atom_off = 0;
+    S.n = n_sites;
+    S.sc_off = 0;
+    S.n_sc = n_sc;
+    S.rep[0] = S.rep[1] = S.rep[2] = 1;
+    for (int q = 0; q < 3; ++q) {
+        S.pa[q] = S.a[q];
+        S.pb[q] = S.b[q];
+        S.pc[q] = S.c[q];
+    }
+    int n_cells = S.cell_off >= 0 ? S.mx * S.my * S.mz : 0;
+    nb->n_structures = 1;
+    nb->n_atoms = n_sites;
+    nb->n_sc_total = n_sc;
+    nb->n_cells = n_cells;
+    nb->host_structs.assign(1, S);
+    size_t N = (size_t)n_sites;
+    if (nb->d_structs.ensure(sizeof(StructDesc)) ||
+        nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)n_sc) ||
+        nb->species_sc.ensure(sizeof(int) * (size_t)n_sc) ||
+        nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
+        nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
+        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
+        nb->start.ensure(sizeof(int64_t) * (N + 1)) || nb->n_neigh.ensure(sizeof(int) * N) ||
+        nb->positions.ensure(sizeof(double) * 3 * N))
+        return set_error(ctx, TGAP_ERR_NOMEM, "neighbor set-up");
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->d_structs.ptr, &S, sizeof(StructDesc), cudaMemcpyHostToDevice,
+                                   ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->pos_sc.ptr, positions_sc, sizeof(double) * 3 * (size_t)n_sc,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    if (species_sc)
+        TGAP_CUDA(ctx, cudaMemcpyAsync(nb->species_sc.ptr, species_sc, sizeof(int) * (size_t)n_sc,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    else
+        TGAP_CUDA(ctx, cudaMemsetAsync(nb->species_sc.ptr, 0, sizeof(int) * (size_t)n_sc, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(nb->site_struct.ptr, 0, sizeof(int) * N, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions_sc, sizeof(double) * 3 * N,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+int neighbors_sync_positions(tgap_context *ctx, NeighborBatch *nb)
+{
+    const int n = nb->n_atoms;
+    const int T = 128;
+    StageScope sc(ctx, "replicate_positions");
+    k_replicate<<<(n + T - 1) / T, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(),
+                                                          nb->d_structs.as<StructDesc>(),
+                                                          nb->positions.as<double>(),
+                                                          nb->pos_sc.as<double>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+}  // namespace tgap

@@ -1,0 +1,76 @@
+// Neighbor-list data of a batch of periodic structures resident on the device.
+#pragma once
+
+#include <cstring>
+#include <vector>
+
+#include "tgap_internal.h"
+
+namespace tgap {
+
+// One periodic structure of a batch. Lattice vectors are those of the (replicated) supercell.
+struct StructDesc {
+    double a[3], b[3], c[3];
+    double inv[9];      // inverse Gram matrix, row-major (triclinic minimum image)
+    double rcut;        // list cutoff (model cutoff + skin)
+    int ortho;
+    int atom_off;       // first global site
+    int n;              // sites
+    int sc_off;         // first supercell position
+    int n_sc;           // supercell atoms (n * replicas)
+    int rep[3];         // replicas along a, b, c
+    int cell_off;       // first cell of the linked-cell grid, -1 = brute-force path
+    int mx, my, mz;
+    double pa[3], pb[3], pc[3];  // primitive lattice vectors (before replication)
+};
+
+struct NeighborBatch {
+    int n_structures = 0;
+    int n_atoms = 0;        // central sites over all structures
+    int n_sc_total = 0;
+    int n_cells = 0;
+    int64_t n_pairs = 0;
+    std::vector<StructDesc> host_structs;
+    DevBuf d_structs;
+    DevBuf positions;       // double [3 n_atoms] (primitive cells; MD state)
+    DevBuf pos_sc;          // double [3 n_sc_total]
+    DevBuf species_sc;      // int [n_sc_total]
+    DevBuf site_struct;     // int [n_atoms]
+    DevBuf atom_cell, cell_count, cell_start, cell_cursor, cell_atoms;
+    DevBuf counts;          // int64 [n_atoms + 1]
+    DevBuf start;           // int64 [n_atoms + 1]
+    DevBuf n_neigh;         // int [n_atoms]
+    DevBuf list;            // int [P], 1-based supercell index within the structure
+    DevBuf rjs, xyz, thetas, phis;
+    DevBuf nspecies;        // int [P] species channel of the neighbor
+    DevBuf jatom;           // int [P] folded global atom of the neighbor
+    DevBuf scan_tmp;
+    int ensure_pairs(int64_t P);
+    void release_all()
+    {
+        DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &atom_cell,
+                          &cell_count, &cell_start, &cell_cursor, &cell_atoms, &counts, &start,
+                          &n_neigh, &list, &rjs, &xyz, &thetas, &phis, &nspecies, &jatom,
+                          &scan_tmp};
+        for (DevBuf *b : bufs) b->release();
+    }
+};
+
+int make_struct_desc(const double a[3], const double b[3], const double c[3], int box_small,
+                     double rcut, StructDesc *S);
+// Host arrays in: offsets[n_structures + 1], positions 3 x n_atoms, boxes 9 per structure,
+// species per atom. force_small (optional, per structure) selects the brute-force path.
+int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, const int *offsets,
+                    const double *positions, const double *boxes, const int *species,
+                    double rcut, const int *force_small);
+// Supercell layout given directly (reference build_neighbors_list surface, one structure).
+int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites, int n_sc,
+                              const double *positions_sc, const double a[3], const double b[3],
+                              const double c[3], int box_small, double rcut,
+                              const int *species_sc);
+int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
+                    int64_t *n_pairs_out, bool with_angles);
+int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb);
+int neighbors_sync_positions(tgap_context *ctx, NeighborBatch *nb);
+
+}  // namespace tgap

@@ -1,0 +1,29 @@
+// Launchers of the descriptor kernels (soap.cu).
+#pragma once
+
+#include <cuda_bf16.h>
+
+#include "tgap_internal.h"
+
+namespace tgap {
+
+// Outputs of the forward pass for n_rows sites (element type double or float by precision).
+struct SoapOut {
+    void *c = nullptr;     // [n_rows][n_max][nlm] expansion coefficients
+    void *q = nullptr;     // [n_rows][q_ld] normalised descriptor (columns >= dim are zero)
+    void *norm = nullptr;  // [n_rows] |p|
+    int q_ld = 0;
+    __nv_bfloat16 *q_hi = nullptr;  // optional bf16 split of q for the tensor-core GEMM
+    __nv_bfloat16 *q_lo = nullptr;
+};
+
+int upload_ylm_constants();
+int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
+                 int n_rows, int precision, SoapOut &o);
+int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
+                  int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
+                  int g_is_double, const int *site_struct, double *d_forces, double *d_virial);
+int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
+                  int n_rows, const SoapOut &o, double *d_der);
+
+}  // namespace tgap

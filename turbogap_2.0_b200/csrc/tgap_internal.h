@@ -1,0 +1,157 @@
+// Internal declarations shared by the CUDA translation units of libtgap.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cstdio>
+#include <string>
+#include <vector>
+
+#include "../../include/tgap.h"
+
+namespace tgap {
+
+// Compile-time bounds of the descriptor kernels.
+constexpr int kMaxSpecies = 4;
+constexpr int kMaxAlpha = 16;     // radial functions per species
+constexpr int kMaxNmax = 16;      // radial functions summed over species
+constexpr int kMaxL = 10;         // l_max
+constexpr int kMaxNodes = 192;    // quadrature nodes per species
+
+struct Error {
+    int status;
+    std::string msg;
+};
+
+// Growable device buffer owned by a context or object.
+struct DevBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+// Pinned host staging buffer.
+struct HostBuf {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    int ensure(size_t n);
+    void release();
+    template <class T> T *as() const { return static_cast<T *>(ptr); }
+};
+
+}  // namespace tgap
+
+namespace tgap {
+struct StageRecord {
+    int stage;
+    cudaEvent_t start, stop;
+};
+}  // namespace tgap
+
+struct tgap_context {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::string last_error;
+    int64_t launches = 0;
+    // scratch buffers reused across calls (host-buffer entry points)
+    tgap::DevBuf scratch[24];
+    tgap::HostBuf pinned[4];
+    int *d_flag = nullptr;  // device error flag (bounded waits, overflow)
+    // stage timing
+    bool timing = false;
+    std::vector<std::string> stage_names;
+    std::vector<double> stage_ms;
+    std::vector<int64_t> stage_count;
+    std::vector<tgap::StageRecord> pending;
+    std::vector<cudaEvent_t> event_pool;
+};
+
+namespace tgap {
+
+// Brackets one kernel stage with CUDA events on the context stream when timing is enabled.
+class StageScope {
+  public:
+    StageScope(tgap_context *ctx, const char *name);
+    ~StageScope();
+
+  private:
+    tgap_context *ctx_;
+    int rec_ = -1;
+};
+
+int set_error(tgap_context *ctx, int status, const char *fmt, ...);
+int cuda_check(tgap_context *ctx, cudaError_t e, const char *what);
+
+#define TGAP_CUDA(ctx, call)                                           \
+    do {                                                               \
+        cudaError_t _e = (call);                                       \
+        if (_e != cudaSuccess) return ::tgap::cuda_check(ctx, _e, #call); \
+    } while (0)
+
+#define TGAP_LAUNCH_CHECK(ctx)                                         \
+    do {                                                               \
+        (ctx)->launches++;                                             \
+        cudaError_t _e = cudaGetLastError();                           \
+        if (_e != cudaSuccess) return ::tgap::cuda_check(ctx, _e, "kernel launch"); \
+    } while (0)
+
+// ---------------------------------------------------------------------------- hypers
+
+// Descriptor settings in device-friendly form (one per model), plus host-built tables.
+struct SoapParams {
+    int n_species;
+    int l_max;
+    int n_max;              // sum of alpha_max
+    int dim;                // n_max (n_max + 1) / 2 (l_max + 1)
+    int radial_enhancement;
+    int alpha_max[kMaxSpecies];
+    int n_off[kMaxSpecies];  // first radial index of each species block
+    int n_nodes[kMaxSpecies];
+    int node_off[kMaxSpecies];
+    int tq_off[kMaxSpecies];
+    int max_alpha;
+    double rcut_hard[kMaxSpecies], rcut_soft[kMaxSpecies], nf[kMaxSpecies];
+    double global_scaling[kMaxSpecies], sigma_r[kMaxSpecies], sigma_r_scaling[kMaxSpecies];
+    double sigma_t[kMaxSpecies], sigma_t_scaling[kMaxSpecies];
+    double amplitude_scaling[kMaxSpecies], central_weight[kMaxSpecies];
+    double rcut_max;
+};
+
+// Host-side tables: quadrature node positions, weighted orthonormal basis values
+// (node-major, alpha_max per node) and the central-atom radial coefficients.
+struct SoapTables {
+    std::vector<double> xq;       // sum n_nodes
+    std::vector<double> tq;       // sum n_nodes * alpha_max
+    std::vector<double> central;  // n_max (R_n(0) * central_weight * Y_00 per species block)
+};
+
+int make_soap_params(const tgap_soap_hypers *h, SoapParams *p, std::string *why);
+// tables.cpp (binary128 arithmetic on the host)
+int build_soap_tables(const SoapParams &p, SoapTables *t);
+void poly3_orthonormaliser(int alpha_max, double *W);  // W = S^{-1/2}, row-major
+
+// Device copy of the tables for one model.
+struct DeviceSoap {
+    SoapParams p;
+    DevBuf xq, tq, central;
+    float *xq_f = nullptr, *tq_f = nullptr, *central_f = nullptr;  // single-precision copies
+    DevBuf xq32, tq32, central32;
+};
+int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, DeviceSoap *d);
+
+// ---------------------------------------------------------------------------- pairs
+
+// Read-only view of a neighbor list for the descriptor kernels.
+struct PairView {
+    const int64_t *start;   // [n_sites_total + 1]
+    const double *xyz;      // [3 P]  r_j - r_i (minimum image)
+    const double *rjs;      // [P]
+    const int *species;     // [P]    species channel of the neighbor (1-based, 0 = blind)
+    const int *jatom;       // [P]    folded global neighbor index (force scatter)
+};
+
+}  // namespace tgap
