@@ -291,7 +291,8 @@ def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
     vel = synth.maxwell_boltzmann(masses, 3000.0, seed=1)
     model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
     system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
-    md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=10, use_graph=True)
+    # rebuild often enough that no pair crosses rcut + skin between rebuilds at 3000 K
+    md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=4, use_graph=True)
     md.set_velocities(vel)
     steps = 12
     md.run(steps)
