@@ -128,6 +128,32 @@ int tgap_get_soap_energy_and_forces(tgap_context *ctx, int n_soap, int n_sites, 
                                     int n_atom_pairs, int do_forces, int n_sites0,
                                     double *energies, double *forces, double *virial);
 
+/* No counterpart in the reference. Per-site GAP energies delta^2 sum_s alpha_s (q_i.Q_s)^zeta
+ * + e0 (the energy half of get_soap_energy_and_forces) for inputs that are already on the
+ * device, without allocating any device memory.
+ *
+ * Who needs it: host programs that only hold device memory handed to them by someone else, for
+ * example a Fortran MD/MC driver whose arrays live in an OpenACC or CUDA Fortran data region, or
+ * a code that sizes one memory pool at start-up and may not create allocations of its own in
+ * its inner loop (cudaMalloc/cudaFree there can synchronize the whole device or fail when the
+ * pool has taken the memory). The MC driver, which asks for energies only, is the typical caller.
+ *
+ * How: the only scratch the computation needs (per-tile energy partials) is a fixed array of
+ * 2^20 doubles (8 MiB) compiled into the library, so every GPU that loads libtgap reserves it
+ * until the process exits. Limit: n_sites * ceil(n_sparse / 64) <= 1048576, otherwise
+ * TGAP_ERR_CAPACITY is returned and nothing runs. The array is shared by all calls: every entry
+ * that is read is first written by the same call, so nothing has to start at zero, but calls
+ * whose work overlaps on the GPU (other streams, other host threads) race on it and must be
+ * serialized by the caller. The first call on each device looks up the array's device address
+ * (cudaGetSymbolAddress) with that device current; make that first call before any stream
+ * capture. Pointers are device pointers in the layout of tgap_get_soap_energy_and_forces
+ * (d_soap: n_soap x n_sites, d_Qs: n_soap x n_sparse, d_alphas: n_sparse, d_energies:
+ * n_sites, overwritten). Work is queued on `stream` (a cudaStream_t, NULL = default stream);
+ * the call does not synchronize. */
+int tgap_soap_energies_noalloc(void *stream, int n_soap, int n_sites, int n_sparse,
+                               const double *d_soap, const double *d_alphas, double delta,
+                               double zeta0, double e0, const double *d_Qs, double *d_energies);
+
 /* Descriptor hyperparameters of one soap_turbo model (read_gap.f90:156-432), per species. */
 typedef struct {
     int n_species;

@@ -8,6 +8,9 @@
 // The first GEMM's epilogue evaluates K^zeta, the energy row partials and the scaled
 // derivative matrix G = zeta delta^2 alpha o K^(zeta-1), which is the A operand of the
 // second GEMM g = G Qs. Both are "NT" products (row-major operands, K contiguous).
+#include <cmath>
+#include <mutex>
+
 #include "gap_kernels.h"
 
 namespace tgap {
@@ -267,6 +270,68 @@ int pair_forces_from_der(tgap_context *ctx, int n_sites, const int64_t *d_start,
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
+
+// ----------------------------------------------------------------------------- no-allocation entry
+
+// Scratch of tgap_soap_energies_noalloc: the per-tile energy partials of the K = q Qs^T
+// product, one double per (64-column tile of sparse points, site). 2^20 doubles (8 MiB) are
+// reserved on every GPU that loads the library, for the lifetime of the process.
+constexpr size_t kNoAllocPartials = (size_t)1 << 20;
+static __device__ __align__(256) double g_noalloc_e_part[kNoAllocPartials];
+
+// Device address of the scratch array, looked up once per device (the symbol name is only a
+// host-side handle; kernels must be given the address cudaGetSymbolAddress returns).
+static int noalloc_scratch(double **out)
+{
+    static std::mutex mu;
+    static double *addr[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return TGAP_ERR_CUDA;
+    std::lock_guard<std::mutex> lock(mu);
+    if (!addr[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_e_part) != cudaSuccess || !p) return TGAP_ERR_CUDA;
+        addr[dev] = static_cast<double *>(p);
+    }
+    *out = addr[dev];
+    return TGAP_OK;
+}
+
+}  // namespace tgap
+
+// Energies of get_soap_energy_and_forces with do_forces = .false. for device-resident inputs,
+// with no device allocation (declaration and contract in include/tgap.h).
+extern "C" int tgap_soap_energies_noalloc(void *stream, int n_soap, int n_sites, int n_sparse,
+                                          const double *d_soap, const double *d_alphas, double delta,
+                                          double zeta0, double e0, const double *d_Qs,
+                                          double *d_energies)
+{
+    using namespace tgap;
+    if (n_soap <= 0 || n_sites <= 0 || n_sparse <= 0 || !d_soap || !d_alphas || !d_Qs || !d_energies)
+        return TGAP_ERR_ARGUMENT;
+    const int n_tiles = (n_sparse + kBN - 1) / kBN;
+    if ((size_t)n_tiles * (size_t)n_sites > kNoAllocPartials) return TGAP_ERR_CAPACITY;
+    double *e_part = nullptr;
+    int rc = noalloc_scratch(&e_part);
+    if (rc) return rc;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    EpiGap e;
+    e.alphas = d_alphas;
+    e.G = nullptr;
+    e.ldg = n_sparse;
+    e.e_part = e_part;  // every (tile, site) entry is written before it is read
+    const bool zi = std::fabs(zeta0 - (double)(int)zeta0) < 1.0e-5;  // gap.f90:99-105
+    e.zeta_int = zi ? (int)zeta0 : -1;
+    e.zeta = zi ? (double)(int)zeta0 : zeta0;
+    e.zd2 = e.zeta * delta * delta;
+    dim3 grid(n_tiles, (n_sites + kBM - 1) / kBM);
+    k_dgemm_nt<EpiGap><<<grid, kGemmThreads, 0, s>>>(n_sites, n_sparse, n_soap, d_soap, n_soap, d_Qs, n_soap, e);
+    k_energy_reduce<<<(n_sites + 127) / 128, 128, 0, s>>>(n_sites, n_tiles, e_part, delta * delta, e0, nullptr,
+                                                          d_energies, nullptr);
+    return cudaGetLastError() == cudaSuccess ? TGAP_OK : TGAP_ERR_CUDA;
+}
+
+namespace tgap {
 
 __global__ void k_transpose(int R, int Cc, const double *__restrict__ in, double *__restrict__ out)
 {
