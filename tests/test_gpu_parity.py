@@ -192,6 +192,24 @@ def test_resident_compute_fp64_matches_oracle(ctx, tg, synth, carbon):
     assert np.max(np.abs(v_g[0] - v_o)) < V_TOL
 
 
+def test_dense_sites_with_more_than_32_pairs(ctx, tg, synth, carbon):
+    """3.5 g/cm3: most sites have 33-46 in-cutoff neighbors, so the warp kernels compact and
+    process each site's pairs in several 32-pair passes."""
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(200, 3.5, 1.1, seed=33)
+    nb = orc.build_neighbors(pos, len(pos), *box, 3.7, sp, False)
+    assert nb["n_neigh"].max() - 1 > 40
+    e_o, f_o, v_o = helpers.oracle_structure_eval(hyp, [m], pos, box, sp)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7)
+    e_g, f_g, v_g = _compute(tg, ctx, system, [model], tg.TGAP_FP64, len(pos))
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g[0] - v_o)) < V_TOL
+    e32, f32, _ = _compute(tg, ctx, system, [model], tg.TGAP_MIXED, len(pos))
+    assert np.sqrt(np.mean((e32 - e_g) ** 2)) < 0.5e-3 and np.sqrt(np.mean((f32 - f_g) ** 2)) < 5e-3
+
+
 def test_batched_uneven_triclinic_structures(ctx, tg, synth, carbon):
     hyp, m = carbon
     structs = []
@@ -286,6 +304,10 @@ def test_mixed_get_gap_soap_matches_resident_mixed(ctx, tg, synth, carbon):
 # ------------------------------------------------------------------------- MD
 
 def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
+    """Every step of the device MD (CUDA-graph steps and the eager rebuild steps in between)
+    against the oracle: forces at the device's positions within F_TOL, and the velocity-Verlet
+    update (md_utils.f90:486-532) of the oracle from the device's previous state within 1e-12.
+    The pair list grows across rebuilds here, which must re-capture the step graph."""
     hyp, m = carbon
     pos, box, sp, masses = synth.random_packing(128, 2.5, 1.2, seed=70)
     vel = synth.maxwell_boltzmann(masses, 3000.0, seed=1)
@@ -294,18 +316,18 @@ def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
     # rebuild often enough that no pair crosses rcut + skin between rebuilds at 3000 K
     md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=4, use_graph=True)
     md.set_velocities(vel)
-    steps = 12
-    md.run(steps)
-    st = md.state()
-    # oracle: forces at x(t) then velocity_verlet, list rebuilt every step at the model cutoff
-    x = pos.copy()
-    v = vel.copy()
-    xp = np.zeros_like(x)
-    fp = np.zeros_like(x)
     mm = masses * synth.AMU_TO_EV_FS2_A2
-    dtp = 1.0
-    for k in range(steps):
+    x, v = pos.copy(), vel.copy()
+    xp, fp = np.zeros_like(x), np.zeros_like(x)
+    pairs = set()
+    for k in range(14):
+        md.run(1)
+        st = md.state()
+        pairs.add(system.n_pairs)
         _, f, _ = helpers.oracle_structure_eval(hyp, [m], x, box, sp)
-        dtp = orc.velocity_verlet(x, xp, v, f, fp, mm, 1.0, dtp, k == 0)
-    assert np.max(np.abs(st["positions"] - x)) < 1e-9
-    assert np.max(np.abs(st["velocities"] - v)) < 1e-9
+        assert np.max(np.abs(st["forces"] - f)) < F_TOL, k
+        orc.velocity_verlet(x, xp, v, st["forces"], fp, mm, 1.0, 1.0, k == 0)
+        assert np.max(np.abs(st["positions"] - x)) < 1e-12, k
+        assert np.max(np.abs(st["velocities"] - v)) < 1e-12, k
+        x, v = st["positions"].copy(), st["velocities"].copy()
+    assert len(pairs) > 1  # the list changed size across rebuilds

@@ -2,6 +2,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstring>
@@ -21,9 +22,13 @@ using namespace tgap;
 
 namespace tgap {
 
+std::atomic<uint64_t> g_alloc_epoch{0};
+
 int DevBuf::ensure(size_t n)
 {
     if (n <= bytes && ptr) return 0;
+    // any (re)allocation can move a buffer that a captured graph still refers to
+    g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;
@@ -39,6 +44,7 @@ int DevBuf::ensure(size_t n)
 
 void DevBuf::release()
 {
+    if (ptr) g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
     if (ptr) cudaFree(ptr);
     ptr = nullptr;
     bytes = 0;
@@ -623,10 +629,9 @@ struct tgap_system {
     double rcut;
     std::vector<int> host_species;
     std::vector<SiteSet> site_sets;
-    DevBuf c, q, norm, q_hi, q_lo, e_rows;
+    DevBuf c, q, norm, q_hi, q_lo, e_rows, vir_rows;
     GapWork gw;
     DevBuf scratch_forces;
-    int generation = 0;  // bumps when a device buffer is reallocated (graph re-capture)
 };
 
 extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
@@ -704,7 +709,7 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
-                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces};
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->vir_rows};
     for (DevBuf *b : bufs) b->release();
     delete s;
     return TGAP_OK;
@@ -736,10 +741,8 @@ extern "C" int tgap_system_update(tgap_system *s, int rebuild)
     tgap_context *ctx = s->ctx;
     CHECK_RC(activate(ctx));
     CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
-    void *before = s->nb.list.ptr;
     int64_t P = 0;
     CHECK_RC(neighbors_build(ctx, &s->nb, rebuild, -1, &P, false));
-    if (s->nb.list.ptr != before) s->generation++;
     return TGAP_OK;
 }
 
@@ -771,21 +774,20 @@ static int ensure_eval_buffers(tgap_system *s, const tgap_model *m, int n_rows, 
     const size_t tsz = precision == TGAP_FP64 ? 8 : 4;
     const int q_ld = precision == TGAP_FP64 ? P.dim : m->gap.dim_pad;
     const int rows_pad = (n_rows + 127) / 128 * 128;
-    void *before[5] = {s->c.ptr, s->q.ptr, s->norm.ptr, s->q_hi.ptr, s->q_lo.ptr};
+    if (s->vir_rows.ensure(sizeof(double) * 6 * (size_t)n_rows))
+        return set_error(s->ctx, TGAP_ERR_NOMEM, "virial rows");
     if (s->c.ensure(tsz * (size_t)n_rows * P.n_max * nlm) || s->q.ensure(tsz * (size_t)rows_pad * q_ld) ||
         s->norm.ensure(tsz * (size_t)n_rows))
         return set_error(s->ctx, TGAP_ERR_NOMEM, "descriptor workspace");
     if (precision != TGAP_FP64) {
+        const uint64_t e0 = g_alloc_epoch.load();
         if (s->q_hi.ensure(2 * (size_t)rows_pad * q_ld) || s->q_lo.ensure(2 * (size_t)rows_pad * q_ld))
             return set_error(s->ctx, TGAP_ERR_NOMEM, "descriptor workspace");
-    }
-    void *after[5] = {s->c.ptr, s->q.ptr, s->norm.ptr, s->q_hi.ptr, s->q_lo.ptr};
-    for (int i = 0; i < 5; ++i)
-        if (before[i] != after[i]) s->generation++;
-    // rows past n_rows feed the 128-row GEMM tiles: keep them zero
-    if (precision != TGAP_FP64 && (before[3] != after[3] || before[4] != after[4])) {
-        TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_hi.ptr, 0, s->q_hi.bytes, s->ctx->stream));
-        TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_lo.ptr, 0, s->q_lo.bytes, s->ctx->stream));
+        // rows past n_rows feed the 128-row GEMM tiles: keep them zero (fresh buffers only)
+        if (g_alloc_epoch.load() != e0) {
+            TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_hi.ptr, 0, s->q_hi.bytes, s->ctx->stream));
+            TGAP_CUDA(s->ctx, cudaMemsetAsync(s->q_lo.ptr, 0, s->q_lo.bytes, s->ctx->stream));
+        }
     }
     return TGAP_OK;
 }
@@ -808,10 +810,8 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     if (precision == TGAP_FP64) {
         o.q_ld = m->gap.dim;
         CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o));
-        void *gb = s->gw.G.ptr;
         CHECK_RC(gap_energy_grad_f64(ctx, m->gap, (const double *)o.q, o.q_ld, n_rows, 0.0, do_forces,
                                      &s->gw, sites, nullptr, d_energies));
-        if (s->gw.G.ptr != gb) s->generation++;
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o, s->gw.g.ptr, m->gap.dim,
                                    1, s->nb.site_struct.as<int>(), d_forces, d_virial));
@@ -821,10 +821,8 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
         o.q_hi = s->q_hi.as<__nv_bfloat16>();
         o.q_lo = s->q_lo.as<__nv_bfloat16>();
         CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o));
-        void *gb = s->gw.G_hi.ptr;
         CHECK_RC(gap_energy_grad_mixed(ctx, m->gap, o.q_hi, o.q_lo, n_rows, 0.0, do_forces, &s->gw, sites,
                                        nullptr, d_energies));
-        if (s->gw.G_hi.ptr != gb) s->generation++;
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o, s->gw.g.ptr,
                                    m->gap.dim_pad, 0, s->nb.site_struct.as<int>(), d_forces, d_virial));
@@ -1033,7 +1031,7 @@ struct tgap_md {
     DevBuf mass, vel, forces, forces_prev, pos_prev, energies, virial;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
-    int graph_generation = -1;
+    uint64_t graph_epoch = 0;  // allocation epoch the graph was captured at
     int64_t graph_kernels = 0;
 };
 
@@ -1128,7 +1126,7 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
                                      md->first ? 1 : 0));
             md->first = false;
         } else if (md->use_graph) {
-            if (!md->exec || md->graph_generation != md->sys->generation) {
+            if (!md->exec || md->graph_epoch != g_alloc_epoch.load(std::memory_order_relaxed)) {
                 if (md->exec) cudaGraphExecDestroy(md->exec);
                 if (md->graph) cudaGraphDestroy(md->graph);
                 md->exec = nullptr;
@@ -1147,7 +1145,7 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
                 if (ce != cudaSuccess) return cuda_check(ctx, ce, "graph capture");
                 md->graph = g;
                 TGAP_CUDA(ctx, cudaGraphInstantiate(&md->exec, g, 0));
-                md->graph_generation = md->sys->generation;
+                md->graph_epoch = g_alloc_epoch.load(std::memory_order_relaxed);
             }
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec, ctx->stream));
             ctx->launches += md->graph_kernels;

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <atomic>
 #include <cstdio>
 #include <string>
 #include <vector>
@@ -23,6 +24,10 @@ struct Error {
     int status;
     std::string msg;
 };
+
+// Incremented by every device (re)allocation or release of a DevBuf; a captured CUDA graph is
+// valid only while the epoch it was captured at is current.
+extern std::atomic<uint64_t> g_alloc_epoch;
 
 // Growable device buffer owned by a context or object.
 struct DevBuf {
