@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <string>
@@ -177,11 +178,15 @@ extern "C" int tgap_create(int device, tgap_context **out)
         return TGAP_ERR_CUDA;
     }
     ctx->stream = ctx->own_stream;
-    if (upload_ylm_constants() != 0) {
+    if (upload_ylm_constants() != 0 || cudaMalloc(&ctx->d_check, 4 * sizeof(int)) != cudaSuccess ||
+        cudaMemset(ctx->d_check, 0, 4 * sizeof(int)) != cudaSuccess) {
+        if (ctx->d_check) cudaFree(ctx->d_check);
         cudaStreamDestroy(ctx->own_stream);
         delete ctx;
         return TGAP_ERR_CUDA;
     }
+    const char *sc = std::getenv("TGAP_SYNC_CHECK");
+    ctx->sync_check = sc && sc[0] == '1';
     *out = ctx;
     return TGAP_OK;
 }
@@ -199,6 +204,7 @@ extern "C" int tgap_destroy(tgap_context *ctx)
     }
     for (cudaEvent_t e : ctx->event_pool) cudaEventDestroy(e);
     if (ctx->d_flag) cudaFree(ctx->d_flag);
+    if (ctx->d_check) cudaFree(ctx->d_check);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return TGAP_OK;
@@ -211,11 +217,42 @@ extern "C" int tgap_set_stream(tgap_context *ctx, void *stream)
     return TGAP_OK;
 }
 
+namespace tgap {
+
+int read_device_check(tgap_context *ctx)
+{
+    int h[4] = {0, 0, 0, 0};
+    TGAP_CUDA(ctx, cudaMemcpyAsync(h, ctx->d_check, sizeof(h), cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (h[0] == kCheckNone) return TGAP_OK;
+    TGAP_CUDA(ctx, cudaMemsetAsync(ctx->d_check, 0, sizeof(h), ctx->stream));
+    static const char *what[] = {"",
+                                 "descriptor forward: pair outside its site",
+                                 "descriptor adjoint: pair outside its site",
+                                 "descriptor adjoint: neighbor atom out of range",
+                                 "descriptor adjoint: self-slot atom out of range",
+                                 "non-finite force",
+                                 "neighbor fill past its counted range"};
+    const char *w = (h[0] > 0 && h[0] <= kCheckListOverrun) ? what[h[0]] : "unknown check";
+    return set_error(ctx, h[0] == kCheckNonFinite ? TGAP_ERR_NUMERIC : TGAP_ERR_CUDA,
+                     "device check %d (%s): index %d value %d, %d failure(s)", h[0], w, h[1], h[2], h[3]);
+}
+
+int sync_check_launch(tgap_context *ctx)
+{
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    TGAP_CUDA(ctx, cudaStreamIsCapturing(ctx->stream, &cs));
+    if (cs != cudaStreamCaptureStatusNone) return TGAP_OK;
+    return read_device_check(ctx);
+}
+
+}  // namespace tgap
+
 extern "C" int tgap_synchronize(tgap_context *ctx)
 {
     CHECK_RC(activate(ctx));
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    return TGAP_OK;
+    return read_device_check(ctx);
 }
 
 extern "C" const char *tgap_last_error(const tgap_context *ctx)
@@ -502,7 +539,8 @@ extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh,
         S[5].ensure(sizeof(double) * (size_t)n_sites * P.dim + 8) ||
         S[6].ensure(sizeof(double) * (size_t)n_sites + 8))
         return set_error(ctx, TGAP_ERR_NOMEM, "descriptor workspace");
-    PairView pv{S[0].as<int64_t>(), S[1].as<double>(), S[2].as<double>(), S[3].as<int>(), nullptr};
+    PairView pv{S[0].as<int64_t>(), S[1].as<double>(), S[2].as<double>(), S[3].as<int>(), nullptr, 0,
+                ctx->d_check};
     SoapOut o;
     o.c = S[4].ptr;
     o.q = S[5].ptr;
@@ -801,7 +839,7 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     if (n_rows == 0) return TGAP_OK;
     CHECK_RC(ensure_eval_buffers(s, m, n_rows, precision));
     PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
-                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>()};
+                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>(), s->nb.n_atoms, ctx->d_check};
     SoapOut o;
     o.c = s->c.ptr;
     o.q = s->q.ptr;
@@ -814,7 +852,8 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
                                      &s->gw, sites, nullptr, d_energies));
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o, s->gw.g.ptr, m->gap.dim,
-                                   1, s->nb.site_struct.as<int>(), d_forces, d_virial));
+                                   1, s->nb.struct_off.as<int>(), s->nb.n_structures, s->vir_rows.as<double>(),
+                                   d_forces, d_virial));
     } else {
         if (!m->mixed_ready) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "mixed path not prepared");
         o.q_ld = m->gap.dim_pad;
@@ -825,7 +864,8 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
                                        nullptr, d_energies));
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o, s->gw.g.ptr,
-                                   m->gap.dim_pad, 0, s->nb.site_struct.as<int>(), d_forces, d_virial));
+                                   m->gap.dim_pad, 0, s->nb.struct_off.as<int>(), s->nb.n_structures,
+                                   s->vir_rows.as<double>(), d_forces, d_virial));
     }
     return TGAP_OK;
 }
@@ -892,7 +932,7 @@ extern "C" int tgap_descriptors(tgap_context *ctx, tgap_system *s, const tgap_mo
     if (ss->n_rows == 0) return TGAP_OK;
     CHECK_RC(ensure_eval_buffers(s, m, ss->n_rows, TGAP_FP64));
     PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
-                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>()};
+                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>(), s->nb.n_atoms, ctx->d_check};
     SoapOut o;
     o.c = s->c.ptr;
     o.q = d_soap;
@@ -954,13 +994,15 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
     if (S[16].ensure(8 * (size_t)n_rows * Pp.n_max * nlm + 8) || S[17].ensure(8 * (size_t)rows_pad * q_ld + 8) ||
         S[18].ensure(8 * (size_t)n_rows + 8) || S[19].ensure(8 * (size_t)n_total_sites) ||
         S[20].ensure(8 * 3 * (size_t)n_total_sites) || S[21].ensure(8 * 9) ||
-        S[22].ensure(2 * (size_t)rows_pad * q_ld + 8) || S[23].ensure(2 * (size_t)rows_pad * q_ld + 8))
+        S[22].ensure(2 * (size_t)rows_pad * q_ld + 8) || S[23].ensure(2 * (size_t)rows_pad * q_ld + 8) ||
+        S[5].ensure(8 * 6 * (size_t)n_rows + 8))
         return set_error(ctx, TGAP_ERR_NOMEM, "get_gap_soap workspace");
     if (precision != TGAP_FP64) {
         TGAP_CUDA(ctx, cudaMemsetAsync(S[22].ptr, 0, 2 * (size_t)rows_pad * q_ld, ctx->stream));
         TGAP_CUDA(ctx, cudaMemsetAsync(S[23].ptr, 0, 2 * (size_t)rows_pad * q_ld, ctx->stream));
     }
-    PairView pv{S[10].as<int64_t>(), S[11].as<double>(), S[12].as<double>(), S[13].as<int>(), S[14].as<int>()};
+    PairView pv{S[10].as<int64_t>(), S[11].as<double>(), S[12].as<double>(), S[13].as<int>(), S[14].as<int>(),
+                n_total_sites, ctx->d_check};
     SoapOut o;
     o.c = S[16].ptr;
     o.q = S[17].ptr;
@@ -983,7 +1025,7 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
                                           S[9].as<int>(), nullptr, d_e);
         if (!rc && do_forces)
             rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_FP64, o, w.g.ptr, Pp.dim, 1,
-                               nullptr, d_f, d_v);
+                               nullptr, 1, S[5].as<double>(), d_f, d_v);
     } else {
         o.q_hi = S[22].as<__nv_bfloat16>();
         o.q_lo = S[23].as<__nv_bfloat16>();
@@ -992,7 +1034,7 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
                                             S[9].as<int>(), nullptr, d_e);
         if (!rc && do_forces)
             rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_MIXED, o, w.g.ptr, m->gap.dim_pad,
-                               0, nullptr, d_f, d_v);
+                               0, nullptr, 1, S[5].as<double>(), d_f, d_v);
     }
     std::vector<double> he(n_total_sites), hf(3 * (size_t)n_total_sites);
     if (!rc) rc = download(ctx, he.data(), S[19], (size_t)n_total_sites);
@@ -1171,6 +1213,7 @@ extern "C" int tgap_md_get_state(tgap_md *md, double *positions, double *velocit
     CHECK_RC(download(ctx, e.data(), md->energies, (size_t)N));
     CHECK_RC(download(ctx, m.data(), md->mass, (size_t)N));
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    CHECK_RC(read_device_check(ctx));
     if (velocities) std::memcpy(velocities, v.data(), sizeof(double) * 3 * N);
     double ep = 0.0, ek = 0.0;
     for (int i = 0; i < N; ++i) {

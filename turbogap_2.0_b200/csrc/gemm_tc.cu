@@ -256,6 +256,11 @@ __global__ void __launch_bounds__(kTcThreads, 1)
             tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tmB_lo, fb, kb * kBK, n0);
             issued = kb + 1;
         }
+        // tail: wait until the MMAs have released the last STAGES tiles, so no asynchronous
+        // arrive on a stage barrier is still pending when the CTA exits (bounded)
+        for (int kb = (num_kb > STAGES ? num_kb - STAGES : 0); kb < issued && !abort_flag; ++kb)
+            if (!mbar_wait(smem_u32(&bar_empty[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &abort_flag))
+                abort_flag = 1;
     } else if (warp == 1 && lane == 0) {
         // MMA issuer
         for (int kb = 0; kb < num_kb; ++kb) {

@@ -153,7 +153,7 @@ __global__ void k_cell_sort(int n_cells, const int *cell_start, int *cell_atoms)
 template <bool FILL>
 __global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const StructDesc *sd,
                              const double *pos_sc, const int *cell_start, const int *cell_atoms,
-                             int64_t *counts, const int64_t *start, int *list)
+                             int64_t *counts, const int64_t *start, int *list, int *check)
 {
     int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= n_atoms_total) return;
@@ -162,8 +162,17 @@ __global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const St
     const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
     const double rc = S.rcut;
     int64_t w = FILL ? start[g] : 0;
+    const int64_t w_end = FILL ? start[g + 1] : 0;
+    // the fill pass repeats the count pass, so it never reaches w_end; checked all the same
+    auto put = [&](int v) {
+        if (w < w_end)
+            list[w] = v;
+        else
+            check_fail(check, kCheckListOverrun, g, v);
+        ++w;
+    };
     int64_t n = 1;
-    if (FILL) list[w++] = i;
+    if (FILL) put(i);
     if (S.cell_off >= 0) {
         int i2, j2, k2, lin;
         cell_of(pi, S, &i2, &j2, &k2, &lin);
@@ -188,7 +197,7 @@ __global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const St
                         double dist[3], d;
                         get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
                         if (d < rc) {
-                            if (FILL) list[w++] = k;
+                            if (FILL) put(k);
                             ++n;
                         }
                     }
@@ -201,7 +210,7 @@ __global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const St
             double dist[3], d;
             get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
             if (d < rc) {
-                if (FILL) list[w++] = j;
+                if (FILL) put(j);
                 ++n;
             }
         }
@@ -384,7 +393,7 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
         }
         k_site_pairs<false><<<grid, T, 0, ctx->stream>>>(
             n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
-            nb->cell_atoms.as<int>(), nb->counts.as<int64_t>(), nullptr, nullptr);
+            nb->cell_atoms.as<int>(), nb->counts.as<int64_t>(), nullptr, nullptr, nullptr);
         TGAP_LAUNCH_CHECK(ctx);
         TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
         int rc = scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
@@ -401,7 +410,7 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
         TGAP_LAUNCH_CHECK(ctx);
         k_site_pairs<true><<<grid, T, 0, ctx->stream>>>(
             n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
-            nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(), nb->list.as<int>());
+            nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(), nb->list.as<int>(), ctx->d_check);
         TGAP_LAUNCH_CHECK(ctx);
     } else {
         *n_pairs_out = nb->n_pairs;
@@ -514,6 +523,7 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
         nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)sc_total) ||
         nb->species_sc.ensure(sizeof(int) * (size_t)sc_total) ||
         nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
+        nb->struct_off.ensure(sizeof(int) * (size_t)(nb->n_structures + 1)) ||
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
@@ -528,6 +538,8 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->species_sc.ptr, sp_sc.data(), sizeof(int) * sp_sc.size(),
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->site_struct.ptr, site_struct.data(), sizeof(int) * N,
+                                   cudaMemcpyHostToDevice, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->struct_off.ptr, offsets, sizeof(int) * (size_t)(n_structures + 1),
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions, sizeof(double) * 3 * N,
                                    cudaMemcpyHostToDevice, ctx->stream));
@@ -588,6 +600,7 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
         nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)n_sc) ||
         nb->species_sc.ensure(sizeof(int) * (size_t)n_sc) ||
         nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
+        nb->struct_off.ensure(sizeof(int) * (size_t)(nb->n_structures + 1)) ||
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
@@ -605,6 +618,8 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
     else
         TGAP_CUDA(ctx, cudaMemsetAsync(nb->species_sc.ptr, 0, sizeof(int) * (size_t)n_sc, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(nb->site_struct.ptr, 0, sizeof(int) * N, ctx->stream));
+    const int so[2] = {0, n_sites};
+    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->struct_off.ptr, so, sizeof(so), cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions_sc, sizeof(double) * 3 * N,
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

@@ -2,13 +2,16 @@
 // back-scatter of dE/dq to forces and virial, and the materialised dq/dr of the reference
 // get_soap surface (soap_cart_der, call site src/gap/gap_interface.f90:301-306).
 //
-// One CTA of 256 threads owns one central site. Pairs are processed in chunks of 64; the
-// four lanes of a pair split the radial quadrature nodes and the harmonic orders m, so a
-// chunk fills the CTA. The expansion c_{n,lm} = sum_j R_n(r_j) A_lm(r_j) is then a small
-// (n_max x 64) x (64 x nlm) product out of shared memory. The templates run in FP64 (plain
-// path) or FP32 (mixed path); positions, pair vectors, forces and the virial stay FP64.
+// Forward and adjoint (soap_warp.cuh): one warp owns one central site, one lane one pair, with
+// l_max a template parameter (0..10). The expansion c_{n,lm} = sum_j R_n(r_j) A_lm(r_j) is a
+// small (n_max x 32) x (32 x nlm) product out of the warp's shared memory per group of 32
+// pairs. The materialised dq/dr keeps one CTA of 256 threads per site, four lanes per pair
+// splitting the quadrature nodes and harmonic orders. The templates run in FP64 (plain path)
+// or FP32 (mixed path); positions, pair vectors, forces and the virial stay FP64.
 #include <cuda_bf16.h>
 
+#include <algorithm>
+#include <climits>
 #include <cmath>
 #include <type_traits>
 
@@ -184,281 +187,7 @@ __device__ __forceinline__ int ps_index(int n, int np, int nmax, int L, int l)
     return (n * nmax - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
 }
 
-// ----------------------------------------------------------------------------- forward
-
-template <class T, bool SPLIT>
-__global__ void __launch_bounds__(kThreads) k_soap_forward(
-    SoapParams P, const T *__restrict__ xq, const T *__restrict__ tq, const T *__restrict__ central,
-    const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
-    const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
-    T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
-    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    T *smem = reinterpret_cast<T *>(smem_raw);
-    const int nmax = P.n_max, L = P.l_max, nlm = (L + 1) * (L + 1), dim = P.dim;
-    T *Rs = smem;                               // [64][nmax]
-    T *As = Rs + kPairsPerChunk * nmax;         // [64][nlm]
-    T *cs = As + kPairsPerChunk * nlm;          // [nmax][nlm]
-    T *ps = cs + nmax * nlm;                    // [dim]
-    T *red = ps + dim;                          // [32]
-
-    const int row = blockIdx.x;
-    if (row >= n_rows) return;
-    const int site = sites ? sites[row] : row;
-    const int64_t kb = start[site], ke = start[site + 1];
-    const int t = threadIdx.x, pl = t >> 2, sub = t & 3;
-    const int nout = nmax * nlm;
-    constexpr int kMaxOut = (kMaxNmax * kNlmMax + kThreads - 1) / kThreads;
-    T creg[kMaxOut];
-#pragma unroll
-    for (int j = 0; j < kMaxOut; ++j) creg[j] = 0;
-
-    for (int64_t cb = kb; cb < ke; cb += kPairsPerChunk) {
-        for (int i = t; i < kPairsPerChunk * (nmax + nlm); i += kThreads) Rs[i] = 0;
-        __syncthreads();
-        const int64_t k = cb + pl;
-        int s;
-        T r, u[3], rv[3];
-        const bool valid = pair_setup<T>(P, k, kb, ke, rjs, xyz, nsp, &s, &r, u, rv);
-        const T rc = (T)P.rcut_hard[s];
-        const T x = r / rc;
-        const T sig = ((T)P.sigma_r[s] + (T)P.sigma_r_scaling[s] * r) / rc;
-        const T dsig = (T)P.sigma_r_scaling[s];
-        T sum[kMaxAlpha], dsum[kMaxAlpha];
-        radial_node_sums<T, false>(P, s, valid, xq, tq, x, sig, dsig, sub, sum, dsum);
-        if (valid) {
-            T A, dA;
-            radial_amplitude<T>(P, s, x, sig, dsig, &A, &dA);
-            const T g = (T)P.global_scaling[s] * A;
-            if (sub == 0) {
-                const int off = P.n_off[s];
-#pragma unroll
-                for (int n = 0; n < kMaxAlpha; ++n)
-                    if (n < P.alpha_max[s]) Rs[pl * nmax + off + n] = g * sum[n];
-            }
-            const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
-            T f[kMaxL + 2];
-            bessel_ratios<T>(L, r * r / (st * st), f);
-            T *Arow = As + pl * nlm;
-            ylm_lane<T, false>(L, u[0], u[1], u[2], sub,
-                               [&](int kk, int l, T Y, T, T, T) { Arow[kk] = f[l] * Y; });
-        }
-        __syncthreads();
-        // c += R^T A over the chunk
-#pragma unroll
-        for (int j = 0; j < kMaxOut; ++j) {
-            const int o = t + j * kThreads;
-            if (o < nout) {
-                const int n = o / nlm, kk = o - n * nlm;
-                T acc = 0;
-#pragma unroll 8
-                for (int p = 0; p < kPairsPerChunk; ++p) acc += Rs[p * nmax + n] * As[p * nlm + kk];
-                creg[j] += acc;
-            }
-        }
-        __syncthreads();
-    }
-    // central atom (self slot species) on l = 0
-    const int s_self = nsp[kb] - 1;
-#pragma unroll
-    for (int j = 0; j < kMaxOut; ++j) {
-        const int o = t + j * kThreads;
-        if (o < nout) {
-            const int n = o / nlm, kk = o - n * nlm;
-            T v = creg[j];
-            if (kk == 0 && s_self >= 0 && s_self < P.n_species && n >= P.n_off[s_self] &&
-                n < P.n_off[s_self] + P.alpha_max[s_self])
-                v += central[n];
-            cs[o] = v;
-            c_out[(size_t)row * nout + o] = v;
-        }
-    }
-    __syncthreads();
-    // power spectrum
-    T part = 0;
-    for (int d = t; d < dim; d += kThreads) {
-        int n, np, l;
-        ps_decode(d, nmax, L, &n, &np, &l);
-        const T *a = cs + n * nlm, *b = cs + np * nlm;
-        T acc = 0;
-        for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
-        const T v = (n == np) ? acc : acc * (T)1.4142135623730951;
-        ps[d] = v;
-        part += v * v;
-    }
-    const T nrm2 = block_sum<T>(part, red);
-    const T nrm = t_sqrt<T>(nrm2);
-    const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-    for (int d = t; d < q_ld; d += kThreads) {
-        T qv = d < dim ? ps[d] * inv : (T)0;
-        q_out[(size_t)row * q_ld + d] = qv;
-        if (SPLIT) {
-            const float qf = (float)qv;
-            const __nv_bfloat16 h = __float2bfloat16_rn(qf);
-            q_hi[(size_t)row * q_ld + d] = h;
-            q_lo[(size_t)row * q_ld + d] = __float2bfloat16_rn(qf - __bfloat162float(h));
-        }
-    }
-    if (t == 0) norm_out[row] = nrm;
-}
-
-// ----------------------------------------------------------------------------- adjoint
-
-// g: dE/dq per row (GT = double or float). forces: 3 per global atom, virial: 9 per structure.
-template <class T, class GT>
-__global__ void __launch_bounds__(kThreads) k_soap_backward(
-    SoapParams P, const T *__restrict__ xq, const T *__restrict__ tq, const int *__restrict__ sites,
-    int n_rows, const int64_t *__restrict__ start, const double *__restrict__ rjs,
-    const double *__restrict__ xyz, const int *__restrict__ nsp, const int *__restrict__ jatom,
-    const int *__restrict__ site_struct, const T *__restrict__ c_in, const T *__restrict__ q_in,
-    int q_ld, const T *__restrict__ norm_in, const GT *__restrict__ g_in, int g_ld,
-    double *__restrict__ forces, double *__restrict__ virial)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    double *dred = reinterpret_cast<double *>(smem_raw);  // [9][8] per-warp partials
-    T *smem = reinterpret_cast<T *>(smem_raw + 80 * sizeof(double));
-    const int nmax = P.n_max, L = P.l_max, nlm = (L + 1) * (L + 1), dim = P.dim;
-    T *cs = smem;               // [nmax][nlm]
-    T *Gc = cs + nmax * nlm;    // [nmax][nlm]
-    T *hs = Gc + nmax * nlm;    // [dim]
-    T *red = hs + dim;          // [32]
-
-    const int row = blockIdx.x;
-    if (row >= n_rows) return;
-    const int site = sites ? sites[row] : row;
-    const int64_t kb = start[site], ke = start[site + 1];
-    const int t = threadIdx.x, pl = t >> 2, sub = t & 3;
-    const int nout = nmax * nlm;
-    for (int o = t; o < nout; o += kThreads) cs[o] = c_in[(size_t)row * nout + o];
-    T part = 0;
-    for (int d = t; d < dim; d += kThreads)
-        part += q_in[(size_t)row * q_ld + d] * (T)g_in[(size_t)row * g_ld + d];
-    const T qg = block_sum<T>(part, red);
-    const T nrm = norm_in[row];
-    const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-    for (int d = t; d < dim; d += kThreads)
-        hs[d] = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
-    __syncthreads();
-    // dE/dc_{n,lm} = sum_n' M_l[n][n'] c_{n',lm}
-    for (int o = t; o < nout; o += kThreads) {
-        const int n = o / nlm, kk = o - n * nlm;
-        int l = 0;
-        while ((l + 1) * (l + 1) <= kk) ++l;
-        T acc = 0;
-        for (int np = 0; np < nmax; ++np) {
-            const T h = hs[ps_index(n, np, nmax, L, l)];
-            const T coef = (np == n) ? (T)2 * h : (T)1.4142135623730951 * h;
-            acc += coef * cs[np * nlm + kk];
-        }
-        Gc[o] = acc;
-    }
-    __syncthreads();
-
-    double fself[3] = {0, 0, 0}, vir[6] = {0, 0, 0, 0, 0, 0};
-    for (int64_t cb = kb; cb < ke; cb += kPairsPerChunk) {
-        const int64_t k = cb + pl;
-        int s;
-        T r, u[3], rv[3];
-        const bool valid = pair_setup<T>(P, k, kb, ke, rjs, xyz, nsp, &s, &r, u, rv);
-        const T rc = (T)P.rcut_hard[s];
-        const T x = r / rc;
-        const T sig = ((T)P.sigma_r[s] + (T)P.sigma_r_scaling[s] * r) / rc;
-        const T dsig = (T)P.sigma_r_scaling[s];
-        T sum[kMaxAlpha], dsum[kMaxAlpha];
-        radial_node_sums<T, true>(P, s, valid, xq, tq, x, sig, dsig, sub, sum, dsum);
-        T w0 = 0, w1 = 0, w2 = 0;
-        if (valid) {
-            T A, dA;
-            radial_amplitude<T>(P, s, x, sig, dsig, &A, &dA);
-            const T gs = (T)P.global_scaling[s];
-            T R[kMaxAlpha], dR[kMaxAlpha];
-#pragma unroll
-            for (int n = 0; n < kMaxAlpha; ++n) {
-                R[n] = gs * A * sum[n];
-                dR[n] = gs * (dA * sum[n] + A * dsum[n]) / rc;
-            }
-            const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
-            const T kap = r * r / (st * st);
-            const T dkap = (T)2 * r / (st * st) -
-                           (T)2 * r * r * (T)P.sigma_t_scaling[s] / (st * st * st);
-            T f[kMaxL + 2];
-            bessel_ratios<T>(L, kap, f);
-            const T ir = (T)1 / r;
-            const int off = P.n_off[s], am = P.alpha_max[s];
-            ylm_lane<T, true>(L, u[0], u[1], u[2], sub, [&](int kk, int l, T Y, T gx, T gy, T gz) {
-                T U = 0, V = 0;
-#pragma unroll
-                for (int n = 0; n < kMaxAlpha; ++n) {
-                    if (n < am) {
-                        const T gcv = Gc[(off + n) * nlm + kk];
-                        U += gcv * R[n];
-                        V += gcv * dR[n];
-                    }
-                }
-                const T fl = f[l];
-                const T dfl = (f[l + 1] + (T)l / kap * fl - fl * f[1]) * dkap;
-                const T ug = u[0] * gx + u[1] * gy + u[2] * gz;
-                const T Ak = fl * Y;
-                const T radial_part = Ak * V + U * dfl * Y;
-                const T tang = U * fl * ir;
-                w0 += u[0] * radial_part + tang * (gx - u[0] * ug);
-                w1 += u[1] * radial_part + tang * (gy - u[1] * ug);
-                w2 += u[2] * radial_part + tang * (gz - u[2] * ug);
-            });
-        }
-        w0 += __shfl_xor_sync(0xffffffffu, w0, 1);
-        w0 += __shfl_xor_sync(0xffffffffu, w0, 2);
-        w1 += __shfl_xor_sync(0xffffffffu, w1, 1);
-        w1 += __shfl_xor_sync(0xffffffffu, w1, 2);
-        w2 += __shfl_xor_sync(0xffffffffu, w2, 1);
-        w2 += __shfl_xor_sync(0xffffffffu, w2, 2);
-        if (valid && sub == 0) {
-            // w = dE_i/dr_ij; force on j is -w, on i is +w (self slot of the reference)
-            const double f0 = -(double)w0, f1 = -(double)w1, f2 = -(double)w2;
-            const int j = jatom[k];
-            atomicAdd(forces + 3 * (size_t)j, f0);
-            atomicAdd(forces + 3 * (size_t)j + 1, f1);
-            atomicAdd(forces + 3 * (size_t)j + 2, f2);
-            fself[0] -= f0;
-            fself[1] -= f1;
-            fself[2] -= f2;
-            const double x0 = xyz[3 * k], x1 = xyz[3 * k + 1], x2 = xyz[3 * k + 2];
-            vir[0] += f0 * x0;
-            vir[1] += f1 * x1;
-            vir[2] += f2 * x2;
-            vir[3] += 0.5 * (f0 * x1 + f1 * x0);
-            vir[4] += 0.5 * (f0 * x2 + f2 * x0);
-            vir[5] += 0.5 * (f1 * x2 + f2 * x1);
-        }
-    }
-    // reduce self force and virial over the CTA
-    double vals[9] = {fself[0], fself[1], fself[2], vir[0], vir[1], vir[2], vir[3], vir[4], vir[5]};
-    const int lane = t & 31, wid = t >> 5;
-#pragma unroll
-    for (int i = 0; i < 9; ++i) {
-        double v = vals[i];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) dred[i * 8 + wid] = v;
-    }
-    __syncthreads();
-    if (t < 9) {
-        double v = 0;
-        for (int w = 0; w < kThreads / 32; ++w) v += dred[t * 8 + w];
-        if (t < 3) {
-            atomicAdd(forces + 3 * (size_t)jatom[kb] + t, v);
-        } else {
-            const int st = site_struct ? site_struct[site] : 0;
-            double *V = virial + 9 * (size_t)st;
-            // xx yy zz xy xz yz -> column-major 3x3 (symmetric)
-            const int idx[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
-            const int a = idx[t - 3][0], b = idx[t - 3][1];
-            atomicAdd(V + a + 3 * b, v);
-            if (a != b) atomicAdd(V + b + 3 * a, v);
-        }
-    }
-}
+#include "soap_warp.cuh"
 
 // ----------------------------------------------------------------------------- dq/dr
 
@@ -617,39 +346,98 @@ __global__ void __launch_bounds__(kThreads) k_soap_cart_der(
 
 // ----------------------------------------------------------------------------- host
 
-static size_t fwd_smem(const SoapParams &P, size_t tsz)
-{
-    const int nlm = (P.l_max + 1) * (P.l_max + 1);
-    return tsz * ((size_t)kPairsPerChunk * (P.n_max + nlm) + (size_t)P.n_max * nlm + P.dim + 32);
-}
-
-static size_t bwd_smem(const SoapParams &P, size_t tsz)
-{
-    const int nlm = (P.l_max + 1) * (P.l_max + 1);
-    return tsz * ((size_t)2 * P.n_max * nlm + P.dim + 34) + sizeof(double) * 80;
-}
-
 static size_t der_smem(const SoapParams &P)
 {
     const int nlm = (P.l_max + 1) * (P.l_max + 1);
     return sizeof(double) * ((size_t)P.n_max * nlm + 4 * (size_t)nlm + 2 * kMaxAlpha + 40);
 }
 
+// Shared memory of one warp: 256 bytes of compacted pair indices, then the T arrays.
+static size_t fwd_warp_bytes(const SoapParams &P, size_t tsz)
+{
+    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+    const size_t area = std::max<size_t>(32 * nlm, (size_t)P.dim);
+    return 256 + (tsz * (32 * (size_t)P.n_max + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
+}
+
+static size_t bwd_warp_bytes(const SoapParams &P, size_t tsz)
+{
+    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+    return 256 + (tsz * (2 * (size_t)P.n_max * nlm + (size_t)P.dim) + 15) / 16 * 16;
+}
+
+constexpr size_t kMaxDynSmem = 227 * 1024;
+
+template <class T> static const T *tab(const DevBuf &d64, const DevBuf &d32)
+{
+    return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
+}
+
+template <class T, bool SPLIT, int L>
+static int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
+                        const int *d_sites, int n_rows, SoapOut &o)
+{
+    const size_t wb = fwd_warp_bytes(ds.p, sizeof(T)), sm = wb * kWarpsPerCta;
+    if (sm > kMaxDynSmem)
+        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", sm);
+    auto kern = k_soap_fwd_warp<T, L, SPLIT>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
+    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+        ds.p, tab<T>(ds.xq, ds.xq32), tab<T>(ds.tq, ds.tq32), tab<T>(ds.central, ds.central32), d_sites,
+        n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c, (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi,
+        o.q_lo, (int)wb, pv.check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+template <class T, class GT, int L>
+static int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
+                        const int *d_sites, int n_rows, const SoapOut &o, const void *d_g, int g_ld,
+                        double *d_forces, double *d_vir_rows)
+{
+    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T)), sm = wb * kWarpsPerCta;
+    if (sm > kMaxDynSmem)
+        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", sm);
+    auto kern = k_soap_bwd_warp<T, GT, L>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
+    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+        ds.p, tab<T>(ds.xq, ds.xq32), tab<T>(ds.tq, ds.tq32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz,
+        pv.species, pv.jatom, (const T *)o.c, (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g,
+        g_ld, d_forces, d_vir_rows, (int)wb, pv.n_atoms, pv.check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+#define TGAP_FOR_EACH_L(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+static_assert(kMaxL == 10, "TGAP_FOR_EACH_L lists l_max = 0..10");
+
 template <class T, bool SPLIT>
 static int launch_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
                           const int *d_sites, int n_rows, SoapOut &o)
 {
-    const size_t sm = fwd_smem(ds.p, sizeof(T));
-    auto kern = k_soap_forward<T, SPLIT>;
-    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const T *xq = std::is_same<T, double>::value ? (const T *)ds.xq.ptr : (const T *)ds.xq32.ptr;
-    const T *tq = std::is_same<T, double>::value ? (const T *)ds.tq.ptr : (const T *)ds.tq32.ptr;
-    const T *ce = std::is_same<T, double>::value ? (const T *)ds.central.ptr : (const T *)ds.central32.ptr;
-    kern<<<n_rows, kThreads, sm, ctx->stream>>>(ds.p, xq, tq, ce, d_sites, n_rows, pv.start, pv.rjs,
-                                                pv.xyz, pv.species, (T *)o.c, (T *)o.q, o.q_ld,
-                                                (T *)o.norm, o.q_hi, o.q_lo);
-    TGAP_LAUNCH_CHECK(ctx);
-    return TGAP_OK;
+    switch (ds.p.l_max) {
+#define TGAP_CASE(l) \
+    case l: return launch_fwd_l<T, SPLIT, l>(ctx, ds, pv, d_sites, n_rows, o);
+        TGAP_FOR_EACH_L(TGAP_CASE)
+#undef TGAP_CASE
+    }
+    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
+}
+
+template <class T, class GT>
+static int launch_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
+                           const int *d_sites, int n_rows, const SoapOut &o, const void *d_g, int g_ld,
+                           double *d_forces, double *d_vir_rows)
+{
+    switch (ds.p.l_max) {
+#define TGAP_CASE(l) \
+    case l: return launch_bwd_l<T, GT, l>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
+        TGAP_FOR_EACH_L(TGAP_CASE)
+#undef TGAP_CASE
+    }
+    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
 }
 
 int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
@@ -664,36 +452,24 @@ int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 
 int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
-                  int g_is_double, const int *site_struct, double *d_forces, double *d_virial)
+                  int g_is_double, const int *d_struct_off, int n_structures, double *d_vir_rows,
+                  double *d_forces, double *d_virial)
 {
     if (n_rows <= 0) return TGAP_OK;
-    StageScope sc(ctx, precision == TGAP_FP64 ? "soap_backward_f64" : "soap_backward_f32");
-    if (precision == TGAP_FP64) {
-        const size_t sm = bwd_smem(ds.p, sizeof(double));
-        auto kern = k_soap_backward<double, double>;
-        TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-        kern<<<n_rows, kThreads, sm, ctx->stream>>>(
-            ds.p, ds.xq.as<double>(), ds.tq.as<double>(), d_sites, n_rows, pv.start, pv.rjs, pv.xyz,
-            pv.species, pv.jatom, site_struct, (const double *)o.c, (const double *)o.q, o.q_ld,
-            (const double *)o.norm, (const double *)d_g, g_ld, d_forces, d_virial);
-    } else {
-        const size_t sm = bwd_smem(ds.p, sizeof(float));
-        if (g_is_double) {
-            auto kern = k_soap_backward<float, double>;
-            TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            kern<<<n_rows, kThreads, sm, ctx->stream>>>(
-                ds.p, ds.xq32.as<float>(), ds.tq32.as<float>(), d_sites, n_rows, pv.start, pv.rjs,
-                pv.xyz, pv.species, pv.jatom, site_struct, (const float *)o.c, (const float *)o.q,
-                o.q_ld, (const float *)o.norm, (const double *)d_g, g_ld, d_forces, d_virial);
-        } else {
-            auto kern = k_soap_backward<float, float>;
-            TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-            kern<<<n_rows, kThreads, sm, ctx->stream>>>(
-                ds.p, ds.xq32.as<float>(), ds.tq32.as<float>(), d_sites, n_rows, pv.start, pv.rjs,
-                pv.xyz, pv.species, pv.jatom, site_struct, (const float *)o.c, (const float *)o.q,
-                o.q_ld, (const float *)o.norm, (const float *)d_g, g_ld, d_forces, d_virial);
-        }
+    {
+        StageScope sc(ctx, precision == TGAP_FP64 ? "soap_backward_f64" : "soap_backward_f32");
+        int rc;
+        if (precision == TGAP_FP64)
+            rc = launch_backward<double, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
+        else if (g_is_double)
+            rc = launch_backward<float, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
+        else
+            rc = launch_backward<float, float>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
+        if (rc) return rc;
     }
+    StageScope sc(ctx, "virial_reduce");
+    const int nb = d_struct_off ? n_structures : 1;
+    k_virial_reduce<<<nb, 256, 0, ctx->stream>>>(n_rows, d_sites, d_struct_off, d_vir_rows, d_virial);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -22,7 +22,8 @@ int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  int n_rows, int precision, SoapOut &o);
 int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
-                  int g_is_double, const int *site_struct, double *d_forces, double *d_virial);
+                  int g_is_double, const int *d_struct_off, int n_structures, double *d_vir_rows,
+                  double *d_forces, double *d_virial);
 int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, const SoapOut &o, double *d_der);
 

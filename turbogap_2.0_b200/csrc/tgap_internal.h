@@ -66,6 +66,8 @@ struct tgap_context {
     tgap::DevBuf scratch[24];
     tgap::HostBuf pinned[4];
     int *d_flag = nullptr;  // device error flag (bounded waits, overflow)
+    int *d_check = nullptr; // device check word: code, index, value, failures (int[4])
+    bool sync_check = false;  // TGAP_SYNC_CHECK=1: synchronize and read the check after each launch
     // stage timing
     bool timing = false;
     std::vector<std::string> stage_names;
@@ -97,12 +99,47 @@ int cuda_check(tgap_context *ctx, cudaError_t e, const char *what);
         if (_e != cudaSuccess) return ::tgap::cuda_check(ctx, _e, #call); \
     } while (0)
 
+// Reads and clears the device check word; a recorded failure becomes TGAP_ERR_NUMERIC (code
+// kCheckNonFinite) or TGAP_ERR_CUDA (an index out of bounds). Synchronizes the context stream.
+int read_device_check(tgap_context *ctx);
+// With ctx->sync_check set and the stream not capturing: synchronize and read the check word.
+int sync_check_launch(tgap_context *ctx);
+
 #define TGAP_LAUNCH_CHECK(ctx)                                         \
     do {                                                               \
         (ctx)->launches++;                                             \
         cudaError_t _e = cudaGetLastError();                           \
         if (_e != cudaSuccess) return ::tgap::cuda_check(ctx, _e, "kernel launch"); \
+        if ((ctx)->sync_check) {                                       \
+            int _rc = ::tgap::sync_check_launch(ctx);                  \
+            if (_rc) return _rc;                                       \
+        }                                                              \
     } while (0)
+
+// Codes of the device check word.
+enum CheckCode {
+    kCheckNone = 0,
+    kCheckFwdPair = 1,      // descriptor forward: compacted pair outside its site
+    kCheckBwdPair = 2,      // adjoint: compacted pair outside its site
+    kCheckBwdAtom = 3,      // adjoint: neighbor atom index out of range
+    kCheckSelfAtom = 4,     // adjoint: self-slot atom index out of range
+    kCheckNonFinite = 5,    // velocity Verlet: non-finite force
+    kCheckListOverrun = 6,  // neighbor fill wrote past its counted range
+};
+
+#ifdef __CUDACC__
+// Records the first failure (code, index, value) and counts all of them; the access that failed
+// is skipped by the caller.
+__device__ __forceinline__ void check_fail(int *check, int code, long long index, long long value)
+{
+    if (!check) return;
+    if (atomicCAS(check, 0, code) == 0) {
+        check[1] = (int)index;
+        check[2] = (int)value;
+    }
+    atomicAdd(check + 3, 1);
+}
+#endif
 
 // ---------------------------------------------------------------------------- hypers
 
@@ -157,6 +194,8 @@ struct PairView {
     const double *rjs;      // [P]
     const int *species;     // [P]    species channel of the neighbor (1-based, 0 = blind)
     const int *jatom;       // [P]    folded global neighbor index (force scatter)
+    int n_atoms;            // bound of jatom
+    int *check;             // device check word
 };
 
 }  // namespace tgap
