@@ -26,6 +26,10 @@ SOURCES = [
     ("capi.cu", []),
     ("neighbors.cu", ["--fmad=false"]),
     ("soap.cu", []),
+    ("soap_fwd_f32.cu", []),
+    ("soap_fwd_f64.cu", []),
+    ("soap_bwd_f32.cu", []),
+    ("soap_bwd_f64.cu", []),
     ("gap.cu", []),
     ("gemm_tc.cu", []),
     ("md.cu", []),

@@ -467,6 +467,7 @@ static void release_soap(DeviceSoap *ds)
     ds->xq32.release();
     ds->tq32.release();
     ds->central32.release();
+    ds->rtab.release();
 }
 
 extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh, int n_species,
@@ -667,7 +668,7 @@ struct tgap_system {
     double rcut;
     std::vector<int> host_species;
     std::vector<SiteSet> site_sets;
-    DevBuf c, q, norm, q_hi, q_lo, e_rows, vir_rows;
+    DevBuf c, q, norm, q_hi, q_lo, e_rows;
     GapWork gw;
     DevBuf scratch_forces;
 };
@@ -747,7 +748,7 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
-                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->vir_rows};
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces};
     for (DevBuf *b : bufs) b->release();
     delete s;
     return TGAP_OK;
@@ -812,8 +813,6 @@ static int ensure_eval_buffers(tgap_system *s, const tgap_model *m, int n_rows, 
     const size_t tsz = precision == TGAP_FP64 ? 8 : 4;
     const int q_ld = precision == TGAP_FP64 ? P.dim : m->gap.dim_pad;
     const int rows_pad = (n_rows + 127) / 128 * 128;
-    if (s->vir_rows.ensure(sizeof(double) * 6 * (size_t)n_rows))
-        return set_error(s->ctx, TGAP_ERR_NOMEM, "virial rows");
     if (s->c.ensure(tsz * (size_t)n_rows * P.n_max * nlm) || s->q.ensure(tsz * (size_t)rows_pad * q_ld) ||
         s->norm.ensure(tsz * (size_t)n_rows))
         return set_error(s->ctx, TGAP_ERR_NOMEM, "descriptor workspace");
@@ -852,8 +851,7 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
                                      &s->gw, sites, nullptr, d_energies));
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o, s->gw.g.ptr, m->gap.dim,
-                                   1, s->nb.struct_off.as<int>(), s->nb.n_structures, s->vir_rows.as<double>(),
-                                   d_forces, d_virial));
+                                   1, s->nb.site_struct.as<int>(), d_forces, d_virial));
     } else {
         if (!m->mixed_ready) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "mixed path not prepared");
         o.q_ld = m->gap.dim_pad;
@@ -864,8 +862,7 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
                                        nullptr, d_energies));
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o, s->gw.g.ptr,
-                                   m->gap.dim_pad, 0, s->nb.struct_off.as<int>(), s->nb.n_structures,
-                                   s->vir_rows.as<double>(), d_forces, d_virial));
+                                   m->gap.dim_pad, 0, s->nb.site_struct.as<int>(), d_forces, d_virial));
     }
     return TGAP_OK;
 }
@@ -994,8 +991,7 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
     if (S[16].ensure(8 * (size_t)n_rows * Pp.n_max * nlm + 8) || S[17].ensure(8 * (size_t)rows_pad * q_ld + 8) ||
         S[18].ensure(8 * (size_t)n_rows + 8) || S[19].ensure(8 * (size_t)n_total_sites) ||
         S[20].ensure(8 * 3 * (size_t)n_total_sites) || S[21].ensure(8 * 9) ||
-        S[22].ensure(2 * (size_t)rows_pad * q_ld + 8) || S[23].ensure(2 * (size_t)rows_pad * q_ld + 8) ||
-        S[5].ensure(8 * 6 * (size_t)n_rows + 8))
+        S[22].ensure(2 * (size_t)rows_pad * q_ld + 8) || S[23].ensure(2 * (size_t)rows_pad * q_ld + 8))
         return set_error(ctx, TGAP_ERR_NOMEM, "get_gap_soap workspace");
     if (precision != TGAP_FP64) {
         TGAP_CUDA(ctx, cudaMemsetAsync(S[22].ptr, 0, 2 * (size_t)rows_pad * q_ld, ctx->stream));
@@ -1025,7 +1021,7 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
                                           S[9].as<int>(), nullptr, d_e);
         if (!rc && do_forces)
             rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_FP64, o, w.g.ptr, Pp.dim, 1,
-                               nullptr, 1, S[5].as<double>(), d_f, d_v);
+                               nullptr, d_f, d_v);
     } else {
         o.q_hi = S[22].as<__nv_bfloat16>();
         o.q_lo = S[23].as<__nv_bfloat16>();
@@ -1034,7 +1030,7 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
                                             S[9].as<int>(), nullptr, d_e);
         if (!rc && do_forces)
             rc = soap_backward(ctx, m->soap, pv, S[15].as<int>(), n_rows, TGAP_MIXED, o, w.g.ptr, m->gap.dim_pad,
-                               0, nullptr, 1, S[5].as<double>(), d_f, d_v);
+                               0, nullptr, d_f, d_v);
     }
     std::vector<double> he(n_total_sites), hf(3 * (size_t)n_total_sites);
     if (!rc) rc = download(ctx, he.data(), S[19], (size_t)n_total_sites);

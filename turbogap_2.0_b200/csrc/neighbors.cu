@@ -523,7 +523,6 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
         nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)sc_total) ||
         nb->species_sc.ensure(sizeof(int) * (size_t)sc_total) ||
         nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
-        nb->struct_off.ensure(sizeof(int) * (size_t)(nb->n_structures + 1)) ||
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
@@ -538,8 +537,6 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->species_sc.ptr, sp_sc.data(), sizeof(int) * sp_sc.size(),
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->site_struct.ptr, site_struct.data(), sizeof(int) * N,
-                                   cudaMemcpyHostToDevice, ctx->stream));
-    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->struct_off.ptr, offsets, sizeof(int) * (size_t)(n_structures + 1),
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions, sizeof(double) * 3 * N,
                                    cudaMemcpyHostToDevice, ctx->stream));
@@ -600,7 +597,6 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
         nb->pos_sc.ensure(sizeof(double) * 3 * (size_t)n_sc) ||
         nb->species_sc.ensure(sizeof(int) * (size_t)n_sc) ||
         nb->site_struct.ensure(sizeof(int) * N) || nb->atom_cell.ensure(sizeof(int) * N) ||
-        nb->struct_off.ensure(sizeof(int) * (size_t)(nb->n_structures + 1)) ||
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
@@ -618,8 +614,6 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
     else
         TGAP_CUDA(ctx, cudaMemsetAsync(nb->species_sc.ptr, 0, sizeof(int) * (size_t)n_sc, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(nb->site_struct.ptr, 0, sizeof(int) * N, ctx->stream));
-    const int so[2] = {0, n_sites};
-    TGAP_CUDA(ctx, cudaMemcpyAsync(nb->struct_off.ptr, so, sizeof(so), cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaMemcpyAsync(nb->positions.ptr, positions_sc, sizeof(double) * 3 * N,
                                    cudaMemcpyHostToDevice, ctx->stream));
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));

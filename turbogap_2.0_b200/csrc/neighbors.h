@@ -36,7 +36,6 @@ struct NeighborBatch {
     DevBuf pos_sc;          // double [3 n_sc_total]
     DevBuf species_sc;      // int [n_sc_total]
     DevBuf site_struct;     // int [n_atoms]
-    DevBuf struct_off;      // int [n_structures + 1] first global site of each structure
     DevBuf atom_cell, cell_count, cell_start, cell_cursor, cell_atoms;
     DevBuf counts;          // int64 [n_atoms + 1]
     DevBuf start;           // int64 [n_atoms + 1]
@@ -49,8 +48,7 @@ struct NeighborBatch {
     int ensure_pairs(int64_t P);
     void release_all()
     {
-        DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &struct_off,
-                          &atom_cell,
+        DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &atom_cell,
                           &cell_count, &cell_start, &cell_cursor, &cell_atoms, &counts, &start,
                           &n_neigh, &list, &rjs, &xyz, &thetas, &phis, &nspecies, &jatom,
                           &scan_tmp};

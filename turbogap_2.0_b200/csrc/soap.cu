@@ -27,20 +27,7 @@ constexpr int kPairsPerChunk = kThreads / kLanesPerPair;
 
 int upload_ylm_constants()
 {
-    YlmConst h;
-    double df = 1.0;
-    for (int m = 0; m <= kMaxL; ++m) {
-        if (m > 0) df *= (2.0 * m - 1.0);
-        h.dfact[m] = df;
-    }
-    for (int l = 0; l <= kMaxL; ++l) {
-        double fr = 1.0;
-        for (int m = 0; m <= l; ++m) {
-            if (m > 0) fr /= (double)(l + m) * (double)(l - m + 1);
-            double N = std::sqrt((2.0 * l + 1.0) / (4.0 * M_PI) * fr);
-            h.norm[l * (l + 1) / 2 + m] = m == 0 ? N : N * M_SQRT2;
-        }
-    }
+    const YlmConst &h = ylm_host_constants();
     return cudaMemcpyToSymbol(c_ylm, &h, sizeof(h)) == cudaSuccess ? 0 : 1;
 }
 
@@ -186,8 +173,6 @@ __device__ __forceinline__ int ps_index(int n, int np, int nmax, int L, int l)
     }
     return (n * nmax - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
 }
-
-#include "soap_warp.cuh"
 
 // ----------------------------------------------------------------------------- dq/dr
 
@@ -352,92 +337,26 @@ static size_t der_smem(const SoapParams &P)
     return sizeof(double) * ((size_t)P.n_max * nlm + 4 * (size_t)nlm + 2 * kMaxAlpha + 40);
 }
 
-// Shared memory of one warp: 256 bytes of compacted pair indices, then the T arrays.
-static size_t fwd_warp_bytes(const SoapParams &P, size_t tsz)
+const YlmConst &ylm_host_constants()
 {
-    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
-    const size_t area = std::max<size_t>(32 * nlm, (size_t)P.dim);
-    return 256 + (tsz * (32 * (size_t)P.n_max + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
-}
-
-static size_t bwd_warp_bytes(const SoapParams &P, size_t tsz)
-{
-    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
-    return 256 + (tsz * (2 * (size_t)P.n_max * nlm + (size_t)P.dim) + 15) / 16 * 16;
-}
-
-constexpr size_t kMaxDynSmem = 227 * 1024;
-
-template <class T> static const T *tab(const DevBuf &d64, const DevBuf &d32)
-{
-    return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
-}
-
-template <class T, bool SPLIT, int L>
-static int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
-                        const int *d_sites, int n_rows, SoapOut &o)
-{
-    const size_t wb = fwd_warp_bytes(ds.p, sizeof(T)), sm = wb * kWarpsPerCta;
-    if (sm > kMaxDynSmem)
-        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", sm);
-    auto kern = k_soap_fwd_warp<T, L, SPLIT>;
-    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
-    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
-        ds.p, tab<T>(ds.xq, ds.xq32), tab<T>(ds.tq, ds.tq32), tab<T>(ds.central, ds.central32), d_sites,
-        n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c, (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi,
-        o.q_lo, (int)wb, pv.check);
-    TGAP_LAUNCH_CHECK(ctx);
-    return TGAP_OK;
-}
-
-template <class T, class GT, int L>
-static int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
-                        const int *d_sites, int n_rows, const SoapOut &o, const void *d_g, int g_ld,
-                        double *d_forces, double *d_vir_rows)
-{
-    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T)), sm = wb * kWarpsPerCta;
-    if (sm > kMaxDynSmem)
-        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", sm);
-    auto kern = k_soap_bwd_warp<T, GT, L>;
-    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
-    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
-        ds.p, tab<T>(ds.xq, ds.xq32), tab<T>(ds.tq, ds.tq32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz,
-        pv.species, pv.jatom, (const T *)o.c, (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g,
-        g_ld, d_forces, d_vir_rows, (int)wb, pv.n_atoms, pv.check);
-    TGAP_LAUNCH_CHECK(ctx);
-    return TGAP_OK;
-}
-
-#define TGAP_FOR_EACH_L(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
-static_assert(kMaxL == 10, "TGAP_FOR_EACH_L lists l_max = 0..10");
-
-template <class T, bool SPLIT>
-static int launch_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
-                          const int *d_sites, int n_rows, SoapOut &o)
-{
-    switch (ds.p.l_max) {
-#define TGAP_CASE(l) \
-    case l: return launch_fwd_l<T, SPLIT, l>(ctx, ds, pv, d_sites, n_rows, o);
-        TGAP_FOR_EACH_L(TGAP_CASE)
-#undef TGAP_CASE
-    }
-    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
-}
-
-template <class T, class GT>
-static int launch_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv,
-                           const int *d_sites, int n_rows, const SoapOut &o, const void *d_g, int g_ld,
-                           double *d_forces, double *d_vir_rows)
-{
-    switch (ds.p.l_max) {
-#define TGAP_CASE(l) \
-    case l: return launch_bwd_l<T, GT, l>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
-        TGAP_FOR_EACH_L(TGAP_CASE)
-#undef TGAP_CASE
-    }
-    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
+    static const YlmConst h = [] {
+        YlmConst y;
+        double df = 1.0;
+        for (int m = 0; m <= kMaxL; ++m) {
+            if (m > 0) df *= (2.0 * m - 1.0);
+            y.dfact[m] = df;
+        }
+        for (int l = 0; l <= kMaxL; ++l) {
+            double fr = 1.0;
+            for (int m = 0; m <= l; ++m) {
+                if (m > 0) fr /= (double)(l + m) * (double)(l - m + 1);
+                const double N = std::sqrt((2.0 * l + 1.0) / (4.0 * M_PI) * fr);
+                y.norm[l * (l + 1) / 2 + m] = m == 0 ? N : N * M_SQRT2;
+            }
+        }
+        return y;
+    }();
+    return h;
 }
 
 int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
@@ -445,33 +364,44 @@ int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 {
     if (n_rows <= 0) return TGAP_OK;
     StageScope sc(ctx, precision == TGAP_FP64 ? "soap_forward_f64" : "soap_forward_f32");
-    if (precision == TGAP_FP64) return launch_forward<double, false>(ctx, ds, pv, d_sites, n_rows, o);
-    if (o.q_hi) return launch_forward<float, true>(ctx, ds, pv, d_sites, n_rows, o);
-    return launch_forward<float, false>(ctx, ds, pv, d_sites, n_rows, o);
+    if (precision == TGAP_FP64) return soap_fwd_f64(ctx, ds, pv, d_sites, n_rows, o);
+    return soap_fwd_f32(ctx, ds, pv, d_sites, n_rows, o);
 }
 
 int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
-                  int g_is_double, const int *d_struct_off, int n_structures, double *d_vir_rows,
-                  double *d_forces, double *d_virial)
+                  int g_is_double, const int *site_struct, double *d_forces, double *d_virial)
 {
     if (n_rows <= 0) return TGAP_OK;
-    {
-        StageScope sc(ctx, precision == TGAP_FP64 ? "soap_backward_f64" : "soap_backward_f32");
-        int rc;
-        if (precision == TGAP_FP64)
-            rc = launch_backward<double, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
-        else if (g_is_double)
-            rc = launch_backward<float, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
-        else
-            rc = launch_backward<float, float>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, d_forces, d_vir_rows);
-        if (rc) return rc;
+    StageScope sc(ctx, precision == TGAP_FP64 ? "soap_backward_f64" : "soap_backward_f32");
+    if (precision == TGAP_FP64)
+        return soap_bwd_f64(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+    return soap_bwd_f32(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, g_is_double, site_struct, d_forces, d_virial);
+}
+
+// Cubic Hermite coefficients of R_n on interval i of species s from FP64 quadrature values and
+// derivatives at both ends: R(t) = a + b t + c t^2 + d t^3, t in [0, 1], h = rcut_hard / kTabIntervals.
+__global__ void k_radial_table(const __grid_constant__ SoapParams P, const double *__restrict__ xq,
+                               const double *__restrict__ tq, float4 *__restrict__ tab)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= P.n_species * kTabIntervals) return;
+    const int s = g / kTabIntervals, i = g - s * kTabIntervals;
+    const double h = P.rcut_hard[s] / kTabIntervals;
+    double R0[kMaxAlpha], dR0[kMaxAlpha], R1[kMaxAlpha], dR1[kMaxAlpha];
+    radial_quad<double, kMaxAlpha, true>(P, s, i * h, xq, tq, R0, dR0);
+    radial_quad<double, kMaxAlpha, true>(P, s, (i + 1) * h, xq, tq, R1, dR1);
+    float4 *e = tab + (size_t)g * P.am_pad;
+    for (int n = 0; n < P.am_pad; ++n) {
+        float4 c = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (n < P.alpha_max[s]) {
+            const double a = R0[n], b = h * dR0[n];
+            const double cc = 3.0 * (R1[n] - R0[n]) - h * (2.0 * dR0[n] + dR1[n]);
+            const double d = 2.0 * (R0[n] - R1[n]) + h * (dR0[n] + dR1[n]);
+            c = make_float4((float)a, (float)b, (float)cc, (float)d);
+        }
+        e[n] = c;
     }
-    StageScope sc(ctx, "virial_reduce");
-    const int nb = d_struct_off ? n_structures : 1;
-    k_virial_reduce<<<nb, 256, 0, ctx->stream>>>(n_rows, d_sites, d_struct_off, d_vir_rows, d_virial);
-    TGAP_LAUNCH_CHECK(ctx);
-    return TGAP_OK;
 }
 
 int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
@@ -503,6 +433,14 @@ int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, Dev
     TGAP_CUDA(ctx, cudaMemcpy(d->xq32.ptr, xf.data(), nx * 4, cudaMemcpyHostToDevice));
     TGAP_CUDA(ctx, cudaMemcpy(d->tq32.ptr, tf.data(), nt * 4, cudaMemcpyHostToDevice));
     TGAP_CUDA(ctx, cudaMemcpy(d->central32.ptr, cf.data(), nc * 4, cudaMemcpyHostToDevice));
+    // radial table of the mixed path
+    const int n_int = p.n_species * kTabIntervals;
+    if (d->rtab.ensure(sizeof(float4) * (size_t)n_int * p.am_pad))
+        return set_error(ctx, TGAP_ERR_NOMEM, "radial table");
+    k_radial_table<<<(n_int + 127) / 128, 128, 0, ctx->stream>>>(p, d->xq.as<double>(), d->tq.as<double>(),
+                                                                 d->rtab.as<float4>());
+    TGAP_LAUNCH_CHECK(ctx);
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return TGAP_OK;
 }
 

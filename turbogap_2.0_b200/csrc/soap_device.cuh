@@ -23,6 +23,9 @@ struct YlmConst {
     double norm[(kMaxL + 1) * (kMaxL + 2) / 2];  // index l (l+1)/2 + m
 };
 
+// Host copy of the harmonic constants (computed once); passed to the warp kernels by value.
+const YlmConst &ylm_host_constants();
+
 template <class T> __device__ __forceinline__ T t_exp(T x);
 template <> __device__ __forceinline__ double t_exp<double>(double x) { return exp(x); }
 template <> __device__ __forceinline__ float t_exp<float>(float x) { return __expf(x); }
@@ -155,6 +158,52 @@ __device__ __forceinline__ void bessel_ratios(int L, T k, T *f)
 #pragma unroll
         for (int l = 1; l <= kMaxL + 1; ++l)
             if (l <= top) f[l] = f[l - 1] * ratio[l];
+    }
+}
+
+// Radial values (and d/dr) by quadrature: R_n = gs A(x) sum_q T[q][n] exp(-(x_q - x)^2 / 2 sig^2).
+template <class T, int AMB, bool DERIV>
+__device__ __forceinline__ void radial_quad(const SoapParams &P, int s, T r, const T *__restrict__ xq,
+                                            const T *__restrict__ tq, T R[AMB], T dR[AMB])
+{
+    const int am = P.alpha_max[s];
+    const T rc = (T)P.rcut_hard[s];
+    const T x = r / rc;
+    const T sig = ((T)P.sigma_r[s] + (T)P.sigma_r_scaling[s] * r) / rc;
+    const T dsig = (T)P.sigma_r_scaling[s];
+    T A, dA;
+    radial_amplitude<T>(P, s, x, sig, dsig, &A, &dA);
+    T sum[AMB], dsum[AMB];
+#pragma unroll
+    for (int n = 0; n < AMB; ++n) {
+        sum[n] = 0;
+        dsum[n] = 0;
+    }
+    const T inv2s2 = (T)1 / ((T)2 * sig * sig);
+    const T is2 = (T)1 / (sig * sig);
+    const T ds3 = dsig / (sig * sig * sig);
+    const T *xs = xq + P.node_off[s];
+    const T *ts = tq + P.tq_off[s];
+    const int nn = P.n_nodes[s];
+    for (int q = 0; q < nn; ++q) {
+        const T u = xs[q] - x;
+        const T G = t_exp<T>(-u * u * inv2s2);
+        const T *t = ts + q * am;
+        const T dG = DERIV ? G * (u * is2 + u * u * ds3) : (T)0;
+#pragma unroll
+        for (int n = 0; n < AMB; ++n) {
+            if (n < am) {
+                const T tv = t[n];
+                sum[n] += tv * G;
+                if (DERIV) dsum[n] += tv * dG;
+            }
+        }
+    }
+    const T gs = (T)P.global_scaling[s];
+#pragma unroll
+    for (int n = 0; n < AMB; ++n) {
+        R[n] = gs * A * sum[n];
+        dR[n] = DERIV ? gs * (dA * sum[n] + A * dsum[n]) / rc : (T)0;
     }
 }
 

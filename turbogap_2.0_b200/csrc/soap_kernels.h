@@ -22,8 +22,19 @@ int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  int n_rows, int precision, SoapOut &o);
 int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
-                  int g_is_double, const int *d_struct_off, int n_structures, double *d_vir_rows,
-                  double *d_forces, double *d_virial);
+                  int g_is_double, const int *site_struct, double *d_forces, double *d_virial);
+// Per-precision instantiations of the warp kernels (soap_fwd_f32.cu, soap_fwd_f64.cu,
+// soap_bwd_f32.cu, soap_bwd_f64.cu).
+int soap_fwd_f32(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 SoapOut &o);
+int soap_fwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 SoapOut &o);
+int soap_bwd_f32(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 const SoapOut &o, const void *d_g, int g_ld, int g_is_double, const int *site_struct,
+                 double *d_forces, double *d_virial);
+int soap_bwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
+                 double *d_virial);
 int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, const SoapOut &o, double *d_der);
 

@@ -1,14 +1,35 @@
-// Warp-per-site SOAP kernels (forward expansion + power spectrum, adjoint back-scatter).
-// Included by soap.cu inside namespace tgap (shares the harmonic constants in constant memory).
+// Warp-per-site SOAP kernels: forward expansion + power spectrum, and the adjoint that turns
+// dE/dq into forces and the virial. Instantiated by soap_fwd_*.cu / soap_bwd_*.cu.
 //
-// A warp owns one central site. The site's in-cutoff pairs are compacted with a ballot into
-// groups of at most 32; each lane then evaluates one pair completely (radial quadrature, Bessel
-// ratios, every real harmonic) with l_max fixed at compile time, so all harmonic indices and
-// per-l factors resolve to registers and every lane walks the same (l, m) sequence (shared-
-// memory reads of per-site data are broadcasts). Four warps share a CTA; nothing synchronizes
-// across warps. Pair and atom indices are bounds-checked: a failed check is recorded in the
-// device check word and the access is skipped.
+// A warp owns one central site; its in-cutoff pairs are compacted with a ballot into groups of
+// at most 32 and each lane evaluates one pair completely (radial values, Bessel ratios, every
+// real harmonic) with l_max (L) and the radial block bound (AMB >= alpha_max of every species)
+// fixed at compile time, so harmonic indices, per-l factors and radial arrays live in registers.
+//
+//  forward   c[s-block][n][lm] = sum_{pairs j of species s} R_n(r_j) f_l(r_j) Y_lm(u_j)
+//            One pass per species: the group's radial rows (AMB wide) and angular rows go to
+//            shared memory and every lane accumulates the product for its own harmonics
+//            lm = lane + 32 i over all n in registers. Then the power spectrum
+//            p[n n' l] = (sqrt 2 if n != n') sum_m c[n][lm] c[n'][lm] and q = p / |p|.
+//  adjoint   h = (g - q (q.g)) / |p|, Gc = dE/dc = M_l c (M from h), stored harmonic-major with
+//            each species block padded to 4 so a lane reads its radial weights with 16-byte
+//            loads; per pair w = sum_lm [R'.G f Y u + R.G (df Y u + f (grad Y)_perp / r)],
+//            force -w on the neighbor and +w on the site, virial sum of r (x) f.
+//
+// FP32 instantiations (mixed path) take the radial values from a cubic Hermite table of R_n
+// and dR_n/dr over kTabIntervals uniform intervals of [0, rcut_hard] (built in FP64 from the
+// quadrature); FP64 instantiations run the Gauss-Legendre quadrature itself.
 #pragma once
+
+#include <cuda_bf16.h>
+
+#include <algorithm>
+#include <type_traits>
+
+#include "soap_device.cuh"
+#include "soap_kernels.h"
+
+namespace tgap {
 
 constexpr int kWarpsPerCta = 4;
 
@@ -19,7 +40,32 @@ __device__ __forceinline__ unsigned lanemask_lt()
     return m;
 }
 
-// f_l = i_l(k)/i_0(k), l = 0..L+1, same rule as bessel_ratios, unrolled for a fixed L.
+// Decode power-spectrum index d -> (n, n', l) with n <= n' (component order n, n', l).
+__device__ __forceinline__ void ps_decode_w(int d, int nmax, int L, int *n, int *np, int *l)
+{
+    int pidx = d / (L + 1);
+    *l = d - pidx * (L + 1);
+    int a = 0;
+    while (pidx >= nmax - a) {
+        pidx -= nmax - a;
+        ++a;
+    }
+    *n = a;
+    *np = a + pidx;
+}
+
+__device__ __forceinline__ int ps_index_w(int n, int np, int nmax, int L, int l)
+{
+    if (n > np) {
+        const int t = n;
+        n = np;
+        np = t;
+    }
+    return (n * nmax - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
+}
+
+// f_l = i_l(k)/i_0(k), l = 0..L+1: upward recurrence when k > L+2, else the continued fraction
+// started at l = L+33 (same rule as the reference restatement).
 template <class T, int L>
 __device__ __forceinline__ void bessel_ratios_fixed(T k, T f[L + 2])
 {
@@ -31,8 +77,14 @@ __device__ __forceinline__ void bessel_ratios_fixed(T k, T f[L + 2])
     if (k > (T)(L + 2)) {
         f[0] = 1;
         f[1] = t_tanh_inv<T>(k) - (T)1 / k;
+        if (std::is_same<T, float>::value) {
+            const T ik = (T)1 / k;
 #pragma unroll
-        for (int l = 1; l <= L; ++l) f[l + 1] = f[l - 1] - (T)(2 * l + 1) / k * f[l];
+            for (int l = 1; l <= L; ++l) f[l + 1] = f[l - 1] - (T)(2 * l + 1) * ik * f[l];
+        } else {
+#pragma unroll
+            for (int l = 1; l <= L; ++l) f[l + 1] = f[l - 1] - (T)(2 * l + 1) / k * f[l];
+        }
     } else {
         T rho = 0;
         for (int l = L + 1 + 32; l > L + 1; --l) rho = k / ((T)(2 * l + 1) + k * rho);
@@ -48,9 +100,10 @@ __device__ __forceinline__ void bessel_ratios_fixed(T k, T f[L + 2])
     }
 }
 
-// Every real harmonic of u for a fixed L: fn(k, l, Y, dY/dux, dY/duy, dY/duz), k = l^2 + ...
+// Every real harmonic of the unit vector u for a fixed L: fn(k, l, Y, dY/dux, dY/duy, dY/duz)
+// with k = l^2 + {0 | 2m-1 (cos) | 2m (sin)}; the gradient treats the components as independent.
 template <class T, int L, bool GRAD, class F>
-__device__ __forceinline__ void ylm_all(T ux, T uy, T uz, F &&fn)
+__device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F &&fn)
 {
     T Cc = 1, Sc = 0, Cp = 0, Sp = 0;
 #pragma unroll
@@ -64,7 +117,7 @@ __device__ __forceinline__ void ylm_all(T ux, T uy, T uz, F &&fn)
             Sc = sn;
         }
         T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
-        const T qmm = (T)c_ylm.dfact[m];
+        const T qmm = (T)Yc.dfact[m];
 #pragma unroll
         for (int l = m; l <= L; ++l) {
             T Q, dQ;
@@ -83,7 +136,7 @@ __device__ __forceinline__ void ylm_all(T ux, T uy, T uz, F &&fn)
             Q1 = Q;
             dQ2 = dQ1;
             dQ1 = dQ;
-            const T N = (T)c_ylm.norm[l * (l + 1) / 2 + m];
+            const T N = (T)Yc.norm[l * (l + 1) / 2 + m];
             if (m == 0) {
                 fn(l * l, l, N * Q, (T)0, (T)0, GRAD ? N * dQ : (T)0);
             } else {
@@ -101,33 +154,34 @@ __device__ __forceinline__ void ylm_all(T ux, T uy, T uz, F &&fn)
     }
 }
 
-// Pair acceptance used by the compaction: species channel known and 0 < r < rcut_hard(s).
-__device__ __forceinline__ bool pair_in_cutoff(const SoapParams &P, int64_t k, const double *__restrict__ rjs,
-                                               const int *__restrict__ nsp)
+// Pair acceptance: species channel known (and equal to only_s when only_s >= 0) and
+// 0 < r < rcut_hard(s).
+__device__ __forceinline__ bool pair_accept(const SoapParams &P, int64_t k, const double *__restrict__ rjs,
+                                            const int *__restrict__ nsp, int only_s)
 {
     const int s = nsp[k] - 1;
-    if (s < 0 || s >= P.n_species) return false;
+    if (s < 0 || s >= P.n_species || (only_s >= 0 && s != only_s)) return false;
     const double r = rjs[k];
     return r > 0.0 && r < P.rcut_hard[s];
 }
 
-// Compacts the next (at most 32) in-cutoff pairs of [scan, ke) into idx[]; returns the count
-// and advances scan past the last pair taken.
+// Compacts the next (at most 32) accepted pairs of [scan, ke) into idx[]; returns the count and
+// advances scan past the last pair taken.
 __device__ __forceinline__ int compact_pairs(const SoapParams &P, int64_t &scan, int64_t ke,
                                              const double *__restrict__ rjs, const int *__restrict__ nsp,
-                                             long long *idx, int lane)
+                                             int only_s, long long *idx, int lane)
 {
     int cnt = 0;
     while (cnt < 32 && scan < ke) {
         const int64_t k = scan + lane;
-        const bool ok = k < ke && pair_in_cutoff(P, k, rjs, nsp);
+        const bool ok = k < ke && pair_accept(P, k, rjs, nsp, only_s);
         const unsigned mask = __ballot_sync(0xffffffffu, ok);
         const int nv = __popc(mask);
         const int room = 32 - cnt;
         const int rank = __popc(mask & lanemask_lt());
         if (ok && rank < room) idx[cnt + rank] = (long long)k;
         if (nv > room) {
-            // resume at the first in-cutoff pair that did not fit
+            // resume at the first accepted pair that did not fit
             scan += __fns(mask, 0, room + 1);
             cnt = 32;
             break;
@@ -139,127 +193,174 @@ __device__ __forceinline__ int compact_pairs(const SoapParams &P, int64_t &scan,
     return cnt;
 }
 
-// Radial coefficients (and optionally d/dr) of one pair evaluated by one lane.
-template <class T, bool DERIV>
-__device__ __forceinline__ void radial_lane(const SoapParams &P, int s, T r, const T *__restrict__ xq,
-                                            const T *__restrict__ tq, T R[kMaxAlpha], T dR[kMaxAlpha])
+// Radial values (and d/dr) from the cubic Hermite table: entry (s, i, n) holds the coefficients
+// (a, b, c, d) of R_n on interval i in t = r/h - i; dR/dr = (b + 2ct + 3dt^2) / h.
+template <int AMB, bool DERIV>
+__device__ __forceinline__ void radial_tab(const SoapParams &P, int s, double r, const float4 *__restrict__ tab,
+                                           float R[AMB], float dR[AMB])
 {
     const int am = P.alpha_max[s];
-    const T rc = (T)P.rcut_hard[s];
-    const T x = r / rc;
-    const T sig = ((T)P.sigma_r[s] + (T)P.sigma_r_scaling[s] * r) / rc;
-    const T dsig = (T)P.sigma_r_scaling[s];
-    T A, dA;
-    radial_amplitude<T>(P, s, x, sig, dsig, &A, &dA);
-    T sum[kMaxAlpha], dsum[kMaxAlpha];
+    const double xr = r * P.tab_scale[s];
+    int i = (int)xr;
+    i = i < 0 ? 0 : (i > kTabIntervals - 1 ? kTabIntervals - 1 : i);
+    const float t = (float)(xr - (double)i);
+    const float ih = (float)P.tab_scale[s];
+    const float4 *e = tab + ((size_t)s * kTabIntervals + i) * P.am_pad;
 #pragma unroll
-    for (int n = 0; n < kMaxAlpha; ++n) {
-        sum[n] = 0;
-        dsum[n] = 0;
-    }
-    const T inv2s2 = (T)1 / ((T)2 * sig * sig);
-    const T is2 = (T)2 * inv2s2;
-    const T ds3 = dsig * is2 / sig;
-    const T *xs = xq + P.node_off[s];
-    const T *ts = tq + P.tq_off[s];
-    const int nn = P.n_nodes[s];
-    for (int q = 0; q < nn; ++q) {
-        const T u = xs[q] - x;
-        const T G = t_exp<T>(-u * u * inv2s2);
-        const T *t = ts + q * am;
-        const T dG = DERIV ? G * (u * is2 + u * u * ds3) : (T)0;
-#pragma unroll
-        for (int n = 0; n < kMaxAlpha; ++n) {
-            if (n < am) {
-                sum[n] += t[n] * G;
-                if (DERIV) dsum[n] += t[n] * dG;
-            }
+    for (int n = 0; n < AMB; ++n) {
+        if (n < am) {
+            const float4 c = __ldg(e + n);
+            R[n] = c.x + t * (c.y + t * (c.z + t * c.w));
+            dR[n] = DERIV ? (c.y + t * (2.0f * c.z + 3.0f * t * c.w)) * ih : 0.0f;
+        } else {
+            R[n] = 0.0f;
+            dR[n] = 0.0f;
         }
-    }
-    const T gs = (T)P.global_scaling[s];
-#pragma unroll
-    for (int n = 0; n < kMaxAlpha; ++n) {
-        R[n] = gs * A * sum[n];
-        if (DERIV) dR[n] = gs * (dA * sum[n] + A * dsum[n]) / rc;
     }
 }
 
+template <class T, int AMB, bool DERIV>
+__device__ __forceinline__ void radial_values(const SoapParams &P, int s, double rd, const T *__restrict__ xq,
+                                              const T *__restrict__ tq, const float4 *__restrict__ tab,
+                                              T R[AMB], T dR[AMB])
+{
+    if constexpr (std::is_same<T, float>::value)
+        radial_tab<AMB, DERIV>(P, s, rd, tab, R, dR);
+    else
+        radial_quad<T, AMB, DERIV>(P, s, (T)rd, xq, tq, R, dR);
+}
+
+// 16-byte loads of N consecutive values (N a multiple of 16 / sizeof(T), p 16-byte aligned).
+template <class T, int N>
+__device__ __forceinline__ void load_vec(const T *__restrict__ p, T v[N])
+{
+    if constexpr (std::is_same<T, float>::value) {
+        static_assert(N % 4 == 0, "float rows are loaded 4 at a time");
+#pragma unroll
+        for (int i = 0; i < N / 4; ++i) {
+            const float4 x = reinterpret_cast<const float4 *>(p)[i];
+            v[4 * i] = x.x;
+            v[4 * i + 1] = x.y;
+            v[4 * i + 2] = x.z;
+            v[4 * i + 3] = x.w;
+        }
+    } else {
+        static_assert(N % 2 == 0, "double rows are loaded 2 at a time");
+#pragma unroll
+        for (int i = 0; i < N / 2; ++i) {
+            const double2 x = reinterpret_cast<const double2 *>(p)[i];
+            v[2 * i] = x.x;
+            v[2 * i + 1] = x.y;
+        }
+    }
+}
+
+// Row stride of the angular rows in shared memory: odd, so the 32 lanes writing their own pair's
+// row hit 32 different banks.
+template <int NLM> struct AStride {
+    static constexpr int value = (NLM % 2 == 0) ? NLM + 1 : NLM;
+};
+
 // ----------------------------------------------------------------------------- forward
 
-template <class T, int L, bool SPLIT>
+// Shared memory of one warp: 256 bytes of pair indices, Rs [32][AMB], then an area holding the
+// angular rows [32][ASTR] during the passes and the power spectrum [dim] after them, then the
+// expansion c [n_max][NLM].
+template <class T, int L, int AMB, bool SPLIT>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
-    SoapParams P, const T *__restrict__ xq, const T *__restrict__ tq, const T *__restrict__ central,
+    const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
+    const T *__restrict__ tq, const float4 *__restrict__ rtab, const T *__restrict__ central,
     const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
     const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
     T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
     __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check)
 {
     constexpr int NLM = (L + 1) * (L + 1);
+    constexpr int ASTR = AStride<NLM>::value;
+    constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = blockIdx.x * kWarpsPerCta + warp;
-    if (row >= n_rows) return;
+    if (row >= n_rows) return;  // no CTA-wide synchronisation in this kernel
     unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
     const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
-    long long *idx = reinterpret_cast<long long *>(wbase);  // [32] compacted pair indices
-    T *Rs = reinterpret_cast<T *>(wbase + 256);             // [32][nmax]
-    T *As = Rs + 32 * nmax;                                 // [32][NLM]   (reused for p)
-    T *cs = As + (32 * NLM > dim ? 32 * NLM : dim);         // [nmax][NLM]
+    long long *idx = reinterpret_cast<long long *>(wbase);
+    T *Rs = reinterpret_cast<T *>(wbase + 256);
+    T *As = Rs + 32 * AMB;
+    T *cs = As + (32 * ASTR > dim ? 32 * ASTR : dim);
 
     const int site = sites ? sites[row] : row;
     const int64_t kb = start[site], ke = start[site + 1];
-    int64_t scan = kb + 1;
-    bool first = true;
-    do {
-        const int cnt = compact_pairs(P, scan, ke, rjs, nsp, idx, lane);
-        if (cnt == 0 && !first) break;
-        if (lane < cnt) {
-            const int64_t k = idx[lane];
-            const bool in_site = k > kb && k < ke;
-            if (!in_site) check_fail(check, kCheckFwdPair, k, site);
-            const int s = in_site ? nsp[k] - 1 : 0;
-            const T r = in_site ? (T)rjs[k] : (T)1;
-            const T ir = (T)1 / r;
-            const T ux = in_site ? (T)xyz[3 * k] * ir : (T)0, uy = in_site ? (T)xyz[3 * k + 1] * ir : (T)0,
-                    uz = in_site ? (T)xyz[3 * k + 2] * ir : (T)1;
-            T R[kMaxAlpha], dR[kMaxAlpha];
-            radial_lane<T, false>(P, s, r, xq, tq, R, dR);
-            T *Rrow = Rs + lane * nmax;
-            for (int n = 0; n < nmax; ++n) Rrow[n] = 0;
-            const int off = P.n_off[s], am = P.alpha_max[s];
+    for (int s = 0; s < P.n_species; ++s) {
+        T acc[KPL][AMB];
 #pragma unroll
-            for (int n = 0; n < kMaxAlpha; ++n)
-                if (n < am && in_site) Rrow[off + n] = R[n];
-            const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
-            T f[L + 2];
-            bessel_ratios_fixed<T, L>(r * r / (st * st), f);
-            T *Arow = As + lane * NLM;
-            ylm_all<T, L, false>(ux, uy, uz, [&](int kk, int l, T Y, T, T, T) { Arow[kk] = f[l] * Y; });
+        for (int j = 0; j < KPL; ++j)
+#pragma unroll
+            for (int n = 0; n < AMB; ++n) acc[j][n] = 0;
+        int64_t scan = kb + 1;
+        while (scan < ke) {
+            const int cnt = compact_pairs(P, scan, ke, rjs, nsp, s, idx, lane);
+            if (cnt == 0) break;
+            if (lane < cnt) {
+                const int64_t k = idx[lane];
+                const bool in_site = k > kb && k < ke;
+                if (!in_site) check_fail(check, kCheckFwdPair, k, site);
+                const double rd = in_site ? rjs[k] : 1.0;
+                const T r = (T)rd, ir = (T)1 / r;
+                const T ux = in_site ? (T)xyz[3 * k] * ir : (T)0;
+                const T uy = in_site ? (T)xyz[3 * k + 1] * ir : (T)0;
+                const T uz = in_site ? (T)xyz[3 * k + 2] * ir : (T)1;
+                T R[AMB], dR[AMB];
+                radial_values<T, AMB, false>(P, s, rd, xq, tq, rtab, R, dR);
+                T *Rrow = Rs + lane * AMB;
+#pragma unroll
+                for (int n = 0; n < AMB; ++n) Rrow[n] = in_site ? R[n] : (T)0;
+                const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
+                T f[L + 2];
+                bessel_ratios_fixed<T, L>(r * r / (st * st), f);
+                T *Arow = As + lane * ASTR;
+                ylm_all<T, L, false>(Yc, ux, uy, uz, [&](int kk, int l, T y, T, T, T) { Arow[kk] = f[l] * y; });
+            }
+            __syncwarp();
+            for (int p = 0; p < cnt; ++p) {
+                T rv[AMB];
+                load_vec<T, AMB>(Rs + p * AMB, rv);
+#pragma unroll
+                for (int j = 0; j < KPL; ++j) {
+                    const int kk = lane + 32 * j;
+                    if (kk < NLM) {
+                        const T a = As[p * ASTR + kk];
+#pragma unroll
+                        for (int n = 0; n < AMB; ++n) acc[j][n] += rv[n] * a;
+                    }
+                }
+            }
+            __syncwarp();
         }
-        __syncwarp();
-        for (int o = lane; o < nout; o += 32) {
-            const int n = o / NLM, kk = o - n * NLM;
-            T acc = first ? (T)0 : cs[o];
-            for (int p = 0; p < cnt; ++p) acc += Rs[p * nmax + n] * As[p * NLM + kk];
-            cs[o] = acc;
+        const int off = P.n_off[s], am = P.alpha_max[s];
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+            const int kk = lane + 32 * j;
+            if (kk < NLM) {
+#pragma unroll
+                for (int n = 0; n < AMB; ++n)
+                    if (n < am) cs[(off + n) * NLM + kk] = acc[j][n];
+            }
         }
-        __syncwarp();
-        first = false;
-    } while (scan < ke);
-
+    }
+    __syncwarp();
     // central atom on l = 0 of its own species block
     const int s_self = nsp[kb] - 1;
-    if (s_self >= 0 && s_self < P.n_species)
-        for (int n = lane; n < P.alpha_max[s_self]; n += 32)
-            cs[(P.n_off[s_self] + n) * NLM] += central[P.n_off[s_self] + n];
+    if (s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self])
+        cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
     __syncwarp();
     for (int o = lane; o < nout; o += 32) c_out[(size_t)row * nout + o] = cs[o];
-    // power spectrum into the (free) A area
+    // power spectrum into the (now free) angular area
     T *ps = As;
     T part = 0;
     for (int d = lane; d < dim; d += 32) {
         int n, np, l;
-        ps_decode(d, nmax, L, &n, &np, &l);
+        ps_decode_w(d, nmax, L, &n, &np, &l);
         const T *a = cs + n * NLM, *b = cs + np * NLM;
         T acc = 0;
         for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
@@ -287,185 +388,304 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
 
 // ----------------------------------------------------------------------------- adjoint
 
-// g = dE/dq per row. Pair forces go to forces[3 * jatom] with FP64 atomics, the site's own
-// force (minus the sum) to forces[3 * jatom[self]], and the row's virial (xx yy zz xy xz yz)
-// to vir_rows[6 * row] for a later per-structure reduction.
-template <class T, class GT, int L>
+// Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (rounded up to 4),
+// GcT [NLM][n_maxp] (species blocks at the padded offsets offp, padding zero), h [dim]; after
+// the warps, the CTA's virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
+template <class T, class GT, int L, int AMB>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
-    SoapParams P, const T *__restrict__ xq, const T *__restrict__ tq, const int *__restrict__ sites,
-    int n_rows, const int64_t *__restrict__ start, const double *__restrict__ rjs,
-    const double *__restrict__ xyz, const int *__restrict__ nsp, const int *__restrict__ jatom,
+    const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
+    const T *__restrict__ tq, const float4 *__restrict__ rtab, const int *__restrict__ sites, int n_rows,
+    const int64_t *__restrict__ start, const double *__restrict__ rjs, const double *__restrict__ xyz,
+    const int *__restrict__ nsp, const int *__restrict__ jatom, const int *__restrict__ site_struct,
     const T *__restrict__ c_in, const T *__restrict__ q_in, int q_ld, const T *__restrict__ norm_in,
-    const GT *__restrict__ g_in, int g_ld, double *__restrict__ forces, double *__restrict__ vir_rows,
+    const GT *__restrict__ g_in, int g_ld, double *__restrict__ forces, double *__restrict__ virial,
     int warp_smem, int n_atoms, int *check)
 {
     constexpr int NLM = (L + 1) * (L + 1);
+    constexpr int VW = std::is_same<T, float>::value ? 4 : 2;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int row = blockIdx.x * kWarpsPerCta + warp;
-    if (row >= n_rows) return;
-    unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
-    const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
-    long long *idx = reinterpret_cast<long long *>(wbase);  // [32] compacted pair indices
-    T *cs = reinterpret_cast<T *>(wbase + 256);             // [nmax][NLM]
-    T *Gc = cs + nout;                                      // [nmax][NLM]
-    T *hs = Gc + nout;                                      // [dim]
+    const bool active = row < n_rows;
+    double *vpart = reinterpret_cast<double *>(smem_raw + (size_t)kWarpsPerCta * warp_smem);
+    int *vstruct = reinterpret_cast<int *>(vpart + 6 * kWarpsPerCta);
+    double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+    int my_struct = -1;
+    if (active) {
+        unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
+        const int nmax = P.n_max, nmaxp = P.n_maxp, dim = P.dim, nout = nmax * NLM;
+        long long *idx = reinterpret_cast<long long *>(wbase);
+        T *cs = reinterpret_cast<T *>(wbase + 256);
+        T *GcT = cs + (nout + 3) / 4 * 4;
+        T *hs = GcT + NLM * nmaxp;
 
-    const int site = sites ? sites[row] : row;
-    const int64_t kb = start[site], ke = start[site + 1];
-    for (int o = lane; o < nout; o += 32) cs[o] = c_in[(size_t)row * nout + o];
-    T qg = 0;
-    for (int d = lane; d < dim; d += 32) qg += q_in[(size_t)row * q_ld + d] * (T)g_in[(size_t)row * g_ld + d];
+        const int site = sites ? sites[row] : row;
+        my_struct = site_struct ? site_struct[site] : 0;
+        const int64_t kb = start[site], ke = start[site + 1];
+        for (int o = lane; o < nout; o += 32) cs[o] = c_in[(size_t)row * nout + o];
+        for (int o = lane; o < NLM * nmaxp; o += 32) GcT[o] = 0;
+        T qg = 0;
+        for (int d = lane; d < dim; d += 32) qg += q_in[(size_t)row * q_ld + d] * (T)g_in[(size_t)row * g_ld + d];
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
-    const T nrm = norm_in[row];
-    const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-    for (int d = lane; d < dim; d += 32)
-        hs[d] = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
-    __syncwarp();
-    // dE/dc_{n,lm} = sum_n' M_l[n][n'] c_{n',lm}
-    for (int o = lane; o < nout; o += 32) {
-        const int n = o / NLM, kk = o - n * NLM;
-        int l = 0;
-        while ((l + 1) * (l + 1) <= kk) ++l;
-        T acc = 0;
-        for (int np = 0; np < nmax; ++np) {
-            const T h = hs[ps_index(n, np, nmax, L, l)];
-            acc += ((np == n) ? (T)2 * h : (T)1.4142135623730951 * h) * cs[np * NLM + kk];
-        }
-        Gc[o] = acc;
-    }
-    __syncwarp();
-
-    double fs0 = 0, fs1 = 0, fs2 = 0, v0 = 0, v1 = 0, v2 = 0, v3 = 0, v4 = 0, v5 = 0;
-    int64_t scan = kb + 1;
-    while (scan < ke) {
-        const int cnt = compact_pairs(P, scan, ke, rjs, nsp, idx, lane);
-        if (cnt == 0) break;
-        const bool mine = lane < cnt;
-        const int64_t k = mine ? idx[lane] : kb;
-        const bool in_site = k > kb && k < ke;
-        if (mine && !in_site) check_fail(check, kCheckBwdPair, k, site);
-        if (mine && in_site) {
-            const int s = nsp[k] - 1;
-            const double xd0 = xyz[3 * k], xd1 = xyz[3 * k + 1], xd2 = xyz[3 * k + 2];
-            const T r = (T)rjs[k];
-            const T ir = (T)1 / r;
-            const T u0 = (T)xd0 * ir, u1 = (T)xd1 * ir, u2 = (T)xd2 * ir;
-            T R[kMaxAlpha], dR[kMaxAlpha];
-            radial_lane<T, true>(P, s, r, xq, tq, R, dR);
-            const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
-            const T kap = r * r / (st * st);
-            const T dkap = (T)2 * r / (st * st) - (T)2 * r * r * (T)P.sigma_t_scaling[s] / (st * st * st);
-            T f[L + 2];
-            bessel_ratios_fixed<T, L>(kap, f);
-            const T ikap = kap > (T)0 ? (T)1 / kap : (T)0;
-            const int off = P.n_off[s], am = P.alpha_max[s];
-            const T *G = Gc + off * NLM;
-            T w0 = 0, w1 = 0, w2 = 0;
-            ylm_all<T, L, true>(u0, u1, u2, [&](int kk, int l, T Y, T gx, T gy, T gz) {
-                T U = 0, V = 0;
-#pragma unroll
-                for (int n = 0; n < kMaxAlpha; ++n) {
-                    if (n < am) {
-                        const T gv = G[n * NLM + kk];
-                        U += gv * R[n];
-                        V += gv * dR[n];
-                    }
-                }
-                const T fl = f[l];
-                const T dfl = (f[l + 1] + (T)l * ikap * fl - fl * f[1]) * dkap;
-                const T ug = u0 * gx + u1 * gy + u2 * gz;
-                const T radial_part = fl * Y * V + U * dfl * Y;
-                const T tang = U * fl * ir;
-                w0 += u0 * radial_part + tang * (gx - u0 * ug);
-                w1 += u1 * radial_part + tang * (gy - u1 * ug);
-                w2 += u2 * radial_part + tang * (gz - u2 * ug);
-            });
-            // w = dE_i/dr_ij: force -w on the neighbor, +w on the site (its self slot)
-            const double f0 = -(double)w0, f1 = -(double)w1, f2 = -(double)w2;
-            const int j = jatom[k];
-            if (j >= 0 && j < n_atoms) {
-                atomicAdd(forces + 3 * (size_t)j, f0);
-                atomicAdd(forces + 3 * (size_t)j + 1, f1);
-                atomicAdd(forces + 3 * (size_t)j + 2, f2);
-            } else {
-                check_fail(check, kCheckBwdAtom, k, j);
+        for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
+        const T nrm = norm_in[row];
+        const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
+        for (int d = lane; d < dim; d += 32)
+            hs[d] = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
+        __syncwarp();
+        // Gc[n][lm] = sum_n' (2 h[n n' l] if n == n' else sqrt2 h[n n' l]) c[n'][lm]
+        for (int o = lane; o < nout; o += 32) {
+            const int kk = o / nmax, n = o - kk * nmax;
+            int l = 0;
+            while ((l + 1) * (l + 1) <= kk) ++l;
+            T acc = 0;
+            for (int np = 0; np < nmax; ++np) {
+                const T h = hs[ps_index_w(n, np, nmax, L, l)];
+                acc += ((np == n) ? (T)2 * h : (T)1.4142135623730951 * h) * cs[np * NLM + kk];
             }
-            fs0 -= f0;
-            fs1 -= f1;
-            fs2 -= f2;
-            v0 += f0 * xd0;
-            v1 += f1 * xd1;
-            v2 += f2 * xd2;
-            v3 += 0.5 * (f0 * xd1 + f1 * xd0);
-            v4 += 0.5 * (f0 * xd2 + f2 * xd0);
-            v5 += 0.5 * (f1 * xd2 + f2 * xd1);
+            int s = 0;
+            while (s + 1 < P.n_species && n >= P.n_off[s + 1]) ++s;
+            GcT[kk * nmaxp + P.offp[s] + (n - P.n_off[s])] = acc;
         }
         __syncwarp();
-    }
-    double vals[9] = {fs0, fs1, fs2, v0, v1, v2, v3, v4, v5};
+
+        int64_t scan = kb + 1;
+        while (scan < ke) {
+            const int cnt = compact_pairs(P, scan, ke, rjs, nsp, -1, idx, lane);
+            if (cnt == 0) break;
+            const bool mine = lane < cnt;
+            const int64_t k = mine ? idx[lane] : kb;
+            const bool in_site = k > kb && k < ke;
+            if (mine && !in_site) check_fail(check, kCheckBwdPair, k, site);
+            if (mine && in_site) {
+                const int s = nsp[k] - 1;
+                const double xd0 = xyz[3 * k], xd1 = xyz[3 * k + 1], xd2 = xyz[3 * k + 2];
+                const double rd = rjs[k];
+                const T r = (T)rd;
+                const T ir = (T)1 / r;
+                const T u0 = (T)xd0 * ir, u1 = (T)xd1 * ir, u2 = (T)xd2 * ir;
+                T R[AMB], dR[AMB];
+                radial_values<T, AMB, true>(P, s, rd, xq, tq, rtab, R, dR);
+                const T sts = (T)P.sigma_t_scaling[s];
+                const T st = (T)P.sigma_t[s] + sts * r;
+                const T kap = r * r / (st * st);
+                const T dkap = (T)2 * r / (st * st) - (T)2 * r * r * sts / (st * st * st);
+                T f[L + 2];
+                bessel_ratios_fixed<T, L>(kap, f);
+                const T ikap = kap > (T)0 ? (T)1 / kap : (T)0;
+                T df[L + 1];
 #pragma unroll
-    for (int i = 0; i < 9; ++i) {
+                for (int l = 0; l <= L; ++l) df[l] = (f[l + 1] + (T)l * ikap * f[l] - f[l] * f[1]) * dkap;
+                const int am = P.alpha_max[s];
+                const T *G = GcT + P.offp[s];
+                T w0 = 0, w1 = 0, w2 = 0;
+                ylm_all<T, L, true>(Yc, u0, u1, u2, [&](int kk, int l, T y, T gx, T gy, T gz) {
+                    T U = 0, V = 0;
+                    const T *g = G + kk * nmaxp;
 #pragma unroll
-        for (int o = 16; o > 0; o >>= 1) vals[i] += __shfl_xor_sync(0xffffffffu, vals[i], o);
+                    for (int v = 0; v < AMB / VW; ++v) {
+                        if (v * VW < am) {
+                            T gv[VW];
+                            load_vec<T, VW>(g + v * VW, gv);
+#pragma unroll
+                            for (int e = 0; e < VW; ++e) {
+                                U += gv[e] * R[v * VW + e];
+                                V += gv[e] * dR[v * VW + e];
+                            }
+                        }
+                    }
+                    const T a = f[l] * V + df[l] * U;
+                    const T b = U * f[l] * ir;
+                    const T ug = u0 * gx + u1 * gy + u2 * gz;
+                    const T ya = y * a;
+                    w0 += u0 * ya + b * (gx - u0 * ug);
+                    w1 += u1 * ya + b * (gy - u1 * ug);
+                    w2 += u2 * ya + b * (gz - u2 * ug);
+                });
+                // w = dE_i/dr_ij: force -w on the neighbor, +w on the site (its self slot)
+                const double f0 = -(double)w0, f1 = -(double)w1, f2 = -(double)w2;
+                const int j = jatom[k];
+                if (j >= 0 && j < n_atoms) {
+                    atomicAdd(forces + 3 * (size_t)j, f0);
+                    atomicAdd(forces + 3 * (size_t)j + 1, f1);
+                    atomicAdd(forces + 3 * (size_t)j + 2, f2);
+                } else {
+                    check_fail(check, kCheckBwdAtom, k, j);
+                }
+                vals[0] -= f0;
+                vals[1] -= f1;
+                vals[2] -= f2;
+                vals[3] += f0 * xd0;
+                vals[4] += f1 * xd1;
+                vals[5] += f2 * xd2;
+                vals[6] += 0.5 * (f0 * xd1 + f1 * xd0);
+                vals[7] += 0.5 * (f0 * xd2 + f2 * xd0);
+                vals[8] += 0.5 * (f1 * xd2 + f2 * xd1);
+            }
+            __syncwarp();
+        }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) vals[i] += __shfl_xor_sync(0xffffffffu, vals[i], o);
+        }
+        if (lane < 3) {
+            const double fv = lane == 0 ? vals[0] : (lane == 1 ? vals[1] : vals[2]);
+            const int js = jatom[kb];
+            if (js >= 0 && js < n_atoms)
+                atomicAdd(forces + 3 * (size_t)js + lane, fv);
+            else if (lane == 0)
+                check_fail(check, kCheckSelfAtom, kb, js);
+        }
     }
-    if (lane < 3) {
-        const double fv = lane == 0 ? vals[0] : (lane == 1 ? vals[1] : vals[2]);
-        const int js = jatom[kb];
-        if (js >= 0 && js < n_atoms)
-            atomicAdd(forces + 3 * (size_t)js + lane, fv);
-        else if (lane == 0)
-            check_fail(check, kCheckSelfAtom, kb, js);
-    }
+    // virial (xx yy zz xy xz yz -> column-major 3x3): one set of atomics per CTA when its rows
+    // share a structure, else one per warp
     if (lane == 0) {
+        vstruct[warp] = my_struct;
 #pragma unroll
-        for (int c = 0; c < 6; ++c) vir_rows[6 * (size_t)row + c] = vals[3 + c];
+        for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = vals[3 + c];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int st0 = vstruct[0];
+        bool same = true;
+#pragma unroll
+        for (int w = 1; w < kWarpsPerCta; ++w)
+            if (vstruct[w] >= 0 && vstruct[w] != st0) same = false;
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        if (same) {
+            if (lane < 6 && st0 >= 0) {
+                double v = 0;
+#pragma unroll
+                for (int w = 0; w < kWarpsPerCta; ++w) v += vpart[6 * w + lane];
+                const int a = ia[lane], c = ib[lane];
+                atomicAdd(virial + 9 * (size_t)st0 + a + 3 * c, v);
+                if (a != c) atomicAdd(virial + 9 * (size_t)st0 + c + 3 * a, v);
+            }
+        } else if (lane < 6 * kWarpsPerCta) {
+            const int w = lane / 6, c6 = lane - 6 * w;
+            const int st = vstruct[w];
+            if (st >= 0) {
+                const int a = ia[c6], c = ib[c6];
+                atomicAdd(virial + 9 * (size_t)st + a + 3 * c, vpart[6 * w + c6]);
+                if (a != c) atomicAdd(virial + 9 * (size_t)st + c + 3 * a, vpart[6 * w + c6]);
+            }
+        }
     }
 }
 
-// Sum of the row virials of each structure (rows of one structure are contiguous because sites
-// ascend); adds into virial[9 * b] (column-major 3x3, symmetric). One CTA per structure.
-__global__ void k_virial_reduce(int n_rows, const int *__restrict__ sites, const int *__restrict__ struct_off,
-                                const double *__restrict__ vir_rows, double *__restrict__ virial)
+// ----------------------------------------------------------------------------- launchers
+
+inline size_t fwd_warp_bytes(const SoapParams &P, size_t tsz, int astr, int amb)
 {
-    const int b = blockIdx.x;
-    // no offsets: one structure holding every row
-    const int a0 = struct_off ? struct_off[b] : INT_MIN, a1 = struct_off ? struct_off[b + 1] : INT_MAX;
-    auto lower = [&](int a) {
-        int lo = 0, hi = n_rows;
-        while (lo < hi) {
-            const int mid = (lo + hi) >> 1;
-            const int sv = sites ? sites[mid] : mid;
-            if (sv < a)
-                lo = mid + 1;
-            else
-                hi = mid;
-        }
-        return lo;
-    };
-    const int r0 = lower(a0), r1 = lower(a1);
-    double acc[6] = {0, 0, 0, 0, 0, 0};
-    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x)
-#pragma unroll
-        for (int c = 0; c < 6; ++c) acc[c] += vir_rows[6 * (size_t)r + c];
-    __shared__ double red[6][32];
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-    for (int c = 0; c < 6; ++c) {
-        double v = acc[c];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-        if (lane == 0) red[c][w] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        double v = 0;
-        for (int i = 0; i < (int)(blockDim.x >> 5); ++i) v += red[threadIdx.x][i];
-        const int ix[6][2] = {{0, 0}, {1, 1}, {2, 2}, {0, 1}, {0, 2}, {1, 2}};
-        const int a = ix[threadIdx.x][0], c = ix[threadIdx.x][1];
-        double *V = virial + 9 * (size_t)b;
-        V[a + 3 * c] += v;
-        if (a != c) V[c + 3 * a] += v;
-    }
+    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+    const size_t area = std::max<size_t>(32 * (size_t)astr, (size_t)P.dim);
+    return 256 + (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
 }
+
+inline size_t bwd_warp_bytes(const SoapParams &P, size_t tsz)
+{
+    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+    const size_t nout = (size_t)P.n_max * nlm;
+    return 256 + (tsz * ((nout + 3) / 4 * 4 + nlm * (size_t)P.n_maxp + (size_t)P.dim) + 15) / 16 * 16;
+}
+
+constexpr size_t kMaxDynSmem = 227 * 1024;
+
+template <class T> inline const T *soap_tab(const DevBuf &d64, const DevBuf &d32)
+{
+    return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
+}
+
+template <class T, bool SPLIT, int L, int AMB>
+int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 SoapOut &o)
+{
+    constexpr int NLM = (L + 1) * (L + 1);
+    const size_t wb = fwd_warp_bytes(ds.p, sizeof(T), AStride<NLM>::value, AMB), sm = wb * kWarpsPerCta;
+    if (sm > kMaxDynSmem)
+        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", sm);
+    auto kern = k_soap_fwd_warp<T, L, AMB, SPLIT>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
+    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+        ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
+        soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c,
+        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+template <class T, class GT, int L, int AMB>
+int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                 const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
+                 double *d_virial)
+{
+    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T));
+    const size_t sm = wb * kWarpsPerCta + kWarpsPerCta * (6 * sizeof(double) + sizeof(int));
+    if (sm > kMaxDynSmem)
+        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", sm);
+    auto kern = k_soap_bwd_warp<T, GT, L, AMB>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
+    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+        ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
+        d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
+        (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial, (int)wb, pv.n_atoms,
+        pv.check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+#define TGAP_FOR_EACH_L(X) X(0) X(1) X(2) X(3) X(4) X(5) X(6) X(7) X(8) X(9) X(10)
+static_assert(kMaxL == 10, "TGAP_FOR_EACH_L lists l_max = 0..10");
+static_assert(kMaxAlpha <= 16, "radial blocks are instantiated for alpha_max <= 8 and <= 16");
+
+template <class T, bool SPLIT, int AMB>
+int launch_fwd_amb(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                   SoapOut &o)
+{
+    switch (ds.p.l_max) {
+#define TGAP_CASE(l) \
+    case l: return launch_fwd_l<T, SPLIT, l, AMB>(ctx, ds, pv, d_sites, n_rows, o);
+        TGAP_FOR_EACH_L(TGAP_CASE)
+#undef TGAP_CASE
+    }
+    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
+}
+
+template <class T, class GT, int AMB>
+int launch_bwd_amb(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                   const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
+                   double *d_virial)
+{
+    switch (ds.p.l_max) {
+#define TGAP_CASE(l)                                                                                          \
+    case l:                                                                                                   \
+        return launch_bwd_l<T, GT, l, AMB>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, \
+                                           d_virial);
+        TGAP_FOR_EACH_L(TGAP_CASE)
+#undef TGAP_CASE
+    }
+    return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
+}
+
+template <class T, bool SPLIT>
+int launch_fwd(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+               SoapOut &o)
+{
+    if (ds.p.max_alpha <= 8) return launch_fwd_amb<T, SPLIT, 8>(ctx, ds, pv, d_sites, n_rows, o);
+    return launch_fwd_amb<T, SPLIT, 16>(ctx, ds, pv, d_sites, n_rows, o);
+}
+
+template <class T, class GT>
+int launch_bwd(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+               const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
+               double *d_virial)
+{
+    if (ds.p.max_alpha <= 8)
+        return launch_bwd_amb<T, GT, 8>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+    return launch_bwd_amb<T, GT, 16>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+}
+
+}  // namespace tgap

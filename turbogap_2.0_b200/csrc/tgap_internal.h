@@ -19,6 +19,7 @@ constexpr int kMaxAlpha = 16;     // radial functions per species
 constexpr int kMaxNmax = 16;      // radial functions summed over species
 constexpr int kMaxL = 10;         // l_max
 constexpr int kMaxNodes = 192;    // quadrature nodes per species
+constexpr int kTabIntervals = 1024;  // radial table intervals over [0, rcut_hard] (mixed path)
 
 struct Error {
     int status;
@@ -156,6 +157,10 @@ struct SoapParams {
     int node_off[kMaxSpecies];
     int tq_off[kMaxSpecies];
     int max_alpha;
+    int n_maxp;              // sum of alpha_max rounded up to 4 per species
+    int offp[kMaxSpecies];   // padded first radial index of each species block
+    int am_pad;              // max_alpha rounded up to 4 (radial table row length)
+    double tab_scale[kMaxSpecies];  // kTabIntervals / rcut_hard
     double rcut_hard[kMaxSpecies], rcut_soft[kMaxSpecies], nf[kMaxSpecies];
     double global_scaling[kMaxSpecies], sigma_r[kMaxSpecies], sigma_r_scaling[kMaxSpecies];
     double sigma_t[kMaxSpecies], sigma_t_scaling[kMaxSpecies];
@@ -182,6 +187,7 @@ struct DeviceSoap {
     DevBuf xq, tq, central;
     float *xq_f = nullptr, *tq_f = nullptr, *central_f = nullptr;  // single-precision copies
     DevBuf xq32, tq32, central32;
+    DevBuf rtab;  // float4 [n_species][kTabIntervals][am_pad]: cubic Hermite radial table
 };
 int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, DeviceSoap *d);
 
