@@ -8,12 +8,12 @@
 //          partials and G = zeta delta^2 alpha o K^(zeta-1), written back as a bf16 split
 //   GEMM2  g = G Qs         (rows x descriptor, K-dim = n_sparse)   epilogue: FP32 store
 //
-// One CTA computes a 128 x BN tile: one thread issues TMA loads (no multicast) into a
-// STAGES-deep ring of 128B-swizzled shared-memory tiles, one thread issues tcgen05.mma
-// (cta_group::1, kind::f16, accumulator in TMEM), and all four warps drain TMEM with
-// tcgen05.ld for the epilogue. Every mbarrier wait is bounded (1 s of globaltimer); on
-// timeout the kernel raises the device error flag, drains its own outstanding copies with a
-// bounded wait, frees TMEM and returns.
+// Persistent kernel, one CTA per SM over 128 x BN tiles: one thread issues TMA loads (no
+// multicast) into a STAGES-deep ring of 128B-swizzled shared-memory tiles, one thread issues
+// tcgen05.mma (cta_group::1, kind::f16) into one of two TMEM accumulator buffers, and eight
+// epilogue warps drain the other buffer with tcgen05.ld. Every mbarrier wait is bounded (1 s of
+// globaltimer); on timeout the kernel raises the device error flag, waits (bounded) for its
+// own copies and MMAs in flight, frees TMEM and returns.
 #include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
@@ -25,7 +25,6 @@
 
 namespace tgap {
 
-constexpr int kTcThreads = 128;
 constexpr int kBM = 128;
 constexpr int kBK = 64;  // bf16 elements per 128-byte swizzle row
 constexpr uint64_t kWaitNs = 1000000000ull;
@@ -53,6 +52,11 @@ __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
 {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes)
                  : "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive(uint32_t bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
@@ -129,45 +133,77 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
 
 // ---------------------------------------------------------------------------- epilogues
 
-// GEMM1: per element k = K[row][s]: energy partial alpha_s k^zeta, G = zd2 alpha_s k^(zeta-1).
+// k^(zeta - 1) for a compile-time integer zeta (ZI >= 1), else powf with the runtime zeta.
+template <int ZI> __device__ __forceinline__ float kpow_zm1(float k, float zeta)
+{
+    if constexpr (ZI == 1) return 1.0f;
+    else if constexpr (ZI == 2) return k;
+    else if constexpr (ZI == 3) return k * k;
+    else if constexpr (ZI == 4) return k * k * k;
+    else if constexpr (ZI == 5) { const float k2 = k * k; return k2 * k2; }
+    else if constexpr (ZI == 6) { const float k2 = k * k; return k2 * k2 * k; }
+    else return powf(k, zeta - 1.0f);
+}
+
+// GEMM1: per element k = K[row][s]: energy partial alpha_s k^zeta, G = zd2 alpha_s k^(zeta-1)
+// written as a bf16 hi/lo split.
 struct EpiKernelGap {
-    const float *alphas;       // [m_pad]
+    const float *alphas;         // [m_pad]
     __nv_bfloat16 *G_hi, *G_lo;  // [rows_pad][ldg]
     int ldg;
-    double *e_part;            // [n_tiles][rows_pad]
+    double *e_part;              // [n_parts][rows_pad]
     int rows_pad;
     float zd2, zeta;
-    int zeta_int;
-    __device__ __forceinline__ void begin(float &acc) const { acc = 0.0f; }
-    __device__ __forceinline__ void chunk(int row, int col, const float v[16], float &acc) const
+    int zeta_int;                // 1..6, or -1 for a non-integer zeta
+
+    template <int ZI>
+    __device__ __forceinline__ void chunk_z(int row, int col, const float v[16], float &acc) const
     {
-        __align__(16) __nv_bfloat16 hi[16], lo[16];
+        uint32_t hi[8], lo[8];
+        const float4 *a4 = reinterpret_cast<const float4 *>(alphas + col);
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-            const float k = v[j], a = alphas[col + j];
-            float kz1;
-            if (zeta_int >= 1) {
-                kz1 = 1.0f;
-                for (int p = 1; p < zeta_int; ++p) kz1 *= k;
-            } else {
-                kz1 = powf(k, zeta - 1.0f);
+        for (int q = 0; q < 4; ++q) {
+            const float4 a = a4[q];
+            const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int j = 4 * q + 2 * h;
+                const float k0 = v[j], k1 = v[j + 1];
+                const float ak0 = av[2 * h] * kpow_zm1<ZI>(k0, zeta);
+                const float ak1 = av[2 * h + 1] * kpow_zm1<ZI>(k1, zeta);
+                acc = fmaf(ak0, k0, acc);
+                acc = fmaf(ak1, k1, acc);
+                const float g0 = zd2 * ak0, g1 = zd2 * ak1;
+                const __nv_bfloat162 h2 = __floats2bfloat162_rn(g0, g1);
+                const float2 hf = __bfloat1622float2(h2);
+                const __nv_bfloat162 l2 = __floats2bfloat162_rn(g0 - hf.x, g1 - hf.y);
+                hi[j / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+                lo[j / 2] = *reinterpret_cast<const uint32_t *>(&l2);
             }
-            acc += a * kz1 * k;
-            const float g = zd2 * a * kz1;
-            const __nv_bfloat16 h = __float2bfloat16_rn(g);
-            hi[j] = h;
-            lo[j] = __float2bfloat16_rn(g - __bfloat162float(h));
         }
         uint4 *dh = reinterpret_cast<uint4 *>(G_hi + (size_t)row * ldg + col);
         uint4 *dl = reinterpret_cast<uint4 *>(G_lo + (size_t)row * ldg + col);
-        dh[0] = reinterpret_cast<const uint4 *>(hi)[0];
-        dh[1] = reinterpret_cast<const uint4 *>(hi)[1];
-        dl[0] = reinterpret_cast<const uint4 *>(lo)[0];
-        dl[1] = reinterpret_cast<const uint4 *>(lo)[1];
+        dh[0] = make_uint4(hi[0], hi[1], hi[2], hi[3]);
+        dh[1] = make_uint4(hi[4], hi[5], hi[6], hi[7]);
+        dl[0] = make_uint4(lo[0], lo[1], lo[2], lo[3]);
+        dl[1] = make_uint4(lo[4], lo[5], lo[6], lo[7]);
     }
-    __device__ __forceinline__ void end(int row, int tile_n, float acc) const
+    __device__ __forceinline__ void begin(float &acc) const { acc = 0.0f; }
+    __device__ __forceinline__ void chunk(int row, int col, const float v[16], float &acc) const
     {
-        e_part[(size_t)tile_n * rows_pad + row] = (double)acc;
+        switch (zeta_int) {
+        case 1: chunk_z<1>(row, col, v, acc); break;
+        case 2: chunk_z<2>(row, col, v, acc); break;
+        case 3: chunk_z<3>(row, col, v, acc); break;
+        case 4: chunk_z<4>(row, col, v, acc); break;
+        case 5: chunk_z<5>(row, col, v, acc); break;
+        case 6: chunk_z<6>(row, col, v, acc); break;
+        default: chunk_z<-1>(row, col, v, acc); break;
+        }
+    }
+    __device__ __forceinline__ void end(int row, int part, float acc) const
+    {
+        e_part[(size_t)part * rows_pad + row] = (double)acc;
     }
 };
 
@@ -186,12 +222,25 @@ struct EpiStoreF32 {
 
 // ---------------------------------------------------------------------------- kernel
 
+// Persistent, warp-specialised: CTA c takes tiles c, c + gridDim.x, ... (tile = m_tile * n_tiles
+// + n_tile). Warp 0 (one lane) streams A/B hi/lo k-blocks into the STAGES-deep ring, warp 1
+// (one lane) issues the MMAs of a tile into one of two TMEM accumulator buffers (128 columns
+// apart), warps 2..9 drain the other buffer through the epilogue, so a tile's epilogue overlaps
+// the next tile's loads and MMAs. Epilogue warp w reads TMEM lanes 32 (w % 4) .. +31 (= tile
+// rows) and one half of the tile's columns ((w - 2) / 4); its epilogue part index is
+// 2 tile_n + half.
+constexpr int kEpiWarps = 8;
+constexpr int kTcWarps = 2 + kEpiWarps;
+constexpr int kTcThreadsP = 32 * kTcWarps;
+constexpr uint32_t kTmemCols = 256;  // two accumulator buffers of up to 128 columns
+
 template <int BN, int STAGES, class Epi>
-__global__ void __launch_bounds__(kTcThreads, 1)
+__global__ void __launch_bounds__(kTcThreadsP, 1)
     k_gemm_bf16x3(const __grid_constant__ CUtensorMap tmA_hi, const __grid_constant__ CUtensorMap tmA_lo,
                   const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
-                  int num_kb, Epi epi, int *err_flag)
+                  int n_tiles_n, int n_tiles, int num_kb, Epi epi, int *err_flag)
 {
+    static_assert(BN % 32 == 0 && BN >= 32 && BN <= 128, "BN: multiple of 32 in 32..128");
     constexpr uint32_t A_BYTES = kBM * kBK * 2;
     constexpr uint32_t B_BYTES = BN * kBK * 2;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -201,7 +250,8 @@ __global__ void __launch_bounds__(kTcThreads, 1)
                                ((uint32_t)(kBM >> 4) << 24);
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES], bar_accum;
+    __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
+    __shared__ __align__(8) uint64_t bar_tfull[2], bar_tempty[2], bar_drain;
     __shared__ uint32_t tmem_base_slot;
     __shared__ volatile int abort_flag;
     __shared__ int issued, consumed;
@@ -209,14 +259,17 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.y * kBM, n0 = blockIdx.x * BN;
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
             mbar_init(smem_u32(&bar_full[s]), 1);
             mbar_init(smem_u32(&bar_empty[s]), 1);
         }
-        mbar_init(smem_u32(&bar_accum), 1);
+        for (int b = 0; b < 2; ++b) {
+            mbar_init(smem_u32(&bar_tfull[b]), 1);
+            mbar_init(smem_u32(&bar_tempty[b]), 32 * kEpiWarps);
+        }
+        mbar_init(smem_u32(&bar_drain), 1);
         abort_flag = 0;
         issued = 0;
         consumed = 0;
@@ -226,10 +279,10 @@ __global__ void __launch_bounds__(kTcThreads, 1)
         asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB_hi) : "memory");
         asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)&tmB_lo) : "memory");
     }
-    if (warp == 2) {
+    if (warp == 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          smem_u32(&tmem_base_slot)),
-                     "r"((uint32_t)BN)
+                     "r"(kTmemCols)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
@@ -238,88 +291,125 @@ __global__ void __launch_bounds__(kTcThreads, 1)
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
 
-    if (warp == 0 && lane == 0) {
-        // TMA producer
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (kb >= STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) {
-                abort_flag = 1;
-                break;
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer
+            int it = 0;
+            for (int t = blockIdx.x; t < n_tiles && !abort_flag; t += gridDim.x) {
+                const int m0 = (t / n_tiles_n) * kBM, n0 = (t % n_tiles_n) * BN;
+                for (int kb = 0; kb < num_kb; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                    if (it >= STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    const uint32_t st = base + s * STAGE_BYTES;
+                    const uint32_t fb = smem_u32(&bar_full[s]);
+                    mbar_expect_tx(fb, STAGE_BYTES);
+                    tma_load_2d(st, &tmA_hi, fb, kb * kBK, m0);
+                    tma_load_2d(st + A_BYTES, &tmA_lo, fb, kb * kBK, m0);
+                    tma_load_2d(st + 2 * A_BYTES, &tmB_hi, fb, kb * kBK, n0);
+                    tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tmB_lo, fb, kb * kBK, n0);
+                    issued = it + 1;
+                }
             }
-            const uint32_t st = base + s * STAGE_BYTES;
-            const uint32_t fb = smem_u32(&bar_full[s]);
-            mbar_expect_tx(fb, STAGE_BYTES);
-            tma_load_2d(st, &tmA_hi, fb, kb * kBK, m0);
-            tma_load_2d(st + A_BYTES, &tmA_lo, fb, kb * kBK, m0);
-            tma_load_2d(st + 2 * A_BYTES, &tmB_hi, fb, kb * kBK, n0);
-            tma_load_2d(st + 2 * A_BYTES + B_BYTES, &tmB_lo, fb, kb * kBK, n0);
-            issued = kb + 1;
+            // tail: wait until the MMAs have released the last STAGES stages, so no asynchronous
+            // arrive on a stage barrier is pending when the CTA exits (bounded)
+            for (int i = (issued > STAGES ? issued - STAGES : 0); i < issued && !abort_flag; ++i)
+                if (!mbar_wait(smem_u32(&bar_empty[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &abort_flag))
+                    abort_flag = 1;
         }
-        // tail: wait until the MMAs have released the last STAGES tiles, so no asynchronous
-        // arrive on a stage barrier is still pending when the CTA exits (bounded)
-        for (int kb = (num_kb > STAGES ? num_kb - STAGES : 0); kb < issued && !abort_flag; ++kb)
-            if (!mbar_wait(smem_u32(&bar_empty[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &abort_flag))
-                abort_flag = 1;
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer
-        for (int kb = 0; kb < num_kb; ++kb) {
-            const int s = kb % STAGES;
-            const uint32_t ph = (uint32_t)(kb / STAGES) & 1u;
-            if (!mbar_wait(smem_u32(&bar_full[s]), ph, &abort_flag)) {
-                abort_flag = 1;
-                break;
-            }
-            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-            const uint32_t st = base + s * STAGE_BYTES;
+    } else if (warp == 1) {
+        if (lane == 0) {
+            // MMA issuer
+            int it = 0, tc = 0;
+            for (int t = blockIdx.x; t < n_tiles && !abort_flag; t += gridDim.x, ++tc) {
+                const int b = tc & 1, use = tc >> 1;
+                if (use > 0 && !mbar_wait(smem_u32(&bar_tempty[b]), (uint32_t)(use - 1) & 1u, &abort_flag)) {
+                    abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                const uint32_t acc = tmem + (uint32_t)(b * 128);
+                for (int kb = 0; kb < num_kb; ++kb, ++it) {
+                    const int s = it % STAGES;
+                    const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                    if (!mbar_wait(smem_u32(&bar_full[s]), ph, &abort_flag)) {
+                        abort_flag = 1;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                    const uint32_t st = base + s * STAGE_BYTES;
 #pragma unroll
-            for (int k = 0; k < kBK / 16; ++k) {
-                const uint64_t ahi = umma_desc(st + 32 * k);
-                const uint64_t alo = umma_desc(st + A_BYTES + 32 * k);
-                const uint64_t bhi = umma_desc(st + 2 * A_BYTES + 32 * k);
-                const uint64_t blo = umma_desc(st + 2 * A_BYTES + B_BYTES + 32 * k);
-                umma_bf16(tmem, ahi, bhi, IDESC, (kb > 0 || k > 0) ? 1u : 0u);
-                umma_bf16(tmem, ahi, blo, IDESC, 1u);
-                umma_bf16(tmem, alo, bhi, IDESC, 1u);
+                    for (int k = 0; k < kBK / 16; ++k) {
+                        const uint64_t ahi = umma_desc(st + 32 * k);
+                        const uint64_t alo = umma_desc(st + A_BYTES + 32 * k);
+                        const uint64_t bhi = umma_desc(st + 2 * A_BYTES + 32 * k);
+                        const uint64_t blo = umma_desc(st + 2 * A_BYTES + B_BYTES + 32 * k);
+                        umma_bf16(acc, ahi, bhi, IDESC, (kb > 0 || k > 0) ? 1u : 0u);
+                        umma_bf16(acc, ahi, blo, IDESC, 1u);
+                        umma_bf16(acc, alo, bhi, IDESC, 1u);
+                    }
+                    umma_commit(smem_u32(&bar_empty[s]));
+                    consumed = it + 1;
+                }
+                if (abort_flag) break;
+                umma_commit(smem_u32(&bar_tfull[b]));
             }
-            umma_commit(smem_u32(&bar_empty[s]));
-            consumed = kb + 1;
+            // every MMA issued so far has completed once bar_drain fires (bounded)
+            umma_commit(smem_u32(&bar_drain));
+            volatile int never = 0;
+            mbar_wait(smem_u32(&bar_drain), 0, &never);
         }
-        umma_commit(smem_u32(&bar_accum));
-    }
-    __syncwarp();
-
-    // epilogue: warp w owns accumulator lanes (rows) 32w .. 32w+31
-    const bool ok = mbar_wait(smem_u32(&bar_accum), 0, &abort_flag);
-    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-    __syncwarp();
-    if (ok && !abort_flag) {
-        const int row = m0 + warp * 32 + lane;
-        float acc;
-        epi.begin(acc);
+    } else {
+        // epilogue: rows 32 (warp % 4) + lane of the tile, columns [half BN/2, (half + 1) BN/2)
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const int r_local = quarter * 32 + lane;
+        constexpr int HB = BN / 2;
+        int tc = 0;
+        for (int t = blockIdx.x; t < n_tiles; t += gridDim.x, ++tc) {
+            const int b = tc & 1, use = tc >> 1;
+            const bool ok = mbar_wait(smem_u32(&bar_tfull[b]), (uint32_t)use & 1u, &abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (!ok || abort_flag) {
+                abort_flag = 1;
+                break;
+            }
+            const int row = (t / n_tiles_n) * kBM + r_local;
+            const int tile_n = t % n_tiles_n, c0 = tile_n * BN + half * HB;
+            const uint32_t taddr =
+                tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * 128) + (uint32_t)(half * HB);
+            float acc;
+            epi.begin(acc);
 #pragma unroll 1
-        for (int c = 0; c < BN; c += 16) {
-            float v[16];
-            tmem_ld16(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)c, v);
-            epi.chunk(row, n0 + c, v, acc);
+            for (int c = 0; c < HB; c += 16) {
+                float v[16];
+                tmem_ld16(taddr + (uint32_t)c, v);
+                epi.chunk(row, c0 + c, v, acc);
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(smem_u32(&bar_tempty[b]));
+            epi.end(row, 2 * tile_n + half, acc);
         }
-        epi.end(row, blockIdx.x, acc);
     }
+    __syncwarp();
     asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     __syncthreads();
-    if (abort_flag || !ok) {
+    if (abort_flag) {
         if (threadIdx.x == 0) {
             atomicExch(err_flag, 1);
             // drain this CTA's own copies still in flight (bounded)
             volatile int dummy = 0;
-            for (int kb = consumed; kb < issued; ++kb)
-                mbar_wait(smem_u32(&bar_full[kb % STAGES]), (uint32_t)(kb / STAGES) & 1u, &dummy);
+            for (int i = consumed; i < issued; ++i)
+                mbar_wait(smem_u32(&bar_full[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &dummy);
         }
         __syncthreads();
     }
-    if (warp == 2) {
+    if (warp == 1) {
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
                      : "memory");
     }
 }
@@ -361,9 +451,16 @@ static int make_map(tgap_context *ctx, CUtensorMap *map, const void *ptr, int ro
     return TGAP_OK;
 }
 
+static int sm_count(tgap_context *ctx)
+{
+    static int n = 0;
+    if (!n && cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, ctx->device) != cudaSuccess) n = 148;
+    return n;
+}
+
 template <int BN, int STAGES, class Epi>
-static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, const void *a_lo, const void *b_hi, const void *b_lo,
-                       int M, int N, int K, Epi epi)
+static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, const void *a_lo, const void *b_hi,
+                       const void *b_lo, int M, int N, int K, Epi epi)
 {
     // M, N, K are padded: M % 128 == 0, N % BN == 0, K % 64 == 0 (checked by the caller)
     CUtensorMap ta_hi, ta_lo, tb_hi, tb_lo;
@@ -372,15 +469,18 @@ static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, c
         (rc = make_map(ctx, &tb_hi, b_hi, N, K, BN)) || (rc = make_map(ctx, &tb_lo, b_lo, N, K, BN)))
         return rc;
     constexpr size_t smem = (size_t)STAGES * (2 * kBM * kBK * 2 + 2 * BN * kBK * 2) + 1024;
+    static_assert(smem <= 227 * 1024 - 256, "stage ring exceeds shared memory");
     auto kern = k_gemm_bf16x3<BN, STAGES, Epi>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     if (!ctx->d_flag) {
         TGAP_CUDA(ctx, cudaMalloc(&ctx->d_flag, sizeof(int)));
         TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
     }
-    dim3 grid(N / BN, M / kBM);
+    const int n_tiles_n = N / BN, n_tiles = (M / kBM) * n_tiles_n;
+    const int grid = n_tiles < sm_count(ctx) ? n_tiles : sm_count(ctx);
     StageScope sc(ctx, stage);
-    kern<<<grid, kTcThreads, smem, ctx->stream>>>(ta_hi, ta_lo, tb_hi, tb_lo, K / kBK, epi, ctx->d_flag);
+    kern<<<grid, kTcThreadsP, smem, ctx->stream>>>(ta_hi, ta_lo, tb_hi, tb_lo, n_tiles_n, n_tiles, K / kBK, epi,
+                                                   ctx->d_flag);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
@@ -449,12 +549,12 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
                           const int *d_sites, double *d_e_rows, double *d_energies)
 {
     if (n_rows <= 0) return TGAP_OK;
-    constexpr int BN1 = 128, BN2 = 64;
+    constexpr int BN1 = 128;
     const int rows_pad = (n_rows + kBM - 1) / kBM * kBM;
-    const int n_tiles = m.m_pad / BN1;
-    if (m.dim_pad % BN2 || m.m_pad % BN1 || m.dim_pad % kBK || m.m_pad % kBK)
+    const int n_parts = 2 * (m.m_pad / BN1);  // one energy partial per tile column half
+    if (m.dim_pad % 128 || m.m_pad % BN1 || m.dim_pad % kBK || m.m_pad % kBK)
         return set_error(ctx, TGAP_ERR_ARGUMENT, "mixed GEMM padding");
-    if (w->e_part.ensure(sizeof(double) * (size_t)n_tiles * rows_pad) ||
+    if (w->e_part.ensure(sizeof(double) * (size_t)n_parts * rows_pad) ||
         w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad) ||
         (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad)))
         return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
@@ -472,14 +572,19 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     int rc = launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr, rows_pad, m.m_pad,
                                                m.dim_pad, e1);
     if (rc) return rc;
-    k_energy_reduce_ld<<<(n_rows + 127) / 128, 128, 0, ctx->stream>>>(n_rows, n_tiles, rows_pad,
+    k_energy_reduce_ld<<<(n_rows + 127) / 128, 128, 0, ctx->stream>>>(n_rows, n_parts, rows_pad,
                                                                        w->e_part.as<double>(), m.delta * m.delta,
                                                                        e0, d_sites, d_e_rows, d_energies);
     TGAP_LAUNCH_CHECK(ctx);
     if (!do_forces) return TGAP_OK;
+    // dE/dq: N = dim_pad is small, so 96-column tiles (when they divide it) give more tiles to
+    // spread over the SMs than 128-column ones
     EpiStoreF32 e2{w->g.as<float>(), m.dim_pad};
-    return launch_gemm<BN2, 4, EpiStoreF32>(ctx, "gemm_bf16x3_grad", w->G_hi.ptr, w->G_lo.ptr, m.QT_hi.ptr, m.QT_lo.ptr, rows_pad,
-                                            m.dim_pad, m.m_pad, e2);
+    if (m.dim_pad % 96 == 0)
+        return launch_gemm<96, 4, EpiStoreF32>(ctx, "gemm_bf16x3_grad", w->G_hi.ptr, w->G_lo.ptr, m.QT_hi.ptr,
+                                               m.QT_lo.ptr, rows_pad, m.dim_pad, m.m_pad, e2);
+    return launch_gemm<128, 3, EpiStoreF32>(ctx, "gemm_bf16x3_grad", w->G_hi.ptr, w->G_lo.ptr, m.QT_hi.ptr,
+                                            m.QT_lo.ptr, rows_pad, m.dim_pad, m.m_pad, e2);
 }
 
 }  // namespace tgap

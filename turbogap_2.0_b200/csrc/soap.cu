@@ -345,6 +345,7 @@ const YlmConst &ylm_host_constants()
         for (int m = 0; m <= kMaxL; ++m) {
             if (m > 0) df *= (2.0 * m - 1.0);
             y.dfact[m] = df;
+            y.inv_int[m] = m > 0 ? 1.0 / m : 0.0;
         }
         for (int l = 0; l <= kMaxL; ++l) {
             double fr = 1.0;
@@ -354,6 +355,11 @@ const YlmConst &ylm_host_constants()
                 y.norm[l * (l + 1) / 2 + m] = m == 0 ? N : N * M_SQRT2;
             }
         }
+        for (int i = 0; i <= kMaxL; ++i) {
+            y.dfact_f[i] = (float)y.dfact[i];
+            y.inv_int_f[i] = (float)y.inv_int[i];
+        }
+        for (int i = 0; i < (kMaxL + 1) * (kMaxL + 2) / 2; ++i) y.norm_f[i] = (float)y.norm[i];
         return y;
     }();
     return h;

@@ -21,7 +21,22 @@ constexpr int kNlmMax = (kMaxL + 1) * (kMaxL + 1);
 struct YlmConst {
     double dfact[kMaxL + 1];
     double norm[(kMaxL + 1) * (kMaxL + 2) / 2];  // index l (l+1)/2 + m
+    double inv_int[kMaxL + 1];                   // 1 / k (0 for k = 0)
+    float dfact_f[kMaxL + 1];                    // single-precision copies
+    float norm_f[(kMaxL + 1) * (kMaxL + 2) / 2];
+    float inv_int_f[kMaxL + 1];
 };
+
+// Constants in the arithmetic type of the caller.
+template <class T> __device__ __forceinline__ T yc_dfact(const YlmConst &Y, int i);
+template <> __device__ __forceinline__ double yc_dfact<double>(const YlmConst &Y, int i) { return Y.dfact[i]; }
+template <> __device__ __forceinline__ float yc_dfact<float>(const YlmConst &Y, int i) { return Y.dfact_f[i]; }
+template <class T> __device__ __forceinline__ T yc_norm(const YlmConst &Y, int i);
+template <> __device__ __forceinline__ double yc_norm<double>(const YlmConst &Y, int i) { return Y.norm[i]; }
+template <> __device__ __forceinline__ float yc_norm<float>(const YlmConst &Y, int i) { return Y.norm_f[i]; }
+template <class T> __device__ __forceinline__ T yc_inv(const YlmConst &Y, int i);
+template <> __device__ __forceinline__ double yc_inv<double>(const YlmConst &Y, int i) { return Y.inv_int[i]; }
+template <> __device__ __forceinline__ float yc_inv<float>(const YlmConst &Y, int i) { return Y.inv_int_f[i]; }
 
 // Host copy of the harmonic constants (computed once); passed to the warp kernels by value.
 const YlmConst &ylm_host_constants();

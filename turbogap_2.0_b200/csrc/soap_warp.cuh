@@ -11,9 +11,9 @@
 //            shared memory and every lane accumulates the product for its own harmonics
 //            lm = lane + 32 i over all n in registers. Then the power spectrum
 //            p[n n' l] = (sqrt 2 if n != n') sum_m c[n][lm] c[n'][lm] and q = p / |p|.
-//  adjoint   h = (g - q (q.g)) / |p|, Gc = dE/dc = M_l c (M from h), stored harmonic-major with
-//            each species block padded to 4 so a lane reads its radial weights with 16-byte
-//            loads; per pair w = sum_lm [R'.G f Y u + R.G (df Y u + f (grad Y)_perp / r)],
+//  adjoint   h = (g - q (q.g)) / |p|, Gc = dE/dc = M_l c (M from h), stored per species block
+//            harmonic-major and AMB wide (zero padded) so a lane reads its radial weights with
+//            16-byte loads; per pair w = sum_lm [R'.G f Y u + R.G (df Y u + f (grad Y)_perp / r)],
 //            force -w on the neighbor and +w on the site, virial sum of r (x) f.
 //
 // FP32 instantiations (mixed path) take the radial values from a cubic Hermite table of R_n
@@ -31,7 +31,7 @@
 
 namespace tgap {
 
-constexpr int kWarpsPerCta = 4;
+constexpr int kWarpsPerCta = 4;  // sites (warps) per CTA, fewer when shared memory is short
 
 __device__ __forceinline__ unsigned lanemask_lt()
 {
@@ -117,7 +117,7 @@ __device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F 
             Sc = sn;
         }
         T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
-        const T qmm = (T)Yc.dfact[m];
+        const T qmm = yc_dfact<T>(Yc, m);
 #pragma unroll
         for (int l = m; l <= L; ++l) {
             T Q, dQ;
@@ -136,7 +136,7 @@ __device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F 
             Q1 = Q;
             dQ2 = dQ1;
             dQ1 = dQ;
-            const T N = (T)Yc.norm[l * (l + 1) / 2 + m];
+            const T N = yc_norm<T>(Yc, l * (l + 1) / 2 + m);
             if (m == 0) {
                 fn(l * l, l, N * Q, (T)0, (T)0, GRAD ? N * dQ : (T)0);
             } else {
@@ -149,6 +149,76 @@ __device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F 
                     fn(l * l + 2 * m - 1, l, NQ * Cc, (T)0, (T)0, (T)0);
                     fn(l * l + 2 * m, l, NQ * Sc, (T)0, (T)0, (T)0);
                 }
+            }
+        }
+    }
+}
+
+// Every real harmonic with its gradient (as ylm_all<GRAD = true>), orders m >= 1 in a runtime
+// loop with l unrolled inside: the adjoint's per-harmonic body is large, and this keeps the
+// kernel's code within the instruction cache while l (and so f_l) stays compile-time.
+template <class T, int L, class F>
+__device__ __forceinline__ void ylm_all_grad(const YlmConst &Yc, T ux, T uy, T uz, F &&fn)
+{
+    {
+        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+#pragma unroll
+        for (int l = 0; l <= L; ++l) {
+            T Q, dQ;
+            if (l == 0) {
+                Q = 1;
+                dQ = 0;
+            } else if (l == 1) {
+                Q = uz;
+                dQ = 1;
+            } else {
+                const T inv = (T)(1.0 / (double)l);
+                Q = ((T)(2 * l - 1) * uz * Q1 - (T)(l - 1) * Q2) * inv;
+                dQ = ((T)(2 * l - 1) * (Q1 + uz * dQ1) - (T)(l - 1) * dQ2) * inv;
+            }
+            Q2 = Q1;
+            Q1 = Q;
+            dQ2 = dQ1;
+            dQ1 = dQ;
+            const T N = yc_norm<T>(Yc, l * (l + 1) / 2);
+            fn(l * l, l, N * Q, (T)0, (T)0, N * dQ);
+        }
+    }
+    T Cc = 1, Sc = 0;
+#pragma unroll 1
+    for (int m = 1; m <= L; ++m) {
+        const T Cp = Cc, Sp = Sc;
+        Cc = ux * Cp - uy * Sp;
+        Sc = ux * Sp + uy * Cp;
+        const T qmm = yc_dfact<T>(Yc, m);
+        const T fm = (T)m;
+        const T tm1 = (T)(2 * m + 1);
+        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+#pragma unroll
+        for (int l = 1; l <= L; ++l) {
+            if (l >= m) {
+                T Q, dQ;
+                if (l == m) {
+                    Q = qmm;
+                    dQ = 0;
+                } else if (l == m + 1) {
+                    Q = tm1 * uz * qmm;
+                    dQ = tm1 * qmm;
+                } else {
+                    const T inv = yc_inv<T>(Yc, l - m);
+                    const T a = (T)(2 * l - 1), b = (T)(l - 1) + fm;
+                    Q = (a * uz * Q1 - b * Q2) * inv;
+                    dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
+                }
+                Q2 = Q1;
+                Q1 = Q;
+                dQ2 = dQ1;
+                dQ1 = dQ;
+                const T N = yc_norm<T>(Yc, l * (l + 1) / 2 + m);
+                const T NQ = N * Q, NQm = NQ * fm, NdQ = N * dQ;
+                const int k0 = l * l + 2 * m - 1;
+                fn(k0, l, NQ * Cc, NQm * Cp, -NQm * Sp, NdQ * Cc);
+                fn(k0 + 1, l, NQ * Sc, NQm * Sp, NQm * Cp, NdQ * Sc);
             }
         }
     }
@@ -279,8 +349,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     constexpr int ASTR = AStride<NLM>::value;
     constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = blockIdx.x * kWarpsPerCta + warp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int row = blockIdx.x * nw + warp;
     if (row >= n_rows) return;  // no CTA-wide synchronisation in this kernel
     unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
     const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
@@ -389,8 +459,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
 // ----------------------------------------------------------------------------- adjoint
 
 // Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (rounded up to 4),
-// GcT [NLM][n_maxp] (species blocks at the padded offsets offp, padding zero), h [dim]; after
-// the warps, the CTA's virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
+// Gc [n_species][NLM][AMB] (dE/dc per species block, zero beyond alpha_max), M [L+1][MS] with
+// M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l] (MS = n_max^2 + 1, odd); after the warps,
+// the CTA's virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
 template <class T, class GT, int L, int AMB>
 __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
@@ -402,50 +473,64 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
     int warp_smem, int n_atoms, int *check)
 {
     constexpr int NLM = (L + 1) * (L + 1);
-    constexpr int VW = std::is_same<T, float>::value ? 4 : 2;
+    constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int row = blockIdx.x * kWarpsPerCta + warp;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int row = blockIdx.x * nw + warp;
     const bool active = row < n_rows;
-    double *vpart = reinterpret_cast<double *>(smem_raw + (size_t)kWarpsPerCta * warp_smem);
+    double *vpart = reinterpret_cast<double *>(smem_raw + (size_t)nw * warp_smem);
     int *vstruct = reinterpret_cast<int *>(vpart + 6 * kWarpsPerCta);
     double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
     int my_struct = -1;
     if (active) {
         unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
-        const int nmax = P.n_max, nmaxp = P.n_maxp, dim = P.dim, nout = nmax * NLM;
+        const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM, MS = nmax * nmax + 1;
         long long *idx = reinterpret_cast<long long *>(wbase);
         T *cs = reinterpret_cast<T *>(wbase + 256);
-        T *GcT = cs + (nout + 3) / 4 * 4;
-        T *hs = GcT + NLM * nmaxp;
+        T *Gc = cs + (nout + 3) / 4 * 4;
+        T *Ms = Gc + P.n_species * NLM * AMB;
 
         const int site = sites ? sites[row] : row;
         my_struct = site_struct ? site_struct[site] : 0;
         const int64_t kb = start[site], ke = start[site + 1];
         for (int o = lane; o < nout; o += 32) cs[o] = c_in[(size_t)row * nout + o];
-        for (int o = lane; o < NLM * nmaxp; o += 32) GcT[o] = 0;
         T qg = 0;
         for (int d = lane; d < dim; d += 32) qg += q_in[(size_t)row * q_ld + d] * (T)g_in[(size_t)row * g_ld + d];
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
         const T nrm = norm_in[row];
         const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-        for (int d = lane; d < dim; d += 32)
-            hs[d] = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
+        // h = dE/dp = (g - q (q.g)) / |p|, scattered into the symmetric M_l
+        for (int d = lane; d < dim; d += 32) {
+            int n, np, l;
+            ps_decode_w(d, nmax, L, &n, &np, &l);
+            const T hv = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
+            const T mv = (n == np) ? (T)2 * hv : (T)1.4142135623730951 * hv;
+            Ms[l * MS + n * nmax + np] = mv;
+            Ms[l * MS + np * nmax + n] = mv;
+        }
         __syncwarp();
-        // Gc[n][lm] = sum_n' (2 h[n n' l] if n == n' else sqrt2 h[n n' l]) c[n'][lm]
-        for (int o = lane; o < nout; o += 32) {
-            const int kk = o / nmax, n = o - kk * nmax;
-            int l = 0;
-            while ((l + 1) * (l + 1) <= kk) ++l;
-            T acc = 0;
-            for (int np = 0; np < nmax; ++np) {
-                const T h = hs[ps_index_w(n, np, nmax, L, l)];
-                acc += ((np == n) ? (T)2 * h : (T)1.4142135623730951 * h) * cs[np * NLM + kk];
+        // Gc[s][lm][n] = sum_n' M_l[off_s + n][n'] c[n'][lm]
+#pragma unroll
+        for (int j = 0; j < KPL; ++j) {
+            const int kk = lane + 32 * j;
+            if (kk < NLM) {
+                int l = (int)sqrtf((float)kk);
+                const T *Ml = Ms + l * MS;
+                for (int s = 0; s < P.n_species; ++s) {
+                    const int off = P.n_off[s], am = P.alpha_max[s];
+                    T *Gk = Gc + (s * NLM + kk) * AMB;
+#pragma unroll
+                    for (int n = 0; n < AMB; ++n) {
+                        T acc = 0;
+                        if (n < am) {
+                            const T *mr = Ml + (off + n) * nmax;
+                            for (int np = 0; np < nmax; ++np) acc += mr[np] * cs[np * NLM + kk];
+                        }
+                        Gk[n] = acc;
+                    }
+                }
             }
-            int s = 0;
-            while (s + 1 < P.n_species && n >= P.n_off[s + 1]) ++s;
-            GcT[kk * nmaxp + P.offp[s] + (n - P.n_off[s])] = acc;
         }
         __syncwarp();
 
@@ -476,23 +561,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
                 T df[L + 1];
 #pragma unroll
                 for (int l = 0; l <= L; ++l) df[l] = (f[l + 1] + (T)l * ikap * f[l] - f[l] * f[1]) * dkap;
-                const int am = P.alpha_max[s];
-                const T *G = GcT + P.offp[s];
+                const T *Gs = Gc + s * NLM * AMB;
                 T w0 = 0, w1 = 0, w2 = 0;
-                ylm_all<T, L, true>(Yc, u0, u1, u2, [&](int kk, int l, T y, T gx, T gy, T gz) {
+                ylm_all_grad<T, L>(Yc, u0, u1, u2, [&](int kk, int l, T y, T gx, T gy, T gz) {
+                    T gv[AMB];
+                    load_vec<T, AMB>(Gs + kk * AMB, gv);
                     T U = 0, V = 0;
-                    const T *g = G + kk * nmaxp;
 #pragma unroll
-                    for (int v = 0; v < AMB / VW; ++v) {
-                        if (v * VW < am) {
-                            T gv[VW];
-                            load_vec<T, VW>(g + v * VW, gv);
-#pragma unroll
-                            for (int e = 0; e < VW; ++e) {
-                                U += gv[e] * R[v * VW + e];
-                                V += gv[e] * dR[v * VW + e];
-                            }
-                        }
+                    for (int e = 0; e < AMB; ++e) {
+                        U += gv[e] * R[e];
+                        V += gv[e] * dR[e];
                     }
                     const T a = f[l] * V + df[l] * U;
                     const T b = U * f[l] * ir;
@@ -549,24 +627,24 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
     if (warp == 0) {
         const int st0 = vstruct[0];
         bool same = true;
-#pragma unroll
-        for (int w = 1; w < kWarpsPerCta; ++w)
+        for (int w = 1; w < nw; ++w)
             if (vstruct[w] >= 0 && vstruct[w] != st0) same = false;
-        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        // component c of (xx yy zz xy xz yz) -> matrix indices (a, b)
+        auto ia = [](int c) { return c < 3 ? c : (c == 5 ? 1 : 0); };
+        auto ib = [](int c) { return c < 3 ? c : (c == 3 ? 1 : 2); };
         if (same) {
             if (lane < 6 && st0 >= 0) {
                 double v = 0;
-#pragma unroll
-                for (int w = 0; w < kWarpsPerCta; ++w) v += vpart[6 * w + lane];
-                const int a = ia[lane], c = ib[lane];
+                for (int w = 0; w < nw; ++w) v += vpart[6 * w + lane];
+                const int a = ia(lane), c = ib(lane);
                 atomicAdd(virial + 9 * (size_t)st0 + a + 3 * c, v);
                 if (a != c) atomicAdd(virial + 9 * (size_t)st0 + c + 3 * a, v);
             }
-        } else if (lane < 6 * kWarpsPerCta) {
+        } else if (lane < 6 * nw) {
             const int w = lane / 6, c6 = lane - 6 * w;
             const int st = vstruct[w];
             if (st >= 0) {
-                const int a = ia[c6], c = ib[c6];
+                const int a = ia(c6), c = ib(c6);
                 atomicAdd(virial + 9 * (size_t)st + a + 3 * c, vpart[6 * w + c6]);
                 if (a != c) atomicAdd(virial + 9 * (size_t)st + c + 3 * a, vpart[6 * w + c6]);
             }
@@ -583,11 +661,12 @@ inline size_t fwd_warp_bytes(const SoapParams &P, size_t tsz, int astr, int amb)
     return 256 + (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
 }
 
-inline size_t bwd_warp_bytes(const SoapParams &P, size_t tsz)
+inline size_t bwd_warp_bytes(const SoapParams &P, size_t tsz, int amb)
 {
     const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
     const size_t nout = (size_t)P.n_max * nlm;
-    return 256 + (tsz * ((nout + 3) / 4 * 4 + nlm * (size_t)P.n_maxp + (size_t)P.dim) + 15) / 16 * 16;
+    const size_t ms = (size_t)(P.l_max + 1) * ((size_t)P.n_max * P.n_max + 1);
+    return 256 + (tsz * ((nout + 3) / 4 * 4 + (size_t)P.n_species * nlm * amb + ms) + 15) / 16 * 16;
 }
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
@@ -602,13 +681,14 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  SoapOut &o)
 {
     constexpr int NLM = (L + 1) * (L + 1);
-    const size_t wb = fwd_warp_bytes(ds.p, sizeof(T), AStride<NLM>::value, AMB), sm = wb * kWarpsPerCta;
-    if (sm > kMaxDynSmem)
-        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", sm);
+    const size_t wb = fwd_warp_bytes(ds.p, sizeof(T), AStride<NLM>::value, AMB);
+    const int nw = (int)std::min<size_t>(kWarpsPerCta, kMaxDynSmem / wb);
+    if (nw < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", wb);
+    const size_t sm = wb * nw;
     auto kern = k_soap_fwd_warp<T, L, AMB, SPLIT>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
-    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+    const int grid = (n_rows + nw - 1) / nw;
+    kern<<<grid, 32 * nw, sm, ctx->stream>>>(
         ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
         soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c,
         (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check);
@@ -621,14 +701,15 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                  double *d_virial)
 {
-    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T));
-    const size_t sm = wb * kWarpsPerCta + kWarpsPerCta * (6 * sizeof(double) + sizeof(int));
-    if (sm > kMaxDynSmem)
-        return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", sm);
+    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T), AMB);
+    const size_t tail = kWarpsPerCta * (6 * sizeof(double) + sizeof(int));
+    const int nw = (int)std::min<size_t>(kWarpsPerCta, (kMaxDynSmem - tail) / wb);
+    if (nw < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", wb);
+    const size_t sm = wb * nw + tail;
     auto kern = k_soap_bwd_warp<T, GT, L, AMB>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + kWarpsPerCta - 1) / kWarpsPerCta;
-    kern<<<grid, 32 * kWarpsPerCta, sm, ctx->stream>>>(
+    const int grid = (n_rows + nw - 1) / nw;
+    kern<<<grid, 32 * nw, sm, ctx->stream>>>(
         ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
         d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
         (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial, (int)wb, pv.n_atoms,

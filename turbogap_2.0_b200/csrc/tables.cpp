@@ -180,13 +180,7 @@ int make_soap_params(const tgap_soap_hypers *h, SoapParams *p, std::string *why)
     }
     p->n_max = nmax;
     p->dim = nmax * (nmax + 1) / 2 * (h->l_max + 1);
-    int np = 0;
-    for (int s = 0; s < h->n_species; ++s) {
-        p->offp[s] = np;
-        np += up4(p->alpha_max[s]);
-        p->tab_scale[s] = (double)kTabIntervals / p->rcut_hard[s];
-    }
-    p->n_maxp = np;
+    for (int s = 0; s < h->n_species; ++s) p->tab_scale[s] = (double)kTabIntervals / p->rcut_hard[s];
     p->am_pad = up4(p->max_alpha);
     return TGAP_OK;
 }

@@ -157,8 +157,6 @@ struct SoapParams {
     int node_off[kMaxSpecies];
     int tq_off[kMaxSpecies];
     int max_alpha;
-    int n_maxp;              // sum of alpha_max rounded up to 4 per species
-    int offp[kMaxSpecies];   // padded first radial index of each species block
     int am_pad;              // max_alpha rounded up to 4 (radial table row length)
     double tab_scale[kMaxSpecies];  // kTabIntervals / rcut_hard
     double rcut_hard[kMaxSpecies], rcut_soft[kMaxSpecies], nf[kMaxSpecies];
