@@ -1154,8 +1154,15 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
     CHECK_RC(activate(ctx));
     for (int it = 0; it < n_steps; ++it) {
         const bool rebuild = (md->step % md->rebuild_every) == 0;
-        if (md->first || rebuild) {
-            // eager step: a rebuild needs the pair count on the host, and it sizes every buffer
+        if (!md->first && rebuild) {
+            // new pair lists on the current positions (one host synchronization for the pair
+            // count); the step below refreshes the geometry on them like any other step
+            CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
+            int64_t n_pairs = 0;
+            CHECK_RC(neighbors_rebuild_lists(ctx, &md->sys->nb, -1, &n_pairs));
+        }
+        if (md->first) {
+            // eager first step: it sizes every buffer
             CHECK_RC(tgap_system_update(md->sys, rebuild ? 1 : 0));
             CHECK_RC(md_eval(md));
             CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),

@@ -20,7 +20,8 @@ namespace tgap {
 
 __device__ __forceinline__ double f_modulo(double a, double p)
 {
-    double r = fmod(a, p);
+    // fmod(a, p) is exact and equals a when |a| < p: skip the call on that (common) path
+    double r = fabs(a) < p ? a : fmod(a, p);
     if (r != 0.0 && ((r < 0.0) != (p < 0.0))) r = r + p;
     return r;
 }
@@ -149,73 +150,102 @@ __global__ void k_cell_sort(int n_cells, const int *cell_start, int *cell_atoms)
     }
 }
 
-// Pass over one site's candidates in reference order; FILL=false counts, FILL=true writes.
-template <bool FILL>
-__global__ void k_site_pairs(int n_atoms_total, const int *site_struct, const StructDesc *sd,
-                             const double *pos_sc, const int *cell_start, const int *cell_atoms,
-                             int64_t *counts, const int64_t *start, int *list, int *check)
+__device__ __forceinline__ unsigned nb_lanemask_lt()
 {
-    int g = blockIdx.x * blockDim.x + threadIdx.x;
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// One warp per site; FILL=false counts the site's pairs, FILL=true writes them in the
+// reference order. Linked-cell path: lane c < 27 owns neighbor cell c of the z -> y -> x
+// traversal (c = 9 dz + 3 dy + dx), walks its members in decreasing index, and a warp scan
+// of the per-cell counts gives each lane its offset in the site's list. Brute-force path:
+// the warp strides over the supercell in ascending order and compacts with a ballot.
+template <bool FILL>
+__global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int *site_struct,
+                                                    const StructDesc *sd, const double *pos_sc,
+                                                    const int *cell_start, const int *cell_atoms,
+                                                    int64_t *counts, const int64_t *start, int *list,
+                                                    int *check)
+{
+    const int lane = threadIdx.x & 31;
+    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= n_atoms_total) return;
-    const StructDesc S = sd[site_struct[g]];
+    const StructDesc &S = sd[site_struct[g]];
     const int i = g - S.atom_off + 1;  // 1-based local site
     const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
     const double rc = S.rcut;
-    int64_t w = FILL ? start[g] : 0;
+    const int64_t w0 = FILL ? start[g] : 0;
     const int64_t w_end = FILL ? start[g + 1] : 0;
     // the fill pass repeats the count pass, so it never reaches w_end; checked all the same
-    auto put = [&](int v) {
+    auto put = [&](int64_t w, int v) {
         if (w < w_end)
             list[w] = v;
         else
             check_fail(check, kCheckListOverrun, g, v);
-        ++w;
     };
-    int64_t n = 1;
-    if (FILL) put(i);
+    if (FILL && lane == 0) put(w0, i);
     if (S.cell_off >= 0) {
         int i2, j2, k2, lin;
         cell_of(pi, S, &i2, &j2, &k2, &lin);
         const int mx = S.mx, my = S.my, mz = S.mz;
-        for (int k3 = k2 - 1; k3 <= k2 + 1; ++k3) {
-            if (mz == 1 && k3 != 1) continue;
-            if (mz == 2 && k2 == 1 && k3 == 0) continue;
-            if (mz == 2 && k2 == 2 && k3 == 3) continue;
-            for (int j3 = j2 - 1; j3 <= j2 + 1; ++j3) {
-                if (my == 1 && j3 != 1) continue;
-                if (my == 2 && j2 == 1 && j3 == 0) continue;
-                if (my == 2 && j2 == 2 && j3 == 3) continue;
-                for (int i3 = i2 - 1; i3 <= i2 + 1; ++i3) {
-                    if (mx == 1 && i3 != 1) continue;
-                    if (mx == 2 && i2 == 1 && i3 == 0) continue;
-                    if (mx == 2 && i2 == 2 && i3 == 3) continue;
-                    int c = S.cell_off + i_modulo(i3 - 1, mx) + i_modulo(j3 - 1, my) * mx +
-                            i_modulo(k3 - 1, mz) * mx * my;
-                    for (int t = cell_start[c]; t < cell_start[c + 1]; ++t) {
-                        int k = cell_atoms[t];
-                        if (k == i) continue;
-                        double dist[3], d;
-                        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
-                        if (d < rc) {
-                            if (FILL) put(k);
-                            ++n;
-                        }
-                    }
-                }
+        int c = -1;
+        if (lane < 27) {
+            const int k3 = k2 - 1 + lane / 9, j3 = j2 - 1 + (lane / 3) % 3, i3 = i2 - 1 + lane % 3;
+            const bool skip = (mz == 1 && k3 != 1) || (mz == 2 && k2 == 1 && k3 == 0) ||
+                              (mz == 2 && k2 == 2 && k3 == 3) || (my == 1 && j3 != 1) ||
+                              (my == 2 && j2 == 1 && j3 == 0) || (my == 2 && j2 == 2 && j3 == 3) ||
+                              (mx == 1 && i3 != 1) || (mx == 2 && i2 == 1 && i3 == 0) ||
+                              (mx == 2 && i2 == 2 && i3 == 3);
+            if (!skip)
+                c = S.cell_off + i_modulo(i3 - 1, mx) + i_modulo(j3 - 1, my) * mx + i_modulo(k3 - 1, mz) * mx * my;
+        }
+        const int t0 = c >= 0 ? cell_start[c] : 0, t1 = c >= 0 ? cell_start[c + 1] : 0;
+        int cnt = 0;
+        for (int t = t0; t < t1; ++t) {
+            const int k = cell_atoms[t];
+            if (k == i) continue;
+            double dist[3], d;
+            get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
+            if (d < rc) ++cnt;
+        }
+        int incl = cnt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int v = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += v;
+        }
+        if (!FILL) {
+            const int total = __shfl_sync(0xffffffffu, incl, 31);
+            if (lane == 0) counts[g] = 1 + total;
+        } else {
+            int64_t w = w0 + 1 + (incl - cnt);
+            for (int t = t0; t < t1; ++t) {
+                const int k = cell_atoms[t];
+                if (k == i) continue;
+                double dist[3], d;
+                get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
+                if (d < rc) put(w++, k);
             }
         }
     } else {
-        for (int j = 1; j <= S.n_sc; ++j) {
-            if (j == i) continue;
-            double dist[3], d;
-            get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
-            if (d < rc) {
-                if (FILL) put(j);
-                ++n;
+        int64_t w = w0 + 1, n = 1;
+        for (int jb = 1; jb <= S.n_sc; jb += 32) {
+            const int j = jb + lane;
+            bool ok = false;
+            if (j <= S.n_sc && j != i) {
+                double dist[3], d;
+                get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
+                ok = d < rc;
             }
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            if (FILL && ok) put(w + __popc(m & nb_lanemask_lt()), j);
+            w += __popc(m);
+            n += __popc(m);
         }
+        if (!FILL && lane == 0) counts[g] = n;
     }
-    if (!FILL) counts[g] = n;
 }
 
 // Geometry of every pair (neighbors_interface.f90:467-510); angles only when requested.
@@ -224,13 +254,14 @@ __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const
                                 const int *list, double *rjs, double *xyz, double *thetas,
                                 double *phis, int *nspecies, int *jatom)
 {
-    int g = blockIdx.x;
+    // one warp per site
+    const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= n_atoms_total) return;
     const StructDesc &S = sd[site_struct[g]];
     const int i = g - S.atom_off + 1;
     const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
     const int64_t b = start[g], e = start[g + 1];
-    for (int64_t k = b + threadIdx.x; k < e; k += blockDim.x) {
+    for (int64_t k = b + (threadIdx.x & 31); k < e; k += 32) {
         int j = list[k];
         if (jatom) jatom[k] = S.atom_off + (j - 1) % S.n;
         if (nspecies) nspecies[k] = species_sc[S.sc_off + j - 1];
@@ -359,8 +390,7 @@ int make_struct_desc(const double a[3], const double b[3], const double c[3], in
     return TGAP_OK;
 }
 
-int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
-                    int64_t *n_pairs_out, bool with_angles)
+int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out)
 {
     const int n = nb->n_atoms;
     if (n <= 0) {
@@ -369,60 +399,75 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
     }
     const int T = 128;
     const int grid = (n + T - 1) / T;
+    const int wgrid = (n + T / 32 - 1) / (T / 32);  // one warp per site
     StructDesc *d_sd = nb->d_structs.as<StructDesc>();
-    if (rebuild) {
-        StageScope sc(ctx, "neighbors_rebuild");
-        // cells
-        if (nb->n_cells > 0) {
-            TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_count.ptr, 0, sizeof(int) * (nb->n_cells + 1), ctx->stream));
-            k_cell_count<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd,
-                                                      nb->pos_sc.as<double>(), nb->atom_cell.as<int>(),
-                                                      nb->cell_count.as<int>());
-            TGAP_LAUNCH_CHECK(ctx);
-            int rc = scan_i32(ctx, nb->scan_tmp, nb->cell_count.as<int>(), nb->cell_start.as<int>(),
-                              nb->n_cells + 1);
-            if (rc) return rc;
-            TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_cursor.ptr, 0, sizeof(int) * nb->n_cells, ctx->stream));
-            k_cell_fill<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd,
-                                                     nb->atom_cell.as<int>(), nb->cell_start.as<int>(),
-                                                     nb->cell_cursor.as<int>(), nb->cell_atoms.as<int>());
-            TGAP_LAUNCH_CHECK(ctx);
-            k_cell_sort<<<(nb->n_cells + T - 1) / T, T, 0, ctx->stream>>>(
-                nb->n_cells, nb->cell_start.as<int>(), nb->cell_atoms.as<int>());
-            TGAP_LAUNCH_CHECK(ctx);
-        }
-        k_site_pairs<false><<<grid, T, 0, ctx->stream>>>(
-            n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
-            nb->cell_atoms.as<int>(), nb->counts.as<int64_t>(), nullptr, nullptr, nullptr);
+    StageScope sc(ctx, "neighbors_rebuild");
+    // cells
+    if (nb->n_cells > 0) {
+        TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_count.ptr, 0, sizeof(int) * (nb->n_cells + 1), ctx->stream));
+        k_cell_count<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
+                                                  nb->atom_cell.as<int>(), nb->cell_count.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
-        TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
-        int rc = scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
+        int rc = scan_i32(ctx, nb->scan_tmp, nb->cell_count.as<int>(), nb->cell_start.as<int>(), nb->n_cells + 1);
         if (rc) return rc;
-        int64_t total = 0;
-        TGAP_CUDA(ctx, cudaMemcpyAsync(&total, nb->start.as<int64_t>() + n, sizeof(int64_t),
-                                       cudaMemcpyDeviceToHost, ctx->stream));
-        TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-        *n_pairs_out = total;
-        if (capacity >= 0 && total > capacity) return TGAP_ERR_CAPACITY;
-        if (nb->ensure_pairs(total)) return set_error(ctx, TGAP_ERR_NOMEM, "pair arrays");
-        nb->n_pairs = total;
-        k_nneigh_from_counts<<<grid, T, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->n_neigh.as<int>());
+        TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_cursor.ptr, 0, sizeof(int) * nb->n_cells, ctx->stream));
+        k_cell_fill<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->atom_cell.as<int>(),
+                                                 nb->cell_start.as<int>(), nb->cell_cursor.as<int>(),
+                                                 nb->cell_atoms.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
-        k_site_pairs<true><<<grid, T, 0, ctx->stream>>>(
-            n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
-            nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(), nb->list.as<int>(), ctx->d_check);
+        k_cell_sort<<<(nb->n_cells + T - 1) / T, T, 0, ctx->stream>>>(nb->n_cells, nb->cell_start.as<int>(),
+                                                                      nb->cell_atoms.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
+    }
+    k_site_pairs<false><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
+                                                      nb->cell_start.as<int>(), nb->cell_atoms.as<int>(),
+                                                      nb->counts.as<int64_t>(), nullptr, nullptr, nullptr);
+    TGAP_LAUNCH_CHECK(ctx);
+    TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
+    int rc = scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
+    if (rc) return rc;
+    int64_t total = 0;
+    TGAP_CUDA(ctx, cudaMemcpyAsync(&total, nb->start.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost,
+                                   ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    *n_pairs_out = total;
+    if (capacity >= 0 && total > capacity) return TGAP_ERR_CAPACITY;
+    if (nb->ensure_pairs(total)) return set_error(ctx, TGAP_ERR_NOMEM, "pair arrays");
+    nb->n_pairs = total;
+    k_nneigh_from_counts<<<grid, T, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->n_neigh.as<int>());
+    TGAP_LAUNCH_CHECK(ctx);
+    k_site_pairs<true><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
+                                                     nb->cell_start.as<int>(), nb->cell_atoms.as<int>(), nullptr,
+                                                     nb->start.as<int64_t>(), nb->list.as<int>(), ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles)
+{
+    const int n = nb->n_atoms;
+    if (n <= 0) return TGAP_OK;
+    const int T = 128;
+    StageScope sc(ctx, "neighbors_geometry");
+    k_pair_geometry<<<(n + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+        n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(), nb->pos_sc.as<double>(),
+        nb->species_sc.as<int>(), nb->start.as<int64_t>(), nb->list.as<int>(), nb->rjs.as<double>(),
+        nb->xyz.as<double>(), with_angles ? nb->thetas.as<double>() : nullptr,
+        with_angles ? nb->phis.as<double>() : nullptr, nb->nspecies.as<int>(), nb->jatom.as<int>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
+                    int64_t *n_pairs_out, bool with_angles)
+{
+    if (rebuild) {
+        const int rc = neighbors_rebuild_lists(ctx, nb, capacity, n_pairs_out);
+        if (rc) return rc;
     } else {
         *n_pairs_out = nb->n_pairs;
     }
-    StageScope sc(ctx, "neighbors_geometry");
-    k_pair_geometry<<<n, 64, 0, ctx->stream>>>(
-        n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(), nb->species_sc.as<int>(),
-        nb->start.as<int64_t>(), nb->list.as<int>(), nb->rjs.as<double>(), nb->xyz.as<double>(),
-        with_angles ? nb->thetas.as<double>() : nullptr, with_angles ? nb->phis.as<double>() : nullptr,
-        nb->nspecies.as<int>(), nb->jatom.as<int>());
-    TGAP_LAUNCH_CHECK(ctx);
-    return TGAP_OK;
+    return neighbors_geometry(ctx, nb, with_angles);
 }
 
 // Start offsets from a caller-provided n_neigh (geometry-only refresh of a given list).
@@ -438,7 +483,10 @@ int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb)
 
 int NeighborBatch::ensure_pairs(int64_t P)
 {
+    // a quarter of headroom: the pair count of a running simulation fluctuates, and every
+    // reallocation synchronizes the device and invalidates captured graphs
     size_t p = (size_t)(P > 0 ? P : 1);
+    if (!list.ptr || p * sizeof(int) > list.bytes) p += p / 4 + 256;
     if (list.ensure(p * sizeof(int))) return 1;
     if (rjs.ensure(p * sizeof(double))) return 1;
     if (xyz.ensure(3 * p * sizeof(double))) return 1;

@@ -68,8 +68,11 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
                               const double *positions_sc, const double a[3], const double b[3],
                               const double c[3], int box_small, double rcut,
                               const int *species_sc);
+// Rebuild the pair lists (one host synchronization for the pair count), then the geometry.
 int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
                     int64_t *n_pairs_out, bool with_angles);
+int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out);
+int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles);
 int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_sync_positions(tgap_context *ctx, NeighborBatch *nb);
 
