@@ -779,9 +779,10 @@ extern "C" int tgap_system_update(tgap_system *s, int rebuild)
     if (!s) return TGAP_ERR_ARGUMENT;
     tgap_context *ctx = s->ctx;
     CHECK_RC(activate(ctx));
+    if (!rebuild) return neighbors_refresh(ctx, &s->nb);
     CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
     int64_t P = 0;
-    CHECK_RC(neighbors_build(ctx, &s->nb, rebuild, -1, &P, false));
+    CHECK_RC(neighbors_build(ctx, &s->nb, 1, -1, &P, false));
     return TGAP_OK;
 }
 
@@ -1083,9 +1084,7 @@ static int md_eval(tgap_md *md)
 static int md_step_body(tgap_md *md)
 {
     tgap_context *ctx = md->ctx;
-    CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
-    int64_t P = 0;
-    CHECK_RC(neighbors_build(ctx, &md->sys->nb, 0, -1, &P, false));
+    CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     CHECK_RC(md_eval(md));
     CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
                              md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),

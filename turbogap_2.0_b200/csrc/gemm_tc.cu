@@ -145,14 +145,18 @@ template <int ZI> __device__ __forceinline__ float kpow_zm1(float k, float zeta)
     else return powf(k, zeta - 1.0f);
 }
 
-// GEMM1: per element k = K[row][s]: energy partial alpha_s k^zeta, G = zd2 alpha_s k^(zeta-1)
-// written as a bf16 hi/lo split.
+// GEMM1: per element k = K[row][s]: energy alpha_s k^zeta summed over the row's columns and
+// added (scaled by delta^2) into the row's atom, and G = zd2 alpha_s k^(zeta-1) written as a
+// bf16 hi/lo split.
 struct EpiKernelGap {
     const float *alphas;         // [m_pad]
     __nv_bfloat16 *G_hi, *G_lo;  // [rows_pad][ldg]
     int ldg;
-    double *e_part;              // [n_parts][rows_pad]
-    int rows_pad;
+    int n_rows;                  // rows past n_rows are padding
+    const int *sites;            // row -> atom (null: identity)
+    double *energies;            // energies[atom] += delta^2 sum_s alpha_s k^zeta (+ e0 once)
+    double *e_rows;              // optional per-row copy (zeroed by the caller)
+    double d2, e0;
     float zd2, zeta;
     int zeta_int;                // 1..6, or -1 for a non-integer zeta
 
@@ -201,9 +205,14 @@ struct EpiKernelGap {
         default: chunk_z<-1>(row, col, v, acc); break;
         }
     }
+    // part = 2 tile_n + half: each row receives one partial per tile column half
     __device__ __forceinline__ void end(int row, int part, float acc) const
     {
-        e_part[(size_t)part * rows_pad + row] = (double)acc;
+        if (row >= n_rows) return;
+        double e = d2 * (double)acc;
+        if (part == 0) e += e0;
+        if (energies) atomicAdd(energies + (sites ? sites[row] : row), e);
+        if (e_rows) atomicAdd(e_rows + row, e);
     }
 };
 
@@ -531,19 +540,6 @@ int model_upload_mixed(tgap_context *ctx, DeviceModel *m)
     return TGAP_OK;
 }
 
-__global__ void k_energy_reduce_ld(int M, int n_tiles, int ld, const double *__restrict__ e_part, double d2,
-                                   double e0, const int *__restrict__ sites, double *__restrict__ e_rows,
-                                   double *__restrict__ energies)
-{
-    const int r = blockIdx.x * blockDim.x + threadIdx.x;
-    if (r >= M) return;
-    double s = 0.0;
-    for (int t = 0; t < n_tiles; ++t) s += e_part[(size_t)t * ld + r];
-    const double e = d2 * s + e0;
-    if (e_rows) e_rows[r] = e;
-    if (energies) energies[sites ? sites[r] : r] += e;
-}
-
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces, GapWork *w,
                           const int *d_sites, double *d_e_rows, double *d_energies)
@@ -551,31 +547,30 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     if (n_rows <= 0) return TGAP_OK;
     constexpr int BN1 = 128;
     const int rows_pad = (n_rows + kBM - 1) / kBM * kBM;
-    const int n_parts = 2 * (m.m_pad / BN1);  // one energy partial per tile column half
     if (m.dim_pad % 128 || m.m_pad % BN1 || m.dim_pad % kBK || m.m_pad % kBK)
         return set_error(ctx, TGAP_ERR_ARGUMENT, "mixed GEMM padding");
-    if (w->e_part.ensure(sizeof(double) * (size_t)n_parts * rows_pad) ||
-        w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad) ||
+    if (w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad) ||
         (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad)))
         return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
+    if (d_e_rows) TGAP_CUDA(ctx, cudaMemsetAsync(d_e_rows, 0, sizeof(double) * (size_t)n_rows, ctx->stream));
     const bool zi = std::fabs(m.zeta - (double)(int)m.zeta) < 1.0e-5;  // gap.f90:99-105
     EpiKernelGap e1;
     e1.alphas = m.alphas32.as<float>();
     e1.G_hi = w->G_hi.as<__nv_bfloat16>();
     e1.G_lo = w->G_lo.as<__nv_bfloat16>();
     e1.ldg = m.m_pad;
-    e1.e_part = w->e_part.as<double>();
-    e1.rows_pad = rows_pad;
+    e1.n_rows = n_rows;
+    e1.sites = d_sites;
+    e1.energies = d_energies;
+    e1.e_rows = d_e_rows;
+    e1.d2 = m.delta * m.delta;
+    e1.e0 = e0;
     e1.zeta_int = zi ? (int)m.zeta : -1;
     e1.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
     e1.zd2 = (float)(e1.zeta * m.delta * m.delta);
-    int rc = launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr, rows_pad, m.m_pad,
-                                               m.dim_pad, e1);
+    int rc = launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr, rows_pad,
+                                               m.m_pad, m.dim_pad, e1);
     if (rc) return rc;
-    k_energy_reduce_ld<<<(n_rows + 127) / 128, 128, 0, ctx->stream>>>(n_rows, n_parts, rows_pad,
-                                                                       w->e_part.as<double>(), m.delta * m.delta,
-                                                                       e0, d_sites, d_e_rows, d_energies);
-    TGAP_LAUNCH_CHECK(ctx);
     if (!do_forces) return TGAP_OK;
     // dE/dq: N = dim_pad is small, so 96-column tiles (when they divide it) give more tiles to
     // spread over the SMs than 128-column ones

@@ -88,6 +88,22 @@ __device__ void get_distance_dev(const double *pi, const double *pj, const Struc
     *d = sqrt(dot3(dist, dist));
 }
 
+// Position of supercell atom j (1-based within structure S) from the primitive positions, with
+// the replication arithmetic of set_supercell (read_xyz.f90:331-345: replicas a -> b -> c outer,
+// atoms inner; no contraction in this file).
+__device__ __forceinline__ void sc_position(const StructDesc &S, const double *pos, int j, double out[3])
+{
+    const int a = (j - 1) % S.n, r = (j - 1) / S.n;
+    const int k2 = r % S.rep[2], j2 = (r / S.rep[2]) % S.rep[1], i2 = r / (S.rep[2] * S.rep[1]);
+    const double *p = pos + 3 * (size_t)(S.atom_off + a);
+    for (int q = 0; q < 3; ++q) {
+        double v = p[q] + (double)i2 * S.pa[q];
+        v = v + (double)j2 * S.pb[q];
+        v = v + (double)k2 * S.pc[q];
+        out[q] = v;
+    }
+}
+
 // Cell coordinates (1-based i2, j2, k2) and the linear cell index of a position.
 __device__ void cell_of(const double *pos, const StructDesc &S, int *i2, int *j2, int *k2,
                         int *lin)
@@ -133,20 +149,25 @@ __global__ void k_cell_fill(int n_atoms_total, const int *site_struct, const Str
     cell_atoms[cell_start[c] + slot] = g - S.atom_off + 1;  // 1-based local index
 }
 
-// Sort each cell's members in decreasing index (the LIFO order of the linked list).
-__global__ void k_cell_sort(int n_cells, const int *cell_start, int *cell_atoms)
+// Each cell's members (in cell_tmp, in arrival order) written to cell_atoms in decreasing index,
+// the LIFO order of the reference linked list. One warp per cell: a member's slot is the number
+// of members with a larger index.
+__global__ void k_cell_sort(int n_cells, const int *cell_start, const int *cell_tmp, int *cell_atoms)
 {
-    int c = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int c = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (c >= n_cells) return;
-    int b = cell_start[c], e = cell_start[c + 1];
-    for (int i = b + 1; i < e; ++i) {
-        int v = cell_atoms[i];
-        int j = i - 1;
-        while (j >= b && cell_atoms[j] < v) {
-            cell_atoms[j + 1] = cell_atoms[j];
-            --j;
+    const int b = cell_start[c], e = cell_start[c + 1];
+    for (int t0 = b; t0 < e; t0 += 32) {
+        const int t = t0 + lane;
+        const int v = t < e ? cell_tmp[t] : 0;
+        int rank = 0;
+        for (int u0 = b; u0 < e; u0 += 32) {
+            const int w = u0 + lane < e ? cell_tmp[u0 + lane] : 0;
+            const int m = e - u0 < 32 ? e - u0 : 32;
+            for (int q = 0; q < m; ++q) rank += __shfl_sync(0xffffffffu, w, q) > v ? 1 : 0;
         }
-        cell_atoms[j + 1] = v;
+        if (t < e) cell_atoms[b + rank] = v;
     }
 }
 
@@ -248,10 +269,13 @@ __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int
     }
 }
 
-// Geometry of every pair (neighbors_interface.f90:467-510); angles only when requested.
+// Geometry of every pair (neighbors_interface.f90:467-510); angles only when requested. With
+// FROM_POS the supercell positions are formed from the primitive ones on the fly (no replicate
+// pass; only for batches whose supercells are pure replicas).
+template <bool FROM_POS>
 __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const StructDesc *sd,
-                                const double *pos_sc, const int *species_sc, const int64_t *start,
-                                const int *list, double *rjs, double *xyz, double *thetas,
+                                const double *pos_sc, const double *pos, const int *species_sc,
+                                const int64_t *start, const int *list, double *rjs, double *xyz, double *thetas,
                                 double *phis, int *nspecies, int *jatom)
 {
     // one warp per site
@@ -259,7 +283,12 @@ __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const
     if (g >= n_atoms_total) return;
     const StructDesc &S = sd[site_struct[g]];
     const int i = g - S.atom_off + 1;
+    double pi_buf[3];
     const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
+    if (FROM_POS) {
+        sc_position(S, pos, i, pi_buf);
+        pi = pi_buf;
+    }
     const int64_t b = start[g], e = start[g + 1];
     for (int64_t k = b + (threadIdx.x & 31); k < e; k += 32) {
         int j = list[k];
@@ -272,8 +301,14 @@ __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const
             if (phis) phis[k] = 0.0;
             continue;
         }
+        double pj_buf[3];
+        const double *pj = pos_sc + 3 * (size_t)(S.sc_off + j - 1);
+        if (FROM_POS) {
+            sc_position(S, pos, j, pj_buf);
+            pj = pj_buf;
+        }
         double dist[3], d;
-        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + j - 1), S, dist, &d);
+        get_distance_dev(pi, pj, S, dist, &d);
         rjs[k] = d;
         xyz[3 * k] = dist[0];
         xyz[3 * k + 1] = dist[1];
@@ -413,10 +448,10 @@ int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capaci
         TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_cursor.ptr, 0, sizeof(int) * nb->n_cells, ctx->stream));
         k_cell_fill<<<grid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->atom_cell.as<int>(),
                                                  nb->cell_start.as<int>(), nb->cell_cursor.as<int>(),
-                                                 nb->cell_atoms.as<int>());
+                                                 nb->cell_tmp.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
-        k_cell_sort<<<(nb->n_cells + T - 1) / T, T, 0, ctx->stream>>>(nb->n_cells, nb->cell_start.as<int>(),
-                                                                      nb->cell_atoms.as<int>());
+        k_cell_sort<<<(nb->n_cells + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+            nb->n_cells, nb->cell_start.as<int>(), nb->cell_tmp.as<int>(), nb->cell_atoms.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
     }
     k_site_pairs<false><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
@@ -443,19 +478,27 @@ int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capaci
     return TGAP_OK;
 }
 
-int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles)
+int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, bool from_positions)
 {
     const int n = nb->n_atoms;
     if (n <= 0) return TGAP_OK;
     const int T = 128;
     StageScope sc(ctx, "neighbors_geometry");
-    k_pair_geometry<<<(n + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+    auto kern = from_positions ? k_pair_geometry<true> : k_pair_geometry<false>;
+    kern<<<(n + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
         n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(), nb->pos_sc.as<double>(),
-        nb->species_sc.as<int>(), nb->start.as<int64_t>(), nb->list.as<int>(), nb->rjs.as<double>(),
-        nb->xyz.as<double>(), with_angles ? nb->thetas.as<double>() : nullptr,
+        nb->positions.as<double>(), nb->species_sc.as<int>(), nb->start.as<int64_t>(), nb->list.as<int>(),
+        nb->rjs.as<double>(), nb->xyz.as<double>(), with_angles ? nb->thetas.as<double>() : nullptr,
         with_angles ? nb->phis.as<double>() : nullptr, nb->nspecies.as<int>(), nb->jatom.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
+}
+
+int neighbors_refresh(tgap_context *ctx, NeighborBatch *nb)
+{
+    if (nb->replicated) return neighbors_geometry(ctx, nb, false, true);
+    const int rc = neighbors_sync_positions(ctx, nb);
+    return rc ? rc : neighbors_geometry(ctx, nb, false, false);
 }
 
 int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
@@ -467,7 +510,7 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
     } else {
         *n_pairs_out = nb->n_pairs;
     }
-    return neighbors_geometry(ctx, nb, with_angles);
+    return neighbors_geometry(ctx, nb, with_angles, false);
 }
 
 // Start offsets from a caller-provided n_neigh (geometry-only refresh of a given list).
@@ -563,6 +606,7 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
     }
     nb->n_structures = n_structures;
     nb->n_atoms = offsets[n_structures];
+    nb->replicated = true;  // supercells built here are replicas of the primitive cells
     nb->n_sc_total = sc_total;
     nb->n_cells = n_cells;
     nb->host_structs = sd;
@@ -574,7 +618,8 @@ int neighbors_setup(tgap_context *ctx, NeighborBatch *nb, int n_structures, cons
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
-        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
+        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->cell_tmp.ensure(sizeof(int) * (N + 1)) ||
+        nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
         nb->start.ensure(sizeof(int64_t) * (N + 1)) || nb->n_neigh.ensure(sizeof(int) * N) ||
         nb->positions.ensure(sizeof(double) * 3 * N))
         return set_error(ctx, TGAP_ERR_NOMEM, "neighbor set-up");
@@ -600,19 +645,8 @@ __global__ void k_replicate(int n_atoms_total, const int *site_struct, const Str
     if (g >= n_atoms_total) return;
     const StructDesc &S = sd[site_struct[g]];
     const int i = g - S.atom_off;
-    // lattice vectors of the primitive cell = supercell vectors / replicas
-    int r = 0;
-    for (int i2 = 0; i2 < S.rep[0]; ++i2)
-        for (int j2 = 0; j2 < S.rep[1]; ++j2)
-            for (int k2 = 0; k2 < S.rep[2]; ++k2, ++r) {
-                double *o = pos_sc + 3 * (size_t)(S.sc_off + r * S.n + i);
-                for (int q = 0; q < 3; ++q) {
-                    double v = pos[3 * (size_t)g + q] + (double)i2 * S.pa[q];
-                    v = v + (double)j2 * S.pb[q];
-                    v = v + (double)k2 * S.pc[q];
-                    o[q] = v;
-                }
-            }
+    const int reps = S.rep[0] * S.rep[1] * S.rep[2];
+    for (int r = 0; r < reps; ++r) sc_position(S, pos, r * S.n + i + 1, pos_sc + 3 * (size_t)(S.sc_off + r * S.n + i));
 }
 
 int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites, int n_sc,
@@ -637,6 +671,7 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
     int n_cells = S.cell_off >= 0 ? S.mx * S.my * S.mz : 0;
     nb->n_structures = 1;
     nb->n_atoms = n_sites;
+    nb->replicated = false;  // caller-given supercell: pos_sc is the source of truth
     nb->n_sc_total = n_sc;
     nb->n_cells = n_cells;
     nb->host_structs.assign(1, S);
@@ -648,7 +683,8 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
         nb->cell_count.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_start.ensure(sizeof(int) * (n_cells + 1)) ||
         nb->cell_cursor.ensure(sizeof(int) * (n_cells + 1)) ||
-        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
+        nb->cell_atoms.ensure(sizeof(int) * (N + 1)) || nb->cell_tmp.ensure(sizeof(int) * (N + 1)) ||
+        nb->counts.ensure(sizeof(int64_t) * (N + 1)) ||
         nb->start.ensure(sizeof(int64_t) * (N + 1)) || nb->n_neigh.ensure(sizeof(int) * N) ||
         nb->positions.ensure(sizeof(double) * 3 * N))
         return set_error(ctx, TGAP_ERR_NOMEM, "neighbor set-up");

@@ -30,13 +30,14 @@ struct NeighborBatch {
     int n_sc_total = 0;
     int n_cells = 0;
     int64_t n_pairs = 0;
+    bool replicated = true;  // every supercell is a pure replica of its primitive cell
     std::vector<StructDesc> host_structs;
     DevBuf d_structs;
     DevBuf positions;       // double [3 n_atoms] (primitive cells; MD state)
     DevBuf pos_sc;          // double [3 n_sc_total]
     DevBuf species_sc;      // int [n_sc_total]
     DevBuf site_struct;     // int [n_atoms]
-    DevBuf atom_cell, cell_count, cell_start, cell_cursor, cell_atoms;
+    DevBuf atom_cell, cell_count, cell_start, cell_cursor, cell_atoms, cell_tmp;
     DevBuf counts;          // int64 [n_atoms + 1]
     DevBuf start;           // int64 [n_atoms + 1]
     DevBuf n_neigh;         // int [n_atoms]
@@ -49,7 +50,7 @@ struct NeighborBatch {
     void release_all()
     {
         DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &atom_cell,
-                          &cell_count, &cell_start, &cell_cursor, &cell_atoms, &counts, &start,
+                          &cell_count, &cell_start, &cell_cursor, &cell_atoms, &cell_tmp, &counts, &start,
                           &n_neigh, &list, &rjs, &xyz, &thetas, &phis, &nspecies, &jatom,
                           &scan_tmp};
         for (DevBuf *b : bufs) b->release();
@@ -72,7 +73,10 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
 int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
                     int64_t *n_pairs_out, bool with_angles);
 int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out);
-int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles);
+// from_positions: form supercell positions from the primitive ones inside the kernel
+int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, bool from_positions);
+// Geometry of the current lists at the current (primitive) positions.
+int neighbors_refresh(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_sync_positions(tgap_context *ctx, NeighborBatch *nb);
 

@@ -425,18 +425,29 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
         cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
     __syncwarp();
     for (int o = lane; o < nout; o += 32) c_out[(size_t)row * nout + o] = cs[o];
-    // power spectrum into the (now free) angular area
+    // power spectrum into the (now free) angular area: lane owns the (n, n') pairs
+    // pp = lane + 32 i (n-major, n <= n') and every l, component d = pp (L + 1) + l
     T *ps = As;
     T part = 0;
-    for (int d = lane; d < dim; d += 32) {
-        int n, np, l;
-        ps_decode_w(d, nmax, L, &n, &np, &l);
+    const int npair = nmax * (nmax + 1) / 2;
+    for (int pp = lane; pp < npair; pp += 32) {
+        int n = 0, rem = pp;
+        while (rem >= nmax - n) {
+            rem -= nmax - n;
+            ++n;
+        }
+        const int np = n + rem;
         const T *a = cs + n * NLM, *b = cs + np * NLM;
-        T acc = 0;
-        for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
-        const T v = (n == np) ? acc : acc * (T)1.4142135623730951;
-        ps[d] = v;
-        part += v * v;
+        const T sc = (n == np) ? (T)1 : (T)1.4142135623730951;
+#pragma unroll
+        for (int l = 0; l <= L; ++l) {
+            T acc = 0;
+#pragma unroll
+            for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
+            const T v = acc * sc;
+            ps[pp * (L + 1) + l] = v;
+            part += v * v;
+        }
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
@@ -566,12 +577,16 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
                 ylm_all_grad<T, L>(Yc, u0, u1, u2, [&](int kk, int l, T y, T gx, T gy, T gz) {
                     T gv[AMB];
                     load_vec<T, AMB>(Gs + kk * AMB, gv);
-                    T U = 0, V = 0;
+                    // two interleaved chains each for U and V (shorter dependency chains)
+                    T U0 = 0, U1 = 0, V0 = 0, V1 = 0;
 #pragma unroll
-                    for (int e = 0; e < AMB; ++e) {
-                        U += gv[e] * R[e];
-                        V += gv[e] * dR[e];
+                    for (int e = 0; e < AMB; e += 2) {
+                        U0 += gv[e] * R[e];
+                        V0 += gv[e] * dR[e];
+                        U1 += gv[e + 1] * R[e + 1];
+                        V1 += gv[e + 1] * dR[e + 1];
                     }
+                    const T U = U0 + U1, V = V0 + V1;
                     const T a = f[l] * V + df[l] * U;
                     const T b = U * f[l] * ir;
                     const T ug = u0 * gx + u1 * gy + u2 * gz;
