@@ -237,33 +237,63 @@ def _stage_profile(tg, ctx, system, model, masses, vel, precision, steps=20):
     return out
 
 
-def _roofline(stages, n_rows, dim, dim_pad, n_sparse, n_sparse_pad, n_pairs, peaks):
-    """Roofline of the dominant kernel: algorithmic work per launch / measured launch time."""
-    if not stages:
-        return None
-    total = sum(v["total_ms"] for v in stages.values())
-    name, st = max(stages.items(), key=lambda kv: kv[1]["total_ms"])
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # B200 CUDA-core FP32, nominal (not measured)
+
+
+def _stage_roofline(name, st, total_ms, n_rows, dim, dim_pad, n_sparse, n_sparse_pad, n_pairs, n_cut, peaks,
+                    alpha=8, l_max=8):
+    """Roofline of one stage: algorithmic work per launch / measured launch time (CUDA events).
+
+    GEMMs: 2 N D M flops against the sustained bf16 peak (the bf16x3 split executes 3x that).
+    Descriptor kernels: the contract's HBM figure from algorithmic bytes, and beside it the FP32
+    figure that actually bounds them, 4 alpha K_l (forward) or 12 alpha K_l (adjoint) flops per
+    in-cutoff pair with K_l = (l+1)(l+2)/2, against the nominal FP32 peak.
+    """
     t = st["avg_us"] * 1e-6
     traffic = _ncu_traffic(name)
-    nlm, nmax = 81, 8
+    share = st["total_ms"] / total_ms
+    nlm, nmax = (l_max + 1) ** 2, alpha
     if name.startswith("gemm_bf16x3"):
         flops = 2.0 * n_rows * dim * n_sparse
         ach = flops / t / 1e12
         return dict(kernel=name, bound="tensor", achieved=ach, peak=peaks["bf16_sus"], unit="TFLOP/s",
-                    frac=ach / peaks["bf16_sus"], traffic=traffic, share=st["total_ms"] / total,
+                    frac=ach / peaks["bf16_sus"], traffic=traffic, share=share, avg_us=st["avg_us"],
                     executed_tflops=3.0 * 2.0 * n_rows * dim_pad * n_sparse_pad / t / 1e12,
                     peak_source=peaks["src"] + " sustained bf16")
+    kl = (l_max + 1) * (l_max + 2) // 2
+    fp32 = None
     if name.startswith("soap_forward"):
         # reads the pair list (xyz, r, species: 36 B/pair), writes c, q (+bf16 split), |p|
         byts = 36.0 * n_pairs + n_rows * (4.0 * nmax * nlm + 8.0 * dim_pad + 4.0)
+        fp32 = 4.0 * alpha * kl * n_cut
     elif name.startswith("soap_backward"):
         # reads pairs (+ neighbor index), c, q, g; scatters 3 FP64 forces per pair
         byts = 40.0 * n_pairs + 24.0 * n_pairs + n_rows * (4.0 * nmax * nlm + 8.0 * dim_pad + 4.0)
+        fp32 = 12.0 * alpha * kl * n_cut
     else:
         byts = 48.0 * n_pairs
     ach = byts / t / 1e9
-    return dict(kernel=name, bound="hbm", achieved=ach, peak=peaks["hbm"], unit="GB/s", frac=ach / peaks["hbm"],
-                traffic=traffic, share=st["total_ms"] / total, peak_source=peaks["src"] + " HBM copy")
+    out = dict(kernel=name, bound="hbm", achieved=ach, peak=peaks["hbm"], unit="GB/s", frac=ach / peaks["hbm"],
+               traffic=traffic, share=share, avg_us=st["avg_us"], peak_source=peaks["src"] + " HBM copy")
+    if fp32 is not None:
+        a32 = fp32 / t / 1e12
+        out["fp32"] = dict(achieved=a32, peak=FP32_NOMINAL_TFLOPS, unit="TFLOP/s", frac=a32 / FP32_NOMINAL_TFLOPS,
+                           peak_source="nominal 148 SM x 128 lanes x 2 x 1.965 GHz", in_cutoff_pairs=n_cut)
+    return out
+
+
+def _roofline(stages, n_rows, dim, dim_pad, n_sparse, n_sparse_pad, n_pairs, n_cut, peaks):
+    """Roofline of the dominant stage, plus every stage's in `all`."""
+    if not stages:
+        return None
+    total = sum(v["total_ms"] for v in stages.values())
+    rows = {k: _stage_roofline(k, v, total, n_rows, dim, dim_pad, n_sparse, n_sparse_pad, n_pairs, n_cut, peaks)
+            for k, v in stages.items() if k.startswith(("gemm_bf16x3", "soap_forward", "soap_backward"))}
+    name = max(stages.items(), key=lambda kv: kv[1]["total_ms"])[0]
+    dom = dict(rows.get(name) or _stage_roofline(name, stages[name], total, n_rows, dim, dim_pad, n_sparse,
+                                                  n_sparse_pad, n_pairs, n_cut, peaks))
+    dom["all"] = {k: {kk: vv for kk, vv in v.items() if kk not in ("kernel",)} for k, v in rows.items()}
+    return dom
 
 
 def _ncu_traffic(kernel):
@@ -378,6 +408,9 @@ def run_ours(args):
     e_rmse = float(torch.sqrt(torch.mean((e32 - e64) ** 2)))
     f_rmse = float(torch.sqrt(torch.mean((f32 - f64) ** 2)))
     n_pairs = system.n_pairs
+    # in-cutoff pairs (r < 3.7 A, self excluded) of the starting box, from the library's own list
+    nbc = ctx.build_neighbors_list(pos, N_ATOMS, *box, 3.7, sp)
+    n_cut = int(np.sum(nbc["n_neigh"])) - N_ATOMS
 
     if dist:
         dist.barrier()
@@ -410,7 +443,7 @@ def run_ours(args):
     peaks = _peaks()
     dim = tg.synth.soap_dim(hyp)
     roof = _roofline(stages, N_ATOMS, dim, (dim + 127) // 128 * 128, N_SPARSE, (N_SPARSE + 127) // 128 * 128,
-                     n_pairs, peaks)
+                     n_pairs, n_cut, peaks)
     system.set_positions(pos)
     system.update(True)
     e2e = _e2e(tg, ctx, system, model, masses, vel, pos, tg.TGAP_MIXED, min(args.steps, 50))
