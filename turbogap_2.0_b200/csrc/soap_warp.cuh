@@ -154,76 +154,6 @@ __device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F 
     }
 }
 
-// Every real harmonic with its gradient (as ylm_all<GRAD = true>), orders m >= 1 in a runtime
-// loop with l unrolled inside: the adjoint's per-harmonic body is large, and this keeps the
-// kernel's code within the instruction cache while l (and so f_l) stays compile-time.
-template <class T, int L, class F>
-__device__ __forceinline__ void ylm_all_grad(const YlmConst &Yc, T ux, T uy, T uz, F &&fn)
-{
-    {
-        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
-#pragma unroll
-        for (int l = 0; l <= L; ++l) {
-            T Q, dQ;
-            if (l == 0) {
-                Q = 1;
-                dQ = 0;
-            } else if (l == 1) {
-                Q = uz;
-                dQ = 1;
-            } else {
-                const T inv = (T)(1.0 / (double)l);
-                Q = ((T)(2 * l - 1) * uz * Q1 - (T)(l - 1) * Q2) * inv;
-                dQ = ((T)(2 * l - 1) * (Q1 + uz * dQ1) - (T)(l - 1) * dQ2) * inv;
-            }
-            Q2 = Q1;
-            Q1 = Q;
-            dQ2 = dQ1;
-            dQ1 = dQ;
-            const T N = yc_norm<T>(Yc, l * (l + 1) / 2);
-            fn(l * l, l, N * Q, (T)0, (T)0, N * dQ);
-        }
-    }
-    T Cc = 1, Sc = 0;
-#pragma unroll 1
-    for (int m = 1; m <= L; ++m) {
-        const T Cp = Cc, Sp = Sc;
-        Cc = ux * Cp - uy * Sp;
-        Sc = ux * Sp + uy * Cp;
-        const T qmm = yc_dfact<T>(Yc, m);
-        const T fm = (T)m;
-        const T tm1 = (T)(2 * m + 1);
-        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
-#pragma unroll
-        for (int l = 1; l <= L; ++l) {
-            if (l >= m) {
-                T Q, dQ;
-                if (l == m) {
-                    Q = qmm;
-                    dQ = 0;
-                } else if (l == m + 1) {
-                    Q = tm1 * uz * qmm;
-                    dQ = tm1 * qmm;
-                } else {
-                    const T inv = yc_inv<T>(Yc, l - m);
-                    const T a = (T)(2 * l - 1), b = (T)(l - 1) + fm;
-                    Q = (a * uz * Q1 - b * Q2) * inv;
-                    dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
-                }
-                Q2 = Q1;
-                Q1 = Q;
-                dQ2 = dQ1;
-                dQ1 = dQ;
-                const T N = yc_norm<T>(Yc, l * (l + 1) / 2 + m);
-                const T NQ = N * Q, NQm = NQ * fm, NdQ = N * dQ;
-                const int k0 = l * l + 2 * m - 1;
-                fn(k0, l, NQ * Cc, NQm * Cp, -NQm * Sp, NdQ * Cc);
-                fn(k0 + 1, l, NQ * Sc, NQm * Sp, NQm * Cp, NdQ * Sc);
-            }
-        }
-    }
-}
-
 // Pair acceptance: species channel known (and equal to only_s when only_s >= 0) and
 // 0 < r < rcut_hard(s).
 __device__ __forceinline__ bool pair_accept(const SoapParams &P, int64_t k, const double *__restrict__ rjs,
@@ -323,6 +253,125 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T v[N])
             v[2 * i + 1] = x.y;
         }
     }
+}
+
+// Adjoint of one pair's angular-radial product, summed over every real harmonic:
+//   w = u (A1 - u.Gam) + Gam,  A1 = sum_lm Y_lm (f_l V_lm + df_l U_lm),
+//   Gam = (1/r) sum_lm f_l U_lm dY_lm/du,   U_lm = Gc[lm].R, V_lm = Gc[lm].R'
+// which equals sum_lm [u Y (f V + df U) + f U (grad Y - u (u.grad Y)) / r]. The order m is
+// unrolled (compile time) and the degree l = m..L runs as a loop (L+1 copies of the body, in the
+// instruction cache); the cos and sin harmonics of one (l, m) share their Legendre factors and
+// read their two adjacent Gc rows together. f_l / df_l come from fl[l * 32] / dfl[l * 32].
+template <class T, int L, int AMB>
+__device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T uz, T ir, const T *fl, const T *dfl,
+                                             const T *__restrict__ Gs, const T R[AMB], const T dR[AMB], T w[3])
+{
+    T A1 = 0, Gx = 0, Gy = 0, Gz = 0;
+    // m = 0: Y = N Q, dY/du = (0, 0, N dQ)
+    {
+        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+#pragma unroll 1
+        for (int l = 0; l <= L; ++l) {
+            T Q, dQ;
+            if (l == 0) {
+                Q = 1;
+                dQ = 0;
+            } else if (l == 1) {
+                Q = uz;
+                dQ = 1;
+            } else {
+                const T inv = yc_inv<T>(Yc, l);
+                const T a = (T)(2 * l - 1), b = (T)(l - 1);
+                Q = (a * uz * Q1 - b * Q2) * inv;
+                dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
+            }
+            Q2 = Q1;
+            Q1 = Q;
+            dQ2 = dQ1;
+            dQ1 = dQ;
+            T g[AMB];
+            load_vec<T, AMB>(Gs + l * l * AMB, g);
+            T U0 = 0, U1 = 0, V0 = 0, V1 = 0;
+#pragma unroll
+            for (int e = 0; e < AMB; e += 2) {
+                U0 += g[e] * R[e];
+                V0 += g[e] * dR[e];
+                U1 += g[e + 1] * R[e + 1];
+                V1 += g[e + 1] * dR[e + 1];
+            }
+            const T U = U0 + U1, V = V0 + V1;
+            const T f = fl[l * 32], df = dfl[l * 32];
+            const T N = yc_norm<T>(Yc, l * (l + 1) / 2);
+            A1 += N * Q * (f * V + df * U);
+            Gz += N * dQ * (f * U);
+        }
+    }
+    T Cc = 1, Sc = 0;
+#pragma unroll
+    for (int m = 1; m <= L; ++m) {
+        const T Cp = Cc, Sp = Sc;
+        Cc = ux * Cp - uy * Sp;
+        Sc = ux * Sp + uy * Cp;
+        const T qmm = yc_dfact<T>(Yc, m);
+        const T fm = (T)m;
+        const T tm1 = (T)(2 * m + 1);
+        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+#pragma unroll 1
+        for (int l = m; l <= L; ++l) {
+            T Q, dQ;
+            if (l == m) {
+                Q = qmm;
+                dQ = 0;
+            } else if (l == m + 1) {
+                Q = tm1 * uz * qmm;
+                dQ = tm1 * qmm;
+            } else {
+                const T inv = yc_inv<T>(Yc, l - m);
+                const T a = (T)(2 * l - 1), b = (T)(l - 1) + fm;
+                Q = (a * uz * Q1 - b * Q2) * inv;
+                dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
+            }
+            Q2 = Q1;
+            Q1 = Q;
+            dQ2 = dQ1;
+            dQ1 = dQ;
+            // rows of the cos (l^2 + 2m - 1) and sin (l^2 + 2m) harmonics, adjacent in Gs
+            T gc[AMB], gs[AMB];
+            const T *row = Gs + (l * l + 2 * m - 1) * AMB;
+            load_vec<T, AMB>(row, gc);
+            load_vec<T, AMB>(row + AMB, gs);
+            T Uc0 = 0, Uc1 = 0, Vc0 = 0, Vc1 = 0, Us0 = 0, Us1 = 0, Vs0 = 0, Vs1 = 0;
+#pragma unroll
+            for (int e = 0; e < AMB; e += 2) {
+                Uc0 += gc[e] * R[e];
+                Vc0 += gc[e] * dR[e];
+                Us0 += gs[e] * R[e];
+                Vs0 += gs[e] * dR[e];
+                Uc1 += gc[e + 1] * R[e + 1];
+                Vc1 += gc[e + 1] * dR[e + 1];
+                Us1 += gs[e + 1] * R[e + 1];
+                Vs1 += gs[e + 1] * dR[e + 1];
+            }
+            const T Uc = Uc0 + Uc1, Vc = Vc0 + Vc1, Us = Us0 + Us1, Vs = Vs0 + Vs1;
+            const T f = fl[l * 32], df = dfl[l * 32];
+            const T ac = f * Vc + df * Uc, as = f * Vs + df * Us;
+            const T bc = f * Uc, bs = f * Us;
+            const T N = yc_norm<T>(Yc, l * (l + 1) / 2 + m);
+            const T NQ = N * Q, NQm = NQ * fm, NdQ = N * dQ;
+            // cos: Y = NQ C, dY/du = (NQm C', -NQm S', NdQ C); sin: Y = NQ S, (NQm S', NQm C', NdQ S)
+            A1 += NQ * (ac * Cc + as * Sc);
+            Gx += NQm * (bc * Cp + bs * Sp);
+            Gy += NQm * (bs * Cp - bc * Sp);
+            Gz += NdQ * (bc * Cc + bs * Sc);
+        }
+    }
+    Gx *= ir;
+    Gy *= ir;
+    Gz *= ir;
+    const T ug = ux * Gx + uy * Gy + uz * Gz;
+    w[0] = ux * (A1 - ug) + Gx;
+    w[1] = uy * (A1 - ug) + Gy;
+    w[2] = uz * (A1 - ug) + Gz;
 }
 
 // Row stride of the angular rows in shared memory: odd, so the 32 lanes writing their own pair's
@@ -469,12 +518,27 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
 
 // ----------------------------------------------------------------------------- adjoint
 
-// Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (rounded up to 4),
-// Gc [n_species][NLM][AMB] (dE/dc per species block, zero beyond alpha_max), M [L+1][MS] with
-// M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l] (MS = n_max^2 + 1, odd); after the warps,
-// the CTA's virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
+// Elements of the c area of the adjoint: c [n_max][NLM] rounded up to 4, and at least the
+// lanes' force/virial partials [32][9] (double) that reuse it after the prologue.
+template <class T> __host__ __device__ constexpr int bwd_c_elems(int nout)
+{
+    return ((nout + 3) / 4 * 4) > (int)(32 * 9 * sizeof(double) / sizeof(T)) ? (nout + 3) / 4 * 4
+                                                                               : (int)(32 * 9 * sizeof(double) / sizeof(T));
+}
+
+// Minimum resident CTAs asked of the compiler (1: every instantiation keeps its natural register
+// count; forcing 6 CTAs on the FP32 kernel spilled and ran slower).
+template <class T, int AMB> struct BwdMinCtas {
+    static constexpr int value = 1;
+};
+
+// Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (then the lanes'
+// force/virial partials), Gc [n_species][NLM][AMB] (dE/dc per species block, zero beyond
+// alpha_max), M [L+1][MS] with M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l]
+// (MS = n_max^2 + 1, odd), f_l / df_l of each lane's pair [2][L+1][32]; after the warps, the CTA's virial partials [kWarpsPerCta][6] and
+// structure ids [kWarpsPerCta].
 template <class T, class GT, int L, int AMB>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
+__global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) k_soap_bwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
     const T *__restrict__ tq, const float4 *__restrict__ rtab, const int *__restrict__ sites, int n_rows,
     const int64_t *__restrict__ start, const double *__restrict__ rjs, const double *__restrict__ xyz,
@@ -498,8 +562,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
         const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM, MS = nmax * nmax + 1;
         long long *idx = reinterpret_cast<long long *>(wbase);
         T *cs = reinterpret_cast<T *>(wbase + 256);
-        T *Gc = cs + (nout + 3) / 4 * 4;
+        T *Gc = cs + bwd_c_elems<T>(nout);
         T *Ms = Gc + P.n_species * NLM * AMB;
+        T *fdf = Ms + (L + 1) * (nmax * nmax + 1);  // [2][L+1][32]: f_l, df_l of each lane's pair
 
         const int site = sites ? sites[row] : row;
         my_struct = site_struct ? site_struct[site] : 0;
@@ -544,6 +609,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
             }
         }
         __syncwarp();
+        // per-lane force/virial partials, kept out of registers during the pair loop; they reuse
+        // the area of c, which is dead once Gc is formed
+        double *vl = reinterpret_cast<double *>(cs) + lane * 9;
+#pragma unroll
+        for (int i = 0; i < 9; ++i) vl[i] = 0.0;
 
         int64_t scan = kb + 1;
         while (scan < ke) {
@@ -566,35 +636,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
                 const T st = (T)P.sigma_t[s] + sts * r;
                 const T kap = r * r / (st * st);
                 const T dkap = (T)2 * r / (st * st) - (T)2 * r * r * sts / (st * st * st);
-                T f[L + 2];
-                bessel_ratios_fixed<T, L>(kap, f);
-                const T ikap = kap > (T)0 ? (T)1 / kap : (T)0;
-                T df[L + 1];
+                {
+                    T f[L + 2];
+                    bessel_ratios_fixed<T, L>(kap, f);
+                    const T ikap = kap > (T)0 ? (T)1 / kap : (T)0;
 #pragma unroll
-                for (int l = 0; l <= L; ++l) df[l] = (f[l + 1] + (T)l * ikap * f[l] - f[l] * f[1]) * dkap;
-                const T *Gs = Gc + s * NLM * AMB;
-                T w0 = 0, w1 = 0, w2 = 0;
-                ylm_all_grad<T, L>(Yc, u0, u1, u2, [&](int kk, int l, T y, T gx, T gy, T gz) {
-                    T gv[AMB];
-                    load_vec<T, AMB>(Gs + kk * AMB, gv);
-                    // two interleaved chains each for U and V (shorter dependency chains)
-                    T U0 = 0, U1 = 0, V0 = 0, V1 = 0;
-#pragma unroll
-                    for (int e = 0; e < AMB; e += 2) {
-                        U0 += gv[e] * R[e];
-                        V0 += gv[e] * dR[e];
-                        U1 += gv[e + 1] * R[e + 1];
-                        V1 += gv[e + 1] * dR[e + 1];
+                    for (int l = 0; l <= L; ++l) {
+                        fdf[l * 32 + lane] = f[l];
+                        fdf[(L + 1 + l) * 32 + lane] = (f[l + 1] + (T)l * ikap * f[l] - f[l] * f[1]) * dkap;
                     }
-                    const T U = U0 + U1, V = V0 + V1;
-                    const T a = f[l] * V + df[l] * U;
-                    const T b = U * f[l] * ir;
-                    const T ug = u0 * gx + u1 * gy + u2 * gz;
-                    const T ya = y * a;
-                    w0 += u0 * ya + b * (gx - u0 * ug);
-                    w1 += u1 * ya + b * (gy - u1 * ug);
-                    w2 += u2 * ya + b * (gz - u2 * ug);
-                });
+                }
+                T w[3];
+                pair_adjoint<T, L, AMB>(Yc, u0, u1, u2, ir, fdf + lane, fdf + (L + 1) * 32 + lane, Gc + s * NLM * AMB,
+                                        R, dR, w);
+                const T w0 = w[0], w1 = w[1], w2 = w[2];
                 // w = dE_i/dr_ij: force -w on the neighbor, +w on the site (its self slot)
                 const double f0 = -(double)w0, f1 = -(double)w1, f2 = -(double)w2;
                 const int j = jatom[k];
@@ -605,18 +660,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_bwd_warp(
                 } else {
                     check_fail(check, kCheckBwdAtom, k, j);
                 }
-                vals[0] -= f0;
-                vals[1] -= f1;
-                vals[2] -= f2;
-                vals[3] += f0 * xd0;
-                vals[4] += f1 * xd1;
-                vals[5] += f2 * xd2;
-                vals[6] += 0.5 * (f0 * xd1 + f1 * xd0);
-                vals[7] += 0.5 * (f0 * xd2 + f2 * xd0);
-                vals[8] += 0.5 * (f1 * xd2 + f2 * xd1);
+                vl[0] -= f0;
+                vl[1] -= f1;
+                vl[2] -= f2;
+                vl[3] += f0 * xd0;
+                vl[4] += f1 * xd1;
+                vl[5] += f2 * xd2;
+                vl[6] += 0.5 * (f0 * xd1 + f1 * xd0);
+                vl[7] += 0.5 * (f0 * xd2 + f2 * xd0);
+                vl[8] += 0.5 * (f1 * xd2 + f2 * xd1);
             }
             __syncwarp();
         }
+#pragma unroll
+        for (int i = 0; i < 9; ++i) vals[i] = vl[i];
 #pragma unroll
         for (int i = 0; i < 9; ++i) {
 #pragma unroll
@@ -676,12 +733,14 @@ inline size_t fwd_warp_bytes(const SoapParams &P, size_t tsz, int astr, int amb)
     return 256 + (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
 }
 
-inline size_t bwd_warp_bytes(const SoapParams &P, size_t tsz, int amb)
+template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
 {
     const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
-    const size_t nout = (size_t)P.n_max * nlm;
+    const int nout = P.n_max * (int)nlm;
     const size_t ms = (size_t)(P.l_max + 1) * ((size_t)P.n_max * P.n_max + 1);
-    return 256 + (tsz * ((nout + 3) / 4 * 4 + (size_t)P.n_species * nlm * amb + ms) + 15) / 16 * 16;
+    const size_t fdf = 2 * (size_t)(P.l_max + 1) * 32;
+    return 256 +
+           (sizeof(T) * ((size_t)bwd_c_elems<T>(nout) + (size_t)P.n_species * nlm * amb + ms + fdf) + 15) / 16 * 16;
 }
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
@@ -716,7 +775,7 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                  double *d_virial)
 {
-    const size_t wb = bwd_warp_bytes(ds.p, sizeof(T), AMB);
+    const size_t wb = bwd_warp_bytes<T>(ds.p, AMB);
     const size_t tail = kWarpsPerCta * (6 * sizeof(double) + sizeof(int));
     const int nw = (int)std::min<size_t>(kWarpsPerCta, (kMaxDynSmem - tail) / wb);
     if (nw < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", wb);
