@@ -255,6 +255,28 @@ int tgap_md_run(tgap_md *md, int n_steps);
 int tgap_md_get_state(tgap_md *md, double *positions, double *velocities, double *forces,
                       double *e_pot, double *e_kin);
 
+/* ------------------------------------------------------------------ Monte Carlo driver */
+
+typedef struct tgap_mc tgap_mc;
+
+/* Metropolis single-atom moves (mc_utils.f90:172-180, 215-277; mc_interface.f90:183-447) on a
+ * resident system whose neighbor lists use (largest model cutoff + skin): the system's rcut_max
+ * must exceed the models' cutoff, the difference is the skin. Each proposal re-evaluates only
+ * the sites within the cutoff of the moved atom's old or new position (local update); the
+ * lists are rebuilt when accumulated displacements could exceed the skin. */
+int tgap_mc_create(tgap_context *ctx, tgap_system *system, int n_models, tgap_model *const *models,
+                   double temperature, int precision, int use_graph, tgap_mc **mc);
+int tgap_mc_destroy(tgap_mc *mc);
+/* n proposals from the caller's generator: atom (0-based), displacement (3 per proposal, Å),
+ * uniform deviate in [0, 1). A move is accepted when min(1, exp(-dE / (kB T))) > u with the
+ * reference's kB. dE and the decision of every proposal go to de_log / acc_log when non-NULL. */
+int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const double *displacements,
+                const double *uniforms, int64_t *n_accepted, double *de_log, unsigned char *acc_log);
+/* Host copies (any pointer may be NULL): positions (3 x n_atoms), site energies summed over
+ * models (n_atoms), their total, moves accepted since creation, neighbor-list rebuilds. */
+int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energies, double *e_total,
+                      int64_t *accepted, int64_t *rebuilds);
+
 #ifdef __cplusplus
 }
 #endif

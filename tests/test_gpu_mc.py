@@ -1,0 +1,160 @@
+"""Metropolis Monte Carlo with local updates (tgap_mc) against the oracle's full recomputation.
+
+Each proposal's energy change on the device comes from re-evaluating only the sites within the
+cutoff of the moved atom; the oracle recomputes the whole structure before and after the move.
+FP64: dE within 1e-9 eV, identical decisions (mc_utils.f90:172-180 with the binary32 kB,
+get_mc_acceptance min(1, p), accept when p > u), identical final positions. The neighbor skin is
+small enough that the lists are rebuilt several times during the run.
+"""
+import numpy as np
+import pytest
+
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+KB = float(np.float32(8.617333262e-5))
+
+
+@pytest.fixture(scope="module")
+def ctx(tg):
+    import torch
+    assert torch.cuda.is_available()
+    c = tg.Context(0)
+    yield c
+    c.close()
+
+
+@pytest.fixture(scope="module")
+def carbon(synth):
+    return helpers.carbon_model(synth, 200, seed=5)
+
+
+def _oracle_chain(hyp, models, pos, box, sp, atoms, disp, u, temperature, de_g, acc_g, de_tol):
+    """Replays the proposals with full oracle evaluations; returns positions and total energy."""
+    p = np.array(pos, dtype=np.float64)
+    e_cur = helpers.oracle_structure_eval(hyp, models, p, box, sp, do_forces=False)[0].sum()
+    n_border = 0
+    for k in range(len(atoms)):
+        q = p.copy()
+        q[atoms[k]] = q[atoms[k]] + disp[k]
+        e_new = helpers.oracle_structure_eval(hyp, models, q, box, sp, do_forces=False)[0].sum()
+        de = e_new - e_cur
+        assert abs(de - de_g[k]) < de_tol, (k, de, de_g[k])
+        pacc = min(1.0, float(np.exp(-de / (KB * temperature))))
+        if abs(pacc - u[k]) > 1e-9:
+            assert (pacc > u[k]) == bool(acc_g[k]), k
+        else:
+            n_border += 1
+        if acc_g[k]:  # follow the device's chain
+            p, e_cur = q, e_new
+    return p, e_cur, n_border
+
+
+def test_mc_fp64_matches_oracle_full_recompute(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=70)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    T = 30.0
+    mc = tg.MC(ctx, system, [model], T, precision=tg.TGAP_FP64)
+    e0 = mc.state()["e_total"]
+    e_o0 = helpers.oracle_structure_eval(hyp, [m], pos, box, sp, do_forces=False)[0].sum()
+    assert abs(e0 - e_o0) < 1e-9
+    atoms, disp, u = synth.mc_proposals(len(pos), 160, 0.2, seed=71)
+    out = mc.run(atoms, disp, u)
+    st = mc.state()
+    p, e, _ = _oracle_chain(hyp, [m], pos, box, sp, atoms, disp, u, T, out["de"], out["accept"], 1e-9)
+    assert 0 < out["accepted"] < len(atoms)
+    assert out["accepted"] == int(out["accept"].sum()) == st["accepted"]
+    assert st["rebuilds"] >= 2
+    assert np.array_equal(st["positions"], p)
+    assert abs(st["e_total"] - e) < 1e-9
+    # a second run continues the same chain
+    atoms2, disp2, u2 = synth.mc_proposals(len(pos), 40, 0.2, seed=72)
+    out2 = mc.run(atoms2, disp2, u2)
+    p2, e2, _ = _oracle_chain(hyp, [m], p, box, sp, atoms2, disp2, u2, T, out2["de"], out2["accept"], 1e-9)
+    st2 = mc.state()
+    assert np.array_equal(st2["positions"], p2)
+    assert abs(st2["e_total"] - e2) < 1e-9
+    mc.close()
+
+
+def test_mc_two_species_two_models_with_replicas(ctx, tg, synth):
+    """SiO2 with one model per centre species; the 9 A cell is smaller than twice the list
+    cutoff, so the moved atom's periodic images are in its own list."""
+    hyp = synth.sio2_hypers()
+    dmin = {("Si", "O"): 1.4, ("O", "O"): 2.2, ("Si", "Si"): 2.5}
+    frac = {"Si": 1 / 3, "O": 2 / 3}
+    pool = [synth.random_packing(48, 2.2, dmin, frac, seed=50 + k)[:3] for k in range(2)]
+    qSi = np.concatenate([helpers.oracle_descriptors(hyp, p, b, s, 1) for p, b, s in pool])
+    qO = np.concatenate([helpers.oracle_descriptors(hyp, p, b, s, 2) for p, b, s in pool])
+    mSi = synth.gap_model(qSi, 20, seed=1)
+    mO = synth.gap_model(qO, 20, seed=2)
+    mSi["central_species"], mO["central_species"] = 1, 2
+    pos, box, sp, _ = synth.random_packing(48, 2.2, dmin, frac, seed=56)
+    models = [tg.Model(ctx, hyp, mm["Qs"], mm["alphas"], 1.0, 4.0, central_species=mm["central_species"])
+              for mm in (mSi, mO)]
+    system = tg.System(ctx, [(pos, box, sp)], 5.0 + 0.4)
+    T = 40.0
+    mc = tg.MC(ctx, system, models, T, precision=tg.TGAP_FP64)
+    atoms, disp, u = synth.mc_proposals(len(pos), 60, 0.2, seed=57)
+    out = mc.run(atoms, disp, u)
+    st = mc.state()
+    p, e, _ = _oracle_chain(hyp, [mSi, mO], pos, box, sp, atoms, disp, u, T, out["de"], out["accept"], 1e-9)
+    assert out["accepted"] > 0
+    assert np.array_equal(st["positions"], p)
+    assert abs(st["e_total"] - e) < 1e-9
+    mc.close()
+
+
+def test_mc_mixed_tracks_fp64(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(96, 2.0, 1.2, seed=73)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    atoms, disp, u = synth.mc_proposals(len(pos), 200, 0.2, seed=74)
+    runs = {}
+    for prec in (tg.TGAP_FP64, tg.TGAP_MIXED):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.5)
+        mc = tg.MC(ctx, system, [model], 30.0, precision=prec)
+        runs[prec] = mc.run(atoms, disp, u)
+        mc.close()
+        system.close()
+    d64, d32 = runs[tg.TGAP_FP64]["de"], runs[tg.TGAP_MIXED]["de"]
+    a64, a32 = runs[tg.TGAP_FP64]["accept"], runs[tg.TGAP_MIXED]["accept"]
+    # identical chains up to the first differing decision; dE agrees to the mixed-path accuracy
+    first = np.argmax(a64 != a32) if np.any(a64 != a32) else len(a64)
+    assert first > 20
+    assert np.max(np.abs(d64[:first] - d32[:first])) < 2e-4
+
+
+def test_mc_graph_and_eager_agree(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=75)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    atoms, disp, u = synth.mc_proposals(len(pos), 100, 0.2, seed=76)
+    res = []
+    for graph in (True, False):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+        mc = tg.MC(ctx, system, [model], 30.0, precision=tg.TGAP_FP64, use_graph=graph)
+        out = mc.run(atoms, disp, u)
+        res.append((out, mc.state()))
+        mc.close()
+        system.close()
+    assert np.array_equal(res[0][0]["accept"], res[1][0]["accept"])
+    assert np.array_equal(res[0][0]["de"], res[1][0]["de"])
+    assert np.array_equal(res[0][1]["positions"], res[1][1]["positions"])
+
+
+def test_mc_rejects_bad_arguments(ctx, tg, synth, carbon):
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=77)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    no_skin = tg.System(ctx, [(pos, box, sp)], 3.7)
+    with pytest.raises(tg.TgapError):
+        tg.MC(ctx, no_skin, [model], 300.0)
+    system = tg.System(ctx, [(pos, box, sp)], 4.0)
+    mc = tg.MC(ctx, system, [model], 300.0)
+    with pytest.raises(tg.TgapError):
+        mc.run(np.array([len(pos)], np.int32), np.zeros((1, 3)), np.zeros(1))
+    mc.close()

@@ -64,3 +64,19 @@ def test_assign_species(tg):
     import pytest
     with pytest.raises(tg.TgapError):
         tg.api.assign_species(["C", "C"], ["C"])
+
+
+def test_package_exports_the_device_api(tg):
+    """Every host-side class of the device API resolves from the package (no GPU needed)."""
+    for name in ("Context", "Model", "System", "MD", "MC", "assign_species"):
+        assert callable(getattr(tg, name)), name
+
+
+def test_mc_proposals_stay_in_the_ball(tg):
+    atoms, d, u = tg.synth.mc_proposals(100, 5000, 0.2, seed=3)
+    assert atoms.min() >= 0 and atoms.max() < 100
+    r = np.linalg.norm(d, axis=1)
+    assert r.max() <= 0.2 + 1e-12
+    # uniform in the ball: P(r < R/2) = 1/8
+    assert abs(np.mean(r < 0.1) - 0.125) < 0.02
+    assert u.min() >= 0.0 and u.max() < 1.0

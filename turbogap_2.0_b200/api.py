@@ -319,3 +319,55 @@ class MD:
             self.close()
         except Exception:
             pass
+
+
+class MC:
+    """Metropolis single-atom moves with local updates on the device (tgap_mc).
+
+    The system must have been built with rcut_max = model cutoff + skin. Proposals come from the
+    caller: atoms (0-based), displacements (n, 3) and uniform deviates in [0, 1)."""
+
+    def __init__(self, ctx, system, models, temperature, precision=TGAP_FP64, use_graph=True):
+        self.ctx = ctx
+        self.system = system
+        self.models = list(models)
+        arr = (C.c_void_p * len(models))(*[m.h.value for m in models])
+        h = C.c_void_p()
+        check(ctx._L.tgap_mc_create(ctx.h, system.h, len(models), arr, float(temperature), int(precision),
+                                    int(use_graph), C.byref(h)), ctx.h, "tgap_mc_create")
+        self.h = h
+
+    def run(self, atoms, displacements, uniforms, logs=True):
+        atoms = np.ascontiguousarray(atoms, dtype=np.int32)
+        disp = _f64(displacements)
+        u = _f64(uniforms)
+        n = len(atoms)
+        if disp.size != 3 * n or u.size != n:
+            raise ValueError("proposal arrays disagree in length")
+        acc = C.c_int64(0)
+        de = np.zeros(n) if logs else None
+        ok = np.zeros(n, np.uint8) if logs else None
+        check(self.ctx._L.tgap_mc_run(self.h, n, ptr(atoms), ptr(disp), ptr(u), C.byref(acc),
+                                      ptr(de) if logs else None, ptr(ok) if logs else None),
+              self.ctx.h, "tgap_mc_run")
+        return dict(accepted=acc.value, de=de, accept=ok.astype(bool) if logs else None)
+
+    def state(self):
+        n = self.system.n_atoms
+        pos = np.zeros((n, 3)); e = np.zeros(n)
+        et = C.c_double(); acc = C.c_int64(); reb = C.c_int64()
+        check(self.ctx._L.tgap_mc_get_state(self.h, ptr(pos), ptr(e), C.byref(et), C.byref(acc), C.byref(reb)),
+              self.ctx.h, "mc_get_state")
+        return dict(positions=pos, energies=e, e_total=et.value, accepted=acc.value, rebuilds=reb.value)
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.ctx._L.tgap_mc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+

@@ -33,6 +33,7 @@ SOURCES = [
     ("gap.cu", []),
     ("gemm_tc.cu", []),
     ("md.cu", []),
+    ("mc.cu", ["--fmad=false"]),
     ("tables.cpp", []),
 ]
 

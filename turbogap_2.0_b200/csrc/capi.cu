@@ -12,6 +12,7 @@
 #include <vector>
 
 #include "gap_kernels.h"
+#include "mc_kernels.h"
 #include "md_kernels.h"
 #include "neighbors.h"
 #include "soap_kernels.h"
@@ -232,8 +233,9 @@ int read_device_check(tgap_context *ctx)
                                  "descriptor adjoint: neighbor atom out of range",
                                  "descriptor adjoint: self-slot atom out of range",
                                  "non-finite force",
-                                 "neighbor fill past its counted range"};
-    const char *w = (h[0] > 0 && h[0] <= kCheckListOverrun) ? what[h[0]] : "unknown check";
+                                 "neighbor fill past its counted range",
+                                 "Monte Carlo trial capacity exceeded"};
+    const char *w = (h[0] > 0 && h[0] <= kCheckMcOverflow) ? what[h[0]] : "unknown check";
     return set_error(ctx, h[0] == kCheckNonFinite ? TGAP_ERR_NUMERIC : TGAP_ERR_CUDA,
                      "device check %d (%s): index %d value %d, %d failure(s)", h[0], w, h[1], h[2], h[3]);
 }
@@ -1224,5 +1226,309 @@ extern "C" int tgap_md_get_state(tgap_md *md, double *positions, double *velocit
     }
     if (e_pot) *e_pot = ep;
     if (e_kin) *e_kin = ek;
+    return TGAP_OK;
+}
+
+// ============================================================================ Monte Carlo
+
+struct tgap_mc {
+    tgap_context *ctx;
+    tgap_system *sys;
+    std::vector<tgap_model *> models;
+    int precision, use_graph;
+    double temperature, rc_sel, skin;
+    int cap = 0, pmax = 0;
+    int64_t rebuilds = 0;
+    McModelSel sel{};
+    DevBuf st, ecache, dacc, mark, sites, tstart, txyz, trjs, tnsp, etrial;
+    std::vector<DevBuf> c, q, norm, q_hi, q_lo;  // per model, the trial rows
+    std::vector<GapWork> gw;
+    DevBuf patom, pdisp, pu, log_de, log_acc;
+    HostBuf hst;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    uint64_t graph_epoch = 0;
+    int64_t graph_kernels = 0;
+};
+
+constexpr int kMcBatch = 32;  // proposals per graph launch
+
+// Trial buffers for the current lists: pmax = longest list, cap = most sites one move can touch.
+static int mc_size_trial(tgap_mc *mc)
+{
+    tgap_context *ctx = mc->ctx;
+    NeighborBatch &nb = mc->sys->nb;
+    const int N = nb.n_atoms;
+    std::vector<int> nn(N);
+    CHECK_RC(download(ctx, nn.data(), nb.n_neigh, (size_t)N));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    int pmax = 1;
+    for (int v : nn) pmax = std::max(pmax, v);
+    if (pmax <= mc->pmax && mc->cap > 0) return TGAP_OK;
+    mc->pmax = (pmax + 7) / 8 * 8 + 8;  // room for a few more pairs before resizing
+    mc->cap = (mc->pmax + 1 + 31) / 32 * 32;
+    const int M = (int)mc->models.size(), cap = mc->cap, pm = mc->pmax;
+    const int rows_pad = (cap + 127) / 128 * 128;
+    std::vector<int64_t> ts(cap + 1);
+    for (int r = 0; r <= cap; ++r) ts[r] = (int64_t)r * pm;
+    const size_t slots = (size_t)M * cap * pm;
+    if (mc->sites.ensure(sizeof(int) * (size_t)M * cap) || mc->tstart.ensure(sizeof(int64_t) * (cap + 1)) ||
+        mc->txyz.ensure(sizeof(double) * 3 * slots) || mc->trjs.ensure(sizeof(double) * slots) ||
+        mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * cap))
+        return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->tnsp.ptr, 0, sizeof(int) * slots, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->trjs.ptr, 0, sizeof(double) * slots, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->txyz.ptr, 0, sizeof(double) * 3 * slots, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->sites.ptr, 0, sizeof(int) * (size_t)M * cap, ctx->stream));
+    CHECK_RC(upload(ctx, mc->tstart, ts.data(), ts.size()));
+    for (int m = 0; m < M; ++m) {
+        const tgap_model *md = mc->models[m];
+        const SoapParams &P = md->soap.p;
+        const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+        const size_t tsz = mc->precision == TGAP_FP64 ? 8 : 4;
+        const int q_ld = mc->precision == TGAP_FP64 ? md->gap.dim : md->gap.dim_pad;
+        if (mc->c[m].ensure(tsz * cap * P.n_max * nlm) || mc->q[m].ensure(tsz * (size_t)rows_pad * q_ld) ||
+            mc->norm[m].ensure(tsz * cap))
+            return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
+        if (mc->precision != TGAP_FP64) {
+            if (mc->q_hi[m].ensure(2 * (size_t)rows_pad * q_ld) || mc->q_lo[m].ensure(2 * (size_t)rows_pad * q_ld))
+                return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
+            // rows past cap feed the 128-row GEMM tile: zero
+            TGAP_CUDA(ctx, cudaMemsetAsync(mc->q_hi[m].ptr, 0, mc->q_hi[m].bytes, ctx->stream));
+            TGAP_CUDA(ctx, cudaMemsetAsync(mc->q_lo[m].ptr, 0, mc->q_lo[m].bytes, ctx->stream));
+        }
+    }
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
+// One proposal: select, trial geometry, descriptor rows and GAP energies per model, acceptance.
+static int mc_step_body(tgap_mc *mc)
+{
+    tgap_context *ctx = mc->ctx;
+    NeighborBatch &nb = mc->sys->nb;
+    const int M = (int)mc->models.size(), cap = mc->cap, pm = mc->pmax, N = nb.n_atoms;
+    McDev *st = mc->st.as<McDev>();
+    CHECK_RC(mc_select(ctx, st, nb, mc->sel, mc->rc_sel, mc->skin, mc->patom.as<int>(), mc->pdisp.as<double>(),
+                       mc->dacc.as<double>(), mc->mark.as<long long>(), mc->sites.as<int>(), cap));
+    CHECK_RC(mc_trial_geometry(ctx, st, nb, M, mc->sites.as<int>(), cap, pm, mc->txyz.as<double>(),
+                               mc->trjs.as<double>(), mc->tnsp.as<int>()));
+    for (int m = 0; m < M; ++m) {
+        const tgap_model *md = mc->models[m];
+        const size_t off = (size_t)m * cap * pm;
+        PairView pv{mc->tstart.as<int64_t>(), mc->txyz.as<double>() + 3 * off, mc->trjs.as<double>() + off,
+                    mc->tnsp.as<int>() + off, nullptr, 0, ctx->d_check};
+        SoapOut o;
+        o.c = mc->c[m].ptr;
+        o.q = mc->q[m].ptr;
+        o.norm = mc->norm[m].ptr;
+        double *e_rows = mc->etrial.as<double>() + (size_t)m * cap;
+        if (mc->precision == TGAP_FP64) {
+            o.q_ld = md->gap.dim;
+            CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, cap, TGAP_FP64, o));
+            CHECK_RC(gap_energy_grad_f64(ctx, md->gap, (const double *)o.q, o.q_ld, cap, 0.0, 0, &mc->gw[m], nullptr,
+                                         e_rows, nullptr));
+        } else {
+            o.q_ld = md->gap.dim_pad;
+            o.q_hi = mc->q_hi[m].as<__nv_bfloat16>();
+            o.q_lo = mc->q_lo[m].as<__nv_bfloat16>();
+            CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, cap, TGAP_MIXED, o));
+            CHECK_RC(gap_energy_grad_mixed(ctx, md->gap, o.q_hi, o.q_lo, cap, 0.0, 0, &mc->gw[m], nullptr, e_rows,
+                                           nullptr));
+        }
+    }
+    return mc_accept(ctx, st, M, mc->sites.as<int>(), cap, mc->etrial.as<double>(), mc->ecache.as<double>(), N,
+                     nb.positions.as<double>(), mc->dacc.as<double>(), mc->pu.as<double>(), mc->temperature,
+                     mc->log_de.as<double>(), mc->log_acc.as<unsigned char>());
+}
+
+static int mc_read_state(tgap_mc *mc, McDev *out)
+{
+    tgap_context *ctx = mc->ctx;
+    TGAP_CUDA(ctx, cudaMemcpyAsync(mc->hst.ptr, mc->st.ptr, sizeof(McDev), cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    std::memcpy(out, mc->hst.ptr, sizeof(McDev));
+    return read_device_check(ctx);
+}
+
+extern "C" int tgap_mc_create(tgap_context *ctx, tgap_system *sys, int n_models, tgap_model *const *models,
+                              double temperature, int precision, int use_graph, tgap_mc **out)
+{
+    CHECK_RC(activate(ctx));
+    if (!sys || n_models <= 0 || n_models > kMcMaxModels || !models || !(temperature > 0) || !out)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_mc_create: bad arguments");
+    if (precision != TGAP_FP64 && precision != TGAP_MIXED)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_mc_create: precision");
+    if (!sys->nb.replicated)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED, "Monte Carlo needs a system built from primitive cells");
+    double rc = 0.0;
+    for (int m = 0; m < n_models; ++m) rc = std::max(rc, models[m]->soap.p.rcut_max);
+    if (!(sys->rcut > rc))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "Monte Carlo needs a neighbor skin: system cutoff %g <= model %g",
+                         sys->rcut, rc);
+    auto *mc = new tgap_mc();
+    std::unique_ptr<tgap_mc, int (*)(tgap_mc *)> guard(mc, tgap_mc_destroy);
+    mc->ctx = ctx;
+    mc->sys = sys;
+    mc->models.assign(models, models + n_models);
+    mc->precision = precision;
+    mc->use_graph = use_graph;
+    mc->temperature = temperature;
+    mc->rc_sel = rc;
+    mc->skin = sys->rcut - rc;
+    mc->sel.n_models = n_models;
+    for (int m = 0; m < n_models; ++m) {
+        mc->sel.central_species[m] = models[m]->central_species;
+        if (precision == TGAP_MIXED && !models[m]->mixed_ready)
+            return set_error(ctx, TGAP_ERR_UNSUPPORTED, "mixed path not prepared");
+    }
+    mc->c.resize(n_models);
+    mc->q.resize(n_models);
+    mc->norm.resize(n_models);
+    mc->q_hi.resize(n_models);
+    mc->q_lo.resize(n_models);
+    mc->gw.resize(n_models);
+    const int N = sys->nb.n_atoms;
+    if (mc->st.ensure(sizeof(McDev)) || mc->ecache.ensure(sizeof(double) * (size_t)n_models * N) ||
+        mc->dacc.ensure(sizeof(double) * N) || mc->mark.ensure(sizeof(long long) * N) ||
+        mc->hst.ensure(sizeof(McDev)))
+        return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo state");
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->st.ptr, 0, sizeof(McDev), ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->ecache.ptr, 0, sizeof(double) * (size_t)n_models * N, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->dacc.ptr, 0, sizeof(double) * N, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->mark.ptr, 0, sizeof(long long) * N, ctx->stream));
+    // fresh lists at the current positions, then the cached site energies of every model
+    CHECK_RC(tgap_system_update(sys, 1));
+    for (int m = 0; m < n_models; ++m)
+        CHECK_RC(compute_model(ctx, sys, models[m], precision, 0, mc->ecache.as<double>() + (size_t)m * N, nullptr,
+                               nullptr));
+    CHECK_RC(mc_size_trial(mc));
+    *out = guard.release();
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_destroy(tgap_mc *mc)
+{
+    if (!mc) return TGAP_OK;
+    cudaSetDevice(mc->ctx->device);
+    cudaStreamSynchronize(mc->ctx->stream);
+    if (mc->exec) cudaGraphExecDestroy(mc->exec);
+    if (mc->graph) cudaGraphDestroy(mc->graph);
+    DevBuf *bufs[] = {&mc->st, &mc->ecache, &mc->dacc, &mc->mark, &mc->sites, &mc->tstart, &mc->txyz, &mc->trjs,
+                      &mc->tnsp, &mc->etrial, &mc->patom, &mc->pdisp, &mc->pu, &mc->log_de, &mc->log_acc};
+    for (DevBuf *b : bufs) b->release();
+    for (auto *v : {&mc->c, &mc->q, &mc->norm, &mc->q_hi, &mc->q_lo})
+        for (DevBuf &b : *v) b.release();
+    for (GapWork &w : mc->gw) {
+        DevBuf *wb[] = {&w.e_part, &w.G, &w.g, &w.G_hi, &w.G_lo};
+        for (DevBuf *b : wb) b->release();
+    }
+    mc->hst.release();
+    delete mc;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const double *disp, const double *uniform,
+                           int64_t *n_accepted, double *de_log, unsigned char *acc_log)
+{
+    if (!mc || n < 0 || (n > 0 && (!atoms || !disp || !uniform))) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = mc->ctx;
+    CHECK_RC(activate(ctx));
+    if (n == 0) {
+        if (n_accepted) *n_accepted = 0;
+        return TGAP_OK;
+    }
+    const int N = mc->sys->nb.n_atoms;
+    for (int64_t k = 0; k < n; ++k)
+        if (atoms[k] < 0 || atoms[k] >= N) return set_error(ctx, TGAP_ERR_ARGUMENT, "proposal %lld: atom", (long long)k);
+    if (mc->patom.ensure(sizeof(int) * n) || mc->pdisp.ensure(sizeof(double) * 3 * n) ||
+        mc->pu.ensure(sizeof(double) * n) || mc->log_de.ensure(sizeof(double) * n) || mc->log_acc.ensure(n))
+        return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo proposals");
+    CHECK_RC(upload(ctx, mc->patom, atoms, (size_t)n));
+    CHECK_RC(upload(ctx, mc->pdisp, disp, 3 * (size_t)n));
+    CHECK_RC(upload(ctx, mc->pu, uniform, (size_t)n));
+    McDev h;
+    CHECK_RC(mc_read_state(mc, &h));
+    const long long acc0 = h.accepted;
+    CHECK_RC(mc_begin(ctx, mc->st.as<McDev>(), n));
+    for (;;) {
+        CHECK_RC(mc_read_state(mc, &h));
+        if (h.status == kMcNeedRebuild) {
+            // lists at the current positions; the cached site energies stay valid
+            NeighborBatch &nb = mc->sys->nb;
+            CHECK_RC(neighbors_sync_positions(ctx, &nb));
+            int64_t n_pairs = 0;
+            CHECK_RC(neighbors_rebuild_lists(ctx, &nb, -1, &n_pairs));
+            CHECK_RC(neighbors_geometry(ctx, &nb, false, false));
+            CHECK_RC(mc_lists_rebuilt(ctx, mc->st.as<McDev>(), mc->dacc.as<double>(), N));
+            CHECK_RC(mc_size_trial(mc));
+            ++mc->rebuilds;
+            continue;
+        }
+        if (h.status == kMcDone || h.next >= n) break;
+        if (mc->use_graph) {
+            if (!mc->exec || mc->graph_epoch != g_alloc_epoch.load(std::memory_order_relaxed)) {
+                if (mc->exec) cudaGraphExecDestroy(mc->exec);
+                if (mc->graph) cudaGraphDestroy(mc->graph);
+                mc->exec = nullptr;
+                mc->graph = nullptr;
+                const uint64_t epoch = g_alloc_epoch.load(std::memory_order_relaxed);
+                TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+                const int64_t launches = ctx->launches;
+                int rc = TGAP_OK;
+                for (int b = 0; b < kMcBatch && !rc; ++b) rc = mc_step_body(mc);
+                cudaGraph_t g = nullptr;
+                cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+                mc->graph_kernels = ctx->launches - launches;
+                ctx->launches = launches;
+                if (rc) {
+                    if (g) cudaGraphDestroy(g);
+                    return rc;
+                }
+                if (ce != cudaSuccess) return cuda_check(ctx, ce, "graph capture");
+                // a buffer allocated during the capture would not be in the graph's view
+                if (g_alloc_epoch.load(std::memory_order_relaxed) != epoch) {
+                    cudaGraphDestroy(g);
+                    continue;
+                }
+                mc->graph = g;
+                TGAP_CUDA(ctx, cudaGraphInstantiate(&mc->exec, g, 0));
+                mc->graph_epoch = epoch;
+            }
+            TGAP_CUDA(ctx, cudaGraphLaunch(mc->exec, ctx->stream));
+            ctx->launches += mc->graph_kernels;
+        } else {
+            for (int b = 0; b < kMcBatch; ++b) CHECK_RC(mc_step_body(mc));
+        }
+    }
+    if (de_log) CHECK_RC(download(ctx, de_log, mc->log_de, (size_t)n));
+    if (acc_log) TGAP_CUDA(ctx, cudaMemcpyAsync(acc_log, mc->log_acc.ptr, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (n_accepted) *n_accepted = h.accepted - acc0;
+    return read_device_check(ctx);
+}
+
+extern "C" int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energies, double *e_total,
+                                 int64_t *accepted, int64_t *rebuilds)
+{
+    if (!mc) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = mc->ctx;
+    CHECK_RC(activate(ctx));
+    const int N = mc->sys->nb.n_atoms, M = (int)mc->models.size();
+    std::vector<double> e((size_t)M * N);
+    if (positions) CHECK_RC(download(ctx, positions, mc->sys->nb.positions, 3 * (size_t)N));
+    CHECK_RC(download(ctx, e.data(), mc->ecache, e.size()));
+    McDev h;
+    CHECK_RC(mc_read_state(mc, &h));
+    double tot = 0.0;
+    for (int i = 0; i < N; ++i) {
+        double v = 0.0;
+        for (int m = 0; m < M; ++m) v += e[(size_t)m * N + i];
+        if (energies) energies[i] = v;
+        tot += v;
+    }
+    if (e_total) *e_total = tot;
+    if (accepted) *accepted = h.accepted;
+    if (rebuilds) *rebuilds = mc->rebuilds;
     return TGAP_OK;
 }

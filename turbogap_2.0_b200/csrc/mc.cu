@@ -1,0 +1,301 @@
+// Metropolis Monte Carlo with local updates: proposal selection, trial geometry and acceptance
+// (mc_utils.f90:172-180, 215-277; mc_interface.f90:183-447). Built with --fmad=false like the
+// neighbor build, so the trial pair vectors carry the same bits as a full rebuild at the trial
+// positions would.
+#include "mc_kernels.h"
+#include "neighbors_device.cuh"
+
+namespace tgap {
+
+// Position of supercell atom j (1-based within structure S) with primitive atom `moved` (global
+// index) at pos_new, by the replication arithmetic of sc_position.
+__device__ __forceinline__ void sc_position_moved(const StructDesc &S, const double *pos, int j, int moved,
+                                                  const double *pos_new, double out[3])
+{
+    const int a = (j - 1) % S.n, r = (j - 1) / S.n;
+    const int k2 = r % S.rep[2], j2 = (r / S.rep[2]) % S.rep[1], i2 = r / (S.rep[2] * S.rep[1]);
+    const double *p = (S.atom_off + a == moved) ? pos_new : pos + 3 * (size_t)(S.atom_off + a);
+    for (int q = 0; q < 3; ++q) {
+        double v = p[q] + (double)i2 * S.pa[q];
+        v = v + (double)j2 * S.pb[q];
+        v = v + (double)k2 * S.pc[q];
+        out[q] = v;
+    }
+}
+
+__device__ __forceinline__ unsigned mc_lanemask_lt()
+{
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// One warp. mark[atom] holds the serial of the last proposal that selected it.
+__global__ void k_mc_select(McDev *st, const int64_t *__restrict__ start, const int *__restrict__ list,
+                            const int *__restrict__ jatom, const int *__restrict__ site_struct,
+                            const StructDesc *__restrict__ sd, const double *__restrict__ pos,
+                            const int *__restrict__ species_sc, McModelSel sel, double rc_sel, double skin,
+                            const int *__restrict__ prop_atom, const double *__restrict__ prop_disp,
+                            const double *__restrict__ dacc, long long *mark, int *sites, int cap, int *check)
+{
+    const int lane = threadIdx.x & 31;
+    __shared__ int s_status;
+    __shared__ long long s_serial;
+    if (lane == 0) {
+        int status = st->status;
+        if (status == kMcRunning) {
+            const long long k = st->next;
+            if (k >= st->n_prop) {
+                status = kMcDone;
+            } else {
+                const int a = prop_atom[k];
+                const double d0 = prop_disp[3 * k], d1 = prop_disp[3 * k + 1], d2 = prop_disp[3 * k + 2];
+                const double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                // list of cutoff rc + skin stays complete while every pair moved by < skin
+                if (st->maxD + dacc[a] + dn >= skin) {
+                    status = kMcNeedRebuild;
+                } else {
+                    st->atom = a;
+                    st->pos_new[0] = pos[3 * (size_t)a] + d0;
+                    st->pos_new[1] = pos[3 * (size_t)a + 1] + d1;
+                    st->pos_new[2] = pos[3 * (size_t)a + 2] + d2;
+                    st->dnorm = dn;
+                }
+            }
+            st->status = status;
+        }
+        if (status != kMcRunning)
+            for (int m = 0; m < kMcMaxModels; ++m) st->count[m] = 0;
+        s_status = status;
+        // serial of this proposal, unique over the object's lifetime (stamps mark[])
+        if (status == kMcRunning) s_serial = ++st->serial;
+    }
+    __syncwarp();
+    if (s_status != kMcRunning) return;
+    const long long serial = s_serial;
+    const int a = st->atom;
+    const double pn[3] = {st->pos_new[0], st->pos_new[1], st->pos_new[2]};
+    const StructDesc &S = sd[site_struct[a]];
+    const int ia = a - S.atom_off + 1;
+    double pa_old[3], pa_new[3];
+    sc_position(S, pos, ia, pa_old);
+    sc_position_moved(S, pos, ia, a, pn, pa_new);
+    int cnt[kMcMaxModels] = {0, 0, 0, 0};
+    auto species_of = [&](int g) { return species_sc[S.sc_off + (g - S.atom_off)]; };
+    // the moved atom first
+    if (lane == 0) mark[a] = serial;
+    {
+        const int sa = species_of(a);
+        for (int m = 0; m < sel.n_models; ++m)
+            if (sel.central_species[m] == 0 || sel.central_species[m] == sa) {
+                if (lane == 0) sites[m * cap] = a;
+                cnt[m] = 1;
+            }
+    }
+    __syncwarp();
+    const int64_t kb = start[a], ke = start[a + 1];
+    for (int64_t k0 = kb + 1; k0 < ke; k0 += 32) {
+        const int64_t k = k0 + lane;
+        bool pick = false;
+        int g = -1;
+        if (k < ke) {
+            const int jsc = list[k];
+            g = jatom[k];
+            double pj_old[3], pj_new[3], dist[3], dd;
+            sc_position(S, pos, jsc, pj_old);
+            sc_position_moved(S, pos, jsc, a, pn, pj_new);
+            get_distance_dev(pa_old, pj_old, S, dist, &dd);
+            pick = dd < rc_sel;
+            get_distance_dev(pa_new, pj_new, S, dist, &dd);
+            pick = pick || dd < rc_sel;
+        }
+        // one entry per atom: the lowest lane among equal atoms, and only if no earlier chunk
+        // (or the moved atom itself) took it
+        const unsigned peers = __match_any_sync(0xffffffffu, pick ? g : -2 - lane);
+        const bool leader = pick && (__ffs(peers) - 1 == lane);
+        const bool fresh = leader && mark[g] != serial;
+        __syncwarp();
+        if (fresh) mark[g] = serial;
+        const int sg = fresh ? species_of(g) : 0;
+        for (int m = 0; m < sel.n_models; ++m) {
+            const bool in_m = fresh && (sel.central_species[m] == 0 || sel.central_species[m] == sg);
+            const unsigned mm = __ballot_sync(0xffffffffu, in_m);
+            if (in_m) {
+                const int slot = cnt[m] + __popc(mm & mc_lanemask_lt());
+                if (slot < cap)
+                    sites[m * cap + slot] = g;
+                else
+                    check_fail(check, kCheckMcOverflow, slot, g);
+            }
+            cnt[m] += __popc(mm);
+        }
+        __syncwarp();
+    }
+    if (lane == 0)
+        for (int m = 0; m < kMcMaxModels; ++m) st->count[m] = m < sel.n_models ? min(cnt[m], cap) : 0;
+}
+
+// Warp per (model, row).
+__global__ void k_mc_trial_geometry(const McDev *st, int n_models, const int *__restrict__ sites, int cap, int pmax,
+                                    const int64_t *__restrict__ start, const int *__restrict__ list,
+                                    const int *__restrict__ nspecies, const int *__restrict__ site_struct,
+                                    const StructDesc *__restrict__ sd, const double *__restrict__ pos,
+                                    double *__restrict__ txyz, double *__restrict__ trjs, int *__restrict__ tnsp,
+                                    int *check)
+{
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w >= n_models * cap) return;
+    const int m = w / cap, r = w - m * cap;
+    const size_t base = (size_t)w * pmax;
+    int ns = 0, g = 0;
+    if (st->status == kMcRunning && r < st->count[m]) {
+        g = sites[m * cap + r];
+        ns = (int)(start[g + 1] - start[g]);
+        if (ns > pmax) {
+            if (lane == 0) check_fail(check, kCheckMcOverflow, g, ns);
+            ns = pmax;
+        }
+    }
+    const int a = st->atom;
+    const double pn[3] = {st->pos_new[0], st->pos_new[1], st->pos_new[2]};
+    for (int t = lane; t < pmax; t += 32) {
+        double x0 = 0.0, x1 = 0.0, x2 = 0.0, rr = 0.0;
+        int sp = 0;
+        if (t < ns) {
+            const int64_t k = start[g] + t;
+            sp = nspecies[k];
+            if (t > 0) {
+                const StructDesc &S = sd[site_struct[g]];
+                double pi[3], pj[3], dist[3];
+                sc_position_moved(S, pos, g - S.atom_off + 1, a, pn, pi);
+                sc_position_moved(S, pos, list[k], a, pn, pj);
+                get_distance_dev(pi, pj, S, dist, &rr);
+                x0 = dist[0];
+                x1 = dist[1];
+                x2 = dist[2];
+            }
+        }
+        txyz[3 * (base + t)] = x0;
+        txyz[3 * (base + t) + 1] = x1;
+        txyz[3 * (base + t) + 2] = x2;
+        trjs[base + t] = rr;
+        tnsp[base + t] = sp;
+    }
+}
+
+// One warp: dE in a fixed reduction order, then the reference's acceptance test.
+__global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sites, int cap,
+                            const double *__restrict__ etrial, double *__restrict__ ecache, int n_atoms,
+                            double *__restrict__ pos, double *__restrict__ dacc, const double *__restrict__ prop_u,
+                            double temperature, double *__restrict__ log_de, unsigned char *__restrict__ log_acc)
+{
+    const int lane = threadIdx.x & 31;
+    if (st->status != kMcRunning) return;
+    const long long k = st->next;
+    double de = 0.0;
+    for (int m = 0; m < n_models; ++m) {
+        const int c = st->count[m];
+        for (int r = lane; r < c; r += 32)
+            de += etrial[(size_t)m * cap + r] - ecache[(size_t)m * n_atoms + sites[m * cap + r]];
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
+    int accept = 0;
+    if (lane == 0) {
+        // mc_utils.f90:172-180: kB is a default-real literal; get_mc_acceptance (:255) takes
+        // min(1, p); mc_interface.f90:286 accepts when p > ranf
+        const double kB = (double)8.617333262e-5f;
+        double p = exp(-de / (kB * temperature));
+        p = p < 1.0 ? p : 1.0;
+        accept = p > prop_u[k] ? 1 : 0;
+        if (log_de) log_de[k] = de;
+        if (log_acc) log_acc[k] = (unsigned char)accept;
+    }
+    accept = __shfl_sync(0xffffffffu, accept, 0);
+    if (accept) {
+        for (int m = 0; m < n_models; ++m) {
+            const int c = st->count[m];
+            for (int r = lane; r < c; r += 32)
+                ecache[(size_t)m * n_atoms + sites[m * cap + r]] = etrial[(size_t)m * cap + r];
+        }
+        if (lane == 0) {
+            const int a = st->atom;
+            pos[3 * (size_t)a] = st->pos_new[0];
+            pos[3 * (size_t)a + 1] = st->pos_new[1];
+            pos[3 * (size_t)a + 2] = st->pos_new[2];
+            dacc[a] += st->dnorm;
+            if (dacc[a] > st->maxD) st->maxD = dacc[a];
+            st->accepted += 1;
+        }
+    }
+    __syncwarp();
+    if (lane == 0) st->next = k + 1;
+}
+
+__global__ void k_mc_begin(McDev *st, long long n_prop)
+{
+    st->next = 0;
+    st->n_prop = n_prop;
+    if (st->status != kMcNeedRebuild) st->status = kMcRunning;
+}
+
+__global__ void k_mc_lists_rebuilt(McDev *st, double *dacc, int n)
+{
+    const int g = blockIdx.x * blockDim.x + threadIdx.x;
+    if (g < n) dacc[g] = 0.0;
+    if (g == 0) {
+        st->maxD = 0.0;
+        if (st->status == kMcNeedRebuild) st->status = kMcRunning;
+    }
+}
+
+int mc_select(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McModelSel &sel, double rc_sel,
+              double skin, const int *d_prop_atom, const double *d_prop_disp, const double *d_dacc,
+              long long *d_mark, int *d_sites, int cap)
+{
+    k_mc_select<<<1, 32, 0, ctx->stream>>>(d_st, nb.start.as<int64_t>(), nb.list.as<int>(), nb.jatom.as<int>(),
+                                           nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(),
+                                           nb.positions.as<double>(), nb.species_sc.as<int>(), sel, rc_sel, skin,
+                                           d_prop_atom, d_prop_disp, d_dacc, d_mark, d_sites, cap, ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_trial_geometry(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
+                      const int *d_sites, int cap, int pmax, double *d_txyz, double *d_trjs, int *d_tnsp)
+{
+    const int warps = n_models * cap, T = 128;
+    k_mc_trial_geometry<<<(warps + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+        d_st, n_models, d_sites, cap, pmax, nb.start.as<int64_t>(), nb.list.as<int>(), nb.nspecies.as<int>(),
+        nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(), nb.positions.as<double>(), d_txyz, d_trjs, d_tnsp,
+        ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
+              double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
+              double temperature, double *d_log_de, unsigned char *d_log_acc)
+{
+    k_mc_accept<<<1, 32, 0, ctx->stream>>>(d_st, n_models, d_sites, cap, d_etrial, d_ecache, n_atoms, d_positions,
+                                           d_dacc, d_prop_u, temperature, d_log_de, d_log_acc);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_begin(tgap_context *ctx, McDev *d_st, long long n_prop)
+{
+    k_mc_begin<<<1, 1, 0, ctx->stream>>>(d_st, n_prop);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_lists_rebuilt(tgap_context *ctx, McDev *d_st, double *d_dacc, int n_atoms)
+{
+    k_mc_lists_rebuilt<<<(n_atoms + 255) / 256, 256, 0, ctx->stream>>>(d_st, d_dacc, n_atoms);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+}  // namespace tgap

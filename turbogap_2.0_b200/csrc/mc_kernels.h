@@ -1,0 +1,63 @@
+// Metropolis Monte Carlo with local updates (mc.cu): device state and launchers.
+//
+// One proposal = move atom a by d. The sites whose descriptor can change are a and every atom
+// within the largest model cutoff of a's old or new position; only those are re-evaluated
+// (trial pair geometry -> descriptor forward -> GAP energy rows), the energy change is the sum
+// of (new - cached) site energies, and the move is accepted when
+// min(1, exp(-dE / (kB T))) > u (mc_utils.f90:172-180, :255; mc_interface.f90:245-300), with
+// the reference's kB literal taken in default-real precision.
+#pragma once
+
+#include "neighbors.h"
+
+namespace tgap {
+
+constexpr int kMcMaxModels = 4;
+
+// Device-resident driver state (one per MC object).
+struct McDev {
+    long long next;      // proposals of the current run consumed so far
+    long long n_prop;    // proposals of the current run
+    long long accepted;  // accepted moves since creation
+    long long serial;    // proposals selected since creation (stamps of the dedupe marks)
+    int status;          // kMcRunning / kMcNeedRebuild / kMcDone
+    int atom;            // atom moved by the proposal in flight
+    double pos_new[3];   // its trial position
+    double dnorm;        // |d|
+    double maxD;         // largest accumulated displacement since the last list build
+    int count[kMcMaxModels];  // affected sites per model for the proposal in flight
+};
+
+enum McStatus { kMcRunning = 0, kMcNeedRebuild = 1, kMcDone = 2 };
+
+struct McModelSel {
+    int n_models;
+    int central_species[kMcMaxModels];  // 0: every site
+};
+
+// Selects the affected sites of proposal st->next into sites[m * cap + r] (list order,
+// duplicates removed). Sets st->status = kMcNeedRebuild when the move could carry a pair of the
+// skin-padded list inside the cutoff unseen (max accumulated displacement + this atom's + |d|
+// >= skin), kMcDone when the run's proposals are exhausted.
+int mc_select(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McModelSel &sel, double rc_sel,
+              double skin, const int *d_prop_atom, const double *d_prop_disp, const double *d_dacc,
+              long long *d_mark, int *d_sites, int cap);
+
+// Pair geometry of the affected sites with the moved atom at its trial position, written as a
+// fixed-stride list: row r of model m holds its site's list pairs at [r * pmax, (r+1) * pmax),
+// unused slots and rows blind (species 0).
+int mc_trial_geometry(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
+                      const int *d_sites, int cap, int pmax, double *d_txyz, double *d_trjs, int *d_tnsp);
+
+// Energy change, acceptance and commit (positions, cached site energies, displacement
+// bookkeeping); logs dE and the decision of proposal st->next and advances it.
+int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
+              double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
+              double temperature, double *d_log_de, unsigned char *d_log_acc);
+
+// Start of a run of n proposals (keeps a pending rebuild request), and the reset after a list
+// rebuild.
+int mc_begin(tgap_context *ctx, McDev *d_st, long long n_prop);
+int mc_lists_rebuilt(tgap_context *ctx, McDev *d_st, double *d_dacc, int n_atoms);
+
+}  // namespace tgap

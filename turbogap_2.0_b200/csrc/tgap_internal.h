@@ -126,6 +126,7 @@ enum CheckCode {
     kCheckSelfAtom = 4,     // adjoint: self-slot atom index out of range
     kCheckNonFinite = 5,    // velocity Verlet: non-finite force
     kCheckListOverrun = 6,  // neighbor fill wrote past its counted range
+    kCheckMcOverflow = 7,   // Monte Carlo: affected sites or pairs beyond the trial capacity
 };
 
 #ifdef __CUDACC__

@@ -116,6 +116,10 @@ def lib():
         "tgap_md_set_velocities": (i32, [vp, vp]),
         "tgap_md_run": (i32, [vp, i32]),
         "tgap_md_get_state": (i32, [vp, vp, vp, vp, P(dbl), P(dbl)]),
+        "tgap_mc_create": (i32, [vp, vp, i32, vp, dbl, i32, i32, P(vp)]),
+        "tgap_mc_destroy": (i32, [vp]),
+        "tgap_mc_run": (i32, [vp, i64, vp, vp, vp, P(i64), vp, vp]),
+        "tgap_mc_get_state": (i32, [vp, vp, vp, P(dbl), P(i64), P(i64)]),
         "tgap_debug_poly3_w": (i32, [i32, vp]),
         "tgap_calculate_gap_soap": (i32, [vp, vp, i32, vp, i32, vp, i32, vp, vp, vp]),
         "tgap_timing_enable": (i32, [vp, i32]),

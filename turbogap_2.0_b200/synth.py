@@ -141,3 +141,14 @@ def gap_model(q_pool, n_sparse, seed=0, zeta=4.0, delta=1.0, alpha_var=1e-6):
     Qs = np.ascontiguousarray(q_pool[idx], dtype=np.float64)
     alphas = rng.normal(0.0, np.sqrt(alpha_var), n_sparse)
     return dict(Qs=Qs, alphas=alphas, zeta=zeta, delta=delta)
+
+
+def mc_proposals(n_atoms, n, radius, seed=0):
+    """Single-atom Monte Carlo proposals: atoms uniform over [0, n_atoms), displacements uniform
+    in a ball of `radius` (A), and the uniform deviates of the acceptance test."""
+    rng = np.random.default_rng(seed)
+    atoms = rng.integers(0, n_atoms, size=n).astype(np.int32)
+    d = rng.normal(size=(n, 3))
+    d *= (radius * rng.random(n) ** (1.0 / 3.0) / np.linalg.norm(d, axis=1))[:, None]
+    u = rng.random(n)
+    return atoms, d, u
