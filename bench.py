@@ -32,6 +32,11 @@ WORKLOAD = ("NVE velocity-Verlet MD, 4096 C atoms, 2.5 g/cm3, dt 1 fs, rebuild e
             "skin 0.3 A, SOAP n_max=l_max=8 rcut 3.7/3.2, GAP 2000 sparse zeta=4")
 N_ATOMS = 4096
 N_SPARSE = 2000
+MC_ATOMS, MC_DENSITY, MC_T, MC_RADIUS, MC_SKIN = 1000, 2.0, 2000.0, 0.2, 0.5
+MC_PROPOSALS = 20000
+MC_WORKLOAD = ("NVT Metropolis MC, 1000 C atoms, 2.0 g/cm3, 2000 K, single-atom moves uniform in a 0.2 A ball, "
+               "local SOAP/GAP update of atoms within rcut of the moved atom (exact GAP, no screen), "
+               "same SOAP settings and 2000-sparse GAP as the MD workload")
 DT = 1.0
 REBUILD = 10
 SKIN = 0.3
@@ -357,6 +362,68 @@ def _cpu_baseline(tg, pos, box, sp, masses, vel, model_np):
                        f"materialised dq/dr as in the reference; not TurboGAP itself)")
 
 
+def _mc_leg(tg, torch, ctx, stream, model, n_prop, seed):
+    """MC moves/s of the local-update driver (both precisions) on the 1000-atom box: CUDA events
+    around tgap_mc_run (its host loop, list rebuilds and graph launches included)."""
+    pos, box, sp, _ = tg.synth.random_packing(MC_ATOMS, MC_DENSITY, 1.2, seed=seed)
+    atoms, disp, u = tg.synth.mc_proposals(MC_ATOMS, n_prop + 256, MC_RADIUS, seed=seed + 1)
+    out = {}
+    for name, prec in (("mixed", tg.TGAP_MIXED), ("fp64", tg.TGAP_FP64)):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + MC_SKIN)
+        mc = tg.MC(ctx, system, [model], MC_T, precision=prec)
+        mc.run(atoms[:256], disp[:256], u[:256], logs=False)  # warm-up: graph capture, first rebuilds
+        st0 = mc.state()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = mc.run(atoms[256:], disp[256:], u[256:], logs=False)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        st1 = mc.state()
+        out[name] = dict(moves_per_s=n_prop / (ms * 1e-3), us_per_move=1e3 * ms / n_prop,
+                         acceptance=r["accepted"] / n_prop, list_rebuilds=st1["rebuilds"] - st0["rebuilds"])
+        mc.close()
+        system.close()
+    return dict(workload=MC_WORKLOAD, proposals=n_prop, unit="moves/s", value=out["mixed"]["moves_per_s"],
+                mixed=out["mixed"], plain_fp64=out["fp64"],
+                speedup_mixed_vs_fp64=out["mixed"]["moves_per_s"] / out["fp64"]["moves_per_s"])
+
+
+def _mc_cpu_baseline(tg, model_np, seed, budget_s=10.0):
+    """The reference's MC semantics on the host cores: every proposal re-evaluates the whole
+    1000-atom box with the FP64 oracle restatement (calculate_mc_step -> full calculate_gap_soap)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_lib as orc
+    hyp = tg.synth.carbon_hypers()
+    H = orc.Hypers(hyp)
+    pos, box, sp, _ = tg.synth.random_packing(MC_ATOMS, MC_DENSITY, 1.2, seed=seed)
+    atoms, disp, u = tg.synth.mc_proposals(MC_ATOMS, 100000, MC_RADIUS, seed=seed + 1)
+    kb = float(np.float32(8.617333262e-5))
+
+    def energy(x):
+        nb = orc.build_neighbors(x, MC_ATOMS, *box, 3.7, sp, False)
+        e, _, _ = orc.get_gap_soap(H, MC_ATOMS, nb, sp, 0, model_np["alphas"], model_np["Qs"], model_np["delta"],
+                                   model_np["zeta"], False)
+        return e.sum()
+
+    x = pos.copy()
+    e_cur = energy(x)
+    t0 = time.perf_counter()
+    k = 0
+    while time.perf_counter() - t0 < budget_s:
+        y = x.copy()
+        y[atoms[k]] += disp[k]
+        e_new = energy(y)
+        if min(1.0, np.exp(-(e_new - e_cur) / (kb * MC_T))) > u[k]:
+            x, e_cur = y, e_new
+        k += 1
+    secs = time.perf_counter() - t0
+    return dict(value=k / secs, unit="moves/s", cores=orc.num_threads(), kind="port",
+                sample=f"{k} proposals on the 1000-atom box, full FP64 re-evaluation per proposal as the "
+                       f"reference does (oracle restatement with OpenMP; not TurboGAP itself)")
+
+
 def run_ours(args):
     import torch
     tg = _load_package()
@@ -451,9 +518,11 @@ def run_ours(args):
         t = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
         dist.all_reduce(t, op=dist.ReduceOp.MIN)
         e2e["value"] = float(t[0]) * world
+    mc_line = _mc_leg(tg, torch, ctx, stream, model, MC_PROPOSALS, 300 + seed)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = _cpu_baseline(tg, pos, box, sp, masses, vel, model_np)
+        mc_line["cpu_baseline"] = _mc_cpu_baseline(tg, model_np, 300 + seed)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "atom-steps/s", "n_gpus": world, "steps": args.steps,
@@ -470,6 +539,7 @@ def run_ours(args):
             "roofline": roof,
             "stages_us_per_step": {k: v["total_ms"] * 1e3 / 20 for k, v in stages.items()},
             "cpu_baseline": cpu,
+            "mc": mc_line,
             "e2e": e2e,
             "gpu_launches": launches,
             "clocks": clk,
