@@ -8,6 +8,8 @@
 //          partials and G = zeta delta^2 alpha o K^(zeta-1), written back as a bf16 split
 //   GEMM2  g = G Qs         (rows x descriptor, K-dim = n_sparse)   epilogue: FP32 store
 //
+// For descriptor widths up to 384 both are fused into k_gap_flash (G stays on the SM).
+//
 // Persistent kernel, one CTA per SM over 128 x BN tiles: one thread issues TMA loads (no
 // multicast) into a STAGES-deep ring of 128B-swizzled shared-memory tiles, one thread issues
 // tcgen05.mma (cta_group::1, kind::f16) into one of two TMEM accumulator buffers, and eight
@@ -233,15 +235,18 @@ struct EpiStoreF32 {
 
 // Persistent, warp-specialised: CTA c takes tiles c, c + gridDim.x, ... (tile = m_tile * n_tiles
 // + n_tile). Warp 0 (one lane) streams A/B hi/lo k-blocks into the STAGES-deep ring, warp 1
-// (one lane) issues the MMAs of a tile into one of two TMEM accumulator buffers (128 columns
-// apart), warps 2..9 drain the other buffer through the epilogue, so a tile's epilogue overlaps
+// (one lane) issues the MMAs of a tile into one of two TMEM accumulator buffers (TmemPlan), warps 2..9 drain the other buffer through the epilogue, so a tile's epilogue overlaps
 // the next tile's loads and MMAs. Epilogue warp w reads TMEM lanes 32 (w % 4) .. +31 (= tile
 // rows) and one half of the tile's columns ((w - 2) / 4); its epilogue part index is
 // 2 tile_n + half.
 constexpr int kEpiWarps = 8;
 constexpr int kTcWarps = 2 + kEpiWarps;
 constexpr int kTcThreadsP = 32 * kTcWarps;
-constexpr uint32_t kTmemCols = 256;  // two accumulator buffers of up to 128 columns
+// Two TMEM accumulator buffers: BN <= 128 columns each in 256 allocated columns, or 256 each in 512.
+template <int BN> struct TmemPlan {
+    static constexpr uint32_t buf = BN <= 128 ? 128u : 256u;  // column stride of the buffers
+    static constexpr uint32_t cols = 2 * buf;                  // allocation (power of two)
+};
 
 template <int BN, int STAGES, class Epi>
 __global__ void __launch_bounds__(kTcThreadsP, 1)
@@ -249,7 +254,8 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
                   const __grid_constant__ CUtensorMap tmB_hi, const __grid_constant__ CUtensorMap tmB_lo,
                   int n_tiles_n, int n_tiles, int num_kb, Epi epi, int *err_flag)
 {
-    static_assert(BN % 32 == 0 && BN >= 32 && BN <= 128, "BN: multiple of 32 in 32..128");
+    static_assert(BN % 32 == 0 && BN >= 32 && BN <= 256, "BN: multiple of 32 in 32..256");
+    constexpr uint32_t kTmemCols = TmemPlan<BN>::cols, kBuf = TmemPlan<BN>::buf;
     constexpr uint32_t A_BYTES = kBM * kBK * 2;
     constexpr uint32_t B_BYTES = BN * kBK * 2;
     constexpr uint32_t STAGE_BYTES = 2 * A_BYTES + 2 * B_BYTES;
@@ -340,7 +346,7 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
                     break;
                 }
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                const uint32_t acc = tmem + (uint32_t)(b * 128);
+                const uint32_t acc = tmem + (uint32_t)b * kBuf;
                 for (int kb = 0; kb < num_kb; ++kb, ++it) {
                     const int s = it % STAGES;
                     const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
@@ -389,7 +395,7 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
             const int row = (t / n_tiles_n) * kBM + r_local;
             const int tile_n = t % n_tiles_n, c0 = tile_n * BN + half * HB;
             const uint32_t taddr =
-                tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)(b * 128) + (uint32_t)(half * HB);
+                tmem + ((uint32_t)(quarter * 32) << 16) + (uint32_t)b * kBuf + (uint32_t)(half * HB);
             float acc;
             epi.begin(acc);
 #pragma unroll 1
@@ -420,6 +426,342 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols)
                      : "memory");
+    }
+}
+
+// ---------------------------------------------------------------------------- fused GAP kernel
+
+// Energies and dE/dq of a 128-row tile against a chunk of T sparse tiles of 128 points, without
+// writing G (flash-style): per sparse tile j
+//   S = q Q_j^T                       (tcgen05 bf16x3, TMEM columns [0, 128))
+//   W = zeta delta^2 alpha o S^(zeta-1)  (epilogue warps: registers -> bf16 hi/lo in shared memory,
+//                                       in the 128B-swizzled K-major layout the MMA reads)
+//   g += W Q_j                        (tcgen05 bf16x3, N = DP split in two halves, TMEM [128, 128+DP))
+// energies += delta^2 sum alpha S^zeta. MMA order S_{j+1} before g_j lets the epilogue of tile
+// j+1 overlap the tensor work of tile j. At the end the tile's g partial is added to global g with
+// vector atomics (g zeroed by the caller), energies with FP64 atomics.
+// Warps: 0 TMA producer, 1 MMA issuer (+ TMEM owner), 2..9 epilogue (rows 32 (w % 4) + lane,
+// columns half = (w - 2) / 4 of the tile). Shared memory: two 64 KB ring slots, W (64 KB).
+constexpr int kFlashEpiWarps = 8;
+constexpr int kFlashThreads = 32 * (2 + kFlashEpiWarps);
+constexpr uint32_t kFlashSlot = 64 * 1024;
+constexpr uint32_t kFlashW = 64 * 1024;
+constexpr int kFlashStages = 2;
+constexpr size_t kFlashSmem = kFlashStages * (size_t)kFlashSlot + kFlashW + 1024;
+
+struct FlashGap {
+    const float *alphas;  // [m_pad]
+    int n_rows;
+    const int *sites;     // row -> atom (null: identity)
+    double *energies;     // += delta^2 sum alpha k^zeta (+ e0 once per row)
+    double *e_rows;       // optional per-row copy (zeroed by the caller)
+    double d2, e0;
+    float zd2, zeta;
+    int zeta_int;
+    float *g;             // dE/dq [rows_pad][ldg], accumulated (zeroed by the caller); null: energies only
+    int ldg;
+};
+
+template <int ZI>
+__device__ __forceinline__ void flash_w16(const float v[16], const float *__restrict__ alpha16, float zd2, float zeta,
+                                          float &eacc, uint32_t hi[8], uint32_t lo[8])
+{
+    const float4 *a4 = reinterpret_cast<const float4 *>(alpha16);
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const float4 a = a4[q];
+        const float av[4] = {a.x, a.y, a.z, a.w};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int j = 4 * q + 2 * h;
+            const float ak0 = av[2 * h] * kpow_zm1<ZI>(v[j], zeta);
+            const float ak1 = av[2 * h + 1] * kpow_zm1<ZI>(v[j + 1], zeta);
+            eacc = fmaf(ak0, v[j], eacc);
+            eacc = fmaf(ak1, v[j + 1], eacc);
+            const float g0 = zd2 * ak0, g1 = zd2 * ak1;
+            const __nv_bfloat162 h2 = __floats2bfloat162_rn(g0, g1);
+            const float2 hf = __bfloat1622float2(h2);
+            const __nv_bfloat162 l2 = __floats2bfloat162_rn(g0 - hf.x, g1 - hf.y);
+            hi[j / 2] = *reinterpret_cast<const uint32_t *>(&h2);
+            lo[j / 2] = *reinterpret_cast<const uint32_t *>(&l2);
+        }
+    }
+}
+
+__device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t b, uint32_t c, uint32_t d)
+{
+    asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
+}
+
+template <int DP>
+__global__ void __launch_bounds__(kFlashThreads, 1)
+    k_gap_flash(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
+                const __grid_constant__ CUtensorMap tm_Q_hi, const __grid_constant__ CUtensorMap tm_Q_lo,
+                const __grid_constant__ CUtensorMap tm_QT_hi, const __grid_constant__ CUtensorMap tm_QT_lo,
+                int n_chunks, int tiles_per_chunk, FlashGap p, int *err_flag)
+{
+    static_assert(DP % 128 == 0 && DP <= 384, "descriptor padding: 128, 256 or 384");
+    constexpr int KB = DP / kBK;   // k-blocks of S
+    constexpr int NH = DP / 2;     // N of each g half
+    constexpr uint32_t TILE = kBM * kBK * 2;  // one 128 x 64 bf16 tile (16 KB)
+    constexpr uint32_t B2 = NH * kBK * 2;     // one NH x 64 bf16 tile of Q^T
+    constexpr uint32_t IDESC_S = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+                                 ((uint32_t)(kBM >> 4) << 24);
+    constexpr uint32_t IDESC_G = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
+                                 ((uint32_t)(kBM >> 4) << 24);
+    constexpr uint32_t kCols = 512;
+    const bool forces = p.g != nullptr;
+
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_full[kFlashStages], bar_empty[kFlashStages];
+    __shared__ __align__(8) uint64_t bar_sfull, bar_sfree, bar_wfull, bar_wempty, bar_drain;
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ volatile int abort_flag;
+    __shared__ int issued, consumed;
+
+    const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const uint32_t wbase = base + kFlashStages * kFlashSlot;  // W: hi kb0, hi kb1, lo kb0, lo kb1
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int unit = blockIdx.x, rt = unit / n_chunks, ch = unit - rt * n_chunks;
+    const int T = tiles_per_chunk, j0 = ch * T, m0 = rt * kBM;
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < kFlashStages; ++s) {
+            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_empty[s]), 1);
+        }
+        mbar_init(smem_u32(&bar_sfull), 1);
+        mbar_init(smem_u32(&bar_sfree), 32 * kFlashEpiWarps);
+        mbar_init(smem_u32(&bar_wfull), 32 * kFlashEpiWarps);
+        mbar_init(smem_u32(&bar_wempty), 1);
+        mbar_init(smem_u32(&bar_drain), 1);
+        abort_flag = 0;
+        issued = 0;
+        consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const CUtensorMap *maps[6] = {&tm_q_hi, &tm_q_lo, &tm_Q_hi, &tm_Q_lo, &tm_QT_hi, &tm_QT_lo};
+        for (int i = 0; i < 6; ++i) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)maps[i]) : "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_slot;
+    const uint32_t tS = tmem, tG = tmem + 128;
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer: S_0 blocks, then per tile t: S_{t+1} blocks, g_t blocks (the MMA order)
+            int it = 0;
+            auto acquire = [&](uint32_t &slot, uint32_t &fb) -> bool {
+                const int s = it % kFlashStages;
+                const uint32_t ph = (uint32_t)(it / kFlashStages) & 1u;
+                if (it >= kFlashStages && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) return false;
+                slot = base + s * kFlashSlot;
+                fb = smem_u32(&bar_full[s]);
+                return true;
+            };
+            auto load_s = [&](int j) -> bool {
+                for (int kb = 0; kb < KB; ++kb) {
+                    uint32_t slot, fb;
+                    if (!acquire(slot, fb)) return false;
+                    mbar_expect_tx(fb, 4 * TILE);
+                    tma_load_2d(slot, &tm_q_hi, fb, kb * kBK, m0);
+                    tma_load_2d(slot + TILE, &tm_q_lo, fb, kb * kBK, m0);
+                    tma_load_2d(slot + 2 * TILE, &tm_Q_hi, fb, kb * kBK, j * 128);
+                    tma_load_2d(slot + 3 * TILE, &tm_Q_lo, fb, kb * kBK, j * 128);
+                    issued = ++it;
+                }
+                return true;
+            };
+            auto load_g = [&](int j) -> bool {
+                for (int kb = 0; kb < 2; ++kb)
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t slot, fb;
+                        if (!acquire(slot, fb)) return false;
+                        mbar_expect_tx(fb, 2 * B2);
+                        tma_load_2d(slot, &tm_QT_hi, fb, j * 128 + kb * kBK, h * NH);
+                        tma_load_2d(slot + B2, &tm_QT_lo, fb, j * 128 + kb * kBK, h * NH);
+                        issued = ++it;
+                    }
+                return true;
+            };
+            bool ok = load_s(j0);
+            for (int t = 0; t < T && ok; ++t) {
+                if (t + 1 < T) ok = load_s(j0 + t + 1);
+                if (ok && forces) ok = load_g(j0 + t);
+            }
+            if (!ok) abort_flag = 1;
+            // tail: the last slots' releases land before the CTA exits (bounded)
+            for (int i = (it > kFlashStages ? it - kFlashStages : 0); i < it && !abort_flag; ++i)
+                if (!mbar_wait(smem_u32(&bar_empty[i % kFlashStages]), (uint32_t)(i / kFlashStages) & 1u, &abort_flag))
+                    abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0) {
+            int it = 0;
+            auto take = [&](uint32_t &slot) -> bool {
+                const int s = it % kFlashStages;
+                if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(it / kFlashStages) & 1u, &abort_flag)) return false;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                slot = base + s * kFlashSlot;
+                return true;
+            };
+            auto release = [&]() {
+                umma_commit(smem_u32(&bar_empty[it % kFlashStages]));
+                consumed = ++it;
+            };
+            auto mma_s = [&]() -> bool {
+                for (int kb = 0; kb < KB; ++kb) {
+                    uint32_t slot;
+                    if (!take(slot)) return false;
+#pragma unroll
+                    for (int k = 0; k < kBK / 16; ++k) {
+                        const uint64_t ahi = umma_desc(slot + 32 * k), alo = umma_desc(slot + TILE + 32 * k);
+                        const uint64_t bhi = umma_desc(slot + 2 * TILE + 32 * k);
+                        const uint64_t blo = umma_desc(slot + 3 * TILE + 32 * k);
+                        umma_bf16(tS, ahi, bhi, IDESC_S, (kb > 0 || k > 0) ? 1u : 0u);
+                        umma_bf16(tS, ahi, blo, IDESC_S, 1u);
+                        umma_bf16(tS, alo, bhi, IDESC_S, 1u);
+                    }
+                    release();
+                }
+                umma_commit(smem_u32(&bar_sfull));
+                return true;
+            };
+            auto mma_g = [&](int t) -> bool {
+                if (!mbar_wait(smem_u32(&bar_wfull), (uint32_t)t & 1u, &abort_flag)) return false;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int kb = 0; kb < 2; ++kb)
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t slot;
+                        if (!take(slot)) return false;
+                        const uint32_t whi = wbase + kb * TILE, wlo = wbase + (2 + kb) * TILE;
+#pragma unroll
+                        for (int k = 0; k < kBK / 16; ++k) {
+                            const uint64_t ahi = umma_desc(whi + 32 * k), alo = umma_desc(wlo + 32 * k);
+                            const uint64_t bhi = umma_desc(slot + 32 * k), blo = umma_desc(slot + B2 + 32 * k);
+                            const uint32_t d = tG + (uint32_t)(h * NH);
+                            umma_bf16(d, ahi, bhi, IDESC_G, (t > 0 || kb > 0 || k > 0) ? 1u : 0u);
+                            umma_bf16(d, ahi, blo, IDESC_G, 1u);
+                            umma_bf16(d, alo, bhi, IDESC_G, 1u);
+                        }
+                        release();
+                    }
+                umma_commit(smem_u32(&bar_wempty));
+                return true;
+            };
+            bool ok = mma_s();
+            for (int t = 0; t < T && ok; ++t) {
+                if (t + 1 < T) {
+                    ok = mbar_wait(smem_u32(&bar_sfree), (uint32_t)t & 1u, &abort_flag);
+                    if (ok) ok = mma_s();
+                }
+                if (ok && forces) ok = mma_g(t);
+            }
+            if (!ok) abort_flag = 1;
+            // every MMA issued so far has completed once bar_drain fires (bounded)
+            umma_commit(smem_u32(&bar_drain));
+            volatile int never = 0;
+            mbar_wait(smem_u32(&bar_drain), 0, &never);
+        }
+    } else {
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const int r = quarter * 32 + lane, row = m0 + r;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        float eacc = 0.0f;
+        bool ok = true;
+        for (int t = 0; t < T && ok; ++t) {
+            const int j = j0 + t;
+            ok = mbar_wait(smem_u32(&bar_sfull), (uint32_t)t & 1u, &abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (!ok || abort_flag) break;
+            uint32_t hi[4][8], lo[4][8];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                float v[16];
+                tmem_ld16(tS + lane_base + (uint32_t)(half * 64 + c * 16), v);
+                const float *a16 = p.alphas + j * 128 + half * 64 + c * 16;
+                switch (p.zeta_int) {
+                case 1: flash_w16<1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 2: flash_w16<2>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 3: flash_w16<3>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 4: flash_w16<4>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 5: flash_w16<5>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 6: flash_w16<6>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                default: flash_w16<-1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                }
+            }
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(smem_u32(&bar_sfree));  // S may be overwritten
+            if (!forces) continue;
+            if (t > 0) {
+                ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(t - 1) & 1u, &abort_flag);
+                if (!ok) break;
+            }
+            // W row r, columns half * 64 .. + 64 = k-block `half` of the K-major 128B-swizzled tile:
+            // 16-byte chunk c of the row sits at chunk c ^ (r % 8)
+            const uint32_t rhi = wbase + half * TILE + r * 128, rlo = wbase + (2 + half) * TILE + r * 128;
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const uint32_t chunk = (uint32_t)((2 * c + u) ^ (r & 7)) * 16;
+                    st_shared_v4(rhi + chunk, hi[c][4 * u], hi[c][4 * u + 1], hi[c][4 * u + 2], hi[c][4 * u + 3]);
+                    st_shared_v4(rlo + chunk, lo[c][4 * u], lo[c][4 * u + 1], lo[c][4 * u + 2], lo[c][4 * u + 3]);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            mbar_arrive(smem_u32(&bar_wfull));
+        }
+        if (ok && !abort_flag && row < p.n_rows) {
+            double e = p.d2 * (double)eacc;
+            if (ch == 0 && half == 0) e += p.e0;
+            if (p.energies) atomicAdd(p.energies + (p.sites ? p.sites[row] : row), e);
+            if (p.e_rows) atomicAdd(p.e_rows + row, e);
+        }
+        if (ok && !abort_flag && forces) {
+            ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(T - 1) & 1u, &abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (ok && !abort_flag) {
+#pragma unroll 1
+                for (int c = 0; c < NH; c += 16) {
+                    float v[16];
+                    tmem_ld16(tG + lane_base + (uint32_t)(half * NH + c), v);
+                    if (row < p.n_rows) {
+                        float4 *dst = reinterpret_cast<float4 *>(p.g + (size_t)row * p.ldg + half * NH + c);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            atomicAdd(dst + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+                    }
+                }
+            }
+        }
+        if (!ok) abort_flag = 1;
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (abort_flag) {
+        if (threadIdx.x == 0) {
+            atomicExch(err_flag, 1);
+            volatile int dummy = 0;
+            for (int i = consumed; i < issued; ++i)
+                mbar_wait(smem_u32(&bar_full[i % kFlashStages]), (uint32_t)(i / kFlashStages) & 1u, &dummy);
+        }
+        __syncthreads();
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
     }
 }
 
@@ -494,6 +836,52 @@ static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, c
     return TGAP_OK;
 }
 
+// Chunks of the sparse tiles per row tile: the fewest waves of (row tiles x chunks) CTAs times
+// the tiles each CTA runs; ties go to fewer chunks (fewer g atomics).
+static int flash_chunks(int n_rt, int J, int sms)
+{
+    int best = 1;
+    long best_cost = -1;
+    for (int nc = 1; nc <= J; ++nc) {
+        if (J % nc) continue;
+        const long waves = ((long)n_rt * nc + sms - 1) / sms;
+        const long cost = waves * (J / nc);
+        if (best_cost < 0 || cost < best_cost) {
+            best = nc;
+            best_cost = cost;
+        }
+    }
+    return best;
+}
+
+template <int DP>
+static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi, const __nv_bfloat16 *q_lo,
+                        int rows_pad, const FlashGap &p)
+{
+    constexpr int NH = DP / 2;
+    CUtensorMap tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo;
+    int rc;
+    if ((rc = make_map(ctx, &tq_hi, q_hi, rows_pad, DP, kBM)) || (rc = make_map(ctx, &tq_lo, q_lo, rows_pad, DP, kBM)) ||
+        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, 128)) ||
+        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, 128)) ||
+        (rc = make_map(ctx, &tT_hi, m.QT_hi.ptr, DP, m.m_pad, NH)) ||
+        (rc = make_map(ctx, &tT_lo, m.QT_lo.ptr, DP, m.m_pad, NH)))
+        return rc;
+    auto kern = k_gap_flash<DP>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlashSmem));
+    if (!ctx->d_flag) {
+        TGAP_CUDA(ctx, cudaMalloc(&ctx->d_flag, sizeof(int)));
+        TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
+    }
+    const int J = m.m_pad / 128, n_rt = rows_pad / kBM;
+    const int nc = flash_chunks(n_rt, J, sm_count(ctx));
+    StageScope sc(ctx, "gemm_bf16x3_fused");
+    kern<<<n_rt * nc, kFlashThreads, kFlashSmem, ctx->stream>>>(tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc, p,
+                                                               ctx->d_flag);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
 // ---------------------------------------------------------------------------- GAP mixed path
 
 __global__ void k_split_bf16(int R, int C, int ld_in, const double *__restrict__ in, int R_pad, int C_pad,
@@ -545,15 +933,39 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
                           const int *d_sites, double *d_e_rows, double *d_energies)
 {
     if (n_rows <= 0) return TGAP_OK;
-    constexpr int BN1 = 128;
+    constexpr int BN1 = 128;  // m_pad is a multiple of 128; 256-column tiles when it allows
     const int rows_pad = (n_rows + kBM - 1) / kBM * kBM;
     if (m.dim_pad % 128 || m.m_pad % BN1 || m.dim_pad % kBK || m.m_pad % kBK)
         return set_error(ctx, TGAP_ERR_ARGUMENT, "mixed GEMM padding");
-    if (w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad) ||
-        (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad)))
+    if (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad))
         return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
     if (d_e_rows) TGAP_CUDA(ctx, cudaMemsetAsync(d_e_rows, 0, sizeof(double) * (size_t)n_rows, ctx->stream));
     const bool zi = std::fabs(m.zeta - (double)(int)m.zeta) < 1.0e-5;  // gap.f90:99-105
+    if (m.dim_pad <= 384 && m.m_pad % 128 == 0) {
+        // fused: G never leaves the SM (k_gap_flash); dE/dq accumulates with atomics
+        if (do_forces)
+            TGAP_CUDA(ctx, cudaMemsetAsync(w->g.ptr, 0, 4 * (size_t)rows_pad * m.dim_pad, ctx->stream));
+        FlashGap p;
+        p.alphas = m.alphas32.as<float>();
+        p.n_rows = n_rows;
+        p.sites = d_sites;
+        p.energies = d_energies;
+        p.e_rows = d_e_rows;
+        p.d2 = m.delta * m.delta;
+        p.e0 = e0;
+        p.zeta_int = zi ? (int)m.zeta : -1;
+        p.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
+        p.zd2 = (float)(p.zeta * m.delta * m.delta);
+        p.g = do_forces ? w->g.as<float>() : nullptr;
+        p.ldg = m.dim_pad;
+        switch (m.dim_pad) {
+        case 128: return launch_flash<128>(ctx, m, q_hi, q_lo, rows_pad, p);
+        case 256: return launch_flash<256>(ctx, m, q_hi, q_lo, rows_pad, p);
+        default: return launch_flash<384>(ctx, m, q_hi, q_lo, rows_pad, p);
+        }
+    }
+    if (w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad))
+        return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
     EpiKernelGap e1;
     e1.alphas = m.alphas32.as<float>();
     e1.G_hi = w->G_hi.as<__nv_bfloat16>();
@@ -568,8 +980,13 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     e1.zeta_int = zi ? (int)m.zeta : -1;
     e1.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
     e1.zd2 = (float)(e1.zeta * m.delta * m.delta);
-    int rc = launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr, rows_pad,
-                                               m.m_pad, m.dim_pad, e1);
+    // 256-column tiles re-read the descriptor rows half as often as 128-column ones (the GEMM is
+    // bound by L2 -> SM operand traffic); two 96 KB stages then fill the shared memory
+    int rc = m.m_pad % 256 == 0
+                 ? launch_gemm<256, 2, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr,
+                                                     rows_pad, m.m_pad, m.dim_pad, e1)
+                 : launch_gemm<BN1, 3, EpiKernelGap>(ctx, "gemm_bf16x3_kernel", q_hi, q_lo, m.Q_hi.ptr, m.Q_lo.ptr,
+                                                     rows_pad, m.m_pad, m.dim_pad, e1);
     if (rc) return rc;
     if (!do_forces) return TGAP_OK;
     // dE/dq: N = dim_pad is small, so 96-column tiles (when they divide it) give more tiles to
