@@ -431,23 +431,31 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
 
 // ---------------------------------------------------------------------------- fused GAP kernel
 
-// Energies and dE/dq of a 128-row tile against a chunk of T sparse tiles of 128 points, without
+// Energies and dE/dq of a 128-row tile against a chunk of T sparse tiles of BS points, without
 // writing G (flash-style): per sparse tile j
-//   S = q Q_j^T                       (tcgen05 bf16x3, TMEM columns [0, 128))
-//   W = zeta delta^2 alpha o S^(zeta-1)  (epilogue warps: registers -> bf16 hi/lo in shared memory,
-//                                       in the 128B-swizzled K-major layout the MMA reads)
-//   g += W Q_j                        (tcgen05 bf16x3, N = DP split in two halves, TMEM [128, 128+DP))
+//   S = q Q_j^T                          (tcgen05 bf16x3, TMEM columns [0, BS))
+//   W = zeta delta^2 alpha o S^(zeta-1)   (epilogue warps: registers -> bf16 hi/lo in shared memory,
+//                                          in the 128B-swizzled K-major layout the MMA reads)
+//   g += W Q_j                           (tcgen05 bf16x3, N = DP in two halves, TMEM [BS, BS+DP))
 // energies += delta^2 sum alpha S^zeta. MMA order S_{j+1} before g_j lets the epilogue of tile
 // j+1 overlap the tensor work of tile j. At the end the tile's g partial is added to global g with
 // vector atomics (g zeroed by the caller), energies with FP64 atomics.
 // Warps: 0 TMA producer, 1 MMA issuer (+ TMEM owner), 2..9 epilogue (rows 32 (w % 4) + lane,
-// columns half = (w - 2) / 4 of the tile). Shared memory: two 64 KB ring slots, W (64 KB).
+// columns half = (w - 2) / 4 of the tile). Shared memory: a STAGES-deep ring of equal slots (one
+// k-block of q and Q_j, or one half of a Q_j^T k-block) and W.
 constexpr int kFlashEpiWarps = 8;
 constexpr int kFlashThreads = 32 * (2 + kFlashEpiWarps);
-constexpr uint32_t kFlashSlot = 64 * 1024;
-constexpr uint32_t kFlashW = 64 * 1024;
-constexpr int kFlashStages = 2;
-constexpr size_t kFlashSmem = kFlashStages * (size_t)kFlashSlot + kFlashW + 1024;
+
+template <int DP, int BS> struct FlashShape {
+    static constexpr uint32_t TILE_A = kBM * kBK * 2;                 // q k-block (hi or lo)
+    static constexpr uint32_t TILE_B = BS * kBK * 2;                  // Q_j k-block (hi or lo)
+    static constexpr uint32_t B2 = (DP / 2) * kBK * 2;                // Q_j^T half k-block (hi or lo)
+    static constexpr uint32_t SLOT_S = 2 * TILE_A + 2 * TILE_B;
+    static constexpr uint32_t SLOT = SLOT_S > 2 * B2 ? SLOT_S : 2 * B2;
+    static constexpr uint32_t W = 2 * (BS / kBK) * TILE_A;            // hi + lo, BS/64 k-blocks each
+    static constexpr int STAGES = (int)((227u * 1024u - 2048u - W) / SLOT) > 4 ? 4 : (int)((227u * 1024u - 2048u - W) / SLOT);
+    static constexpr size_t SMEM = (size_t)STAGES * SLOT + W + 1024;
+};
 
 struct FlashGap {
     const float *alphas;  // [m_pad]
@@ -493,19 +501,24 @@ __device__ __forceinline__ void st_shared_v4(uint32_t addr, uint32_t a, uint32_t
     asm volatile("st.shared.v4.b32 [%0], {%1, %2, %3, %4};" ::"r"(addr), "r"(a), "r"(b), "r"(c), "r"(d) : "memory");
 }
 
-template <int DP>
+template <int DP, int BS>
 __global__ void __launch_bounds__(kFlashThreads, 1)
     k_gap_flash(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
                 const __grid_constant__ CUtensorMap tm_Q_hi, const __grid_constant__ CUtensorMap tm_Q_lo,
                 const __grid_constant__ CUtensorMap tm_QT_hi, const __grid_constant__ CUtensorMap tm_QT_lo,
                 int n_chunks, int tiles_per_chunk, FlashGap p, int *err_flag)
 {
-    static_assert(DP % 128 == 0 && DP <= 384, "descriptor padding: 128, 256 or 384");
-    constexpr int KB = DP / kBK;   // k-blocks of S
-    constexpr int NH = DP / 2;     // N of each g half
-    constexpr uint32_t TILE = kBM * kBK * 2;  // one 128 x 64 bf16 tile (16 KB)
-    constexpr uint32_t B2 = NH * kBK * 2;     // one NH x 64 bf16 tile of Q^T
-    constexpr uint32_t IDESC_S = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(128 >> 3) << 17) |
+    using Sh = FlashShape<DP, BS>;
+    static_assert(DP % 128 == 0 && DP + BS <= 512 && DP / 2 <= 256, "descriptor padding vs TMEM");
+    static_assert(BS % 64 == 0 && BS <= 128, "sparse tile: 64 or 128");
+    constexpr int STAGES = Sh::STAGES;
+    static_assert(STAGES >= 2, "ring of at least two slots");
+    constexpr int KB = DP / kBK;     // k-blocks of S
+    constexpr int KG = BS / kBK;     // k-blocks of g per sparse tile
+    constexpr int NH = DP / 2;       // N of each g half
+    constexpr int HC = BS / 2;       // S columns per epilogue half
+    constexpr uint32_t TILE_A = Sh::TILE_A, TILE_B = Sh::TILE_B, B2 = Sh::B2, SLOT = Sh::SLOT;
+    constexpr uint32_t IDESC_S = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BS >> 3) << 17) |
                                  ((uint32_t)(kBM >> 4) << 24);
     constexpr uint32_t IDESC_G = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
                                  ((uint32_t)(kBM >> 4) << 24);
@@ -513,20 +526,20 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     const bool forces = p.g != nullptr;
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
-    __shared__ __align__(8) uint64_t bar_full[kFlashStages], bar_empty[kFlashStages];
+    __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
     __shared__ __align__(8) uint64_t bar_sfull, bar_sfree, bar_wfull, bar_wempty, bar_drain;
     __shared__ uint32_t tmem_base_slot;
     __shared__ volatile int abort_flag;
     __shared__ int issued, consumed;
 
     const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
-    const uint32_t wbase = base + kFlashStages * kFlashSlot;  // W: hi kb0, hi kb1, lo kb0, lo kb1
+    const uint32_t wbase = base + STAGES * SLOT;  // W: hi k-blocks, then lo k-blocks (TILE_A each)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int unit = blockIdx.x, rt = unit / n_chunks, ch = unit - rt * n_chunks;
     const int T = tiles_per_chunk, j0 = ch * T, m0 = rt * kBM;
 
     if (threadIdx.x == 0) {
-        for (int s = 0; s < kFlashStages; ++s) {
+        for (int s = 0; s < STAGES; ++s) {
             mbar_init(smem_u32(&bar_full[s]), 1);
             mbar_init(smem_u32(&bar_empty[s]), 1);
         }
@@ -553,17 +566,17 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
     const uint32_t tmem = tmem_base_slot;
-    const uint32_t tS = tmem, tG = tmem + 128;
+    const uint32_t tS = tmem, tG = tmem + BS;
 
     if (warp == 0) {
         if (lane == 0) {
             // TMA producer: S_0 blocks, then per tile t: S_{t+1} blocks, g_t blocks (the MMA order)
             int it = 0;
             auto acquire = [&](uint32_t &slot, uint32_t &fb) -> bool {
-                const int s = it % kFlashStages;
-                const uint32_t ph = (uint32_t)(it / kFlashStages) & 1u;
-                if (it >= kFlashStages && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) return false;
-                slot = base + s * kFlashSlot;
+                const int s = it % STAGES;
+                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                if (it >= STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) return false;
+                slot = base + s * SLOT;
                 fb = smem_u32(&bar_full[s]);
                 return true;
             };
@@ -571,23 +584,23 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                 for (int kb = 0; kb < KB; ++kb) {
                     uint32_t slot, fb;
                     if (!acquire(slot, fb)) return false;
-                    mbar_expect_tx(fb, 4 * TILE);
+                    mbar_expect_tx(fb, 2 * TILE_A + 2 * TILE_B);
                     tma_load_2d(slot, &tm_q_hi, fb, kb * kBK, m0);
-                    tma_load_2d(slot + TILE, &tm_q_lo, fb, kb * kBK, m0);
-                    tma_load_2d(slot + 2 * TILE, &tm_Q_hi, fb, kb * kBK, j * 128);
-                    tma_load_2d(slot + 3 * TILE, &tm_Q_lo, fb, kb * kBK, j * 128);
+                    tma_load_2d(slot + TILE_A, &tm_q_lo, fb, kb * kBK, m0);
+                    tma_load_2d(slot + 2 * TILE_A, &tm_Q_hi, fb, kb * kBK, j * BS);
+                    tma_load_2d(slot + 2 * TILE_A + TILE_B, &tm_Q_lo, fb, kb * kBK, j * BS);
                     issued = ++it;
                 }
                 return true;
             };
             auto load_g = [&](int j) -> bool {
-                for (int kb = 0; kb < 2; ++kb)
+                for (int kb = 0; kb < KG; ++kb)
                     for (int h = 0; h < 2; ++h) {
                         uint32_t slot, fb;
                         if (!acquire(slot, fb)) return false;
                         mbar_expect_tx(fb, 2 * B2);
-                        tma_load_2d(slot, &tm_QT_hi, fb, j * 128 + kb * kBK, h * NH);
-                        tma_load_2d(slot + B2, &tm_QT_lo, fb, j * 128 + kb * kBK, h * NH);
+                        tma_load_2d(slot, &tm_QT_hi, fb, j * BS + kb * kBK, h * NH);
+                        tma_load_2d(slot + B2, &tm_QT_lo, fb, j * BS + kb * kBK, h * NH);
                         issued = ++it;
                     }
                 return true;
@@ -599,22 +612,22 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             }
             if (!ok) abort_flag = 1;
             // tail: the last slots' releases land before the CTA exits (bounded)
-            for (int i = (it > kFlashStages ? it - kFlashStages : 0); i < it && !abort_flag; ++i)
-                if (!mbar_wait(smem_u32(&bar_empty[i % kFlashStages]), (uint32_t)(i / kFlashStages) & 1u, &abort_flag))
+            for (int i = (it > STAGES ? it - STAGES : 0); i < it && !abort_flag; ++i)
+                if (!mbar_wait(smem_u32(&bar_empty[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &abort_flag))
                     abort_flag = 1;
         }
     } else if (warp == 1) {
         if (lane == 0) {
             int it = 0;
             auto take = [&](uint32_t &slot) -> bool {
-                const int s = it % kFlashStages;
-                if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(it / kFlashStages) & 1u, &abort_flag)) return false;
+                const int s = it % STAGES;
+                if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(it / STAGES) & 1u, &abort_flag)) return false;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                slot = base + s * kFlashSlot;
+                slot = base + s * SLOT;
                 return true;
             };
             auto release = [&]() {
-                umma_commit(smem_u32(&bar_empty[it % kFlashStages]));
+                umma_commit(smem_u32(&bar_empty[it % STAGES]));
                 consumed = ++it;
             };
             auto mma_s = [&]() -> bool {
@@ -623,9 +636,9 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                     if (!take(slot)) return false;
 #pragma unroll
                     for (int k = 0; k < kBK / 16; ++k) {
-                        const uint64_t ahi = umma_desc(slot + 32 * k), alo = umma_desc(slot + TILE + 32 * k);
-                        const uint64_t bhi = umma_desc(slot + 2 * TILE + 32 * k);
-                        const uint64_t blo = umma_desc(slot + 3 * TILE + 32 * k);
+                        const uint64_t ahi = umma_desc(slot + 32 * k), alo = umma_desc(slot + TILE_A + 32 * k);
+                        const uint64_t bhi = umma_desc(slot + 2 * TILE_A + 32 * k);
+                        const uint64_t blo = umma_desc(slot + 2 * TILE_A + TILE_B + 32 * k);
                         umma_bf16(tS, ahi, bhi, IDESC_S, (kb > 0 || k > 0) ? 1u : 0u);
                         umma_bf16(tS, ahi, blo, IDESC_S, 1u);
                         umma_bf16(tS, alo, bhi, IDESC_S, 1u);
@@ -638,11 +651,11 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             auto mma_g = [&](int t) -> bool {
                 if (!mbar_wait(smem_u32(&bar_wfull), (uint32_t)t & 1u, &abort_flag)) return false;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                for (int kb = 0; kb < 2; ++kb)
+                for (int kb = 0; kb < KG; ++kb)
                     for (int h = 0; h < 2; ++h) {
                         uint32_t slot;
                         if (!take(slot)) return false;
-                        const uint32_t whi = wbase + kb * TILE, wlo = wbase + (2 + kb) * TILE;
+                        const uint32_t whi = wbase + kb * TILE_A, wlo = wbase + (KG + kb) * TILE_A;
 #pragma unroll
                         for (int k = 0; k < kBK / 16; ++k) {
                             const uint64_t ahi = umma_desc(whi + 32 * k), alo = umma_desc(wlo + 32 * k);
@@ -683,12 +696,12 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             __syncwarp();
             if (!ok || abort_flag) break;
-            uint32_t hi[4][8], lo[4][8];
+            uint32_t hi[HC / 16][8], lo[HC / 16][8];
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < HC / 16; ++c) {
                 float v[16];
-                tmem_ld16(tS + lane_base + (uint32_t)(half * 64 + c * 16), v);
-                const float *a16 = p.alphas + j * 128 + half * 64 + c * 16;
+                tmem_ld16(tS + lane_base + (uint32_t)(half * HC + c * 16), v);
+                const float *a16 = p.alphas + j * BS + half * HC + c * 16;
                 switch (p.zeta_int) {
                 case 1: flash_w16<1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
                 case 2: flash_w16<2>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
@@ -706,16 +719,18 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                 ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(t - 1) & 1u, &abort_flag);
                 if (!ok) break;
             }
-            // W row r, columns half * 64 .. + 64 = k-block `half` of the K-major 128B-swizzled tile:
-            // 16-byte chunk c of the row sits at chunk c ^ (r % 8)
-            const uint32_t rhi = wbase + half * TILE + r * 128, rlo = wbase + (2 + half) * TILE + r * 128;
+            // W row r, sparse column col lies in k-block col / 64 of the K-major 128B-swizzled
+            // tile, 16-byte chunk (col % 64) / 8 of the row, stored at chunk ^ (r % 8)
 #pragma unroll
-            for (int c = 0; c < 4; ++c) {
+            for (int c = 0; c < HC / 16; ++c) {
 #pragma unroll
                 for (int u = 0; u < 2; ++u) {
-                    const uint32_t chunk = (uint32_t)((2 * c + u) ^ (r & 7)) * 16;
-                    st_shared_v4(rhi + chunk, hi[c][4 * u], hi[c][4 * u + 1], hi[c][4 * u + 2], hi[c][4 * u + 3]);
-                    st_shared_v4(rlo + chunk, lo[c][4 * u], lo[c][4 * u + 1], lo[c][4 * u + 2], lo[c][4 * u + 3]);
+                    const int col = half * HC + c * 16 + u * 8;
+                    const uint32_t off = (uint32_t)(col / kBK) * TILE_A + r * 128 +
+                                         (uint32_t)(((col % kBK) / 8) ^ (r & 7)) * 16;
+                    st_shared_v4(wbase + off, hi[c][4 * u], hi[c][4 * u + 1], hi[c][4 * u + 2], hi[c][4 * u + 3]);
+                    st_shared_v4(wbase + KG * TILE_A + off, lo[c][4 * u], lo[c][4 * u + 1], lo[c][4 * u + 2],
+                                 lo[c][4 * u + 3]);
                 }
             }
             asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
@@ -755,7 +770,7 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             atomicExch(err_flag, 1);
             volatile int dummy = 0;
             for (int i = consumed; i < issued; ++i)
-                mbar_wait(smem_u32(&bar_full[i % kFlashStages]), (uint32_t)(i / kFlashStages) & 1u, &dummy);
+                mbar_wait(smem_u32(&bar_full[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &dummy);
         }
         __syncthreads();
     }
@@ -836,6 +851,11 @@ static int launch_gemm(tgap_context *ctx, const char *stage, const void *a_hi, c
     return TGAP_OK;
 }
 
+#ifndef TGAP_FLASH_BS
+#define TGAP_FLASH_BS 128
+#endif
+constexpr int kFlashBS = TGAP_FLASH_BS;  // sparse points per tile of the fused kernel
+
 // Chunks of the sparse tiles per row tile: the fewest waves of (row tiles x chunks) CTAs times
 // the tiles each CTA runs; ties go to fewer chunks (fewer g atomics).
 static int flash_chunks(int n_rt, int J, int sms)
@@ -854,30 +874,31 @@ static int flash_chunks(int n_rt, int J, int sms)
     return best;
 }
 
-template <int DP>
+template <int DP, int BS>
 static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi, const __nv_bfloat16 *q_lo,
                         int rows_pad, const FlashGap &p)
 {
+    using Sh = FlashShape<DP, BS>;
     constexpr int NH = DP / 2;
     CUtensorMap tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo;
     int rc;
     if ((rc = make_map(ctx, &tq_hi, q_hi, rows_pad, DP, kBM)) || (rc = make_map(ctx, &tq_lo, q_lo, rows_pad, DP, kBM)) ||
-        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, 128)) ||
-        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, 128)) ||
+        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, BS)) ||
+        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, BS)) ||
         (rc = make_map(ctx, &tT_hi, m.QT_hi.ptr, DP, m.m_pad, NH)) ||
         (rc = make_map(ctx, &tT_lo, m.QT_lo.ptr, DP, m.m_pad, NH)))
         return rc;
-    auto kern = k_gap_flash<DP>;
-    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFlashSmem));
+    auto kern = k_gap_flash<DP, BS>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM));
     if (!ctx->d_flag) {
         TGAP_CUDA(ctx, cudaMalloc(&ctx->d_flag, sizeof(int)));
         TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
     }
-    const int J = m.m_pad / 128, n_rt = rows_pad / kBM;
+    const int J = m.m_pad / BS, n_rt = rows_pad / kBM;
     const int nc = flash_chunks(n_rt, J, sm_count(ctx));
     StageScope sc(ctx, "gemm_bf16x3_fused");
-    kern<<<n_rt * nc, kFlashThreads, kFlashSmem, ctx->stream>>>(tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc, p,
-                                                               ctx->d_flag);
+    kern<<<n_rt * nc, kFlashThreads, Sh::SMEM, ctx->stream>>>(tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc,
+                                                             p, ctx->d_flag);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
@@ -958,10 +979,12 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         p.zd2 = (float)(p.zeta * m.delta * m.delta);
         p.g = do_forces ? w->g.as<float>() : nullptr;
         p.ldg = m.dim_pad;
+        // 128-point sparse tiles (64-point ones allow a deeper ring but double the per-tile handoffs,
+        // and measured slower)
         switch (m.dim_pad) {
-        case 128: return launch_flash<128>(ctx, m, q_hi, q_lo, rows_pad, p);
-        case 256: return launch_flash<256>(ctx, m, q_hi, q_lo, rows_pad, p);
-        default: return launch_flash<384>(ctx, m, q_hi, q_lo, rows_pad, p);
+        case 128: return launch_flash<128, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
+        case 256: return launch_flash<256, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
+        default: return launch_flash<384, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
         }
     }
     if (w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad))
