@@ -441,6 +441,22 @@ def _mc_cpu_baseline(tg, model_np, seed, budget_s=10.0):
                        f"reference does (oracle restatement with OpenMP; not TurboGAP itself)")
 
 
+def _over_ranks(values, op, dist, device):
+    """Max or min of per-rank values over the process group (identity without one): each rank
+    runs its own replica, and the job is as slow as its slowest rank."""
+    if dist is None:
+        return [float(v) for v in values]
+    import torch
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX if op == "max" else dist.ReduceOp.MIN)
+    return [float(v) for v in t.cpu()]
+
+
+def _job_throughput(world, units_per_rank, ms_max):
+    """Whole-job units per second: every rank processed units_per_rank in at most ms_max."""
+    return world * units_per_rank / (ms_max * 1e-3)
+
+
 def run_ours(args):
     import torch
     tg = _load_package()
@@ -512,13 +528,10 @@ def run_ours(args):
                                        args.steps, args.warmup)
     clk = clocks.stop()
     torch.cuda.synchronize()
-    if dist:
-        t = torch.tensor([ms, ms64], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms, ms64 = float(t[0]), float(t[1])
+    ms, ms64 = _over_ranks([ms, ms64], "max", dist, "cuda")
     drift = ((st1["e_pot"] + st1["e_kin"]) - (st0["e_pot"] + st0["e_kin"])) / N_ATOMS
-    value = world * N_ATOMS * args.steps / (ms * 1e-3)
-    value64 = world * N_ATOMS * args.steps / (ms64 * 1e-3)
+    value = _job_throughput(world, N_ATOMS * args.steps, ms)
+    value64 = _job_throughput(world, N_ATOMS * args.steps, ms64)
 
     # per-kernel times (mixed) and roofline of the dominant kernel
     system.set_positions(pos)
@@ -531,10 +544,7 @@ def run_ours(args):
     system.set_positions(pos)
     system.update(True)
     e2e = _e2e(tg, ctx, system, model, masses, vel, pos, tg.TGAP_MIXED, min(args.steps, 50))
-    if dist:
-        t = torch.tensor([e2e["value"]], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MIN)
-        e2e["value"] = float(t[0]) * world
+    e2e["value"] = _over_ranks([e2e["value"]], "min", dist, "cuda")[0] * world
     mc_line = _mc_leg(tg, torch, ctx, stream, model, MC_PROPOSALS, 300 + seed)
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
