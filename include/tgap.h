@@ -276,6 +276,18 @@ int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const double *displace
  * models (n_atoms), their total, moves accepted since creation, neighbor-list rebuilds. */
 int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energies, double *e_total,
                       int64_t *accepted, int64_t *rebuilds);
+/* Learned screen for delayed acceptance (Christen and Fox): per-atom surrogate energy
+ * e(q) = w3 . silu(W2 silu(W1 P (q - mean) + b1) + b2) + b3 on the normalised descriptor
+ * (row-major P: n_pca x dim, W1: n_hidden x n_pca, W2: n_hidden x n_hidden; weights kept in bf16,
+ * FP32 accumulation). Each proposal is first tested with min(1, exp(-dE_s / kB T)) > u1; only
+ * survivors get the exact GAP energies and min(1, exp(-(dE - dE_s) / kB T)) > u2. With a screen
+ * set, tgap_mc_run takes two deviates per proposal (u1, u2 interleaved). Mixed precision, one
+ * model over all sites. */
+int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden, const float *mean,
+                       const float *pca, const float *w1, const float *b1, const float *w2,
+                       const float *b2, const float *w3, float b3);
+/* Screen dE and the deciding stage (1: screen, 2: exact) of the last run's first n proposals. */
+int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char *stage);
 
 #ifdef __cplusplus
 }

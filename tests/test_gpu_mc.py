@@ -158,3 +158,75 @@ def test_mc_rejects_bad_arguments(ctx, tg, synth, carbon):
     with pytest.raises(tg.TgapError):
         mc.run(np.array([len(pos)], np.int32), np.zeros((1, 3)), np.zeros(1))
     mc.close()
+
+
+def _gpu_snapshot_data(ctx, tg, synth, hyp, model, pos, box, sp, n_snap, sigma, seed):
+    """(descriptor, per-atom GAP energy) pairs of perturbed copies of a box, from the device (FP64)."""
+    import ctypes as C
+    import torch
+    from turbogap_b200 import native
+    rng = np.random.default_rng(seed)
+    n = len(pos)
+    qs, es = [], []
+    for k in range(n_snap):
+        p = pos + rng.normal(scale=sigma, size=pos.shape)
+        system = tg.System(ctx, [(p, box, sp)], 3.7)
+        e = torch.zeros(n, dtype=torch.float64, device="cuda")
+        f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+        v = torch.zeros(9, dtype=torch.float64, device="cuda")
+        q = torch.zeros((n, model.dim), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        system.compute_device([model], tg.TGAP_FP64, e.data_ptr(), f.data_ptr(), v.data_ptr())
+        nr = C.c_int(0)
+        native.check(native.lib().tgap_descriptors(ctx.h, system.h, model.h, 0, C.c_void_p(q.data_ptr()),
+                                                   C.byref(nr)), ctx.h, "descriptors")
+        ctx.synchronize()
+        qs.append(q.cpu().numpy())
+        es.append(e.cpu().numpy())
+        system.close()
+    return np.concatenate(qs), np.concatenate(es)
+
+
+def test_mc_screen_delayed_acceptance_matches_cpu_chain(ctx, tg, synth, carbon):
+    """Delayed acceptance: stage 1 on the learned screen (its dE against the numpy evaluation of
+    the same bf16 weights on oracle descriptors), stage 2 on the exact mixed-precision GAP energies
+    (against the oracle), same decisions, same final positions."""
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=80)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    q_tr, e_tr = _gpu_snapshot_data(ctx, tg, synth, hyp, model, pos, box, sp, 40, 0.08, seed=81)
+    w = tg.screen.fit(q_tr, e_tr, n_pca=32, hidden=64, epochs=40, seed=2)
+    T = 30.0
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.4)
+    mc = tg.MC(ctx, system, [model], T, precision=tg.TGAP_MIXED)
+    mc.set_screen(w)
+    atoms, disp, _ = synth.mc_proposals(len(pos), 150, 0.2, seed=82)
+    u = np.random.default_rng(83).random((150, 2))
+    out = mc.run(atoms, disp, u)
+    des_g, stage_g = mc.screen_log(150)
+    st = mc.state()
+    assert np.all(np.isnan(out["de"][stage_g == 1]))
+    assert np.sum(stage_g == 1) > 0 and np.sum(stage_g == 2) > 0
+    # CPU replay
+    p = np.array(pos, dtype=np.float64)
+    es_cur = tg.screen.predict(w, helpers.oracle_descriptors(hyp, p, box, sp))
+    e_cur = helpers.oracle_structure_eval(hyp, [m], p, box, sp, do_forces=False)[0].sum()
+    for k in range(len(atoms)):
+        qn = p.copy()
+        qn[atoms[k]] = qn[atoms[k]] + disp[k]
+        es_new = tg.screen.predict(w, helpers.oracle_descriptors(hyp, qn, box, sp))
+        des = es_new.sum() - es_cur.sum()
+        assert abs(des - des_g[k]) < 2e-4, (k, des, des_g[k])
+        p1 = min(1.0, float(np.exp(-des / (KB * T))))
+        if abs(p1 - u[k, 0]) > 1e-3:
+            assert (stage_g[k] == 2) == (p1 > u[k, 0]), k
+        if stage_g[k] == 2:
+            e_new = helpers.oracle_structure_eval(hyp, [m], qn, box, sp, do_forces=False)[0].sum()
+            de = e_new - e_cur
+            assert abs(de - out["de"][k]) < 2e-4, (k, de, out["de"][k])
+            p2 = min(1.0, float(np.exp(-(out["de"][k] - des_g[k]) / (KB * T))))
+            assert (p2 > u[k, 1]) == bool(out["accept"][k]), k
+            if out["accept"][k]:
+                p, es_cur, e_cur = qn, es_new, e_new
+    assert np.array_equal(st["positions"], p)
+    mc.close()

@@ -80,3 +80,25 @@ def test_mc_proposals_stay_in_the_ball(tg):
     # uniform in the ball: P(r < R/2) = 1/8
     assert abs(np.mean(r < 0.1) - 0.125) < 0.02
     assert u.min() >= 0.0 and u.max() < 1.0
+
+
+def test_screen_fit_learns_a_smooth_target(tg):
+    """The host trainer fits a smooth function of a low-dimensional projection; the bf16-rounded
+    evaluation (the device's arithmetic) stays close to the float one."""
+    rng = np.random.default_rng(0)
+    q = rng.normal(size=(4000, 40)) * np.r_[np.full(4, 4.0), np.ones(36)]  # leading directions dominate
+    q /= np.linalg.norm(q, axis=1)[:, None]
+    e = np.sin(3 * q[:, 0]) + 0.5 * q[:, 1] ** 2
+    w = tg.screen.fit(q, e, n_pca=16, hidden=32, epochs=60, seed=1)
+    pred = tg.screen.predict(w, q)
+    assert np.sqrt(np.mean((pred - e) ** 2)) < 0.2 * e.std()
+
+
+def test_bf16_round_is_round_to_nearest_even(tg):
+    x = np.array([1.0, 1.0 + 2.0 ** -8, 1.0 + 3 * 2.0 ** -8, -2.5, 3.14159], np.float32)
+    r = tg.screen.bf16_round(x)
+    assert r[0] == 1.0
+    assert r[1] == 1.0  # tie to even
+    assert r[2] == np.float32(1.0 + 2.0 ** -6)
+    assert r[3] == -2.5
+    assert abs(r[4] - 3.14159) < 2 ** -7 * 4

@@ -337,12 +337,31 @@ class MC:
                                     int(use_graph), C.byref(h)), ctx.h, "tgap_mc_create")
         self.h = h
 
+    def set_screen(self, w):
+        """Installs a learned screen (weights as returned by turbogap_b200.screen.fit); proposals then
+        take two uniform deviates each (uniforms of shape (n, 2))."""
+        f32 = lambda a: np.ascontiguousarray(a, dtype=np.float32)
+        pca = f32(w["pca"])
+        n_pca, dim = pca.shape
+        hidden = len(w["b1"])
+        keep = [f32(w[k]) for k in ("mean", "pca", "w1", "b1", "w2", "b2", "w3")]
+        check(self.ctx._L.tgap_mc_set_screen(self.h, dim, n_pca, hidden, *[ptr(a) for a in keep], float(w["b3"])),
+              self.ctx.h, "tgap_mc_set_screen")
+        self.screened = True
+
+    def screen_log(self, n):
+        des = np.zeros(n)
+        st = np.zeros(n, np.uint8)
+        check(self.ctx._L.tgap_mc_screen_log(self.h, n, ptr(des), ptr(st)), self.ctx.h, "tgap_mc_screen_log")
+        return des, st
+
     def run(self, atoms, displacements, uniforms, logs=True):
         atoms = np.ascontiguousarray(atoms, dtype=np.int32)
         disp = _f64(displacements)
         u = _f64(uniforms)
         n = len(atoms)
-        if disp.size != 3 * n or u.size != n:
+        per = 2 if getattr(self, "screened", False) else 1
+        if disp.size != 3 * n or u.size != per * n:
             raise ValueError("proposal arrays disagree in length")
         acc = C.c_int64(0)
         de = np.zeros(n) if logs else None

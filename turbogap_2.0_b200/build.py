@@ -34,6 +34,7 @@ SOURCES = [
     ("gemm_tc.cu", []),
     ("md.cu", []),
     ("mc.cu", ["--fmad=false"]),
+    ("screen.cu", []),
     ("tables.cpp", []),
 ]
 

@@ -5,6 +5,7 @@
 #include <atomic>
 #include <cmath>
 #include <cstdarg>
+#include <cstddef>
 #include <cstdlib>
 #include <cstring>
 #include <memory>
@@ -13,6 +14,7 @@
 
 #include "gap_kernels.h"
 #include "mc_kernels.h"
+#include "screen_kernels.h"
 #include "md_kernels.h"
 #include "neighbors.h"
 #include "soap_kernels.h"
@@ -1243,12 +1245,17 @@ struct tgap_mc {
     DevBuf st, ecache, dacc, mark, sites, tstart, txyz, trjs, tnsp, etrial;
     std::vector<DevBuf> c, q, norm, q_hi, q_lo;  // per model, the trial rows
     std::vector<GapWork> gw;
-    DevBuf patom, pdisp, pu, log_de, log_acc;
+    DevBuf patom, pdisp, pu, log_de, log_acc, log_des, log_stage;
     HostBuf hst;
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     uint64_t graph_epoch = 0;
     int64_t graph_kernels = 0;
+    // learned screen (delayed acceptance)
+    bool screened = false;
+    ScreenDev sd{};
+    DevBuf s_mean, s_pca, s_w1, s_b1, s_w2, s_b2, s_w3, es_cache, es_trial;
+    int64_t last_n = 0;
 };
 
 constexpr int kMcBatch = 32;  // proposals per graph launch
@@ -1274,7 +1281,8 @@ static int mc_size_trial(tgap_mc *mc)
     const size_t slots = (size_t)M * cap * pm;
     if (mc->sites.ensure(sizeof(int) * (size_t)M * cap) || mc->tstart.ensure(sizeof(int64_t) * (cap + 1)) ||
         mc->txyz.ensure(sizeof(double) * 3 * slots) || mc->trjs.ensure(sizeof(double) * slots) ||
-        mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * cap))
+        mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * cap) ||
+        mc->es_trial.ensure(sizeof(float) * cap))
         return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->tnsp.ptr, 0, sizeof(int) * slots, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->trjs.ptr, 0, sizeof(double) * slots, ctx->stream));
@@ -1302,7 +1310,14 @@ static int mc_size_trial(tgap_mc *mc)
     return TGAP_OK;
 }
 
-// One proposal: select, trial geometry, descriptor rows and GAP energies per model, acceptance.
+static McLogs mc_logs(tgap_mc *mc)
+{
+    return McLogs{mc->log_de.as<double>(), mc->log_acc.as<unsigned char>(), mc->log_des.as<double>(),
+                  mc->log_stage.as<unsigned char>()};
+}
+
+// One proposal: select, trial geometry, descriptor rows and GAP energies per model (with the
+// screen stage before the exact one when a screen is set), acceptance.
 static int mc_step_body(tgap_mc *mc)
 {
     tgap_context *ctx = mc->ctx;
@@ -1333,13 +1348,23 @@ static int mc_step_body(tgap_mc *mc)
             o.q_hi = mc->q_hi[m].as<__nv_bfloat16>();
             o.q_lo = mc->q_lo[m].as<__nv_bfloat16>();
             CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, cap, TGAP_MIXED, o));
+            const int *skip = nullptr;
+            if (mc->screened) {
+                // stage 1 on the trial rows' screen energies; a rejection skips the exact GEMM
+                const int *d_count = reinterpret_cast<const int *>(reinterpret_cast<const char *>(st) +
+                                                                   offsetof(McDev, count));
+                CHECK_RC(screen_rows(ctx, mc->sd, (const float *)o.q, o.q_ld, cap, d_count, mc->es_trial.as<float>()));
+                CHECK_RC(mc_screen_stage(ctx, st, mc->sites.as<int>(), mc->es_trial.as<float>(),
+                                         mc->es_cache.as<float>(), mc->pu.as<double>(), mc->temperature, mc_logs(mc)));
+                skip = reinterpret_cast<const int *>(reinterpret_cast<const char *>(st) + offsetof(McDev, skip));
+            }
             CHECK_RC(gap_energy_grad_mixed(ctx, md->gap, o.q_hi, o.q_lo, cap, 0.0, 0, &mc->gw[m], nullptr, e_rows,
-                                           nullptr));
+                                           nullptr, skip));
         }
     }
     return mc_accept(ctx, st, M, mc->sites.as<int>(), cap, mc->etrial.as<double>(), mc->ecache.as<double>(), N,
                      nb.positions.as<double>(), mc->dacc.as<double>(), mc->pu.as<double>(), mc->temperature,
-                     mc->log_de.as<double>(), mc->log_acc.as<unsigned char>());
+                     mc_logs(mc), mc->screened ? 1 : 0, mc->es_trial.as<float>(), mc->es_cache.as<float>());
 }
 
 static int mc_read_state(tgap_mc *mc, McDev *out)
@@ -1415,7 +1440,9 @@ extern "C" int tgap_mc_destroy(tgap_mc *mc)
     if (mc->exec) cudaGraphExecDestroy(mc->exec);
     if (mc->graph) cudaGraphDestroy(mc->graph);
     DevBuf *bufs[] = {&mc->st, &mc->ecache, &mc->dacc, &mc->mark, &mc->sites, &mc->tstart, &mc->txyz, &mc->trjs,
-                      &mc->tnsp, &mc->etrial, &mc->patom, &mc->pdisp, &mc->pu, &mc->log_de, &mc->log_acc};
+                      &mc->tnsp, &mc->etrial, &mc->patom, &mc->pdisp, &mc->pu, &mc->log_de, &mc->log_acc,
+                      &mc->log_des, &mc->log_stage, &mc->s_mean, &mc->s_pca, &mc->s_w1, &mc->s_b1, &mc->s_w2,
+                      &mc->s_b2, &mc->s_w3, &mc->es_cache, &mc->es_trial};
     for (DevBuf *b : bufs) b->release();
     for (auto *v : {&mc->c, &mc->q, &mc->norm, &mc->q_hi, &mc->q_lo})
         for (DevBuf &b : *v) b.release();
@@ -1441,12 +1468,15 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
     const int N = mc->sys->nb.n_atoms;
     for (int64_t k = 0; k < n; ++k)
         if (atoms[k] < 0 || atoms[k] >= N) return set_error(ctx, TGAP_ERR_ARGUMENT, "proposal %lld: atom", (long long)k);
+    const size_t nu = (mc->screened ? 2 : 1) * (size_t)n;  // two deviates per proposal with a screen
     if (mc->patom.ensure(sizeof(int) * n) || mc->pdisp.ensure(sizeof(double) * 3 * n) ||
-        mc->pu.ensure(sizeof(double) * n) || mc->log_de.ensure(sizeof(double) * n) || mc->log_acc.ensure(n))
+        mc->pu.ensure(sizeof(double) * nu) || mc->log_de.ensure(sizeof(double) * n) || mc->log_acc.ensure(n) ||
+        mc->log_des.ensure(sizeof(double) * n) || mc->log_stage.ensure(n))
         return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo proposals");
     CHECK_RC(upload(ctx, mc->patom, atoms, (size_t)n));
     CHECK_RC(upload(ctx, mc->pdisp, disp, 3 * (size_t)n));
-    CHECK_RC(upload(ctx, mc->pu, uniform, (size_t)n));
+    CHECK_RC(upload(ctx, mc->pu, uniform, nu));
+    mc->last_n = n;
     McDev h;
     CHECK_RC(mc_read_state(mc, &h));
     const long long acc0 = h.accepted;
@@ -1530,5 +1560,82 @@ extern "C" int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energie
     if (e_total) *e_total = tot;
     if (accepted) *accepted = h.accepted;
     if (rebuilds) *rebuilds = mc->rebuilds;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden, const float *mean, const float *pca,
+                                  const float *w1, const float *b1, const float *w2, const float *b2,
+                                  const float *w3, float b3)
+{
+    if (!mc) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = mc->ctx;
+    CHECK_RC(activate(ctx));
+    if (!mean || !pca || !w1 || !b1 || !w2 || !b2 || !w3 || n_pca < 1 || n_pca > kScreenMaxPca || n_hidden < 1 ||
+        n_hidden > kScreenMaxHidden)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_mc_set_screen: bad arguments");
+    if (mc->precision != TGAP_MIXED || mc->models.size() != 1 || mc->models[0]->central_species != 0 ||
+        mc->models[0]->gap.dim_pad > 384)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED,
+                         "the screen needs the mixed path, one model over all sites and a descriptor of <= 384");
+    const tgap_model *md = mc->models[0];
+    if (dim != md->gap.dim) return set_error(ctx, TGAP_ERR_ARGUMENT, "screen dim %d != descriptor %d", dim, md->gap.dim);
+    auto to_bf16 = [](const float *x, size_t n) {
+        std::vector<__nv_bfloat16> v(n);
+        for (size_t i = 0; i < n; ++i) v[i] = __float2bfloat16_rn(x[i]);
+        return v;
+    };
+    const auto vp = to_bf16(pca, (size_t)n_pca * dim), v1 = to_bf16(w1, (size_t)n_hidden * n_pca),
+               v2 = to_bf16(w2, (size_t)n_hidden * n_hidden), v3 = to_bf16(w3, (size_t)n_hidden);
+    CHECK_RC(upload(ctx, mc->s_mean, mean, (size_t)dim));
+    CHECK_RC(upload(ctx, mc->s_pca, vp.data(), vp.size()));
+    CHECK_RC(upload(ctx, mc->s_w1, v1.data(), v1.size()));
+    CHECK_RC(upload(ctx, mc->s_b1, b1, (size_t)n_hidden));
+    CHECK_RC(upload(ctx, mc->s_w2, v2.data(), v2.size()));
+    CHECK_RC(upload(ctx, mc->s_b2, b2, (size_t)n_hidden));
+    CHECK_RC(upload(ctx, mc->s_w3, v3.data(), v3.size()));
+    mc->sd = ScreenDev{dim, n_pca, n_hidden, mc->s_mean.as<float>(), mc->s_pca.as<__nv_bfloat16>(),
+                       mc->s_w1.as<__nv_bfloat16>(), mc->s_b1.as<float>(), mc->s_w2.as<__nv_bfloat16>(),
+                       mc->s_b2.as<float>(), mc->s_w3.as<__nv_bfloat16>(), b3};
+    // screen energies of every atom at the current positions (FP32 descriptors of the mixed path)
+    tgap_system *sys = mc->sys;
+    const int N = sys->nb.n_atoms;
+    if (mc->es_cache.ensure(sizeof(float) * N) || mc->es_trial.ensure(sizeof(float) * mc->cap))
+        return set_error(ctx, TGAP_ERR_NOMEM, "screen caches");
+    CHECK_RC(neighbors_refresh(ctx, &sys->nb));
+    DevBuf c, q, norm;
+    std::unique_ptr<DevBuf, void (*)(DevBuf *)> gc(&c, [](DevBuf *b) { b->release(); });
+    std::unique_ptr<DevBuf, void (*)(DevBuf *)> gq(&q, [](DevBuf *b) { b->release(); });
+    std::unique_ptr<DevBuf, void (*)(DevBuf *)> gn(&norm, [](DevBuf *b) { b->release(); });
+    const SoapParams &P = md->soap.p;
+    const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
+    if (c.ensure(4 * (size_t)N * P.n_max * nlm) || q.ensure(4 * (size_t)N * md->gap.dim_pad) || norm.ensure(4 * (size_t)N))
+        return set_error(ctx, TGAP_ERR_NOMEM, "screen initialisation");
+    PairView pv{sys->nb.start.as<int64_t>(), sys->nb.xyz.as<double>(), sys->nb.rjs.as<double>(),
+                sys->nb.nspecies.as<int>(), sys->nb.jatom.as<int>(), N, ctx->d_check};
+    SoapOut o;
+    o.c = c.ptr;
+    o.q = q.ptr;
+    o.norm = norm.ptr;
+    o.q_ld = md->gap.dim_pad;
+    CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, N, TGAP_MIXED, o));
+    CHECK_RC(screen_rows(ctx, mc->sd, q.as<float>(), o.q_ld, N, nullptr, mc->es_cache.as<float>()));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    mc->screened = true;
+    // the per-proposal graph changes shape
+    if (mc->exec) cudaGraphExecDestroy(mc->exec);
+    if (mc->graph) cudaGraphDestroy(mc->graph);
+    mc->exec = nullptr;
+    mc->graph = nullptr;
+    return read_device_check(ctx);
+}
+
+extern "C" int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char *stage)
+{
+    if (!mc || n < 0 || n > mc->last_n) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = mc->ctx;
+    CHECK_RC(activate(ctx));
+    if (de_screen) CHECK_RC(download(ctx, de_screen, mc->log_des, (size_t)n));
+    if (stage) TGAP_CUDA(ctx, cudaMemcpyAsync(stage, mc->log_stage.ptr, (size_t)n, cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return TGAP_OK;
 }

@@ -38,9 +38,11 @@ int gap_energy_grad_f64(tgap_context *ctx, const DeviceModel &m, const double *d
                         double *d_e_rows, double *d_energies);
 
 // Mixed path: q given as bf16 hi/lo [rows_pad][dim_pad]; w->g = dE/dq (float [n_rows][dim_pad]).
+// d_skip (fused kernel only): a device flag that, when set at run time, makes the launch a no-op.
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces,
-                          GapWork *w, const int *d_sites, double *d_e_rows, double *d_energies);
+                          GapWork *w, const int *d_sites, double *d_e_rows, double *d_energies,
+                          const int *d_skip = nullptr);
 int model_upload_mixed(tgap_context *ctx, DeviceModel *m);
 
 int pair_forces_from_der(tgap_context *ctx, int n_sites, const int64_t *d_start, const int *d_nl,

@@ -468,6 +468,7 @@ struct FlashGap {
     int zeta_int;
     float *g;             // dE/dq [rows_pad][ldg], accumulated (zeroed by the caller); null: energies only
     int ldg;
+    const int *skip;      // optional device flag: when set, the launch does nothing
 };
 
 template <int ZI>
@@ -524,6 +525,7 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                                  ((uint32_t)(kBM >> 4) << 24);
     constexpr uint32_t kCols = 512;
     const bool forces = p.g != nullptr;
+    if (p.skip && *p.skip) return;  // uniform over the grid, before any TMEM or barrier set-up
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
@@ -951,7 +953,7 @@ int model_upload_mixed(tgap_context *ctx, DeviceModel *m)
 
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces, GapWork *w,
-                          const int *d_sites, double *d_e_rows, double *d_energies)
+                          const int *d_sites, double *d_e_rows, double *d_energies, const int *d_skip)
 {
     if (n_rows <= 0) return TGAP_OK;
     constexpr int BN1 = 128;  // m_pad is a multiple of 128; 256-column tiles when it allows
@@ -979,6 +981,7 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         p.zd2 = (float)(p.zeta * m.delta * m.delta);
         p.g = do_forces ? w->g.as<float>() : nullptr;
         p.ldg = m.dim_pad;
+        p.skip = d_skip;
         // 128-point sparse tiles (64-point ones allow a deeper ring but double the per-tile handoffs,
         // and measured slower)
         switch (m.dim_pad) {
@@ -987,6 +990,7 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         default: return launch_flash<384, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
         }
     }
+    if (d_skip) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "skippable launch needs the fused GAP kernel");
     if (w->G_hi.ensure(2 * (size_t)rows_pad * m.m_pad) || w->G_lo.ensure(2 * (size_t)rows_pad * m.m_pad))
         return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
     EpiKernelGap e1;

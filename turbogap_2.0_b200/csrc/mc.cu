@@ -66,6 +66,7 @@ __global__ void k_mc_select(McDev *st, const int64_t *__restrict__ start, const 
         }
         if (status != kMcRunning)
             for (int m = 0; m < kMcMaxModels; ++m) st->count[m] = 0;
+        st->skip = 0;
         s_status = status;
         // serial of this proposal, unique over the object's lifetime (stamps mark[])
         if (status == kMcRunning) s_serial = ++st->serial;
@@ -184,14 +185,46 @@ __global__ void k_mc_trial_geometry(const McDev *st, int n_models, const int *__
     }
 }
 
+// kB of mc_utils.f90:176, a default-real literal
+__device__ __forceinline__ double mc_kb() { return (double)8.617333262e-5f; }
+
+// One warp: screen dE of the affected sites (model 0) in a fixed reduction order, stage-1 test.
+__global__ void k_mc_screen_stage(McDev *st, const int *__restrict__ sites, const float *__restrict__ es_trial,
+                                  const float *__restrict__ es_cache, const double *__restrict__ prop_u,
+                                  double temperature, McLogs logs)
+{
+    const int lane = threadIdx.x & 31;
+    if (st->status != kMcRunning) return;
+    const long long k = st->next;
+    const int c = st->count[0];
+    double des = 0.0;
+    for (int r = lane; r < c; r += 32) des += (double)es_trial[r] - (double)es_cache[sites[r]];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) des += __shfl_xor_sync(0xffffffffu, des, o);
+    if (lane == 0) {
+        double p = exp(-des / (mc_kb() * temperature));
+        p = p < 1.0 ? p : 1.0;
+        st->de_screen = des;
+        if (logs.de_screen) logs.de_screen[k] = des;
+        if (!(p > prop_u[2 * k])) {
+            st->skip = 1;
+            if (logs.de) logs.de[k] = __longlong_as_double(0x7ff8000000000000ll);
+            if (logs.acc) logs.acc[k] = 0;
+            if (logs.stage) logs.stage[k] = 1;
+            st->next = k + 1;
+        }
+    }
+}
+
 // One warp: dE in a fixed reduction order, then the reference's acceptance test.
 __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sites, int cap,
                             const double *__restrict__ etrial, double *__restrict__ ecache, int n_atoms,
                             double *__restrict__ pos, double *__restrict__ dacc, const double *__restrict__ prop_u,
-                            double temperature, double *__restrict__ log_de, unsigned char *__restrict__ log_acc)
+                            double temperature, McLogs logs, int screened, const float *__restrict__ es_trial,
+                            float *__restrict__ es_cache)
 {
     const int lane = threadIdx.x & 31;
-    if (st->status != kMcRunning) return;
+    if (st->status != kMcRunning || st->skip) return;
     const long long k = st->next;
     double de = 0.0;
     for (int m = 0; m < n_models; ++m) {
@@ -203,14 +236,16 @@ __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sit
     for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
     int accept = 0;
     if (lane == 0) {
-        // mc_utils.f90:172-180: kB is a default-real literal; get_mc_acceptance (:255) takes
-        // min(1, p); mc_interface.f90:286 accepts when p > ranf
-        const double kB = (double)8.617333262e-5f;
-        double p = exp(-de / (kB * temperature));
+        // mc_utils.f90:172-180 (p = exp(-dE / kB T)); get_mc_acceptance (:255) takes min(1, p);
+        // mc_interface.f90:286 accepts when p > ranf. Delayed acceptance replaces dE by dE - dE_s
+        // and uses the second deviate.
+        const double x = screened ? de - st->de_screen : de;
+        double p = exp(-x / (mc_kb() * temperature));
         p = p < 1.0 ? p : 1.0;
-        accept = p > prop_u[k] ? 1 : 0;
-        if (log_de) log_de[k] = de;
-        if (log_acc) log_acc[k] = (unsigned char)accept;
+        accept = p > (screened ? prop_u[2 * k + 1] : prop_u[k]) ? 1 : 0;
+        if (logs.de) logs.de[k] = de;
+        if (logs.acc) logs.acc[k] = (unsigned char)accept;
+        if (logs.stage) logs.stage[k] = 2;
     }
     accept = __shfl_sync(0xffffffffu, accept, 0);
     if (accept) {
@@ -219,6 +254,8 @@ __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sit
             for (int r = lane; r < c; r += 32)
                 ecache[(size_t)m * n_atoms + sites[m * cap + r]] = etrial[(size_t)m * cap + r];
         }
+        if (screened)
+            for (int r = lane; r < st->count[0]; r += 32) es_cache[sites[r]] = es_trial[r];
         if (lane == 0) {
             const int a = st->atom;
             pos[3 * (size_t)a] = st->pos_new[0];
@@ -274,12 +311,20 @@ int mc_trial_geometry(tgap_context *ctx, const McDev *d_st, const NeighborBatch 
     return TGAP_OK;
 }
 
+int mc_screen_stage(tgap_context *ctx, McDev *d_st, const int *d_sites, const float *d_es_trial,
+                    const float *d_es_cache, const double *d_prop_u, double temperature, McLogs logs)
+{
+    k_mc_screen_stage<<<1, 32, 0, ctx->stream>>>(d_st, d_sites, d_es_trial, d_es_cache, d_prop_u, temperature, logs);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
 int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
               double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
-              double temperature, double *d_log_de, unsigned char *d_log_acc)
+              double temperature, McLogs logs, int screened, const float *d_es_trial, float *d_es_cache)
 {
     k_mc_accept<<<1, 32, 0, ctx->stream>>>(d_st, n_models, d_sites, cap, d_etrial, d_ecache, n_atoms, d_positions,
-                                           d_dacc, d_prop_u, temperature, d_log_de, d_log_acc);
+                                           d_dacc, d_prop_u, temperature, logs, screened, d_es_trial, d_es_cache);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -25,7 +25,17 @@ struct McDev {
     double pos_new[3];   // its trial position
     double dnorm;        // |d|
     double maxD;         // largest accumulated displacement since the last list build
+    double de_screen;    // screen energy change of the proposal in flight
+    int skip;            // 1: the proposal was settled by the screen (exact stage skipped)
     int count[kMcMaxModels];  // affected sites per model for the proposal in flight
+};
+
+// Per-proposal logs (device arrays of the run's length, any may be null).
+struct McLogs {
+    double *de;            // exact dE (NaN when the screen rejected the move)
+    unsigned char *acc;    // 1 accepted
+    double *de_screen;     // screen dE (delayed acceptance only)
+    unsigned char *stage;  // 1: settled by the screen, 2: by the exact energies
 };
 
 enum McStatus { kMcRunning = 0, kMcNeedRebuild = 1, kMcDone = 2 };
@@ -49,11 +59,19 @@ int mc_select(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McM
 int mc_trial_geometry(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
                       const int *d_sites, int cap, int pmax, double *d_txyz, double *d_trjs, int *d_tnsp);
 
+// Delayed acceptance, stage 1 (Christen and Fox): the screen's energy change dE_s of the
+// affected sites (model 0's rows) against u1 = prop_u[2k]; a rejection settles the proposal
+// (st->skip = 1, logged, st->next advanced) and the exact stage does nothing.
+int mc_screen_stage(tgap_context *ctx, McDev *d_st, const int *d_sites, const float *d_es_trial,
+                    const float *d_es_cache, const double *d_prop_u, double temperature, McLogs logs);
+
 // Energy change, acceptance and commit (positions, cached site energies, displacement
-// bookkeeping); logs dE and the decision of proposal st->next and advances it.
+// bookkeeping); logs dE and the decision of proposal st->next and advances it. With a screen
+// (screened != 0) the test is min(1, exp(-(dE - dE_s) / kB T)) > u2 = prop_u[2k + 1] and the
+// screen cache of the affected sites is committed too; otherwise min(1, exp(-dE / kB T)) > prop_u[k].
 int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
               double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
-              double temperature, double *d_log_de, unsigned char *d_log_acc);
+              double temperature, McLogs logs, int screened, const float *d_es_trial, float *d_es_cache);
 
 // Start of a run of n proposals (keeps a pending rebuild request), and the reset after a list
 // rebuild.
