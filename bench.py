@@ -35,8 +35,9 @@ N_SPARSE = 2000
 MC_ATOMS, MC_DENSITY, MC_T, MC_RADIUS, MC_SKIN = 1000, 2.0, 2000.0, 0.2, 0.5
 MC_PROPOSALS = 20000
 MC_WORKLOAD = ("NVT Metropolis MC, 1000 C atoms, 2.0 g/cm3, 2000 K, single-atom moves uniform in a 0.2 A ball, "
-               "local SOAP/GAP update of atoms within rcut of the moved atom (exact GAP, no screen), "
-               "same SOAP settings and 2000-sparse GAP as the MD workload")
+               "local SOAP/GAP update of atoms within rcut of the moved atom, same SOAP settings and 2000-sparse "
+               "GAP as the MD workload; 'screened': delayed acceptance with a PCA-64 / 128 / 128 SiLU bf16 screen "
+               "trained on 200k atomic energies of 2000 plain-MC snapshots")
 DT = 1.0
 REBUILD = 10
 SKIN = 0.3
@@ -400,11 +401,89 @@ def _mc_leg(tg, torch, ctx, stream, model, n_prop, seed):
         st1 = mc.state()
         out[name] = dict(moves_per_s=n_prop / (ms * 1e-3), us_per_move=1e3 * ms / n_prop,
                          acceptance=r["accepted"] / n_prop, list_rebuilds=st1["rebuilds"] - st0["rebuilds"])
+        if name == "mixed":
+            final = st1
         mc.close()
         system.close()
+    screened = _mc_screen_leg(tg, torch, ctx, stream, model, n_prop, seed, final)
     return dict(workload=MC_WORKLOAD, proposals=n_prop, unit="moves/s", value=out["mixed"]["moves_per_s"],
-                mixed=out["mixed"], plain_fp64=out["fp64"],
+                mixed=out["mixed"], plain_fp64=out["fp64"], screened=screened,
                 speedup_mixed_vs_fp64=out["mixed"]["moves_per_s"] / out["fp64"]["moves_per_s"])
+
+
+def _rdf(pos, box, r_max=6.0, bins=60):
+    """g(r) of a cubic periodic box (minimum image), numpy."""
+    L = box[0][0]
+    n = len(pos)
+    d = pos[:, None, :] - pos[None, :, :]
+    d -= L * np.round(d / L)
+    r = np.sqrt((d ** 2).sum(-1))[np.triu_indices(n, 1)]
+    h, edges = np.histogram(r, bins=bins, range=(0.0, r_max))
+    shell = 4.0 / 3.0 * np.pi * (edges[1:] ** 3 - edges[:-1] ** 3)
+    return h / (shell * n * (n - 1) / 2 / L ** 3)
+
+
+def _mc_screen_leg(tg, torch, ctx, stream, model, n_prop, seed, plain):
+    """The MC workload with the learned screen (delayed acceptance): training on 200k atomic
+    energies from 2000 snapshots of plain (exact) MC, then screened moves/s on a fresh chain, and
+    the comparison with the plain chain (energy statistics, radial distribution function)."""
+    import ctypes as C
+    from turbogap_b200 import native
+    pos, box, sp, _ = tg.synth.random_packing(MC_ATOMS, MC_DENSITY, 1.2, seed=seed)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + MC_SKIN)
+    mc = tg.MC(ctx, system, [model], MC_T, precision=tg.TGAP_MIXED)
+    n_snap, gap = 2000, 5
+    atoms, disp, u = tg.synth.mc_proposals(MC_ATOMS, n_snap * gap, MC_RADIUS, seed=seed + 7)
+    rng = np.random.default_rng(seed + 8)
+    q = torch.zeros((MC_ATOMS, model.dim), dtype=torch.float64, device="cuda")
+    qs, es = [], []
+    t0 = time.perf_counter()
+    for k in range(n_snap):
+        mc.run(atoms[k * gap:(k + 1) * gap], disp[k * gap:(k + 1) * gap], u[k * gap:(k + 1) * gap], logs=False)
+        e_atoms = mc.state()["energies"]
+        system.update(False)
+        nr = C.c_int(0)
+        native.check(native.lib().tgap_descriptors(ctx.h, system.h, model.h, 0, C.c_void_p(q.data_ptr()),
+                                                   C.byref(nr)), ctx.h, "descriptors")
+        ctx.synchronize()
+        pick = rng.choice(MC_ATOMS, size=100, replace=False)
+        qs.append(q[torch.as_tensor(pick, device="cuda")].cpu().numpy())
+        es.append(e_atoms[pick])
+    t_data = time.perf_counter() - t0
+    mc.close()
+    system.close()
+    qs, es = np.concatenate(qs), np.concatenate(es)
+    val = rng.random(len(es)) < 0.05
+    t0 = time.perf_counter()
+    w = tg.screen.fit(qs[~val], es[~val], n_pca=64, hidden=128, epochs=6, batch=1024, seed=seed)
+    t_fit = time.perf_counter() - t0
+    rmse = float(np.sqrt(np.mean((tg.screen.predict(w, qs[val]) - es[val]) ** 2)))
+    # screened chain from the same start on the plain leg's proposals (second deviate added)
+    atoms, disp, u1 = tg.synth.mc_proposals(MC_ATOMS, n_prop + 256, MC_RADIUS, seed=seed + 1)
+    u = np.stack([u1, np.random.default_rng(seed + 9).random(len(u1))], axis=1)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + MC_SKIN)
+    mc = tg.MC(ctx, system, [model], MC_T, precision=tg.TGAP_MIXED)
+    mc.set_screen(w)
+    mc.run(atoms[:256], disp[:256], u[:256], logs=False)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    r = mc.run(atoms[256:], disp[256:], u[256:], logs=True)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    _, stage = mc.screen_log(n_prop)
+    st = mc.state()
+    out = dict(moves_per_s=n_prop / (ms * 1e-3), us_per_move=1e3 * ms / n_prop, acceptance=r["accepted"] / n_prop,
+               settled_by_screen=float(np.mean(stage == 1)), exact_evaluations_per_move=float(np.mean(stage == 2)),
+               screen_validation_rmse_meV_per_atom=1e3 * rmse, training=dict(
+                   snapshots=n_snap, energies=int((~val).sum()), data_s=round(t_data, 1), fit_s=round(t_fit, 1)),
+               energy_mean_meV_per_atom=1e3 * st["e_total"] / MC_ATOMS,
+               plain_energy_mean_meV_per_atom=1e3 * plain["e_total"] / MC_ATOMS,
+               rdf_l1_vs_plain=float(np.abs(_rdf(st["positions"], box) - _rdf(plain["positions"], box)).mean()))
+    mc.close()
+    system.close()
+    return out
 
 
 def _mc_cpu_baseline(tg, model_np, seed, budget_s=10.0):

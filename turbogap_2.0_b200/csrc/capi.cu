@@ -1579,13 +1579,17 @@ extern "C" int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden,
                          "the screen needs the mixed path, one model over all sites and a descriptor of <= 384");
     const tgap_model *md = mc->models[0];
     if (dim != md->gap.dim) return set_error(ctx, TGAP_ERR_ARGUMENT, "screen dim %d != descriptor %d", dim, md->gap.dim);
-    auto to_bf16 = [](const float *x, size_t n) {
-        std::vector<__nv_bfloat16> v(n);
-        for (size_t i = 0; i < n; ++i) v[i] = __float2bfloat16_rn(x[i]);
+    if (screen_smem_bytes(dim, n_pca, n_hidden) > 227 * 1024)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "screen too large for one CTA's shared memory");
+    // bf16, transposed to input-index-major (the kernel reads along the output index)
+    auto to_bf16_t = [](const float *x, size_t rows, size_t cols) {
+        std::vector<__nv_bfloat16> v(rows * cols);
+        for (size_t r = 0; r < rows; ++r)
+            for (size_t c = 0; c < cols; ++c) v[c * rows + r] = __float2bfloat16_rn(x[r * cols + c]);
         return v;
     };
-    const auto vp = to_bf16(pca, (size_t)n_pca * dim), v1 = to_bf16(w1, (size_t)n_hidden * n_pca),
-               v2 = to_bf16(w2, (size_t)n_hidden * n_hidden), v3 = to_bf16(w3, (size_t)n_hidden);
+    const auto vp = to_bf16_t(pca, n_pca, dim), v1 = to_bf16_t(w1, n_hidden, n_pca),
+               v2 = to_bf16_t(w2, n_hidden, n_hidden), v3 = to_bf16_t(w3, n_hidden, 1);
     CHECK_RC(upload(ctx, mc->s_mean, mean, (size_t)dim));
     CHECK_RC(upload(ctx, mc->s_pca, vp.data(), vp.size()));
     CHECK_RC(upload(ctx, mc->s_w1, v1.data(), v1.size()));
