@@ -288,6 +288,44 @@ int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden, const floa
                        const float *b2, const float *w3, float b3);
 /* Screen dE and the deciding stage (1: screen, 2: exact) of the last run's first n proposals. */
 int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char *stage);
+/* Fallback to plain GAP MC (no counterpart in the reference, whose MC has no screen). Over each
+ * window of `window` screen-judged proposals, pass = fraction passed to the exact stage and
+ * confirm = fraction of those the exact stage accepts; when pass < min_pass, or confirm <
+ * min_confirm with at least 32 passed, the screen is switched off for the rest of the MC object's
+ * life (or until tgap_mc_set_screen installs one again). Proposals still take deviate pairs; plain
+ * moves use the first. Defaults: 2048, 0.1, 0.002. */
+int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass);
+/* Screen counters since creation (any pointer may be NULL): whether the screen is in use,
+ * proposals it judged, passed to the exact stage, confirmed there, and fallbacks taken. */
+int tgap_mc_screen_stats(tgap_mc *mc, int *active, int64_t *judged, int64_t *passed,
+                         int64_t *confirmed, int64_t *fallbacks);
+
+/* ---- Screen network training and evaluation (no counterpart in the reference). The network
+ * part of the screen, on standardised PCA coordinates z (row-major n x n_pca):
+ *   out = w3 . silu(W2 silu(W1 z + b1) + b2) + b3   (W1: n_hidden x n_pca, W2: n_hidden x n_hidden)
+ * and the loss (1/n) sum (out - t)^2 against targets t. FP32 throughout; n_pca <= 256,
+ * n_hidden <= 512, with the pair limited to one CTA's shared memory (64 x 128 fits). */
+
+/* Loss and its gradients over all n rows (n <= 16384), as one batch. Host arrays. */
+int tgap_screen_grad(tgap_context *ctx, int64_t n, int n_pca, int n_hidden, const float *z,
+                     const float *t, const float *w1, const float *b1, const float *w2,
+                     const float *b2, const float *w3, float b3, float *g_w1, float *g_b1,
+                     float *g_w2, float *g_b2, float *g_w3, float *g_b3, double *loss);
+/* Adam (beta 0.9 / 0.999, eps 1e-8, bias-corrected) on minibatches of `batch` rows, epoch e
+ * visiting rows order[e * n .. e * n + n) in that order (the last batch of an epoch may be
+ * short), learning rate lr * (1 + cos(pi e / epochs)) / 2. The weights are read as the initial
+ * point and overwritten with the result; loss_log (optional, `epochs` entries) gets each
+ * epoch's mean squared error over its minibatches (weights before each update). */
+int tgap_screen_train(tgap_context *ctx, int64_t n, int n_pca, int n_hidden, const float *z,
+                      const float *t, int epochs, int batch, float lr, const int *order, float *w1,
+                      float *b1, float *w2, float *b2, float *w3, float *b3, double *loss_log);
+/* Screen energies e (n) of descriptor rows q (row-major n x dim, FP32) with the full screen
+ * (PCA and network, weights as tgap_mc_set_screen takes them, rounded to bf16 the same way);
+ * the kernel the Monte Carlo driver runs. */
+int tgap_screen_eval(tgap_context *ctx, int64_t n, int dim, int n_pca, int n_hidden,
+                     const float *mean, const float *pca, const float *w1, const float *b1,
+                     const float *w2, const float *b2, const float *w3, float b3, const float *q,
+                     double *e);
 
 #ifdef __cplusplus
 }

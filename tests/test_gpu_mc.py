@@ -10,6 +10,7 @@ import numpy as np
 import pytest
 
 import helpers
+import screen_ref
 
 pytestmark = pytest.mark.gpu
 
@@ -195,7 +196,7 @@ def test_mc_screen_delayed_acceptance_matches_cpu_chain(ctx, tg, synth, carbon):
     pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=80)
     model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
     q_tr, e_tr = _gpu_snapshot_data(ctx, tg, synth, hyp, model, pos, box, sp, 40, 0.08, seed=81)
-    w = tg.screen.fit(q_tr, e_tr, n_pca=32, hidden=64, epochs=40, seed=2)
+    w = tg.screen.fit(ctx, q_tr, e_tr, n_pca=32, hidden=64, epochs=40, seed=2)
     T = 30.0
     system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.4)
     mc = tg.MC(ctx, system, [model], T, precision=tg.TGAP_MIXED)
@@ -209,12 +210,12 @@ def test_mc_screen_delayed_acceptance_matches_cpu_chain(ctx, tg, synth, carbon):
     assert np.sum(stage_g == 1) > 0 and np.sum(stage_g == 2) > 0
     # CPU replay
     p = np.array(pos, dtype=np.float64)
-    es_cur = tg.screen.predict(w, helpers.oracle_descriptors(hyp, p, box, sp))
+    es_cur = screen_ref.predict(w, helpers.oracle_descriptors(hyp, p, box, sp))
     e_cur = helpers.oracle_structure_eval(hyp, [m], p, box, sp, do_forces=False)[0].sum()
     for k in range(len(atoms)):
         qn = p.copy()
         qn[atoms[k]] = qn[atoms[k]] + disp[k]
-        es_new = tg.screen.predict(w, helpers.oracle_descriptors(hyp, qn, box, sp))
+        es_new = screen_ref.predict(w, helpers.oracle_descriptors(hyp, qn, box, sp))
         des = es_new.sum() - es_cur.sum()
         assert abs(des - des_g[k]) < 2e-4, (k, des, des_g[k])
         p1 = min(1.0, float(np.exp(-des / (KB * T))))
@@ -230,3 +231,64 @@ def test_mc_screen_delayed_acceptance_matches_cpu_chain(ctx, tg, synth, carbon):
                 p, es_cur, e_cur = qn, es_new, e_new
     assert np.array_equal(st["positions"], p)
     mc.close()
+
+
+def test_mc_screen_fallback_to_plain_when_acceptance_collapses(ctx, tg, synth, carbon):
+    """A screen whose energies are noise (large random output weights): the exact stage rejects
+    what it lets through, so over the first window the confirmation rate collapses and the driver
+    switches to plain GAP MC. Before the switch every decision follows the delayed-acceptance
+    rule, after it the plain rule on the first deviate of each pair."""
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=90)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    dim = tg.synth.soap_dim(hyp)
+    rng = np.random.default_rng(91)
+    K, H = 16, 32
+    bad = dict(mean=np.zeros(dim), pca=rng.normal(size=(K, dim)), w1=rng.normal(size=(H, K)), b1=np.zeros(H),
+               w2=rng.normal(size=(H, H)) * 0.3, b2=np.zeros(H), w3=rng.normal(size=H) * 0.5, b3=0.0)
+    T = 300.0
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.4)
+    mc = tg.MC(ctx, system, [model], T, precision=tg.TGAP_MIXED)
+    mc.set_screen(bad)
+    mc.screen_fallback(window=128, min_confirm=0.2, min_pass=0.0)
+    n = 512
+    atoms, disp, _ = synth.mc_proposals(len(pos), n, 0.2, seed=92)
+    u = rng.random((n, 2))
+    out = mc.run(atoms, disp, u)
+    des, stage = mc.screen_log(n)
+    s = mc.screen_stats()
+    assert not s["active"] and s["fallbacks"] == 1
+    k_fb = s["judged"]
+    assert 128 <= k_fb < n and k_fb % 32 == 0  # checked between graph batches of 32
+    assert s["passed"] >= 32
+    for k in range(n):
+        if k < k_fb:
+            if stage[k] == 1:
+                assert not out["accept"][k]
+                continue
+            p2 = min(1.0, float(np.exp(-(out["de"][k] - des[k]) / (KB * T))))
+            assert (p2 > u[k, 1]) == bool(out["accept"][k]), k
+        else:
+            assert stage[k] == 2 and np.isfinite(out["de"][k])
+            p = min(1.0, float(np.exp(-out["de"][k] / (KB * T))))
+            assert (p > u[k, 0]) == bool(out["accept"][k]), k
+    mc.close()
+    system.close()
+
+
+def test_mc_rejects_moves_beyond_the_skin(ctx, tg, synth, carbon):
+    """A displacement at or above the neighbor skin could bring in a pair no list holds, even
+    right after a rebuild: the run refuses it before any work, and the driver stays usable."""
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=93)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    mc = tg.MC(ctx, system, [model], 300.0, precision=tg.TGAP_MIXED)
+    atoms = np.array([3, 5], np.int32)
+    disp = np.array([[0.1, 0.0, 0.0], [0.0, 0.35, 0.0]])
+    with pytest.raises(Exception):
+        mc.run(atoms, disp, np.array([0.5, 0.5]))
+    r = mc.run(atoms[:1], disp[:1], np.array([0.5]))
+    assert r["accepted"] in (0, 1)
+    mc.close()
+    system.close()

@@ -355,6 +355,21 @@ class MC:
         check(self.ctx._L.tgap_mc_screen_log(self.h, n, ptr(des), ptr(st)), self.ctx.h, "tgap_mc_screen_log")
         return des, st
 
+    def screen_fallback(self, window=2048, min_confirm=0.1, min_pass=0.002):
+        """Sets when the driver gives up on the screen and continues as plain GAP MC: over each
+        window of screen-judged proposals, a pass rate below min_pass or an exact-stage
+        confirmation rate below min_confirm switches it off."""
+        check(self.ctx._L.tgap_mc_screen_fallback(self.h, int(window), float(min_confirm), float(min_pass)),
+              self.ctx.h, "tgap_mc_screen_fallback")
+
+    def screen_stats(self):
+        active = C.c_int()
+        v = [C.c_int64() for _ in range(4)]
+        check(self.ctx._L.tgap_mc_screen_stats(self.h, C.byref(active), *[C.byref(x) for x in v]),
+              self.ctx.h, "tgap_mc_screen_stats")
+        return dict(active=bool(active.value), judged=v[0].value, passed=v[1].value, confirmed=v[2].value,
+                    fallbacks=v[3].value)
+
     def run(self, atoms, displacements, uniforms, logs=True):
         atoms = np.ascontiguousarray(atoms, dtype=np.int32)
         disp = _f64(displacements)

@@ -35,6 +35,7 @@ SOURCES = [
     ("md.cu", []),
     ("mc.cu", ["--fmad=false"]),
     ("screen.cu", []),
+    ("screen_train.cu", []),
     ("tables.cpp", []),
 ]
 

@@ -1251,8 +1251,13 @@ struct tgap_mc {
     cudaGraphExec_t exec = nullptr;
     uint64_t graph_epoch = 0;
     int64_t graph_kernels = 0;
-    // learned screen (delayed acceptance)
-    bool screened = false;
+    // learned screen (delayed acceptance); screened: installed (proposals carry deviate pairs),
+    // screen_active: used by the step (off after a fallback to plain GAP MC)
+    bool screened = false, screen_active = false;
+    int64_t fb_window = 2048;                     // screened proposals per fallback check
+    double fb_min_confirm = 0.1, fb_min_pass = 0.002;
+    long long fb_prop0 = 0, fb_pass0 = 0, fb_conf0 = 0;  // counters at the start of the window
+    int64_t fallbacks = 0;
     ScreenDev sd{};
     DevBuf s_mean, s_pca, s_w1, s_b1, s_w2, s_b2, s_w3, es_cache, es_trial;
     int64_t last_n = 0;
@@ -1349,7 +1354,7 @@ static int mc_step_body(tgap_mc *mc)
             o.q_lo = mc->q_lo[m].as<__nv_bfloat16>();
             CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, cap, TGAP_MIXED, o));
             const int *skip = nullptr;
-            if (mc->screened) {
+            if (mc->screen_active) {
                 // stage 1 on the trial rows' screen energies; a rejection skips the exact GEMM
                 const int *d_count = reinterpret_cast<const int *>(reinterpret_cast<const char *>(st) +
                                                                    offsetof(McDev, count));
@@ -1364,7 +1369,39 @@ static int mc_step_body(tgap_mc *mc)
     }
     return mc_accept(ctx, st, M, mc->sites.as<int>(), cap, mc->etrial.as<double>(), mc->ecache.as<double>(), N,
                      nb.positions.as<double>(), mc->dacc.as<double>(), mc->pu.as<double>(), mc->temperature,
-                     mc_logs(mc), mc->screened ? 1 : 0, mc->es_trial.as<float>(), mc->es_cache.as<float>());
+                     mc_logs(mc), mc->screen_active ? 1 : 0, mc->screened ? 2 : 1, mc->es_trial.as<float>(),
+                     mc->es_cache.as<float>());
+}
+
+static void mc_drop_graph(tgap_mc *mc)
+{
+    if (mc->exec) cudaGraphExecDestroy(mc->exec);
+    if (mc->graph) cudaGraphDestroy(mc->graph);
+    mc->exec = nullptr;
+    mc->graph = nullptr;
+}
+
+// Fallback to plain GAP MC when the screen's acceptance collapses: over each window of
+// fb_window screened proposals, the fraction passed to the exact stage (pass) and the fraction of
+// those the exact energies confirm (confirm). Either falling below its floor switches the screen
+// off; the chain's target distribution is the same either way, so the switch may happen at any
+// proposal boundary. Returns true when it switched.
+static bool mc_screen_check(tgap_mc *mc, const McDev &h)
+{
+    if (!mc->screen_active) return false;
+    const long long np = h.s_prop - mc->fb_prop0;
+    if (np < mc->fb_window) return false;
+    const long long npass = h.s_pass - mc->fb_pass0, nconf = h.s_conf - mc->fb_conf0;
+    const double pass = (double)npass / (double)np;
+    const double confirm = npass > 0 ? (double)nconf / (double)npass : 1.0;
+    mc->fb_prop0 = h.s_prop;
+    mc->fb_pass0 = h.s_pass;
+    mc->fb_conf0 = h.s_conf;
+    if (pass >= mc->fb_min_pass && (npass < 32 || confirm >= mc->fb_min_confirm)) return false;
+    mc->screen_active = false;
+    ++mc->fallbacks;
+    mc_drop_graph(mc);
+    return true;
 }
 
 static int mc_read_state(tgap_mc *mc, McDev *out)
@@ -1466,8 +1503,17 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
         return TGAP_OK;
     }
     const int N = mc->sys->nb.n_atoms;
-    for (int64_t k = 0; k < n; ++k)
+    for (int64_t k = 0; k < n; ++k) {
         if (atoms[k] < 0 || atoms[k] >= N) return set_error(ctx, TGAP_ERR_ARGUMENT, "proposal %lld: atom", (long long)k);
+        // a move of |d| >= skin could bring a pair into the cutoff that no skin-padded list holds,
+        // even right after a rebuild
+        const double d2 = disp[3 * k] * disp[3 * k] + disp[3 * k + 1] * disp[3 * k + 1] + disp[3 * k + 2] * disp[3 * k + 2];
+        if (!(d2 < mc->skin * mc->skin))
+            return set_error(ctx, TGAP_ERR_ARGUMENT,
+                             "proposal %lld: displacement %g A is not below the neighbor skin %g A (system cutoff "
+                             "minus model cutoff)",
+                             (long long)k, std::sqrt(d2), mc->skin);
+    }
     const size_t nu = (mc->screened ? 2 : 1) * (size_t)n;  // two deviates per proposal with a screen
     if (mc->patom.ensure(sizeof(int) * n) || mc->pdisp.ensure(sizeof(double) * 3 * n) ||
         mc->pu.ensure(sizeof(double) * nu) || mc->log_de.ensure(sizeof(double) * n) || mc->log_acc.ensure(n) ||
@@ -1481,9 +1527,15 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
     CHECK_RC(mc_read_state(mc, &h));
     const long long acc0 = h.accepted;
     CHECK_RC(mc_begin(ctx, mc->st.as<McDev>(), n));
+    long long rebuilt_at = -1;  // proposal index of the last rebuild
     for (;;) {
         CHECK_RC(mc_read_state(mc, &h));
         if (h.status == kMcNeedRebuild) {
+            // fresh lists always admit a move below the skin; a second request for the same
+            // proposal means the state is inconsistent, not that another rebuild would help
+            if (rebuilt_at == h.next)
+                return set_error(ctx, TGAP_ERR_NUMERIC, "proposal %lld still needs a list rebuild after one", h.next);
+            rebuilt_at = h.next;
             // lists at the current positions; the cached site energies stay valid
             NeighborBatch &nb = mc->sys->nb;
             CHECK_RC(neighbors_sync_positions(ctx, &nb));
@@ -1496,6 +1548,7 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
             continue;
         }
         if (h.status == kMcDone || h.next >= n) break;
+        mc_screen_check(mc, h);
         if (mc->use_graph) {
             if (!mc->exec || mc->graph_epoch != g_alloc_epoch.load(std::memory_order_relaxed)) {
                 if (mc->exec) cudaGraphExecDestroy(mc->exec);
@@ -1623,14 +1676,40 @@ extern "C" int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden,
     o.q_ld = md->gap.dim_pad;
     CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, N, TGAP_MIXED, o));
     CHECK_RC(screen_rows(ctx, mc->sd, q.as<float>(), o.q_ld, N, nullptr, mc->es_cache.as<float>()));
-    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    McDev h;
+    CHECK_RC(mc_read_state(mc, &h));
     mc->screened = true;
-    // the per-proposal graph changes shape
-    if (mc->exec) cudaGraphExecDestroy(mc->exec);
-    if (mc->graph) cudaGraphDestroy(mc->graph);
-    mc->exec = nullptr;
-    mc->graph = nullptr;
-    return read_device_check(ctx);
+    mc->screen_active = true;
+    mc->fb_prop0 = h.s_prop;
+    mc->fb_pass0 = h.s_pass;
+    mc->fb_conf0 = h.s_conf;
+    mc_drop_graph(mc);  // the per-proposal graph changes shape
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass)
+{
+    if (!mc || window < 1 || !(min_confirm >= 0.0 && min_confirm <= 1.0) || !(min_pass >= 0.0 && min_pass <= 1.0))
+        return TGAP_ERR_ARGUMENT;
+    mc->fb_window = window;
+    mc->fb_min_confirm = min_confirm;
+    mc->fb_min_pass = min_pass;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_screen_stats(tgap_mc *mc, int *active, int64_t *judged, int64_t *passed, int64_t *confirmed,
+                                    int64_t *fallbacks)
+{
+    if (!mc) return TGAP_ERR_ARGUMENT;
+    CHECK_RC(activate(mc->ctx));
+    McDev h;
+    CHECK_RC(mc_read_state(mc, &h));
+    if (active) *active = mc->screen_active ? 1 : 0;
+    if (judged) *judged = h.s_prop;
+    if (passed) *passed = h.s_pass;
+    if (confirmed) *confirmed = h.s_conf;
+    if (fallbacks) *fallbacks = mc->fallbacks;
+    return TGAP_OK;
 }
 
 extern "C" int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char *stage)

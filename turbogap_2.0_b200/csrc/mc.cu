@@ -205,6 +205,7 @@ __global__ void k_mc_screen_stage(McDev *st, const int *__restrict__ sites, cons
         double p = exp(-des / (mc_kb() * temperature));
         p = p < 1.0 ? p : 1.0;
         st->de_screen = des;
+        st->s_prop += 1;
         if (logs.de_screen) logs.de_screen[k] = des;
         if (!(p > prop_u[2 * k])) {
             st->skip = 1;
@@ -220,8 +221,8 @@ __global__ void k_mc_screen_stage(McDev *st, const int *__restrict__ sites, cons
 __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sites, int cap,
                             const double *__restrict__ etrial, double *__restrict__ ecache, int n_atoms,
                             double *__restrict__ pos, double *__restrict__ dacc, const double *__restrict__ prop_u,
-                            double temperature, McLogs logs, int screened, const float *__restrict__ es_trial,
-                            float *__restrict__ es_cache)
+                            double temperature, McLogs logs, int screened, int u_stride,
+                            const float *__restrict__ es_trial, float *__restrict__ es_cache)
 {
     const int lane = threadIdx.x & 31;
     if (st->status != kMcRunning || st->skip) return;
@@ -242,7 +243,11 @@ __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sit
         const double x = screened ? de - st->de_screen : de;
         double p = exp(-x / (mc_kb() * temperature));
         p = p < 1.0 ? p : 1.0;
-        accept = p > (screened ? prop_u[2 * k + 1] : prop_u[k]) ? 1 : 0;
+        accept = p > (screened ? prop_u[2 * k + 1] : prop_u[(long long)u_stride * k]) ? 1 : 0;
+        if (screened) {
+            st->s_pass += 1;
+            st->s_conf += accept;
+        }
         if (logs.de) logs.de[k] = de;
         if (logs.acc) logs.acc[k] = (unsigned char)accept;
         if (logs.stage) logs.stage[k] = 2;
@@ -321,10 +326,12 @@ int mc_screen_stage(tgap_context *ctx, McDev *d_st, const int *d_sites, const fl
 
 int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
               double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
-              double temperature, McLogs logs, int screened, const float *d_es_trial, float *d_es_cache)
+              double temperature, McLogs logs, int screened, int u_stride, const float *d_es_trial,
+              float *d_es_cache)
 {
     k_mc_accept<<<1, 32, 0, ctx->stream>>>(d_st, n_models, d_sites, cap, d_etrial, d_ecache, n_atoms, d_positions,
-                                           d_dacc, d_prop_u, temperature, logs, screened, d_es_trial, d_es_cache);
+                                           d_dacc, d_prop_u, temperature, logs, screened, u_stride, d_es_trial,
+                                           d_es_cache);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

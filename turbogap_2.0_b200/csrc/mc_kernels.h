@@ -28,6 +28,9 @@ struct McDev {
     double de_screen;    // screen energy change of the proposal in flight
     int skip;            // 1: the proposal was settled by the screen (exact stage skipped)
     int count[kMcMaxModels];  // affected sites per model for the proposal in flight
+    long long s_prop;    // proposals judged by the screen since creation (stage 1)
+    long long s_pass;    // of those, passed on to the exact stage
+    long long s_conf;    // of those, accepted by the exact stage
 };
 
 // Per-proposal logs (device arrays of the run's length, any may be null).
@@ -68,10 +71,13 @@ int mc_screen_stage(tgap_context *ctx, McDev *d_st, const int *d_sites, const fl
 // Energy change, acceptance and commit (positions, cached site energies, displacement
 // bookkeeping); logs dE and the decision of proposal st->next and advances it. With a screen
 // (screened != 0) the test is min(1, exp(-(dE - dE_s) / kB T)) > u2 = prop_u[2k + 1] and the
-// screen cache of the affected sites is committed too; otherwise min(1, exp(-dE / kB T)) > prop_u[k].
+// screen cache of the affected sites is committed too; otherwise min(1, exp(-dE / kB T)) >
+// prop_u[u_stride k] (u_stride 2 when the proposals carry deviate pairs for a screen that is
+// installed but switched off).
 int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, int cap, const double *d_etrial,
               double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
-              double temperature, McLogs logs, int screened, const float *d_es_trial, float *d_es_cache);
+              double temperature, McLogs logs, int screened, int u_stride, const float *d_es_trial,
+              float *d_es_cache);
 
 // Start of a run of n proposals (keeps a pending rebuild request), and the reset after a list
 // rebuild.

@@ -122,6 +122,13 @@ def lib():
         "tgap_mc_get_state": (i32, [vp, vp, vp, P(dbl), P(i64), P(i64)]),
         "tgap_mc_set_screen": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, C.c_float]),
         "tgap_mc_screen_log": (i32, [vp, i64, vp, vp]),
+        "tgap_mc_screen_fallback": (i32, [vp, i64, C.c_double, C.c_double]),
+        "tgap_mc_screen_stats": (i32, [vp, vp, vp, vp, vp, vp]),
+        "tgap_screen_grad": (i32, [vp, i64, i32, i32, vp, vp, vp, vp, vp, vp, vp, C.c_float,
+                                   vp, vp, vp, vp, vp, vp, vp]),
+        "tgap_screen_train": (i32, [vp, i64, i32, i32, vp, vp, i32, i32, C.c_float, vp,
+                                    vp, vp, vp, vp, vp, vp, vp]),
+        "tgap_screen_eval": (i32, [vp, i64, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, C.c_float, vp, vp]),
         "tgap_debug_poly3_w": (i32, [i32, vp]),
         "tgap_calculate_gap_soap": (i32, [vp, vp, i32, vp, i32, vp, i32, vp, vp, vp]),
         "tgap_timing_enable": (i32, [vp, i32]),
