@@ -580,6 +580,8 @@ def run_ours(args):
     model = tg.Model(ctx, hyp, model_np["Qs"], model_np["alphas"], model_np["delta"], model_np["zeta"])
     system = tg.System(ctx, [(pos, box, sp)], 3.7 + SKIN)
     flush = L2Flush(torch)
+    # launch shapes picked by the autotuner on this system, both precisions (before any graph)
+    tuning = system.autotune([model], tg.TGAP_MIXED, reps=5) + system.autotune([model], tg.TGAP_FP64, reps=3)
 
     # accuracy: single point, mixed vs FP64
     e64 = torch.zeros(N_ATOMS, dtype=torch.float64, device="cuda")
@@ -650,6 +652,7 @@ def run_ours(args):
             "energy_drift_meV_per_atom": 1e3 * drift,
             "roofline": roof,
             "stages_us_per_step": {k: v["total_ms"] * 1e3 / 20 for k, v in stages.items()},
+            "autotune": tuning,
             "cpu_baseline": cpu,
             "mc": mc_line,
             "e2e": e2e,

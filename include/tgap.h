@@ -224,6 +224,22 @@ int tgap_compute(tgap_context *ctx, tgap_system *system, int n_models,
                  tgap_model *const *models, int precision, int do_forces, double *d_energies,
                  double *d_forces, double *d_virial);
 
+/* Autotuner (no counterpart in the reference, which has no GPU launch shapes to choose). Runs
+ * tgap_compute on this system and these models once to collect the tunable launches (sites per
+ * CTA of the descriptor forward and adjoint kernels; sparse-tile chunks per CTA of the fused GAP
+ * kernel), then times every candidate of each, one at a time, over `reps` evaluations with CUDA
+ * events, and keeps the fastest in the context. Later launches with the same shape key (kernel,
+ * precision, l_max, radial block, rows rounded up to a power of two; GAP: padded dimension,
+ * row and sparse tile counts) use it; MD and MC objects capture their graphs with the tuned
+ * shapes, so tune before creating them. The caller's stage timers are left as they were. */
+int tgap_autotune(tgap_context *ctx, tgap_system *system, int n_models, tgap_model *const *models,
+                  int precision, int reps);
+/* The last tuning as text, one line per key: key, chosen value, its time, the default and its
+ * time. `needed` gets the size with the terminating NUL; TGAP_ERR_CAPACITY when cap is short. */
+int tgap_autotune_report(tgap_context *ctx, char *buf, int64_t cap, int64_t *needed);
+/* Forgets every tuned choice (launches go back to the built-in heuristics). */
+int tgap_autotune_clear(tgap_context *ctx);
+
 /* calculate_gap_soap (src/gap/calculate_gap_soap.f90:171-481) with HOST buffers: copies
  * `positions` (3 x n_atoms, NULL = keep the resident ones) to the device, rebuilds the
  * neighbor list when rebuild != 0 (else refreshes geometry), evaluates all models and copies

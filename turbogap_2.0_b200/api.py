@@ -268,6 +268,19 @@ class System:
                                        C.c_void_p(d_energies), C.c_void_p(d_forces) if d_forces else None,
                                        C.c_void_p(d_virial) if d_virial else None), self.ctx.h, "tgap_compute")
 
+    def autotune(self, models, precision, reps=5):
+        """Times the tunable launch shapes of this system's evaluation and keeps the fastest in the
+        context (tgap_autotune); returns the report lines."""
+        arr = (C.c_void_p * len(models))(*[m.h.value for m in models])
+        check(self.ctx._L.tgap_autotune(self.ctx.h, self.h, len(models), arr, int(precision), int(reps)),
+              self.ctx.h, "tgap_autotune")
+        need = C.c_int64(0)
+        check(self.ctx._L.tgap_autotune_report(self.ctx.h, None, 0, C.byref(need)), self.ctx.h, "autotune report")
+        buf = C.create_string_buffer(max(1, need.value))
+        check(self.ctx._L.tgap_autotune_report(self.ctx.h, buf, need.value, C.byref(need)), self.ctx.h,
+              "autotune report")
+        return [line for line in buf.value.decode().splitlines() if line]
+
     def close(self):
         if getattr(self, "h", None):
             self.ctx._L.tgap_system_destroy(self.h)

@@ -89,6 +89,15 @@ int set_error(tgap_context *ctx, int status, const char *fmt, ...)
     return status;
 }
 
+int tuned(tgap_context *ctx, const std::string &key, const char *stage, const std::vector<int> &candidates, int dflt)
+{
+    if (!ctx) return dflt;
+    if (!ctx->probe_key.empty() && key == ctx->probe_key) return ctx->probe_val;
+    if (!ctx->tune_seen.count(key)) ctx->tune_seen[key] = tgap_context::TuneSlot{stage, candidates, dflt};
+    const auto it = ctx->tune.find(key);
+    return it != ctx->tune.end() ? it->second : dflt;
+}
+
 int cuda_check(tgap_context *ctx, cudaError_t e, const char *what)
 {
     return set_error(ctx, e == cudaErrorMemoryAllocation ? TGAP_ERR_NOMEM : TGAP_ERR_CUDA,
@@ -889,6 +898,104 @@ extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tga
     }
     for (int i = 0; i < n_models; ++i)
         CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial));
+    return TGAP_OK;
+}
+
+// ============================================================================ autotuner
+
+// Mean time of `stage` over the last timed runs (ms), or -1 when it did not run.
+static double stage_mean_ms(tgap_context *ctx, const std::string &stage)
+{
+    timing_collect(ctx);
+    for (size_t i = 0; i < ctx->stage_names.size(); ++i)
+        if (ctx->stage_names[i] == stage && ctx->stage_count[i] > 0) return ctx->stage_ms[i] / ctx->stage_count[i];
+    return -1.0;
+}
+
+extern "C" int tgap_autotune(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                             int precision, int reps)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || n_models <= 0 || !models || reps < 1) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_autotune: bad arguments");
+    const int N = s->nb.n_atoms;
+    DevBuf out;
+    std::unique_ptr<DevBuf, void (*)(DevBuf *)> guard(&out, [](DevBuf *b) { b->release(); });
+    if (out.ensure(sizeof(double) * (4 * (size_t)N + 9 * (size_t)s->nb.n_structures)))
+        return set_error(ctx, TGAP_ERR_NOMEM, "autotuner outputs");
+    double *d_e = out.as<double>(), *d_f = d_e + N, *d_v = d_f + 3 * (size_t)N;
+    auto run = [&]() { return tgap_compute(ctx, s, n_models, models, precision, 1, d_e, d_f, d_v); };
+    const bool timing0 = ctx->timing;
+    timing_collect(ctx);
+    const std::vector<double> ms0 = ctx->stage_ms;
+    const std::vector<int64_t> cnt0 = ctx->stage_count;
+    // discovery: the launches of this evaluation register their keys
+    ctx->probe_key.clear();
+    ctx->tune_seen.clear();
+    int rc = run();
+    const auto seen = ctx->tune_seen;
+    std::string report;
+    for (const auto &kv : seen) {
+        if (rc) break;
+        const std::string &key = kv.first;
+        const tgap_context::TuneSlot &slot = kv.second;
+        int best = slot.dflt;
+        double best_ms = -1.0, dflt_ms = -1.0;
+        for (int cand : slot.candidates) {
+            ctx->probe_key = key;
+            ctx->probe_val = cand;
+            ctx->timing = false;
+            if ((rc = run())) break;  // warm-up (first launch of a variant sets its attributes)
+            timing_collect(ctx);
+            for (auto &v : ctx->stage_ms) v = 0.0;
+            for (auto &c : ctx->stage_count) c = 0;
+            ctx->timing = true;
+            for (int r = 0; r < reps && !rc; ++r) rc = run();
+            ctx->timing = false;
+            if (rc) break;
+            const double ms = stage_mean_ms(ctx, slot.stage);
+            if (cand == slot.dflt) dflt_ms = ms;
+            if (ms >= 0.0 && (best_ms < 0.0 || ms < best_ms)) {
+                best_ms = ms;
+                best = cand;
+            }
+        }
+        ctx->probe_key.clear();
+        if (rc) break;
+        ctx->tune[key] = best;
+        char line[256];
+        std::snprintf(line, sizeof(line), "%s %d %.2f us (default %d: %.2f us)\n", key.c_str(), best, 1e3 * best_ms,
+                      slot.dflt, 1e3 * dflt_ms);
+        report += line;
+    }
+    ctx->probe_key.clear();
+    // the caller's stage timers as they were
+    timing_collect(ctx);
+    for (size_t i = 0; i < ctx->stage_ms.size(); ++i) {
+        ctx->stage_ms[i] = i < ms0.size() ? ms0[i] : 0.0;
+        ctx->stage_count[i] = i < cnt0.size() ? cnt0[i] : 0;
+    }
+    ctx->timing = timing0;
+    if (rc) return rc;
+    ctx->tune_report = report;
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return read_device_check(ctx);
+}
+
+extern "C" int tgap_autotune_report(tgap_context *ctx, char *buf, int64_t cap, int64_t *needed)
+{
+    if (!ctx) return TGAP_ERR_ARGUMENT;
+    const int64_t n = (int64_t)ctx->tune_report.size() + 1;
+    if (needed) *needed = n;
+    if (!buf || cap < n) return buf ? TGAP_ERR_CAPACITY : TGAP_OK;
+    std::memcpy(buf, ctx->tune_report.c_str(), (size_t)n);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_autotune_clear(tgap_context *ctx)
+{
+    if (!ctx) return TGAP_ERR_ARGUMENT;
+    ctx->tune.clear();
+    ctx->tune_report.clear();
     return TGAP_OK;
 }
 

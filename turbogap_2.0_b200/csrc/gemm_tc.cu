@@ -897,7 +897,12 @@ static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bflo
         TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
     }
     const int J = m.m_pad / BS, n_rt = rows_pad / kBM;
-    const int nc = flash_chunks(n_rt, J, sm_count(ctx));
+    std::vector<int> divisors;
+    for (int d = 1; d <= J; ++d)
+        if (J % d == 0) divisors.push_back(d);
+    char key[96];
+    std::snprintf(key, sizeof(key), "gap_fused/dp%d/bs%d/row_tiles%d/sparse_tiles%d", DP, BS, n_rt, J);
+    const int nc = tuned(ctx, key, "gemm_bf16x3_fused", divisors, flash_chunks(n_rt, J, sm_count(ctx)));
     StageScope sc(ctx, "gemm_bf16x3_fused");
     kern<<<n_rt * nc, kFlashThreads, Sh::SMEM, ctx->stream>>>(tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc,
                                                              p, ctx->d_flag);

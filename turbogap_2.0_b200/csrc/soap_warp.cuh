@@ -745,6 +745,25 @@ template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
 
+// Autotuner key of a descriptor launch (sites per CTA): kernel, precision, l_max, radial block,
+// bf16 split, and the row count rounded up to a power of two.
+inline std::string warps_key(const char *kind, bool f64, int L, int amb, bool split, int n_rows)
+{
+    int b = 1;
+    while (b < n_rows) b <<= 1;
+    char k[96];
+    std::snprintf(k, sizeof(k), "soap_%s/%s/l%d/a%d/s%d/rows%d", kind, f64 ? "f64" : "f32", L, amb, (int)split, b);
+    return k;
+}
+
+inline std::vector<int> warp_candidates(int nw_max)
+{
+    std::vector<int> c;
+    for (int v = 1; v <= nw_max; v *= 2) c.push_back(v);
+    if (c.back() != nw_max) c.push_back(nw_max);
+    return c;
+}
+
 template <class T> inline const T *soap_tab(const DevBuf &d64, const DevBuf &d32)
 {
     return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
@@ -756,8 +775,11 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 {
     constexpr int NLM = (L + 1) * (L + 1);
     const size_t wb = fwd_warp_bytes(ds.p, sizeof(T), AStride<NLM>::value, AMB);
-    const int nw = (int)std::min<size_t>(kWarpsPerCta, kMaxDynSmem / wb);
-    if (nw < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", wb);
+    const int nw_max = (int)std::min<size_t>(kWarpsPerCta, kMaxDynSmem / wb);
+    if (nw_max < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", wb);
+    const bool f64 = std::is_same<T, double>::value;
+    const int nw = tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows), f64 ? "soap_forward_f64" : "soap_forward_f32",
+                         warp_candidates(nw_max), nw_max);
     const size_t sm = wb * nw;
     auto kern = k_soap_fwd_warp<T, L, AMB, SPLIT>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -777,8 +799,11 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 {
     const size_t wb = bwd_warp_bytes<T>(ds.p, AMB);
     const size_t tail = kWarpsPerCta * (6 * sizeof(double) + sizeof(int));
-    const int nw = (int)std::min<size_t>(kWarpsPerCta, (kMaxDynSmem - tail) / wb);
-    if (nw < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", wb);
+    const int nw_max = (int)std::min<size_t>(kWarpsPerCta, (kMaxDynSmem - tail) / wb);
+    if (nw_max < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", wb);
+    const bool f64 = std::is_same<T, double>::value;
+    const int nw = tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows), f64 ? "soap_backward_f64" : "soap_backward_f32",
+                         warp_candidates(nw_max), nw_max);
     const size_t sm = wb * nw + tail;
     auto kern = k_soap_bwd_warp<T, GT, L, AMB>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));

@@ -6,6 +6,7 @@
 
 #include <atomic>
 #include <cstdio>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -76,6 +77,19 @@ struct tgap_context {
     std::vector<int64_t> stage_count;
     std::vector<tgap::StageRecord> pending;
     std::vector<cudaEvent_t> event_pool;
+    // autotuned launch choices (tgap_autotune): key -> value. Launchers register their key, the
+    // stage that times it and the candidate values on first use; while tuning, probe_key's value
+    // is forced to probe_val.
+    struct TuneSlot {
+        std::string stage;
+        std::vector<int> candidates;
+        int dflt = 0;
+    };
+    std::map<std::string, int> tune;
+    std::map<std::string, TuneSlot> tune_seen;
+    std::string probe_key;
+    int probe_val = 0;
+    std::string tune_report;
 };
 
 namespace tgap {
@@ -92,6 +106,11 @@ class StageScope {
 };
 
 int set_error(tgap_context *ctx, int status, const char *fmt, ...);
+
+// Launch choice for `key`: the probed value while the autotuner times it, else the tuned value,
+// else dflt. Registers the key with its timing stage and candidates (the first candidate list
+// seen for a key is kept).
+int tuned(tgap_context *ctx, const std::string &key, const char *stage, const std::vector<int> &candidates, int dflt);
 int cuda_check(tgap_context *ctx, cudaError_t e, const char *what);
 
 #define TGAP_CUDA(ctx, call)                                           \
