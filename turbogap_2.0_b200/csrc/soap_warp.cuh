@@ -255,6 +255,49 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T v[N])
     }
 }
 
+// acc[n] += x[n] a for n < N. FP32 rows use the packed two-lane FMA of sm_100 (FFMA2: two
+// independent FMAs per instruction, each rounded as a scalar fmaf, so results are unchanged).
+template <class T, int N>
+__device__ __forceinline__ void axpy_row(T acc[N], const T x[N], T a)
+{
+    if constexpr (std::is_same<T, float>::value && N % 2 == 0) {
+        const float2 a2 = make_float2(a, a);
+#pragma unroll
+        for (int n = 0; n < N; n += 2) {
+            const float2 r = __ffma2_rn(make_float2(x[n], x[n + 1]), a2, make_float2(acc[n], acc[n + 1]));
+            acc[n] = r.x;
+            acc[n + 1] = r.y;
+        }
+    } else {
+#pragma unroll
+        for (int n = 0; n < N; ++n) acc[n] += x[n] * a;
+    }
+}
+
+// Even and odd partial sums of x . y (s0 over even indices, s1 over odd, each in index order);
+// FP32 with the packed two-lane FMA.
+template <class T, int N>
+__device__ __forceinline__ void dot_even_odd(const T x[N], const T y[N], T &s0, T &s1)
+{
+    static_assert(N % 2 == 0, "even length");
+    if constexpr (std::is_same<T, float>::value) {
+        float2 acc = make_float2(0.0f, 0.0f);
+#pragma unroll
+        for (int e = 0; e < N; e += 2) acc = __ffma2_rn(make_float2(x[e], x[e + 1]), make_float2(y[e], y[e + 1]), acc);
+        s0 = acc.x;
+        s1 = acc.y;
+    } else {
+        T a0 = 0, a1 = 0;
+#pragma unroll
+        for (int e = 0; e < N; e += 2) {
+            a0 += x[e] * y[e];
+            a1 += x[e + 1] * y[e + 1];
+        }
+        s0 = a0;
+        s1 = a1;
+    }
+}
+
 // Adjoint of one pair's angular-radial product, summed over every real harmonic:
 //   w = u (A1 - u.Gam) + Gam,  A1 = sum_lm Y_lm (f_l V_lm + df_l U_lm),
 //   Gam = (1/r) sum_lm f_l U_lm dY_lm/du,   U_lm = Gc[lm].R, V_lm = Gc[lm].R'
@@ -291,14 +334,9 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
             dQ1 = dQ;
             T g[AMB];
             load_vec<T, AMB>(Gs + l * l * AMB, g);
-            T U0 = 0, U1 = 0, V0 = 0, V1 = 0;
-#pragma unroll
-            for (int e = 0; e < AMB; e += 2) {
-                U0 += g[e] * R[e];
-                V0 += g[e] * dR[e];
-                U1 += g[e + 1] * R[e + 1];
-                V1 += g[e + 1] * dR[e + 1];
-            }
+            T U0, U1, V0, V1;
+            dot_even_odd<T, AMB>(g, R, U0, U1);
+            dot_even_odd<T, AMB>(g, dR, V0, V1);
             const T U = U0 + U1, V = V0 + V1;
             const T f = fl[l * 32], df = dfl[l * 32];
             const T N = yc_norm<T>(Yc, l * (l + 1) / 2);
@@ -340,18 +378,11 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
             const T *row = Gs + (l * l + 2 * m - 1) * AMB;
             load_vec<T, AMB>(row, gc);
             load_vec<T, AMB>(row + AMB, gs);
-            T Uc0 = 0, Uc1 = 0, Vc0 = 0, Vc1 = 0, Us0 = 0, Us1 = 0, Vs0 = 0, Vs1 = 0;
-#pragma unroll
-            for (int e = 0; e < AMB; e += 2) {
-                Uc0 += gc[e] * R[e];
-                Vc0 += gc[e] * dR[e];
-                Us0 += gs[e] * R[e];
-                Vs0 += gs[e] * dR[e];
-                Uc1 += gc[e + 1] * R[e + 1];
-                Vc1 += gc[e + 1] * dR[e + 1];
-                Us1 += gs[e + 1] * R[e + 1];
-                Vs1 += gs[e + 1] * dR[e + 1];
-            }
+            T Uc0, Uc1, Vc0, Vc1, Us0, Us1, Vs0, Vs1;
+            dot_even_odd<T, AMB>(gc, R, Uc0, Uc1);
+            dot_even_odd<T, AMB>(gc, dR, Vc0, Vc1);
+            dot_even_odd<T, AMB>(gs, R, Us0, Us1);
+            dot_even_odd<T, AMB>(gs, dR, Vs0, Vs1);
             const T Uc = Uc0 + Uc1, Vc = Vc0 + Vc1, Us = Us0 + Us1, Vs = Vs0 + Vs1;
             const T f = fl[l * 32], df = dfl[l * 32];
             const T ac = f * Vc + df * Uc, as = f * Vs + df * Us;
@@ -447,11 +478,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
 #pragma unroll
                 for (int j = 0; j < KPL; ++j) {
                     const int kk = lane + 32 * j;
-                    if (kk < NLM) {
-                        const T a = As[p * ASTR + kk];
-#pragma unroll
-                        for (int n = 0; n < AMB; ++n) acc[j][n] += rv[n] * a;
-                    }
+                    if (kk < NLM) axpy_row<T, AMB>(acc[j], rv, As[p * ASTR + kk]);
                 }
             }
             __syncwarp();
