@@ -36,8 +36,11 @@ MC_ATOMS, MC_DENSITY, MC_T, MC_RADIUS, MC_SKIN = 1000, 2.0, 2000.0, 0.2, 0.5
 MC_PROPOSALS = 20000
 MC_WORKLOAD = ("NVT Metropolis MC, 1000 C atoms, 2.0 g/cm3, 2000 K, single-atom moves uniform in a 0.2 A ball, "
                "local SOAP/GAP update of atoms within rcut of the moved atom, same SOAP settings and 2000-sparse "
-               "GAP as the MD workload; 'screened': delayed acceptance with a PCA-64 / 128 / 128 SiLU bf16 screen "
-               "trained on 200k atomic energies of 2000 plain-MC snapshots")
+               "GAP as the MD workload; plain GAP MC evaluates 12 (mixed) or 4 (FP64) consecutive proposals side by "
+               "side and settles them in order (speculative batch: the same chain as one at a time); 'screened': "
+               "delayed acceptance "
+               "with a PCA-64 / 128 / 128 SiLU bf16 screen trained on 200k atomic energies of 2000 plain-MC "
+               "snapshots, proposals one at a time")
 DT = 1.0
 REBUILD = 10
 SKIN = 0.3
@@ -399,8 +402,10 @@ def _mc_leg(tg, torch, ctx, stream, model, n_prop, seed):
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
         st1 = mc.state()
+        bs = mc.batch_stats()
         out[name] = dict(moves_per_s=n_prop / (ms * 1e-3), us_per_move=1e3 * ms / n_prop,
-                         acceptance=r["accepted"] / n_prop, list_rebuilds=st1["rebuilds"] - st0["rebuilds"])
+                         acceptance=r["accepted"] / n_prop, list_rebuilds=st1["rebuilds"] - st0["rebuilds"],
+                         proposals_per_speculative_batch=round(bs["settled"] / max(1, bs["batches"]), 3))
         if name == "mixed":
             final = st1
         mc.close()

@@ -311,6 +311,17 @@ int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char 
  * life (or until tgap_mc_set_screen installs one again). Proposals still take deviate pairs; plain
  * moves use the first. Defaults: 2048, 0.1, 0.002. */
 int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass);
+/* Speculative batch of plain GAP MC (no counterpart in the reference, which judges proposals one
+ * at a time): `slots` consecutive proposals (1..16; default 12 mixed, 4 FP64) are evaluated side by side from
+ * the same state and then settled in order on the device. A proposal's energy change depends
+ * only on atoms within twice the model cutoff of its atom, so it stays valid unless an accepted
+ * earlier proposal of the batch moved an atom within 2 rc + |d_i| + |d_k| of it (minimum image;
+ * in a cell replicated into a supercell, any two proposals of the structure); the batch stops
+ * at the first one that is not valid, and that proposal opens the next batch. Decisions and
+ * final positions are those of one-at-a-time evaluation. Used whenever no screen is active. */
+int tgap_mc_set_batch(tgap_mc *mc, int slots);
+/* Batches run since creation and the proposals they settled. */
+int tgap_mc_batch_stats(tgap_mc *mc, int64_t *batches, int64_t *settled);
 /* Screen counters since creation (any pointer may be NULL): whether the screen is in use,
  * proposals it judged, passed to the exact stage, confirmed there, and fallbacks taken. */
 int tgap_mc_screen_stats(tgap_mc *mc, int *active, int64_t *judged, int64_t *passed,

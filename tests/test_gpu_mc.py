@@ -292,3 +292,32 @@ def test_mc_rejects_moves_beyond_the_skin(ctx, tg, synth, carbon):
     assert r["accepted"] in (0, 1)
     mc.close()
     system.close()
+
+
+def test_mc_speculative_batch_matches_one_at_a_time(ctx, tg, synth, carbon):
+    """Batches of 1, 5 and 16 proposals give the same decisions, the same dE (FP64, bitwise: a
+    row's energy does not depend on the rows beside it) and the same final positions; on a box
+    several cutoffs wide a batch settles more than one proposal on average."""
+    hyp, m = carbon
+    pos, box, sp, _ = synth.random_packing(1000, 2.0, 1.2, seed=60)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    atoms, disp, u = synth.mc_proposals(len(pos), 300, 0.2, seed=61)
+    runs = {}
+    for B in (1, 5, 16):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.5)
+        mc = tg.MC(ctx, system, [model], 2000.0, precision=tg.TGAP_FP64)
+        mc.set_batch(B)
+        out = mc.run(atoms, disp, u)
+        runs[B] = (out, mc.state(), mc.batch_stats())
+        mc.close()
+        system.close()
+    ref_out, ref_st, ref_bs = runs[1]
+    assert ref_bs["settled"] == 300 and ref_bs["batches"] >= 300
+    for B in (5, 16):
+        out, st, bs = runs[B]
+        assert np.array_equal(out["accept"], ref_out["accept"]), B
+        assert np.array_equal(out["de"], ref_out["de"]), B
+        assert np.array_equal(st["positions"], ref_st["positions"]), B
+        assert st["accepted"] == ref_st["accepted"]
+        assert bs["settled"] == 300
+        assert bs["batches"] < 0.75 * 300, (B, bs)

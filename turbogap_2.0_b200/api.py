@@ -216,7 +216,10 @@ class Model:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx._L.tgap_model_destroy(self.h)
+            # a handle whose context was closed first cannot be destroyed (its destroy would use
+            # the freed context); its device memory goes with the process
+            if getattr(self.ctx, "h", None):
+                self.ctx._L.tgap_model_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -283,7 +286,10 @@ class System:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx._L.tgap_system_destroy(self.h)
+            # a handle whose context was closed first cannot be destroyed (its destroy would use
+            # the freed context); its device memory goes with the process
+            if getattr(self.ctx, "h", None):
+                self.ctx._L.tgap_system_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -324,7 +330,10 @@ class MD:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx._L.tgap_md_destroy(self.h)
+            # a handle whose context was closed first cannot be destroyed (its destroy would use
+            # the freed context); its device memory goes with the process
+            if getattr(self.ctx, "h", None):
+                self.ctx._L.tgap_md_destroy(self.h)
             self.h = None
 
     def __del__(self):
@@ -375,6 +384,15 @@ class MC:
         check(self.ctx._L.tgap_mc_screen_fallback(self.h, int(window), float(min_confirm), float(min_pass)),
               self.ctx.h, "tgap_mc_screen_fallback")
 
+    def set_batch(self, slots):
+        """Proposals evaluated side by side by the speculative batch of plain GAP MC (1..16)."""
+        check(self.ctx._L.tgap_mc_set_batch(self.h, int(slots)), self.ctx.h, "tgap_mc_set_batch")
+
+    def batch_stats(self):
+        b, n = C.c_int64(), C.c_int64()
+        check(self.ctx._L.tgap_mc_batch_stats(self.h, C.byref(b), C.byref(n)), self.ctx.h, "tgap_mc_batch_stats")
+        return dict(batches=b.value, settled=n.value)
+
     def screen_stats(self):
         active = C.c_int()
         v = [C.c_int64() for _ in range(4)]
@@ -409,7 +427,10 @@ class MC:
 
     def close(self):
         if getattr(self, "h", None):
-            self.ctx._L.tgap_mc_destroy(self.h)
+            # a handle whose context was closed first cannot be destroyed (its destroy would use
+            # the freed context); its device memory goes with the process
+            if getattr(self.ctx, "h", None):
+                self.ctx._L.tgap_mc_destroy(self.h)
             self.h = None
 
     def __del__(self):

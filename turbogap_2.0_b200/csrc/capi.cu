@@ -1347,6 +1347,7 @@ struct tgap_mc {
     int precision, use_graph;
     double temperature, rc_sel, skin;
     int cap = 0, pmax = 0;
+    int batch = 8, sized_batch = 0;  // speculative batch slots (plain GAP MC); slots the buffers hold
     int64_t rebuilds = 0;
     McModelSel sel{};
     DevBuf st, ecache, dacc, mark, sites, tstart, txyz, trjs, tnsp, etrial;
@@ -1370,7 +1371,8 @@ struct tgap_mc {
     int64_t last_n = 0;
 };
 
-constexpr int kMcBatch = 32;  // proposals per graph launch
+constexpr int kMcBatch = 32;       // proposals per graph launch, one at a time (screened)
+constexpr int kMcBatchSteps = 12;  // speculative batches per graph launch (plain GAP MC)
 
 // Trial buffers for the current lists: pmax = longest list, cap = most sites one move can touch.
 static int mc_size_trial(tgap_mc *mc)
@@ -1383,23 +1385,27 @@ static int mc_size_trial(tgap_mc *mc)
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     int pmax = 1;
     for (int v : nn) pmax = std::max(pmax, v);
-    if (pmax <= mc->pmax && mc->cap > 0) return TGAP_OK;
-    mc->pmax = (pmax + 7) / 8 * 8 + 8;  // room for a few more pairs before resizing
-    mc->cap = (mc->pmax + 1 + 31) / 32 * 32;
+    if (pmax <= mc->pmax && mc->cap > 0 && mc->batch <= mc->sized_batch) return TGAP_OK;
+    if (pmax > mc->pmax || mc->cap == 0) {
+        mc->pmax = (pmax + 7) / 8 * 8 + 8;  // room for a few more pairs before resizing
+        mc->cap = (mc->pmax + 1 + 31) / 32 * 32;
+    }
+    mc->sized_batch = std::max(mc->batch, 1);
     const int M = (int)mc->models.size(), cap = mc->cap, pm = mc->pmax;
-    const int rows_pad = (cap + 127) / 128 * 128;
-    std::vector<int64_t> ts(cap + 1);
-    for (int r = 0; r <= cap; ++r) ts[r] = (int64_t)r * pm;
-    const size_t slots = (size_t)M * cap * pm;
-    if (mc->sites.ensure(sizeof(int) * (size_t)M * cap) || mc->tstart.ensure(sizeof(int64_t) * (cap + 1)) ||
+    const int rows = mc->sized_batch * cap;  // trial rows per model: slots x cap
+    const int rows_pad = (rows + 127) / 128 * 128;
+    std::vector<int64_t> ts(rows + 1);
+    for (int r = 0; r <= rows; ++r) ts[r] = (int64_t)r * pm;
+    const size_t slots = (size_t)M * rows * pm;
+    if (mc->sites.ensure(sizeof(int) * (size_t)M * rows) || mc->tstart.ensure(sizeof(int64_t) * (rows + 1)) ||
         mc->txyz.ensure(sizeof(double) * 3 * slots) || mc->trjs.ensure(sizeof(double) * slots) ||
-        mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * cap) ||
+        mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * rows) ||
         mc->es_trial.ensure(sizeof(float) * cap))
         return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->tnsp.ptr, 0, sizeof(int) * slots, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->trjs.ptr, 0, sizeof(double) * slots, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->txyz.ptr, 0, sizeof(double) * 3 * slots, ctx->stream));
-    TGAP_CUDA(ctx, cudaMemsetAsync(mc->sites.ptr, 0, sizeof(int) * (size_t)M * cap, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->sites.ptr, 0, sizeof(int) * (size_t)M * rows, ctx->stream));
     CHECK_RC(upload(ctx, mc->tstart, ts.data(), ts.size()));
     for (int m = 0; m < M; ++m) {
         const tgap_model *md = mc->models[m];
@@ -1407,8 +1413,8 @@ static int mc_size_trial(tgap_mc *mc)
         const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
         const size_t tsz = mc->precision == TGAP_FP64 ? 8 : 4;
         const int q_ld = mc->precision == TGAP_FP64 ? md->gap.dim : md->gap.dim_pad;
-        if (mc->c[m].ensure(tsz * cap * P.n_max * nlm) || mc->q[m].ensure(tsz * (size_t)rows_pad * q_ld) ||
-            mc->norm[m].ensure(tsz * cap))
+        if (mc->c[m].ensure(tsz * rows * P.n_max * nlm) || mc->q[m].ensure(tsz * (size_t)rows_pad * q_ld) ||
+            mc->norm[m].ensure(tsz * rows))
             return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
         if (mc->precision != TGAP_FP64) {
             if (mc->q_hi[m].ensure(2 * (size_t)rows_pad * q_ld) || mc->q_lo[m].ensure(2 * (size_t)rows_pad * q_ld))
@@ -1480,6 +1486,48 @@ static int mc_step_body(tgap_mc *mc)
                      mc->es_cache.as<float>());
 }
 
+// One speculative batch of plain GAP MC (mc_select_batch): select, trial geometry, descriptor rows
+// and GAP energies of every slot per model, then the in-order settlement.
+static int mc_step_body_batch(tgap_mc *mc)
+{
+    tgap_context *ctx = mc->ctx;
+    NeighborBatch &nb = mc->sys->nb;
+    const int M = (int)mc->models.size(), cap = mc->cap, pm = mc->pmax, B = mc->batch, rows = B * cap;
+    McDev *st = mc->st.as<McDev>();
+    CHECK_RC(mc_select_batch(ctx, st, nb, mc->sel, mc->rc_sel, mc->skin, mc->patom.as<int>(), mc->pdisp.as<double>(),
+                             mc->dacc.as<double>(), mc->mark.as<long long>(), mc->sites.as<int>(), cap, B));
+    CHECK_RC(mc_trial_geometry_batch(ctx, st, nb, M, mc->sites.as<int>(), cap, pm, B, mc->txyz.as<double>(),
+                                     mc->trjs.as<double>(), mc->tnsp.as<int>()));
+    for (int m = 0; m < M; ++m) {
+        const tgap_model *md = mc->models[m];
+        const size_t off = (size_t)m * rows * pm;
+        PairView pv{mc->tstart.as<int64_t>(), mc->txyz.as<double>() + 3 * off, mc->trjs.as<double>() + off,
+                    mc->tnsp.as<int>() + off, nullptr, 0, ctx->d_check};
+        SoapOut o;
+        o.c = mc->c[m].ptr;
+        o.q = mc->q[m].ptr;
+        o.norm = mc->norm[m].ptr;
+        double *e_rows = mc->etrial.as<double>() + (size_t)m * rows;
+        if (mc->precision == TGAP_FP64) {
+            o.q_ld = md->gap.dim;
+            CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, rows, TGAP_FP64, o));
+            CHECK_RC(gap_energy_grad_f64(ctx, md->gap, (const double *)o.q, o.q_ld, rows, 0.0, 0, &mc->gw[m], nullptr,
+                                         e_rows, nullptr));
+        } else {
+            o.q_ld = md->gap.dim_pad;
+            o.q_hi = mc->q_hi[m].as<__nv_bfloat16>();
+            o.q_lo = mc->q_lo[m].as<__nv_bfloat16>();
+            CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, rows, TGAP_MIXED, o));
+            CHECK_RC(gap_energy_grad_mixed(ctx, md->gap, o.q_hi, o.q_lo, rows, 0.0, 0, &mc->gw[m], nullptr, e_rows,
+                                           nullptr));
+        }
+    }
+    return mc_resolve_batch(ctx, st, nb, M, mc->sites.as<int>(), cap, B, mc->etrial.as<double>(),
+                            mc->ecache.as<double>(), nb.positions.as<double>(), mc->dacc.as<double>(),
+                            mc->pu.as<double>(), mc->screened ? 2 : 1, mc->temperature, mc->rc_sel, mc->skin,
+                            mc_logs(mc));
+}
+
 static void mc_drop_graph(tgap_mc *mc)
 {
     if (mc->exec) cudaGraphExecDestroy(mc->exec);
@@ -1546,6 +1594,9 @@ extern "C" int tgap_mc_create(tgap_context *ctx, tgap_system *sys, int n_models,
     mc->rc_sel = rc;
     mc->skin = sys->rcut - rc;
     mc->sel.n_models = n_models;
+    // speculative batch width: the FP32/bf16 rows are cheap enough that 12 side-by-side
+    // proposals cost little more than one; FP64 rows are not (measured on the 1000-atom MC box)
+    mc->batch = precision == TGAP_MIXED ? 12 : 4;
     for (int m = 0; m < n_models; ++m) {
         mc->sel.central_species[m] = models[m]->central_species;
         if (precision == TGAP_MIXED && !models[m]->mixed_ready)
@@ -1559,13 +1610,13 @@ extern "C" int tgap_mc_create(tgap_context *ctx, tgap_system *sys, int n_models,
     mc->gw.resize(n_models);
     const int N = sys->nb.n_atoms;
     if (mc->st.ensure(sizeof(McDev)) || mc->ecache.ensure(sizeof(double) * (size_t)n_models * N) ||
-        mc->dacc.ensure(sizeof(double) * N) || mc->mark.ensure(sizeof(long long) * N) ||
+        mc->dacc.ensure(sizeof(double) * N) || mc->mark.ensure(sizeof(long long) * (size_t)kMcMaxBatch * N) ||
         mc->hst.ensure(sizeof(McDev)))
         return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo state");
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->st.ptr, 0, sizeof(McDev), ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->ecache.ptr, 0, sizeof(double) * (size_t)n_models * N, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->dacc.ptr, 0, sizeof(double) * N, ctx->stream));
-    TGAP_CUDA(ctx, cudaMemsetAsync(mc->mark.ptr, 0, sizeof(long long) * N, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(mc->mark.ptr, 0, sizeof(long long) * (size_t)kMcMaxBatch * N, ctx->stream));
     // fresh lists at the current positions, then the cached site energies of every model
     CHECK_RC(tgap_system_update(sys, 1));
     for (int m = 0; m < n_models; ++m)
@@ -1666,7 +1717,10 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
                 TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
                 const int64_t launches = ctx->launches;
                 int rc = TGAP_OK;
-                for (int b = 0; b < kMcBatch && !rc; ++b) rc = mc_step_body(mc);
+                if (mc->screen_active)
+                    for (int b = 0; b < kMcBatch && !rc; ++b) rc = mc_step_body(mc);
+                else
+                    for (int b = 0; b < kMcBatchSteps && !rc; ++b) rc = mc_step_body_batch(mc);
                 cudaGraph_t g = nullptr;
                 cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
                 mc->graph_kernels = ctx->launches - launches;
@@ -1687,8 +1741,10 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
             }
             TGAP_CUDA(ctx, cudaGraphLaunch(mc->exec, ctx->stream));
             ctx->launches += mc->graph_kernels;
-        } else {
+        } else if (mc->screen_active) {
             for (int b = 0; b < kMcBatch; ++b) CHECK_RC(mc_step_body(mc));
+        } else {
+            for (int b = 0; b < kMcBatchSteps; ++b) CHECK_RC(mc_step_body_batch(mc));
         }
     }
     if (de_log) CHECK_RC(download(ctx, de_log, mc->log_de, (size_t)n));
@@ -1801,6 +1857,27 @@ extern "C" int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_c
     mc->fb_window = window;
     mc->fb_min_confirm = min_confirm;
     mc->fb_min_pass = min_pass;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_set_batch(tgap_mc *mc, int slots)
+{
+    if (!mc || slots < 1 || slots > kMcMaxBatch) return TGAP_ERR_ARGUMENT;
+    CHECK_RC(activate(mc->ctx));
+    mc->batch = slots;
+    CHECK_RC(mc_size_trial(mc));
+    mc_drop_graph(mc);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_mc_batch_stats(tgap_mc *mc, int64_t *batches, int64_t *settled)
+{
+    if (!mc) return TGAP_ERR_ARGUMENT;
+    CHECK_RC(activate(mc->ctx));
+    McDev h;
+    CHECK_RC(mc_read_state(mc, &h));
+    if (batches) *batches = h.batches;
+    if (settled) *settled = h.batch_resolved;
     return TGAP_OK;
 }
 

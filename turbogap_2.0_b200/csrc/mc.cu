@@ -292,6 +292,290 @@ __global__ void k_mc_lists_rebuilt(McDev *st, double *dacc, int n)
     }
 }
 
+// ----------------------------------------------------------------------------- speculative batch
+
+// Block b (one warp) selects the affected sites of proposal next + b from the state before the
+// batch; mark[b N + atom] holds the stamp of the last batch whose slot b took the atom.
+__global__ void k_mc_select_batch(McDev *st, const int64_t *__restrict__ start, const int *__restrict__ list,
+                                  const int *__restrict__ jatom, const int *__restrict__ site_struct,
+                                  const StructDesc *__restrict__ sd, const double *__restrict__ pos,
+                                  const int *__restrict__ species_sc, McModelSel sel, double rc_sel, double skin,
+                                  const int *__restrict__ prop_atom, const double *__restrict__ prop_disp,
+                                  const double *__restrict__ dacc, long long *mark, int n_atoms, int *sites, int cap,
+                                  int B, int *check)
+{
+    const int lane = threadIdx.x & 31, b = blockIdx.x;
+    __shared__ int s_flag;
+    if (lane == 0) {
+        int flag = 1;
+        if (st->status == kMcRunning) {
+            const long long k = st->next + b;
+            if (k < st->n_prop) {
+                const int a = prop_atom[k];
+                const double d0 = prop_disp[3 * k], d1 = prop_disp[3 * k + 1], d2 = prop_disp[3 * k + 2];
+                const double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
+                if (st->maxD + dacc[a] + dn >= skin) {
+                    flag = 2;
+                } else {
+                    flag = 0;
+                    st->slot_atom[b] = a;
+                    for (int q = 0; q < 3; ++q) st->slot_old[b][q] = pos[3 * (size_t)a + q];
+                    st->slot_new[b][0] = pos[3 * (size_t)a] + d0;
+                    st->slot_new[b][1] = pos[3 * (size_t)a + 1] + d1;
+                    st->slot_new[b][2] = pos[3 * (size_t)a + 2] + d2;
+                    st->slot_dn[b] = dn;
+                }
+            }
+        }
+        st->slot_flag[b] = flag;
+        if (flag != 0)
+            for (int m = 0; m < kMcMaxModels; ++m) st->slot_count[b][m] = 0;
+        s_flag = flag;
+    }
+    __syncwarp();
+    if (s_flag != 0) return;
+    const long long stamp = st->serial + 1;  // advanced by the resolve kernel after every batch
+    long long *mk = mark + (size_t)b * n_atoms;
+    const int a = st->slot_atom[b];
+    const double pn[3] = {st->slot_new[b][0], st->slot_new[b][1], st->slot_new[b][2]};
+    const StructDesc &S = sd[site_struct[a]];
+    const int ia = a - S.atom_off + 1;
+    double pa_old[3], pa_new[3];
+    sc_position(S, pos, ia, pa_old);
+    sc_position_moved(S, pos, ia, a, pn, pa_new);
+    int cnt[kMcMaxModels] = {0, 0, 0, 0};
+    auto species_of = [&](int g) { return species_sc[S.sc_off + (g - S.atom_off)]; };
+    if (lane == 0) mk[a] = stamp;
+    {
+        const int sa = species_of(a);
+        for (int m = 0; m < sel.n_models; ++m)
+            if (sel.central_species[m] == 0 || sel.central_species[m] == sa) {
+                if (lane == 0) sites[(m * B + b) * cap] = a;
+                cnt[m] = 1;
+            }
+    }
+    __syncwarp();
+    const int64_t kb = start[a], ke = start[a + 1];
+    for (int64_t k0 = kb + 1; k0 < ke; k0 += 32) {
+        const int64_t k = k0 + lane;
+        bool pick = false;
+        int g = -1;
+        if (k < ke) {
+            const int jsc = list[k];
+            g = jatom[k];
+            double pj_old[3], pj_new[3], dist[3], dd;
+            sc_position(S, pos, jsc, pj_old);
+            sc_position_moved(S, pos, jsc, a, pn, pj_new);
+            get_distance_dev(pa_old, pj_old, S, dist, &dd);
+            pick = dd < rc_sel;
+            get_distance_dev(pa_new, pj_new, S, dist, &dd);
+            pick = pick || dd < rc_sel;
+        }
+        const unsigned peers = __match_any_sync(0xffffffffu, pick ? g : -2 - lane);
+        const bool leader = pick && (__ffs(peers) - 1 == lane);
+        const bool fresh = leader && mk[g] != stamp;
+        __syncwarp();
+        if (fresh) mk[g] = stamp;
+        const int sg = fresh ? species_of(g) : 0;
+        for (int m = 0; m < sel.n_models; ++m) {
+            const bool in_m = fresh && (sel.central_species[m] == 0 || sel.central_species[m] == sg);
+            const unsigned mm = __ballot_sync(0xffffffffu, in_m);
+            if (in_m) {
+                const int slot = cnt[m] + __popc(mm & mc_lanemask_lt());
+                if (slot < cap)
+                    sites[(m * B + b) * cap + slot] = g;
+                else
+                    check_fail(check, kCheckMcOverflow, slot, g);
+            }
+            cnt[m] += __popc(mm);
+        }
+        __syncwarp();
+    }
+    if (lane == 0)
+        for (int m = 0; m < kMcMaxModels; ++m) st->slot_count[b][m] = m < sel.n_models ? min(cnt[m], cap) : 0;
+}
+
+// Warp per (model, slot, row): the row's pair geometry with its slot's atom at the trial position.
+__global__ void k_mc_trial_geometry_batch(const McDev *st, int n_models, const int *__restrict__ sites, int cap,
+                                          int pmax, int B, const int64_t *__restrict__ start,
+                                          const int *__restrict__ list, const int *__restrict__ nspecies,
+                                          const int *__restrict__ site_struct, const StructDesc *__restrict__ sd,
+                                          const double *__restrict__ pos, double *__restrict__ txyz,
+                                          double *__restrict__ trjs, int *__restrict__ tnsp, int *check)
+{
+    const int lane = threadIdx.x & 31;
+    const int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (w >= n_models * B * cap) return;
+    const int m = w / (B * cap), rem = w - m * B * cap, b = rem / cap, r = rem - b * cap;
+    const size_t base = (size_t)w * pmax;
+    int ns = 0, g = 0;
+    if (st->slot_flag[b] == 0 && r < st->slot_count[b][m]) {
+        g = sites[(m * B + b) * cap + r];
+        ns = (int)(start[g + 1] - start[g]);
+        if (ns > pmax) {
+            if (lane == 0) check_fail(check, kCheckMcOverflow, g, ns);
+            ns = pmax;
+        }
+    }
+    const int a = st->slot_atom[b];
+    const double pn[3] = {st->slot_new[b][0], st->slot_new[b][1], st->slot_new[b][2]};
+    for (int t = lane; t < pmax; t += 32) {
+        double x0 = 0.0, x1 = 0.0, x2 = 0.0, rr = 0.0;
+        int sp = 0;
+        if (t < ns) {
+            const int64_t k = start[g] + t;
+            sp = nspecies[k];
+            if (t > 0) {
+                const StructDesc &S = sd[site_struct[g]];
+                double pi[3], pj[3], dist[3];
+                sc_position_moved(S, pos, g - S.atom_off + 1, a, pn, pi);
+                sc_position_moved(S, pos, list[k], a, pn, pj);
+                get_distance_dev(pi, pj, S, dist, &rr);
+                x0 = dist[0];
+                x1 = dist[1];
+                x2 = dist[2];
+            }
+        }
+        txyz[3 * (base + t)] = x0;
+        txyz[3 * (base + t) + 1] = x1;
+        txyz[3 * (base + t) + 2] = x2;
+        trjs[base + t] = rr;
+        tnsp[base + t] = sp;
+    }
+}
+
+// One warp: settles the batch's proposals in order (see mc_select_batch for the validity rule).
+__global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restrict__ sites, int cap, int B,
+                                   const double *__restrict__ etrial, double *__restrict__ ecache, int n_atoms,
+                                   double *__restrict__ pos, double *__restrict__ dacc,
+                                   const double *__restrict__ prop_u, int u_stride, double temperature,
+                                   double rc_sel, double skin, const int *__restrict__ site_struct,
+                                   const StructDesc *__restrict__ sd, McLogs logs)
+{
+    const int lane = threadIdx.x & 31;
+    __shared__ int acc_slot[kMcMaxBatch];
+    if (st->status != kMcRunning) return;
+    long long k = st->next;
+    int n_acc = 0, settled = 0;
+    for (int b = 0; b < B; ++b) {
+        const int flag = st->slot_flag[b];
+        if (flag == 1) break;
+        if (flag == 2) {
+            if (lane == 0) st->status = kMcNeedRebuild;
+            break;
+        }
+        const int a = st->slot_atom[b];
+        const double dn = st->slot_dn[b];
+        // valid unless an accepted earlier slot moved an atom within 2 rc + |d_i| + |d_b|
+        bool conflict = false;
+        if (lane < n_acc) {
+            const int i = acc_slot[lane];
+            const int ai = st->slot_atom[i];
+            if (ai == a) {
+                conflict = true;
+            } else if (site_struct[ai] == site_struct[a]) {
+                const StructDesc &S = sd[site_struct[a]];
+                if (S.rep[0] * S.rep[1] * S.rep[2] > 1) {
+                    // a replicated cell moves every replica of the atom: its images repeat with the
+                    // primitive cell, which is smaller than twice the list cutoff
+                    conflict = true;
+                } else {
+                    double dist[3], dd;
+                    get_distance_dev(st->slot_old[i], st->slot_old[b], S, dist, &dd);
+                    conflict = !(dd >= 2.0 * rc_sel + st->slot_dn[i] + dn + 1e-9);
+                }
+            }
+        }
+        if (__any_sync(0xffffffffu, conflict)) break;
+        if (st->maxD + dacc[a] + dn >= skin) {
+            if (lane == 0) st->status = kMcNeedRebuild;
+            break;
+        }
+        // dE in the fixed order of the one-at-a-time kernel
+        double de = 0.0;
+        for (int m = 0; m < n_models; ++m) {
+            const int c = st->slot_count[b][m];
+            const int *sm = sites + (size_t)(m * B + b) * cap;
+            const double *em = etrial + (size_t)m * B * cap + (size_t)b * cap;
+            for (int r = lane; r < c; r += 32) de += em[r] - ecache[(size_t)m * n_atoms + sm[r]];
+        }
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
+        int accept = 0;
+        if (lane == 0) {
+            double p = exp(-de / (mc_kb() * temperature));
+            p = p < 1.0 ? p : 1.0;
+            accept = p > prop_u[(long long)u_stride * k] ? 1 : 0;
+            if (logs.de) logs.de[k] = de;
+            if (logs.acc) logs.acc[k] = (unsigned char)accept;
+            if (logs.stage) logs.stage[k] = 2;
+        }
+        accept = __shfl_sync(0xffffffffu, accept, 0);
+        if (accept) {
+            for (int m = 0; m < n_models; ++m) {
+                const int c = st->slot_count[b][m];
+                const int *sm = sites + (size_t)(m * B + b) * cap;
+                const double *em = etrial + (size_t)m * B * cap + (size_t)b * cap;
+                for (int r = lane; r < c; r += 32) ecache[(size_t)m * n_atoms + sm[r]] = em[r];
+            }
+            if (lane == 0) {
+                for (int q = 0; q < 3; ++q) pos[3 * (size_t)a + q] = st->slot_new[b][q];
+                dacc[a] += dn;
+                if (dacc[a] > st->maxD) st->maxD = dacc[a];
+                st->accepted += 1;
+                acc_slot[n_acc] = b;
+            }
+            ++n_acc;
+        }
+        __syncwarp();
+        ++k;
+        ++settled;
+    }
+    if (lane == 0) {
+        st->next = k;
+        st->serial += 1;
+        st->batches += 1;
+        st->batch_resolved += settled;
+    }
+}
+
+int mc_select_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McModelSel &sel, double rc_sel,
+                    double skin, const int *d_prop_atom, const double *d_prop_disp, const double *d_dacc,
+                    long long *d_mark, int *d_sites, int cap, int B)
+{
+    k_mc_select_batch<<<B, 32, 0, ctx->stream>>>(d_st, nb.start.as<int64_t>(), nb.list.as<int>(), nb.jatom.as<int>(),
+                                                 nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(),
+                                                 nb.positions.as<double>(), nb.species_sc.as<int>(), sel, rc_sel,
+                                                 skin, d_prop_atom, d_prop_disp, d_dacc, d_mark, nb.n_atoms, d_sites,
+                                                 cap, B, ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_trial_geometry_batch(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
+                            const int *d_sites, int cap, int pmax, int B, double *d_txyz, double *d_trjs, int *d_tnsp)
+{
+    const int warps = n_models * B * cap, T = 128;
+    k_mc_trial_geometry_batch<<<(warps + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+        d_st, n_models, d_sites, cap, pmax, B, nb.start.as<int64_t>(), nb.list.as<int>(), nb.nspecies.as<int>(),
+        nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(), nb.positions.as<double>(), d_txyz, d_trjs, d_tnsp,
+        ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int mc_resolve_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, int n_models, const int *d_sites,
+                     int cap, int B, const double *d_etrial, double *d_ecache, double *d_positions, double *d_dacc,
+                     const double *d_prop_u, int u_stride, double temperature, double rc_sel, double skin,
+                     McLogs logs)
+{
+    k_mc_resolve_batch<<<1, 32, 0, ctx->stream>>>(d_st, n_models, d_sites, cap, B, d_etrial, d_ecache, nb.n_atoms,
+                                                  d_positions, d_dacc, d_prop_u, u_stride, temperature, rc_sel, skin,
+                                                  nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(), logs);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
 int mc_select(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McModelSel &sel, double rc_sel,
               double skin, const int *d_prop_atom, const double *d_prop_disp, const double *d_dacc,
               long long *d_mark, int *d_sites, int cap)

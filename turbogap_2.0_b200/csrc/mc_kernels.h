@@ -13,6 +13,7 @@
 namespace tgap {
 
 constexpr int kMcMaxModels = 4;
+constexpr int kMcMaxBatch = 16;  // proposals evaluated side by side by the speculative batch
 
 // Device-resident driver state (one per MC object).
 struct McDev {
@@ -31,6 +32,13 @@ struct McDev {
     long long s_prop;    // proposals judged by the screen since creation (stage 1)
     long long s_pass;    // of those, passed on to the exact stage
     long long s_conf;    // of those, accepted by the exact stage
+    // speculative batch (plain GAP MC): slot b holds proposal next + b, evaluated from the state
+    // before the batch
+    int slot_flag[kMcMaxBatch];  // 0 evaluated, 1 no proposal left, 2 needs a list rebuild
+    int slot_atom[kMcMaxBatch];
+    double slot_old[kMcMaxBatch][3], slot_new[kMcMaxBatch][3], slot_dn[kMcMaxBatch];
+    int slot_count[kMcMaxBatch][kMcMaxModels];
+    long long batches, batch_resolved;  // batches run and proposals they settled
 };
 
 // Per-proposal logs (device arrays of the run's length, any may be null).
@@ -78,6 +86,24 @@ int mc_accept(tgap_context *ctx, McDev *d_st, int n_models, const int *d_sites, 
               double *d_ecache, int n_atoms, double *d_positions, double *d_dacc, const double *d_prop_u,
               double temperature, McLogs logs, int screened, int u_stride, const float *d_es_trial,
               float *d_es_cache);
+
+// Speculative batch of B consecutive proposals (plain GAP MC, same decisions as one at a time).
+// Proposal k's energy change depends only on atoms within 2 rc of its atom's old or new
+// position, so the proposals next .. next + B - 1 are evaluated side by side from the state
+// before the batch, then settled in order: each is valid unless an accepted earlier one of the
+// batch moved an atom within 2 rc + |d_i| + |d_k| of it (minimum image, same structure), and the
+// batch stops at the first invalid one (it is proposed again in the next batch), at the first
+// that needs a list rebuild, or when the run's proposals are exhausted. Layout: sites
+// [(m B + b) cap + r], trial rows of model m contiguous over (b, r), etrial [m][B cap].
+int mc_select_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, const McModelSel &sel, double rc_sel,
+                    double skin, const int *d_prop_atom, const double *d_prop_disp, const double *d_dacc,
+                    long long *d_mark, int *d_sites, int cap, int B);
+int mc_trial_geometry_batch(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
+                            const int *d_sites, int cap, int pmax, int B, double *d_txyz, double *d_trjs, int *d_tnsp);
+int mc_resolve_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, int n_models, const int *d_sites,
+                     int cap, int B, const double *d_etrial, double *d_ecache, double *d_positions, double *d_dacc,
+                     const double *d_prop_u, int u_stride, double temperature, double rc_sel, double skin,
+                     McLogs logs);
 
 // Start of a run of n proposals (keeps a pending rebuild request), and the reset after a list
 // rebuild.
