@@ -128,6 +128,18 @@ int tgap_get_soap_energy_and_forces(tgap_context *ctx, int n_soap, int n_sites, 
                                     int n_atom_pairs, int do_forces, int n_sites0,
                                     double *energies, double *forces, double *virial);
 
+/* local_property_predict (src/gap/local_properties.f90:46-147): a per-site property model (e.g.
+ * Hirshfeld volumes), V(i) = delta^2 sum_s alphas(s) K(i,s)^zeta + V0 clipped at 0, zeta taken as
+ * an integer when nint(zeta) is within 1e-10 (:76-77). With do_derivatives, V_der (3 x
+ * n_atom_pairs) = Qss(i,:) . soap_cart_der(:,:,j) for every pair j of site i, zero for a site whose
+ * V was clipped. soap (n_soap x n_sites), Qs (n_soap x n_sparse), soap_cart_der (3 x n_soap x
+ * n_atom_pairs) as get_soap gives them. FP64. */
+int tgap_local_property_predict(tgap_context *ctx, int n_soap, int n_sites, int n_sparse,
+                                const double *soap, const double *Qs, const double *alphas,
+                                double V0, double delta, double zeta, int do_derivatives,
+                                const double *soap_cart_der, const int *n_neigh, int n_atom_pairs,
+                                double *V, double *V_der);
+
 /* No counterpart in the reference. Per-site GAP energies delta^2 sum_s alpha_s (q_i.Q_s)^zeta
  * + e0 (the energy half of get_soap_energy_and_forces) for inputs that are already on the
  * device, without allocating any device memory.
@@ -223,6 +235,16 @@ int64_t tgap_system_n_pairs(const tgap_system *system);
 int tgap_compute(tgap_context *ctx, tgap_system *system, int n_models,
                  tgap_model *const *models, int precision, int do_forces, double *d_energies,
                  double *d_forces, double *d_virial);
+
+/* Resident form of local_property_predict (local_properties.f90:46-147, as get_gap_soap calls it,
+ * gap_interface.f90:314-364) for a property model held as a tgap_model (its delta, zeta, alphas
+ * and sparse set; the integer-zeta test of local_properties.f90): device pointers d_V (n_atoms;
+ * sites outside the model's centre species get 0) and, with do_derivatives, d_V_der (3 x the
+ * system's list pairs, list order): dV_i/dr_j for each pair, the self slot holding dV_i/dr_i,
+ * zero outside the model cutoff and for clipped sites. The descriptor derivatives are never
+ * materialised (the adjoint writes each pair's vector). Overwrites the outputs. */
+int tgap_local_property(tgap_context *ctx, tgap_system *system, tgap_model *model, double V0,
+                        int precision, int do_derivatives, double *d_V, double *d_V_der);
 
 /* Autotuner (no counterpart in the reference, which has no GPU launch shapes to choose). Runs
  * tgap_compute on this system and these models once to collect the tunable launches (sites per

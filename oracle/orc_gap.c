@@ -4,6 +4,7 @@
  * Restatement of the GAP prediction layer and of the dynamics arithmetic:
  *   get_soap_energy_and_forces   src/gap/gap.f90:39-244
  *   get_gap_soap                 src/gap/gap_interface.f90:41-433 (subset, renumber, scatter)
+ *   local_property_predict       src/gap/local_properties.f90:46-147
  *   velocity_verlet              src/md/md_utils.f90:486-532
  *   monte_carlo_move             src/mc/mc_utils.f90:172-180 (+ min(1,p) of :255)
  */
@@ -100,6 +101,62 @@ void orc_get_soap_energy_and_forces(int n_soap, int n_sites, int n_sparse, const
         }
     }
     free(Qss);
+    free(K);
+}
+
+void orc_local_property_predict(int n_soap, int n_sites, int n_sparse, const double *soap, const double *Qs,
+                                 const double *alphas, double V0, double delta, double zeta, int do_derivatives,
+                                 const double *soap_cart_der, const int *n_neigh, double *V, double *V_der)
+{
+    /* local_properties.f90:77: integer zeta when nint(zeta) is within 1e-10 (not gap.f90's 1e-5) */
+    const int zi = (int)lround(zeta);
+    const int is_int = fabs((double)zi - zeta) < 1.0e-10;
+    double *K = (double *)malloc(sizeof(double) * ((size_t)n_sites * (size_t)n_sparse + 1));
+    /* :73-76 K = soap^T Qs */
+#pragma omp parallel for schedule(static)
+    for (int i = 0; i < n_sites; ++i)
+        for (int s = 0; s < n_sparse; ++s) {
+            const double *a = soap + (size_t)i * n_soap, *b = Qs + (size_t)s * n_soap;
+            double acc = 0.0;
+            for (int d = 0; d < n_soap; ++d) acc += a[d] * b[d];
+            K[(size_t)i * n_sparse + s] = acc;
+        }
+    /* :110-122 V = delta^2 K^zeta alphas + V0, clipped at zero */
+    for (int i = 0; i < n_sites; ++i) {
+        double v = 0.0;
+        for (int s = 0; s < n_sparse; ++s) {
+            const double k = K[(size_t)i * n_sparse + s];
+            v += (is_int ? ipow(k, zi) : pow(k, zeta)) * alphas[s];
+        }
+        v = delta * delta * v + V0;
+        V[i] = v < 0.0 ? 0.0 : v;
+    }
+    if (do_derivatives) {
+        /* :82-107, :124-142 Qss = delta^2 (zeta K^(zeta-1) o alphas) Qs^T; V_der(:, j) = Qss(i, :) .
+         * soap_cart_der(:, :, j), zero for the pairs of a site whose V was clipped */
+        double *qs = (double *)malloc(sizeof(double) * (size_t)n_soap);
+        int64_t j = 0;
+        for (int i = 0; i < n_sites; ++i) {
+            for (int d = 0; d < n_soap; ++d) qs[d] = 0.0;
+            for (int s = 0; s < n_sparse; ++s) {
+                const double k = K[(size_t)i * n_sparse + s];
+                const double kd = (is_int ? (double)zi * ipow(k, zi - 1) : zeta * pow(k, zeta - 1.0)) * alphas[s];
+                const double w = delta * delta * kd;
+                const double *b = Qs + (size_t)s * n_soap;
+                for (int d = 0; d < n_soap; ++d) qs[d] += w * b[d];
+            }
+            for (int n = 0; n < n_neigh[i]; ++n, ++j)
+                for (int c = 0; c < 3; ++c) {
+                    double acc = 0.0;
+                    if (V[i] != 0.0) {
+                        const double *der = soap_cart_der + (size_t)j * n_soap * 3;
+                        for (int d = 0; d < n_soap; ++d) acc += qs[d] * der[3 * d + c];
+                    }
+                    V_der[3 * j + c] = acc;
+                }
+        }
+        free(qs);
+    }
     free(K);
 }
 

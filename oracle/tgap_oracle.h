@@ -124,6 +124,12 @@ void orc_get_soap_energy_and_forces(int n_soap, int n_sites, int n_sparse, const
                                     const double *xyz, int do_forces, int n_sites0,
                                     double *energies, double *forces, double *virial);
 
+/* local_property_predict (local_properties.f90:46-147): V (n_sites) = delta^2 K^zeta alphas + V0
+ * clipped at zero; with do_derivatives, V_der (3 x n_pairs) = Qss(i,:) . soap_cart_der(:,:,j). */
+void orc_local_property_predict(int n_soap, int n_sites, int n_sparse, const double *soap, const double *Qs,
+                                 const double *alphas, double V0, double delta, double zeta, int do_derivatives,
+                                 const double *soap_cart_der, const int *n_neigh, double *V, double *V_der);
+
 /* get_gap_soap (gap_interface.f90:41-433) for one SOAP model on the global neighbor list:
  * subset by rcut/species, central-species filter, get_soap, energies/forces, scatter back.
  * species_supercell: species channel (1..n_species) per supercell atom, 0 = blind.

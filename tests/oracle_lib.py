@@ -73,6 +73,8 @@ def lib():
         L.orc_get_gap_soap.argtypes = [C.POINTER(_Hypers), C.c_int, C.c_int, _ip, _ip, _dp, _dp,
                                        _dp, _dp, _ip, C.c_int, C.c_int, _dp, _dp, C.c_double,
                                        C.c_double, C.c_int, _dp, _dp, _dp]
+        L.orc_local_property_predict.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
+                                                 C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp]
         L.orc_velocity_verlet.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double,
                                           C.POINTER(C.c_double), C.c_int]
         L.orc_mc_move_acceptance.restype = C.c_double
@@ -234,6 +236,22 @@ def soap_energy_and_forces(soap, soap_der, alphas, delta, zeta, e0, Qs, n_neigh,
         np.ascontiguousarray(n_neigh, np.int32), np.ascontiguousarray(nl, np.int32),
         np.ascontiguousarray(xyz, float), int(do_forces), n_sites0, en, fo, vir)
     return en, fo, vir.reshape(3, 3, order="F")
+
+
+def local_property_predict(soap, Qs, alphas, V0, delta, zeta, soap_cart_der=None, n_neigh=None):
+    """local_property_predict: soap (n_sites, D), Qs (M, D), soap_cart_der (P, D, 3) or None."""
+    soap = np.ascontiguousarray(soap, float)
+    n_sites, D = soap.shape
+    do_der = soap_cart_der is not None
+    P = int(np.sum(n_neigh)) if do_der else 0
+    V = np.zeros(n_sites)
+    V_der = np.zeros((max(P, 1), 3))
+    der = np.ascontiguousarray(soap_cart_der, float) if do_der else np.zeros(3)
+    nn = np.ascontiguousarray(n_neigh if do_der else np.zeros(max(n_sites, 1)), np.int32)
+    lib().orc_local_property_predict(D, n_sites, len(alphas), soap, np.ascontiguousarray(Qs, float),
+                                     np.ascontiguousarray(alphas, float), V0, delta, zeta, int(do_der), der, nn,
+                                     V, V_der)
+    return V, (V_der[:P] if do_der else None)
 
 
 def get_gap_soap(h, n_total_sites, nb, species_sc, central_species, alphas, Qs, delta, zeta,

@@ -331,3 +331,64 @@ def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
         assert np.max(np.abs(st["velocities"] - v)) < 1e-12, k
         x, v = st["positions"].copy(), st["velocities"].copy()
     assert len(pairs) > 1  # the list changed size across rebuilds
+
+
+# ------------------------------------------------------------------------- local properties
+
+def test_local_property_predict_matches_oracle(ctx, synth):
+    """tgap_local_property_predict (local_properties.f90:46-147, host arrays) against the oracle:
+    an integer zeta with nothing clipped, then zeta = 4 + 5e-6 (real power under the 1e-10 rule)
+    with V0 set so that about half the sites clip to zero."""
+    hyp, nb, mask = _soap_inputs(synth, 23)
+    q, der = orc.get_soap(orc.Hypers(hyp), nb["n_neigh"], mask, nb["rjs"], nb["thetas"], nb["phis"])
+    model = synth.gap_model(q, 30, seed=5)
+    a_pos = np.abs(model["alphas"])
+    raw = 1.2 ** 2 * (q @ model["Qs"].T) ** 4 @ model["alphas"]
+    for alphas, V0, zeta in ((a_pos, 0.0, 4.0), (model["alphas"], -np.median(raw), 4.0 + 5e-6)):
+        V_o, Vd_o = orc.local_property_predict(q, model["Qs"], alphas, V0, 1.2, zeta, der, nb["n_neigh"])
+        V_g, Vd_g = ctx.local_property_predict(q, model["Qs"], alphas, V0, 1.2, zeta, der, nb["n_neigh"])
+        assert np.max(np.abs(V_g - V_o)) <= 1e-12 * np.max(np.abs(V_o))
+        assert np.max(np.abs(Vd_g - Vd_o)) <= 1e-10 * np.max(np.abs(Vd_o))
+        assert np.array_equal(V_g == 0.0, V_o == 0.0)
+    assert 0 < np.sum(V_o == 0.0) < len(V_o)
+
+
+@pytest.mark.parametrize("precision_name", ["TGAP_FP64", "TGAP_MIXED"])
+def test_local_property_resident_matches_oracle(ctx, tg, synth, carbon, precision_name):
+    """tgap_local_property on a resident system (descriptor derivatives never materialised: the
+    adjoint writes each pair's dV_i/dr_j) against the oracle on the same neighbor list. FP64: V to
+    1e-12 and V_der to 1e-9 of their largest entry. Mixed: V to 1e-4 of the property's scale before
+    the offset V0 (the mixed path's energy accuracy) and V_der to 2e-3 of its largest entry, on the
+    sites that are not within 1e-3 of that scale from the clipping point (where rounding may decide
+    the clip)."""
+    precision = getattr(tg, precision_name)
+    hyp, m = carbon
+    pos, box, sp = synth.diamond_supercell(3, seed=35)
+    n = len(pos)
+    nb = orc.build_neighbors(pos, n, *box, 3.7, sp, False)
+    P = len(nb["rjs"])
+    q, der = orc.get_soap(orc.Hypers(hyp), nb["n_neigh"], np.ones((P, 1), bool), nb["rjs"], nb["thetas"],
+                          nb["phis"])
+    raw = (q @ m["Qs"].T) ** 4 @ m["alphas"]
+    V0 = -np.median(raw)
+    V_o, Vd_o = orc.local_property_predict(q, m["Qs"], m["alphas"], V0, 1.0, 4.0, der, nb["n_neigh"])
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7)
+    assert system.n_pairs == P
+    V_g, Vd_g = system.local_property(model, V0, precision)
+    start = np.concatenate([[0], np.cumsum(nb["n_neigh"])])
+    if precision == tg.TGAP_FP64:
+        assert np.max(np.abs(V_g - V_o)) <= 1e-12 * np.max(np.abs(V_o))
+        assert np.max(np.abs(Vd_g - Vd_o)) <= 1e-9 * np.max(np.abs(Vd_o))
+        assert np.array_equal(V_g == 0.0, V_o == 0.0)
+    else:
+        far = np.abs(raw + V0) > 1e-3 * np.max(np.abs(raw))
+        assert np.max(np.abs(V_g - V_o)[far]) <= 1e-4 * np.max(np.abs(raw))
+        pf = np.repeat(far, nb["n_neigh"])
+        assert np.max(np.abs(Vd_g - Vd_o)[pf]) <= 2e-3 * np.max(np.abs(Vd_o))
+    assert 0 < np.sum(V_o == 0.0) < n
+    clipped = np.nonzero(V_g == 0.0)[0]
+    for i in clipped:
+        assert np.all(Vd_g[start[i]:start[i + 1]] == 0.0)
+    system.close()
+    model.close()

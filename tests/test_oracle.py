@@ -310,3 +310,49 @@ def test_mc_acceptance_uses_single_precision_kb(orc):
     p = orc.mc_move_acceptance(0.1, 0.0, 2000.0)
     assert p == np.exp(-0.1 / (kb32 * 2000.0))
     assert orc.mc_move_acceptance(-1.0, 0.0, 300.0) == 1.0
+
+
+def test_local_property_predict_pinned_by_gap_forces_and_formula(orc, synth):
+    """local_property_predict (local_properties.f90:46-147). With V0 = 0, positive alphas (no
+    clipping) and an integer zeta, V equals the GAP energies and minus the sum of V_der over the
+    pairs that end on atom j equals the GAP force on j (the force path is pinned by finite
+    differences above); each site's pair derivatives sum to zero. With a negative V0 and a zeta
+    4 + 5e-6 (an integer for gap.f90's 1e-5 test, not for the 1e-10 test of
+    local_properties.f90:76-77), V matches a direct evaluation, clipped sites get 0 and so do
+    their derivatives."""
+    hyp = synth.carbon_hypers()
+    H = orc.Hypers(hyp)
+    pos, box, sp = synth.diamond_supercell(3, seed=13)
+    N = len(pos)
+    nb = orc.build_neighbors(pos, N, *box, 3.7, sp, False)
+    P = len(nb["rjs"])
+    q, der = orc.get_soap(H, nb["n_neigh"], np.ones((P, 1), bool), nb["rjs"], nb["thetas"], nb["phis"])
+    model = synth.gap_model(q, 40, seed=4)
+    Qs = model["Qs"]
+    a_pos = np.abs(model["alphas"])
+    V, Vd = orc.local_property_predict(q, Qs, a_pos, 0.0, 1.0, 4.0, der, nb["n_neigh"])
+    e, f, _ = orc.soap_energy_and_forces(q, der, a_pos, 1.0, 4.0, 0.0, Qs, nb["n_neigh"], nb["neighbors_list"],
+                                         nb["xyz"], n_sites0=N)
+    assert np.max(np.abs(V - e)) <= 1e-14 * np.max(np.abs(e))
+    F = np.zeros((N, 3))
+    np.add.at(F, (nb["neighbors_list"] - 1) % N, -Vd)
+    assert np.max(np.abs(F - f)) <= 1e-12 * np.max(np.abs(f))
+    start = np.concatenate([[0], np.cumsum(nb["n_neigh"])])
+    sums = np.array([Vd[start[i]:start[i + 1]].sum(0) for i in range(N)])
+    assert np.max(np.abs(sums)) <= 1e-12 * np.max(np.abs(Vd))
+    # clipping and the local-property integer-zeta rule
+    K = q @ Qs.T
+    assert K.min() > 0.0
+    zeta, d = 4.0 + 5e-6, 1.3
+    raw = d * d * (K ** zeta) @ model["alphas"]
+    V0 = -np.median(raw)
+    V2, Vd2 = orc.local_property_predict(q, Qs, model["alphas"], V0, d, zeta, der, nb["n_neigh"])
+    ref = np.maximum(raw + V0, 0.0)
+    assert np.max(np.abs(V2 - ref)) <= 1e-13 * np.max(np.abs(raw))
+    clipped = V2 == 0.0
+    assert 0 < clipped.sum() < N
+    for i in np.nonzero(clipped)[0]:
+        assert np.all(Vd2[start[i]:start[i + 1]] == 0.0)
+    # the integer-power path would differ by more than the rounding
+    raw_int = d * d * (K ** 4) @ model["alphas"]
+    assert np.max(np.abs(raw_int - raw)) > 1e3 * 1e-13 * np.max(np.abs(raw))

@@ -164,6 +164,23 @@ class Context:
             int(n_sites0), ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_soap_energy_and_forces")
         return en, fo, vir.reshape(3, 3, order="F")
 
+    def local_property_predict(self, soap, Qs, alphas, V0, delta, zeta, soap_cart_der=None, n_neigh=None):
+        """local_property_predict: soap (n_sites, D), Qs (M, D), soap_cart_der (P, D, 3) or None.
+        Returns V (n_sites) and V_der (P, 3) or None."""
+        soap = _f64(soap)
+        n_sites, D = soap.shape
+        Qs = _f64(Qs)
+        do_der = soap_cart_der is not None
+        nn = _i32(n_neigh) if do_der else None
+        P = int(nn.sum()) if do_der else 0
+        V = np.zeros(n_sites)
+        Vd = np.zeros((max(P, 1), 3))
+        check(self._L.tgap_local_property_predict(
+            self.h, D, n_sites, Qs.shape[0], ptr(soap), ptr(Qs), ptr(_f64(alphas)), float(V0), float(delta),
+            float(zeta), int(do_der), ptr(_f64(soap_cart_der)) if do_der else None, ptr(nn) if do_der else None, P,
+            ptr(V), ptr(Vd)), self.h, "tgap_local_property_predict")
+        return V, (Vd[:P] if do_der else None)
+
     def get_gap_soap(self, hypers, n_total_sites, nb, species_supercell, central_species, alphas, Qs, delta,
                      zeta, do_forces=True, precision=TGAP_FP64, energies0=None, forces0=None, want_soap=False):
         """get_gap_soap for one model on a global neighbor list `nb` (dict as returned by
@@ -270,6 +287,21 @@ class System:
         check(self.ctx._L.tgap_compute(self.ctx.h, self.h, len(models), arr, int(precision), int(do_forces),
                                        C.c_void_p(d_energies), C.c_void_p(d_forces) if d_forces else None,
                                        C.c_void_p(d_virial) if d_virial else None), self.ctx.h, "tgap_compute")
+
+    def local_property(self, model, V0, precision, do_derivatives=True):
+        """Per-site property of a property model (tgap_local_property): V (n_atoms) and, with
+        do_derivatives, dV_i/dr_j per list pair (n_pairs, 3), as host arrays."""
+        import torch
+        n, P = self.n_atoms, self.n_pairs
+        V = torch.zeros(n, dtype=torch.float64, device="cuda")
+        Vd = torch.zeros(3 * max(P, 1), dtype=torch.float64, device="cuda")
+        torch.cuda.synchronize()
+        check(self.ctx._L.tgap_local_property(self.ctx.h, self.h, model.h, float(V0), int(precision),
+                                              int(do_derivatives), C.c_void_p(V.data_ptr()),
+                                              C.c_void_p(Vd.data_ptr()) if do_derivatives else None),
+              self.ctx.h, "tgap_local_property")
+        self.ctx.synchronize()
+        return V.cpu().numpy(), (Vd.cpu().numpy()[:3 * P].reshape(P, 3) if do_derivatives else None)
 
     def autotune(self, models, precision, reps=5):
         """Times the tunable launch shapes of this system's evaluation and keeps the fastest in the

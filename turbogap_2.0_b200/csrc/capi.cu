@@ -635,6 +635,66 @@ extern "C" int tgap_get_soap_energy_and_forces(tgap_context *ctx, int n_soap, in
     return rc;
 }
 
+extern "C" int tgap_local_property_predict(tgap_context *ctx, int n_soap, int n_sites, int n_sparse,
+                                           const double *soap, const double *Qs, const double *alphas, double V0,
+                                           double delta, double zeta, int do_derivatives,
+                                           const double *soap_cart_der, const int *n_neigh, int n_atom_pairs,
+                                           double *V, double *V_der)
+{
+    CHECK_RC(activate(ctx));
+    if (n_soap <= 0 || n_sites < 0 || n_sparse <= 0 || !soap || !Qs || !alphas || !V ||
+        (do_derivatives && (!soap_cart_der || !n_neigh || !V_der || n_atom_pairs < 0)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_local_property_predict: bad arguments");
+    if (n_sites == 0) return TGAP_OK;
+    DeviceModel m;
+    m.n_sparse = n_sparse;
+    m.dim = n_soap;
+    m.delta = delta;
+    m.zeta = zeta;
+    m.zeta_tol = 1.0e-10;  // local_properties.f90:76-77
+    m.zeta_nint = true;
+    DevBuf *S = ctx->scratch;
+    GapWork w;
+    auto cleanup = [&]() {
+        m.Qs.release();
+        m.QsT.release();
+        m.alphas.release();
+        w.e_part.release();
+        w.G.release();
+        w.g.release();
+    };
+    int rc = upload(ctx, m.Qs, Qs, (size_t)n_sparse * n_soap);
+    if (!rc) rc = upload(ctx, m.alphas, alphas, (size_t)n_sparse);
+    if (!rc && m.QsT.ensure(sizeof(double) * (size_t)n_sparse * n_soap)) rc = set_error(ctx, TGAP_ERR_NOMEM, "Qs transpose");
+    if (!rc) rc = transpose_f64(ctx, n_sparse, n_soap, m.Qs.as<double>(), m.QsT.as<double>());
+    if (!rc) rc = upload(ctx, S[0], soap, (size_t)n_sites * n_soap);
+    if (!rc && S[1].ensure(sizeof(double) * (size_t)n_sites)) rc = TGAP_ERR_NOMEM;
+    // V = delta^2 K^zeta alphas + V0 (the GAP energy with e0 = V0), clipped; g = dV/dq
+    if (!rc)
+        rc = gap_energy_grad_f64(ctx, m, S[0].as<double>(), n_soap, n_sites, V0, do_derivatives, &w, nullptr,
+                                 S[1].as<double>(), nullptr);
+    if (!rc) rc = clip_nonneg(ctx, n_sites, S[1].as<double>());
+    if (!rc) rc = download(ctx, V, S[1], (size_t)n_sites);
+    if (!rc && do_derivatives) {
+        std::vector<int64_t> hstart(n_sites + 1, 0);
+        for (int i = 0; i < n_sites; ++i) hstart[i + 1] = hstart[i] + n_neigh[i];
+        const size_t P = (size_t)hstart[n_sites];
+        if ((int64_t)P != (int64_t)n_atom_pairs) rc = set_error(ctx, TGAP_ERR_ARGUMENT, "sum(n_neigh) != n_atom_pairs");
+        if (!rc && P > 0) {
+            rc = upload(ctx, S[2], hstart.data(), hstart.size());
+            if (!rc) rc = upload(ctx, S[4], soap_cart_der, 3 * P * (size_t)n_soap);
+            if (!rc && S[6].ensure(sizeof(double) * 3 * P)) rc = TGAP_ERR_NOMEM;
+            if (!rc)
+                rc = local_property_pairs(ctx, n_sites, S[2].as<int64_t>(), w.g.as<double>(), n_soap, S[4].as<double>(),
+                                          S[1].as<double>(), S[6].as<double>());
+            if (!rc) rc = download(ctx, V_der, S[6], 3 * P);
+        }
+    }
+    if (!rc) rc = cudaStreamSynchronize(ctx->stream) == cudaSuccess ? TGAP_OK : TGAP_ERR_CUDA;
+    cleanup();
+    return rc ? rc : read_device_check(ctx);
+}
+
 extern "C" int tgap_assign_species(int n_species, const char *species_types, int n, const char *names,
                                    int *out)
 {
@@ -898,6 +958,63 @@ extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tga
     }
     for (int i = 0; i < n_models; ++i)
         CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial));
+    return TGAP_OK;
+}
+
+extern "C" int tgap_local_property(tgap_context *ctx, tgap_system *s, tgap_model *m, double V0, int precision,
+                                   int do_derivatives, double *d_V, double *d_V_der)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || !m || !d_V || (do_derivatives && !d_V_der))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_local_property: bad arguments");
+    if (precision != TGAP_FP64 && precision != TGAP_MIXED) return set_error(ctx, TGAP_ERR_ARGUMENT, "precision");
+    const int N = s->nb.n_atoms;
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_V, 0, sizeof(double) * N, ctx->stream));
+    if (do_derivatives)
+        TGAP_CUDA(ctx, cudaMemsetAsync(d_V_der, 0, sizeof(double) * 3 * (size_t)s->nb.n_pairs, ctx->stream));
+    SiteSet *ss = nullptr;
+    CHECK_RC(site_set(s, m->central_species, &ss));
+    const int n_rows = ss->n_rows;
+    if (n_rows == 0) return TGAP_OK;
+    CHECK_RC(ensure_eval_buffers(s, m, n_rows, precision));
+    DeviceModel gm = m->gap;  // shallow copy: the same device operands, the local-property zeta test
+    gm.zeta_tol = 1.0e-10;
+    gm.zeta_nint = true;
+    PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
+                s->nb.nspecies.as<int>(), s->nb.jatom.as<int>(), s->nb.n_atoms, ctx->d_check};
+    SoapOut o;
+    o.c = s->c.ptr;
+    o.q = s->q.ptr;
+    o.norm = s->norm.ptr;
+    const int *sites = ss->sites.as<int>();
+    const void *g = nullptr;
+    int g_ld = 0, g_double = 0;
+    if (precision == TGAP_FP64) {
+        o.q_ld = m->gap.dim;
+        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o));
+        CHECK_RC(gap_energy_grad_f64(ctx, gm, (const double *)o.q, o.q_ld, n_rows, V0, do_derivatives, &s->gw, sites,
+                                     nullptr, d_V));
+        g = s->gw.g.ptr;
+        g_ld = m->gap.dim;
+        g_double = 1;
+    } else {
+        if (!m->mixed_ready) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "mixed path not prepared");
+        o.q_ld = m->gap.dim_pad;
+        o.q_hi = s->q_hi.as<__nv_bfloat16>();
+        o.q_lo = s->q_lo.as<__nv_bfloat16>();
+        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o));
+        CHECK_RC(gap_energy_grad_mixed(ctx, gm, o.q_hi, o.q_lo, n_rows, V0, do_derivatives, &s->gw, sites, nullptr,
+                                       d_V));
+        g = s->gw.g.ptr;
+        g_ld = m->gap.dim_pad;
+    }
+    CHECK_RC(clip_nonneg(ctx, N, d_V));
+    if (do_derivatives) {
+        pv.pair_der = d_V_der;
+        pv.gate = d_V;
+        CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, precision, o, g, g_ld, g_double, nullptr, nullptr,
+                               nullptr));
+    }
     return TGAP_OK;
 }
 

@@ -184,9 +184,10 @@ int gap_energy_grad_f64(tgap_context *ctx, const DeviceModel &m, const double *d
     e.G = do_forces ? w->G.as<double>() : nullptr;
     e.ldg = N;
     e.e_part = w->e_part.as<double>();
-    const bool zi = std::fabs(m.zeta - (double)(int)m.zeta) < 1.0e-5;  // gap.f90:99-105
-    e.zeta_int = zi ? (int)m.zeta : -1;
-    e.zeta = zi ? (double)(int)m.zeta : m.zeta;
+    const double zr = m.zeta_nint ? std::nearbyint(m.zeta) : (double)(int)m.zeta;
+    const bool zi = std::fabs(m.zeta - zr) < m.zeta_tol;  // gap.f90:99-105 (local properties: :76-77)
+    e.zeta_int = zi ? (int)zr : -1;
+    e.zeta = zi ? zr : m.zeta;
     e.zd2 = e.zeta * m.delta * m.delta;
     dim3 grid(n_tiles, (M + kBM - 1) / kBM);
     StageScope sc(ctx, "dgemm_gap_kernel_f64");
@@ -203,6 +204,66 @@ int gap_energy_grad_f64(tgap_context *ctx, const DeviceModel &m, const double *d
                           w->g.as<double>(), K, 1.0);
         if (rc) return rc;
     }
+    return TGAP_OK;
+}
+
+// local_properties.f90:117-122: every V >= 0.
+__global__ void k_clip_nonneg(int n, double *__restrict__ v)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n && v[i] < 0.0) v[i] = 0.0;
+}
+
+int clip_nonneg(tgap_context *ctx, int n, double *d_v)
+{
+    if (n <= 0) return TGAP_OK;
+    k_clip_nonneg<<<(n + 255) / 256, 256, 0, ctx->stream>>>(n, d_v);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+// local_properties.f90:124-142 over a materialised soap_cart_der: one warp per site, V_der(:, j)
+// = g_i . der(:, :, j) for each of its pairs (lanes over the descriptor, fixed reduction order),
+// zero when V_i was clipped to 0.
+__global__ void k_local_property_pairs(int n_sites, const int64_t *__restrict__ start, const double *__restrict__ g,
+                                       int D, const double *__restrict__ der, const double *__restrict__ V,
+                                       double *__restrict__ V_der)
+{
+    const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
+    if (i >= n_sites) return;
+    const double *gi = g + (size_t)i * D;
+    const bool zero = V[i] == 0.0;
+    for (int64_t j = start[i]; j < start[i + 1]; ++j) {
+        double a0 = 0.0, a1 = 0.0, a2 = 0.0;
+        if (!zero) {
+            const double *dj = der + (size_t)j * 3 * D;
+            for (int d = lane; d < D; d += 32) {
+                const double gd = gi[d];
+                a0 += gd * dj[3 * d];
+                a1 += gd * dj[3 * d + 1];
+                a2 += gd * dj[3 * d + 2];
+            }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                a0 += __shfl_xor_sync(0xffffffffu, a0, o);
+                a1 += __shfl_xor_sync(0xffffffffu, a1, o);
+                a2 += __shfl_xor_sync(0xffffffffu, a2, o);
+            }
+        }
+        if (lane == 0) {
+            V_der[3 * j] = a0;
+            V_der[3 * j + 1] = a1;
+            V_der[3 * j + 2] = a2;
+        }
+    }
+}
+
+int local_property_pairs(tgap_context *ctx, int n_sites, const int64_t *d_start, const double *d_g, int D,
+                         const double *d_der, const double *d_V, double *d_V_der)
+{
+    if (n_sites <= 0) return TGAP_OK;
+    k_local_property_pairs<<<(n_sites + 3) / 4, 128, 0, ctx->stream>>>(n_sites, d_start, d_g, D, d_der, d_V, d_V_der);
+    TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
 

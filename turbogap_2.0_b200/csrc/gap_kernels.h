@@ -12,6 +12,10 @@ struct DeviceModel {
     int n_sparse = 0, dim = 0;
     int dim_pad = 0, m_pad = 0;  // padded sizes of the bf16 operands (multiples of 64 / 128)
     double delta = 1.0, zeta = 4.0;
+    // integer-zeta test: |zeta - z| < zeta_tol with z = trunc(zeta) (gap.f90:99-105, 1e-5) or, for
+    // local properties, z = nint(zeta) and 1e-10 (local_properties.f90:76-77)
+    double zeta_tol = 1.0e-5;
+    bool zeta_nint = false;
     DevBuf Qs;        // double [n_sparse][dim]  (row = sparse point; Fortran Qs(dim, n_sparse))
     DevBuf QsT;       // double [dim][n_sparse]
     DevBuf alphas;    // double [n_sparse]
@@ -44,6 +48,12 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
                           GapWork *w, const int *d_sites, double *d_e_rows, double *d_energies,
                           const int *d_skip = nullptr);
 int model_upload_mixed(tgap_context *ctx, DeviceModel *m);
+
+// Local properties (local_properties.f90:46-147): V clipped at zero, and per-pair derivatives
+// V_der(:, j) = g_i . der(:, :, j) (zero for clipped sites) from a materialised soap_cart_der.
+int clip_nonneg(tgap_context *ctx, int n, double *d_v);
+int local_property_pairs(tgap_context *ctx, int n_sites, const int64_t *d_start, const double *d_g, int D,
+                         const double *d_der, const double *d_V, double *d_V_der);
 
 int pair_forces_from_der(tgap_context *ctx, int n_sites, const int64_t *d_start, const int *d_nl,
                          int n_sites0, const double *d_g, int D, const double *d_der,

@@ -968,7 +968,8 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     if (do_forces && w->g.ensure(4 * (size_t)rows_pad * m.dim_pad))
         return set_error(ctx, TGAP_ERR_NOMEM, "mixed GAP workspace");
     if (d_e_rows) TGAP_CUDA(ctx, cudaMemsetAsync(d_e_rows, 0, sizeof(double) * (size_t)n_rows, ctx->stream));
-    const bool zi = std::fabs(m.zeta - (double)(int)m.zeta) < 1.0e-5;  // gap.f90:99-105
+    const double zr = m.zeta_nint ? std::nearbyint(m.zeta) : (double)(int)m.zeta;
+    const bool zi = std::fabs(m.zeta - zr) < m.zeta_tol;  // gap.f90:99-105 (local properties: :76-77)
     if (m.dim_pad <= 384 && m.m_pad % 128 == 0) {
         // fused: G never leaves the SM (k_gap_flash); dE/dq accumulates with atomics
         if (do_forces)
@@ -981,8 +982,8 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         p.e_rows = d_e_rows;
         p.d2 = m.delta * m.delta;
         p.e0 = e0;
-        p.zeta_int = zi ? (int)m.zeta : -1;
-        p.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
+        p.zeta_int = zi ? (int)zr : -1;
+        p.zeta = (float)(zi ? zr : m.zeta);
         p.zd2 = (float)(p.zeta * m.delta * m.delta);
         p.g = do_forces ? w->g.as<float>() : nullptr;
         p.ldg = m.dim_pad;
@@ -1009,8 +1010,8 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     e1.e_rows = d_e_rows;
     e1.d2 = m.delta * m.delta;
     e1.e0 = e0;
-    e1.zeta_int = zi ? (int)m.zeta : -1;
-    e1.zeta = (float)(zi ? (double)(int)m.zeta : m.zeta);
+    e1.zeta_int = zi ? (int)zr : -1;
+    e1.zeta = (float)(zi ? zr : m.zeta);
     e1.zd2 = (float)(e1.zeta * m.delta * m.delta);
     // 256-column tiles re-read the descriptor rows half as often as 128-column ones (the GEMM is
     // bound by L2 -> SM operand traffic); two 96 KB stages then fill the shared memory

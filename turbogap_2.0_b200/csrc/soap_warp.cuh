@@ -572,14 +572,15 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
     const int *__restrict__ nsp, const int *__restrict__ jatom, const int *__restrict__ site_struct,
     const T *__restrict__ c_in, const T *__restrict__ q_in, int q_ld, const T *__restrict__ norm_in,
     const GT *__restrict__ g_in, int g_ld, double *__restrict__ forces, double *__restrict__ virial,
-    int warp_smem, int n_atoms, int *check)
+    int warp_smem, int n_atoms, int *check, double *__restrict__ pair_der, const double *__restrict__ gate)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int row = blockIdx.x * nw + warp;
-    const bool active = row < n_rows;
+    // pair-derivative mode: a site whose gate is 0 writes nothing (its pairs stay zero)
+    const bool active = row < n_rows && !(pair_der && gate && gate[sites ? sites[row] : row] == 0.0);
     double *vpart = reinterpret_cast<double *>(smem_raw + (size_t)nw * warp_smem);
     int *vstruct = reinterpret_cast<int *>(vpart + 6 * kWarpsPerCta);
     double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
@@ -679,13 +680,19 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
                 const T w0 = w[0], w1 = w[1], w2 = w[2];
                 // w = dE_i/dr_ij: force -w on the neighbor, +w on the site (its self slot)
                 const double f0 = -(double)w0, f1 = -(double)w1, f2 = -(double)w2;
-                const int j = jatom[k];
-                if (j >= 0 && j < n_atoms) {
-                    atomicAdd(forces + 3 * (size_t)j, f0);
-                    atomicAdd(forces + 3 * (size_t)j + 1, f1);
-                    atomicAdd(forces + 3 * (size_t)j + 2, f2);
+                if (pair_der) {
+                    pair_der[3 * k] = (double)w0;
+                    pair_der[3 * k + 1] = (double)w1;
+                    pair_der[3 * k + 2] = (double)w2;
                 } else {
-                    check_fail(check, kCheckBwdAtom, k, j);
+                    const int j = jatom[k];
+                    if (j >= 0 && j < n_atoms) {
+                        atomicAdd(forces + 3 * (size_t)j, f0);
+                        atomicAdd(forces + 3 * (size_t)j + 1, f1);
+                        atomicAdd(forces + 3 * (size_t)j + 2, f2);
+                    } else {
+                        check_fail(check, kCheckBwdAtom, k, j);
+                    }
                 }
                 vl[0] -= f0;
                 vl[1] -= f1;
@@ -708,13 +715,18 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
         }
         if (lane < 3) {
             const double fv = lane == 0 ? vals[0] : (lane == 1 ? vals[1] : vals[2]);
-            const int js = jatom[kb];
-            if (js >= 0 && js < n_atoms)
-                atomicAdd(forces + 3 * (size_t)js + lane, fv);
-            else if (lane == 0)
-                check_fail(check, kCheckSelfAtom, kb, js);
+            if (pair_der) {
+                pair_der[3 * kb + lane] = -fv;  // dq_i/dr_i = -sum_j dq_i/dr_j
+            } else {
+                const int js = jatom[kb];
+                if (js >= 0 && js < n_atoms)
+                    atomicAdd(forces + 3 * (size_t)js + lane, fv);
+                else if (lane == 0)
+                    check_fail(check, kCheckSelfAtom, kb, js);
+            }
         }
     }
+    if (pair_der) return;  // uniform over the grid: no virial in pair-derivative mode
     // virial (xx yy zz xy xz yz -> column-major 3x3): one set of atomics per CTA when its rows
     // share a structure, else one per warp
     if (lane == 0) {
@@ -839,7 +851,7 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
         ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
         d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
         (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial, (int)wb, pv.n_atoms,
-        pv.check);
+        pv.check, pv.pair_der, pv.gate);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -220,6 +220,10 @@ struct PairView {
     const int *jatom;       // [P]    folded global neighbor index (force scatter)
     int n_atoms;            // bound of jatom
     int *check;             // device check word
+    // adjoint only: when set, dq_i/dr_j contracted with dE_i/dq_i is written per pair (3 per list
+    // pair, self slot = minus the sum) instead of being scattered into forces and virial
+    double *pair_der = nullptr;
+    const double *gate = nullptr;  // with pair_der: sites whose gate value is 0 write nothing
 };
 
 }  // namespace tgap

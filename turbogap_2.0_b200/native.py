@@ -130,6 +130,9 @@ def lib():
                                    vp, vp, vp, vp, vp, vp, vp]),
         "tgap_screen_train": (i32, [vp, i64, i32, i32, vp, vp, i32, i32, C.c_float, vp,
                                     vp, vp, vp, vp, vp, vp, vp]),
+        "tgap_local_property_predict": (i32, [vp, i32, i32, i32, vp, vp, vp, C.c_double, C.c_double, C.c_double,
+                                              i32, vp, vp, i32, vp, vp]),
+        "tgap_local_property": (i32, [vp, vp, vp, C.c_double, i32, i32, vp, vp]),
         "tgap_autotune": (i32, [vp, vp, i32, vp, i32, i32]),
         "tgap_autotune_report": (i32, [vp, vp, i64, vp]),
         "tgap_autotune_clear": (i32, [vp]),
