@@ -118,6 +118,19 @@ module tgap_iface
          real(c_double) :: energies0(*), forces0(3, *), virial(3, 3)
          type(c_ptr), value :: soap_out
       end function
+
+      integer(c_int) function tgap_local_property_predict(ctx, n_soap, n_sites, n_sparse, soap, Qs, alphas, &
+                                                          V0, delta, zeta, do_derivatives, soap_cart_der, &
+                                                          n_neigh, n_atom_pairs, V, V_der) &
+         bind(C, name="tgap_local_property_predict")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: n_soap, n_sites, n_sparse, do_derivatives, n_atom_pairs
+         real(c_double), intent(in) :: soap(n_soap, *), Qs(n_soap, *), alphas(*), soap_cart_der(3, n_soap, *)
+         real(c_double), value :: V0, delta, zeta
+         integer(c_int), intent(in) :: n_neigh(*)
+         real(c_double) :: V(*), V_der(3, *)
+      end function
    end interface
 
 contains
@@ -138,6 +151,24 @@ contains
                                            forces, virial)
       if (st /= TGAP_OK) then
          write (*, *) "tgap_get_soap_energy_and_forces failed with status", st
+         stop
+      end if
+   end subroutine
+
+   ! Drop-in body for local_property_predict (local_properties.f90:46-50 argument list).
+   subroutine tgap_local_property_predict_f(ctx, soap, Qs, alphas, V0, delta, zeta, V, do_derivatives, &
+                                            soap_cart_der, n_neigh, V_der)
+      type(c_ptr), intent(in) :: ctx
+      real(c_double), intent(in) :: soap(:, :), Qs(:, :), alphas(:), V0, delta, zeta, soap_cart_der(:, :, :)
+      integer, intent(in) :: n_neigh(:)
+      logical, intent(in) :: do_derivatives
+      real(c_double), intent(out) :: V(:), V_der(:, :)
+      integer(c_int) :: st
+      st = tgap_local_property_predict(ctx, size(soap, 1), size(soap, 2), size(alphas), soap, Qs, alphas, V0, &
+                                       delta, zeta, merge(1, 0, do_derivatives), soap_cart_der, n_neigh, &
+                                       sum(n_neigh), V, V_der)
+      if (st /= TGAP_OK) then
+         write (*, *) "tgap_local_property_predict failed with status", st
          stop
       end if
    end subroutine
