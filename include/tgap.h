@@ -236,6 +236,30 @@ int tgap_compute(tgap_context *ctx, tgap_system *system, int n_models,
                  tgap_model *const *models, int precision, int do_forces, double *d_energies,
                  double *d_forces, double *d_virial);
 
+/* get_2b_energy_and_forces (src/gap/gap.f90:329-460): the distance_2b GAP between species1 and
+ * species2 (channel indices, as tgap_assign_species maps the reference's character*8 names) on a
+ * full neighbor list (self first in each site's block, as build_neighbors_list writes it). Per
+ * site energies = e0 + sum over its pairs of delta^2 alphas(s) cutoff(s) fcut(r) exp(-(r - Qs(s))^2
+ * / 2 sigma^2), fcut the cosine taper over [rcut - buffer, rcut]; forces (3 x n_sites0, overwritten)
+ * on the sites only; virial (3 x 3) half the pair virial. FP64. */
+int tgap_get_2b_energy_and_forces(tgap_context *ctx, int n_sites, int n_atom_pairs, const double *rjs,
+                                  const double *xyz, int n_sparse, const double *alphas,
+                                  const double *cutoff, double rcut, double buffer, double delta,
+                                  double sigma, double e0, const double *Qs, const int *n_neigh,
+                                  int do_forces, const int *species, const int *neighbor_species,
+                                  int species1, int species2, int n_sites0, double *energies,
+                                  double *forces, double *virial);
+/* get_core_pot_energy_and_forces (src/gap/gap.f90:552-686): tabulated pair potential V(x) on an
+ * increasing grid x (n_sparse points) with precomputed spline second derivatives dVdx2 and end
+ * slopes yp1 / ypn, evaluated as the cubic spline of src/utils/splines.f90:33-156 for pairs with
+ * r < max(x); energies = 1/2 V per pair of each site, forces on the sites, half pair virial. FP64. */
+int tgap_get_core_pot_energy_and_forces(tgap_context *ctx, int n_sparse, int n_sites, int n_atom_pairs,
+                                        int n_sites0, const double *rjs, const double *xyz,
+                                        const double *x, const double *V, double yp1, double ypn,
+                                        const double *dVdx2, const int *n_neigh, int do_forces,
+                                        const int *species, const int *neighbor_species, int species1,
+                                        int species2, double *energies, double *forces, double *virial);
+
 /* Resident form of local_property_predict (local_properties.f90:46-147, as get_gap_soap calls it,
  * gap_interface.f90:314-364) for a property model held as a tgap_model (its delta, zeta, alphas
  * and sparse set; the integer-zeta test of local_properties.f90): device pointers d_V (n_atoms;

@@ -5,6 +5,8 @@
  *   get_soap_energy_and_forces   src/gap/gap.f90:39-244
  *   get_gap_soap                 src/gap/gap_interface.f90:41-433 (subset, renumber, scatter)
  *   local_property_predict       src/gap/local_properties.f90:46-147
+ *   get_2b_energy_and_forces     src/gap/gap.f90:329-460
+ *   get_core_pot_energy_and_forces src/gap/gap.f90:552-686 (spline, spline_der: src/utils/splines.f90:33-156)
  *   velocity_verlet              src/md/md_utils.f90:486-532
  *   monte_carlo_move             src/mc/mc_utils.f90:172-180 (+ min(1,p) of :255)
  */
@@ -158,6 +160,154 @@ void orc_local_property_predict(int n_soap, int n_sites, int n_sparse, const dou
         free(qs);
     }
     free(K);
+}
+
+/* species pair test of gap.f90:381-386 */
+static int pair_matches(int si, int sj, int sp1, int sp2)
+{
+    return (si == sp1 && sj == sp2) || (si == sp2 && sj == sp1);
+}
+
+static void virial_add_sym(double *virial, const double *f, const double *r)
+{
+    for (int k1 = 0; k1 < 3; ++k1)
+        for (int k2 = 0; k2 < 3; ++k2) virial[k1 + 3 * k2] -= 0.5 * (f[k1] * r[k2] + f[k2] * r[k1]);
+}
+
+void orc_get_2b_energy_and_forces(int n_sites, const double *rjs, const double *xyz, int n_sparse,
+                                  const double *alphas, const double *cutoff, double rcut, double buffer,
+                                  double delta, double sigma, double e0, const double *Qs, const int *n_neigh,
+                                  int do_forces, const int *species, const int *neighbor_species, int sp1, int sp2,
+                                  int n_sites0, double *energies, double *forces, double *virial)
+{
+    const double pi = acos(-1.0);
+    /* :374-402 energies */
+    for (int i = 0; i < n_sites; ++i) energies[i] = e0;
+    int64_t k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp1 && species[i] != sp2) {
+            k += n_neigh[i];
+            continue;
+        }
+        ++k;
+        for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+            if (!pair_matches(species[i], neighbor_species[k], sp1, sp2)) continue;
+            const double r = rjs[k];
+            if (!(r < rcut)) continue;
+            const double fcut = r < rcut - buffer ? 1.0 : (cos(pi * (r - rcut + buffer) / buffer) + 1.0) / 2.0;
+            for (int s = 0; s < n_sparse; ++s)
+                energies[i] += delta * delta * alphas[s] * cutoff[s] * fcut *
+                               exp(-0.5 * (r - Qs[s]) * (r - Qs[s]) / (sigma * sigma));
+        }
+    }
+    if (!do_forces) return;
+    /* :405-445 forces on the site, then half of the pair virial */
+    for (int x = 0; x < 3 * n_sites0; ++x) forces[x] = 0.0;
+    for (int x = 0; x < 9; ++x) virial[x] = 0.0;
+    k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp1 && species[i] != sp2) {
+            k += n_neigh[i];
+            continue;
+        }
+        ++k;
+        for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+            if (!pair_matches(species[i], neighbor_species[k], sp1, sp2)) continue;
+            const double r = rjs[k];
+            if (!(r < rcut)) continue;
+            double fcut, dfcut;
+            if (r < rcut - buffer) {
+                fcut = 1.0;
+                dfcut = 0.0;
+            } else {
+                fcut = (cos(pi * (r - rcut + buffer) / buffer) + 1.0) / 2.0;
+                dfcut = pi / 2.0 / buffer * sin(pi * (r - rcut + buffer) / buffer);
+            }
+            for (int s = 0; s < n_sparse; ++s) {
+                double f[3];
+                const double g = -2.0 * delta * delta * alphas[s] * cutoff[s] *
+                                 exp(-0.5 * (r - Qs[s]) * (r - Qs[s]) / (sigma * sigma));
+                const double h = (r - Qs[s]) / (sigma * sigma) * fcut + dfcut;
+                for (int c = 0; c < 3; ++c) f[c] = g * xyz[3 * k + c] / r * h;
+                for (int c = 0; c < 3; ++c) forces[3 * i + c] += f[c];
+                virial_add_sym(virial, f, xyz + 3 * k);
+            }
+        }
+    }
+    for (int x = 0; x < 9; ++x) virial[x] *= 0.5;
+}
+
+/* splines.f90:33-105 (one point) */
+static double spline_at(int n, const double *x, const double *y, const double *y2, double yp1, double ypn,
+                        double r)
+{
+    if (r < x[0]) return y[0] + (r - x[0]) * yp1;
+    if (r > x[n - 1]) return y[n - 1] + (r - x[n - 1]) * ypn;
+    int j = 0;
+    while (j < n - 2 && !(r < x[j + 1])) ++j;
+    const double h = x[j + 1] - x[j], h26 = h * h / 6.0;
+    const double A = (x[j + 1] - r) / h, B = 1.0 - A;
+    const double C = (A * A * A - A) * h26, D = (B * B * B - B) * h26;
+    return A * y[j] + B * y[j + 1] + C * y2[j] + D * y2[j + 1];
+}
+
+/* splines.f90:107-156 (one point) */
+static double spline_der_at(int n, const double *x, const double *y, const double *y2, double yp1, double ypn,
+                            double r)
+{
+    if (r < x[0]) return yp1;
+    if (r > x[n - 1]) return ypn;
+    int j = 0;
+    while (j < n - 2 && !(r < x[j + 1])) ++j;
+    const double h = x[j + 1] - x[j], h6 = h / 6.0;
+    const double A = (x[j + 1] - r) / h, B = 1.0 - A;
+    const double dAdx = -1.0 / h, dBdx = -dAdx;
+    const double dCdx = (1.0 - 3.0 * A * A) * h6, dDdx = (3.0 * B * B - 1.0) * h6;
+    return dAdx * y[j] + dBdx * y[j + 1] + dCdx * y2[j] + dDdx * y2[j + 1];
+}
+
+void orc_get_core_pot_energy_and_forces(int n_sparse, int n_sites, int n_sites0, const double *rjs,
+                                        const double *xyz, const double *x, const double *V, double yp1,
+                                        double ypn, const double *dVdx2, const int *n_neigh, int do_forces,
+                                        const int *species, const int *neighbor_species, int sp1, int sp2,
+                                        double *energies, double *forces, double *virial)
+{
+    double rcut = x[0];
+    for (int s = 1; s < n_sparse; ++s) rcut = x[s] > rcut ? x[s] : rcut; /* :593 maxval(x) */
+    for (int i = 0; i < n_sites; ++i) energies[i] = 0.0;
+    int64_t k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp1 && species[i] != sp2) {
+            k += n_neigh[i];
+            continue;
+        }
+        ++k;
+        for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+            if (!pair_matches(species[i], neighbor_species[k], sp1, sp2)) continue;
+            if (rjs[k] < rcut) energies[i] += 0.5 * spline_at(n_sparse, x, V, dVdx2, yp1, ypn, rjs[k]);
+        }
+    }
+    if (!do_forces) return;
+    for (int q = 0; q < 3 * n_sites0; ++q) forces[q] = 0.0;
+    for (int q = 0; q < 9; ++q) virial[q] = 0.0;
+    k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp1 && species[i] != sp2) {
+            k += n_neigh[i];
+            continue;
+        }
+        ++k;
+        for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+            if (!pair_matches(species[i], neighbor_species[k], sp1, sp2)) continue;
+            if (!(rjs[k] < rcut)) continue;
+            const double dv = spline_der_at(n_sparse, x, V, dVdx2, yp1, ypn, rjs[k]);
+            double f[3];
+            for (int c = 0; c < 3; ++c) f[c] = dv * xyz[3 * k + c] / rjs[k];
+            for (int c = 0; c < 3; ++c) forces[3 * i + c] += f[c];
+            virial_add_sym(virial, f, xyz + 3 * k);
+        }
+    }
+    for (int q = 0; q < 9; ++q) virial[q] *= 0.5;
 }
 
 int orc_get_gap_soap(const orc_soap_hypers *h, int n_total_sites, int n_sites0,

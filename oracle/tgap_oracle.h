@@ -130,6 +130,20 @@ void orc_local_property_predict(int n_soap, int n_sites, int n_sparse, const dou
                                  const double *alphas, double V0, double delta, double zeta, int do_derivatives,
                                  const double *soap_cart_der, const int *n_neigh, double *V, double *V_der);
 
+/* get_2b_energy_and_forces (gap.f90:329-460): species given as channel indices (sp1, sp2 the
+ * pair's); energies = e0 + the pair terms of each site, forces on the sites, half pair virial. */
+void orc_get_2b_energy_and_forces(int n_sites, const double *rjs, const double *xyz, int n_sparse,
+                                  const double *alphas, const double *cutoff, double rcut, double buffer,
+                                  double delta, double sigma, double e0, const double *Qs, const int *n_neigh,
+                                  int do_forces, const int *species, const int *neighbor_species, int sp1, int sp2,
+                                  int n_sites0, double *energies, double *forces, double *virial);
+/* get_core_pot_energy_and_forces (gap.f90:552-686) with the cubic spline of splines.f90:33-156. */
+void orc_get_core_pot_energy_and_forces(int n_sparse, int n_sites, int n_sites0, const double *rjs,
+                                        const double *xyz, const double *x, const double *V, double yp1,
+                                        double ypn, const double *dVdx2, const int *n_neigh, int do_forces,
+                                        const int *species, const int *neighbor_species, int sp1, int sp2,
+                                        double *energies, double *forces, double *virial);
+
 /* get_gap_soap (gap_interface.f90:41-433) for one SOAP model on the global neighbor list:
  * subset by rcut/species, central-species filter, get_soap, energies/forces, scatter back.
  * species_supercell: species channel (1..n_species) per supercell atom, 0 = blind.

@@ -75,6 +75,12 @@ def lib():
                                        C.c_double, C.c_int, _dp, _dp, _dp]
         L.orc_local_property_predict.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                                  C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp]
+        L.orc_get_2b_energy_and_forces.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double, C.c_double,
+                                                   C.c_double, C.c_double, C.c_double, _dp, _ip, C.c_int, _ip,
+                                                   _ip, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
+        L.orc_get_core_pot_energy_and_forces.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_double,
+                                                         C.c_double, _dp, _ip, C.c_int, _ip, _ip, C.c_int, C.c_int,
+                                                         _dp, _dp, _dp]
         L.orc_velocity_verlet.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double,
                                           C.POINTER(C.c_double), C.c_int]
         L.orc_mc_move_acceptance.restype = C.c_double
@@ -252,6 +258,63 @@ def local_property_predict(soap, Qs, alphas, V0, delta, zeta, soap_cart_der=None
                                      np.ascontiguousarray(alphas, float), V0, delta, zeta, int(do_der), der, nn,
                                      V, V_der)
     return V, (V_der[:P] if do_der else None)
+
+
+def get_2b_energy_and_forces(nb, species, sp1, sp2, alphas, cutoff, rcut, buffer, delta, sigma, e0, Qs,
+                             n_sites0=None, do_forces=True):
+    """get_2b_energy_and_forces on a neighbor-list dict; species per site (channel indices)."""
+    n = len(nb["n_neigh"])
+    n0 = n if n_sites0 is None else n_sites0
+    en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+    lib().orc_get_2b_energy_and_forces(
+        n, np.ascontiguousarray(nb["rjs"], float), np.ascontiguousarray(nb["xyz"], float), len(alphas),
+        np.ascontiguousarray(alphas, float), np.ascontiguousarray(cutoff, float), rcut, buffer, delta, sigma, e0,
+        np.ascontiguousarray(Qs, float), np.ascontiguousarray(nb["n_neigh"], np.int32), int(do_forces),
+        np.ascontiguousarray(species, np.int32), np.ascontiguousarray(nb["neighbor_species"], np.int32), sp1, sp2,
+        n0, en, fo, vir)
+    return en, fo, vir.reshape(3, 3, order="F")
+
+
+def get_core_pot_energy_and_forces(nb, species, sp1, sp2, x, V, yp1, ypn, dVdx2, n_sites0=None, do_forces=True):
+    n = len(nb["n_neigh"])
+    n0 = n if n_sites0 is None else n_sites0
+    en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+    lib().orc_get_core_pot_energy_and_forces(
+        len(x), n, n0, np.ascontiguousarray(nb["rjs"], float), np.ascontiguousarray(nb["xyz"], float),
+        np.ascontiguousarray(x, float), np.ascontiguousarray(V, float), yp1, ypn, np.ascontiguousarray(dVdx2, float),
+        np.ascontiguousarray(nb["n_neigh"], np.int32), int(do_forces), np.ascontiguousarray(species, np.int32),
+        np.ascontiguousarray(nb["neighbor_species"], np.int32), sp1, sp2, en, fo, vir)
+    return en, fo, vir.reshape(3, 3, order="F")
+
+
+def spline_second_derivatives(x, y, yp1, ypn):
+    """Second derivatives of the interpolating cubic spline (the tridiagonal solve of the standard
+    cubic spline, clamped end slopes yp1/ypn, natural ends when a slope is > 0.99e30), as TurboGAP's
+    model reader prepares dVdx2 for get_core_pot_energy_and_forces."""
+    x = np.asarray(x, float)
+    y = np.asarray(y, float)
+    n = len(x)
+    y2, u = np.zeros(n), np.zeros(n)
+    if yp1 > 0.99e30:
+        y2[0], u[0] = 0.0, 0.0
+    else:
+        y2[0] = -0.5
+        u[0] = (3.0 / (x[1] - x[0])) * ((y[1] - y[0]) / (x[1] - x[0]) - yp1)
+    for i in range(1, n - 1):
+        sig = (x[i] - x[i - 1]) / (x[i + 1] - x[i - 1])
+        p = sig * y2[i - 1] + 2.0
+        y2[i] = (sig - 1.0) / p
+        u[i] = (y[i + 1] - y[i]) / (x[i + 1] - x[i]) - (y[i] - y[i - 1]) / (x[i] - x[i - 1])
+        u[i] = (6.0 * u[i] / (x[i + 1] - x[i - 1]) - sig * u[i - 1]) / p
+    if ypn > 0.99e30:
+        qn, un = 0.0, 0.0
+    else:
+        qn = 0.5
+        un = (3.0 / (x[-1] - x[-2])) * (ypn - (y[-1] - y[-2]) / (x[-1] - x[-2]))
+    y2[-1] = (un - qn * u[-2]) / (qn * y2[-2] + 1.0)
+    for k in range(n - 2, -1, -1):
+        y2[k] = y2[k] * y2[k + 1] + u[k]
+    return y2
 
 
 def get_gap_soap(h, n_total_sites, nb, species_sc, central_species, alphas, Qs, delta, zeta,

@@ -392,3 +392,43 @@ def test_local_property_resident_matches_oracle(ctx, tg, synth, carbon, precisio
         assert np.all(Vd_g[start[i]:start[i + 1]] == 0.0)
     system.close()
     model.close()
+
+
+# ------------------------------------------------------------------------- pairwise terms
+
+def _sio2_pairs(synth):
+    pos, box, sp, _ = synth.random_packing(192, 2.2, {("Si", "O"): 1.4, ("O", "O"): 2.2, ("Si", "Si"): 2.5},
+                                           {"Si": 1 / 3, "O": 2 / 3}, seed=43)
+    nb = orc.build_neighbors(pos, len(pos), *box, 4.0, sp, False)
+    return nb, sp
+
+
+@pytest.mark.parametrize("species_pair", [(1, 2), (2, 2)])
+def test_2b_matches_oracle(ctx, synth, species_pair):
+    nb, sp = _sio2_pairs(synth)
+    rng = np.random.default_rng(7)
+    M = 15
+    args = dict(alphas=rng.normal(size=M) * 0.1, cutoff=rng.uniform(0.5, 1.0, M), rcut=4.0, buffer=0.6,
+                delta=1.1, sigma=0.4, e0=0.05, Qs=np.linspace(1.3, 3.8, M))
+    e_o, f_o, v_o = orc.get_2b_energy_and_forces(nb, sp, *species_pair, n_sites0=len(sp) + 5, **args)
+    e_g, f_g, v_g = ctx.get_2b_energy_and_forces(nb, sp, *species_pair, n_sites0=len(sp) + 5, **args)
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g - v_o)) < V_TOL
+    assert np.all(f_g[len(sp):] == 0.0)
+
+
+def test_core_pot_matches_oracle(ctx, synth):
+    nb, sp = _sio2_pairs(synth)
+    x = np.linspace(0.8, 3.5, 40)
+    Vk = 5.0 * np.exp(-2.0 * x) * (1.0 - x / 3.5) ** 2
+    yp1, ypn = -12.0, 0.0
+    y2 = orc.spline_second_derivatives(x, Vk, yp1, ypn)
+    for s1, s2 in ((1, 2), (1, 1)):
+        e_o, f_o, v_o = orc.get_core_pot_energy_and_forces(nb, sp, s1, s2, x, Vk, yp1, ypn, y2)
+        e_g, f_g, v_g = ctx.get_core_pot_energy_and_forces(nb, sp, s1, s2, x, Vk, yp1, ypn, y2)
+        assert np.max(np.abs(e_g - e_o)) < E_TOL
+        assert np.max(np.abs(f_g - f_o)) < F_TOL
+        assert np.max(np.abs(v_g - v_o)) < V_TOL
+    with pytest.raises(Exception):
+        ctx.get_core_pot_energy_and_forces(nb, sp, 1, 2, x[::-1], Vk, yp1, ypn, y2)

@@ -356,3 +356,74 @@ def test_local_property_predict_pinned_by_gap_forces_and_formula(orc, synth):
     # the integer-power path would differ by more than the rounding
     raw_int = d * d * (K ** 4) @ model["alphas"]
     assert np.max(np.abs(raw_int - raw)) > 1e3 * 1e-13 * np.max(np.abs(raw))
+
+
+def _sio2_box(synth, n=192, seed=41):
+    return synth.random_packing(n, 2.2, {("Si", "O"): 1.4, ("O", "O"): 2.2, ("Si", "Si"): 2.5},
+                                {"Si": 1 / 3, "O": 2 / 3}, seed=seed)[:3]
+
+
+def _pair_term_fd(orc, pos, box, sp, rc, term):
+    """Forces and virial of a pair term against central differences of the total energy (the sum
+    of the site energies) over atom moves and homogeneous strains."""
+    N = len(pos)
+
+    def ev(p, bx):
+        nb = orc.build_neighbors(p, N, *bx, rc, sp, False)
+        return term(nb)
+
+    e, f, v = ev(pos, box)
+    h = 1e-5
+    for i, x in [(0, 0), (17, 2), (101, 1)]:
+        pp, pm = pos.copy(), pos.copy()
+        pp[i, x] += h
+        pm[i, x] -= h
+        fd = -(ev(pp, box)[0].sum() - ev(pm, box)[0].sum()) / (2 * h)
+        assert abs(fd - f[i, x]) < 1e-7 * max(1.0, np.abs(f).max()), (i, x, fd, f[i, x])
+    for a, b in [(0, 0), (1, 2)]:
+        Fp, Fn = np.eye(3), np.eye(3)
+        Fp[a, b] += 1e-6
+        Fn[a, b] -= 1e-6
+        d = -(ev(pos @ Fp.T, box @ Fp.T)[0].sum() - ev(pos @ Fn.T, box @ Fn.T)[0].sum()) / 2e-6
+        assert abs(d - 0.5 * (v[a, b] + v[b, a])) < 1e-6 * max(1.0, np.abs(v).max()), (a, b, d, v)
+    assert abs(f.sum(axis=0)).max() < 1e-10 * max(1.0, np.abs(f).max())
+    return e, f, v
+
+
+def test_2b_energy_forces_virial_finite_differences(orc, synth):
+    """get_2b_energy_and_forces (gap.f90:329-460) on Si-O pairs of a SiO2 box: the site forces
+    are minus the gradient of the summed site energies (each pair counted from both ends) and the
+    halved pair virial minus its strain derivative; sites of other species get e0 and no force."""
+    pos, box, sp = _sio2_box(synth)
+    rng = np.random.default_rng(3)
+    M = 12
+    alphas, cutoff, Qs = rng.normal(size=M) * 0.1, rng.uniform(0.5, 1.0, M), np.linspace(1.3, 3.8, M)
+    args = dict(alphas=alphas, cutoff=cutoff, rcut=4.0, buffer=0.6, delta=1.1, sigma=0.4, e0=0.05, Qs=Qs)
+    e, f, _ = _pair_term_fd(orc, pos, box, sp, 4.0,
+                            lambda nb: orc.get_2b_energy_and_forces(nb, sp, 1, 2, **args))
+    nb = orc.build_neighbors(pos, len(pos), *box, 4.0, sp, False)
+    e_oo, f_oo, _ = orc.get_2b_energy_and_forces(nb, sp, 2, 2, **args)  # O-O term: Si sites untouched
+    assert np.all(e_oo[sp == 1] == 0.05) and np.all(f_oo[sp == 1] == 0.0)
+    assert np.any(e_oo[sp == 2] != 0.05)
+
+
+def test_core_pot_spline_energy_forces_virial(orc, synth):
+    """get_core_pot_energy_and_forces (gap.f90:552-686) with a clamped cubic spline of a smooth
+    repulsion: the spline reproduces its knots, and forces and virial are consistent with the
+    energy (finite differences)."""
+    pos, box, sp = _sio2_box(synth)
+    x = np.linspace(0.8, 3.5, 40)
+    Vk = 5.0 * np.exp(-2.0 * x) * (1.0 - x / 3.5) ** 2
+    dV = lambda r: 5.0 * np.exp(-2.0 * r) * ((1 - r / 3.5) ** 2 * -2.0 - 2.0 / 3.5 * (1 - r / 3.5))
+    yp1, ypn = dV(x[0]), dV(x[-1])
+    y2 = orc.spline_second_derivatives(x, Vk, yp1, ypn)
+    e, f, v = _pair_term_fd(orc, pos, box, sp, 4.0,
+                            lambda nb: orc.get_core_pot_energy_and_forces(nb, sp, 1, 2, x, Vk, yp1, ypn, y2))
+    # a two-atom box at knot distances returns the tabulated values (1/2 per atom)
+    for r in (x[5], x[17]):
+        p2 = np.array([[1.0, 1.0, 1.0], [1.0 + r, 1.0, 1.0]])
+        b2 = np.eye(3) * 12.0
+        nb2 = orc.build_neighbors(p2, 2, *b2, 4.0, np.array([1, 2], np.int32), False)
+        e2, _, _ = orc.get_core_pot_energy_and_forces(nb2, np.array([1, 2]), 1, 2, x, Vk, yp1, ypn, y2)
+        k = int(np.argmin(np.abs(x - r)))
+        assert abs(e2.sum() - Vk[k]) < 1e-12

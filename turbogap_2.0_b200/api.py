@@ -164,6 +164,34 @@ class Context:
             int(n_sites0), ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_soap_energy_and_forces")
         return en, fo, vir.reshape(3, 3, order="F")
 
+    def get_2b_energy_and_forces(self, nb, species, species1, species2, alphas, cutoff, rcut, buffer, delta, sigma,
+                                 e0, Qs, n_sites0=None, do_forces=True):
+        """get_2b_energy_and_forces on a neighbor-list dict (n_neigh, rjs, xyz, neighbor_species);
+        species per site and species1/2 as channel indices."""
+        nn = _i32(nb["n_neigh"])
+        n, P = len(nn), int(nn.sum())
+        n0 = n if n_sites0 is None else n_sites0
+        en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+        check(self._L.tgap_get_2b_energy_and_forces(
+            self.h, n, P, ptr(_f64(nb["rjs"])), ptr(_f64(nb["xyz"])), len(alphas), ptr(_f64(alphas)),
+            ptr(_f64(cutoff)), float(rcut), float(buffer), float(delta), float(sigma), float(e0), ptr(_f64(Qs)),
+            ptr(nn), int(do_forces), ptr(_i32(species)), ptr(_i32(nb["neighbor_species"])), int(species1),
+            int(species2), n0, ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_2b_energy_and_forces")
+        return en, fo, vir.reshape(3, 3, order="F")
+
+    def get_core_pot_energy_and_forces(self, nb, species, species1, species2, x, V, yp1, ypn, dVdx2, n_sites0=None,
+                                       do_forces=True):
+        nn = _i32(nb["n_neigh"])
+        n, P = len(nn), int(nn.sum())
+        n0 = n if n_sites0 is None else n_sites0
+        en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+        check(self._L.tgap_get_core_pot_energy_and_forces(
+            self.h, len(x), n, P, n0, ptr(_f64(nb["rjs"])), ptr(_f64(nb["xyz"])), ptr(_f64(x)), ptr(_f64(V)),
+            float(yp1), float(ypn), ptr(_f64(dVdx2)), ptr(nn), int(do_forces), ptr(_i32(species)),
+            ptr(_i32(nb["neighbor_species"])), int(species1), int(species2), ptr(en), ptr(fo), ptr(vir)),
+            self.h, "tgap_get_core_pot_energy_and_forces")
+        return en, fo, vir.reshape(3, 3, order="F")
+
     def local_property_predict(self, soap, Qs, alphas, V0, delta, zeta, soap_cart_der=None, n_neigh=None):
         """local_property_predict: soap (n_sites, D), Qs (M, D), soap_cart_der (P, D, 3) or None.
         Returns V (n_sites) and V_der (P, 3) or None."""

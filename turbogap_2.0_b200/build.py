@@ -36,6 +36,7 @@ SOURCES = [
     ("mc.cu", ["--fmad=false"]),
     ("screen.cu", []),
     ("screen_train.cu", []),
+    ("pair_terms.cu", []),
     ("tables.cpp", []),
 ]
 

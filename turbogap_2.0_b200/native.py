@@ -133,6 +133,11 @@ def lib():
         "tgap_local_property_predict": (i32, [vp, i32, i32, i32, vp, vp, vp, C.c_double, C.c_double, C.c_double,
                                               i32, vp, vp, i32, vp, vp]),
         "tgap_local_property": (i32, [vp, vp, vp, C.c_double, i32, i32, vp, vp]),
+        "tgap_get_2b_energy_and_forces": (i32, [vp, i32, i32, vp, vp, i32, vp, vp, C.c_double, C.c_double,
+                                                C.c_double, C.c_double, C.c_double, vp, vp, i32, vp, vp, i32, i32,
+                                                i32, vp, vp, vp]),
+        "tgap_get_core_pot_energy_and_forces": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp, C.c_double,
+                                                      C.c_double, vp, vp, i32, vp, vp, i32, i32, vp, vp, vp]),
         "tgap_autotune": (i32, [vp, vp, i32, vp, i32, i32]),
         "tgap_autotune_report": (i32, [vp, vp, i64, vp]),
         "tgap_autotune_clear": (i32, [vp]),
