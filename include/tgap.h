@@ -260,6 +260,22 @@ int tgap_get_core_pot_energy_and_forces(tgap_context *ctx, int n_sparse, int n_s
                                         const int *species, const int *neighbor_species, int species1,
                                         int species2, double *energies, double *forces, double *virial);
 
+/* get_3b_energy_and_forces (src/gap/gap.f90:756-1015): the angle_3b GAP on the triplets (i; j < k)
+ * of each species_center site with neighbors of species1 and species2 inside rcut, descriptor
+ * q = (r_ij + r_ik, (r_ij - r_ik)^2, r_jk), kernel_type 0 "exp" or 1 "pol" (cov_pp, d = 3, q = 1,
+ * :1022-1081); Qs is n_sparse x 3 (column-major), sigma[3]. Energies = e0 + the triplet terms of
+ * each site; forces (3 x n_sites0, overwritten) on the three atoms of each triplet, folded with
+ * mod(neighbors_list - 1, n_sites0); virial from the arms ij and ik. At most 512 eligible pairs per
+ * site. FP64. */
+int tgap_get_3b_energy_and_forces(tgap_context *ctx, int n_sites0, int n_sites, int n_atom_pairs,
+                                  const double *rjs, const double *xyz, int n_sparse,
+                                  const double *alphas, const double *cutoff, double rcut, double buffer,
+                                  double delta, const double *sigma, double e0, const double *Qs,
+                                  const int *n_neigh, const int *neighbors_list, int do_forces,
+                                  int kernel_type, const int *species, const int *neighbor_species,
+                                  int species_center, int species1, int species2, double *energies,
+                                  double *forces, double *virial);
+
 /* Resident form of local_property_predict (local_properties.f90:46-147, as get_gap_soap calls it,
  * gap_interface.f90:314-364) for a property model held as a tgap_model (its delta, zeta, alphas
  * and sparse set; the integer-zeta test of local_properties.f90): device pointers d_V (n_atoms;

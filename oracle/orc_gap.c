@@ -7,6 +7,7 @@
  *   local_property_predict       src/gap/local_properties.f90:46-147
  *   get_2b_energy_and_forces     src/gap/gap.f90:329-460
  *   get_core_pot_energy_and_forces src/gap/gap.f90:552-686 (spline, spline_der: src/utils/splines.f90:33-156)
+ *   get_3b_energy_and_forces     src/gap/gap.f90:756-1015 (cov_pp, cov_pp_der: :1022-1081)
  *   velocity_verlet              src/md/md_utils.f90:486-532
  *   monte_carlo_move             src/mc/mc_utils.f90:172-180 (+ min(1,p) of :255)
  */
@@ -308,6 +309,150 @@ void orc_get_core_pot_energy_and_forces(int n_sparse, int n_sites, int n_sites0,
         }
     }
     for (int q = 0; q < 9; ++q) virial[q] *= 0.5;
+}
+
+/* cov_pp / cov_pp_der (gap.f90:1022-1081) for d = 3, q = 1: j = 3 */
+static double cov_pp31(double r)
+{
+    if (r >= 1.0) return 0.0;
+    if (r <= 0.0) return 1.0;
+    return pow(1.0 - r, 4) * (4.0 * r + 1.0);
+}
+
+static double cov_pp31_der(double r) /* includes the 1/r factor */
+{
+    if (r >= 1.0 || r <= 0.0) return 0.0;
+    return (-4.0 * pow(1.0 - r, 3) * (4.0 * r + 1.0) + pow(1.0 - r, 4) * 4.0) / r;
+}
+
+void orc_get_3b_energy_and_forces(int n_sites0, int n_sites, const double *rjs, const double *xyz, int n_sparse,
+                                  const double *alphas, const double *cutoff, double rcut, double buffer,
+                                  double delta, const double *sigma, double e0, const double *Qs,
+                                  const int *n_neigh, const int *neighbors_list, int do_forces, int kernel_pol,
+                                  const int *species, const int *neighbor_species, int sp0, int sp1, int sp2,
+                                  double *energies, double *forces, double *virial)
+{
+    const double pi = acos(-1.0);
+    double *pref = (double *)malloc(sizeof(double) * (size_t)n_sparse);
+    double *rr = (double *)malloc(sizeof(double) * (size_t)n_sparse);
+    double *kern = (double *)malloc(sizeof(double) * (size_t)n_sparse);
+    double *kder = (double *)malloc(sizeof(double) * (size_t)n_sparse);
+    double *drdq = (double *)malloc(sizeof(double) * 3 * (size_t)n_sparse);
+    for (int s = 0; s < n_sparse; ++s) pref[s] = 2.0 * delta * delta * alphas[s] * cutoff[s]; /* :829 */
+    for (int i = 0; i < n_sites; ++i) energies[i] = e0;
+    if (do_forces) {
+        for (int x = 0; x < 3 * n_sites0; ++x) forces[x] = 0.0;
+        for (int x = 0; x < 9; ++x) virial[x] = 0.0;
+    }
+    int64_t k = 0;
+    for (int i = 0; i < n_sites; ++i) {
+        if (species[i] != sp0) {
+            k += n_neigh[i];
+            continue;
+        }
+        const int i3 = (neighbors_list[k] - 1) % n_sites0;
+        ++k;
+        for (int j = 1; j < n_neigh[i]; ++j, ++k) {
+            const double r12 = rjs[k];
+            if ((neighbor_species[k] != sp1 && neighbor_species[k] != sp2) || r12 > rcut) continue;
+            const int j3 = (neighbors_list[k] - 1) % n_sites0;
+            const double *x12 = xyz + 3 * k;
+            double x12r[3];
+            for (int c = 0; c < 3; ++c) x12r[c] = x12[c] / r12;
+            int64_t k2 = k;
+            for (int j2 = j + 1; j2 < n_neigh[i]; ++j2) {
+                ++k2;
+                const double r13 = rjs[k2];
+                const int ok = ((neighbor_species[k] == sp1 && neighbor_species[k2] == sp2) ||
+                                (neighbor_species[k] == sp2 && neighbor_species[k2] == sp1)) &&
+                               r13 < rcut;
+                if (!ok) continue;
+                const int k3 = (neighbors_list[k2] - 1) % n_sites0;
+                const double *x13 = xyz + 3 * k2;
+                double x13r[3], x23[3], x23r[3];
+                for (int c = 0; c < 3; ++c) {
+                    x13r[c] = x13[c] / r13;
+                    x23[c] = x13[c] - x12[c];
+                }
+                const double r23 = sqrt(x23[0] * x23[0] + x23[1] * x23[1] + x23[2] * x23[2]);
+                for (int c = 0; c < 3; ++c) x23r[c] = x23[c] / r23;
+                if (!(r12 < rcut && r13 < rcut)) continue;
+                double fcut12, fcut13, dfcut12[3], dfcut13[3];
+                if (r12 < rcut - buffer) {
+                    fcut12 = 1.0;
+                    dfcut12[0] = dfcut12[1] = dfcut12[2] = 0.0;
+                } else {
+                    fcut12 = (cos(pi * (r12 - rcut + buffer) / buffer) + 1.0) / 2.0;
+                    for (int c = 0; c < 3; ++c)
+                        dfcut12[c] = sin(pi * (r12 - rcut + buffer) / buffer) / 2.0 * pi / buffer * x12r[c];
+                }
+                if (r13 < rcut - buffer) {
+                    fcut13 = 1.0;
+                    dfcut13[0] = dfcut13[1] = dfcut13[2] = 0.0;
+                } else {
+                    fcut13 = (cos(pi * (r13 - rcut + buffer) / buffer) + 1.0) / 2.0;
+                    for (int c = 0; c < 3; ++c)
+                        dfcut13[c] = sin(pi * (r13 - rcut + buffer) / buffer) / 2.0 * pi / buffer * x13r[c];
+                }
+                const double fcut = fcut12 * fcut13;
+                double dfcut[3];
+                for (int c = 0; c < 3; ++c) dfcut[c] = fcut12 * dfcut13[c] + fcut13 * dfcut12[c];
+                const double q[3] = {r12 + r13, (r12 - r13) * (r12 - r13), r23};
+                for (int s = 0; s < n_sparse; ++s) {
+                    double a = 0.0;
+                    for (int c = 0; c < 3; ++c) {
+                        const double dq = q[c] - Qs[s + (size_t)c * n_sparse];
+                        a += dq * dq / (sigma[c] * sigma[c]);
+                        drdq[3 * s + c] = dq / (sigma[c] * sigma[c]);
+                    }
+                    rr[s] = sqrt(a);
+                    kern[s] = kernel_pol ? pref[s] * cov_pp31(rr[s]) : pref[s] * exp(-0.5 * rr[s] * rr[s]);
+                    if (kernel_pol) kder[s] = pref[s] * cov_pp31_der(rr[s]);
+                }
+                double ksum = 0.0;
+                for (int s = 0; s < n_sparse; ++s) ksum += kern[s];
+                energies[i] += fcut * ksum;
+                if (!do_forces) continue;
+                double f1[3], f2[3], f3[3];
+                for (int l = 0; l < 3; ++l) {
+                    double s1 = 0.0, s2 = 0.0, s3 = 0.0;
+                    for (int s = 0; s < n_sparse; ++s) {
+                        const double *d = drdq + 3 * s;
+                        const double dx1 = d[0] * (x12r[l] + x13r[l]) + d[1] * 2.0 * (r12 - r13) * (x12r[l] - x13r[l]);
+                        const double dx2 = -d[0] * x12r[l] - d[1] * 2.0 * (r12 - r13) * x12r[l] + d[2] * x23r[l];
+                        const double dx3 = -d[0] * x13r[l] - d[1] * 2.0 * (r13 - r12) * x13r[l] - d[2] * x23r[l];
+                        if (kernel_pol) {
+                            s1 += kern[s] * dfcut[l] - kder[s] * fcut * dx1;
+                            s2 += -kern[s] * fcut13 * dfcut12[l] - kder[s] * fcut * dx2;
+                            s3 += -kern[s] * fcut12 * dfcut13[l] - kder[s] * fcut * dx3;
+                        } else {
+                            s1 += kern[s] * (dfcut[l] + fcut * dx1);
+                            s2 += kern[s] * (-fcut13 * dfcut12[l] + fcut * dx2);
+                            s3 += kern[s] * (-fcut12 * dfcut13[l] + fcut * dx3);
+                        }
+                    }
+                    f1[l] = -s1;
+                    f2[l] = -s2;
+                    f3[l] = -s3;
+                }
+                for (int c = 0; c < 3; ++c) {
+                    forces[3 * i3 + c] += f1[c];
+                    forces[3 * j3 + c] += f2[c];
+                    forces[3 * k3 + c] += f3[c];
+                }
+                for (int a1 = 0; a1 < 3; ++a1)
+                    for (int a2 = 0; a2 < 3; ++a2) {
+                        virial[a1 + 3 * a2] += 0.5 * (f2[a1] * x12[a2] + f2[a2] * x12[a1]);
+                        virial[a1 + 3 * a2] += 0.5 * (f3[a1] * x13[a2] + f3[a2] * x13[a1]);
+                    }
+            }
+        }
+    }
+    free(pref);
+    free(rr);
+    free(kern);
+    free(kder);
+    free(drdq);
 }
 
 int orc_get_gap_soap(const orc_soap_hypers *h, int n_total_sites, int n_sites0,

@@ -144,6 +144,16 @@ void orc_get_core_pot_energy_and_forces(int n_sparse, int n_sites, int n_sites0,
                                         const int *species, const int *neighbor_species, int sp1, int sp2,
                                         double *energies, double *forces, double *virial);
 
+/* get_3b_energy_and_forces (gap.f90:756-1015): angle_3b GAP on triplets (i; j < k) of each
+ * species_center site; kernel_pol 0: "exp", 1: "pol" (cov_pp, d = 3, q = 1); Qs (n_sparse x 3,
+ * column-major), sigma[3]; forces (3 x n_sites0) on the folded triplet atoms. */
+void orc_get_3b_energy_and_forces(int n_sites0, int n_sites, const double *rjs, const double *xyz, int n_sparse,
+                                  const double *alphas, const double *cutoff, double rcut, double buffer,
+                                  double delta, const double *sigma, double e0, const double *Qs,
+                                  const int *n_neigh, const int *neighbors_list, int do_forces, int kernel_pol,
+                                  const int *species, const int *neighbor_species, int sp0, int sp1, int sp2,
+                                  double *energies, double *forces, double *virial);
+
 /* get_gap_soap (gap_interface.f90:41-433) for one SOAP model on the global neighbor list:
  * subset by rcut/species, central-species filter, get_soap, energies/forces, scatter back.
  * species_supercell: species channel (1..n_species) per supercell atom, 0 = blind.

@@ -81,6 +81,9 @@ def lib():
         L.orc_get_core_pot_energy_and_forces.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, _dp, C.c_double,
                                                          C.c_double, _dp, _ip, C.c_int, _ip, _ip, C.c_int, C.c_int,
                                                          _dp, _dp, _dp]
+        L.orc_get_3b_energy_and_forces.argtypes = [C.c_int, C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double,
+                                                   C.c_double, C.c_double, _dp, C.c_double, _dp, _ip, _ip, C.c_int,
+                                                   C.c_int, _ip, _ip, C.c_int, C.c_int, C.c_int, _dp, _dp, _dp]
         L.orc_velocity_verlet.argtypes = [C.c_int, _dp, _dp, _dp, _dp, _dp, _dp, C.c_double,
                                           C.POINTER(C.c_double), C.c_int]
         L.orc_mc_move_acceptance.restype = C.c_double
@@ -284,6 +287,22 @@ def get_core_pot_energy_and_forces(nb, species, sp1, sp2, x, V, yp1, ypn, dVdx2,
         np.ascontiguousarray(x, float), np.ascontiguousarray(V, float), yp1, ypn, np.ascontiguousarray(dVdx2, float),
         np.ascontiguousarray(nb["n_neigh"], np.int32), int(do_forces), np.ascontiguousarray(species, np.int32),
         np.ascontiguousarray(nb["neighbor_species"], np.int32), sp1, sp2, en, fo, vir)
+    return en, fo, vir.reshape(3, 3, order="F")
+
+
+def get_3b_energy_and_forces(nb, species, sp0, sp1, sp2, alphas, cutoff, rcut, buffer, delta, sigma, e0, Qs,
+                             kernel="exp", n_sites0=None, do_forces=True):
+    """get_3b_energy_and_forces on a neighbor-list dict; Qs (n_sparse, 3), sigma (3,)."""
+    n = len(nb["n_neigh"])
+    n0 = n if n_sites0 is None else n_sites0
+    en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+    lib().orc_get_3b_energy_and_forces(
+        n0, n, np.ascontiguousarray(nb["rjs"], float), np.ascontiguousarray(nb["xyz"], float), len(alphas),
+        np.ascontiguousarray(alphas, float), np.ascontiguousarray(cutoff, float), rcut, buffer, delta,
+        np.ascontiguousarray(sigma, float), e0, np.asfortranarray(Qs, float).ravel(order="F"),
+        np.ascontiguousarray(nb["n_neigh"], np.int32), np.ascontiguousarray(nb["neighbors_list"], np.int32),
+        int(do_forces), 1 if kernel == "pol" else 0, np.ascontiguousarray(species, np.int32),
+        np.ascontiguousarray(nb["neighbor_species"], np.int32), sp0, sp1, sp2, en, fo, vir)
     return en, fo, vir.reshape(3, 3, order="F")
 
 

@@ -432,3 +432,20 @@ def test_core_pot_matches_oracle(ctx, synth):
         assert np.max(np.abs(v_g - v_o)) < V_TOL
     with pytest.raises(Exception):
         ctx.get_core_pot_energy_and_forces(nb, sp, 1, 2, x[::-1], Vk, yp1, ypn, y2)
+
+
+@pytest.mark.parametrize("kernel,centre,pair", [("exp", 2, (2, 1)), ("pol", 2, (1, 1)), ("exp", 1, (2, 2))])
+def test_3b_matches_oracle(ctx, synth, kernel, centre, pair):
+    nb, sp = _sio2_pairs(synth)
+    rng = np.random.default_rng(11)
+    M = 12
+    Qs = np.stack([rng.uniform(3.0, 7.0, M), rng.uniform(0.0, 2.0, M), rng.uniform(2.0, 6.0, M)], axis=1)
+    sigma = np.array([1.0, 1.0, 1.2]) * (3.0 if kernel == "pol" else 1.0)
+    args = dict(alphas=rng.normal(size=M) * 0.05, cutoff=rng.uniform(0.5, 1.0, M), rcut=3.8, buffer=0.5,
+                delta=0.9, sigma=sigma, e0=0.02, Qs=Qs, kernel=kernel)
+    e_o, f_o, v_o = orc.get_3b_energy_and_forces(nb, sp, centre, *pair, **args)
+    e_g, f_g, v_g = ctx.get_3b_energy_and_forces(nb, sp, centre, *pair, **args)
+    assert np.abs(f_o).max() > 0.0
+    assert np.max(np.abs(e_g - e_o)) < E_TOL
+    assert np.max(np.abs(f_g - f_o)) < F_TOL
+    assert np.max(np.abs(v_g - v_o)) < V_TOL

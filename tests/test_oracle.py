@@ -427,3 +427,20 @@ def test_core_pot_spline_energy_forces_virial(orc, synth):
         e2, _, _ = orc.get_core_pot_energy_and_forces(nb2, np.array([1, 2]), 1, 2, x, Vk, yp1, ypn, y2)
         k = int(np.argmin(np.abs(x - r)))
         assert abs(e2.sum() - Vk[k]) < 1e-12
+
+
+@pytest.mark.parametrize("kernel", ["exp", "pol"])
+def test_3b_energy_forces_virial_finite_differences(orc, synth, kernel):
+    """get_3b_energy_and_forces (gap.f90:756-1015) for O-centred Si-O-Si-like triplets (centre O,
+    neighbors O and Si in either order) with both kernels: forces on the three atoms of every
+    triplet and the virial against finite differences of the summed site energies."""
+    pos, box, sp = _sio2_box(synth, seed=45)
+    rng = np.random.default_rng(5)
+    M = 10
+    Qs = np.stack([rng.uniform(3.0, 6.5, M), rng.uniform(0.0, 2.0, M), rng.uniform(2.0, 5.5, M)], axis=1)
+    sigma = np.array([1.0, 1.0, 1.2]) * (3.0 if kernel == "pol" else 1.0)
+    args = dict(alphas=rng.normal(size=M) * 0.05, cutoff=rng.uniform(0.5, 1.0, M), rcut=3.5, buffer=0.5,
+                delta=0.9, sigma=sigma, e0=0.02, Qs=Qs, kernel=kernel)
+    e, f, v = _pair_term_fd(orc, pos, box, sp, 3.5, lambda nb: orc.get_3b_energy_and_forces(nb, sp, 2, 2, 1, **args))
+    assert np.all(e[sp == 1] == 0.02)  # Si centres untouched
+    assert np.abs(f).max() > 0.0

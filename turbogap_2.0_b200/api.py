@@ -179,6 +179,22 @@ class Context:
             int(species2), n0, ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_2b_energy_and_forces")
         return en, fo, vir.reshape(3, 3, order="F")
 
+    def get_3b_energy_and_forces(self, nb, species, species_center, species1, species2, alphas, cutoff, rcut,
+                                 buffer, delta, sigma, e0, Qs, kernel="exp", n_sites0=None, do_forces=True):
+        """get_3b_energy_and_forces on a neighbor-list dict (with neighbors_list); Qs (n_sparse, 3)."""
+        nn = _i32(nb["n_neigh"])
+        n, P = len(nn), int(nn.sum())
+        n0 = n if n_sites0 is None else n_sites0
+        en, fo, vir = np.zeros(n), np.zeros((n0, 3)), np.zeros(9)
+        Qf = np.asfortranarray(Qs, dtype=np.float64).ravel(order="F")
+        check(self._L.tgap_get_3b_energy_and_forces(
+            self.h, n0, n, P, ptr(_f64(nb["rjs"])), ptr(_f64(nb["xyz"])), len(alphas), ptr(_f64(alphas)),
+            ptr(_f64(cutoff)), float(rcut), float(buffer), float(delta), ptr(_f64(sigma)), float(e0), ptr(Qf),
+            ptr(nn), ptr(_i32(nb["neighbors_list"])), int(do_forces), 1 if kernel == "pol" else 0,
+            ptr(_i32(species)), ptr(_i32(nb["neighbor_species"])), int(species_center), int(species1),
+            int(species2), ptr(en), ptr(fo), ptr(vir)), self.h, "tgap_get_3b_energy_and_forces")
+        return en, fo, vir.reshape(3, 3, order="F")
+
     def get_core_pot_energy_and_forces(self, nb, species, species1, species2, x, V, yp1, ypn, dVdx2, n_sites0=None,
                                        do_forces=True):
         nn = _i32(nb["n_neigh"])

@@ -1,12 +1,13 @@
-// Pairwise GAP terms on the neighbor list (FP64): the distance_2b GAP (gap.f90:329-460) and the
-// tabulated core potential with its cubic spline (gap.f90:552-686; splines.f90:33-156).
+// Pair and triplet GAP terms on the neighbor list (FP64): the distance_2b GAP (gap.f90:329-460),
+// the tabulated core potential with its cubic spline (gap.f90:552-686; splines.f90:33-156) and the
+// angle_3b GAP (gap.f90:756-1015, cov_pp of :1022-1081).
 //
-// One warp per site, lanes over the site's pairs (the self slot skipped, as the reference's
-// j = 2 .. n_neigh loop does). Each lane sums its pairs' energy, force and virial terms; the warp
-// reduces them in a fixed order, writes the site's energy and force (a full neighbor list gives
-// each pair to both of its atoms, so the force of a site comes from its own pairs only) and adds
-// its virial share with FP64 atomics. Both terms are a few hundred flops per pair: they are
-// latency-bound passes over the list, not worth fusing into the SOAP kernels.
+// Pair terms: one warp per site, lanes over the site's pairs (the self slot skipped, as the
+// reference's j = 2 .. n_neigh loop does). Each lane sums its pairs' energy, force and virial terms;
+// the warp reduces them in a fixed order, writes the site's energy and force (a full neighbor list
+// gives each pair to both of its atoms, so the force of a site comes from its own pairs only) and
+// adds its virial share with FP64 atomics. They are a few hundred flops per pair: latency-bound
+// passes over the list. The triplet term (k_triplet_3b) is described at its kernel.
 #include <cuda_runtime.h>
 
 #include <vector>
@@ -165,6 +166,152 @@ __global__ void k_pair_core_pot(int n_sites, const int64_t *__restrict__ start, 
     site_out(i, lane, e, f, v, 0.0, do_forces, energies, forces, virial);
 }
 
+constexpr int k3bMaxPairs = 512;  // eligible pairs of one site held in shared memory
+constexpr int k3bWarps = 4;
+
+// cov_pp (d = 3, q = 1) and its derivative with the 1/r factor (gap.f90:1022-1081)
+__device__ __forceinline__ double cov_pp31(double r)
+{
+    if (r >= 1.0) return 0.0;
+    if (r <= 0.0) return 1.0;
+    const double u = 1.0 - r;
+    return u * u * u * u * (4.0 * r + 1.0);
+}
+__device__ __forceinline__ double cov_pp31_der(double r)
+{
+    if (r >= 1.0 || r <= 0.0) return 0.0;
+    const double u = 1.0 - r;
+    return (-4.0 * u * u * u * (4.0 * r + 1.0) + u * u * u * u * 4.0) / r;
+}
+
+// One warp per site of species sp0. Its pairs with a neighbor of species sp1 or sp2 inside rcut
+// are compacted in list order; lanes then take the triplets (a < b in that order), each summing
+// over the sparse points K0 = sum kernel and G_c = sum w dr/dq_c (w = kernel for "exp", -kernel'
+// for "pol"), from which the three forces follow in closed form.
+__global__ void __launch_bounds__(32 * k3bWarps) k_triplet_3b(
+    int n_sites0, int n_sites, const int64_t *__restrict__ start, const double *__restrict__ rjs,
+    const double *__restrict__ xyz, const int *__restrict__ nl, const int *__restrict__ species,
+    const int *__restrict__ nsp, int sp0, int sp1, int sp2, int n_sparse, const double *__restrict__ pref,
+    const double *__restrict__ Qs, double is0, double is1, double is2, double rcut, double buffer, int kernel_pol,
+    double e0, int do_forces, double *__restrict__ energies, double *__restrict__ forces,
+    double *__restrict__ virial, int *check)
+{
+    __shared__ int pk[k3bWarps][k3bMaxPairs];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * k3bWarps + w;
+    if (i >= n_sites) return;
+    const double pi = 3.141592653589793;
+    double e = 0.0, v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+    if (species[i] == sp0) {
+        const int64_t kb = start[i], ke = start[i + 1];
+        const int i3 = (nl[kb] - 1) % n_sites0;
+        int n = 0;
+        for (int64_t k0 = kb + 1; k0 < ke; k0 += 32) {
+            const int64_t k = k0 + lane;
+            const bool ok = k < ke && (nsp[k] == sp1 || nsp[k] == sp2) && rjs[k] < rcut;
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            const int slot = n + __popc(m & ((1u << lane) - 1u));
+            if (ok) {
+                if (slot < k3bMaxPairs)
+                    pk[w][slot] = (int)(k - kb);
+                else
+                    check_fail(check, kCheckListOverrun, k, i);
+            }
+            n += __popc(m);
+        }
+        __syncwarp();
+        n = min(n, k3bMaxPairs);
+        const int T = n * (n - 1) / 2;
+        for (int t = lane; t < T; t += 32) {
+            int a = 0, rem = t;
+            while (rem >= n - 1 - a) {
+                rem -= n - 1 - a;
+                ++a;
+            }
+            const int64_t k = kb + pk[w][a], k2 = kb + pk[w][a + 1 + rem];
+            const int sj = nsp[k], sk = nsp[k2];
+            if (!((sj == sp1 && sk == sp2) || (sj == sp2 && sk == sp1))) continue;
+            const double r12 = rjs[k], r13 = rjs[k2];
+            const double x12[3] = {xyz[3 * k], xyz[3 * k + 1], xyz[3 * k + 2]};
+            const double x13[3] = {xyz[3 * k2], xyz[3 * k2 + 1], xyz[3 * k2 + 2]};
+            double x12r[3], x13r[3], x23[3];
+            for (int c = 0; c < 3; ++c) {
+                x12r[c] = x12[c] / r12;
+                x13r[c] = x13[c] / r13;
+                x23[c] = x13[c] - x12[c];
+            }
+            const double r23 = sqrt(x23[0] * x23[0] + x23[1] * x23[1] + x23[2] * x23[2]);
+            double fc12 = 1.0, fc13 = 1.0, dfc12[3] = {0.0, 0.0, 0.0}, dfc13[3] = {0.0, 0.0, 0.0};
+            if (!(r12 < rcut - buffer)) {
+                const double t12 = pi * (r12 - rcut + buffer) / buffer;
+                fc12 = (cos(t12) + 1.0) / 2.0;
+                for (int c = 0; c < 3; ++c) dfc12[c] = sin(t12) / 2.0 * pi / buffer * x12r[c];
+            }
+            if (!(r13 < rcut - buffer)) {
+                const double t13 = pi * (r13 - rcut + buffer) / buffer;
+                fc13 = (cos(t13) + 1.0) / 2.0;
+                for (int c = 0; c < 3; ++c) dfc13[c] = sin(t13) / 2.0 * pi / buffer * x13r[c];
+            }
+            const double fcut = fc12 * fc13;
+            const double q0 = r12 + r13, q1 = (r12 - r13) * (r12 - r13), q2 = r23;
+            double K0 = 0.0, G0 = 0.0, G1 = 0.0, G2 = 0.0;
+            for (int s = 0; s < n_sparse; ++s) {
+                const double d0 = q0 - Qs[s], d1 = q1 - Qs[n_sparse + s], d2 = q2 - Qs[2 * n_sparse + s];
+                const double a2 = d0 * d0 * is0 + d1 * d1 * is1 + d2 * d2 * is2;
+                double kern, wgt;
+                if (kernel_pol) {
+                    const double rr = sqrt(a2);
+                    kern = pref[s] * cov_pp31(rr);
+                    wgt = -pref[s] * cov_pp31_der(rr);
+                } else {
+                    kern = pref[s] * exp(-0.5 * a2);
+                    wgt = kern;
+                }
+                K0 += kern;
+                G0 += wgt * d0 * is0;
+                G1 += wgt * d1 * is1;
+                G2 += wgt * d2 * is2;
+            }
+            e += fcut * K0;
+            if (!do_forces) continue;
+            const int j3 = (nl[k] - 1) % n_sites0, k3 = (nl[k2] - 1) % n_sites0;
+            double f1[3], f2[3], f3[3];
+            const double x23r[3] = {x23[0] / r23, x23[1] / r23, x23[2] / r23};
+            for (int l = 0; l < 3; ++l) {
+                const double dfc = fc12 * dfc13[l] + fc13 * dfc12[l];
+                const double s1 = G0 * (x12r[l] + x13r[l]) + G1 * 2.0 * (r12 - r13) * (x12r[l] - x13r[l]);
+                const double s2 = -G0 * x12r[l] - G1 * 2.0 * (r12 - r13) * x12r[l] + G2 * x23r[l];
+                const double s3 = -G0 * x13r[l] - G1 * 2.0 * (r13 - r12) * x13r[l] - G2 * x23r[l];
+                f1[l] = -(K0 * dfc + fcut * s1);
+                f2[l] = -(-K0 * fc13 * dfc12[l] + fcut * s2);
+                f3[l] = -(-K0 * fc12 * dfc13[l] + fcut * s3);
+            }
+            for (int c = 0; c < 3; ++c) {
+                atomicAdd(forces + 3 * (size_t)i3 + c, f1[c]);
+                atomicAdd(forces + 3 * (size_t)j3 + c, f2[c]);
+                atomicAdd(forces + 3 * (size_t)k3 + c, f3[c]);
+            }
+            v[0] += f2[0] * x12[0] + f3[0] * x13[0];
+            v[1] += f2[1] * x12[1] + f3[1] * x13[1];
+            v[2] += f2[2] * x12[2] + f3[2] * x13[2];
+            v[3] += 0.5 * (f2[0] * x12[1] + f2[1] * x12[0] + f3[0] * x13[1] + f3[1] * x13[0]);
+            v[4] += 0.5 * (f2[0] * x12[2] + f2[2] * x12[0] + f3[0] * x13[2] + f3[2] * x13[0]);
+            v[5] += 0.5 * (f2[1] * x12[2] + f2[2] * x12[1] + f3[1] * x13[2] + f3[2] * x13[1]);
+        }
+    }
+    e = warp_sum(e);
+    if (lane == 0) energies[i] = e0 + e;
+    if (!do_forces) return;
+    for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
+    if (lane == 0) {
+        const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
+        for (int c = 0; c < 6; ++c) {
+            atomicAdd(virial + ia[c] + 3 * ib[c], v[c]);
+            if (ia[c] != ib[c]) atomicAdd(virial + ib[c] + 3 * ia[c], v[c]);
+        }
+    }
+}
+
 int up(tgap_context *ctx, DevBuf &b, const void *h, size_t bytes)
 {
     if (b.ensure(bytes ? bytes : 8)) return set_error(ctx, TGAP_ERR_NOMEM, "pair-term buffers");
@@ -179,10 +326,10 @@ int up(tgap_context *ctx, DevBuf &b, const void *h, size_t bytes)
     } while (0)
 
 struct PairBufs {
-    DevBuf start, rjs, xyz, species, nsp, a, b, c, d, e, f, out;
+    DevBuf start, rjs, xyz, species, nsp, nl, a, b, c, out;
     ~PairBufs()
     {
-        for (DevBuf *p : {&start, &rjs, &xyz, &species, &nsp, &a, &b, &c, &d, &e, &f, &out}) p->release();
+        for (DevBuf *p : {&start, &rjs, &xyz, &species, &nsp, &nl, &a, &b, &c, &out}) p->release();
     }
 };
 
@@ -291,6 +438,44 @@ extern "C" int tgap_get_core_pot_energy_and_forces(tgap_context *ctx, int n_spar
             n_sites, B.start.as<int64_t>(), B.rjs.as<double>(), B.xyz.as<double>(), B.species.as<int>(),
             B.nsp.as<int>(), species1, species2, n_sparse, B.a.as<double>(), B.b.as<double>(), yp1, ypn,
             B.c.as<double>(), rcut, do_forces, o, o + n_sites, o + n_sites + 3 * (size_t)n0);
+        TGAP_LAUNCH_CHECK(ctx);
+    }
+    return download_out(ctx, B, n_sites, n0, do_forces, energies, forces, virial);
+}
+
+extern "C" int tgap_get_3b_energy_and_forces(tgap_context *ctx, int n_sites0, int n_sites, int n_atom_pairs,
+                                             const double *rjs, const double *xyz, int n_sparse,
+                                             const double *alphas, const double *cutoff, double rcut, double buffer,
+                                             double delta, const double *sigma, double e0, const double *Qs,
+                                             const int *n_neigh, const int *neighbors_list, int do_forces,
+                                             int kernel_type, const int *species, const int *neighbor_species,
+                                             int species_center, int species1, int species2, double *energies,
+                                             double *forces, double *virial)
+{
+    if (!ctx) return TGAP_ERR_ARGUMENT;
+    if (n_sites < 0 || n_atom_pairs < 0 || n_sparse < 1 || n_sites0 < 1 || !rjs || !xyz || !alphas || !cutoff ||
+        !sigma || !Qs || !n_neigh || !neighbors_list || !species || !neighbor_species || !energies ||
+        !(sigma[0] > 0.0 && sigma[1] > 0.0 && sigma[2] > 0.0) || !(buffer > 0.0) ||
+        (kernel_type != 0 && kernel_type != 1) || (do_forces && (!forces || !virial)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_3b_energy_and_forces: bad arguments");
+    TGAP_CUDA(ctx, cudaSetDevice(ctx->device));
+    if (n_sites == 0) return TGAP_OK;
+    const int n0 = do_forces ? n_sites0 : 0;
+    PairBufs B;
+    PRC(upload_list(ctx, B, n_sites, n_atom_pairs, n_neigh, rjs, xyz, species, neighbor_species, n0));
+    PRC(up(ctx, B.nl, neighbors_list, sizeof(int) * (size_t)n_atom_pairs));
+    std::vector<double> pref(n_sparse);
+    for (int s = 0; s < n_sparse; ++s) pref[s] = 2.0 * delta * delta * alphas[s] * cutoff[s];  // gap.f90:829
+    PRC(up(ctx, B.a, pref.data(), sizeof(double) * n_sparse));
+    PRC(up(ctx, B.b, Qs, sizeof(double) * 3 * (size_t)n_sparse));
+    double *o = B.out.as<double>();
+    {
+        StageScope sc(ctx, "triplet_3b_f64");
+        k_triplet_3b<<<(n_sites + k3bWarps - 1) / k3bWarps, 32 * k3bWarps, 0, ctx->stream>>>(
+            n_sites0, n_sites, B.start.as<int64_t>(), B.rjs.as<double>(), B.xyz.as<double>(), B.nl.as<int>(),
+            B.species.as<int>(), B.nsp.as<int>(), species_center, species1, species2, n_sparse, B.a.as<double>(),
+            B.b.as<double>(), 1.0 / (sigma[0] * sigma[0]), 1.0 / (sigma[1] * sigma[1]), 1.0 / (sigma[2] * sigma[2]),
+            rcut, buffer, kernel_type, e0, do_forces, o, o + n_sites, o + n_sites + 3 * (size_t)n0, ctx->d_check);
         TGAP_LAUNCH_CHECK(ctx);
     }
     return download_out(ctx, B, n_sites, n0, do_forces, energies, forces, virial);

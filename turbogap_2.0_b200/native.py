@@ -136,6 +136,9 @@ def lib():
         "tgap_get_2b_energy_and_forces": (i32, [vp, i32, i32, vp, vp, i32, vp, vp, C.c_double, C.c_double,
                                                 C.c_double, C.c_double, C.c_double, vp, vp, i32, vp, vp, i32, i32,
                                                 i32, vp, vp, vp]),
+        "tgap_get_3b_energy_and_forces": (i32, [vp, i32, i32, i32, vp, vp, i32, vp, vp, C.c_double, C.c_double,
+                                                C.c_double, vp, C.c_double, vp, vp, vp, i32, i32, vp, vp, i32, i32,
+                                                i32, vp, vp, vp]),
         "tgap_get_core_pot_energy_and_forces": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp, C.c_double,
                                                       C.c_double, vp, vp, i32, vp, vp, i32, i32, vp, vp, vp]),
         "tgap_autotune": (i32, [vp, vp, i32, vp, i32, i32]),
