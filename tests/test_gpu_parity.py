@@ -449,3 +449,44 @@ def test_3b_matches_oracle(ctx, synth, kernel, centre, pair):
     assert np.max(np.abs(e_g - e_o)) < E_TOL
     assert np.max(np.abs(f_g - f_o)) < F_TOL
     assert np.max(np.abs(v_g - v_o)) < V_TOL
+
+
+def test_model_files_drive_the_device_path(ctx, tg, synth, carbon, tmp_path):
+    """A carbon soap_turbo model written as TurboGAP files (.gap + alphas + desc), read back by
+    gap_file and loaded on the device, gives the oracle's FP64 energies and forces."""
+    hyp, m = carbon
+    (tmp_path / "c.alphas").write_text("".join(f"{a:.17g}\n" for a in m["alphas"]))
+    (tmp_path / "c.desc").write_text("".join(f"{q:.17g}\n" for q in np.asarray(m["Qs"]).ravel()))
+    buf = hyp["rcut_hard"][0] - hyp["rcut_soft"][0]
+    (tmp_path / "c.gap").write_text(f"""gap_beg soap_turbo
+ n_species = 1
+ species = C
+ rcut = {hyp['rcut_hard'][0]}
+ buffer = {buf}
+ atom_sigma_r = {hyp['atom_sigma_r'][0]}
+ atom_sigma_t = {hyp['atom_sigma_t'][0]}
+ n_max = {hyp['alpha_max'][0]}
+ l_max = {hyp['l_max']}
+ zeta = 4
+ delta = 1.0
+ alphas_sparse = c.alphas
+ desc_sparse = c.desc
+gap_end
+""")
+    g = tg.gap_file.read_gap(str(tmp_path / "c.gap"), base_dir=str(tmp_path))
+    (model,) = tg.gap_file.load_soap_models(ctx, g)
+    pos, box, sp = synth.diamond_supercell(3, seed=37)
+    n = len(pos)
+    system = tg.System(ctx, [(pos, box, sp)], g["rcut_max"])
+    import torch
+    e = torch.zeros(n, dtype=torch.float64, device="cuda")
+    f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    v = torch.zeros(9, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    system.compute_device([model], tg.TGAP_FP64, e.data_ptr(), f.data_ptr(), v.data_ptr())
+    ctx.synchronize()
+    e_o, f_o, _ = helpers.oracle_structure_eval(hyp, [m], pos, box, sp)
+    assert np.max(np.abs(e.cpu().numpy() - e_o)) < E_TOL
+    assert np.max(np.abs(f.cpu().numpy().reshape(n, 3) - f_o)) < F_TOL
+    system.close()
+    model.close()

@@ -112,3 +112,92 @@ def test_bf16_round_is_round_to_nearest_even():
     assert r[2] == np.float32(1.0 + 2.0 ** -6)
     assert r[3] == -2.5
     assert abs(r[4] - 3.14159) < 2 ** -7 * 4
+
+
+def _write_model_files(d, rng):
+    """A .gap file with one block of each kind and its sparse-set files (TurboGAP's layout)."""
+    D, M = 12, 5
+    Qs = rng.random((M, D))
+    alphas = rng.normal(size=M)
+    (d / "soap.alphas").write_text("".join(f"{a:.17g}\n" for a in alphas))
+    (d / "soap.desc").write_text("".join(f"{q:.17g}\n" for q in Qs.ravel()))  # descriptor index fastest
+    a2, c2, q2 = rng.normal(size=4), rng.random(4), np.linspace(1.0, 3.0, 4)
+    (d / "b2.alphas").write_text("".join(f"{a:.17g} {c:.17g}\n" for a, c in zip(a2, c2)))
+    (d / "b2.desc").write_text("".join(f"{q:.17g}\n" for q in q2))
+    a3, c3, q3 = rng.normal(size=3), rng.random(3), rng.random((3, 3)) * 4
+    (d / "b3.alphas").write_text("".join(f"{a:.17g}, {c:.17g}\n" for a, c in zip(a3, c3)))
+    (d / "b3.desc").write_text("".join(f"{q:.17g}\n" for q in q3.ravel()))
+    x = np.linspace(0.5, 3.0, 11)
+    V = 4.0 * np.exp(-2.0 * x)
+    (d / "core.dat").write_text(f"11 1.0e31 0.0\n" + "".join(f"{a:.17g} {b:.17g}\n" for a, b in zip(x, V)))
+    (d / "model.gap").write_text(f"""# a model of every kind
+gap_beg soap_turbo
+  n_species = 2
+  species = C H
+  rcut = 3.7 3.0
+  buffer = 0.5 0.0
+  atom_sigma_r = 0.5 0.4
+  atom_sigma_t = 0.5 0.4
+  n_max = 4 2
+  l_max = 3
+  zeta = 4.0
+  delta = 0.2
+  central_species = 1
+  alphas_sparse = "soap.alphas"
+  desc_sparse = 'soap.desc'
+gap_end
+! a comment line
+gap_beg distance_2b
+  delta = 0.5
+  sigma = 0.3
+  rcut = 4.5
+  species1 = C
+  species2 = H
+  desc_sparse = b2.desc
+  alphas_sparse = b2.alphas
+gap_end
+gap_beg angle_3b
+  sigma = 1.0, 2.0, 3.0
+  rcut = 3.0
+  Z_center = C
+  Z1 = C
+  Z2 = H
+  kernel_type = pol
+  desc_sparse = b3.desc
+  alphas_sparse = b3.alphas
+gap_end
+gap_beg core_pot
+  species1 = C
+  species2 = C
+  core_pot_file = core.dat
+gap_end
+""")
+    return dict(Qs=Qs, alphas=alphas, a2=a2, c2=c2, q2=q2, a3=a3, c3=c3, q3=q3, x=x, V=V)
+
+
+def test_gap_file_reader(tg, tmp_path):
+    """read_gap on a file of every model kind: defaults, buffer -> rcut_soft, the sparse-set file
+    layouts and the core_pot table (natural start slope replaced by the spline's derivative)."""
+    import oracle_lib as orc
+    ref = _write_model_files(tmp_path, np.random.default_rng(0))
+    g = tg.gap_file.read_gap(str(tmp_path / "model.gap"), base_dir=str(tmp_path))
+    assert [len(g[k]) for k in ("soap_turbo", "distance_2b", "angle_3b", "core_pot")] == [1, 1, 1, 1]
+    s = g["soap_turbo"][0]
+    h = s["hypers"]
+    assert h["species"] == ["C", "H"] and h["alpha_max"] == [4, 2] and h["l_max"] == 3
+    assert h["rcut_hard"] == [3.7, 3.0] and h["rcut_soft"] == [3.2, 3.0]  # buffer 0 keeps rcut
+    assert h["nf"] == [4.0, 4.0] and h["amplitude_scaling"] == [1.0, 1.0] and h["atom_sigma_t_scaling"] == [0.0, 0.0]
+    assert s["zeta"] == 4.0 and s["delta"] == 0.2 and s["central_species"] == 1 and s["basis"] == "poly3"
+    assert np.array_equal(s["Qs"], ref["Qs"]) and np.array_equal(s["alphas"], ref["alphas"])
+    b2 = g["distance_2b"][0]
+    assert b2["buffer"] == 0.5 and b2["sigma"] == 0.3 and b2["species2"] == "H"
+    assert np.array_equal(b2["alphas"], ref["a2"]) and np.array_equal(b2["cutoff"], ref["c2"])
+    assert np.array_equal(b2["Qs"], ref["q2"])
+    b3 = g["angle_3b"][0]
+    assert b3["kernel_type"] == "pol" and list(b3["sigma"]) == [1.0, 2.0, 3.0] and b3["species_center"] == "C"
+    assert np.array_equal(b3["Qs"], ref["q3"]) and b3["delta"] == 1.0
+    cp = g["core_pot"][0]
+    y2 = orc.spline_second_derivatives(ref["x"], ref["V"], 1.0e31, 0.0)
+    assert np.allclose(cp["dVdx2"], y2, rtol=0, atol=1e-12)
+    assert cp["ypn"] == 0.0 and abs(cp["yp1"]) < 1e30  # natural start: slope taken from the spline
+    assert g["rcut_max"] == 4.5
