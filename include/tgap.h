@@ -286,6 +286,26 @@ int tgap_get_3b_energy_and_forces(tgap_context *ctx, int n_sites0, int n_sites, 
 int tgap_local_property(tgap_context *ctx, tgap_system *system, tgap_model *model, double V0,
                         int precision, int do_derivatives, double *d_V, double *d_V_der);
 
+/* Resident pair and triplet terms (the 2b / core_pot / 3b routines above, as calculate_gap_2b,
+ * calculate_gap_core_pot and calculate_gap_3b apply them, gap.f90:246-754): a set of terms held on
+ * the device, evaluated on a system's resident neighbor list (its cutoff must reach every term's)
+ * and ADDED to energies, forces and per-structure virial. With tgap_md_set_terms the MD step adds
+ * them after its SOAP models (full production GAPs: soap_turbo + 2b + 3b + core_pot). Species are
+ * channel indices. Qs of a 3b term is n_sparse x 3 column-major; kernel_type 0 "exp", 1 "pol". */
+typedef struct tgap_terms tgap_terms;
+int tgap_terms_create(tgap_context *ctx, tgap_terms **terms);
+int tgap_terms_destroy(tgap_terms *terms);
+int tgap_terms_add_2b(tgap_terms *terms, int species1, int species2, int n_sparse, const double *alphas,
+                      const double *cutoff, const double *Qs, double rcut, double buffer, double delta,
+                      double sigma, double e0);
+int tgap_terms_add_core_pot(tgap_terms *terms, int species1, int species2, int n, const double *x,
+                            const double *V, double yp1, double ypn, const double *dVdx2);
+int tgap_terms_add_3b(tgap_terms *terms, int species_center, int species1, int species2, int n_sparse,
+                      const double *alphas, const double *cutoff, const double *Qs, double rcut,
+                      double buffer, double delta, const double *sigma, double e0, int kernel_type);
+int tgap_terms_compute(tgap_context *ctx, tgap_system *system, tgap_terms *terms, int do_forces,
+                       double *d_energies, double *d_forces, double *d_virial);
+
 /* Autotuner (no counterpart in the reference, which has no GPU launch shapes to choose). Runs
  * tgap_compute on this system and these models once to collect the tunable launches (sites per
  * CTA of the descriptor forward and adjoint kernels; sparse-tile chunks per CTA of the fused GAP
@@ -326,6 +346,9 @@ int tgap_md_create(tgap_context *ctx, tgap_system *system, int n_models,
                    tgap_model *const *models, const double *masses_amu, double dt,
                    int rebuild_every, int precision, int use_graph, tgap_md **md);
 int tgap_md_destroy(tgap_md *md);
+/* Adds the terms (tgap_terms_*) to every MD force evaluation after the SOAP models; NULL removes
+ * them. The terms object must outlive its use by the MD object. */
+int tgap_md_set_terms(tgap_md *md, struct tgap_terms *terms);
 int tgap_md_set_velocities(tgap_md *md, const double *velocities);
 int tgap_md_run(tgap_md *md, int n_steps);
 /* Host copies of the current state; any pointer may be NULL. energies: potential and

@@ -12,7 +12,7 @@ from .native import TGAP_FP64, TGAP_MIXED, TgapError, LIB_PATH  # noqa: F401
 
 def __getattr__(name):
     # the GPU API loads libtgap.so on first use and raises if it is missing
-    if name in ("Context", "Model", "System", "MD", "MC", "assign_species", "api"):
+    if name in ("Context", "Model", "System", "MD", "MC", "Terms", "assign_species", "api"):
         api = importlib.import_module(__name__ + ".api")
         return api if name == "api" else getattr(api, name)
     raise AttributeError(name)

@@ -375,6 +375,58 @@ class System:
             pass
 
 
+class Terms:
+    """Pair and triplet GAP terms resident on the device (tgap_terms): distance_2b, core_pot and
+    angle_3b, added after the SOAP models. Species are channel indices (1-based)."""
+
+    def __init__(self, ctx):
+        self.ctx = ctx
+        h = C.c_void_p()
+        check(ctx._L.tgap_terms_create(ctx.h, C.byref(h)), ctx.h, "tgap_terms_create")
+        self.h = h
+        self._keep = []
+
+    def add_2b(self, species1, species2, alphas, cutoff, Qs, rcut, buffer=0.5, delta=1.0, sigma=1.0, e0=0.0):
+        a = [_f64(alphas), _f64(cutoff), _f64(Qs)]
+        check(self.ctx._L.tgap_terms_add_2b(self.h, int(species1), int(species2), len(a[0]), *[ptr(x) for x in a],
+                                            float(rcut), float(buffer), float(delta), float(sigma), float(e0)),
+              self.ctx.h, "tgap_terms_add_2b")
+
+    def add_core_pot(self, species1, species2, x, V, yp1, ypn, dVdx2):
+        a = [_f64(x), _f64(V)]
+        check(self.ctx._L.tgap_terms_add_core_pot(self.h, int(species1), int(species2), len(a[0]), ptr(a[0]),
+                                                  ptr(a[1]), float(yp1), float(ypn), ptr(_f64(dVdx2))),
+              self.ctx.h, "tgap_terms_add_core_pot")
+
+    def add_3b(self, species_center, species1, species2, alphas, cutoff, Qs, rcut, sigma, buffer=0.5, delta=1.0,
+               e0=0.0, kernel="exp"):
+        Qf = np.asfortranarray(Qs, dtype=np.float64).ravel(order="F")
+        a = [_f64(alphas), _f64(cutoff)]
+        check(self.ctx._L.tgap_terms_add_3b(self.h, int(species_center), int(species1), int(species2), len(a[0]),
+                                            ptr(a[0]), ptr(a[1]), ptr(Qf), float(rcut), float(buffer), float(delta),
+                                            ptr(_f64(sigma)), float(e0), 1 if kernel == "pol" else 0),
+              self.ctx.h, "tgap_terms_add_3b")
+
+    def compute_device(self, system, d_energies, d_forces, d_virial, do_forces=True):
+        """Adds the terms' energies, forces and virial into device arrays."""
+        check(self.ctx._L.tgap_terms_compute(self.ctx.h, system.h, self.h, int(do_forces), C.c_void_p(d_energies),
+                                             C.c_void_p(d_forces) if d_forces else None,
+                                             C.c_void_p(d_virial) if d_virial else None),
+              self.ctx.h, "tgap_terms_compute")
+
+    def close(self):
+        if getattr(self, "h", None):
+            if getattr(self.ctx, "h", None):
+                self.ctx._L.tgap_terms_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class MD:
     """NVE velocity-Verlet driver on the device (tgap_md)."""
 
@@ -403,6 +455,12 @@ class MD:
         check(self.ctx._L.tgap_md_get_state(self.h, ptr(pos), ptr(vel), ptr(f), C.byref(ep), C.byref(ek)),
               self.ctx.h, "md_get_state")
         return dict(positions=pos, velocities=vel, forces=f, e_pot=ep.value, e_kin=ek.value)
+
+    def set_terms(self, terms):
+        """Adds pair and triplet terms (Terms) to every force evaluation; None removes them."""
+        check(self.ctx._L.tgap_md_set_terms(self.h, terms.h if terms is not None else None), self.ctx.h,
+              "tgap_md_set_terms")
+        self._terms = terms
 
     def close(self):
         if getattr(self, "h", None):

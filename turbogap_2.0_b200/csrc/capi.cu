@@ -17,6 +17,7 @@
 #include "screen_kernels.h"
 #include "md_kernels.h"
 #include "neighbors.h"
+#include "pair_kernels.h"
 #include "soap_kernels.h"
 #include "tgap_internal.h"
 
@@ -740,6 +741,7 @@ struct tgap_system {
     NeighborBatch nb;
     double rcut;
     std::vector<int> host_species;
+    DevBuf d_species;  // species channel per site (pair and triplet terms), uploaded on first use
     std::vector<SiteSet> site_sets;
     DevBuf c, q, norm, q_hi, q_lo, e_rows;
     GapWork gw;
@@ -821,7 +823,7 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
-                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces};
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species};
     for (DevBuf *b : bufs) b->release();
     delete s;
     return TGAP_OK;
@@ -1287,10 +1289,16 @@ extern "C" int tgap_get_gap_soap(tgap_context *ctx, const tgap_soap_hypers *hype
 
 // ============================================================================ MD
 
+struct tgap_terms {
+    tgap_context *ctx;
+    TermSet set;
+};
+
 struct tgap_md {
     tgap_context *ctx;
     tgap_system *sys;
     std::vector<tgap_model *> models;
+    tgap_terms *terms = nullptr;  // pair and triplet terms added after the SOAP models
     int precision, rebuild_every, use_graph;
     double dt, dt_prev = 0.0;
     int64_t step = 0;
@@ -1302,10 +1310,27 @@ struct tgap_md {
     int64_t graph_kernels = 0;
 };
 
+static int terms_add(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_forces, double *d_e, double *d_f,
+                     double *d_v)
+{
+    if (t->set.rcut_max() > s->rcut)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "terms reach %g A, beyond the system's list cutoff %g A",
+                         t->set.rcut_max(), s->rcut);
+    if (!s->d_species.ptr) CHECK_RC(upload(ctx, s->d_species, s->host_species.data(), s->host_species.size()));
+    NeighborBatch &nb = s->nb;
+    return terms_compute(ctx, t->set, nb.n_atoms, nb.start.as<int64_t>(), nb.rjs.as<double>(), nb.xyz.as<double>(),
+                         s->d_species.as<int>(), nb.nspecies.as<int>(), nb.jatom.as<int>(), nb.site_struct.as<int>(),
+                         do_forces, d_e, d_f, d_v);
+}
+
 static int md_eval(tgap_md *md)
 {
-    return tgap_compute(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
-                        md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>());
+    CHECK_RC(tgap_compute(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
+                          md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>()));
+    if (md->terms)
+        CHECK_RC(terms_add(md->ctx, md->sys, md->terms, 1, md->energies.as<double>(), md->forces.as<double>(),
+                           md->virial.as<double>()));
+    return TGAP_OK;
 }
 
 // one step after the first: geometry refresh, forces, velocity Verlet
@@ -1317,6 +1342,146 @@ static int md_step_body(tgap_md *md)
     CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
                              md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),
                              md->forces_prev.as<double>(), md->mass.as<double>(), md->dt, md->dt, 0));
+    return TGAP_OK;
+}
+
+// ---------------------------------------------------------------------------- pair/triplet terms
+
+extern "C" int tgap_terms_create(tgap_context *ctx, tgap_terms **out)
+{
+    if (!ctx || !out) return TGAP_ERR_ARGUMENT;
+    auto *t = new tgap_terms();
+    t->ctx = ctx;
+    *out = t;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_terms_destroy(tgap_terms *t)
+{
+    if (!t) return TGAP_OK;
+    cudaSetDevice(t->ctx->device);
+    cudaStreamSynchronize(t->ctx->stream);
+    t->set.release();
+    delete t;
+    return TGAP_OK;
+}
+
+extern "C" int tgap_terms_add_2b(tgap_terms *t, int species1, int species2, int n_sparse, const double *alphas,
+                                 const double *cutoff, const double *Qs, double rcut, double buffer, double delta,
+                                 double sigma, double e0)
+{
+    if (!t) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = t->ctx;
+    CHECK_RC(activate(ctx));
+    if (n_sparse < 1 || !alphas || !cutoff || !Qs || !(rcut > 0) || !(buffer > 0) || !(sigma > 0))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_terms_add_2b: bad arguments");
+    Term2b b;
+    b.sp1 = species1;
+    b.sp2 = species2;
+    b.n_sparse = n_sparse;
+    b.rcut = rcut;
+    b.buffer = buffer;
+    b.delta = delta;
+    b.sigma = sigma;
+    b.e0 = e0;
+    int rc = upload(ctx, b.alphas, alphas, (size_t)n_sparse);
+    if (!rc) rc = upload(ctx, b.cutoff, cutoff, (size_t)n_sparse);
+    if (!rc) rc = upload(ctx, b.Qs, Qs, (size_t)n_sparse);
+    if (rc) {
+        for (DevBuf *p : {&b.alphas, &b.cutoff, &b.Qs}) p->release();
+        return rc;
+    }
+    t->set.t2b.push_back(b);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_terms_add_core_pot(tgap_terms *t, int species1, int species2, int n, const double *x,
+                                       const double *V, double yp1, double ypn, const double *dVdx2)
+{
+    if (!t) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = t->ctx;
+    CHECK_RC(activate(ctx));
+    if (n < 2 || !x || !V || !dVdx2) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_terms_add_core_pot: bad arguments");
+    TermCore c;
+    c.sp1 = species1;
+    c.sp2 = species2;
+    c.n = n;
+    c.yp1 = yp1;
+    c.ypn = ypn;
+    c.rcut = x[0];
+    for (int i = 1; i < n; ++i) {
+        if (!(x[i] > x[i - 1]))  // splines.f90 stops on h = 0
+            return set_error(ctx, TGAP_ERR_ARGUMENT, "core_pot table: x must increase (x[%d] <= x[%d])", i, i - 1);
+        c.rcut = std::max(c.rcut, x[i]);
+    }
+    int rc = upload(ctx, c.x, x, (size_t)n);
+    if (!rc) rc = upload(ctx, c.V, V, (size_t)n);
+    if (!rc) rc = upload(ctx, c.y2, dVdx2, (size_t)n);
+    if (rc) {
+        for (DevBuf *p : {&c.x, &c.V, &c.y2}) p->release();
+        return rc;
+    }
+    t->set.core.push_back(c);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_terms_add_3b(tgap_terms *t, int species_center, int species1, int species2, int n_sparse,
+                                 const double *alphas, const double *cutoff, const double *Qs, double rcut,
+                                 double buffer, double delta, const double *sigma, double e0, int kernel_type)
+{
+    if (!t) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = t->ctx;
+    CHECK_RC(activate(ctx));
+    if (n_sparse < 1 || !alphas || !cutoff || !Qs || !sigma || !(rcut > 0) || !(buffer > 0) ||
+        !(sigma[0] > 0 && sigma[1] > 0 && sigma[2] > 0) || (kernel_type != 0 && kernel_type != 1))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_terms_add_3b: bad arguments");
+    Term3b b;
+    b.sp0 = species_center;
+    b.sp1 = species1;
+    b.sp2 = species2;
+    b.n_sparse = n_sparse;
+    b.kernel = kernel_type;
+    b.rcut = rcut;
+    b.buffer = buffer;
+    b.e0 = e0;
+    for (int c = 0; c < 3; ++c) b.is[c] = 1.0 / (sigma[c] * sigma[c]);
+    std::vector<double> pref(n_sparse);
+    for (int s = 0; s < n_sparse; ++s) pref[s] = 2.0 * delta * delta * alphas[s] * cutoff[s];  // gap.f90:829
+    int rc = upload(ctx, b.pref, pref.data(), pref.size());
+    if (!rc) rc = upload(ctx, b.Qs, Qs, 3 * (size_t)n_sparse);
+    if (rc) {
+        for (DevBuf *p : {&b.pref, &b.Qs}) p->release();
+        return rc;
+    }
+    t->set.t3b.push_back(b);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_terms_compute(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_forces, double *d_energies,
+                                  double *d_forces, double *d_virial)
+{
+    CHECK_RC(activate(ctx));
+    if (!s || !t || !d_energies || (do_forces && (!d_forces || !d_virial)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_terms_compute: bad arguments");
+    return terms_add(ctx, s, t, do_forces, d_energies, d_forces, d_virial);
+}
+
+extern "C" int tgap_md_set_terms(tgap_md *md, tgap_terms *t)
+{
+    if (!md) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = md->ctx;
+    CHECK_RC(activate(ctx));
+    if (t && t->set.rcut_max() > md->sys->rcut)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "terms reach %g A, beyond the system's list cutoff %g A",
+                         t->set.rcut_max(), md->sys->rcut);
+    if (t && !md->sys->d_species.ptr)
+        CHECK_RC(upload(ctx, md->sys->d_species, md->sys->host_species.data(), md->sys->host_species.size()));
+    md->terms = t;
+    // the per-step graph changes
+    if (md->exec) cudaGraphExecDestroy(md->exec);
+    if (md->graph) cudaGraphDestroy(md->graph);
+    md->exec = nullptr;
+    md->graph = nullptr;
     return TGAP_OK;
 }
 

@@ -12,6 +12,7 @@
 
 #include <vector>
 
+#include "pair_kernels.h"
 #include "tgap_internal.h"
 
 namespace tgap {
@@ -42,17 +43,20 @@ __device__ __forceinline__ void virial_sym_add(double v[6], const double f[3], c
     v[5] -= 0.5 * (f[1] * r[2] + f[2] * r[1]);
 }
 
-// Site energy and force, and 1/2 of the pair virial (the reference's final halving), written out.
+// Site energy and force, and 1/2 of the pair virial (the reference's final halving), written out
+// (add != 0: added to the outputs, the resident evaluation summing several terms).
 __device__ __forceinline__ void site_out(int i, int lane, double e, double f[3], double v[6], double e_base,
-                                         int do_forces, double *energies, double *forces, double *virial)
+                                         int do_forces, int add, double *energies, double *forces, double *virial,
+                                         const int *site_struct)
 {
     e = warp_sum(e);
-    if (lane == 0) energies[i] = e_base + e;
+    if (lane == 0) energies[i] = (add ? energies[i] : 0.0) + e_base + e;
     if (!do_forces) return;
     for (int c = 0; c < 3; ++c) f[c] = warp_sum(f[c]);
     for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
     if (lane == 0) {
-        for (int c = 0; c < 3; ++c) forces[3 * (size_t)i + c] = f[c];
+        for (int c = 0; c < 3; ++c) forces[3 * (size_t)i + c] = (add ? forces[3 * (size_t)i + c] : 0.0) + f[c];
+        if (site_struct) virial += 9 * (size_t)site_struct[i];  // per structure of a batch
         const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
         for (int c = 0; c < 6; ++c) {
             const double h = 0.5 * v[c];
@@ -67,8 +71,8 @@ __global__ void k_pair_2b(int n_sites, const int64_t *__restrict__ start, const 
                           const int *__restrict__ nsp, int sp1, int sp2, int n_sparse,
                           const double *__restrict__ alphas, const double *__restrict__ cutoff,
                           const double *__restrict__ Qs, double rcut, double buffer, double delta, double sigma,
-                          double e0, int do_forces, double *__restrict__ energies, double *__restrict__ forces,
-                          double *__restrict__ virial)
+                          double e0, int do_forces, int add, double *__restrict__ energies,
+                          double *__restrict__ forces, double *__restrict__ virial, const int *__restrict__ site_struct)
 {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (i >= n_sites) return;
@@ -101,7 +105,7 @@ __global__ void k_pair_2b(int n_sites, const int64_t *__restrict__ start, const 
             }
         }
     }
-    site_out(i, lane, e, f, v, e0, do_forces, energies, forces, virial);
+    site_out(i, lane, e, f, v, e0, do_forces, add, energies, forces, virial, site_struct);
 }
 
 // Cubic spline of splines.f90 at r (x strictly increasing, n >= 2): value and derivative.
@@ -139,9 +143,9 @@ __global__ void k_pair_core_pot(int n_sites, const int64_t *__restrict__ start, 
                                 const double *__restrict__ xyz, const int *__restrict__ species,
                                 const int *__restrict__ nsp, int sp1, int sp2, int n, const double *__restrict__ x,
                                 const double *__restrict__ V, double yp1, double ypn,
-                                const double *__restrict__ dVdx2, double rcut, int do_forces,
+                                const double *__restrict__ dVdx2, double rcut, int do_forces, int add,
                                 double *__restrict__ energies, double *__restrict__ forces,
-                                double *__restrict__ virial)
+                                double *__restrict__ virial, const int *__restrict__ site_struct)
 {
     const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5), lane = threadIdx.x & 31;
     if (i >= n_sites) return;
@@ -163,7 +167,7 @@ __global__ void k_pair_core_pot(int n_sites, const int64_t *__restrict__ start, 
             }
         }
     }
-    site_out(i, lane, e, f, v, 0.0, do_forces, energies, forces, virial);
+    site_out(i, lane, e, f, v, 0.0, do_forces, add, energies, forces, virial, site_struct);
 }
 
 constexpr int k3bMaxPairs = 512;  // eligible pairs of one site held in shared memory
@@ -193,8 +197,8 @@ __global__ void __launch_bounds__(32 * k3bWarps) k_triplet_3b(
     const double *__restrict__ xyz, const int *__restrict__ nl, const int *__restrict__ species,
     const int *__restrict__ nsp, int sp0, int sp1, int sp2, int n_sparse, const double *__restrict__ pref,
     const double *__restrict__ Qs, double is0, double is1, double is2, double rcut, double buffer, int kernel_pol,
-    double e0, int do_forces, double *__restrict__ energies, double *__restrict__ forces,
-    double *__restrict__ virial, int *check)
+    double e0, int do_forces, int add, const int *__restrict__ jatom, double *__restrict__ energies,
+    double *__restrict__ forces, double *__restrict__ virial, const int *__restrict__ site_struct, int *check)
 {
     __shared__ int pk[k3bWarps][k3bMaxPairs];
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -204,7 +208,8 @@ __global__ void __launch_bounds__(32 * k3bWarps) k_triplet_3b(
     double e = 0.0, v[6] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
     if (species[i] == sp0) {
         const int64_t kb = start[i], ke = start[i + 1];
-        const int i3 = (nl[kb] - 1) % n_sites0;
+        // folded atoms: the list's atom map (resident lists) or mod(neighbors_list - 1, n_sites0)
+        const int i3 = jatom ? jatom[kb] : (nl[kb] - 1) % n_sites0;
         int n = 0;
         for (int64_t k0 = kb + 1; k0 < ke; k0 += 32) {
             const int64_t k = k0 + lane;
@@ -274,7 +279,8 @@ __global__ void __launch_bounds__(32 * k3bWarps) k_triplet_3b(
             }
             e += fcut * K0;
             if (!do_forces) continue;
-            const int j3 = (nl[k] - 1) % n_sites0, k3 = (nl[k2] - 1) % n_sites0;
+            const int j3 = jatom ? jatom[k] : (nl[k] - 1) % n_sites0;
+            const int k3 = jatom ? jatom[k2] : (nl[k2] - 1) % n_sites0;
             double f1[3], f2[3], f3[3];
             const double x23r[3] = {x23[0] / r23, x23[1] / r23, x23[2] / r23};
             for (int l = 0; l < 3; ++l) {
@@ -300,10 +306,11 @@ __global__ void __launch_bounds__(32 * k3bWarps) k_triplet_3b(
         }
     }
     e = warp_sum(e);
-    if (lane == 0) energies[i] = e0 + e;
+    if (lane == 0) energies[i] = (add ? energies[i] : 0.0) + e0 + e;
     if (!do_forces) return;
     for (int c = 0; c < 6; ++c) v[c] = warp_sum(v[c]);
     if (lane == 0) {
+        if (site_struct) virial += 9 * (size_t)site_struct[i];
         const int ia[6] = {0, 1, 2, 0, 0, 1}, ib[6] = {0, 1, 2, 1, 2, 2};
         for (int c = 0; c < 6; ++c) {
             atomicAdd(virial + ia[c] + 3 * ib[c], v[c]);
@@ -368,6 +375,39 @@ int download_out(tgap_context *ctx, PairBufs &B, int n_sites, int n_sites0, int 
 
 }  // namespace
 
+int terms_compute(tgap_context *ctx, const TermSet &t, int n_sites, const int64_t *d_start, const double *d_rjs,
+                  const double *d_xyz, const int *d_site_species, const int *d_nsp, const int *d_jatom,
+                  const int *d_site_struct, int do_forces, double *d_energies, double *d_forces, double *d_virial)
+{
+    if (n_sites <= 0) return TGAP_OK;
+    const int grid = (n_sites + 3) / 4;
+    for (const Term2b &b : t.t2b) {
+        StageScope sc(ctx, "pair_2b_f64");
+        k_pair_2b<<<grid, 128, 0, ctx->stream>>>(n_sites, d_start, d_rjs, d_xyz, d_site_species, d_nsp, b.sp1, b.sp2,
+                                                 b.n_sparse, b.alphas.as<double>(), b.cutoff.as<double>(),
+                                                 b.Qs.as<double>(), b.rcut, b.buffer, b.delta, b.sigma, b.e0,
+                                                 do_forces, 1, d_energies, d_forces, d_virial, d_site_struct);
+        TGAP_LAUNCH_CHECK(ctx);
+    }
+    for (const TermCore &c : t.core) {
+        StageScope sc(ctx, "pair_core_pot_f64");
+        k_pair_core_pot<<<grid, 128, 0, ctx->stream>>>(n_sites, d_start, d_rjs, d_xyz, d_site_species, d_nsp, c.sp1,
+                                                       c.sp2, c.n, c.x.as<double>(), c.V.as<double>(), c.yp1, c.ypn,
+                                                       c.y2.as<double>(), c.rcut, do_forces, 1, d_energies, d_forces,
+                                                       d_virial, d_site_struct);
+        TGAP_LAUNCH_CHECK(ctx);
+    }
+    for (const Term3b &b : t.t3b) {
+        StageScope sc(ctx, "triplet_3b_f64");
+        k_triplet_3b<<<(n_sites + k3bWarps - 1) / k3bWarps, 32 * k3bWarps, 0, ctx->stream>>>(
+            1, n_sites, d_start, d_rjs, d_xyz, nullptr, d_site_species, d_nsp, b.sp0, b.sp1, b.sp2, b.n_sparse,
+            b.pref.as<double>(), b.Qs.as<double>(), b.is[0], b.is[1], b.is[2], b.rcut, b.buffer, b.kernel, b.e0,
+            do_forces, 1, d_jatom, d_energies, d_forces, d_virial, d_site_struct, ctx->d_check);
+        TGAP_LAUNCH_CHECK(ctx);
+    }
+    return TGAP_OK;
+}
+
 }  // namespace tgap
 
 using namespace tgap;
@@ -399,7 +439,7 @@ extern "C" int tgap_get_2b_energy_and_forces(tgap_context *ctx, int n_sites, int
         k_pair_2b<<<(n_sites + 3) / 4, 128, 0, ctx->stream>>>(
             n_sites, B.start.as<int64_t>(), B.rjs.as<double>(), B.xyz.as<double>(), B.species.as<int>(),
             B.nsp.as<int>(), species1, species2, n_sparse, B.a.as<double>(), B.b.as<double>(), B.c.as<double>(), rcut,
-            buffer, delta, sigma, e0, do_forces, o, o + n_sites, o + n_sites + 3 * (size_t)n0);
+            buffer, delta, sigma, e0, do_forces, 0, o, o + n_sites, o + n_sites + 3 * (size_t)n0, nullptr);
         TGAP_LAUNCH_CHECK(ctx);
     }
     return download_out(ctx, B, n_sites, n0, do_forces, energies, forces, virial);
@@ -437,7 +477,7 @@ extern "C" int tgap_get_core_pot_energy_and_forces(tgap_context *ctx, int n_spar
         k_pair_core_pot<<<(n_sites + 3) / 4, 128, 0, ctx->stream>>>(
             n_sites, B.start.as<int64_t>(), B.rjs.as<double>(), B.xyz.as<double>(), B.species.as<int>(),
             B.nsp.as<int>(), species1, species2, n_sparse, B.a.as<double>(), B.b.as<double>(), yp1, ypn,
-            B.c.as<double>(), rcut, do_forces, o, o + n_sites, o + n_sites + 3 * (size_t)n0);
+            B.c.as<double>(), rcut, do_forces, 0, o, o + n_sites, o + n_sites + 3 * (size_t)n0, nullptr);
         TGAP_LAUNCH_CHECK(ctx);
     }
     return download_out(ctx, B, n_sites, n0, do_forces, energies, forces, virial);
@@ -475,7 +515,8 @@ extern "C" int tgap_get_3b_energy_and_forces(tgap_context *ctx, int n_sites0, in
             n_sites0, n_sites, B.start.as<int64_t>(), B.rjs.as<double>(), B.xyz.as<double>(), B.nl.as<int>(),
             B.species.as<int>(), B.nsp.as<int>(), species_center, species1, species2, n_sparse, B.a.as<double>(),
             B.b.as<double>(), 1.0 / (sigma[0] * sigma[0]), 1.0 / (sigma[1] * sigma[1]), 1.0 / (sigma[2] * sigma[2]),
-            rcut, buffer, kernel_type, e0, do_forces, o, o + n_sites, o + n_sites + 3 * (size_t)n0, ctx->d_check);
+            rcut, buffer, kernel_type, e0, do_forces, 0, nullptr, o, o + n_sites, o + n_sites + 3 * (size_t)n0,
+            nullptr, ctx->d_check);
         TGAP_LAUNCH_CHECK(ctx);
     }
     return download_out(ctx, B, n_sites, n0, do_forces, energies, forces, virial);

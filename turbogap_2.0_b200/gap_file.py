@@ -295,3 +295,21 @@ def load_soap_models(ctx, gap, precision_ready=True):
         models.append(Model(ctx, m["hypers"], m["Qs"], m["alphas"], m["delta"], m["zeta"],
                             central_species=m["central_species"]))
     return models
+
+
+def load_terms(ctx, gap, species):
+    """Device pair/triplet terms (api.Terms) of the distance_2b, angle_3b and core_pot blocks of a
+    read_gap result; `species` lists the species names in channel order (index 1 first), as the
+    system's species channels are numbered."""
+    from .api import Terms
+    idx = {name: i + 1 for i, name in enumerate(species)}
+    t = Terms(ctx)
+    for b in gap["distance_2b"]:
+        t.add_2b(idx[b["species1"]], idx[b["species2"]], b["alphas"], b["cutoff"], b["Qs"], b["rcut"],
+                 b["buffer"], b["delta"], b["sigma"], 0.0)
+    for c in gap["core_pot"]:
+        t.add_core_pot(idx[c["species1"]], idx[c["species2"]], c["x"], c["V"], c["yp1"], c["ypn"], c["dVdx2"])
+    for b in gap["angle_3b"]:
+        t.add_3b(idx[b["species_center"]], idx[b["species1"]], idx[b["species2"]], b["alphas"], b["cutoff"], b["Qs"],
+                 b["rcut"], b["sigma"], b["buffer"], b["delta"], 0.0, b["kernel_type"])
+    return t

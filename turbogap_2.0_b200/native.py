@@ -141,6 +141,15 @@ def lib():
                                                 i32, vp, vp, vp]),
         "tgap_get_core_pot_energy_and_forces": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, vp, C.c_double,
                                                       C.c_double, vp, vp, i32, vp, vp, i32, i32, vp, vp, vp]),
+        "tgap_terms_create": (i32, [vp, vp]),
+        "tgap_terms_destroy": (i32, [vp]),
+        "tgap_terms_add_2b": (i32, [vp, i32, i32, i32, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_double,
+                                    C.c_double]),
+        "tgap_terms_add_core_pot": (i32, [vp, i32, i32, i32, vp, vp, C.c_double, C.c_double, vp]),
+        "tgap_terms_add_3b": (i32, [vp, i32, i32, i32, i32, vp, vp, vp, C.c_double, C.c_double, C.c_double, vp,
+                                    C.c_double, i32]),
+        "tgap_terms_compute": (i32, [vp, vp, vp, i32, vp, vp, vp]),
+        "tgap_md_set_terms": (i32, [vp, vp]),
         "tgap_autotune": (i32, [vp, vp, i32, vp, i32, i32]),
         "tgap_autotune_report": (i32, [vp, vp, i64, vp]),
         "tgap_autotune_clear": (i32, [vp]),
