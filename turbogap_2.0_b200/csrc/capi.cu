@@ -905,8 +905,10 @@ static int ensure_eval_buffers(tgap_system *s, const tgap_model *m, int n_rows, 
     return TGAP_OK;
 }
 
+// geom: the descriptor forward writes this step's pair geometry from the primitive positions
+// (pure-replica systems; every site of the list must belong to some model's site set)
 static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m, int precision,
-                         int do_forces, double *d_energies, double *d_forces, double *d_virial)
+                         int do_forces, double *d_energies, double *d_forces, double *d_virial, bool geom = false)
 {
     SiteSet *ss = nullptr;
     CHECK_RC(site_set(s, m->central_species, &ss));
@@ -915,6 +917,15 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     CHECK_RC(ensure_eval_buffers(s, m, n_rows, precision));
     PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
                 s->nb.nspecies.as<int>(), s->nb.jatom.as<int>(), s->nb.n_atoms, ctx->d_check};
+    PairView pvf = pv;  // the forward's view, writing the geometry first when asked
+    if (geom) {
+        pvf.geo.pos = s->nb.positions.as<double>();
+        pvf.geo.list = s->nb.list.as<int>();
+        pvf.geo.site_struct = s->nb.site_struct.as<int>();
+        pvf.geo.sd = s->nb.d_structs.ptr;
+        pvf.geo.rjs_out = s->nb.rjs.as<double>();
+        pvf.geo.xyz_out = s->nb.xyz.as<double>();
+    }
     SoapOut o;
     o.c = s->c.ptr;
     o.q = s->q.ptr;
@@ -922,7 +933,7 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     const int *sites = ss->sites.as<int>();
     if (precision == TGAP_FP64) {
         o.q_ld = m->gap.dim;
-        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_FP64, o));
+        CHECK_RC(soap_forward(ctx, m->soap, pvf, sites, n_rows, TGAP_FP64, o));
         CHECK_RC(gap_energy_grad_f64(ctx, m->gap, (const double *)o.q, o.q_ld, n_rows, 0.0, do_forces,
                                      &s->gw, sites, nullptr, d_energies));
         if (do_forces)
@@ -933,7 +944,7 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
         o.q_ld = m->gap.dim_pad;
         o.q_hi = s->q_hi.as<__nv_bfloat16>();
         o.q_lo = s->q_lo.as<__nv_bfloat16>();
-        CHECK_RC(soap_forward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o));
+        CHECK_RC(soap_forward(ctx, m->soap, pvf, sites, n_rows, TGAP_MIXED, o));
         CHECK_RC(gap_energy_grad_mixed(ctx, m->gap, o.q_hi, o.q_lo, n_rows, 0.0, do_forces, &s->gw, sites,
                                        nullptr, d_energies));
         if (do_forces)
@@ -943,9 +954,20 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     return TGAP_OK;
 }
 
+static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                          int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
+                          bool geom);
+
 extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                             int precision, int do_forces, double *d_energies, double *d_forces,
                             double *d_virial)
+{
+    return compute_models(ctx, s, n_models, models, precision, do_forces, d_energies, d_forces, d_virial, false);
+}
+
+static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                          int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
+                          bool geom)
 {
     CHECK_RC(activate(ctx));
     if (!s || n_models <= 0 || !models || !d_energies || (do_forces && (!d_forces || !d_virial)))
@@ -959,7 +981,7 @@ extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tga
         TGAP_CUDA(ctx, cudaMemsetAsync(d_virial, 0, sizeof(double) * 9 * s->nb.n_structures, ctx->stream));
     }
     for (int i = 0; i < n_models; ++i)
-        CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial));
+        CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial, geom));
     return TGAP_OK;
 }
 
@@ -1299,6 +1321,9 @@ struct tgap_md {
     tgap_system *sys;
     std::vector<tgap_model *> models;
     tgap_terms *terms = nullptr;  // pair and triplet terms added after the SOAP models
+    // the descriptor forward writes each step's pair geometry (no separate geometry pass): a
+    // pure-replica system whose sites all belong to some model, and no pair/triplet terms
+    bool fused_geom = false;
     int precision, rebuild_every, use_graph;
     double dt, dt_prev = 0.0;
     int64_t step = 0;
@@ -1323,10 +1348,24 @@ static int terms_add(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_fo
                          do_forces, d_e, d_f, d_v);
 }
 
+static bool md_can_fuse_geometry(const tgap_md *md)
+{
+    if (!md->sys->nb.replicated || md->terms) return false;
+    std::vector<int> covered;
+    for (const tgap_model *m : md->models) {
+        if (m->central_species == 0) return true;
+        covered.push_back(m->central_species);
+    }
+    for (int sp : md->sys->host_species)
+        if (std::find(covered.begin(), covered.end(), sp) == covered.end()) return false;
+    return true;
+}
+
 static int md_eval(tgap_md *md)
 {
-    CHECK_RC(tgap_compute(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
-                          md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>()));
+    CHECK_RC(compute_models(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
+                            md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>(),
+                            md->fused_geom));
     if (md->terms)
         CHECK_RC(terms_add(md->ctx, md->sys, md->terms, 1, md->energies.as<double>(), md->forces.as<double>(),
                            md->virial.as<double>()));
@@ -1337,7 +1376,7 @@ static int md_eval(tgap_md *md)
 static int md_step_body(tgap_md *md)
 {
     tgap_context *ctx = md->ctx;
-    CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
+    if (!md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     CHECK_RC(md_eval(md));
     CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
                              md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),
@@ -1477,6 +1516,7 @@ extern "C" int tgap_md_set_terms(tgap_md *md, tgap_terms *t)
     if (t && !md->sys->d_species.ptr)
         CHECK_RC(upload(ctx, md->sys->d_species, md->sys->host_species.data(), md->sys->host_species.size()));
     md->terms = t;
+    md->fused_geom = md_can_fuse_geometry(md);
     // the per-step graph changes
     if (md->exec) cudaGraphExecDestroy(md->exec);
     if (md->graph) cudaGraphDestroy(md->graph);
@@ -1497,6 +1537,7 @@ extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models,
     md->sys = sys;
     md->models.assign(models, models + n_models);
     md->precision = precision;
+    md->fused_geom = md_can_fuse_geometry(md);
     md->rebuild_every = rebuild_every;
     md->use_graph = use_graph;
     md->dt = dt;
@@ -1552,6 +1593,8 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
             CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
             int64_t n_pairs = 0;
             CHECK_RC(neighbors_rebuild_lists(ctx, &md->sys->nb, -1, &n_pairs));
+            // the per-pair species and atom maps of the new lists (the step refreshes geometry)
+            if (md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
         }
         if (md->first) {
             // eager first step: it sizes every buffer

@@ -26,6 +26,7 @@
 #include <algorithm>
 #include <type_traits>
 
+#include "neighbors_device.cuh"
 #include "soap_device.cuh"
 #include "soap_kernels.h"
 
@@ -161,7 +162,7 @@ __device__ __forceinline__ bool pair_accept(const SoapParams &P, int64_t k, cons
 {
     const int s = nsp[k] - 1;
     if (s < 0 || s >= P.n_species || (only_s >= 0 && s != only_s)) return false;
-    const double r = rjs[k];
+    const double r = __ldcg(rjs + k);  // L2-coherent: the forward may have written it this launch
     return r > 0.0 && r < P.rcut_hard[s];
 }
 
@@ -423,7 +424,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
     const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
     T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
-    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check)
+    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check, GeomSrc geo)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int ASTR = AStride<NLM>::value;
@@ -441,6 +442,27 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
 
     const int site = sites ? sites[row] : row;
     const int64_t kb = start[site], ke = start[site + 1];
+    if (geo.pos) {
+        // this step's pair geometry from the primitive positions (what the neighbor module's
+        // geometry pass would write), read back below through L2-coherent loads
+        const StructDesc &S = static_cast<const StructDesc *>(geo.sd)[geo.site_struct[site]];
+        double pi[3];
+        sc_position(S, geo.pos, site - S.atom_off + 1, pi);
+        for (int64_t k = kb + lane; k < ke; k += 32) {
+            double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
+            if (k > kb) {
+                double pj[3];
+                sc_position(S, geo.pos, geo.list[k], pj);
+                get_distance_dev(pi, pj, S, dist, &d);
+            }
+            geo.rjs_out[k] = d;
+            geo.xyz_out[3 * k] = dist[0];
+            geo.xyz_out[3 * k + 1] = dist[1];
+            geo.xyz_out[3 * k + 2] = dist[2];
+        }
+        __threadfence_block();
+        __syncwarp();
+    }
     for (int s = 0; s < P.n_species; ++s) {
         T acc[KPL][AMB];
 #pragma unroll
@@ -455,11 +477,11 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
                 const int64_t k = idx[lane];
                 const bool in_site = k > kb && k < ke;
                 if (!in_site) check_fail(check, kCheckFwdPair, k, site);
-                const double rd = in_site ? rjs[k] : 1.0;
+                const double rd = in_site ? __ldcg(rjs + k) : 1.0;
                 const T r = (T)rd, ir = (T)1 / r;
-                const T ux = in_site ? (T)xyz[3 * k] * ir : (T)0;
-                const T uy = in_site ? (T)xyz[3 * k + 1] * ir : (T)0;
-                const T uz = in_site ? (T)xyz[3 * k + 2] * ir : (T)1;
+                const T ux = in_site ? (T)__ldcg(xyz + 3 * k) * ir : (T)0;
+                const T uy = in_site ? (T)__ldcg(xyz + 3 * k + 1) * ir : (T)0;
+                const T uz = in_site ? (T)__ldcg(xyz + 3 * k + 2) * ir : (T)1;
                 T R[AMB], dR[AMB];
                 radial_values<T, AMB, false>(P, s, rd, xq, tq, rtab, R, dR);
                 T *Rrow = Rs + lane * AMB;
@@ -826,7 +848,7 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     kern<<<grid, 32 * nw, sm, ctx->stream>>>(
         ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
         soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c,
-        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check);
+        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check, pv.geo);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

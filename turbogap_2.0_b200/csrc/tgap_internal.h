@@ -212,6 +212,18 @@ int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, Dev
 // ---------------------------------------------------------------------------- pairs
 
 // Read-only view of a neighbor list for the descriptor kernels.
+// Descriptor forward only: with pos set, each site's warp first writes the minimum-image pair
+// vectors and distances of its list pairs (rjs_out / xyz_out, the arrays the view reads) from the
+// primitive positions, so a per-step geometry pass is not needed. sd: const StructDesc *.
+struct GeomSrc {
+    const double *pos = nullptr;
+    const int *list = nullptr;
+    const int *site_struct = nullptr;
+    const void *sd = nullptr;
+    double *rjs_out = nullptr;
+    double *xyz_out = nullptr;
+};
+
 struct PairView {
     const int64_t *start;   // [n_sites_total + 1]
     const double *xyz;      // [3 P]  r_j - r_i (minimum image)
@@ -224,6 +236,7 @@ struct PairView {
     // pair, self slot = minus the sum) instead of being scattered into forces and virial
     double *pair_der = nullptr;
     const double *gate = nullptr;  // with pair_der: sites whose gate value is 0 write nothing
+    GeomSrc geo;                   // descriptor forward: pair geometry from positions
 };
 
 }  // namespace tgap
