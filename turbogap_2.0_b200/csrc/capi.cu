@@ -944,9 +944,16 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
         o.q_ld = m->gap.dim_pad;
         o.q_hi = s->q_hi.as<__nv_bfloat16>();
         o.q_lo = s->q_lo.as<__nv_bfloat16>();
+        // the fused GAP kernel accumulates dE/dq: the forward clears each row it writes
+        const bool clear_g = do_forces && m->gap.dim_pad <= 384;
+        if (clear_g) {
+            const size_t rows_pad = ((size_t)n_rows + 127) / 128 * 128;
+            if (s->gw.g.ensure(4 * rows_pad * m->gap.dim_pad)) return set_error(ctx, TGAP_ERR_NOMEM, "dE/dq rows");
+            o.g_clear = s->gw.g.as<float>();
+        }
         CHECK_RC(soap_forward(ctx, m->soap, pvf, sites, n_rows, TGAP_MIXED, o));
         CHECK_RC(gap_energy_grad_mixed(ctx, m->gap, o.q_hi, o.q_lo, n_rows, 0.0, do_forces, &s->gw, sites,
-                                       nullptr, d_energies));
+                                       nullptr, d_energies, nullptr, clear_g));
         if (do_forces)
             CHECK_RC(soap_backward(ctx, m->soap, pv, sites, n_rows, TGAP_MIXED, o, s->gw.g.ptr,
                                    m->gap.dim_pad, 0, s->nb.site_struct.as<int>(), d_forces, d_virial));
@@ -954,20 +961,22 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     return TGAP_OK;
 }
 
+// zeroed: the caller cleared the outputs already (the MD step clears its contiguous block at once)
 static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                           int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
-                          bool geom);
+                          bool geom, bool zeroed);
 
 extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                             int precision, int do_forces, double *d_energies, double *d_forces,
                             double *d_virial)
 {
-    return compute_models(ctx, s, n_models, models, precision, do_forces, d_energies, d_forces, d_virial, false);
+    return compute_models(ctx, s, n_models, models, precision, do_forces, d_energies, d_forces, d_virial, false,
+                          false);
 }
 
 static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                           int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
-                          bool geom)
+                          bool geom, bool zeroed)
 {
     CHECK_RC(activate(ctx));
     if (!s || n_models <= 0 || !models || !d_energies || (do_forces && (!d_forces || !d_virial)))
@@ -975,8 +984,8 @@ static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_
     if (precision != TGAP_FP64 && precision != TGAP_MIXED)
         return set_error(ctx, TGAP_ERR_ARGUMENT, "precision");
     const int N = s->nb.n_atoms;
-    TGAP_CUDA(ctx, cudaMemsetAsync(d_energies, 0, sizeof(double) * N, ctx->stream));
-    if (do_forces) {
+    if (!zeroed) TGAP_CUDA(ctx, cudaMemsetAsync(d_energies, 0, sizeof(double) * N, ctx->stream));
+    if (do_forces && !zeroed) {
         TGAP_CUDA(ctx, cudaMemsetAsync(d_forces, 0, sizeof(double) * 3 * N, ctx->stream));
         TGAP_CUDA(ctx, cudaMemsetAsync(d_virial, 0, sizeof(double) * 9 * s->nb.n_structures, ctx->stream));
     }
@@ -1321,6 +1330,7 @@ struct tgap_md {
     tgap_system *sys;
     std::vector<tgap_model *> models;
     tgap_terms *terms = nullptr;  // pair and triplet terms added after the SOAP models
+    DevBuf out;  // forces (3 N), energies (N), virial (9 per structure), contiguous: one clear per step
     // the descriptor forward writes each step's pair geometry (no separate geometry pass): a
     // pure-replica system whose sites all belong to some model, and no pair/triplet terms
     bool fused_geom = false;
@@ -1363,9 +1373,10 @@ static bool md_can_fuse_geometry(const tgap_md *md)
 
 static int md_eval(tgap_md *md)
 {
+    TGAP_CUDA(md->ctx, cudaMemsetAsync(md->out.ptr, 0, md->out.bytes, md->ctx->stream));
     CHECK_RC(compute_models(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
                             md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>(),
-                            md->fused_geom));
+                            md->fused_geom, true));
     if (md->terms)
         CHECK_RC(terms_add(md->ctx, md->sys, md->terms, 1, md->energies.as<double>(), md->forces.as<double>(),
                            md->virial.as<double>()));
@@ -1545,12 +1556,24 @@ extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models,
     std::vector<double> m(N);
     for (int i = 0; i < N; ++i) m[i] = masses_amu[i] * 103.6426965268;  // read_files.f90:333
     int rc = upload(ctx, md->mass, m.data(), (size_t)N);
-    DevBuf *bufs[] = {&md->vel, &md->forces, &md->forces_prev, &md->pos_prev};
+    DevBuf *bufs[] = {&md->vel, &md->forces_prev, &md->pos_prev};
     for (DevBuf *b : bufs)
         if (!rc && (b->ensure(sizeof(double) * 3 * N) || cudaMemsetAsync(b->ptr, 0, sizeof(double) * 3 * N, ctx->stream)))
             rc = TGAP_ERR_NOMEM;
-    if (!rc && (md->energies.ensure(sizeof(double) * N) || md->virial.ensure(sizeof(double) * 9 * sys->nb.n_structures)))
+    // forces, energies and virial share one block (views into md->out, never resized)
+    const size_t n_out = 4 * (size_t)N + 9 * (size_t)sys->nb.n_structures;
+    if (!rc && (md->out.ensure(sizeof(double) * n_out) ||
+                cudaMemsetAsync(md->out.ptr, 0, sizeof(double) * n_out, ctx->stream)))
         rc = TGAP_ERR_NOMEM;
+    if (!rc) {
+        double *o = md->out.as<double>();
+        md->forces.ptr = o;
+        md->forces.bytes = sizeof(double) * 3 * (size_t)N;
+        md->energies.ptr = o + 3 * (size_t)N;
+        md->energies.bytes = sizeof(double) * (size_t)N;
+        md->virial.ptr = o + 4 * (size_t)N;
+        md->virial.bytes = sizeof(double) * 9 * (size_t)sys->nb.n_structures;
+    }
     if (rc) {
         tgap_md_destroy(md);
         return rc;
@@ -1565,7 +1588,7 @@ extern "C" int tgap_md_destroy(tgap_md *md)
     cudaSetDevice(md->ctx->device);
     if (md->exec) cudaGraphExecDestroy(md->exec);
     if (md->graph) cudaGraphDestroy(md->graph);
-    DevBuf *bufs[] = {&md->mass, &md->vel, &md->forces, &md->forces_prev, &md->pos_prev, &md->energies, &md->virial};
+    DevBuf *bufs[] = {&md->mass, &md->vel, &md->forces_prev, &md->pos_prev, &md->out};
     for (DevBuf *b : bufs) b->release();
     delete md;
     return TGAP_OK;

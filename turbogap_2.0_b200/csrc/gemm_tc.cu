@@ -958,7 +958,8 @@ int model_upload_mixed(tgap_context *ctx, DeviceModel *m)
 
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces, GapWork *w,
-                          const int *d_sites, double *d_e_rows, double *d_energies, const int *d_skip)
+                          const int *d_sites, double *d_e_rows, double *d_energies, const int *d_skip,
+                          bool g_cleared)
 {
     if (n_rows <= 0) return TGAP_OK;
     constexpr int BN1 = 128;  // m_pad is a multiple of 128; 256-column tiles when it allows
@@ -972,7 +973,7 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
     const bool zi = std::fabs(m.zeta - zr) < m.zeta_tol;  // gap.f90:99-105 (local properties: :76-77)
     if (m.dim_pad <= 384 && m.m_pad % 128 == 0) {
         // fused: G never leaves the SM (k_gap_flash); dE/dq accumulates with atomics
-        if (do_forces)
+        if (do_forces && !g_cleared)
             TGAP_CUDA(ctx, cudaMemsetAsync(w->g.ptr, 0, 4 * (size_t)rows_pad * m.dim_pad, ctx->stream));
         FlashGap p;
         p.alphas = m.alphas32.as<float>();

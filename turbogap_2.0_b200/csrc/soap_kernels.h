@@ -15,6 +15,7 @@ struct SoapOut {
     int q_ld = 0;
     __nv_bfloat16 *q_hi = nullptr;  // optional bf16 split of q for the tensor-core GEMM
     __nv_bfloat16 *q_lo = nullptr;
+    float *g_clear = nullptr;  // optional: row r of this [n_rows][q_ld] FP32 accumulator is zeroed
 };
 
 int upload_ylm_constants();

@@ -424,7 +424,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
     const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
     T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
-    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check, GeomSrc geo)
+    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check, GeomSrc geo,
+    float *__restrict__ g_clear)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int ASTR = AStride<NLM>::value;
@@ -552,6 +553,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     const T nrm = t_sqrt<T>(part);
     const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
     __syncwarp();
+    // the row of the dE/dq accumulator the GAP kernel adds into (saves a separate clear)
+    if (g_clear)
+        for (int d = lane; d < q_ld; d += 32) g_clear[(size_t)row * q_ld + d] = 0.0f;
     for (int d = lane; d < q_ld; d += 32) {
         const T qv = d < dim ? ps[d] * inv : (T)0;
         q_out[(size_t)row * q_ld + d] = qv;
@@ -848,7 +852,7 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     kern<<<grid, 32 * nw, sm, ctx->stream>>>(
         ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
         soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c,
-        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check, pv.geo);
+        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check, pv.geo, o.g_clear);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
