@@ -525,6 +525,7 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                                  ((uint32_t)(kBM >> 4) << 24);
     constexpr uint32_t kCols = 512;
     const bool forces = p.g != nullptr;
+    pdl_enter();  // q, the cleared dE/dq rows and the skip flag come from earlier kernels
     if (p.skip && *p.skip) return;  // uniform over the grid, before any TMEM or barrier set-up
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
@@ -904,8 +905,8 @@ static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bflo
     std::snprintf(key, sizeof(key), "gap_fused/dp%d/bs%d/row_tiles%d/sparse_tiles%d", DP, BS, n_rt, J);
     const int nc = tuned(ctx, key, "gemm_bf16x3_fused", divisors, flash_chunks(n_rt, J, sm_count(ctx)));
     StageScope sc(ctx, "gemm_bf16x3_fused");
-    kern<<<n_rt * nc, kFlashThreads, Sh::SMEM, ctx->stream>>>(tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc,
-                                                             p, ctx->d_flag);
+    TGAP_CUDA(ctx, launch_pdl(kern, dim3(n_rt * nc), dim3(kFlashThreads), Sh::SMEM, ctx->stream, tq_hi, tq_lo, tQ_hi,
+                              tQ_lo, tT_hi, tT_lo, nc, J / nc, p, ctx->d_flag));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

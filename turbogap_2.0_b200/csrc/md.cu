@@ -13,6 +13,7 @@ __global__ void k_velocity_verlet(int n, double *__restrict__ pos, double *__res
                                   double *__restrict__ f_prev, const double *__restrict__ mass,
                                   double dt, double dt_prev, int first_step, int *check)
 {
+    pdl_enter();
     const int g = blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= 3 * n) return;
     const int i = g / 3;
@@ -35,9 +36,8 @@ int velocity_verlet(tgap_context *ctx, int n, double *pos, double *pos_prev, dou
     if (n <= 0) return TGAP_OK;
     const int T = 256;
     StageScope sc(ctx, "velocity_verlet");
-    k_velocity_verlet<<<(3 * n + T - 1) / T, T, 0, ctx->stream>>>(n, pos, pos_prev, vel, forces,
-                                                                  forces_prev, mass, dt, dt_prev,
-                                                                  first_step, ctx->d_check);
+    TGAP_CUDA(ctx, launch_pdl(k_velocity_verlet, dim3((3 * n + T - 1) / T), dim3(T), 0, ctx->stream, n, pos,
+                              pos_prev, vel, forces, forces_prev, mass, dt, dt_prev, first_step, ctx->d_check));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -431,6 +431,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     constexpr int ASTR = AStride<NLM>::value;
     constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int row = blockIdx.x * nw + warp;
     if (row >= n_rows) return;  // no CTA-wide synchronisation in this kernel
@@ -603,6 +604,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
+    pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
     const int row = blockIdx.x * nw + warp;
     // pair-derivative mode: a site whose gate is 0 writes nothing (its pairs stay zero)
@@ -849,10 +851,11 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     auto kern = k_soap_fwd_warp<T, L, AMB, SPLIT>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = (n_rows + nw - 1) / nw;
-    kern<<<grid, 32 * nw, sm, ctx->stream>>>(
-        ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
-        soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, (T *)o.c,
-        (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check, pv.geo, o.g_clear);
+    TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
+                              soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
+                              soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz,
+                              pv.species, (T *)o.c, (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check,
+                              pv.geo, o.g_clear));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
@@ -873,11 +876,11 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     auto kern = k_soap_bwd_warp<T, GT, L, AMB>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = (n_rows + nw - 1) / nw;
-    kern<<<grid, 32 * nw, sm, ctx->stream>>>(
-        ds.p, ylm_host_constants(), soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
-        d_sites, n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
-        (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial, (int)wb, pv.n_atoms,
-        pv.check, pv.pair_der, pv.gate);
+    TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
+                              soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(), d_sites,
+                              n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
+                              (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial,
+                              (int)wb, pv.n_atoms, pv.check, pv.pair_der, pv.gate));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

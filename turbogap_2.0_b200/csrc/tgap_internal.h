@@ -149,6 +149,35 @@ enum CheckCode {
 };
 
 #ifdef __CUDACC__
+// Programmatic dependent launch, at the top of a kernel launched with launch_pdl: wait until the
+// preceding kernel's grid has completed and its memory is visible, then allow the next kernel to
+// be scheduled (it holds at its own wait until this grid completes). Outside such a launch both
+// instructions do nothing.
+__device__ __forceinline__ void pdl_enter()
+{
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+// Launches kern with programmatic stream serialization: its blocks may be scheduled while the
+// preceding kernel finishes; kern must call pdl_enter() before reading that kernel's output.
+template <typename... KArgs, typename... Args>
+inline cudaError_t launch_pdl(void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream,
+                              Args... args)
+{
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, kern, args...);
+}
+
 // Records the first failure (code, index, value) and counts all of them; the access that failed
 // is skipped by the caller.
 __device__ __forceinline__ void check_fail(int *check, int code, long long index, long long value)
