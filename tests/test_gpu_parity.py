@@ -490,3 +490,29 @@ gap_end
     assert np.max(np.abs(f.cpu().numpy().reshape(n, 3) - f_o)) < F_TOL
     system.close()
     model.close()
+
+
+def test_md_multi_step_graph_matches_single_steps(ctx, tg, synth, carbon):
+    """md.run(20) sends the rebuild-free stretches (9 steps) as one graph launch; the trajectory
+    matches twenty md.run(1) calls (single-step graphs) to 1e-9 A (only the order of FP64 atomic
+    additions can differ)."""
+    hyp, m = carbon
+    pos, box, sp = synth.diamond_supercell(3, seed=39)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    masses = np.full(len(pos), 12.011)
+    vel = np.random.default_rng(4).normal(size=(len(pos), 3)) * 0.01
+    out = []
+    for chunked in (False, True):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+        md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=10, precision=tg.TGAP_MIXED)
+        md.set_velocities(vel)
+        if chunked:
+            md.run(20)
+        else:
+            for _ in range(20):
+                md.run(1)
+        out.append(md.state())
+        md.close()
+        system.close()
+    assert np.max(np.abs(out[0]["positions"] - out[1]["positions"])) < 1e-9
+    assert abs(out[0]["e_pot"] - out[1]["e_pot"]) < 1e-9

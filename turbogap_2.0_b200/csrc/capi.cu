@@ -1343,6 +1343,11 @@ struct tgap_md {
     cudaGraphExec_t exec = nullptr;
     uint64_t graph_epoch = 0;  // allocation epoch the graph was captured at
     int64_t graph_kernels = 0;
+    // the steps between two list rebuilds (rebuild_every - 1 of them) as one graph
+    cudaGraph_t graph_run = nullptr;
+    cudaGraphExec_t exec_run = nullptr;
+    uint64_t run_epoch = 0;
+    int64_t run_kernels = 0;
 };
 
 static int terms_add(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_forces, double *d_e, double *d_f,
@@ -1528,11 +1533,15 @@ extern "C" int tgap_md_set_terms(tgap_md *md, tgap_terms *t)
         CHECK_RC(upload(ctx, md->sys->d_species, md->sys->host_species.data(), md->sys->host_species.size()));
     md->terms = t;
     md->fused_geom = md_can_fuse_geometry(md);
-    // the per-step graph changes
+    // the step graphs change
     if (md->exec) cudaGraphExecDestroy(md->exec);
     if (md->graph) cudaGraphDestroy(md->graph);
+    if (md->exec_run) cudaGraphExecDestroy(md->exec_run);
+    if (md->graph_run) cudaGraphDestroy(md->graph_run);
     md->exec = nullptr;
     md->graph = nullptr;
+    md->exec_run = nullptr;
+    md->graph_run = nullptr;
     return TGAP_OK;
 }
 
@@ -1588,6 +1597,8 @@ extern "C" int tgap_md_destroy(tgap_md *md)
     cudaSetDevice(md->ctx->device);
     if (md->exec) cudaGraphExecDestroy(md->exec);
     if (md->graph) cudaGraphDestroy(md->graph);
+    if (md->exec_run) cudaGraphExecDestroy(md->exec_run);
+    if (md->graph_run) cudaGraphDestroy(md->graph_run);
     DevBuf *bufs[] = {&md->mass, &md->vel, &md->forces_prev, &md->pos_prev, &md->out};
     for (DevBuf *b : bufs) b->release();
     delete md;
@@ -1603,6 +1614,36 @@ extern "C" int tgap_md_set_velocities(tgap_md *md, const double *v)
     return TGAP_OK;
 }
 
+// Captures n_steps step bodies into one graph (re-captured when an allocation moved a buffer).
+static int md_graph(tgap_md *md, int n_steps, cudaGraph_t *graph, cudaGraphExec_t *exec, uint64_t *epoch,
+                    int64_t *kernels)
+{
+    tgap_context *ctx = md->ctx;
+    if (*exec && *epoch == g_alloc_epoch.load(std::memory_order_relaxed)) return TGAP_OK;
+    if (*exec) cudaGraphExecDestroy(*exec);
+    if (*graph) cudaGraphDestroy(*graph);
+    *exec = nullptr;
+    *graph = nullptr;
+    const uint64_t e0 = g_alloc_epoch.load(std::memory_order_relaxed);
+    TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+    const int64_t launches = ctx->launches;
+    int rc = TGAP_OK;
+    for (int i = 0; i < n_steps && !rc; ++i) rc = md_step_body(md);
+    cudaGraph_t g = nullptr;
+    cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+    *kernels = ctx->launches - launches;
+    ctx->launches = launches;
+    if (rc) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess) return cuda_check(ctx, ce, "graph capture");
+    *graph = g;
+    TGAP_CUDA(ctx, cudaGraphInstantiate(exec, g, 0));
+    *epoch = e0;
+    return TGAP_OK;
+}
+
 extern "C" int tgap_md_run(tgap_md *md, int n_steps)
 {
     if (!md || n_steps < 0) return TGAP_ERR_ARGUMENT;
@@ -1610,6 +1651,17 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
     CHECK_RC(activate(ctx));
     for (int it = 0; it < n_steps; ++it) {
         const bool rebuild = (md->step % md->rebuild_every) == 0;
+        // a full run of rebuild-free steps goes out as one graph launch
+        const int run = md->rebuild_every - 1;
+        if (md->use_graph && !md->first && !rebuild && run > 1 && md->step % md->rebuild_every == 1 &&
+            n_steps - it >= run) {
+            CHECK_RC(md_graph(md, run, &md->graph_run, &md->exec_run, &md->run_epoch, &md->run_kernels));
+            TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_run, ctx->stream));
+            ctx->launches += md->run_kernels;
+            md->step += run;
+            it += run - 1;
+            continue;
+        }
         if (!md->first && rebuild) {
             // new pair lists on the current positions (one host synchronization for the pair
             // count); the step below refreshes the geometry on them like any other step
@@ -1629,27 +1681,7 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
                                      md->first ? 1 : 0));
             md->first = false;
         } else if (md->use_graph) {
-            if (!md->exec || md->graph_epoch != g_alloc_epoch.load(std::memory_order_relaxed)) {
-                if (md->exec) cudaGraphExecDestroy(md->exec);
-                if (md->graph) cudaGraphDestroy(md->graph);
-                md->exec = nullptr;
-                md->graph = nullptr;
-                TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
-                const int64_t launches = ctx->launches;
-                int rc = md_step_body(md);
-                cudaGraph_t g = nullptr;
-                cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
-                md->graph_kernels = ctx->launches - launches;
-                ctx->launches = launches;
-                if (rc) {
-                    if (g) cudaGraphDestroy(g);
-                    return rc;
-                }
-                if (ce != cudaSuccess) return cuda_check(ctx, ce, "graph capture");
-                md->graph = g;
-                TGAP_CUDA(ctx, cudaGraphInstantiate(&md->exec, g, 0));
-                md->graph_epoch = g_alloc_epoch.load(std::memory_order_relaxed);
-            }
+            CHECK_RC(md_graph(md, 1, &md->graph, &md->exec, &md->graph_epoch, &md->graph_kernels));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec, ctx->stream));
             ctx->launches += md->graph_kernels;
         } else {
