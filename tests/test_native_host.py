@@ -201,3 +201,38 @@ def test_gap_file_reader(tg, tmp_path):
     assert np.allclose(cp["dVdx2"], y2, rtol=0, atol=1e-12)
     assert cp["ypn"] == 0.0 and abs(cp["yp1"]) < 1e30  # natural start: slope taken from the spline
     assert g["rcut_max"] == 4.5
+
+
+def test_extended_xyz_read_and_round_trip(tg, tmp_path):
+    """An extended-XYZ frame as TurboGAP files hold them (case-insensitive keys, quoted Lattice,
+    Properties with a column to skip, fix flags and masses), then a write/read round trip of two
+    frames with velocities, forces, local energies, energy and virial."""
+    (tmp_path / "in.xyz").write_text(
+        '3\nlattice="10.0 0 0 0 11.0 0 0.5 0 12.0" PROPERTIES=species:S:1:pos:R:3:charge:R:1:fix_atoms:L:3:masses:R:1'
+        ' pbc="T T T"\n'
+        "C 0.1 0.2 0.3 -0.5 T F F 12.011\n"
+        "H 1.0 2.0 3.0 0.25 F F F 1.008\n"
+        "C -1.5 0.0 7.25 0.25 F T T 12.011\n")
+    (fr,) = tg.xyz.read_xyz(str(tmp_path / "in.xyz"))
+    assert fr["n"] == 3 and fr["species"] == ["C", "H", "C"]
+    assert np.array_equal(fr["lattice"], [[10, 0, 0], [0, 11, 0], [0.5, 0, 12]])
+    assert np.array_equal(fr["positions"][2], [-1.5, 0.0, 7.25])
+    assert fr["fix_atom"].tolist() == [[True, False, False], [False, False, False], [False, True, True]]
+    assert np.allclose(fr["masses"], [12.011, 1.008, 12.011]) and fr["info"]["pbc"] == "T T T"
+    assert list(tg.xyz.species_channels(fr, ["H", "C"])) == [2, 1, 2]
+    rng = np.random.default_rng(1)
+    frames = []
+    for k in range(2):
+        frames.append(dict(species=["Si", "O", "O"], positions=rng.random((3, 3)) * 5, lattice=np.eye(3) * 5.1,
+                           velocities=rng.normal(size=(3, 3)), forces=rng.normal(size=(3, 3)),
+                           local_energy=rng.normal(size=3), energy=float(rng.normal()),
+                           virial=rng.normal(size=(3, 3))))
+    tg.xyz.write_xyz(str(tmp_path / "out.xyz"), frames)
+    back = tg.xyz.read_xyz(str(tmp_path / "out.xyz"))
+    assert len(back) == 2
+    for a, b in zip(frames, back):
+        assert np.array_equal(a["positions"], b["positions"]) and np.array_equal(a["velocities"], b["velocities"])
+        assert np.array_equal(a["lattice"], b["lattice"]) and b["species"] == ["Si", "O", "O"]
+        assert float(b["info"]["energy"]) == a["energy"]
+        v = np.array([float(x) for x in b["info"]["virial"].split()]).reshape(3, 3)
+        assert np.array_equal(v, a["virial"])

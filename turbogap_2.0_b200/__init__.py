@@ -6,7 +6,7 @@ include/tgap.h); this package is the host-side mirror of the reference interface
 """
 import importlib
 
-from . import gap_file, screen, synth  # noqa: F401
+from . import gap_file, screen, synth, xyz  # noqa: F401
 from .native import TGAP_FP64, TGAP_MIXED, TgapError, LIB_PATH  # noqa: F401
 
 
