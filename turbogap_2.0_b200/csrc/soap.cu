@@ -355,11 +355,27 @@ const YlmConst &ylm_host_constants()
                 y.norm[l * (l + 1) / 2 + m] = m == 0 ? N : N * M_SQRT2;
             }
         }
+        for (int m = 0; m <= kMaxL; ++m) {
+            y.qb0[m] = y.norm[m * (m + 1) / 2 + m] * y.dfact[m];
+            for (int l = m + 1; l <= kMaxL + 1; ++l) {
+                const double dl = l, dm = m;
+                const int i = rec_off(m) + l - m - 1;
+                y.ra[i] = std::sqrt((4.0 * dl * dl - 1.0) / (dl * dl - dm * dm));
+                y.rb[i] = l == m + 1 ? 0.0
+                                     : std::sqrt((2.0 * dl + 1.0) * (dl + dm - 1.0) * (dl - dm - 1.0) /
+                                                 ((2.0 * dl - 3.0) * (dl + dm) * (dl - dm)));
+            }
+        }
         for (int i = 0; i <= kMaxL; ++i) {
             y.dfact_f[i] = (float)y.dfact[i];
             y.inv_int_f[i] = (float)y.inv_int[i];
+            y.qb0_f[i] = (float)y.qb0[i];
         }
         for (int i = 0; i < (kMaxL + 1) * (kMaxL + 2) / 2; ++i) y.norm_f[i] = (float)y.norm[i];
+        for (int i = 0; i < kRecN; ++i) {
+            y.ra_f[i] = (float)y.ra[i];
+            y.rb_f[i] = (float)y.rb[i];
+        }
         return y;
     }();
     return h;

@@ -17,14 +17,27 @@ namespace tgap {
 constexpr int kLanesPerPair = 4;
 constexpr int kNlmMax = (kMaxL + 1) * (kMaxL + 1);
 
+// Fully normalised Legendre recurrence (Qb_l = N_lm Q_l, Q the polynomial part of P_l^m):
+//   Qb_m = N_mm (2m-1)!!,  Qb_l = ra_lm uz Qb_{l-1} - rb_lm Qb_{l-2}  (l > m)
+//   ra_lm = sqrt((4l^2 - 1) / (l^2 - m^2)),
+//   rb_lm = sqrt((2l+1) (l+m-1) (l-m-1) / ((2l-3) (l+m) (l-m)))  (0 for l = m + 1),
+// the three-term recurrence of the unnormalised Q divided through by the normalisations. The
+// coefficients of order m for target degrees l = m+1 .. kMaxL+1 sit at rec_off(m) + l - m - 1.
+constexpr int kRecN = (kMaxL + 1) * (kMaxL + 2) / 2;
+__host__ __device__ constexpr int rec_off(int m) { return m * (kMaxL + 1) - m * (m - 1) / 2; }
+
 // (2m-1)!! and the normalisation sqrt((2l+1)/(4 pi) (l-m)!/(l+m)!) (times sqrt 2 for m > 0).
 struct YlmConst {
     double dfact[kMaxL + 1];
     double norm[(kMaxL + 1) * (kMaxL + 2) / 2];  // index l (l+1)/2 + m
     double inv_int[kMaxL + 1];                   // 1 / k (0 for k = 0)
+    double qb0[kMaxL + 1];                       // Qb_m = N_mm (2m-1)!!
+    double ra[kRecN], rb[kRecN];                 // recurrence coefficients, packed by rec_off
     float dfact_f[kMaxL + 1];                    // single-precision copies
     float norm_f[(kMaxL + 1) * (kMaxL + 2) / 2];
     float inv_int_f[kMaxL + 1];
+    float qb0_f[kMaxL + 1];
+    float ra_f[kRecN], rb_f[kRecN];
 };
 
 // Constants in the arithmetic type of the caller.
@@ -37,6 +50,15 @@ template <> __device__ __forceinline__ float yc_norm<float>(const YlmConst &Y, i
 template <class T> __device__ __forceinline__ T yc_inv(const YlmConst &Y, int i);
 template <> __device__ __forceinline__ double yc_inv<double>(const YlmConst &Y, int i) { return Y.inv_int[i]; }
 template <> __device__ __forceinline__ float yc_inv<float>(const YlmConst &Y, int i) { return Y.inv_int_f[i]; }
+template <class T> __device__ __forceinline__ T yc_qb0(const YlmConst &Y, int m);
+template <> __device__ __forceinline__ double yc_qb0<double>(const YlmConst &Y, int m) { return Y.qb0[m]; }
+template <> __device__ __forceinline__ float yc_qb0<float>(const YlmConst &Y, int m) { return Y.qb0_f[m]; }
+template <class T> __device__ __forceinline__ T yc_ra(const YlmConst &Y, int i);
+template <> __device__ __forceinline__ double yc_ra<double>(const YlmConst &Y, int i) { return Y.ra[i]; }
+template <> __device__ __forceinline__ float yc_ra<float>(const YlmConst &Y, int i) { return Y.ra_f[i]; }
+template <class T> __device__ __forceinline__ T yc_rb(const YlmConst &Y, int i);
+template <> __device__ __forceinline__ double yc_rb<double>(const YlmConst &Y, int i) { return Y.rb[i]; }
+template <> __device__ __forceinline__ float yc_rb<float>(const YlmConst &Y, int i) { return Y.rb_f[i]; }
 
 // Host copy of the harmonic constants (computed once); passed to the warp kernels by value.
 const YlmConst &ylm_host_constants();

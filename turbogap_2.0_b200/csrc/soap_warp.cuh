@@ -41,32 +41,9 @@ __device__ __forceinline__ unsigned lanemask_lt()
     return m;
 }
 
-// Decode power-spectrum index d -> (n, n', l) with n <= n' (component order n, n', l).
-__device__ __forceinline__ void ps_decode_w(int d, int nmax, int L, int *n, int *np, int *l)
-{
-    int pidx = d / (L + 1);
-    *l = d - pidx * (L + 1);
-    int a = 0;
-    while (pidx >= nmax - a) {
-        pidx -= nmax - a;
-        ++a;
-    }
-    *n = a;
-    *np = a + pidx;
-}
-
-__device__ __forceinline__ int ps_index_w(int n, int np, int nmax, int L, int l)
-{
-    if (n > np) {
-        const int t = n;
-        n = np;
-        np = t;
-    }
-    return (n * nmax - n * (n - 1) / 2 + (np - n)) * (L + 1) + l;
-}
-
 // f_l = i_l(k)/i_0(k), l = 0..L+1: upward recurrence when k > L+2, else the continued fraction
-// started at l = L+33 (same rule as the reference restatement).
+// started at l = L+33 (same rule as the reference restatement; L+13 in FP32, where the start error
+// has decayed below the rounding).
 template <class T, int L>
 __device__ __forceinline__ void bessel_ratios_fixed(T k, T f[L + 2])
 {
@@ -88,7 +65,15 @@ __device__ __forceinline__ void bessel_ratios_fixed(T k, T f[L + 2])
         }
     } else {
         T rho = 0;
-        for (int l = L + 1 + 32; l > L + 1; --l) rho = k / ((T)(2 * l + 1) + k * rho);
+        if constexpr (std::is_same<T, float>::value) {
+            // each backward step scales the error of its start value by k^2 / (2l+1)^2 < 1/4 (k <= L+2,
+            // l >= L+2), so 12 steps leave < 4^-12 < 6e-8 of it, below the FP32 rounding; the fast
+            // division's own rounding in these steps is damped the same way
+#pragma unroll
+            for (int l = L + 1 + 12; l > L + 1; --l) rho = __fdividef(k, (T)(2 * l + 1) + k * rho);
+        } else {
+            for (int l = L + 1 + 32; l > L + 1; --l) rho = k / ((T)(2 * l + 1) + k * rho);
+        }
         T ratio[L + 2];
 #pragma unroll
         for (int l = L + 1; l >= 1; --l) {
@@ -256,6 +241,62 @@ __device__ __forceinline__ void load_vec(const T *__restrict__ p, T v[N])
     }
 }
 
+// 16-byte stores of N consecutive values (p 16-byte aligned).
+template <class T, int N>
+__device__ __forceinline__ void store_vec(T *p, const T v[N])
+{
+    if constexpr (std::is_same<T, float>::value) {
+        static_assert(N % 4 == 0, "float rows are stored 4 at a time");
+#pragma unroll
+        for (int i = 0; i < N / 4; ++i)
+            reinterpret_cast<float4 *>(p)[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
+    } else {
+        static_assert(N % 2 == 0, "double rows are stored 2 at a time");
+#pragma unroll
+        for (int i = 0; i < N / 2; ++i) reinterpret_cast<double2 *>(p)[i] = make_double2(v[2 * i], v[2 * i + 1]);
+    }
+}
+
+// dst[o] = src[o] for o < n by the 32 lanes of a warp, 16 bytes at a time when n and both
+// pointers allow it.
+template <class T>
+__device__ __forceinline__ void warp_copy_row(T *dst, const T *__restrict__ src, int n, int lane)
+{
+    constexpr int VW = 16 / (int)sizeof(T);
+    using V = typename std::conditional<std::is_same<T, float>::value, float4, double2>::type;
+    if (n % VW == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+        const V *sv = reinterpret_cast<const V *>(src);
+        V *dv = reinterpret_cast<V *>(dst);
+        for (int o = lane; o < n / VW; o += 32) dv[o] = sv[o];
+    } else {
+        for (int o = lane; o < n; o += 32) dst[o] = src[o];
+    }
+}
+
+// Lane partial of q . g over n elements (FP32 rows of the same type four at a time when aligned;
+// the caller reduces across the warp).
+template <class T, class GT>
+__device__ __forceinline__ T warp_dot_part(const T *__restrict__ q, const GT *__restrict__ g, int n, int lane)
+{
+    T acc = 0;
+    if constexpr (std::is_same<T, float>::value && std::is_same<GT, float>::value) {
+        if (n % 4 == 0 && ((reinterpret_cast<uintptr_t>(q) | reinterpret_cast<uintptr_t>(g)) & 15) == 0) {
+            const float4 *q4 = reinterpret_cast<const float4 *>(q);
+            const float4 *g4 = reinterpret_cast<const float4 *>(g);
+            for (int o = lane; o < n / 4; o += 32) {
+                const float4 a = q4[o], b = g4[o];
+                acc += a.x * b.x;
+                acc += a.y * b.y;
+                acc += a.z * b.z;
+                acc += a.w * b.w;
+            }
+            return acc;
+        }
+    }
+    for (int d = lane; d < n; d += 32) acc += q[d] * (T)g[d];
+    return acc;
+}
+
 // acc[n] += x[n] a for n < N. FP32 rows use the packed two-lane FMA of sm_100 (FFMA2: two
 // independent FMAs per instruction, each rounded as a scalar fmaf, so results are unchanged).
 template <class T, int N>
@@ -304,45 +345,45 @@ __device__ __forceinline__ void dot_even_odd(const T x[N], const T y[N], T &s0, 
 //   Gam = (1/r) sum_lm f_l U_lm dY_lm/du,   U_lm = Gc[lm].R, V_lm = Gc[lm].R'
 // which equals sum_lm [u Y (f V + df U) + f U (grad Y - u (u.grad Y)) / r]. The order m is
 // unrolled (compile time) and the degree l = m..L runs as a loop (L+1 copies of the body, in the
-// instruction cache); the cos and sin harmonics of one (l, m) share their Legendre factors and
-// read their two adjacent Gc rows together. f_l / df_l come from fl[l * 32] / dfl[l * 32].
+// instruction cache). The Legendre factor is carried fully normalised (Qb = N Q) by the
+// three-term recurrence Qb_{l+1} = ra uz Qb_l - rb Qb_{l-1}, advanced at the end of each pass so
+// the body has no branch; the Gc row, f_l / df_l (fl[l * 32] / dfl[l * 32]) and the recurrence
+// coefficients are reached by running offsets. The cos and sin harmonics of one (l, m) share
+// their Legendre factors and read their two adjacent Gc rows together.
 template <class T, int L, int AMB>
 __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T uz, T ir, const T *fl, const T *dfl,
                                              const T *__restrict__ Gs, const T R[AMB], const T dR[AMB], T w[3])
 {
     T A1 = 0, Gx = 0, Gy = 0, Gz = 0;
-    // m = 0: Y = N Q, dY/du = (0, 0, N dQ)
+    // m = 0: Y = Qb, dY/du = (0, 0, dQb)
     {
-        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+        T Q = yc_qb0<T>(Yc, 0), dQ = 0, Qp = 0, dQp = 0;
+        const T *row = Gs;
+        int step = AMB;  // row (l+1)^2 - row l^2, in elements
+        const T *f = fl, *df = dfl;
 #pragma unroll 1
         for (int l = 0; l <= L; ++l) {
-            T Q, dQ;
-            if (l == 0) {
-                Q = 1;
-                dQ = 0;
-            } else if (l == 1) {
-                Q = uz;
-                dQ = 1;
-            } else {
-                const T inv = yc_inv<T>(Yc, l);
-                const T a = (T)(2 * l - 1), b = (T)(l - 1);
-                Q = (a * uz * Q1 - b * Q2) * inv;
-                dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
-            }
-            Q2 = Q1;
-            Q1 = Q;
-            dQ2 = dQ1;
-            dQ1 = dQ;
             T g[AMB];
-            load_vec<T, AMB>(Gs + l * l * AMB, g);
+            load_vec<T, AMB>(row, g);
             T U0, U1, V0, V1;
             dot_even_odd<T, AMB>(g, R, U0, U1);
             dot_even_odd<T, AMB>(g, dR, V0, V1);
             const T U = U0 + U1, V = V0 + V1;
-            const T f = fl[l * 32], df = dfl[l * 32];
-            const T N = yc_norm<T>(Yc, l * (l + 1) / 2);
-            A1 += N * Q * (f * V + df * U);
-            Gz += N * dQ * (f * U);
+            const T fv = *f, dfv = *df;
+            A1 += Q * (fv * V + dfv * U);
+            Gz += dQ * (fv * U);
+            const int ri = rec_off(0) + l;  // target degree l + 1
+            const T ra = yc_ra<T>(Yc, ri), rb = yc_rb<T>(Yc, ri);
+            const T Qn = ra * uz * Q - rb * Qp;
+            const T dQn = ra * (Q + uz * dQ) - rb * dQp;
+            Qp = Q;
+            Q = Qn;
+            dQp = dQ;
+            dQ = dQn;
+            row += step;
+            step += 2 * AMB;
+            f += 32;
+            df += 32;
         }
     }
     T Cc = 1, Sc = 0;
@@ -351,32 +392,15 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
         const T Cp = Cc, Sp = Sc;
         Cc = ux * Cp - uy * Sp;
         Sc = ux * Sp + uy * Cp;
-        const T qmm = yc_dfact<T>(Yc, m);
         const T fm = (T)m;
-        const T tm1 = (T)(2 * m + 1);
-        T Q2 = 0, Q1 = 0, dQ2 = 0, dQ1 = 0;
+        T Q = yc_qb0<T>(Yc, m), dQ = 0, Qp = 0, dQp = 0;
+        // rows of the cos (l^2 + 2m - 1) and sin (l^2 + 2m) harmonics, adjacent in Gs
+        const T *row = Gs + (m * m + 2 * m - 1) * AMB;
+        int step = (2 * m + 1) * AMB;
+        const T *f = fl + m * 32, *df = dfl + m * 32;
 #pragma unroll 1
         for (int l = m; l <= L; ++l) {
-            T Q, dQ;
-            if (l == m) {
-                Q = qmm;
-                dQ = 0;
-            } else if (l == m + 1) {
-                Q = tm1 * uz * qmm;
-                dQ = tm1 * qmm;
-            } else {
-                const T inv = yc_inv<T>(Yc, l - m);
-                const T a = (T)(2 * l - 1), b = (T)(l - 1) + fm;
-                Q = (a * uz * Q1 - b * Q2) * inv;
-                dQ = (a * (Q1 + uz * dQ1) - b * dQ2) * inv;
-            }
-            Q2 = Q1;
-            Q1 = Q;
-            dQ2 = dQ1;
-            dQ1 = dQ;
-            // rows of the cos (l^2 + 2m - 1) and sin (l^2 + 2m) harmonics, adjacent in Gs
             T gc[AMB], gs[AMB];
-            const T *row = Gs + (l * l + 2 * m - 1) * AMB;
             load_vec<T, AMB>(row, gc);
             load_vec<T, AMB>(row + AMB, gs);
             T Uc0, Uc1, Vc0, Vc1, Us0, Us1, Vs0, Vs1;
@@ -385,16 +409,27 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
             dot_even_odd<T, AMB>(gs, R, Us0, Us1);
             dot_even_odd<T, AMB>(gs, dR, Vs0, Vs1);
             const T Uc = Uc0 + Uc1, Vc = Vc0 + Vc1, Us = Us0 + Us1, Vs = Vs0 + Vs1;
-            const T f = fl[l * 32], df = dfl[l * 32];
-            const T ac = f * Vc + df * Uc, as = f * Vs + df * Us;
-            const T bc = f * Uc, bs = f * Us;
-            const T N = yc_norm<T>(Yc, l * (l + 1) / 2 + m);
-            const T NQ = N * Q, NQm = NQ * fm, NdQ = N * dQ;
-            // cos: Y = NQ C, dY/du = (NQm C', -NQm S', NdQ C); sin: Y = NQ S, (NQm S', NQm C', NdQ S)
-            A1 += NQ * (ac * Cc + as * Sc);
-            Gx += NQm * (bc * Cp + bs * Sp);
-            Gy += NQm * (bs * Cp - bc * Sp);
-            Gz += NdQ * (bc * Cc + bs * Sc);
+            const T fv = *f, dfv = *df;
+            const T ac = fv * Vc + dfv * Uc, as = fv * Vs + dfv * Us;
+            const T bc = fv * Uc, bs = fv * Us;
+            const T Qm = Q * fm;
+            // cos: Y = Qb C, dY/du = (m Qb C', -m Qb S', dQb C); sin: Y = Qb S, (m Qb S', m Qb C', dQb S)
+            A1 += Q * (ac * Cc + as * Sc);
+            Gx += Qm * (bc * Cp + bs * Sp);
+            Gy += Qm * (bs * Cp - bc * Sp);
+            Gz += dQ * (bc * Cc + bs * Sc);
+            const int ri = rec_off(m) + (l - m);  // target degree l + 1
+            const T ra = yc_ra<T>(Yc, ri), rb = yc_rb<T>(Yc, ri);
+            const T Qn = ra * uz * Q - rb * Qp;
+            const T dQn = ra * (Q + uz * dQ) - rb * dQp;
+            Qp = Q;
+            Q = Qn;
+            dQp = dQ;
+            dQ = dQn;
+            row += step;
+            step += 2 * AMB;
+            f += 32;
+            df += 32;
         }
     }
     Gx *= ir;
@@ -524,7 +559,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     if (s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self])
         cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
     __syncwarp();
-    for (int o = lane; o < nout; o += 32) c_out[(size_t)row * nout + o] = cs[o];
+    warp_copy_row<T>(c_out + (size_t)row * nout, cs, nout, lane);
     // power spectrum into the (now free) angular area: lane owns the (n, n') pairs
     // pp = lane + 32 i (n-major, n <= n') and every l, component d = pp (L + 1) + l
     T *ps = As;
@@ -555,6 +590,34 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
     __syncwarp();
     // the row of the dE/dq accumulator the GAP kernel adds into (saves a separate clear)
+    if constexpr (std::is_same<T, float>::value) {
+        const bool vec = (q_ld & 3) == 0 && (reinterpret_cast<uintptr_t>(q_out) & 15) == 0 &&
+                         (reinterpret_cast<uintptr_t>(g_clear) & 15) == 0 &&
+                         (!SPLIT || ((reinterpret_cast<uintptr_t>(q_hi) | reinterpret_cast<uintptr_t>(q_lo)) & 7) == 0);
+        // four consecutive components per lane: 16-byte q and dE/dq stores, 8-byte bf16 halves
+        for (int d = 4 * lane; vec && d < q_ld; d += 128) {
+            float v[4];
+#pragma unroll
+            for (int e = 0; e < 4; ++e) v[e] = d + e < dim ? (float)(ps[d + e] * inv) : 0.0f;
+            const size_t o = (size_t)row * q_ld + d;
+            *reinterpret_cast<float4 *>(q_out + o) = make_float4(v[0], v[1], v[2], v[3]);
+            if (g_clear) *reinterpret_cast<float4 *>(g_clear + o) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            if (SPLIT) {
+                const __nv_bfloat162 h01 = __floats2bfloat162_rn(v[0], v[1]), h23 = __floats2bfloat162_rn(v[2], v[3]);
+                const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                const __nv_bfloat162 l01 = __floats2bfloat162_rn(v[0] - f01.x, v[1] - f01.y);
+                const __nv_bfloat162 l23 = __floats2bfloat162_rn(v[2] - f23.x, v[3] - f23.y);
+                *reinterpret_cast<uint2 *>(q_hi + o) = make_uint2(*reinterpret_cast<const unsigned *>(&h01),
+                                                                  *reinterpret_cast<const unsigned *>(&h23));
+                *reinterpret_cast<uint2 *>(q_lo + o) = make_uint2(*reinterpret_cast<const unsigned *>(&l01),
+                                                                  *reinterpret_cast<const unsigned *>(&l23));
+            }
+        }
+        if (vec) {
+            if (lane == 0) norm_out[row] = nrm;
+            return;
+        }
+    }
     if (g_clear)
         for (int d = lane; d < q_ld; d += 32) g_clear[(size_t)row * q_ld + d] = 0.0f;
     for (int d = lane; d < q_ld; d += 32) {
@@ -580,6 +643,14 @@ template <class T> __host__ __device__ constexpr int bwd_c_elems(int nout)
                                                                                : (int)(32 * 9 * sizeof(double) / sizeof(T));
 }
 
+// Pitch (elements) of one M_l block of the adjoint: n_max rows of n_species * AMB columns, rounded
+// to an odd number of 16-byte vectors, so lanes that read blocks of different l with 16-byte loads
+// fall in different banks.
+template <class T> __host__ __device__ constexpr int bwd_m_pitch(int nmax, int mp)
+{
+    return (((nmax * mp + (int)(16 / sizeof(T)) - 1) / (int)(16 / sizeof(T))) | 1) * (int)(16 / sizeof(T));
+}
+
 // Minimum resident CTAs asked of the compiler (1: every instantiation keeps its natural register
 // count; forcing 6 CTAs on the FP32 kernel spilled and ran slower).
 template <class T, int AMB> struct BwdMinCtas {
@@ -588,8 +659,9 @@ template <class T, int AMB> struct BwdMinCtas {
 
 // Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (then the lanes'
 // force/virial partials), Gc [n_species][NLM][AMB] (dE/dc per species block, zero beyond
-// alpha_max), M [L+1][MS] with M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l]
-// (MS = n_max^2 + 1, odd), f_l / df_l of each lane's pair [2][L+1][32]; after the warps, the CTA's virial partials [kWarpsPerCta][6] and
+// alpha_max), M [L+1][MSP] with M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l] in padded
+// species columns (MSP = bwd_m_pitch), f_l / df_l of each lane's pair [2][L+1][32]; after the
+// warps, the CTA's virial partials [kWarpsPerCta][6] and
 // structure ids [kWarpsPerCta].
 template <class T, class GT, int L, int AMB>
 __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) k_soap_bwd_warp(
@@ -620,47 +692,78 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
         T *cs = reinterpret_cast<T *>(wbase + 256);
         T *Gc = cs + bwd_c_elems<T>(nout);
         T *Ms = Gc + P.n_species * NLM * AMB;
-        T *fdf = Ms + (L + 1) * (nmax * nmax + 1);  // [2][L+1][32]: f_l, df_l of each lane's pair
+        const int MP = P.n_species * AMB, MSP = bwd_m_pitch<T>(nmax, MP);
+        T *fdf = Ms + (L + 1) * MSP;  // [2][L+1][32]: f_l, df_l of each lane's pair
 
         const int site = sites ? sites[row] : row;
         my_struct = site_struct ? site_struct[site] : 0;
         const int64_t kb = start[site], ke = start[site + 1];
-        for (int o = lane; o < nout; o += 32) cs[o] = c_in[(size_t)row * nout + o];
-        T qg = 0;
-        for (int d = lane; d < dim; d += 32) qg += q_in[(size_t)row * q_ld + d] * (T)g_in[(size_t)row * g_ld + d];
+        warp_copy_row<T>(cs, c_in + (size_t)row * nout, nout, lane);
+        const T *qrow = q_in + (size_t)row * q_ld;
+        const GT *grow = g_in + (size_t)row * g_ld;
+        T qg = warp_dot_part<T, GT>(qrow, grow, dim, lane);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
         const T nrm = norm_in[row];
         const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-        // h = dE/dp = (g - q (q.g)) / |p|, scattered into the symmetric M_l
-        for (int d = lane; d < dim; d += 32) {
-            int n, np, l;
-            ps_decode_w(d, nmax, L, &n, &np, &l);
-            const T hv = ((T)g_in[(size_t)row * g_ld + d] - q_in[(size_t)row * q_ld + d] * qg) * inv;
-            const T mv = (n == np) ? (T)2 * hv : (T)1.4142135623730951 * hv;
-            Ms[l * MS + n * nmax + np] = mv;
-            Ms[l * MS + np * nmax + n] = mv;
+        // M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l], h = dE/dp = (g - q (q.g)) / |p|, stored
+        // as rows n' of n_species blocks of AMB columns (radial index n_off[s] + a in column
+        // s AMB + a; columns beyond alpha_max stay zero). M_l is symmetric, so the slice of row n'
+        // in block s holds M_l[n_off[s] + a][n'] for every a.
+        if (nmax != MP) {
+            for (int o = lane; o < (L + 1) * MSP; o += 32) Ms[o] = (T)0;
+            __syncwarp();
+        }
+        {
+            // lane -> (sub, l); it visits the pairs pp = sub + PPW t (n-major, n <= n'), component
+            // d = pp (L + 1) + l, with (n, n') advanced incrementally
+            constexpr int PPW = 32 / (L + 1);
+            const int sub = lane / (L + 1), l = lane - sub * (L + 1);
+            const int npair = nmax * (nmax + 1) / 2;
+            int n = 0, rem = sub;
+            while (n < nmax && rem >= nmax - n) {
+                rem -= nmax - n;
+                ++n;
+            }
+            for (int pp = sub; sub < PPW && pp < npair; pp += PPW) {
+                const int np = n + rem, d = pp * (L + 1) + l;
+                const T hv = ((T)grow[d] - qrow[d] * qg) * inv;
+                const T mv = (n == np) ? (T)2 * hv : (T)1.4142135623730951 * hv;
+                int sn = 0, snp = 0;  // species blocks of n and n'
+                for (int s = 1; s < P.n_species; ++s) {
+                    if (n >= P.n_off[s]) sn = s;
+                    if (np >= P.n_off[s]) snp = s;
+                }
+                const int cn = sn * AMB + n - P.n_off[sn], cnp = snp * AMB + np - P.n_off[snp];
+                Ms[l * MSP + np * MP + cn] = mv;
+                Ms[l * MSP + n * MP + cnp] = mv;
+                rem += PPW;
+                while (n < nmax && rem >= nmax - n) {
+                    rem -= nmax - n;
+                    ++n;
+                }
+            }
         }
         __syncwarp();
-        // Gc[s][lm][n] = sum_n' M_l[off_s + n][n'] c[n'][lm]
+        // Gc[s][lm][a] = sum_n' M_l[n_off[s] + a][n'] c[n'][lm]: one c value and one padded M row
+        // slice per n', accumulated with row FMAs
 #pragma unroll
         for (int j = 0; j < KPL; ++j) {
             const int kk = lane + 32 * j;
             if (kk < NLM) {
-                int l = (int)sqrtf((float)kk);
-                const T *Ml = Ms + l * MS;
+                const int l = (int)sqrtf((float)kk);
+                const T *Ml = Ms + l * MSP;
                 for (int s = 0; s < P.n_species; ++s) {
-                    const int off = P.n_off[s], am = P.alpha_max[s];
-                    T *Gk = Gc + (s * NLM + kk) * AMB;
+                    T acc[AMB];
 #pragma unroll
-                    for (int n = 0; n < AMB; ++n) {
-                        T acc = 0;
-                        if (n < am) {
-                            const T *mr = Ml + (off + n) * nmax;
-                            for (int np = 0; np < nmax; ++np) acc += mr[np] * cs[np * NLM + kk];
-                        }
-                        Gk[n] = acc;
+                    for (int a = 0; a < AMB; ++a) acc[a] = (T)0;
+                    const T *mcol = Ml + s * AMB;
+                    for (int np = 0; np < nmax; ++np) {
+                        T mr[AMB];
+                        load_vec<T, AMB>(mcol + np * MP, mr);
+                        axpy_row<T, AMB>(acc, mr, cs[np * NLM + kk]);
                     }
+                    store_vec<T, AMB>(Gc + (s * NLM + kk) * AMB, acc);
                 }
             }
         }
@@ -804,7 +907,7 @@ template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
 {
     const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
     const int nout = P.n_max * (int)nlm;
-    const size_t ms = (size_t)(P.l_max + 1) * ((size_t)P.n_max * P.n_max + 1);
+    const size_t ms = (size_t)(P.l_max + 1) * bwd_m_pitch<T>(P.n_max, P.n_species * amb);
     const size_t fdf = 2 * (size_t)(P.l_max + 1) * 32;
     return 256 +
            (sizeof(T) * ((size_t)bwd_c_elems<T>(nout) + (size_t)P.n_species * nlm * amb + ms + fdf) + 15) / 16 * 16;
