@@ -60,6 +60,15 @@ class Context:
     def synchronize(self):
         check(self._L.tgap_synchronize(self.h), self.h, "synchronize")
 
+    def autotune_set(self, key, value):
+        """Fixes one launch choice (tgap_autotune_set): a key of the autotune report, or '*' and a
+        suffix for every key ending with it ('*/persist': 0 = one site per warp, 1 = persistent
+        work-queue descriptor kernels)."""
+        check(self._L.tgap_autotune_set(self.h, key.encode(), int(value)), self.h, "autotune_set")
+
+    def autotune_clear(self):
+        check(self._L.tgap_autotune_clear(self.h), self.h, "autotune_clear")
+
     def set_stream(self, stream_handle):
         check(self._L.tgap_set_stream(self.h, C.c_void_p(stream_handle) if stream_handle else None),
               self.h, "set_stream")

@@ -96,7 +96,11 @@ int tuned(tgap_context *ctx, const std::string &key, const char *stage, const st
     if (!ctx->probe_key.empty() && key == ctx->probe_key) return ctx->probe_val;
     if (!ctx->tune_seen.count(key)) ctx->tune_seen[key] = tgap_context::TuneSlot{stage, candidates, dflt};
     const auto it = ctx->tune.find(key);
-    return it != ctx->tune.end() ? it->second : dflt;
+    if (it != ctx->tune.end()) return it->second;
+    for (const auto &pat : ctx->tune_suffix)
+        if (key.size() >= pat.first.size() && key.compare(key.size() - pat.first.size(), pat.first.size(), pat.first) == 0)
+            return pat.second;
+    return dflt;
 }
 
 int cuda_check(tgap_context *ctx, cudaError_t e, const char *what)
@@ -742,6 +746,7 @@ struct tgap_system {
     double rcut;
     std::vector<int> host_species;
     DevBuf d_species;  // species channel per site (pair and triplet terms), uploaded on first use
+    DevBuf queue;      // site counters of the persistent descriptor launches (kQueueInts)
     std::vector<SiteSet> site_sets;
     DevBuf c, q, norm, q_hi, q_lo, e_rows;
     GapWork gw;
@@ -823,7 +828,7 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
-                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species};
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species, &s->queue};
     for (DevBuf *b : bufs) b->release();
     delete s;
     return TGAP_OK;
@@ -907,8 +912,10 @@ static int ensure_eval_buffers(tgap_system *s, const tgap_model *m, int n_rows, 
 
 // geom: the descriptor forward writes this step's pair geometry from the primitive positions
 // (pure-replica systems; every site of the list must belong to some model's site set)
+// queue: two zeroed site counters (forward, adjoint) for the persistent descriptor launches, or null
 static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m, int precision,
-                         int do_forces, double *d_energies, double *d_forces, double *d_virial, bool geom = false)
+                         int do_forces, double *d_energies, double *d_forces, double *d_virial, bool geom = false,
+                         int *queue = nullptr)
 {
     SiteSet *ss = nullptr;
     CHECK_RC(site_set(s, m->central_species, &ss));
@@ -918,6 +925,10 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     PairView pv{s->nb.start.as<int64_t>(), s->nb.xyz.as<double>(), s->nb.rjs.as<double>(),
                 s->nb.nspecies.as<int>(), s->nb.jatom.as<int>(), s->nb.n_atoms, ctx->d_check};
     PairView pvf = pv;  // the forward's view, writing the geometry first when asked
+    if (queue) {
+        pvf.queue = queue;
+        pv.queue = queue + 1;
+    }
     if (geom) {
         pvf.geo.pos = s->nb.positions.as<double>();
         pvf.geo.list = s->nb.list.as<int>();
@@ -961,10 +972,11 @@ static int compute_model(tgap_context *ctx, tgap_system *s, const tgap_model *m,
     return TGAP_OK;
 }
 
-// zeroed: the caller cleared the outputs already (the MD step clears its contiguous block at once)
+// zeroed: the caller cleared the outputs already (the MD step clears its contiguous block at once,
+// with kQueueInts zeroed site counters at queue)
 static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                           int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
-                          bool geom, bool zeroed);
+                          bool geom, bool zeroed, int *queue = nullptr);
 
 extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                             int precision, int do_forces, double *d_energies, double *d_forces,
@@ -976,7 +988,7 @@ extern "C" int tgap_compute(tgap_context *ctx, tgap_system *s, int n_models, tga
 
 static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                           int precision, int do_forces, double *d_energies, double *d_forces, double *d_virial,
-                          bool geom, bool zeroed)
+                          bool geom, bool zeroed, int *queue)
 {
     CHECK_RC(activate(ctx));
     if (!s || n_models <= 0 || !models || !d_energies || (do_forces && (!d_forces || !d_virial)))
@@ -989,8 +1001,15 @@ static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_
         TGAP_CUDA(ctx, cudaMemsetAsync(d_forces, 0, sizeof(double) * 3 * N, ctx->stream));
         TGAP_CUDA(ctx, cudaMemsetAsync(d_virial, 0, sizeof(double) * 9 * s->nb.n_structures, ctx->stream));
     }
+    if (!zeroed && 2 * n_models <= kQueueInts) {
+        if (s->queue.ensure(sizeof(int) * kQueueInts)) return set_error(ctx, TGAP_ERR_NOMEM, "site counters");
+        TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
+        queue = s->queue.as<int>();
+    }
+    if (2 * n_models > kQueueInts) queue = nullptr;
     for (int i = 0; i < n_models; ++i)
-        CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial, geom));
+        CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial, geom,
+                               queue ? queue + 2 * i : nullptr));
     return TGAP_OK;
 }
 
@@ -1145,7 +1164,25 @@ extern "C" int tgap_autotune_clear(tgap_context *ctx)
 {
     if (!ctx) return TGAP_ERR_ARGUMENT;
     ctx->tune.clear();
+    ctx->tune_suffix.clear();
     ctx->tune_report.clear();
+    return TGAP_OK;
+}
+
+extern "C" int tgap_autotune_set(tgap_context *ctx, const char *key, int value)
+{
+    if (!ctx || !key || !key[0]) return TGAP_ERR_ARGUMENT;
+    if (key[0] == '*') {
+        const std::string suffix(key + 1);
+        for (auto &pat : ctx->tune_suffix)
+            if (pat.first == suffix) {
+                pat.second = value;
+                return TGAP_OK;
+            }
+        ctx->tune_suffix.emplace_back(suffix, value);
+    } else {
+        ctx->tune[key] = value;
+    }
     return TGAP_OK;
 }
 
@@ -1330,7 +1367,8 @@ struct tgap_md {
     tgap_system *sys;
     std::vector<tgap_model *> models;
     tgap_terms *terms = nullptr;  // pair and triplet terms added after the SOAP models
-    DevBuf out;  // forces (3 N), energies (N), virial (9 per structure), contiguous: one clear per step
+    DevBuf out;  // forces (3 N), energies (N), virial (9 per structure), site counters: one clear per step
+    int *queue = nullptr;  // the site counters in out (kQueueInts)
     // the descriptor forward writes each step's pair geometry (no separate geometry pass): a
     // pure-replica system whose sites all belong to some model, and no pair/triplet terms
     bool fused_geom = false;
@@ -1381,7 +1419,7 @@ static int md_eval(tgap_md *md)
     TGAP_CUDA(md->ctx, cudaMemsetAsync(md->out.ptr, 0, md->out.bytes, md->ctx->stream));
     CHECK_RC(compute_models(md->ctx, md->sys, (int)md->models.size(), md->models.data(), md->precision, 1,
                             md->energies.as<double>(), md->forces.as<double>(), md->virial.as<double>(),
-                            md->fused_geom, true));
+                            md->fused_geom, true, md->queue));
     if (md->terms)
         CHECK_RC(terms_add(md->ctx, md->sys, md->terms, 1, md->energies.as<double>(), md->forces.as<double>(),
                            md->virial.as<double>()));
@@ -1569,8 +1607,9 @@ extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models,
     for (DevBuf *b : bufs)
         if (!rc && (b->ensure(sizeof(double) * 3 * N) || cudaMemsetAsync(b->ptr, 0, sizeof(double) * 3 * N, ctx->stream)))
             rc = TGAP_ERR_NOMEM;
-    // forces, energies and virial share one block (views into md->out, never resized)
-    const size_t n_out = 4 * (size_t)N + 9 * (size_t)sys->nb.n_structures;
+    // forces, energies, virial and the site counters share one block (views into md->out, never
+    // resized), cleared by one memset per step
+    const size_t n_out = 4 * (size_t)N + 9 * (size_t)sys->nb.n_structures + kQueueInts / 2;
     if (!rc && (md->out.ensure(sizeof(double) * n_out) ||
                 cudaMemsetAsync(md->out.ptr, 0, sizeof(double) * n_out, ctx->stream)))
         rc = TGAP_ERR_NOMEM;
@@ -1582,6 +1621,7 @@ extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models,
         md->energies.bytes = sizeof(double) * (size_t)N;
         md->virial.ptr = o + 4 * (size_t)N;
         md->virial.bytes = sizeof(double) * 9 * (size_t)sys->nb.n_structures;
+        md->queue = reinterpret_cast<int *>(o + 4 * (size_t)N + 9 * (size_t)sys->nb.n_structures);
     }
     if (rc) {
         tgap_md_destroy(md);

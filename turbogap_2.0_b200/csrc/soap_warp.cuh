@@ -24,6 +24,9 @@
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 #include <type_traits>
 
 #include "neighbors_device.cuh"
@@ -452,15 +455,22 @@ template <int NLM> struct AStride {
 // Shared memory of one warp: 256 bytes of pair indices, Rs [32][AMB], then an area holding the
 // angular rows [32][ASTR] during the passes and the power spectrum [dim] after them, then the
 // expansion c [n_max][NLM].
-template <class T, int L, int AMB, bool SPLIT>
-__global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
+// Minimum resident CTAs of 4 warps asked of the compiler for the forward (0: no bound; an explicit
+// 1 grows the one-site FP32 form from 124 registers to 190). The persistent FP32 form asks for 4
+// (at most 128 registers; its site loop takes 158 without it); FP64 has none (128 spills).
+template <class T, bool PERSIST> struct FwdMinCtas {
+    static constexpr int value = (PERSIST && std::is_same<T, float>::value) ? 4 : 0;
+};
+
+template <class T, int L, int AMB, bool SPLIT, bool PERSIST>
+__global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::value) k_soap_fwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
     const T *__restrict__ tq, const float4 *__restrict__ rtab, const T *__restrict__ central,
     const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
     const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
     T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
     __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check, GeomSrc geo,
-    float *__restrict__ g_clear)
+    float *__restrict__ g_clear, int *queue)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int ASTR = AStride<NLM>::value;
@@ -468,172 +478,202 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta) k_soap_fwd_warp(
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int row = blockIdx.x * nw + warp;
-    if (row >= n_rows) return;  // no CTA-wide synchronisation in this kernel
-    unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
-    const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
-    long long *idx = reinterpret_cast<long long *>(wbase);
-    T *Rs = reinterpret_cast<T *>(wbase + 256);
-    T *As = Rs + 32 * AMB;
-    T *cs = As + (32 * ASTR > dim ? 32 * ASTR : dim);
+    // one site: no CTA-wide synchronisation in this kernel
+    auto site_body = [&](const int row) {
+        unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
+        const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
+        long long *idx = reinterpret_cast<long long *>(wbase);
+        T *Rs = reinterpret_cast<T *>(wbase + 256);
+        T *As = Rs + 32 * AMB;
+        T *cs = As + (32 * ASTR > dim ? 32 * ASTR : dim);
 
-    const int site = sites ? sites[row] : row;
-    const int64_t kb = start[site], ke = start[site + 1];
-    if (geo.pos) {
-        // this step's pair geometry from the primitive positions (what the neighbor module's
-        // geometry pass would write), read back below through L2-coherent loads
-        const StructDesc &S = static_cast<const StructDesc *>(geo.sd)[geo.site_struct[site]];
-        double pi[3];
-        sc_position(S, geo.pos, site - S.atom_off + 1, pi);
-        for (int64_t k = kb + lane; k < ke; k += 32) {
-            double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
-            if (k > kb) {
-                double pj[3];
-                sc_position(S, geo.pos, geo.list[k], pj);
-                get_distance_dev(pi, pj, S, dist, &d);
+        const int site = sites ? sites[row] : row;
+        const int64_t kb = start[site], ke = start[site + 1];
+        if (geo.pos) {
+            // this step's pair geometry from the primitive positions (what the neighbor module's
+            // geometry pass would write), read back below through L2-coherent loads
+            const StructDesc &S = static_cast<const StructDesc *>(geo.sd)[geo.site_struct[site]];
+            double pi[3];
+            sc_position(S, geo.pos, site - S.atom_off + 1, pi);
+            for (int64_t k = kb + lane; k < ke; k += 32) {
+                double dist[3] = {0.0, 0.0, 0.0}, d = 0.0;
+                if (k > kb) {
+                    double pj[3];
+                    sc_position(S, geo.pos, geo.list[k], pj);
+                    get_distance_dev(pi, pj, S, dist, &d);
+                }
+                geo.rjs_out[k] = d;
+                geo.xyz_out[3 * k] = dist[0];
+                geo.xyz_out[3 * k + 1] = dist[1];
+                geo.xyz_out[3 * k + 2] = dist[2];
             }
-            geo.rjs_out[k] = d;
-            geo.xyz_out[3 * k] = dist[0];
-            geo.xyz_out[3 * k + 1] = dist[1];
-            geo.xyz_out[3 * k + 2] = dist[2];
-        }
-        __threadfence_block();
-        __syncwarp();
-    }
-    for (int s = 0; s < P.n_species; ++s) {
-        T acc[KPL][AMB];
-#pragma unroll
-        for (int j = 0; j < KPL; ++j)
-#pragma unroll
-            for (int n = 0; n < AMB; ++n) acc[j][n] = 0;
-        int64_t scan = kb + 1;
-        while (scan < ke) {
-            const int cnt = compact_pairs(P, scan, ke, rjs, nsp, s, idx, lane);
-            if (cnt == 0) break;
-            if (lane < cnt) {
-                const int64_t k = idx[lane];
-                const bool in_site = k > kb && k < ke;
-                if (!in_site) check_fail(check, kCheckFwdPair, k, site);
-                const double rd = in_site ? __ldcg(rjs + k) : 1.0;
-                const T r = (T)rd, ir = (T)1 / r;
-                const T ux = in_site ? (T)__ldcg(xyz + 3 * k) * ir : (T)0;
-                const T uy = in_site ? (T)__ldcg(xyz + 3 * k + 1) * ir : (T)0;
-                const T uz = in_site ? (T)__ldcg(xyz + 3 * k + 2) * ir : (T)1;
-                T R[AMB], dR[AMB];
-                radial_values<T, AMB, false>(P, s, rd, xq, tq, rtab, R, dR);
-                T *Rrow = Rs + lane * AMB;
-#pragma unroll
-                for (int n = 0; n < AMB; ++n) Rrow[n] = in_site ? R[n] : (T)0;
-                const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
-                T f[L + 2];
-                bessel_ratios_fixed<T, L>(r * r / (st * st), f);
-                T *Arow = As + lane * ASTR;
-                ylm_all<T, L, false>(Yc, ux, uy, uz, [&](int kk, int l, T y, T, T, T) { Arow[kk] = f[l] * y; });
-            }
+            __threadfence_block();
             __syncwarp();
-            for (int p = 0; p < cnt; ++p) {
-                T rv[AMB];
-                load_vec<T, AMB>(Rs + p * AMB, rv);
-#pragma unroll
-                for (int j = 0; j < KPL; ++j) {
-                    const int kk = lane + 32 * j;
-                    if (kk < NLM) axpy_row<T, AMB>(acc[j], rv, As[p * ASTR + kk]);
+        }
+        for (int s = 0; s < P.n_species; ++s) {
+            T acc[KPL][AMB];
+    #pragma unroll
+            for (int j = 0; j < KPL; ++j)
+    #pragma unroll
+                for (int n = 0; n < AMB; ++n) acc[j][n] = 0;
+            int64_t scan = kb + 1;
+            while (scan < ke) {
+                const int cnt = compact_pairs(P, scan, ke, rjs, nsp, s, idx, lane);
+                if (cnt == 0) break;
+                if (lane < cnt) {
+                    const int64_t k = idx[lane];
+                    const bool in_site = k > kb && k < ke;
+                    if (!in_site) check_fail(check, kCheckFwdPair, k, site);
+                    const double rd = in_site ? __ldcg(rjs + k) : 1.0;
+                    const T r = (T)rd, ir = (T)1 / r;
+                    const T ux = in_site ? (T)__ldcg(xyz + 3 * k) * ir : (T)0;
+                    const T uy = in_site ? (T)__ldcg(xyz + 3 * k + 1) * ir : (T)0;
+                    const T uz = in_site ? (T)__ldcg(xyz + 3 * k + 2) * ir : (T)1;
+                    T R[AMB], dR[AMB];
+                    radial_values<T, AMB, false>(P, s, rd, xq, tq, rtab, R, dR);
+                    T *Rrow = Rs + lane * AMB;
+    #pragma unroll
+                    for (int n = 0; n < AMB; ++n) Rrow[n] = in_site ? R[n] : (T)0;
+                    const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
+                    T f[L + 2];
+                    bessel_ratios_fixed<T, L>(r * r / (st * st), f);
+                    T *Arow = As + lane * ASTR;
+                    ylm_all<T, L, false>(Yc, ux, uy, uz, [&](int kk, int l, T y, T, T, T) { Arow[kk] = f[l] * y; });
+                }
+                __syncwarp();
+                for (int p = 0; p < cnt; ++p) {
+                    T rv[AMB];
+                    load_vec<T, AMB>(Rs + p * AMB, rv);
+    #pragma unroll
+                    for (int j = 0; j < KPL; ++j) {
+                        const int kk = lane + 32 * j;
+                        if (kk < NLM) axpy_row<T, AMB>(acc[j], rv, As[p * ASTR + kk]);
+                    }
+                }
+                __syncwarp();
+            }
+            const int off = P.n_off[s], am = P.alpha_max[s];
+    #pragma unroll
+            for (int j = 0; j < KPL; ++j) {
+                const int kk = lane + 32 * j;
+                if (kk < NLM) {
+    #pragma unroll
+                    for (int n = 0; n < AMB; ++n)
+                        if (n < am) cs[(off + n) * NLM + kk] = acc[j][n];
                 }
             }
+        }
+        __syncwarp();
+        // central atom on l = 0 of its own species block
+        const int s_self = nsp[kb] - 1;
+        if (s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self])
+            cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
+        __syncwarp();
+        warp_copy_row<T>(c_out + (size_t)row * nout, cs, nout, lane);
+        // power spectrum into the (now free) angular area: lane owns the (n, n') pairs
+        // pp = lane + 32 i (n-major, n <= n') and every l, component d = pp (L + 1) + l
+        T *ps = As;
+        T part = 0;
+        const int npair = nmax * (nmax + 1) / 2;
+        for (int pp = lane; pp < npair; pp += 32) {
+            int n = 0, rem = pp;
+            while (rem >= nmax - n) {
+                rem -= nmax - n;
+                ++n;
+            }
+            const int np = n + rem;
+            const T *a = cs + n * NLM, *b = cs + np * NLM;
+            const T sc = (n == np) ? (T)1 : (T)1.4142135623730951;
+    #pragma unroll
+            for (int l = 0; l <= L; ++l) {
+                T acc = 0;
+    #pragma unroll
+                for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
+                const T v = acc * sc;
+                ps[pp * (L + 1) + l] = v;
+                part += v * v;
+            }
+        }
+    #pragma unroll
+        for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+        const T nrm = t_sqrt<T>(part);
+        const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
+        __syncwarp();
+        // the row of the dE/dq accumulator the GAP kernel adds into (saves a separate clear)
+        if constexpr (std::is_same<T, float>::value) {
+            const bool vec = (q_ld & 3) == 0 && (reinterpret_cast<uintptr_t>(q_out) & 15) == 0 &&
+                             (reinterpret_cast<uintptr_t>(g_clear) & 15) == 0 &&
+                             (!SPLIT || ((reinterpret_cast<uintptr_t>(q_hi) | reinterpret_cast<uintptr_t>(q_lo)) & 7) == 0);
+            // four consecutive components per lane: 16-byte q and dE/dq stores, 8-byte bf16 halves
+            for (int d = 4 * lane; vec && d < q_ld; d += 128) {
+                float v[4];
+    #pragma unroll
+                for (int e = 0; e < 4; ++e) v[e] = d + e < dim ? (float)(ps[d + e] * inv) : 0.0f;
+                const size_t o = (size_t)row * q_ld + d;
+                *reinterpret_cast<float4 *>(q_out + o) = make_float4(v[0], v[1], v[2], v[3]);
+                if (g_clear) *reinterpret_cast<float4 *>(g_clear + o) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                if (SPLIT) {
+                    const __nv_bfloat162 h01 = __floats2bfloat162_rn(v[0], v[1]), h23 = __floats2bfloat162_rn(v[2], v[3]);
+                    const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
+                    const __nv_bfloat162 l01 = __floats2bfloat162_rn(v[0] - f01.x, v[1] - f01.y);
+                    const __nv_bfloat162 l23 = __floats2bfloat162_rn(v[2] - f23.x, v[3] - f23.y);
+                    *reinterpret_cast<uint2 *>(q_hi + o) = make_uint2(*reinterpret_cast<const unsigned *>(&h01),
+                                                                      *reinterpret_cast<const unsigned *>(&h23));
+                    *reinterpret_cast<uint2 *>(q_lo + o) = make_uint2(*reinterpret_cast<const unsigned *>(&l01),
+                                                                      *reinterpret_cast<const unsigned *>(&l23));
+                }
+            }
+            if (vec) {
+                if (lane == 0) norm_out[row] = nrm;
+                return;
+            }
+        }
+        if (g_clear)
+            for (int d = lane; d < q_ld; d += 32) g_clear[(size_t)row * q_ld + d] = 0.0f;
+        for (int d = lane; d < q_ld; d += 32) {
+            const T qv = d < dim ? ps[d] * inv : (T)0;
+            q_out[(size_t)row * q_ld + d] = qv;
+            if (SPLIT) {
+                const float qf = (float)qv;
+                const __nv_bfloat16 h = __float2bfloat16_rn(qf);
+                q_hi[(size_t)row * q_ld + d] = h;
+                q_lo[(size_t)row * q_ld + d] = __float2bfloat16_rn(qf - __bfloat162float(h));
+            }
+        }
+        if (lane == 0) norm_out[row] = nrm;
+    };
+    if constexpr (!PERSIST) {
+        const int row = blockIdx.x * nw + warp;
+        if (row < n_rows) site_body(row);
+    } else {
+        // persistent form: the warp takes sites from the queue until it runs dry
+        for (;;) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(queue, 1);
+            const int row = __shfl_sync(0xffffffffu, r, 0);
+            if (row >= n_rows) break;
+            site_body(row);
             __syncwarp();
         }
-        const int off = P.n_off[s], am = P.alpha_max[s];
-#pragma unroll
-        for (int j = 0; j < KPL; ++j) {
-            const int kk = lane + 32 * j;
-            if (kk < NLM) {
-#pragma unroll
-                for (int n = 0; n < AMB; ++n)
-                    if (n < am) cs[(off + n) * NLM + kk] = acc[j][n];
-            }
-        }
     }
-    __syncwarp();
-    // central atom on l = 0 of its own species block
-    const int s_self = nsp[kb] - 1;
-    if (s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self])
-        cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
-    __syncwarp();
-    warp_copy_row<T>(c_out + (size_t)row * nout, cs, nout, lane);
-    // power spectrum into the (now free) angular area: lane owns the (n, n') pairs
-    // pp = lane + 32 i (n-major, n <= n') and every l, component d = pp (L + 1) + l
-    T *ps = As;
-    T part = 0;
-    const int npair = nmax * (nmax + 1) / 2;
-    for (int pp = lane; pp < npair; pp += 32) {
-        int n = 0, rem = pp;
-        while (rem >= nmax - n) {
-            rem -= nmax - n;
-            ++n;
-        }
-        const int np = n + rem;
-        const T *a = cs + n * NLM, *b = cs + np * NLM;
-        const T sc = (n == np) ? (T)1 : (T)1.4142135623730951;
-#pragma unroll
-        for (int l = 0; l <= L; ++l) {
-            T acc = 0;
-#pragma unroll
-            for (int kk = l * l; kk < (l + 1) * (l + 1); ++kk) acc += a[kk] * b[kk];
-            const T v = acc * sc;
-            ps[pp * (L + 1) + l] = v;
-            part += v * v;
-        }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    const T nrm = t_sqrt<T>(part);
-    const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
-    __syncwarp();
-    // the row of the dE/dq accumulator the GAP kernel adds into (saves a separate clear)
-    if constexpr (std::is_same<T, float>::value) {
-        const bool vec = (q_ld & 3) == 0 && (reinterpret_cast<uintptr_t>(q_out) & 15) == 0 &&
-                         (reinterpret_cast<uintptr_t>(g_clear) & 15) == 0 &&
-                         (!SPLIT || ((reinterpret_cast<uintptr_t>(q_hi) | reinterpret_cast<uintptr_t>(q_lo)) & 7) == 0);
-        // four consecutive components per lane: 16-byte q and dE/dq stores, 8-byte bf16 halves
-        for (int d = 4 * lane; vec && d < q_ld; d += 128) {
-            float v[4];
-#pragma unroll
-            for (int e = 0; e < 4; ++e) v[e] = d + e < dim ? (float)(ps[d + e] * inv) : 0.0f;
-            const size_t o = (size_t)row * q_ld + d;
-            *reinterpret_cast<float4 *>(q_out + o) = make_float4(v[0], v[1], v[2], v[3]);
-            if (g_clear) *reinterpret_cast<float4 *>(g_clear + o) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            if (SPLIT) {
-                const __nv_bfloat162 h01 = __floats2bfloat162_rn(v[0], v[1]), h23 = __floats2bfloat162_rn(v[2], v[3]);
-                const float2 f01 = __bfloat1622float2(h01), f23 = __bfloat1622float2(h23);
-                const __nv_bfloat162 l01 = __floats2bfloat162_rn(v[0] - f01.x, v[1] - f01.y);
-                const __nv_bfloat162 l23 = __floats2bfloat162_rn(v[2] - f23.x, v[3] - f23.y);
-                *reinterpret_cast<uint2 *>(q_hi + o) = make_uint2(*reinterpret_cast<const unsigned *>(&h01),
-                                                                  *reinterpret_cast<const unsigned *>(&h23));
-                *reinterpret_cast<uint2 *>(q_lo + o) = make_uint2(*reinterpret_cast<const unsigned *>(&l01),
-                                                                  *reinterpret_cast<const unsigned *>(&l23));
-            }
-        }
-        if (vec) {
-            if (lane == 0) norm_out[row] = nrm;
-            return;
-        }
-    }
-    if (g_clear)
-        for (int d = lane; d < q_ld; d += 32) g_clear[(size_t)row * q_ld + d] = 0.0f;
-    for (int d = lane; d < q_ld; d += 32) {
-        const T qv = d < dim ? ps[d] * inv : (T)0;
-        q_out[(size_t)row * q_ld + d] = qv;
-        if (SPLIT) {
-            const float qf = (float)qv;
-            const __nv_bfloat16 h = __float2bfloat16_rn(qf);
-            q_hi[(size_t)row * q_ld + d] = h;
-            q_lo[(size_t)row * q_ld + d] = __float2bfloat16_rn(qf - __bfloat162float(h));
-        }
-    }
-    if (lane == 0) norm_out[row] = nrm;
 }
 
 // ----------------------------------------------------------------------------- adjoint
+
+// virial[st] += the symmetric tensor (xx yy zz xy xz yz) in v6 (column-major 3x3).
+__device__ __forceinline__ void add_virial6(double *virial, int st, const double *v6)
+{
+    double *V = virial + 9 * (size_t)st;
+    atomicAdd(V + 0, v6[0]);
+    atomicAdd(V + 4, v6[1]);
+    atomicAdd(V + 8, v6[2]);
+    atomicAdd(V + 3, v6[3]);
+    atomicAdd(V + 1, v6[3]);
+    atomicAdd(V + 6, v6[4]);
+    atomicAdd(V + 2, v6[4]);
+    atomicAdd(V + 7, v6[5]);
+    atomicAdd(V + 5, v6[5]);
+}
 
 // Elements of the c area of the adjoint: c [n_max][NLM] rounded up to 4, and at least the
 // lanes' force/virial partials [32][9] (double) that reuse it after the prologue.
@@ -651,10 +691,12 @@ template <class T> __host__ __device__ constexpr int bwd_m_pitch(int nmax, int m
     return (((nmax * mp + (int)(16 / sizeof(T)) - 1) / (int)(16 / sizeof(T))) | 1) * (int)(16 / sizeof(T));
 }
 
-// Minimum resident CTAs asked of the compiler (1: every instantiation keeps its natural register
-// count; forcing 6 CTAs on the FP32 kernel spilled and ran slower).
-template <class T, int AMB> struct BwdMinCtas {
-    static constexpr int value = 1;
+// Minimum resident CTAs of 4 warps asked of the compiler. The one-site adjoint asks for 1 (its
+// natural register count; forcing 6 CTAs on the FP32 kernel spilled and ran slower). The site loop
+// of the persistent form otherwise keeps loop-invariant values in registers (168 instead of 112 in
+// FP32): it asks for 4 (at most 128 registers) in FP32 and 2 in FP64, where 128 spills.
+template <class T, bool PERSIST> struct BwdMinCtas {
+    static constexpr int value = PERSIST ? (std::is_same<T, float>::value ? 4 : 2) : 1;
 };
 
 // Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (then the lanes'
@@ -663,31 +705,36 @@ template <class T, int AMB> struct BwdMinCtas {
 // species columns (MSP = bwd_m_pitch), f_l / df_l of each lane's pair [2][L+1][32]; after the
 // warps, the CTA's virial partials [kWarpsPerCta][6] and
 // structure ids [kWarpsPerCta].
-template <class T, class GT, int L, int AMB>
-__global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) k_soap_bwd_warp(
+template <class T, class GT, int L, int AMB, bool PERSIST>
+__global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::value) k_soap_bwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
     const T *__restrict__ tq, const float4 *__restrict__ rtab, const int *__restrict__ sites, int n_rows,
     const int64_t *__restrict__ start, const double *__restrict__ rjs, const double *__restrict__ xyz,
     const int *__restrict__ nsp, const int *__restrict__ jatom, const int *__restrict__ site_struct,
     const T *__restrict__ c_in, const T *__restrict__ q_in, int q_ld, const T *__restrict__ norm_in,
     const GT *__restrict__ g_in, int g_ld, double *__restrict__ forces, double *__restrict__ virial,
-    int warp_smem, int n_atoms, int *check, double *__restrict__ pair_der, const double *__restrict__ gate)
+    int warp_smem, int n_atoms, int *check, double *__restrict__ pair_der, const double *__restrict__ gate,
+    int *queue)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int KPL = (NLM + 31) / 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     pdl_enter();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    const int row = blockIdx.x * nw + warp;
-    // pair-derivative mode: a site whose gate is 0 writes nothing (its pairs stay zero)
-    const bool active = row < n_rows && !(pair_der && gate && gate[sites ? sites[row] : row] == 0.0);
     double *vpart = reinterpret_cast<double *>(smem_raw + (size_t)nw * warp_smem);
     int *vstruct = reinterpret_cast<int *>(vpart + 6 * kWarpsPerCta);
-    double vals[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
-    int my_struct = -1;
-    if (active) {
+    if (lane == 0) {
+        vstruct[warp] = -1;
+#pragma unroll
+        for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = 0.0;
+    }
+    __syncwarp();
+    auto site_body = [&](const int row) {
+        // pair-derivative mode: a site whose gate is 0 writes nothing (its pairs stay zero)
+        if (pair_der && gate && gate[sites ? sites[row] : row] == 0.0) return;
+        double vals[9];
         unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
-        const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM, MS = nmax * nmax + 1;
+        const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
         long long *idx = reinterpret_cast<long long *>(wbase);
         T *cs = reinterpret_cast<T *>(wbase + 256);
         T *Gc = cs + bwd_c_elems<T>(nout);
@@ -696,7 +743,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
         T *fdf = Ms + (L + 1) * MSP;  // [2][L+1][32]: f_l, df_l of each lane's pair
 
         const int site = sites ? sites[row] : row;
-        my_struct = site_struct ? site_struct[site] : 0;
+        const int my_struct = site_struct ? site_struct[site] : 0;
         const int64_t kb = start[site], ke = start[site + 1];
         warp_copy_row<T>(cs, c_in + (size_t)row * nout, nout, lane);
         const T *qrow = q_in + (size_t)row * q_ld;
@@ -856,15 +903,37 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, AMB>::value) 
                     check_fail(check, kCheckSelfAtom, kb, js);
             }
         }
+        // the site's virial into the warp's partial, flushed to its structure when the next site
+        // belongs to another one
+        if (!pair_der && lane == 0) {
+            const int cur = vstruct[warp];
+            if (cur != my_struct) {
+                if (cur >= 0) add_virial6(virial, cur, vpart + 6 * warp);
+                vstruct[warp] = my_struct;
+#pragma unroll
+                for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = 0.0;
+            }
+#pragma unroll
+            for (int c = 0; c < 6; ++c) vpart[6 * warp + c] += vals[3 + c];
+        }
+    };
+    if constexpr (!PERSIST) {
+        const int row = blockIdx.x * nw + warp;
+        if (row < n_rows) site_body(row);
+    } else {
+        // persistent form: the warp takes sites from the queue until it runs dry
+        for (;;) {
+            int r = 0;
+            if (lane == 0) r = atomicAdd(queue, 1);
+            const int row = __shfl_sync(0xffffffffu, r, 0);
+            if (row >= n_rows) break;
+            site_body(row);
+            __syncwarp();
+        }
     }
     if (pair_der) return;  // uniform over the grid: no virial in pair-derivative mode
-    // virial (xx yy zz xy xz yz -> column-major 3x3): one set of atomics per CTA when its rows
-    // share a structure, else one per warp
-    if (lane == 0) {
-        vstruct[warp] = my_struct;
-#pragma unroll
-        for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = vals[3 + c];
-    }
+    // virial (xx yy zz xy xz yz -> column-major 3x3): one set of atomics per CTA when its warps'
+    // last structures agree, else one per warp
     __syncthreads();
     if (warp == 0) {
         const int st0 = vstruct[0];
@@ -934,6 +1003,32 @@ inline std::vector<int> warp_candidates(int nw_max)
     return c;
 }
 
+// CTAs of a descriptor launch: one per nw rows, or in the persistent form no more than can be
+// resident on the device at once (the warps loop over the queue).
+inline int site_grid(const void *kern, int nw, size_t smem, int n_rows, bool persistent)
+{
+    const int g = (n_rows + nw - 1) / nw;
+    if (!persistent) return g;
+    static std::mutex mu;
+    static std::map<std::tuple<const void *, int, size_t, int>, int> cache;
+    int dev = 0;
+    cudaGetDevice(&dev);
+    const auto key = std::make_tuple(kern, nw, smem, dev);
+    int cap;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        auto it = cache.find(key);
+        if (it == cache.end()) {
+            int nb = 0, sms = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 32 * nw, smem);
+            cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+            it = cache.emplace(key, std::max(1, nb * sms)).first;
+        }
+        cap = it->second;
+    }
+    return std::min(g, cap);
+}
+
 template <class T> inline const T *soap_tab(const DevBuf &d64, const DevBuf &d32)
 {
     return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
@@ -950,15 +1045,18 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     const bool f64 = std::is_same<T, double>::value;
     const int nw = tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows), f64 ? "soap_forward_f64" : "soap_forward_f32",
                          warp_candidates(nw_max), nw_max);
+    const bool persist =
+        pv.queue && tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows) + "/persist",
+                          f64 ? "soap_forward_f64" : "soap_forward_f32", {0, 1}, 1);
     const size_t sm = wb * nw;
-    auto kern = k_soap_fwd_warp<T, L, AMB, SPLIT>;
+    auto kern = persist ? k_soap_fwd_warp<T, L, AMB, SPLIT, true> : k_soap_fwd_warp<T, L, AMB, SPLIT, false>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + nw - 1) / nw;
+    const int grid = site_grid((const void *)kern, nw, sm, n_rows, persist);
     TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
                               soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(),
                               soap_tab<T>(ds.central, ds.central32), d_sites, n_rows, pv.start, pv.rjs, pv.xyz,
                               pv.species, (T *)o.c, (T *)o.q, o.q_ld, (T *)o.norm, o.q_hi, o.q_lo, (int)wb, pv.check,
-                              pv.geo, o.g_clear));
+                              pv.geo, o.g_clear, persist ? pv.queue : nullptr));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
@@ -975,15 +1073,18 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     const bool f64 = std::is_same<T, double>::value;
     const int nw = tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows), f64 ? "soap_backward_f64" : "soap_backward_f32",
                          warp_candidates(nw_max), nw_max);
+    const bool persist =
+        pv.queue && tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows) + "/persist",
+                          f64 ? "soap_backward_f64" : "soap_backward_f32", {0, 1}, 1);
     const size_t sm = wb * nw + tail;
-    auto kern = k_soap_bwd_warp<T, GT, L, AMB>;
+    auto kern = persist ? k_soap_bwd_warp<T, GT, L, AMB, true> : k_soap_bwd_warp<T, GT, L, AMB, false>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    const int grid = (n_rows + nw - 1) / nw;
+    const int grid = site_grid((const void *)kern, nw, sm, n_rows, persist);
     TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
                               soap_tab<T>(ds.xq, ds.xq32), soap_tab<T>(ds.tq, ds.tq32), ds.rtab.as<float4>(), d_sites,
                               n_rows, pv.start, pv.rjs, pv.xyz, pv.species, pv.jatom, site_struct, (const T *)o.c,
                               (const T *)o.q, o.q_ld, (const T *)o.norm, (const GT *)d_g, g_ld, d_forces, d_virial,
-                              (int)wb, pv.n_atoms, pv.check, pv.pair_der, pv.gate));
+                              (int)wb, pv.n_atoms, pv.check, pv.pair_der, pv.gate, persist ? pv.queue : nullptr));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

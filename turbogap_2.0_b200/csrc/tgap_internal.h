@@ -86,6 +86,7 @@ struct tgap_context {
         int dflt = 0;
     };
     std::map<std::string, int> tune;
+    std::vector<std::pair<std::string, int>> tune_suffix;  // tgap_autotune_set("*suffix", v)
     std::map<std::string, TuneSlot> tune_seen;
     std::string probe_key;
     int probe_val = 0;
@@ -266,6 +267,12 @@ struct PairView {
     double *pair_der = nullptr;
     const double *gate = nullptr;  // with pair_der: sites whose gate value is 0 write nothing
     GeomSrc geo;                   // descriptor forward: pair geometry from positions
+    // persistent form: a zeroed site counter the launch's warps take sites from (grid sized to
+    // what is resident at once); null: one site per warp
+    int *queue = nullptr;
 };
+
+// Site counters of one evaluation (two per model: forward, adjoint), zeroed with its outputs.
+constexpr int kQueueInts = 64;
 
 }  // namespace tgap

@@ -153,6 +153,7 @@ def lib():
         "tgap_autotune": (i32, [vp, vp, i32, vp, i32, i32]),
         "tgap_autotune_report": (i32, [vp, vp, i64, vp]),
         "tgap_autotune_clear": (i32, [vp]),
+        "tgap_autotune_set": (i32, [vp, C.c_char_p, i32]),
         "tgap_screen_eval": (i32, [vp, i64, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, C.c_float, vp, vp]),
         "tgap_debug_poly3_w": (i32, [i32, vp]),
         "tgap_calculate_gap_soap": (i32, [vp, vp, i32, vp, i32, vp, i32, vp, vp, vp]),
