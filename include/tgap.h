@@ -323,8 +323,9 @@ int tgap_autotune_report(tgap_context *ctx, char *buf, int64_t cap, int64_t *nee
 int tgap_autotune_clear(tgap_context *ctx);
 /* Fixes one launch choice: `key` as tgap_autotune_report prints it, or '*' followed by a suffix
  * for every key that ends with that suffix. The suffix "/persist" selects the form of the
- * descriptor kernels: 1 (the default where the evaluation supplies site counters) the persistent
- * work-queue form, 0 one site per warp. An exact key wins over a suffix. */
+ * descriptor kernels: 1 the persistent work-queue form (the default of the mixed path where the
+ * evaluation supplies site counters), 0 one site per warp (the FP64 default). An exact key wins
+ * over a suffix. */
 int tgap_autotune_set(tgap_context *ctx, const char *key, int value);
 
 /* calculate_gap_soap (src/gap/calculate_gap_soap.f90:171-481) with HOST buffers: copies

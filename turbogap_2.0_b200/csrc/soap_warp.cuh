@@ -1004,7 +1004,10 @@ inline std::vector<int> warp_candidates(int nw_max)
 }
 
 // CTAs of a descriptor launch: one per nw rows, or in the persistent form no more than can be
-// resident on the device at once (the warps loop over the queue).
+// resident on the device at once (the warps loop over the queue). The persistent form is the
+// default in FP32 (as fast as one site per warp on a uniform system, and it balances uneven
+// batches); FP64 defaults to one site per warp (its site loop needs 182 registers: 198 against
+// 170 us for the 4096-atom adjoint).
 inline int site_grid(const void *kern, int nw, size_t smem, int n_rows, bool persistent)
 {
     const int g = (n_rows + nw - 1) / nw;
@@ -1047,7 +1050,7 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                          warp_candidates(nw_max), nw_max);
     const bool persist =
         pv.queue && tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows) + "/persist",
-                          f64 ? "soap_forward_f64" : "soap_forward_f32", {0, 1}, 1);
+                          f64 ? "soap_forward_f64" : "soap_forward_f32", {0, 1}, f64 ? 0 : 1);
     const size_t sm = wb * nw;
     auto kern = persist ? k_soap_fwd_warp<T, L, AMB, SPLIT, true> : k_soap_fwd_warp<T, L, AMB, SPLIT, false>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
@@ -1075,7 +1078,7 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                          warp_candidates(nw_max), nw_max);
     const bool persist =
         pv.queue && tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows) + "/persist",
-                          f64 ? "soap_backward_f64" : "soap_backward_f32", {0, 1}, 1);
+                          f64 ? "soap_backward_f64" : "soap_backward_f32", {0, 1}, f64 ? 0 : 1);
     const size_t sm = wb * nw + tail;
     auto kern = persist ? k_soap_bwd_warp<T, GT, L, AMB, true> : k_soap_bwd_warp<T, GT, L, AMB, false>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
