@@ -20,7 +20,11 @@ constexpr int kMaxAlpha = 16;     // radial functions per species
 constexpr int kMaxNmax = 16;      // radial functions summed over species
 constexpr int kMaxL = 10;         // l_max
 constexpr int kMaxNodes = 192;    // quadrature nodes per species
-constexpr int kTabIntervals = 1024;  // radial table intervals over [0, rcut_hard] (mixed path)
+// Radial table intervals over [0, rcut_hard] (mixed path). The cubic Hermite interpolant's error
+// against the FP64 radial functions is 6.6e-9 of max |R_n| at 256 intervals for the carbon
+// settings (rcut 3.7 A, sigma 0.5 A; 2.5e-11 at 1024, 1.0e-7 at 128), ten times below the FP32
+// rounding of the stored coefficients, and the table (32 KB per species at alpha_max 8) stays in L1.
+constexpr int kTabIntervals = 256;
 
 struct Error {
     int status;
