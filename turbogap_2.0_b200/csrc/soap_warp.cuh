@@ -347,16 +347,19 @@ __device__ __forceinline__ void dot_even_odd(const T x[N], const T y[N], T &s0, 
 //   w = u (A1 - u.Gam) + Gam,  A1 = sum_lm Y_lm (f_l V_lm + df_l U_lm),
 //   Gam = (1/r) sum_lm f_l U_lm dY_lm/du,   U_lm = Gc[lm].R, V_lm = Gc[lm].R'
 // which equals sum_lm [u Y (f V + df U) + f U (grad Y - u (u.grad Y)) / r]. The order m is
-// unrolled (compile time) and the degree l = m..L runs as a loop (L+1 copies of the body, in the
-// instruction cache). The Legendre factor is carried fully normalised (Qb = N Q) by the
-// three-term recurrence Qb_{l+1} = ra uz Qb_l - rb Qb_{l-1}, advanced at the end of each pass so
-// the body has no branch; the Gc row, f_l / df_l (fl[l * 32] / dfl[l * 32]) and the recurrence
+// unrolled (compile time) and the degree l = m..L runs as a loop (in the instruction cache). The
+// Legendre factor is carried fully normalised (Qb = N Q) by the three-term recurrence
+// Qb_{l+1} = ra uz Qb_l - rb Qb_{l-1}, advanced at the end of each pass so the body has no
+// branch; the Gc row, f_l / df_l (fl[l * 32] / dfl[l * 32]) and the recurrence
 // coefficients are reached by running offsets. The cos and sin harmonics of one (l, m) share
 // their Legendre factors and read their two adjacent Gc rows together.
 template <class T, int L, int AMB>
 __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T uz, T ir, const T *fl, const T *dfl,
                                              const T *__restrict__ Gs, const T R[AMB], const T dR[AMB], T w[3])
 {
+    // the degree loop runs unrolled by 2 in FP32 (46 against 48 us for the 4096-atom adjoint: the
+    // recurrence's rotation of Q, dQ needs no moves); in FP64 that costs registers and runs slower
+    constexpr int kDegUnroll = std::is_same<T, float>::value ? 2 : 1;
     T A1 = 0, Gx = 0, Gy = 0, Gz = 0;
     // m = 0: Y = Qb, dY/du = (0, 0, dQb)
     {
@@ -364,7 +367,7 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
         const T *row = Gs;
         int step = AMB;  // row (l+1)^2 - row l^2, in elements
         const T *f = fl, *df = dfl;
-#pragma unroll 1
+#pragma unroll(kDegUnroll)
         for (int l = 0; l <= L; ++l) {
             T g[AMB];
             load_vec<T, AMB>(row, g);
@@ -401,7 +404,7 @@ __device__ __forceinline__ void pair_adjoint(const YlmConst &Yc, T ux, T uy, T u
         const T *row = Gs + (m * m + 2 * m - 1) * AMB;
         int step = (2 * m + 1) * AMB;
         const T *f = fl + m * 32, *df = dfl + m * 32;
-#pragma unroll 1
+#pragma unroll(kDegUnroll)
         for (int l = m; l <= L; ++l) {
             T gc[AMB], gs[AMB];
             load_vec<T, AMB>(row, gc);
