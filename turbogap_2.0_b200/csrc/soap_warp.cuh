@@ -735,7 +735,6 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
     auto site_body = [&](const int row) {
         // pair-derivative mode: a site whose gate is 0 writes nothing (its pairs stay zero)
         if (pair_der && gate && gate[sites ? sites[row] : row] == 0.0) return;
-        double vals[9];
         unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
         const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
         long long *idx = reinterpret_cast<long long *>(wbase);
@@ -887,15 +886,17 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
             }
             __syncwarp();
         }
-#pragma unroll
-        for (int i = 0; i < 9; ++i) vals[i] = vl[i];
-#pragma unroll
-        for (int i = 0; i < 9; ++i) {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) vals[i] += __shfl_xor_sync(0xffffffffu, vals[i], o);
+        // component c < 9 of the site's sum: lane c adds column c of the 32 lanes' rows in lane
+        // order (components 0-2: the self force; 3-8: the virial)
+        __syncwarp();  // every lane's row is complete (also when the site had no pairs)
+        double csum = 0.0;
+        if (lane < 9) {
+            const double *col = reinterpret_cast<const double *>(cs) + lane;
+#pragma unroll 8
+            for (int q = 0; q < 32; ++q) csum += col[9 * q];
         }
         if (lane < 3) {
-            const double fv = lane == 0 ? vals[0] : (lane == 1 ? vals[1] : vals[2]);
+            const double fv = csum;
             if (pair_der) {
                 pair_der[3 * kb + lane] = -fv;  // dq_i/dr_i = -sum_j dq_i/dr_j
             } else {
@@ -908,16 +909,18 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
         }
         // the site's virial into the warp's partial, flushed to its structure when the next site
         // belongs to another one
-        if (!pair_der && lane == 0) {
-            const int cur = vstruct[warp];
-            if (cur != my_struct) {
-                if (cur >= 0) add_virial6(virial, cur, vpart + 6 * warp);
-                vstruct[warp] = my_struct;
+        if (!pair_der) {
+            if (lane == 0) {
+                const int cur = vstruct[warp];
+                if (cur != my_struct) {
+                    if (cur >= 0) add_virial6(virial, cur, vpart + 6 * warp);
+                    vstruct[warp] = my_struct;
 #pragma unroll
-                for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = 0.0;
+                    for (int c = 0; c < 6; ++c) vpart[6 * warp + c] = 0.0;
+                }
             }
-#pragma unroll
-            for (int c = 0; c < 6; ++c) vpart[6 * warp + c] += vals[3 + c];
+            __syncwarp();
+            if (lane >= 3 && lane < 9) vpart[6 * warp + lane - 3] += csum;
         }
     };
     if constexpr (!PERSIST) {
