@@ -57,6 +57,8 @@ int tgap_destroy(tgap_context *ctx);
 /* Use an external stream (cudaStream_t) for all later work; NULL restores the own stream. */
 int tgap_set_stream(tgap_context *ctx, void *stream);
 int tgap_synchronize(tgap_context *ctx);
+/* Message of the last failed call on ctx; with ctx == NULL, of the last failed context-free call
+ * (tgap_soap_energies_noalloc) made by the calling host thread. */
 const char *tgap_last_error(const tgap_context *ctx);
 const char *tgap_version(void);
 /* Number of kernels this library launched on ctx since creation (instrumentation). */
@@ -157,11 +159,16 @@ int tgap_local_property_predict(tgap_context *ctx, int n_soap, int n_sites, int 
  * that is read is first written by the same call, so nothing has to start at zero, but calls
  * whose work overlaps on the GPU (other streams, other host threads) race on it and must be
  * serialized by the caller. The first call on each device looks up the array's device address
- * (cudaGetSymbolAddress) with that device current; make that first call before any stream
- * capture. Pointers are device pointers in the layout of tgap_get_soap_energy_and_forces
- * (d_soap: n_soap x n_sites, d_Qs: n_soap x n_sparse, d_alphas: n_sparse, d_energies:
- * n_sites, overwritten). Work is queued on `stream` (a cudaStream_t, NULL = default stream);
- * the call does not synchronize. */
+ * (cudaGetSymbolAddress) with that device current and keeps it for later calls; make that first
+ * call before any stream capture. The kept address belongs to the device's primary context: after
+ * a cudaDeviceReset of that device, do not call this entry again in the same process.
+ * `stream` (a cudaStream_t, NULL = default stream) must belong to the current device, otherwise
+ * TGAP_ERR_ARGUMENT; the scratch address used is the current device's. Pointers are device
+ * pointers in the layout of tgap_get_soap_energy_and_forces (d_soap: n_soap x n_sites, d_Qs:
+ * n_soap x n_sparse, d_alphas: n_sparse, d_energies: n_sites, overwritten). The call does not
+ * synchronize; its status covers its own launches (an error left pending by earlier work on the
+ * device is neither reported nor cleared), and a failure leaves a message for
+ * tgap_last_error(NULL). */
 int tgap_soap_energies_noalloc(void *stream, int n_soap, int n_sites, int n_sparse,
                                const double *d_soap, const double *d_alphas, double delta,
                                double zeta0, double e0, const double *d_Qs, double *d_energies);
@@ -230,8 +237,18 @@ int tgap_system_set_positions(tgap_system *system, const double *positions);
 int tgap_system_update(tgap_system *system, int rebuild);
 int64_t tgap_system_n_pairs(const tgap_system *system);
 
+/* calculate_e0 (src/gap/calculate_gap_soap.f90:135-169): isolated-atom energies per species
+ * channel, e0[c - 1] for channel c = 1..n_species (the input file's `e0` keyword,
+ * src/read/read_files.f90:380-385). Every later energy output of the system (tgap_compute,
+ * tgap_calculate_gap_soap, the MD potential energy, the MC state) adds each atom's e0, as
+ * turbogap_main.f90:993-994 adds energies_e0 to the total; atoms of a channel outside 1..n_species
+ * get 0. Set it before creating MD objects on the system, or call it again with the same
+ * n_species to change the values. Forces, virials and MC energy differences are unaffected. */
+int tgap_system_set_e0(tgap_system *system, int n_species, const double *e0);
+
 /* Energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure), device pointers,
- * summed over models (e0 = 0). Overwrites the outputs. */
+ * summed over models, plus each atom's e0 (tgap_system_set_e0; 0 when never set). Overwrites the
+ * outputs. */
 int tgap_compute(tgap_context *ctx, tgap_system *system, int n_models,
                  tgap_model *const *models, int precision, int do_forces, double *d_energies,
                  double *d_forces, double *d_virial);
@@ -331,7 +348,8 @@ int tgap_autotune_set(tgap_context *ctx, const char *key, int value);
 /* calculate_gap_soap (src/gap/calculate_gap_soap.f90:171-481) with HOST buffers: copies
  * `positions` (3 x n_atoms, NULL = keep the resident ones) to the device, rebuilds the
  * neighbor list when rebuild != 0 (else refreshes geometry), evaluates all models and copies
- * energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure) back. */
+ * energies (n_atoms, with the system's e0 as in tgap_compute), forces (3 x n_atoms) and virial
+ * (9 per structure) back. */
 int tgap_calculate_gap_soap(tgap_context *ctx, tgap_system *system, int n_models,
                             tgap_model *const *models, int precision, const double *positions,
                             int rebuild, double *energies, double *forces, double *virial);

@@ -608,3 +608,14 @@ double orc_mc_move_acceptance(double e_new, double e_prev, double temp)
     double p = exp(-(e_new - e_prev) / (kB * temp));
     return p < 1.0 ? p : 1.0;
 }
+
+/* calculate_e0 (src/gap/calculate_gap_soap.f90:135-169): for every site, the loop over
+ * j = 1..n_species sets energies_e0(i) = e0(j) when the site's species is species_types(j);
+ * species are channel ids here (1..n_species), so the match is species(i) == j. Sites of no
+ * listed species keep the value they had (zero after reset, calculation.f90:234-235). */
+void orc_calculate_e0(int n_sites, const int *species, int n_species, const double *e0, double *energies_e0)
+{
+    for (int i = 0; i < n_sites; ++i)
+        for (int j = 1; j <= n_species; ++j)
+            if (species[i] == j) energies_e0[i] = e0[j - 1];
+}

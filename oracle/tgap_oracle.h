@@ -176,6 +176,9 @@ void orc_velocity_verlet(int n_sites, double *positions, double *positions_prev,
  * kB is the reference's default-real literal 8.617333262e-5 (rounded to binary32). */
 double orc_mc_move_acceptance(double e_new, double e_prev, double temp);
 
+/* calculate_e0 (calculate_gap_soap.f90:135-169): per-site e0 by species channel. */
+void orc_calculate_e0(int n_sites, const int *species, int n_species, const double *e0, double *energies_e0);
+
 /* Thread count used by the OpenMP regions (for the CPU baseline). */
 int orc_num_threads(void);
 

@@ -73,6 +73,7 @@ def lib():
         L.orc_get_gap_soap.argtypes = [C.POINTER(_Hypers), C.c_int, C.c_int, _ip, _ip, _dp, _dp,
                                        _dp, _dp, _ip, C.c_int, C.c_int, _dp, _dp, C.c_double,
                                        C.c_double, C.c_int, _dp, _dp, _dp]
+        L.orc_calculate_e0.argtypes = [C.c_int, _ip, C.c_int, _dp, _dp]
         L.orc_local_property_predict.argtypes = [C.c_int, C.c_int, C.c_int, _dp, _dp, _dp, C.c_double,
                                                  C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, _dp]
         L.orc_get_2b_energy_and_forces.argtypes = [C.c_int, _dp, _dp, C.c_int, _dp, _dp, C.c_double, C.c_double,
@@ -364,6 +365,15 @@ def velocity_verlet(pos, pos_prev, vel, forces, forces_prev, masses, dt, dt_prev
 
 def mc_move_acceptance(e_new, e_prev, temp):
     return lib().orc_mc_move_acceptance(e_new, e_prev, temp)
+
+
+def calculate_e0(species, e0):
+    """Per-site e0 by species channel (calculate_gap_soap.f90:135-169), zero for other sites."""
+    sp = np.ascontiguousarray(species, np.int32)
+    e = np.ascontiguousarray(e0, float)
+    out = np.zeros(len(sp))
+    lib().orc_calculate_e0(len(sp), sp, len(e), e, out)
+    return out
 
 
 def num_threads():

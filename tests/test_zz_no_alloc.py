@@ -36,7 +36,10 @@ def _inputs(seed, n_sites=300, n_sparse=150, dim=324):
     return q, Qs, alphas
 
 
-def test_noalloc_energies_match_allocating_entry_twice(tg):
+@pytest.mark.parametrize("zeta,delta", [(4.0, 1.0), (2.5, 0.7), (4.0, 1.3)])
+def test_noalloc_energies_match_allocating_entry_twice(tg, zeta, delta):
+    """zeta = 4 takes the integer-power path of the GEMM epilogue, 2.5 the real power (the
+    integer test of gap.f90:99-105 fails); delta scales every energy by delta^2."""
     import torch
     from turbogap_b200 import native
     noalloc = _bind(native)
@@ -44,7 +47,7 @@ def test_noalloc_energies_match_allocating_entry_twice(tg):
     n_sites, dim = q.shape
     ctx = tg.Context(0)
     ones = np.ones(n_sites, np.int32)
-    e_ref, _, _ = ctx.get_soap_energy_and_forces(q, None, alphas, 1.0, 4.0, -0.25, Qs, ones,
+    e_ref, _, _ = ctx.get_soap_energy_and_forces(q, None, alphas, delta, zeta, -0.25, Qs, ones,
                                                  np.arange(1, n_sites + 1), np.zeros((n_sites, 3)),
                                                  do_forces=False)
     ctx.close()
@@ -56,7 +59,7 @@ def test_noalloc_energies_match_allocating_entry_twice(tg):
     for call in range(2):
         de.fill_(float("nan"))  # the call must overwrite every output
         st = noalloc(C.c_void_p(stream), dim, n_sites, len(alphas), C.c_void_p(dq.data_ptr()),
-                     C.c_void_p(da.data_ptr()), 1.0, 4.0, -0.25, C.c_void_p(dQ.data_ptr()),
+                     C.c_void_p(da.data_ptr()), delta, zeta, -0.25, C.c_void_p(dQ.data_ptr()),
                      C.c_void_p(de.data_ptr()))
         assert st == 0, f"call {call}: status {st}"
         torch.cuda.synchronize()
@@ -74,4 +77,5 @@ def test_noalloc_rejects_sizes_beyond_its_scratch(tg):
     # 2^20 + 1 sites x 1 tile of sparse points exceeds the 2^20 partials; refused before any launch
     st = noalloc(None, 8, (1 << 20) + 1, 64, p, p, 1.0, 4.0, 0.0, p, p)
     assert st == 3  # TGAP_ERR_CAPACITY
+    assert b"exceeds" in native.lib().tgap_last_error(None)  # the calling thread's context-free message
     assert noalloc(None, 8, 0, 64, p, p, 1.0, 4.0, 0.0, p, p) == 1  # TGAP_ERR_ARGUMENT

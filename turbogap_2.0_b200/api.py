@@ -334,6 +334,26 @@ class System:
     def update(self, rebuild=True):
         check(self.ctx._L.tgap_system_update(self.h, int(rebuild)), self.ctx.h, "tgap_system_update")
 
+    def set_e0(self, e0):
+        """Isolated-atom energy per species channel (e0[c - 1] for channel c), added to every
+        energy output of the system (calculate_e0, calculate_gap_soap.f90:135-169)."""
+        e = _f64(e0).reshape(-1)
+        check(self.ctx._L.tgap_system_set_e0(self.h, len(e), ptr(e)), self.ctx.h, "tgap_system_set_e0")
+
+    def calculate_gap_soap(self, models, precision, positions=None, rebuild=True):
+        """Host-buffer evaluation (tgap_calculate_gap_soap): positions (n, 3) in (None keeps the
+        resident ones), energies (n,), forces (n, 3) and per-structure virials (n_structures, 3, 3)
+        out."""
+        arr = (C.c_void_p * len(models))(*[m.h.value for m in models])
+        e = np.zeros(self.n_atoms)
+        f = np.zeros((self.n_atoms, 3))
+        v = np.zeros((self.n_structures, 9))
+        x = None if positions is None else _f64(positions).reshape(self.n_atoms, 3)
+        check(self.ctx._L.tgap_calculate_gap_soap(self.ctx.h, self.h, len(models), arr, int(precision),
+                                                  ptr(x) if x is not None else None, int(rebuild), ptr(e), ptr(f),
+                                                  ptr(v)), self.ctx.h, "tgap_calculate_gap_soap")
+        return e, f, v.reshape(self.n_structures, 3, 3)
+
     def compute_device(self, models, precision, d_energies, d_forces, d_virial, do_forces=True):
         """Device-pointer form: outputs are raw device addresses (ints)."""
         arr = (C.c_void_p * len(models))(*[m.h.value for m in models])

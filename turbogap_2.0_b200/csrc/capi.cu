@@ -90,6 +90,21 @@ int set_error(tgap_context *ctx, int status, const char *fmt, ...)
     return status;
 }
 
+static thread_local std::string t_last_error;
+
+int thread_error(int status, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    t_last_error = buf;
+    return status;
+}
+
+const char *thread_error_text() { return t_last_error.c_str(); }
+
 int tuned(tgap_context *ctx, const std::string &key, const char *stage, const std::vector<int> &candidates, int dflt)
 {
     if (!ctx) return dflt;
@@ -275,7 +290,7 @@ extern "C" int tgap_synchronize(tgap_context *ctx)
 
 extern "C" const char *tgap_last_error(const tgap_context *ctx)
 {
-    return ctx ? ctx->last_error.c_str() : "null context";
+    return ctx ? ctx->last_error.c_str() : thread_error_text();
 }
 
 extern "C" int64_t tgap_kernel_launches(const tgap_context *ctx) { return ctx ? ctx->launches : 0; }
@@ -751,6 +766,9 @@ struct tgap_system {
     DevBuf c, q, norm, q_hi, q_lo, e_rows;
     GapWork gw;
     DevBuf scratch_forces;
+    // per-atom isolated-atom energies (calculate_e0), added to every energy output when set
+    std::vector<double> host_e0;
+    DevBuf d_e0;
 };
 
 extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
@@ -828,7 +846,8 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
-                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species, &s->queue};
+                      &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species, &s->queue,
+                      &s->d_e0};
     for (DevBuf *b : bufs) b->release();
     delete s;
     return TGAP_OK;
@@ -852,6 +871,31 @@ extern "C" int tgap_system_set_positions(tgap_system *s, const double *positions
     TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, positions, sizeof(double) * 3 * s->nb.n_atoms,
                                    cudaMemcpyHostToDevice, ctx->stream));
     return TGAP_OK;
+}
+
+// calculate_e0 (calculate_gap_soap.f90:135-169): every atom gets the e0 of its species (the input
+// file's e0 keyword, read_files.f90:380-385); atoms of no listed species keep 0.
+extern "C" int tgap_system_set_e0(tgap_system *s, int n_species, const double *e0)
+{
+    if (!s || n_species < 0 || (n_species > 0 && !e0)) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = s->ctx;
+    CHECK_RC(activate(ctx));
+    const size_t N = s->host_species.size();
+    std::vector<double> v(N, 0.0);
+    for (size_t i = 0; i < N; ++i) {
+        const int sp = s->host_species[i];
+        if (sp >= 1 && sp <= n_species) v[i] = e0[sp - 1];
+    }
+    CHECK_RC(upload(ctx, s->d_e0, v.data(), N));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    s->host_e0.swap(v);
+    return TGAP_OK;
+}
+
+__global__ void k_add_e0(int n, const double *__restrict__ e0, double *__restrict__ energies)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) energies[i] += e0[i];
 }
 
 extern "C" int tgap_system_update(tgap_system *s, int rebuild)
@@ -1010,6 +1054,11 @@ static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_
     for (int i = 0; i < n_models; ++i)
         CHECK_RC(compute_model(ctx, s, models[i], precision, do_forces, d_energies, d_forces, d_virial, geom,
                                queue ? queue + 2 * i : nullptr));
+    if (!s->host_e0.empty()) {
+        // turbogap_main.f90:994: the total energy of each atom adds its e0
+        k_add_e0<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, s->d_e0.as<double>(), d_energies);
+        TGAP_LAUNCH_CHECK(ctx);
+    }
     return TGAP_OK;
 }
 
@@ -2187,9 +2236,11 @@ extern "C" int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energie
     McDev h;
     CHECK_RC(mc_read_state(mc, &h));
     double tot = 0.0;
+    const std::vector<double> &e0 = mc->sys->host_e0;  // calculate_e0: constant under moves
     for (int i = 0; i < N; ++i) {
         double v = 0.0;
         for (int m = 0; m < M; ++m) v += e[(size_t)m * N + i];
+        if (!e0.empty()) v += e0[i];
         if (energies) energies[i] = v;
         tot += v;
     }

@@ -111,6 +111,8 @@ class StageScope {
 };
 
 int set_error(tgap_context *ctx, int status, const char *fmt, ...);
+// Error message of an entry point that has no context (per host thread; tgap_last_error(NULL)).
+int thread_error(int status, const char *fmt, ...);
 
 // Launch choice for `key`: the probed value while the autotuner times it, else the tuned value,
 // else dflt. Registers the key with its timing stage and candidates (the first candidate list
