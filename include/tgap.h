@@ -407,7 +407,10 @@ int tgap_mc_get_state(tgap_mc *mc, double *positions, double *energies, double *
  * FP32 accumulation). Each proposal is first tested with min(1, exp(-dE_s / kB T)) > u1; only
  * survivors get the exact GAP energies and min(1, exp(-(dE - dE_s) / kB T)) > u2. With a screen
  * set, tgap_mc_run takes two deviates per proposal (u1, u2 interleaved). Mixed precision, one
- * model over all sites. */
+ * model over all sites. With a speculative batch (tgap_mc_set_batch, default 12 slots) the screen
+ * judges every slot of a batch from the state before it, the exact GAP kernel skips the 128-row
+ * tiles of slots it rejects, and the slots are settled in order with the same decisions as one at a
+ * time. */
 int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden, const float *mean,
                        const float *pca, const float *w1, const float *b1, const float *w2,
                        const float *b2, const float *w3, float b3);
@@ -416,10 +419,12 @@ int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char 
 /* Fallback to plain GAP MC (no counterpart in the reference, whose MC has no screen). Over each
  * window of `window` screen-judged proposals, pass = fraction passed to the exact stage and
  * confirm = fraction of those the exact stage accepts; when pass < min_pass, or confirm <
- * min_confirm with at least 32 passed, the screen is switched off for the rest of the MC object's
- * life (or until tgap_mc_set_screen installs one again). Proposals still take deviate pairs; plain
- * moves use the first. Defaults: 2048, 0.1, 0.002. */
-int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass);
+ * min_confirm with at least 32 passed, or pass > max_pass (the screen settles too few proposals to
+ * pay for its own evaluation: delayed acceptance saves only the exact energies of the proposals it
+ * rejects), the screen is switched off for the rest of the MC object's life (or until
+ * tgap_mc_set_screen installs one again). Proposals still take deviate pairs; plain moves use the
+ * first. Defaults: 2048, 0.1, 0.002, 0.99. */
+int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass, double max_pass);
 /* Speculative batch of plain GAP MC (no counterpart in the reference, which judges proposals one
  * at a time): `slots` consecutive proposals (1..16; default 12 mixed, 4 FP64) are evaluated side by side from
  * the same state and then settled in order on the device. A proposal's energy change depends
@@ -427,7 +432,8 @@ int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, dou
  * earlier proposal of the batch moved an atom within 2 rc + |d_i| + |d_k| of it (minimum image;
  * in a cell replicated into a supercell, any two proposals of the structure); the batch stops
  * at the first one that is not valid, and that proposal opens the next batch. Decisions and
- * final positions are those of one-at-a-time evaluation. Used whenever no screen is active. */
+ * final positions are those of one-at-a-time evaluation. With a screen active the batch applies
+ * delayed acceptance (tgap_mc_set_screen); one slot keeps the one-at-a-time screened step. */
 int tgap_mc_set_batch(tgap_mc *mc, int slots);
 /* Batches run since creation and the proposals they settled. */
 int tgap_mc_batch_stats(tgap_mc *mc, int64_t *batches, int64_t *settled);

@@ -1832,11 +1832,12 @@ struct tgap_mc {
     // screen_active: used by the step (off after a fallback to plain GAP MC)
     bool screened = false, screen_active = false;
     int64_t fb_window = 2048;                     // screened proposals per fallback check
-    double fb_min_confirm = 0.1, fb_min_pass = 0.002;
+    double fb_min_confirm = 0.1, fb_min_pass = 0.002, fb_max_pass = 0.99;
     long long fb_prop0 = 0, fb_pass0 = 0, fb_conf0 = 0;  // counters at the start of the window
     int64_t fallbacks = 0;
     ScreenDev sd{};
     DevBuf s_mean, s_pca, s_w1, s_b1, s_w2, s_b2, s_w3, es_cache, es_trial;
+    DevBuf tskip;  // per row tile of the trial rows: skipped by the exact GAP kernel (screened batch)
     int64_t last_n = 0;
 };
 
@@ -1869,7 +1870,8 @@ static int mc_size_trial(tgap_mc *mc)
     if (mc->sites.ensure(sizeof(int) * (size_t)M * rows) || mc->tstart.ensure(sizeof(int64_t) * (rows + 1)) ||
         mc->txyz.ensure(sizeof(double) * 3 * slots) || mc->trjs.ensure(sizeof(double) * slots) ||
         mc->tnsp.ensure(sizeof(int) * slots) || mc->etrial.ensure(sizeof(double) * (size_t)M * rows) ||
-        mc->es_trial.ensure(sizeof(float) * cap))
+        mc->es_trial.ensure(sizeof(float) * (size_t)rows) ||
+        mc->tskip.ensure(sizeof(int) * (size_t)((rows + 127) / 128)))
         return set_error(ctx, TGAP_ERR_NOMEM, "Monte Carlo trial buffers");
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->tnsp.ptr, 0, sizeof(int) * slots, ctx->stream));
     TGAP_CUDA(ctx, cudaMemsetAsync(mc->trjs.ptr, 0, sizeof(double) * slots, ctx->stream));
@@ -1987,14 +1989,26 @@ static int mc_step_body_batch(tgap_mc *mc)
             o.q_hi = mc->q_hi[m].as<__nv_bfloat16>();
             o.q_lo = mc->q_lo[m].as<__nv_bfloat16>();
             CHECK_RC(soap_forward(ctx, md->soap, pv, nullptr, rows, TGAP_MIXED, o));
+            const int *skip_tiles = nullptr;
+            if (mc->screen_active) {
+                // delayed acceptance, stage 1 of every slot from the screen energies of its rows;
+                // the exact GAP kernel skips the row tiles of slots the screen rejects
+                const int n_tiles = (rows + 127) / 128;
+                CHECK_RC(screen_rows(ctx, mc->sd, (const float *)o.q, o.q_ld, rows, nullptr, mc->es_trial.as<float>()));
+                CHECK_RC(mc_screen_batch(ctx, st, mc->sites.as<int>(), cap, B, mc->es_trial.as<float>(),
+                                         mc->es_cache.as<float>(), mc->pu.as<double>(), mc->temperature,
+                                         mc->tskip.as<int>(), n_tiles));
+                skip_tiles = mc->tskip.as<int>();
+            }
             CHECK_RC(gap_energy_grad_mixed(ctx, md->gap, o.q_hi, o.q_lo, rows, 0.0, 0, &mc->gw[m], nullptr, e_rows,
-                                           nullptr));
+                                           nullptr, nullptr, false, skip_tiles));
         }
     }
     return mc_resolve_batch(ctx, st, nb, M, mc->sites.as<int>(), cap, B, mc->etrial.as<double>(),
                             mc->ecache.as<double>(), nb.positions.as<double>(), mc->dacc.as<double>(),
                             mc->pu.as<double>(), mc->screened ? 2 : 1, mc->temperature, mc->rc_sel, mc->skin,
-                            mc_logs(mc));
+                            mc_logs(mc), mc->screen_active ? 1 : 0, mc->es_trial.as<float>(),
+                            mc->es_cache.as<float>());
 }
 
 static void mc_drop_graph(tgap_mc *mc)
@@ -2005,11 +2019,13 @@ static void mc_drop_graph(tgap_mc *mc)
     mc->graph = nullptr;
 }
 
-// Fallback to plain GAP MC when the screen's acceptance collapses: over each window of
-// fb_window screened proposals, the fraction passed to the exact stage (pass) and the fraction of
-// those the exact energies confirm (confirm). Either falling below its floor switches the screen
-// off; the chain's target distribution is the same either way, so the switch may happen at any
-// proposal boundary. Returns true when it switched.
+// Fallback to plain GAP MC when the screen's acceptance collapses, or when it settles almost
+// nothing: over each window of fb_window screened proposals, the fraction passed to the exact stage
+// (pass) and the fraction of those the exact energies confirm (confirm). Either falling below its
+// floor switches the screen off, and so does pass above fb_max_pass (delayed acceptance saves only
+// the exact evaluations of the proposals the screen rejects; when it rejects fewer than 1 - max_pass
+// of them, its own evaluation costs more than it saves). The chain's target distribution is the
+// same either way, so the switch may happen at any proposal boundary. Returns true when it switched.
 static bool mc_screen_check(tgap_mc *mc, const McDev &h)
 {
     if (!mc->screen_active) return false;
@@ -2021,7 +2037,8 @@ static bool mc_screen_check(tgap_mc *mc, const McDev &h)
     mc->fb_prop0 = h.s_prop;
     mc->fb_pass0 = h.s_pass;
     mc->fb_conf0 = h.s_conf;
-    if (pass >= mc->fb_min_pass && (npass < 32 || confirm >= mc->fb_min_confirm)) return false;
+    if (pass >= mc->fb_min_pass && pass <= mc->fb_max_pass && (npass < 32 || confirm >= mc->fb_min_confirm))
+        return false;
     mc->screen_active = false;
     ++mc->fallbacks;
     mc_drop_graph(mc);
@@ -2106,7 +2123,7 @@ extern "C" int tgap_mc_destroy(tgap_mc *mc)
     DevBuf *bufs[] = {&mc->st, &mc->ecache, &mc->dacc, &mc->mark, &mc->sites, &mc->tstart, &mc->txyz, &mc->trjs,
                       &mc->tnsp, &mc->etrial, &mc->patom, &mc->pdisp, &mc->pu, &mc->log_de, &mc->log_acc,
                       &mc->log_des, &mc->log_stage, &mc->s_mean, &mc->s_pca, &mc->s_w1, &mc->s_b1, &mc->s_w2,
-                      &mc->s_b2, &mc->s_w3, &mc->es_cache, &mc->es_trial};
+                      &mc->s_b2, &mc->s_w3, &mc->es_cache, &mc->es_trial, &mc->tskip};
     for (DevBuf *b : bufs) b->release();
     for (auto *v : {&mc->c, &mc->q, &mc->norm, &mc->q_hi, &mc->q_lo})
         for (DevBuf &b : *v) b.release();
@@ -2186,7 +2203,7 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
                 TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
                 const int64_t launches = ctx->launches;
                 int rc = TGAP_OK;
-                if (mc->screen_active)
+                if (mc->screen_active && mc->batch <= 1)
                     for (int b = 0; b < kMcBatch && !rc; ++b) rc = mc_step_body(mc);
                 else
                     for (int b = 0; b < kMcBatchSteps && !rc; ++b) rc = mc_step_body_batch(mc);
@@ -2210,7 +2227,7 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
             }
             TGAP_CUDA(ctx, cudaGraphLaunch(mc->exec, ctx->stream));
             ctx->launches += mc->graph_kernels;
-        } else if (mc->screen_active) {
+        } else if (mc->screen_active && mc->batch <= 1) {
             for (int b = 0; b < kMcBatch; ++b) CHECK_RC(mc_step_body(mc));
         } else {
             for (int b = 0; b < kMcBatchSteps; ++b) CHECK_RC(mc_step_body_batch(mc));
@@ -2290,7 +2307,8 @@ extern "C" int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden,
     // screen energies of every atom at the current positions (FP32 descriptors of the mixed path)
     tgap_system *sys = mc->sys;
     const int N = sys->nb.n_atoms;
-    if (mc->es_cache.ensure(sizeof(float) * N) || mc->es_trial.ensure(sizeof(float) * mc->cap))
+    if (mc->es_cache.ensure(sizeof(float) * N) ||
+        mc->es_trial.ensure(sizeof(float) * (size_t)std::max(mc->sized_batch, 1) * mc->cap))
         return set_error(ctx, TGAP_ERR_NOMEM, "screen caches");
     CHECK_RC(neighbors_refresh(ctx, &sys->nb));
     DevBuf c, q, norm;
@@ -2321,13 +2339,16 @@ extern "C" int tgap_mc_set_screen(tgap_mc *mc, int dim, int n_pca, int n_hidden,
     return TGAP_OK;
 }
 
-extern "C" int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass)
+extern "C" int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass,
+                                       double max_pass)
 {
-    if (!mc || window < 1 || !(min_confirm >= 0.0 && min_confirm <= 1.0) || !(min_pass >= 0.0 && min_pass <= 1.0))
+    if (!mc || window < 1 || !(min_confirm >= 0.0 && min_confirm <= 1.0) || !(min_pass >= 0.0 && min_pass <= 1.0) ||
+        !(max_pass >= min_pass && max_pass <= 1.0))
         return TGAP_ERR_ARGUMENT;
     mc->fb_window = window;
     mc->fb_min_confirm = min_confirm;
     mc->fb_min_pass = min_pass;
+    mc->fb_max_pass = max_pass;
     return TGAP_OK;
 }
 

@@ -44,10 +44,13 @@ int gap_energy_grad_f64(tgap_context *ctx, const DeviceModel &m, const double *d
 // Mixed path: q given as bf16 hi/lo [rows_pad][dim_pad]; w->g = dE/dq (float [n_rows][dim_pad]).
 // d_skip (fused kernel only): a device flag that, when set at run time, makes the launch a no-op.
 // g_cleared: the caller zeroed rows [0, n_rows) of w->g (sized [rows_pad][dim_pad]) already.
+// d_skip_tiles: optional device flags per 128-row tile; the fused kernel leaves the energies (and
+// dE/dq) of a flagged tile's rows untouched (the unfused path computes every tile).
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces,
                           GapWork *w, const int *d_sites, double *d_e_rows, double *d_energies,
-                          const int *d_skip = nullptr, bool g_cleared = false);
+                          const int *d_skip = nullptr, bool g_cleared = false,
+                          const int *d_skip_tiles = nullptr);
 int model_upload_mixed(tgap_context *ctx, DeviceModel *m);
 
 // Local properties (local_properties.f90:46-147): V clipped at zero, and per-pair derivatives

@@ -469,6 +469,7 @@ struct FlashGap {
     float *g;             // dE/dq [rows_pad][ldg], accumulated (zeroed by the caller); null: energies only
     int ldg;
     const int *skip;      // optional device flag: when set, the launch does nothing
+    const int *skip_tiles;  // optional per-row-tile flags: a CTA of a flagged tile does nothing
 };
 
 template <int ZI>
@@ -527,6 +528,7 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     const bool forces = p.g != nullptr;
     pdl_enter();  // q, the cleared dE/dq rows and the skip flag come from earlier kernels
     if (p.skip && *p.skip) return;  // uniform over the grid, before any TMEM or barrier set-up
+    if (p.skip_tiles && p.skip_tiles[blockIdx.x / n_chunks]) return;  // uniform over the CTA
 
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
@@ -960,7 +962,7 @@ int model_upload_mixed(tgap_context *ctx, DeviceModel *m)
 int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
                           const __nv_bfloat16 *q_lo, int n_rows, double e0, int do_forces, GapWork *w,
                           const int *d_sites, double *d_e_rows, double *d_energies, const int *d_skip,
-                          bool g_cleared)
+                          bool g_cleared, const int *d_skip_tiles)
 {
     if (n_rows <= 0) return TGAP_OK;
     constexpr int BN1 = 128;  // m_pad is a multiple of 128; 256-column tiles when it allows
@@ -990,6 +992,7 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         p.g = do_forces ? w->g.as<float>() : nullptr;
         p.ldg = m.dim_pad;
         p.skip = d_skip;
+        p.skip_tiles = d_skip_tiles;
         // 128-point sparse tiles (64-point ones allow a deeper ring but double the per-tile handoffs,
         // and measured slower)
         switch (m.dim_pad) {

@@ -450,7 +450,8 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
                                    double *__restrict__ pos, double *__restrict__ dacc,
                                    const double *__restrict__ prop_u, int u_stride, double temperature,
                                    double rc_sel, double skin, const int *__restrict__ site_struct,
-                                   const StructDesc *__restrict__ sd, McLogs logs)
+                                   const StructDesc *__restrict__ sd, McLogs logs, int screened,
+                                   const float *__restrict__ es_trial, float *__restrict__ es_cache)
 {
     const int lane = threadIdx.x & 31;
     __shared__ int acc_slot[kMcMaxBatch];
@@ -491,6 +492,24 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
             if (lane == 0) st->status = kMcNeedRebuild;
             break;
         }
+        if (screened) {
+            // stage 1 was decided before the exact energies (k_mc_screen_batch)
+            if (lane == 0) {
+                st->s_prop += 1;
+                if (logs.de_screen) logs.de_screen[k] = st->slot_des[b];
+            }
+            if (!st->slot_pass[b]) {
+                if (lane == 0) {
+                    if (logs.de) logs.de[k] = __longlong_as_double(0x7ff8000000000000ll);
+                    if (logs.acc) logs.acc[k] = 0;
+                    if (logs.stage) logs.stage[k] = 1;
+                }
+                __syncwarp();
+                ++k;
+                ++settled;
+                continue;
+            }
+        }
         // dE in the fixed order of the one-at-a-time kernel
         double de = 0.0;
         for (int m = 0; m < n_models; ++m) {
@@ -503,9 +522,15 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
         for (int o = 16; o > 0; o >>= 1) de += __shfl_xor_sync(0xffffffffu, de, o);
         int accept = 0;
         if (lane == 0) {
-            double p = exp(-de / (mc_kb() * temperature));
+            // delayed acceptance, stage 2 (Christen and Fox): dE - dE_s against the second deviate
+            const double x = screened ? de - st->slot_des[b] : de;
+            double p = exp(-x / (mc_kb() * temperature));
             p = p < 1.0 ? p : 1.0;
-            accept = p > prop_u[(long long)u_stride * k] ? 1 : 0;
+            accept = p > (screened ? prop_u[2 * k + 1] : prop_u[(long long)u_stride * k]) ? 1 : 0;
+            if (screened) {
+                st->s_pass += 1;
+                st->s_conf += accept;
+            }
             if (logs.de) logs.de[k] = de;
             if (logs.acc) logs.acc[k] = (unsigned char)accept;
             if (logs.stage) logs.stage[k] = 2;
@@ -517,6 +542,11 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
                 const int *sm = sites + (size_t)(m * B + b) * cap;
                 const double *em = etrial + (size_t)m * B * cap + (size_t)b * cap;
                 for (int r = lane; r < c; r += 32) ecache[(size_t)m * n_atoms + sm[r]] = em[r];
+            }
+            if (screened) {
+                const int c = st->slot_count[b][0];
+                const int *sm = sites + (size_t)b * cap;
+                for (int r = lane; r < c; r += 32) es_cache[sm[r]] = es_trial[(size_t)b * cap + r];
             }
             if (lane == 0) {
                 for (int q = 0; q < 3; ++q) pos[3 * (size_t)a + q] = st->slot_new[b][q];
@@ -567,11 +597,62 @@ int mc_trial_geometry_batch(tgap_context *ctx, const McDev *d_st, const Neighbor
 int mc_resolve_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, int n_models, const int *d_sites,
                      int cap, int B, const double *d_etrial, double *d_ecache, double *d_positions, double *d_dacc,
                      const double *d_prop_u, int u_stride, double temperature, double rc_sel, double skin,
-                     McLogs logs)
+                     McLogs logs, int screened, const float *d_es_trial, float *d_es_cache)
 {
     k_mc_resolve_batch<<<1, 32, 0, ctx->stream>>>(d_st, n_models, d_sites, cap, B, d_etrial, d_ecache, nb.n_atoms,
                                                   d_positions, d_dacc, d_prop_u, u_stride, temperature, rc_sel, skin,
-                                                  nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(), logs);
+                                                  nb.site_struct.as<int>(), nb.d_structs.as<StructDesc>(), logs,
+                                                  screened, d_es_trial, d_es_cache);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+// Warp b: slot b's screen energy change over its model-0 rows in a fixed reduction order and the
+// stage-1 test against u1 of proposal next + b (the proposal the slot holds if the batch settles
+// that far; a slot the batch does not reach is evaluated again in the next batch). Then one thread
+// per row tile of 128 trial rows: the tile is needed when a passing slot's rows fall into it.
+__global__ void k_mc_screen_batch(McDev *st, const int *__restrict__ sites, int cap, int B,
+                                  const float *__restrict__ es_trial, const float *__restrict__ es_cache,
+                                  const double *__restrict__ prop_u, double temperature, int *__restrict__ tile_skip,
+                                  int n_tiles)
+{
+    const int lane = threadIdx.x & 31, b = threadIdx.x >> 5;
+    const bool running = st->status == kMcRunning;
+    if (b < B) {
+        int pass = 0;
+        double des = 0.0;
+        if (running && st->slot_flag[b] == 0) {
+            const int c = st->slot_count[b][0];
+            const int *sb = sites + (size_t)b * cap;
+            const float *eb = es_trial + (size_t)b * cap;
+            for (int r = lane; r < c; r += 32) des += (double)eb[r] - (double)es_cache[sb[r]];
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) des += __shfl_xor_sync(0xffffffffu, des, o);
+            double p = exp(-des / (mc_kb() * temperature));
+            p = p < 1.0 ? p : 1.0;
+            pass = p > prop_u[2 * (st->next + b)] ? 1 : 0;
+        }
+        if (lane == 0) {
+            st->slot_des[b] = des;
+            st->slot_pass[b] = pass;
+        }
+    }
+    __syncthreads();
+    for (int t = threadIdx.x; t < n_tiles; t += blockDim.x) {
+        int need = 0;
+        const int r0 = 128 * t, r1 = 128 * t + 127;
+        for (int bb = r0 / cap; bb <= r1 / cap && bb < B; ++bb) need |= st->slot_pass[bb];
+        tile_skip[t] = need ? 0 : 1;
+    }
+}
+
+int mc_screen_batch(tgap_context *ctx, McDev *d_st, const int *d_sites, int cap, int B, const float *d_es_trial,
+                    const float *d_es_cache, const double *d_prop_u, double temperature, int *d_tile_skip,
+                    int n_tiles)
+{
+    if (B < 1 || B > kMcMaxBatch) return set_error(ctx, TGAP_ERR_ARGUMENT, "screen batch width");
+    k_mc_screen_batch<<<1, 32 * B, 0, ctx->stream>>>(d_st, d_sites, cap, B, d_es_trial, d_es_cache, d_prop_u,
+                                                      temperature, d_tile_skip, n_tiles);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -39,6 +39,9 @@ struct McDev {
     double slot_old[kMcMaxBatch][3], slot_new[kMcMaxBatch][3], slot_dn[kMcMaxBatch];
     int slot_count[kMcMaxBatch][kMcMaxModels];
     long long batches, batch_resolved;  // batches run and proposals they settled
+    // delayed acceptance inside the batch: each slot's screen energy change and stage-1 verdict
+    double slot_des[kMcMaxBatch];
+    int slot_pass[kMcMaxBatch];
 };
 
 // Per-proposal logs (device arrays of the run's length, any may be null).
@@ -100,10 +103,23 @@ int mc_select_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, con
                     long long *d_mark, int *d_sites, int cap, int B);
 int mc_trial_geometry_batch(tgap_context *ctx, const McDev *d_st, const NeighborBatch &nb, int n_models,
                             const int *d_sites, int cap, int pmax, int B, double *d_txyz, double *d_trjs, int *d_tnsp);
+// With a screen (screened != 0, one model, two deviates per proposal): stage 1 of every slot is
+// decided before the exact energies (mc_screen_batch) and the settlement applies delayed
+// acceptance in order, a slot rejected by the screen settling without its exact energies; the
+// screen cache of an accepted slot's sites is committed with its exact energies.
 int mc_resolve_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, int n_models, const int *d_sites,
                      int cap, int B, const double *d_etrial, double *d_ecache, double *d_positions, double *d_dacc,
                      const double *d_prop_u, int u_stride, double temperature, double rc_sel, double skin,
-                     McLogs logs);
+                     McLogs logs, int screened = 0, const float *d_es_trial = nullptr, float *d_es_cache = nullptr);
+
+// Delayed acceptance, stage 1, for every slot of a speculative batch (one model): the screen's
+// energy change over the slot's rows (screen energies es_trial [B cap], cache es_cache [atoms])
+// against u1 of the proposal the slot holds. tile_skip[t] (n_tiles row tiles of 128 trial rows)
+// is set when no slot with rows in tile t passes, so the exact GAP kernel skips that tile; rows
+// of a skipped tile keep stale energies that the settlement never reads.
+int mc_screen_batch(tgap_context *ctx, McDev *d_st, const int *d_sites, int cap, int B, const float *d_es_trial,
+                    const float *d_es_cache, const double *d_prop_u, double temperature, int *d_tile_skip,
+                    int n_tiles);
 
 // Start of a run of n proposals (keeps a pending rebuild request), and the reset after a list
 // rebuild.

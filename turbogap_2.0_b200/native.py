@@ -123,7 +123,7 @@ def lib():
         "tgap_mc_get_state": (i32, [vp, vp, vp, P(dbl), P(i64), P(i64)]),
         "tgap_mc_set_screen": (i32, [vp, i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, C.c_float]),
         "tgap_mc_screen_log": (i32, [vp, i64, vp, vp]),
-        "tgap_mc_screen_fallback": (i32, [vp, i64, C.c_double, C.c_double]),
+        "tgap_mc_screen_fallback": (i32, [vp, i64, C.c_double, C.c_double, C.c_double]),
         "tgap_mc_screen_stats": (i32, [vp, vp, vp, vp, vp, vp]),
         "tgap_mc_set_batch": (i32, [vp, i32]),
         "tgap_mc_batch_stats": (i32, [vp, vp, vp]),
