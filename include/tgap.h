@@ -231,6 +231,8 @@ int tgap_system_destroy(tgap_system *system);
 int tgap_system_n_atoms(const tgap_system *system);
 /* Device pointer to the 3 x n_atoms positions (read/write, layout as on input). */
 int tgap_system_positions(tgap_system *system, double **d_positions);
+/* Copy the resident positions (3 x n_atoms) to the host (synchronizes the context stream). */
+int tgap_system_get_positions(tgap_system *system, double *positions);
 /* Copy host positions (3 x n_atoms) into the resident structure. */
 int tgap_system_set_positions(tgap_system *system, const double *positions);
 /* Rebuild the neighbor lists (or only refresh geometry when rebuild == 0). */
@@ -245,6 +247,23 @@ int64_t tgap_system_n_pairs(const tgap_system *system);
  * get 0. Set it before creating MD objects on the system, or call it again with the same
  * n_species to change the values. Forces, virials and MC energy differences are unaffected. */
 int tgap_system_set_e0(tgap_system *system, int n_species, const double *e0);
+
+/* split_tasks (src/utils/misc.f90:88-111) for one rank of an atom decomposition: only atoms
+ * [beg, end) (0-based; end < 0 = n_atoms) are descriptor centres of later evaluations of the
+ * system. Energies of the other atoms come out 0; forces and virials hold the range's
+ * contributions on every atom its sites see (the pair lists still cover all atoms), so summing the
+ * outputs of ranks whose ranges partition the atoms gives the full result, as collect_calculation
+ * (src/mpi/mpi_utils.f90:515-545) sums the MPI ranks. e0 (tgap_system_set_e0) is added for the range
+ * only. Monte Carlo objects need every site. */
+int tgap_system_set_site_range(tgap_system *system, int beg, int end);
+
+/* velocity_verlet (src/md/md_utils.f90:486-532) on device arrays (3 x n_sites each, masses in
+ * eV fs^2 / A^2 as md_interface.f90 keeps them): v += 0.5 (F + F_prev) / m dt_prev unless
+ * first_step, x_prev = x, x += v dt + 0.5 F / m dt^2, F_prev = F. For drivers that assemble the
+ * forces themselves, e.g. summed over the ranks of an atom decomposition. */
+int tgap_velocity_verlet(tgap_context *ctx, int n_sites, double *d_positions, double *d_positions_prev,
+                         double *d_velocities, const double *d_forces, double *d_forces_prev,
+                         const double *d_masses, double dt, double dt_prev, int first_step);
 
 /* Energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure), device pointers,
  * summed over models, plus each atom's e0 (tgap_system_set_e0; 0 when never set). Overwrites the

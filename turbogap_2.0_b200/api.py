@@ -340,6 +340,18 @@ class System:
         e = _f64(e0).reshape(-1)
         check(self.ctx._L.tgap_system_set_e0(self.h, len(e), ptr(e)), self.ctx.h, "tgap_system_set_e0")
 
+    def get_positions(self):
+        """Host copy of the resident positions (n_atoms, 3)."""
+        x = np.zeros((self.n_atoms, 3))
+        check(self.ctx._L.tgap_system_get_positions(self.h, ptr(x)), self.ctx.h, "tgap_system_get_positions")
+        return x
+
+    def set_site_range(self, beg, end=None):
+        """Only atoms [beg, end) are descriptor centres of later evaluations (one rank's share of
+        an atom decomposition, split_tasks misc.f90:88-111); None restores all sites."""
+        check(self.ctx._L.tgap_system_set_site_range(self.h, int(beg), -1 if end is None else int(end)),
+              self.ctx.h, "tgap_system_set_site_range")
+
     def calculate_gap_soap(self, models, precision, positions=None, rebuild=True):
         """Host-buffer evaluation (tgap_calculate_gap_soap): positions (n, 3) in (None keeps the
         resident ones), energies (n,), forces (n, 3) and per-structure virials (n_structures, 3, 3)

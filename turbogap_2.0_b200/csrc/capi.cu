@@ -769,6 +769,8 @@ struct tgap_system {
     // per-atom isolated-atom energies (calculate_e0), added to every energy output when set
     std::vector<double> host_e0;
     DevBuf d_e0;
+    // sites evaluated as descriptor centres: atoms [range_beg, range_end) (split_tasks of one rank)
+    int range_beg = 0, range_end = -1;
 };
 
 extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
@@ -863,6 +865,17 @@ extern "C" int tgap_system_positions(tgap_system *s, double **d_positions)
     return TGAP_OK;
 }
 
+extern "C" int tgap_system_get_positions(tgap_system *s, double *positions)
+{
+    if (!s || !positions) return TGAP_ERR_ARGUMENT;
+    tgap_context *ctx = s->ctx;
+    CHECK_RC(activate(ctx));
+    TGAP_CUDA(ctx, cudaMemcpyAsync(positions, s->nb.positions.ptr, sizeof(double) * 3 * s->nb.n_atoms,
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    return TGAP_OK;
+}
+
 extern "C" int tgap_system_set_positions(tgap_system *s, const double *positions)
 {
     if (!s || !positions) return TGAP_ERR_ARGUMENT;
@@ -871,6 +884,39 @@ extern "C" int tgap_system_set_positions(tgap_system *s, const double *positions
     TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, positions, sizeof(double) * 3 * s->nb.n_atoms,
                                    cudaMemcpyHostToDevice, ctx->stream));
     return TGAP_OK;
+}
+
+// split_tasks (misc.f90:88-111) on the device side: only atoms [beg, end) are descriptor centres of
+// later evaluations; their energies, and their force and virial contributions on every atom they
+// see, are computed (the other energies are 0), as one rank of the reference's MPI split does before
+// collect_calculation (mpi_utils.f90:515-545) sums the ranks.
+extern "C" int tgap_system_set_site_range(tgap_system *s, int beg, int end)
+{
+    if (!s) return TGAP_ERR_ARGUMENT;
+    const int N = (int)s->host_species.size();
+    if (end < 0) end = N;
+    if (beg < 0 || beg > end || end > N) return set_error(s->ctx, TGAP_ERR_ARGUMENT, "site range [%d, %d) of %d", beg, end, N);
+    CHECK_RC(activate(s->ctx));
+    TGAP_CUDA(s->ctx, cudaStreamSynchronize(s->ctx->stream));
+    for (auto &ss : s->site_sets) ss.sites.release();  // rebuilt for the new range on next use
+    s->site_sets.clear();
+    s->range_beg = beg;
+    s->range_end = end == N ? -1 : end;
+    return TGAP_OK;
+}
+
+// velocity_verlet (md_utils.f90:486-532) on device arrays, for drivers that assemble the forces
+// themselves (for example summed over ranks): masses in eV fs^2 / A^2.
+extern "C" int tgap_velocity_verlet(tgap_context *ctx, int n_sites, double *d_positions, double *d_positions_prev,
+                                    double *d_velocities, const double *d_forces, double *d_forces_prev,
+                                    const double *d_masses, double dt, double dt_prev, int first_step)
+{
+    CHECK_RC(activate(ctx));
+    if (n_sites < 0 || (n_sites > 0 && (!d_positions || !d_positions_prev || !d_velocities || !d_forces ||
+                                        !d_forces_prev || !d_masses)))
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_velocity_verlet: bad arguments");
+    return velocity_verlet(ctx, n_sites, d_positions, d_positions_prev, d_velocities, d_forces, d_forces_prev,
+                           d_masses, dt, dt_prev, first_step);
 }
 
 // calculate_e0 (calculate_gap_soap.f90:135-169): every atom gets the e0 of its species (the input
@@ -892,10 +938,10 @@ extern "C" int tgap_system_set_e0(tgap_system *s, int n_species, const double *e
     return TGAP_OK;
 }
 
-__global__ void k_add_e0(int n, const double *__restrict__ e0, double *__restrict__ energies)
+__global__ void k_add_e0(int beg, int end, const double *__restrict__ e0, double *__restrict__ energies)
 {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) energies[i] += e0[i];
+    const int i = beg + blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < end) energies[i] += e0[i];
 }
 
 extern "C" int tgap_system_update(tgap_system *s, int rebuild)
@@ -919,7 +965,8 @@ static int site_set(tgap_system *s, int central_species, SiteSet **out)
         }
     tgap_context *ctx = s->ctx;
     std::vector<int> rows;
-    for (int i = 0; i < (int)s->host_species.size(); ++i)
+    const int beg = s->range_beg, end = s->range_end < 0 ? (int)s->host_species.size() : s->range_end;
+    for (int i = beg; i < end; ++i)
         if (central_species == 0 || s->host_species[i] == central_species) rows.push_back(i);
     s->site_sets.emplace_back();
     SiteSet &ss = s->site_sets.back();
@@ -1056,7 +1103,10 @@ static int compute_models(tgap_context *ctx, tgap_system *s, int n_models, tgap_
                                queue ? queue + 2 * i : nullptr));
     if (!s->host_e0.empty()) {
         // turbogap_main.f90:994: the total energy of each atom adds its e0
-        k_add_e0<<<(N + 255) / 256, 256, 0, ctx->stream>>>(N, s->d_e0.as<double>(), d_energies);
+        // the atoms of this system's site range only, so ranks that split the sites count each once
+        const int beg = s->range_beg, end = s->range_end < 0 ? N : s->range_end;
+        if (end > beg)
+            k_add_e0<<<(end - beg + 255) / 256, 256, 0, ctx->stream>>>(beg, end, s->d_e0.as<double>(), d_energies);
         TGAP_LAUNCH_CHECK(ctx);
     }
     return TGAP_OK;
@@ -2064,6 +2114,8 @@ extern "C" int tgap_mc_create(tgap_context *ctx, tgap_system *sys, int n_models,
         return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_mc_create: precision");
     if (!sys->nb.replicated)
         return set_error(ctx, TGAP_ERR_UNSUPPORTED, "Monte Carlo needs a system built from primitive cells");
+    if (sys->range_beg != 0 || sys->range_end >= 0)
+        return set_error(ctx, TGAP_ERR_UNSUPPORTED, "Monte Carlo needs every site (tgap_system_set_site_range)");
     double rc = 0.0;
     for (int m = 0; m < n_models; ++m) rc = std::max(rc, models[m]->soap.p.rcut_max);
     if (!(sys->rcut > rc))

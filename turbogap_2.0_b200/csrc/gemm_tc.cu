@@ -103,6 +103,15 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr)
            ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
 }
 
+// K-major operand tile of 32-element (64-byte) rows, 64-byte swizzle: 8-row groups 512 bytes apart
+// (SBO>>4 = 32), layout [61,64) = 4 (SWIZZLE_64B); the tile base is 512-byte aligned and a 16-wide
+// k-step advances the start address by 32 bytes, as in the 128-byte layout.
+__device__ __forceinline__ uint64_t umma_desc64(uint32_t saddr)
+{
+    return (uint64_t)((saddr & 0x3FFFF) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)32 << 32) |
+           ((uint64_t)1 << 46) | ((uint64_t)4 << 61);
+}
+
 __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
                                           uint32_t accumulate)
 {
@@ -131,6 +140,15 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float v[16])
     asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
 #pragma unroll
     for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+__device__ __forceinline__ void tmem_ld16_nowait(uint32_t taddr, uint32_t r[16])
+{
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(taddr));
 }
 
 // ---------------------------------------------------------------------------- epilogues
@@ -444,16 +462,38 @@ __global__ void __launch_bounds__(kTcThreadsP, 1)
 // columns half = (w - 2) / 4 of the tile). Shared memory: a STAGES-deep ring of equal slots (one
 // k-block of q and Q_j, or one half of a Q_j^T k-block) and W.
 constexpr int kFlashEpiWarps = 8;
+constexpr int kFlashMaxChunkTiles = 16;  // sparse tiles per CTA (the chunk) at most
 constexpr int kFlashThreads = 32 * (2 + kFlashEpiWarps);
 
+// Ring slots hold kHK-element slices of the k dimension: for S the q rows and the sparse tile's rows
+// over kHK descriptor components, for g one half of the tile's Q_j^T rows over kHK sparse points. The
+// S product stops at the last 16-wide k-step holding descriptor components and the g halves cover
+// the components only (the operands are zero past dim), which saves the padding's MMAs.
+#ifndef TGAP_FLASH_HK
+#define TGAP_FLASH_HK 64
+#endif
+// k elements per ring slot: 64 (128-byte swizzle, two 64 KB slots; the default) or 32 (64-byte
+// swizzle, five 32 KB slots: measured 15 % slower on the MD workload, the kernel being bound by the
+// L2 bandwidth all CTAs share rather than by one CTA's copies in flight)
+constexpr int kHK = TGAP_FLASH_HK;
+static_assert(kHK == 64 || kHK == 32, "ring slot width");
+// operand descriptor of a ring slot
+__device__ __forceinline__ uint64_t ring_desc(uint32_t saddr)
+{
+    if constexpr (kHK == 64) return umma_desc(saddr);
+    else return umma_desc64(saddr);
+}
 template <int DP, int BS> struct FlashShape {
-    static constexpr uint32_t TILE_A = kBM * kBK * 2;                 // q k-block (hi or lo)
-    static constexpr uint32_t TILE_B = BS * kBK * 2;                  // Q_j k-block (hi or lo)
-    static constexpr uint32_t B2 = (DP / 2) * kBK * 2;                // Q_j^T half k-block (hi or lo)
-    static constexpr uint32_t SLOT_S = 2 * TILE_A + 2 * TILE_B;
-    static constexpr uint32_t SLOT = SLOT_S > 2 * B2 ? SLOT_S : 2 * B2;
+    static constexpr uint32_t TILE_A = kBM * kBK * 2;                 // W k-block of 64 (hi or lo), 128B swizzle
+    static constexpr uint32_t HA = kBM * kHK * 2;                     // q slice (hi or lo)
+    static constexpr uint32_t HB = BS * kHK * 2;                      // Q_j slice (hi or lo)
+    static constexpr uint32_t HG = (DP / 2) * kHK * 2;                // Q_j^T half slice (hi or lo), largest
+    static constexpr uint32_t SLOT_S = 2 * HA + 2 * HB;
+    static constexpr uint32_t SLOT = SLOT_S > 2 * HG ? SLOT_S : 2 * HG;
     static constexpr uint32_t W = 2 * (BS / kBK) * TILE_A;            // hi + lo, BS/64 k-blocks each
-    static constexpr int STAGES = (int)((227u * 1024u - 2048u - W) / SLOT) > 4 ? 4 : (int)((227u * 1024u - 2048u - W) / SLOT);
+    // 227 KB per CTA less the static part (barriers, the chunk's alphas)
+    static constexpr int FIT = (int)((227u * 1024u - 2048u - 4u * kFlashMaxChunkTiles * BS - W) / SLOT);
+    static constexpr int STAGES = FIT > 8 ? 8 : FIT;
     static constexpr size_t SMEM = (size_t)STAGES * SLOT + W + 1024;
 };
 
@@ -470,6 +510,9 @@ struct FlashGap {
     int ldg;
     const int *skip;      // optional device flag: when set, the launch does nothing
     const int *skip_tiles;  // optional per-row-tile flags: a CTA of a flagged tile does nothing
+    // the descriptor's real width dim (<= DP): S takes n_kh 32-wide slices, the last with ks_last
+    // 16-wide k-steps; g takes two halves of nh columns (nh a multiple of 16, 2 nh >= dim)
+    int n_kh, ks_last, nh;
 };
 
 template <int ZI>
@@ -515,15 +558,14 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     static_assert(BS % 64 == 0 && BS <= 128, "sparse tile: 64 or 128");
     constexpr int STAGES = Sh::STAGES;
     static_assert(STAGES >= 2, "ring of at least two slots");
-    constexpr int KB = DP / kBK;     // k-blocks of S
-    constexpr int KG = BS / kBK;     // k-blocks of g per sparse tile
-    constexpr int NH = DP / 2;       // N of each g half
+    constexpr int KG = BS / kBK;     // W k-blocks (64 wide) per sparse tile
     constexpr int HC = BS / 2;       // S columns per epilogue half
-    constexpr uint32_t TILE_A = Sh::TILE_A, TILE_B = Sh::TILE_B, B2 = Sh::B2, SLOT = Sh::SLOT;
+    constexpr uint32_t TILE_A = Sh::TILE_A, HA = Sh::HA, HB = Sh::HB, HG = Sh::HG, SLOT = Sh::SLOT;
     constexpr uint32_t IDESC_S = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BS >> 3) << 17) |
                                  ((uint32_t)(kBM >> 4) << 24);
-    constexpr uint32_t IDESC_G = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
-                                 ((uint32_t)(kBM >> 4) << 24);
+    const int NH = p.nh;             // N of each g half
+    const uint32_t IDESC_G = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
+                             ((uint32_t)(kBM >> 4) << 24);
     constexpr uint32_t kCols = 512;
     const bool forces = p.g != nullptr;
     pdl_enter();  // q, the cleared dE/dq rows and the skip flag come from earlier kernels
@@ -533,6 +575,9 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     extern __shared__ __align__(1024) unsigned char smem_raw[];
     __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
     __shared__ __align__(8) uint64_t bar_sfull, bar_sfree, bar_wfull, bar_wempty, bar_drain;
+    // the alphas of the CTA's sparse tiles, read by the epilogue at shared-memory latency (a global
+    // load per 16 columns put an L2 round trip between each S tile and its release)
+    __shared__ __align__(16) float s_alpha[kFlashMaxChunkTiles * BS];
     __shared__ uint32_t tmem_base_slot;
     __shared__ volatile int abort_flag;
     __shared__ int issued, consumed;
@@ -542,6 +587,7 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int unit = blockIdx.x, rt = unit / n_chunks, ch = unit - rt * n_chunks;
     const int T = tiles_per_chunk, j0 = ch * T, m0 = rt * kBM;
+    for (int i = threadIdx.x; i < T * BS; i += blockDim.x) s_alpha[i] = p.alphas[j0 * BS + i];
 
     if (threadIdx.x == 0) {
         for (int s = 0; s < STAGES; ++s) {
@@ -586,26 +632,27 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                 return true;
             };
             auto load_s = [&](int j) -> bool {
-                for (int kb = 0; kb < KB; ++kb) {
+                for (int kh = 0; kh < p.n_kh; ++kh) {
                     uint32_t slot, fb;
                     if (!acquire(slot, fb)) return false;
-                    mbar_expect_tx(fb, 2 * TILE_A + 2 * TILE_B);
-                    tma_load_2d(slot, &tm_q_hi, fb, kb * kBK, m0);
-                    tma_load_2d(slot + TILE_A, &tm_q_lo, fb, kb * kBK, m0);
-                    tma_load_2d(slot + 2 * TILE_A, &tm_Q_hi, fb, kb * kBK, j * BS);
-                    tma_load_2d(slot + 2 * TILE_A + TILE_B, &tm_Q_lo, fb, kb * kBK, j * BS);
+                    mbar_expect_tx(fb, 2 * HA + 2 * HB);
+                    tma_load_2d(slot, &tm_q_hi, fb, kh * kHK, m0);
+                    tma_load_2d(slot + HA, &tm_q_lo, fb, kh * kHK, m0);
+                    tma_load_2d(slot + 2 * HA, &tm_Q_hi, fb, kh * kHK, j * BS);
+                    tma_load_2d(slot + 2 * HA + HB, &tm_Q_lo, fb, kh * kHK, j * BS);
                     issued = ++it;
                 }
                 return true;
             };
+            const uint32_t g_bytes = 2u * (uint32_t)NH * (uint32_t)(kHK * 2);
             auto load_g = [&](int j) -> bool {
-                for (int kb = 0; kb < KG; ++kb)
+                for (int kh = 0; kh < BS / kHK; ++kh)
                     for (int h = 0; h < 2; ++h) {
                         uint32_t slot, fb;
                         if (!acquire(slot, fb)) return false;
-                        mbar_expect_tx(fb, 2 * B2);
-                        tma_load_2d(slot, &tm_QT_hi, fb, j * BS + kb * kBK, h * NH);
-                        tma_load_2d(slot + B2, &tm_QT_lo, fb, j * BS + kb * kBK, h * NH);
+                        mbar_expect_tx(fb, g_bytes);
+                        tma_load_2d(slot, &tm_QT_hi, fb, j * BS + kh * kHK, h * NH);
+                        tma_load_2d(slot + HG, &tm_QT_lo, fb, j * BS + kh * kHK, h * NH);
                         issued = ++it;
                     }
                 return true;
@@ -636,15 +683,15 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                 consumed = ++it;
             };
             auto mma_s = [&]() -> bool {
-                for (int kb = 0; kb < KB; ++kb) {
+                for (int kh = 0; kh < p.n_kh; ++kh) {
                     uint32_t slot;
                     if (!take(slot)) return false;
-#pragma unroll
-                    for (int k = 0; k < kBK / 16; ++k) {
-                        const uint64_t ahi = umma_desc(slot + 32 * k), alo = umma_desc(slot + TILE_A + 32 * k);
-                        const uint64_t bhi = umma_desc(slot + 2 * TILE_A + 32 * k);
-                        const uint64_t blo = umma_desc(slot + 2 * TILE_A + TILE_B + 32 * k);
-                        umma_bf16(tS, ahi, bhi, IDESC_S, (kb > 0 || k > 0) ? 1u : 0u);
+                    const int ks = kh == p.n_kh - 1 ? p.ks_last : kHK / 16;  // past dim the slice is zero
+                    for (int k = 0; k < ks; ++k) {
+                        const uint64_t ahi = ring_desc(slot + 32 * k), alo = ring_desc(slot + HA + 32 * k);
+                        const uint64_t bhi = ring_desc(slot + 2 * HA + 32 * k);
+                        const uint64_t blo = ring_desc(slot + 2 * HA + HB + 32 * k);
+                        umma_bf16(tS, ahi, bhi, IDESC_S, (kh > 0 || k > 0) ? 1u : 0u);
                         umma_bf16(tS, ahi, blo, IDESC_S, 1u);
                         umma_bf16(tS, alo, bhi, IDESC_S, 1u);
                     }
@@ -656,17 +703,19 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             auto mma_g = [&](int t) -> bool {
                 if (!mbar_wait(smem_u32(&bar_wfull), (uint32_t)t & 1u, &abort_flag)) return false;
                 asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-                for (int kb = 0; kb < KG; ++kb)
+                for (int kh = 0; kh < BS / kHK; ++kh)
                     for (int h = 0; h < 2; ++h) {
                         uint32_t slot;
                         if (!take(slot)) return false;
-                        const uint32_t whi = wbase + kb * TILE_A, wlo = wbase + (KG + kb) * TILE_A;
 #pragma unroll
-                        for (int k = 0; k < kBK / 16; ++k) {
-                            const uint64_t ahi = umma_desc(whi + 32 * k), alo = umma_desc(wlo + 32 * k);
-                            const uint64_t bhi = umma_desc(slot + 32 * k), blo = umma_desc(slot + B2 + 32 * k);
+                        for (int k = 0; k < kHK / 16; ++k) {
+                            // W is K-major in 64-wide 128B-swizzled blocks: k-step kk of the tile
+                            const int kk = kh * (kHK / 16) + k;
+                            const uint32_t wo = (uint32_t)(kk / 4) * TILE_A + (uint32_t)(kk % 4) * 32;
+                            const uint64_t ahi = umma_desc(wbase + wo), alo = umma_desc(wbase + KG * TILE_A + wo);
+                            const uint64_t bhi = ring_desc(slot + 32 * k), blo = ring_desc(slot + HG + 32 * k);
                             const uint32_t d = tG + (uint32_t)(h * NH);
-                            umma_bf16(d, ahi, bhi, IDESC_G, (t > 0 || kb > 0 || k > 0) ? 1u : 0u);
+                            umma_bf16(d, ahi, bhi, IDESC_G, (t > 0 || kh > 0 || k > 0) ? 1u : 0u);
                             umma_bf16(d, ahi, blo, IDESC_G, 1u);
                             umma_bf16(d, alo, bhi, IDESC_G, 1u);
                         }
@@ -701,12 +750,21 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             __syncwarp();
             if (!ok || abort_flag) break;
+            // S leaves TMEM first (one wait for all loads), so the next tile's S product can start
+            // while the W rows are computed
+            uint32_t sraw[HC / 16][16];
+#pragma unroll
+            for (int c = 0; c < HC / 16; ++c) tmem_ld16_nowait(tS + lane_base + (uint32_t)(half * HC + c * 16), sraw[c]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            mbar_arrive(smem_u32(&bar_sfree));  // S may be overwritten
             uint32_t hi[HC / 16][8], lo[HC / 16][8];
 #pragma unroll
             for (int c = 0; c < HC / 16; ++c) {
                 float v[16];
-                tmem_ld16(tS + lane_base + (uint32_t)(half * HC + c * 16), v);
-                const float *a16 = p.alphas + j * BS + half * HC + c * 16;
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(sraw[c][i]);
+                const float *a16 = s_alpha + (j - j0) * BS + half * HC + c * 16;
                 switch (p.zeta_int) {
                 case 1: flash_w16<1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
                 case 2: flash_w16<2>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
@@ -717,8 +775,6 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
                 default: flash_w16<-1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
                 }
             }
-            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
-            mbar_arrive(smem_u32(&bar_sfree));  // S may be overwritten
             if (!forces) continue;
             if (t > 0) {
                 ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(t - 1) & 1u, &abort_flag);
@@ -804,19 +860,22 @@ static PFN_encodeTiled encode_fn()
     return fn;
 }
 
-// Row-major bf16 matrix [rows][cols] (cols contiguous), box kBK x box_rows, 128B swizzle.
-static int make_map(tgap_context *ctx, CUtensorMap *map, const void *ptr, int rows, int cols, int box_rows)
+// Row-major bf16 matrix [rows][cols] (cols contiguous), box box_cols x box_rows: 64 columns with
+// the 128-byte swizzle, 32 columns with the 64-byte one.
+static int make_map(tgap_context *ctx, CUtensorMap *map, const void *ptr, int rows, int cols, int box_rows,
+                    int box_cols = kBK)
 {
     PFN_encodeTiled enc = encode_fn();
     if (!enc) return set_error(ctx, TGAP_ERR_CUDA, "cuTensorMapEncodeTiled unavailable");
-    if (((uintptr_t)ptr & 15) || (cols * 2) % 16)
+    if (((uintptr_t)ptr & 15) || (cols * 2) % 16 || (box_cols != kBK && box_cols != 32))
         return set_error(ctx, TGAP_ERR_ARGUMENT, "tensor map alignment");
     cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
     cuuint64_t strides[1] = {(cuuint64_t)cols * 2};
-    cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
+    cuuint32_t box[2] = {(cuuint32_t)box_cols, (cuuint32_t)box_rows};
     cuuint32_t estr[2] = {1, 1};
     CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 2, const_cast<void *>(ptr), dims, strides, box, estr,
-                     CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
+                     CU_TENSOR_MAP_INTERLEAVE_NONE,
+                     box_cols == kBK ? CU_TENSOR_MAP_SWIZZLE_128B : CU_TENSOR_MAP_SWIZZLE_64B,
                      CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
     if (r != CUDA_SUCCESS) return set_error(ctx, TGAP_ERR_CUDA, "cuTensorMapEncodeTiled failed (%d)", (int)r);
     return TGAP_OK;
@@ -868,7 +927,7 @@ static int flash_chunks(int n_rt, int J, int sms)
     int best = 1;
     long best_cost = -1;
     for (int nc = 1; nc <= J; ++nc) {
-        if (J % nc) continue;
+        if (J % nc || J / nc > kFlashMaxChunkTiles) continue;
         const long waves = ((long)n_rt * nc + sms - 1) / sms;
         const long cost = waves * (J / nc);
         if (best_cost < 0 || cost < best_cost) {
@@ -884,14 +943,21 @@ static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bflo
                         int rows_pad, const FlashGap &p)
 {
     using Sh = FlashShape<DP, BS>;
-    constexpr int NH = DP / 2;
+    // the real descriptor width: S stops at the last 16-wide k-step that holds components, g at the
+    // two halves of NH columns that cover them (the operands are zero beyond dim)
+    FlashGap q = p;
+    q.n_kh = (m.dim + kHK - 1) / kHK;
+    q.ks_last = (m.dim - (q.n_kh - 1) * kHK + 15) / 16;
+    q.nh = ((m.dim + 1) / 2 + 15) / 16 * 16;
+    if (q.nh > DP / 2 || q.n_kh > DP / kHK) return set_error(ctx, TGAP_ERR_ARGUMENT, "fused GAP shape");
     CUtensorMap tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo;
     int rc;
-    if ((rc = make_map(ctx, &tq_hi, q_hi, rows_pad, DP, kBM)) || (rc = make_map(ctx, &tq_lo, q_lo, rows_pad, DP, kBM)) ||
-        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, BS)) ||
-        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, BS)) ||
-        (rc = make_map(ctx, &tT_hi, m.QT_hi.ptr, DP, m.m_pad, NH)) ||
-        (rc = make_map(ctx, &tT_lo, m.QT_lo.ptr, DP, m.m_pad, NH)))
+    if ((rc = make_map(ctx, &tq_hi, q_hi, rows_pad, DP, kBM, kHK)) ||
+        (rc = make_map(ctx, &tq_lo, q_lo, rows_pad, DP, kBM, kHK)) ||
+        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, BS, kHK)) ||
+        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, BS, kHK)) ||
+        (rc = make_map(ctx, &tT_hi, m.QT_hi.ptr, DP, m.m_pad, q.nh, kHK)) ||
+        (rc = make_map(ctx, &tT_lo, m.QT_lo.ptr, DP, m.m_pad, q.nh, kHK)))
         return rc;
     auto kern = k_gap_flash<DP, BS>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM));
@@ -902,13 +968,13 @@ static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bflo
     const int J = m.m_pad / BS, n_rt = rows_pad / kBM;
     std::vector<int> divisors;
     for (int d = 1; d <= J; ++d)
-        if (J % d == 0) divisors.push_back(d);
+        if (J % d == 0 && J / d <= kFlashMaxChunkTiles) divisors.push_back(d);
     char key[96];
     std::snprintf(key, sizeof(key), "gap_fused/dp%d/bs%d/row_tiles%d/sparse_tiles%d", DP, BS, n_rt, J);
     const int nc = tuned(ctx, key, "gemm_bf16x3_fused", divisors, flash_chunks(n_rt, J, sm_count(ctx)));
     StageScope sc(ctx, "gemm_bf16x3_fused");
     TGAP_CUDA(ctx, launch_pdl(kern, dim3(n_rt * nc), dim3(kFlashThreads), Sh::SMEM, ctx->stream, tq_hi, tq_lo, tQ_hi,
-                              tQ_lo, tT_hi, tT_lo, nc, J / nc, p, ctx->d_flag));
+                              tQ_lo, tT_hi, tT_lo, nc, J / nc, q, ctx->d_flag));
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
