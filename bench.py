@@ -834,6 +834,36 @@ def _cfg3_leg(tg, torch, ctx, stream, peaks, with_cpu, warmup):
     return out
 
 
+def _sharded_leg(tg, torch, ctx, model, dist, world, rank, steps, warmup):
+    """Atom decomposition across the ranks (N > 1): one box of 4096 N carbon atoms at the MD
+    workload's density, split_tasks over the ranks, one all-reduce of forces, energies and virial
+    per step (NCCL), the same velocity Verlet on every rank. Per-GPU work is fixed as N grows
+    (weak scaling of the decomposition); device time per step, max over ranks."""
+    from turbogap_b200 import decomposition as dc
+    n = N_ATOMS * world
+    pos, box, sp, masses = tg.synth.random_packing(n, 2.5, 1.2, seed=4242)
+    vel = tg.synth.maxwell_boltzmann(masses, 3000.0, seed=4243)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + SKIN)
+    sh = dc.ShardedMD(ctx, system, [model], masses, DT, rebuild_every=REBUILD, precision=tg.TGAP_MIXED, dist=dist)
+    sh.set_velocities(vel)
+    sh.run(warmup)
+    dist.barrier()
+    torch.cuda.synchronize()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    s0.record()
+    sh.run(steps)
+    s1.record()
+    torch.cuda.synchronize()
+    ms = _over_ranks([s0.elapsed_time(s1)], "max", dist, "cuda")[0]
+    st = sh.state()
+    system.close()
+    return dict(workload=f"NVE MD of one {n}-atom carbon box (2.5 g/cm3, same model and settings as the headline), "
+                         f"sites split over {world} ranks (split_tasks), one NCCL all-reduce of forces, energies "
+                         f"and virial per step", n_atoms=n, sites_per_rank=sh.range[1] - sh.range[0], steps=steps,
+                atom_steps_per_s=n * steps / (ms * 1e-3), ms_per_step=ms / steps, scaling="weak",
+                e_pot_per_atom=st["e_pot"] / n)
+
+
 def _over_ranks(values, op, dist, device):
     """Max or min of per-rank values over the process group (identity without one): each rank
     runs its own replica, and the job is as slow as its slowest rank."""
@@ -947,6 +977,8 @@ def run_ours(args):
         cpu = _cpu_baseline(tg, pos, box, sp, masses, vel, model_np)
         mc_line["cpu_baseline"] = _mc_cpu_baseline(tg, model_np, 300 + seed)
     legs = {}
+    if world > 1:
+        legs["sharded_md"] = _sharded_leg(tg, torch, ctx, model, dist, world, rank, args.steps, args.warmup)
     if world == 1 and not args.headline_only:
         legs["predict_216"] = _cfg0_leg(tg, torch, ctx, stream, flush, peaks, with_cpu)
         legs["batched_512_cells"] = _cfg2_leg(tg, torch, ctx, stream, flush, peaks, with_cpu)
@@ -987,6 +1019,37 @@ def run_ours(args):
     return 0
 
 
+def run_profile(args):
+    """The MD workload only (no other legs, no CPU baseline): warm-up, then `steps` eager MD steps in
+    one precision, for profiler captures of its kernels."""
+    import torch
+    tg = _load_package()
+    torch.cuda.set_device(0)
+    pos, box, sp, masses, vel = _workload(tg, 0)
+    ctx = tg.Context(0)
+    hyp = tg.synth.carbon_hypers()
+    pool = _device_descriptors(tg, torch, ctx, hyp, _pool_structures(tg, 1000))
+    m = tg.synth.gap_model(pool, N_SPARSE, seed=7)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], m["delta"], m["zeta"])
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + SKIN)
+    prec = tg.TGAP_FP64 if args.profile == "fp64" else tg.TGAP_MIXED
+    md = tg.MD(ctx, system, [model], masses, DT, rebuild_every=REBUILD, precision=prec, use_graph=False)
+    md.set_velocities(vel)
+    md.run(args.warmup)
+    ctx.synchronize()
+    l0 = ctx.kernel_launches
+    md.run(args.steps)
+    ctx.synchronize()
+    st = md.state()
+    print(json.dumps({"profile": args.profile, "steps": args.steps, "warmup": args.warmup,
+                      "launches": ctx.kernel_launches - l0, "e_pot": st["e_pot"]}), flush=True)
+    md.close()
+    system.close()
+    model.close()
+    ctx.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -995,11 +1058,15 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--headline-only", action="store_true", help="skip the predict, batched and SiO2 legs")
+    ap.add_argument("--profile", choices=["mixed", "fp64"], default=None,
+                    help="only the MD workload's steps in one precision (for profiler captures)")
     args = ap.parse_args()
     if args.warmup < 3 and args.impl == "ours":
         args.warmup = 3
     if args.impl == "reference":
         return run_reference(args)
+    if args.profile:
+        return run_profile(args)
     return run_ours(args)
 
 
