@@ -131,6 +131,33 @@ module tgap_iface
          integer(c_int), intent(in) :: n_neigh(*)
          real(c_double) :: V(*), V_der(3, *)
       end function
+
+      ! calculate_e0 (calculate_gap_soap.f90:135-169) on a resident system: species_info%e0(1:n_species)
+      integer(c_int) function tgap_system_set_e0(system, n_species, e0) bind(C, name="tgap_system_set_e0")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: system
+         integer(c_int), value :: n_species
+         real(c_double), intent(in) :: e0(*)
+      end function
+
+      ! split_tasks (misc.f90:88-111): this rank's sites are split%i_beg .. split%i_end, passed as
+      ! the 0-based half-open range (i_beg - 1, i_end)
+      integer(c_int) function tgap_system_set_site_range(system, beg, end) bind(C, name="tgap_system_set_site_range")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: system
+         integer(c_int), value :: beg, end
+      end function
+
+      ! velocity_verlet (md_utils.f90:486-532) on device arrays (CUDA Fortran device memory or
+      ! OpenACC host_data use_device), after the ranks' forces have been summed
+      integer(c_int) function tgap_velocity_verlet(ctx, n_sites, positions, positions_prev, velocities, &
+                                                   forces, forces_prev, masses, dt, dt_prev, first_step) &
+         bind(C, name="tgap_velocity_verlet")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx, positions, positions_prev, velocities, forces, forces_prev, masses
+         integer(c_int), value :: n_sites, first_step
+         real(c_double), value :: dt, dt_prev
+      end function
    end interface
 
 contains
