@@ -44,11 +44,11 @@ def test_autotune_keeps_results_and_reports_choices(ctx, tg, synth, precision_na
     kinds = {ln.split("/")[0] for ln in lines}
     assert {"soap_fwd", "soap_bwd"} <= kinds, lines
     if precision == tg.TGAP_MIXED:
-        assert "gap_fused" in kinds, lines
+        assert any(k.startswith("gap_fused") for k in kinds), lines  # single-CTA or CTA-pair form
     for ln in lines:
         parts = ln.split()
         best, best_us, dflt_us = int(parts[1]), float(parts[2]), float(parts[-2])
-        assert best >= (0 if parts[0].endswith("/persist") else 1) and best_us > 0.0
+        assert best >= (0 if parts[0].endswith(("/persist", "/pair")) else 1) and best_us > 0.0
         assert best_us <= dflt_us * (1.0 + 1e-9), ln  # the default is a candidate
     e1, f1, v1 = _eval(system, model, tg, precision, len(pos))
     te, tf = (1e-6, 1e-6) if precision == tg.TGAP_MIXED else (1e-12, 1e-9)

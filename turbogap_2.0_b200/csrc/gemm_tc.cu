@@ -74,15 +74,20 @@ __device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity)
     return ok != 0;
 }
 
-// Bounded wait: false after kWaitNs or once *abort is set by another thread of the CTA.
+// Bounded wait: false after kWaitNs or once *abort is set by another thread of the CTA. The timer
+// and the abort flag are read only when the phase has not completed on the first tries (every 8th
+// try after that), so a wait that succeeds at once costs one try_wait and no %globaltimer read.
 __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int *abort)
 {
+    if (mbar_try(bar, parity)) return true;
     const uint64_t t0 = globaltimer();
-    while (!mbar_try(bar, parity)) {
-        if (*abort) return false;
-        if (globaltimer() - t0 > kWaitNs) return false;
+    for (unsigned i = 0;; ++i) {
+        if (mbar_try(bar, parity)) return true;
+        if ((i & 7u) == 7u) {
+            if (*abort) return false;
+            if (globaltimer() - t0 > kWaitNs) return false;
+        }
     }
-    return true;
 }
 
 __device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x,
@@ -841,6 +846,386 @@ __global__ void __launch_bounds__(kFlashThreads, 1)
     }
 }
 
+// ---------------------------------------------------------------------------- fused GAP kernel, CTA pair
+
+// The same contraction on a pair of CTAs (a 2-CTA cluster on neighboring SMs) that share each sparse
+// tile: tcgen05 MMAs of cta_group::2 have M = 256 (CTA r holds rows 128 r .. 128 r + 127 of the pair's
+// two row tiles in its shared memory and TMEM) and read the B operand split along N, half from each
+// CTA. Each CTA therefore loads its own q rows but only half of every Q_j and Q_j^T slice, which cuts
+// the operand stream from L2 per SM by about a third (the single-CTA kernel is bound by that stream).
+// The leader (rank 0) issues the MMAs and waits on its barriers for both CTAs' copies (each CTA's
+// copies complete on the leader's full barrier) and both CTAs' epilogues (remote arrivals); the
+// leader's commits arrive on the barriers of both CTAs. Every wait is bounded; a pair whose waits
+// give up raises the error flag, and both CTAs meet at the closing cluster barrier before releasing
+// TMEM.
+__device__ __forceinline__ uint32_t cluster_ctarank()
+{
+    uint32_t r;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    return r;
+}
+
+// shared::cluster address of the same shared variable in CTA `rank` of the cluster
+__device__ __forceinline__ uint32_t cluster_addr(uint32_t saddr, uint32_t rank)
+{
+    uint32_t r;
+    asm volatile("mapa.shared::cluster.u32 %0, %1, %2;" : "=r"(r) : "r"(saddr), "r"(rank));
+    return r;
+}
+
+__device__ __forceinline__ void mbar_arrive_cluster(uint32_t cluster_bar)
+{
+    asm volatile("mbarrier.arrive.release.cluster.shared::cluster.b64 _, [%0];" ::"r"(cluster_bar) : "memory");
+}
+
+__device__ __forceinline__ void cluster_sync_all()
+{
+    asm volatile("barrier.cluster.arrive.release.aligned;" ::: "memory");
+    asm volatile("barrier.cluster.wait.acquire.aligned;" ::: "memory");
+}
+
+// copy into this CTA's shared memory, completing bytes on the barrier `cluster_bar` (the leader's)
+__device__ __forceinline__ void tma_load_2d_pair(uint32_t dst, const CUtensorMap *map, uint32_t cluster_bar, int x,
+                                                 int y)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.2d.cta_group::2.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1, {%3, %4}], "
+        "[%2];" ::"r"(dst),
+        "l"((uint64_t)map), "r"(cluster_bar), "r"(x), "r"(y)
+        : "memory");
+}
+
+__device__ __forceinline__ void umma_bf16_pair(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t idesc,
+                                               uint32_t accumulate)
+{
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::2.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(idesc), "r"(accumulate)
+        : "memory");
+}
+
+// arrives once on the barrier at this shared offset in every CTA of `mask` when the pair's MMAs
+// issued so far have completed
+__device__ __forceinline__ void umma_commit_pair(uint32_t bar, uint16_t mask)
+{
+    asm volatile("tcgen05.commit.cta_group::2.mbarrier::arrive::one.shared::cluster.multicast::cluster.b64 [%0], %1;"
+                 ::"r"(bar), "h"(mask)
+                 : "memory");
+}
+
+template <int DP, int BS> struct FlashPairShape {
+    static constexpr uint32_t TILE_A = kBM * kBK * 2;           // W k-block of 64 (hi or lo), own rows
+    static constexpr uint32_t HA = kBM * kBK * 2;               // q slice (hi or lo), own rows
+    static constexpr uint32_t HB = (BS / 2) * kBK * 2;          // this CTA's half of a Q_j slice
+    static constexpr uint32_t HG = (DP / 4) * kBK * 2;          // this CTA's half of a Q_j^T half slice, largest
+    static constexpr uint32_t SLOT_S = 2 * HA + 2 * HB;
+    static constexpr uint32_t SLOT = SLOT_S > 2 * HG ? SLOT_S : 2 * HG;
+    static constexpr uint32_t W = 2 * (BS / kBK) * TILE_A;
+    static constexpr int FIT = (int)((227u * 1024u - 2048u - 4u * kFlashMaxChunkTiles * BS - W) / SLOT);
+    static constexpr int STAGES = FIT > 8 ? 8 : FIT;
+    static constexpr size_t SMEM = (size_t)STAGES * SLOT + W + 1024;
+};
+
+template <int DP, int BS>
+__global__ void __launch_bounds__(kFlashThreads, 1)
+    k_gap_flash_pair(const __grid_constant__ CUtensorMap tm_q_hi, const __grid_constant__ CUtensorMap tm_q_lo,
+                     const __grid_constant__ CUtensorMap tm_Q_hi, const __grid_constant__ CUtensorMap tm_Q_lo,
+                     const __grid_constant__ CUtensorMap tm_QT_hi, const __grid_constant__ CUtensorMap tm_QT_lo,
+                     int n_chunks, int tiles_per_chunk, FlashGap p, int *err_flag)
+{
+    using Sh = FlashPairShape<DP, BS>;
+    static_assert(DP % 128 == 0 && DP + BS <= 512 && DP / 2 <= 256, "descriptor padding vs TMEM");
+    static_assert(BS == 128, "sparse tile of 128 points, 64 per CTA");
+    constexpr int STAGES = Sh::STAGES;
+    static_assert(STAGES >= 2, "ring of at least two slots");
+    constexpr int KG = BS / kBK;
+    constexpr int HC = BS / 2;
+    constexpr uint32_t TILE_A = Sh::TILE_A, HA = Sh::HA, HB = Sh::HB, HG = Sh::HG, SLOT = Sh::SLOT;
+    // M = 256 over the pair (bits [24, 29) hold M >> 4)
+    constexpr uint32_t IDESC_S = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BS >> 3) << 17) |
+                                 ((uint32_t)((2 * kBM) >> 4) << 24);
+    const int NH = p.nh;
+    const uint32_t IDESC_G = (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(NH >> 3) << 17) |
+                             ((uint32_t)((2 * kBM) >> 4) << 24);
+    constexpr uint32_t kCols = 512;
+    const bool forces = p.g != nullptr;
+    pdl_enter();
+    if (p.skip && *p.skip) return;  // uniform over the grid: both CTAs of every pair leave together
+
+    extern __shared__ __align__(1024) unsigned char smem_raw[];
+    __shared__ __align__(8) uint64_t bar_full[STAGES], bar_empty[STAGES];
+    __shared__ __align__(8) uint64_t bar_sfull, bar_sfree, bar_wfull, bar_wempty, bar_drain;
+    __shared__ __align__(16) float s_alpha[kFlashMaxChunkTiles * BS];
+    __shared__ uint32_t tmem_base_slot;
+    __shared__ volatile int abort_flag;
+    __shared__ int issued, consumed;
+
+    const uint32_t base = (smem_u32(smem_raw) + 1023u) & ~1023u;
+    const uint32_t wbase = base + STAGES * SLOT;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t rank = cluster_ctarank();
+    const int pair = blockIdx.x >> 1, rtp = pair / n_chunks, ch = pair - rtp * n_chunks;
+    const int T = tiles_per_chunk, j0 = ch * T, m0 = (2 * rtp + (int)rank) * kBM;
+    for (int i = threadIdx.x; i < T * BS; i += blockDim.x) s_alpha[i] = p.alphas[j0 * BS + i];
+
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < STAGES; ++s) {
+            mbar_init(smem_u32(&bar_full[s]), 1);
+            mbar_init(smem_u32(&bar_empty[s]), 1);
+        }
+        mbar_init(smem_u32(&bar_sfull), 1);
+        mbar_init(smem_u32(&bar_sfree), 2 * kFlashEpiWarps);  // one arrival per epilogue warp of the pair
+        mbar_init(smem_u32(&bar_wfull), 2 * kFlashEpiWarps);
+        mbar_init(smem_u32(&bar_wempty), 1);
+        mbar_init(smem_u32(&bar_drain), 1);
+        abort_flag = 0;
+        issued = 0;
+        consumed = 0;
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        const CUtensorMap *maps[6] = {&tm_q_hi, &tm_q_lo, &tm_Q_hi, &tm_Q_lo, &tm_QT_hi, &tm_QT_lo};
+        for (int i = 0; i < 6; ++i) asm volatile("prefetch.tensormap [%0];" ::"l"((uint64_t)maps[i]) : "memory");
+    }
+    if (warp == 1) {
+        asm volatile("tcgen05.alloc.cta_group::2.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
+                         smem_u32(&tmem_base_slot)),
+                     "r"(kCols)
+                     : "memory");
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::2.sync.aligned;" ::: "memory");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    // both CTAs' barriers exist and both hold their TMEM before any copy, MMA or remote arrival
+    cluster_sync_all();
+    asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+    const uint32_t tmem = tmem_base_slot;
+    const uint32_t tS = tmem, tG = tmem + BS;
+    const uint32_t lead_sfree = cluster_addr(smem_u32(&bar_sfree), 0);
+    const uint32_t lead_wfull = cluster_addr(smem_u32(&bar_wfull), 0);
+
+    if (warp == 0) {
+        if (lane == 0) {
+            // TMA producer of both CTAs, same slot order as the single-CTA kernel; the leader posts the
+            // pair's byte count on its full barrier, on which both CTAs' copies complete
+            int it = 0;
+            auto acquire = [&](uint32_t &slot, uint32_t &fb_own, uint32_t &fb_lead) -> bool {
+                const int s = it % STAGES;
+                const uint32_t ph = (uint32_t)(it / STAGES) & 1u;
+                if (it >= STAGES && !mbar_wait(smem_u32(&bar_empty[s]), ph ^ 1u, &abort_flag)) return false;
+                slot = base + s * SLOT;
+                fb_own = smem_u32(&bar_full[s]);
+                fb_lead = cluster_addr(fb_own, 0);
+                return true;
+            };
+            auto load_s = [&](int j) -> bool {
+                for (int kh = 0; kh < p.n_kh; ++kh) {
+                    uint32_t slot, fo, fl;
+                    if (!acquire(slot, fo, fl)) return false;
+                    if (rank == 0) mbar_expect_tx(fo, 2u * (2 * HA + 2 * HB));
+                    const int qrow = j * BS + (int)rank * (BS / 2);
+                    tma_load_2d_pair(slot, &tm_q_hi, fl, kh * kBK, m0);
+                    tma_load_2d_pair(slot + HA, &tm_q_lo, fl, kh * kBK, m0);
+                    tma_load_2d_pair(slot + 2 * HA, &tm_Q_hi, fl, kh * kBK, qrow);
+                    tma_load_2d_pair(slot + 2 * HA + HB, &tm_Q_lo, fl, kh * kBK, qrow);
+                    issued = ++it;
+                }
+                return true;
+            };
+            const uint32_t g_bytes = 2u * 2u * (uint32_t)(NH / 2) * (uint32_t)(kBK * 2);
+            auto load_g = [&](int j) -> bool {
+                for (int kh = 0; kh < BS / kBK; ++kh)
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t slot, fo, fl;
+                        if (!acquire(slot, fo, fl)) return false;
+                        if (rank == 0) mbar_expect_tx(fo, g_bytes);
+                        const int grow = h * NH + (int)rank * (NH / 2);
+                        tma_load_2d_pair(slot, &tm_QT_hi, fl, j * BS + kh * kBK, grow);
+                        tma_load_2d_pair(slot + HG, &tm_QT_lo, fl, j * BS + kh * kBK, grow);
+                        issued = ++it;
+                    }
+                return true;
+            };
+            bool ok = load_s(j0);
+            for (int t = 0; t < T && ok; ++t) {
+                if (t + 1 < T) ok = load_s(j0 + t + 1);
+                if (ok && forces) ok = load_g(j0 + t);
+            }
+            if (!ok) abort_flag = 1;
+            for (int i = (it > STAGES ? it - STAGES : 0); i < it && !abort_flag; ++i)
+                if (!mbar_wait(smem_u32(&bar_empty[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &abort_flag))
+                    abort_flag = 1;
+        }
+    } else if (warp == 1) {
+        if (lane == 0 && rank == 0) {
+            int it = 0;
+            auto take = [&](uint32_t &slot) -> bool {
+                const int s = it % STAGES;
+                if (!mbar_wait(smem_u32(&bar_full[s]), (uint32_t)(it / STAGES) & 1u, &abort_flag)) return false;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                slot = base + s * SLOT;
+                return true;
+            };
+            auto release = [&]() {
+                umma_commit_pair(smem_u32(&bar_empty[it % STAGES]), 0x3);  // the slot of both CTAs
+                consumed = ++it;
+            };
+            auto mma_s = [&]() -> bool {
+                for (int kh = 0; kh < p.n_kh; ++kh) {
+                    uint32_t slot;
+                    if (!take(slot)) return false;
+                    const int ks = kh == p.n_kh - 1 ? p.ks_last : kBK / 16;
+                    for (int k = 0; k < ks; ++k) {
+                        const uint64_t ahi = umma_desc(slot + 32 * k), alo = umma_desc(slot + HA + 32 * k);
+                        const uint64_t bhi = umma_desc(slot + 2 * HA + 32 * k);
+                        const uint64_t blo = umma_desc(slot + 2 * HA + HB + 32 * k);
+                        umma_bf16_pair(tS, ahi, bhi, IDESC_S, (kh > 0 || k > 0) ? 1u : 0u);
+                        umma_bf16_pair(tS, ahi, blo, IDESC_S, 1u);
+                        umma_bf16_pair(tS, alo, bhi, IDESC_S, 1u);
+                    }
+                    release();
+                }
+                umma_commit_pair(smem_u32(&bar_sfull), 0x3);
+                return true;
+            };
+            auto mma_g = [&](int t) -> bool {
+                if (!mbar_wait(smem_u32(&bar_wfull), (uint32_t)t & 1u, &abort_flag)) return false;
+                asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+                for (int kh = 0; kh < BS / kBK; ++kh)
+                    for (int h = 0; h < 2; ++h) {
+                        uint32_t slot;
+                        if (!take(slot)) return false;
+#pragma unroll
+                        for (int k = 0; k < kBK / 16; ++k) {
+                            const uint32_t wo = (uint32_t)kh * TILE_A + (uint32_t)k * 32;
+                            const uint64_t ahi = umma_desc(wbase + wo), alo = umma_desc(wbase + KG * TILE_A + wo);
+                            const uint64_t bhi = umma_desc(slot + 32 * k), blo = umma_desc(slot + HG + 32 * k);
+                            const uint32_t d = tG + (uint32_t)(h * NH);
+                            umma_bf16_pair(d, ahi, bhi, IDESC_G, (t > 0 || kh > 0 || k > 0) ? 1u : 0u);
+                            umma_bf16_pair(d, ahi, blo, IDESC_G, 1u);
+                            umma_bf16_pair(d, alo, bhi, IDESC_G, 1u);
+                        }
+                        release();
+                    }
+                umma_commit_pair(smem_u32(&bar_wempty), 0x3);
+                return true;
+            };
+            bool ok = mma_s();
+            for (int t = 0; t < T && ok; ++t) {
+                if (t + 1 < T) {
+                    ok = mbar_wait(smem_u32(&bar_sfree), (uint32_t)t & 1u, &abort_flag);
+                    if (ok) ok = mma_s();
+                }
+                if (ok && forces) ok = mma_g(t);
+            }
+            if (!ok) abort_flag = 1;
+            umma_commit_pair(smem_u32(&bar_drain), 0x1);
+            volatile int never = 0;
+            mbar_wait(smem_u32(&bar_drain), 0, &never);
+        }
+    } else {
+        const int quarter = warp & 3, half = (warp - 2) >> 2;
+        const int r = quarter * 32 + lane, row = m0 + r;
+        const uint32_t lane_base = (uint32_t)(quarter * 32) << 16;
+        float eacc = 0.0f;
+        bool ok = true;
+        for (int t = 0; t < T && ok; ++t) {
+            const int j = j0 + t;
+            ok = mbar_wait(smem_u32(&bar_sfull), (uint32_t)t & 1u, &abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (!ok || abort_flag) break;
+            uint32_t sraw[HC / 16][16];
+#pragma unroll
+            for (int c = 0; c < HC / 16; ++c) tmem_ld16_nowait(tS + lane_base + (uint32_t)(half * HC + c * 16), sraw[c]);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(lead_sfree);  // this warp's share of S may be overwritten
+            uint32_t hi[HC / 16][8], lo[HC / 16][8];
+#pragma unroll
+            for (int c = 0; c < HC / 16; ++c) {
+                float v[16];
+#pragma unroll
+                for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(sraw[c][i]);
+                const float *a16 = s_alpha + (j - j0) * BS + half * HC + c * 16;
+                switch (p.zeta_int) {
+                case 1: flash_w16<1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 2: flash_w16<2>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 3: flash_w16<3>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 4: flash_w16<4>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 5: flash_w16<5>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                case 6: flash_w16<6>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                default: flash_w16<-1>(v, a16, p.zd2, p.zeta, eacc, hi[c], lo[c]); break;
+                }
+            }
+            if (!forces) continue;
+            if (t > 0) {
+                ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(t - 1) & 1u, &abort_flag);
+                if (!ok) break;
+            }
+#pragma unroll
+            for (int c = 0; c < HC / 16; ++c) {
+#pragma unroll
+                for (int u = 0; u < 2; ++u) {
+                    const int col = half * HC + c * 16 + u * 8;
+                    const uint32_t off = (uint32_t)(col / kBK) * TILE_A + r * 128 +
+                                         (uint32_t)(((col % kBK) / 8) ^ (r & 7)) * 16;
+                    st_shared_v4(wbase + off, hi[c][4 * u], hi[c][4 * u + 1], hi[c][4 * u + 2], hi[c][4 * u + 3]);
+                    st_shared_v4(wbase + KG * TILE_A + off, lo[c][4 * u], lo[c][4 * u + 1], lo[c][4 * u + 2],
+                                 lo[c][4 * u + 3]);
+                }
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+            __syncwarp();
+            if (lane == 0) mbar_arrive_cluster(lead_wfull);  // this warp's W rows are in place
+        }
+        if (ok && !abort_flag && row < p.n_rows) {
+            double e = p.d2 * (double)eacc;
+            if (ch == 0 && half == 0) e += p.e0;
+            if (p.energies) atomicAdd(p.energies + (p.sites ? p.sites[row] : row), e);
+            if (p.e_rows) atomicAdd(p.e_rows + row, e);
+        }
+        if (ok && !abort_flag && forces) {
+            ok = mbar_wait(smem_u32(&bar_wempty), (uint32_t)(T - 1) & 1u, &abort_flag);
+            asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+            __syncwarp();
+            if (ok && !abort_flag) {
+#pragma unroll 1
+                for (int c = 0; c < NH; c += 16) {
+                    float v[16];
+                    tmem_ld16(tG + lane_base + (uint32_t)(half * NH + c), v);
+                    if (row < p.n_rows) {
+                        float4 *dst = reinterpret_cast<float4 *>(p.g + (size_t)row * p.ldg + half * NH + c);
+#pragma unroll
+                        for (int i = 0; i < 4; ++i)
+                            atomicAdd(dst + i, make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]));
+                    }
+                }
+            }
+        }
+        if (!ok) abort_flag = 1;
+    }
+    __syncwarp();
+    asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
+    __syncthreads();
+    if (abort_flag) {
+        if (threadIdx.x == 0) {
+            atomicExch(err_flag, 1);
+            volatile int dummy = 0;
+            if (rank == 0)
+                for (int i = consumed; i < issued; ++i)
+                    mbar_wait(smem_u32(&bar_full[i % STAGES]), (uint32_t)(i / STAGES) & 1u, &dummy);
+        }
+        __syncthreads();
+    }
+    // neither CTA releases TMEM while the pair's MMAs or the other CTA's reads may still use it
+    cluster_sync_all();
+    if (warp == 1) {
+        asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
+        asm volatile("tcgen05.dealloc.cta_group::2.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kCols) : "memory");
+    }
+}
+
 // ---------------------------------------------------------------------------- host
 
 typedef CUresult (*PFN_encodeTiled)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
@@ -979,6 +1364,73 @@ static int launch_flash(tgap_context *ctx, const DeviceModel &m, const __nv_bflo
     return TGAP_OK;
 }
 
+// The CTA-pair form (k_gap_flash_pair): row tiles in pairs, a 2-CTA cluster per (pair, sparse chunk).
+template <int DP, int BS>
+static int launch_flash_pair(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
+                             const __nv_bfloat16 *q_lo, int rows_pad, const FlashGap &p)
+{
+    using Sh = FlashPairShape<DP, BS>;
+    FlashGap q = p;
+    q.n_kh = (m.dim + kBK - 1) / kBK;
+    q.ks_last = (m.dim - (q.n_kh - 1) * kBK + 15) / 16;
+    q.nh = ((m.dim + 1) / 2 + 15) / 16 * 16;  // halves split again between the two CTAs: nh / 2 rows each
+    if (q.nh > DP / 2 || q.n_kh > DP / kBK) return set_error(ctx, TGAP_ERR_ARGUMENT, "fused GAP shape");
+    CUtensorMap tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo;
+    int rc;
+    if ((rc = make_map(ctx, &tq_hi, q_hi, rows_pad, DP, kBM)) || (rc = make_map(ctx, &tq_lo, q_lo, rows_pad, DP, kBM)) ||
+        (rc = make_map(ctx, &tQ_hi, m.Q_hi.ptr, m.m_pad, DP, BS / 2)) ||
+        (rc = make_map(ctx, &tQ_lo, m.Q_lo.ptr, m.m_pad, DP, BS / 2)) ||
+        (rc = make_map(ctx, &tT_hi, m.QT_hi.ptr, DP, m.m_pad, q.nh / 2)) ||
+        (rc = make_map(ctx, &tT_lo, m.QT_lo.ptr, DP, m.m_pad, q.nh / 2)))
+        return rc;
+    auto kern = k_gap_flash_pair<DP, BS>;
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)Sh::SMEM));
+    if (!ctx->d_flag) {
+        TGAP_CUDA(ctx, cudaMalloc(&ctx->d_flag, sizeof(int)));
+        TGAP_CUDA(ctx, cudaMemset(ctx->d_flag, 0, sizeof(int)));
+    }
+    const int J = m.m_pad / BS, n_rt = rows_pad / kBM, n_pairs = (n_rt + 1) / 2;
+    std::vector<int> divisors;
+    for (int d = 1; d <= J; ++d)
+        if (J % d == 0 && J / d <= kFlashMaxChunkTiles) divisors.push_back(d);
+    char key[96];
+    std::snprintf(key, sizeof(key), "gap_fused_pair/dp%d/bs%d/row_tiles%d/sparse_tiles%d", DP, BS, n_rt, J);
+    const int nc = tuned(ctx, key, "gemm_bf16x3_fused", divisors, flash_chunks(2 * n_pairs, J, sm_count(ctx)));
+    StageScope sc(ctx, "gemm_bf16x3_fused");
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(2 * n_pairs * nc);
+    cfg.blockDim = dim3(kFlashThreads);
+    cfg.dynamicSmemBytes = Sh::SMEM;
+    cfg.stream = ctx->stream;
+    cudaLaunchAttribute at[2];
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = 2;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    at[1].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[1].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 2;
+    TGAP_CUDA(ctx, cudaLaunchKernelEx(&cfg, kern, tq_hi, tq_lo, tQ_hi, tQ_lo, tT_hi, tT_lo, nc, J / nc, q, ctx->d_flag));
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+// The pair form where it applies (forces, no per-launch skip, at least two row tiles), else the
+// single-CTA kernel; the autotuner may pick either ("gap_fused_pair/.../pair" 1 or 0).
+template <int DP, int BS>
+static int launch_flash_any(tgap_context *ctx, const DeviceModel &m, const __nv_bfloat16 *q_hi,
+                            const __nv_bfloat16 *q_lo, int rows_pad, const FlashGap &p)
+{
+    const int n_rt = rows_pad / kBM, J = m.m_pad / BS;
+    if (p.g && !p.skip && !p.skip_tiles && n_rt >= 2) {
+        char key[96];
+        std::snprintf(key, sizeof(key), "gap_fused_pair/dp%d/bs%d/row_tiles%d/sparse_tiles%d/pair", DP, BS, n_rt, J);
+        if (tuned(ctx, key, "gemm_bf16x3_fused", {0, 1}, 1)) return launch_flash_pair<DP, BS>(ctx, m, q_hi, q_lo, rows_pad, p);
+    }
+    return launch_flash<DP, BS>(ctx, m, q_hi, q_lo, rows_pad, p);
+}
+
 // ---------------------------------------------------------------------------- GAP mixed path
 
 __global__ void k_split_bf16(int R, int C, int ld_in, const double *__restrict__ in, int R_pad, int C_pad,
@@ -1062,9 +1514,9 @@ int gap_energy_grad_mixed(tgap_context *ctx, const DeviceModel &m, const __nv_bf
         // 128-point sparse tiles (64-point ones allow a deeper ring but double the per-tile handoffs,
         // and measured slower)
         switch (m.dim_pad) {
-        case 128: return launch_flash<128, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
-        case 256: return launch_flash<256, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
-        default: return launch_flash<384, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
+        case 128: return launch_flash_any<128, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
+        case 256: return launch_flash_any<256, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
+        default: return launch_flash_any<384, kFlashBS>(ctx, m, q_hi, q_lo, rows_pad, p);
         }
     }
     if (d_skip) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "skippable launch needs the fused GAP kernel");
