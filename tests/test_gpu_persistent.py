@@ -69,3 +69,28 @@ def test_persistent_matches_one_site_per_warp(ctx, tg, synth, precision_name):
             assert np.max(np.abs(v1[b] - v_o)) < 1e-8, b
     system.close()
     model.close()
+
+
+def test_fused_gap_single_cta_and_cta_pair_forms_agree(ctx, tg, synth):
+    """The fused GAP kernel in its single-CTA form and in its CTA-pair form (tcgen05 cta_group::2,
+    each CTA of a 2-CTA cluster loading half of every sparse slice) give the same energies and
+    forces to FP32 accumulation order, on a system with an odd number of 128-row tiles (600 sites:
+    5 tiles, the last pair's second tile is padding)."""
+    hyp, m = helpers.carbon_model(synth, 300, seed=13)
+    pos, box, sp, _ = synth.random_packing(600, 2.5, 1.2, seed=14)
+    n = len(pos)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7)
+    out = {}
+    for form in (0, 1):
+        ctx.autotune_set("*/pair", form)
+        out[form] = _eval(system, model, tg.TGAP_MIXED, n, 1)
+    ctx.autotune_clear()
+    (e0, f0, v0), (e1, f1, v1) = out[0], out[1]
+    assert np.max(np.abs(e1 - e0)) <= 1e-6 * np.abs(e0).max() + 1e-15
+    assert np.max(np.abs(f1 - f0)) <= 1e-6 * np.abs(f0).max()
+    assert np.max(np.abs(v1 - v0)) <= 1e-6 * np.abs(v0).max()
+    e_d, f_d, _ = _eval(system, model, tg.TGAP_FP64, n, 1)
+    assert np.max(np.abs(e1 - e_d)) <= 1e-5 * np.abs(e_d).max() + 1e-12
+    system.close()
+    model.close()
