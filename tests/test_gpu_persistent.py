@@ -91,6 +91,6 @@ def test_fused_gap_single_cta_and_cta_pair_forms_agree(ctx, tg, synth):
     assert np.max(np.abs(f1 - f0)) <= 1e-6 * np.abs(f0).max()
     assert np.max(np.abs(v1 - v0)) <= 1e-6 * np.abs(v0).max()
     e_d, f_d, _ = _eval(system, model, tg.TGAP_FP64, n, 1)
-    assert np.max(np.abs(e1 - e_d)) <= 1e-5 * np.abs(e_d).max() + 1e-12
+    assert np.max(np.abs(e1 - e_d)) <= 1e-5  # eV per atom, far inside the 0.5 meV/atom bar
     system.close()
     model.close()

@@ -143,32 +143,51 @@ __device__ __forceinline__ void ylm_all(const YlmConst &Yc, T ux, T uy, T uz, F 
     }
 }
 
-// Pair acceptance: species channel known (and equal to only_s when only_s >= 0) and
-// 0 < r < rcut_hard(s).
-__device__ __forceinline__ bool pair_accept(const SoapParams &P, int64_t k, const double *__restrict__ rjs,
-                                            const int *__restrict__ nsp, int only_s)
-{
-    const int s = nsp[k] - 1;
-    if (s < 0 || s >= P.n_species || (only_s >= 0 && s != only_s)) return false;
-    const double r = __ldcg(rjs + k);  // L2-coherent: the forward may have written it this launch
-    return r > 0.0 && r < P.rcut_hard[s];
-}
+// Geometry of a group of at most 32 accepted pairs, staged per warp by the compaction so that the
+// lane evaluating pair p reads it from shared memory: |r_ij|, r_j - r_i, the list index and the
+// neighbor's species channel (0-based).
+struct GroupStage {
+    double r[32], x[32], y[32], z[32];
+    long long k[32];
+    int s[32];
+};
 
-// Compacts the next (at most 32) accepted pairs of [scan, ke) into idx[]; returns the count and
-// advances scan past the last pair taken.
-__device__ __forceinline__ int compact_pairs(const SoapParams &P, int64_t &scan, int64_t ke,
-                                             const double *__restrict__ rjs, const int *__restrict__ nsp,
-                                             int only_s, long long *idx, int lane)
+// Compacts the next (at most 32) accepted pairs of [scan, ke) into st with their geometry (accepted:
+// species channel known, and equal to only_s when only_s >= 0, and 0 < r < rcut_hard(s)); returns
+// the count and advances scan past the last pair taken. Every lane loads the geometry of its list
+// entry together with its species, so the group costs one round trip to L2 per 32 entries scanned.
+__device__ __forceinline__ int compact_stage(const SoapParams &P, int64_t &scan, int64_t ke,
+                                             const double *__restrict__ rjs, const double *__restrict__ xyz,
+                                             const int *__restrict__ nsp, int only_s, GroupStage *st, int lane)
 {
     int cnt = 0;
     while (cnt < 32 && scan < ke) {
         const int64_t k = scan + lane;
-        const bool ok = k < ke && pair_accept(P, k, rjs, nsp, only_s);
+        bool ok = false;
+        double d = 0.0, x = 0.0, y = 0.0, z = 0.0;
+        int s = -1;
+        if (k < ke) {
+            s = nsp[k] - 1;
+            // L2-coherent: an MD step's forward may have written them this launch
+            d = __ldcg(rjs + k);
+            x = __ldcg(xyz + 3 * k);
+            y = __ldcg(xyz + 3 * k + 1);
+            z = __ldcg(xyz + 3 * k + 2);
+            ok = s >= 0 && s < P.n_species && (only_s < 0 || s == only_s) && d > 0.0 && d < P.rcut_hard[s];
+        }
         const unsigned mask = __ballot_sync(0xffffffffu, ok);
         const int nv = __popc(mask);
         const int room = 32 - cnt;
         const int rank = __popc(mask & lanemask_lt());
-        if (ok && rank < room) idx[cnt + rank] = (long long)k;
+        if (ok && rank < room) {
+            const int o = cnt + rank;
+            st->r[o] = d;
+            st->x[o] = x;
+            st->y[o] = y;
+            st->z[o] = z;
+            st->k[o] = (long long)k;
+            st->s[o] = s;
+        }
         if (nv > room) {
             // resume at the first accepted pair that did not fit
             scan += __fns(mask, 0, room + 1);
@@ -275,6 +294,26 @@ __device__ __forceinline__ void warp_copy_row(T *dst, const T *__restrict__ src,
         for (int o = lane; o < n; o += 32) dst[o] = src[o];
     }
 }
+
+// dst[o] = src[o] for o < n as warp_copy_row, with asynchronous 16-byte copies (cp.async, one
+// commit group) where n and both pointers allow it, else a plain copy; dst may be read after
+// cp_async_wait_all and a __syncwarp.
+template <class T>
+__device__ __forceinline__ void warp_copy_row_async(T *dst, const T *__restrict__ src, int n, int lane)
+{
+    constexpr int VW = 16 / (int)sizeof(T);
+    if (n % VW == 0 && ((reinterpret_cast<uintptr_t>(src) | reinterpret_cast<uintptr_t>(dst)) & 15) == 0) {
+        const uint32_t d0 = (uint32_t)__cvta_generic_to_shared(dst);
+        for (int o = lane; o < n / VW; o += 32)
+            asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(d0 + 16u * (uint32_t)o), "l"(src + VW * o)
+                         : "memory");
+        asm volatile("cp.async.commit_group;" ::: "memory");
+    } else {
+        for (int o = lane; o < n; o += 32) dst[o] = src[o];
+    }
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Lane partial of q . g over n elements (FP32 rows of the same type four at a time when aligned;
 // the caller reduces across the warp).
@@ -455,14 +494,23 @@ template <int NLM> struct AStride {
 
 // ----------------------------------------------------------------------------- forward
 
-// Shared memory of one warp: 256 bytes of pair indices, Rs [32][AMB], then an area holding the
-// angular rows [32][ASTR] during the passes and the power spectrum [dim] after them, then the
-// expansion c [n_max][NLM].
-// Minimum resident CTAs of 4 warps asked of the compiler for the forward (0: no bound; an explicit
-// 1 grows the one-site FP32 form from 124 registers to 190). The persistent FP32 form asks for 4
-// (at most 128 registers; its site loop takes 158 without it); FP64 has none (128 spills).
+// Elements of the forward's middle area: the angular rows [32][astr], the power spectrum [dim] and
+// the group stage, whichever is largest, rounded to 16 bytes.
+template <class T> __host__ __device__ constexpr int fwd_area(int astr, int dim)
+{
+    const int a = 32 * astr > dim ? 32 * astr : dim;
+    const int g = (int)((sizeof(GroupStage) + sizeof(T) - 1) / sizeof(T));
+    const int m = a > g ? a : g;
+    return (m + (int)(16 / sizeof(T)) - 1) / (int)(16 / sizeof(T)) * (int)(16 / sizeof(T));
+}
+
+// Shared memory of one warp: Rs [32][AMB], then an area holding the group's staged geometry
+// (GroupStage, until the lanes have read it) and the angular rows [32][ASTR] during the passes and
+// the power spectrum [dim] after them, then the expansion c [n_max][NLM].
+// Minimum resident CTAs of 4 warps asked of the compiler for the forward: 4 in FP32 (at most 128
+// registers, the count at which four CTAs' shared memory also fits), none in FP64 (128 spills).
 template <class T, bool PERSIST> struct FwdMinCtas {
-    static constexpr int value = (PERSIST && std::is_same<T, float>::value) ? 4 : 0;
+    static constexpr int value = std::is_same<T, float>::value ? 4 : 0;
 };
 
 template <class T, int L, int AMB, bool SPLIT, bool PERSIST>
@@ -472,8 +520,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
     const int *__restrict__ sites, int n_rows, const int64_t *__restrict__ start,
     const double *__restrict__ rjs, const double *__restrict__ xyz, const int *__restrict__ nsp,
     T *__restrict__ c_out, T *__restrict__ q_out, int q_ld, T *__restrict__ norm_out,
-    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check, GeomSrc geo,
-    float *__restrict__ g_clear, int *queue)
+    __nv_bfloat16 *__restrict__ q_hi, __nv_bfloat16 *__restrict__ q_lo, int warp_smem, int *check,
+    const __grid_constant__ GeomSrc geo, float *__restrict__ g_clear, int *queue)
 {
     constexpr int NLM = (L + 1) * (L + 1);
     constexpr int ASTR = AStride<NLM>::value;
@@ -485,16 +533,20 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
     auto site_body = [&](const int row) {
         unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
         const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
-        long long *idx = reinterpret_cast<long long *>(wbase);
-        T *Rs = reinterpret_cast<T *>(wbase + 256);
+        T *Rs = reinterpret_cast<T *>(wbase);
         T *As = Rs + 32 * AMB;
-        T *cs = As + (32 * ASTR > dim ? 32 * ASTR : dim);
+        GroupStage *stage = reinterpret_cast<GroupStage *>(As);
+        T *cs = As + fwd_area<T>(ASTR, dim);
 
         const int site = sites ? sites[row] : row;
         const int64_t kb = start[site], ke = start[site + 1];
+        // the central atom's weights, loaded now and added to l = 0 of its own species block at the end
+        const int s_self = nsp[kb] - 1;
+        const bool has_central = s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self];
+        const T cen = has_central ? central[P.n_off[s_self] + lane] : (T)0;
         if (geo.pos) {
             // this step's pair geometry from the primitive positions (what the neighbor module's
-            // geometry pass would write), read back below through L2-coherent loads
+            // geometry pass would write), read back by the compaction through L2-coherent loads
             const StructDesc &S = static_cast<const StructDesc *>(geo.sd)[geo.site_struct[site]];
             double pi[3];
             sc_position(S, geo.pos, site - S.atom_off + 1, pi);
@@ -521,22 +573,24 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
                 for (int n = 0; n < AMB; ++n) acc[j][n] = 0;
             int64_t scan = kb + 1;
             while (scan < ke) {
-                const int cnt = compact_pairs(P, scan, ke, rjs, nsp, s, idx, lane);
+                const int cnt = compact_stage(P, scan, ke, rjs, xyz, nsp, s, stage, lane);
                 if (cnt == 0) break;
+                double rd = 1.0, xd = 0.0, yd = 0.0, zd = 1.0;
                 if (lane < cnt) {
-                    const int64_t k = idx[lane];
-                    const bool in_site = k > kb && k < ke;
-                    if (!in_site) check_fail(check, kCheckFwdPair, k, site);
-                    const double rd = in_site ? __ldcg(rjs + k) : 1.0;
+                    rd = stage->r[lane];
+                    xd = stage->x[lane];
+                    yd = stage->y[lane];
+                    zd = stage->z[lane];
+                }
+                __syncwarp();  // the angular rows below overwrite the stage
+                if (lane < cnt) {
                     const T r = (T)rd, ir = (T)1 / r;
-                    const T ux = in_site ? (T)__ldcg(xyz + 3 * k) * ir : (T)0;
-                    const T uy = in_site ? (T)__ldcg(xyz + 3 * k + 1) * ir : (T)0;
-                    const T uz = in_site ? (T)__ldcg(xyz + 3 * k + 2) * ir : (T)1;
+                    const T ux = (T)xd * ir, uy = (T)yd * ir, uz = (T)zd * ir;
                     T R[AMB], dR[AMB];
                     radial_values<T, AMB, false>(P, s, rd, xq, tq, rtab, R, dR);
                     T *Rrow = Rs + lane * AMB;
     #pragma unroll
-                    for (int n = 0; n < AMB; ++n) Rrow[n] = in_site ? R[n] : (T)0;
+                    for (int n = 0; n < AMB; ++n) Rrow[n] = R[n];
                     const T st = (T)P.sigma_t[s] + (T)P.sigma_t_scaling[s] * r;
                     T f[L + 2];
                     bessel_ratios_fixed<T, L>(r * r / (st * st), f);
@@ -568,9 +622,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         }
         __syncwarp();
         // central atom on l = 0 of its own species block
-        const int s_self = nsp[kb] - 1;
-        if (s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self])
-            cs[(P.n_off[s_self] + lane) * NLM] += central[P.n_off[s_self] + lane];
+        if (has_central) cs[(P.n_off[s_self] + lane) * NLM] += cen;
         __syncwarp();
         warp_copy_row<T>(c_out + (size_t)row * nout, cs, nout, lane);
         // power spectrum into the (now free) angular area: lane owns the (n, n') pairs
@@ -702,12 +754,12 @@ template <class T, bool PERSIST> struct BwdMinCtas {
     static constexpr int value = PERSIST ? (std::is_same<T, float>::value ? 4 : 2) : 1;
 };
 
-// Shared memory of one warp: 256 bytes of pair indices, c [n_max][NLM] (then the lanes'
-// force/virial partials), Gc [n_species][NLM][AMB] (dE/dc per species block, zero beyond
-// alpha_max), M [L+1][MSP] with M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l] in padded
-// species columns (MSP = bwd_m_pitch), f_l / df_l of each lane's pair [2][L+1][32]; after the
-// warps, the CTA's virial partials [kWarpsPerCta][6] and
-// structure ids [kWarpsPerCta].
+// Shared memory of one warp: the group's staged geometry (GroupStage), c [n_max][NLM] (then the lanes'
+// force/virial partials), M [L+1][MSP] with M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l] in
+// padded species columns (MSP = bwd_m_pitch), Gc [n_species][NLM][AMB] (dE/dc per species block,
+// zero beyond alpha_max), f_l / df_l of each lane's pair [2][L+1][32]; h [dim] occupies the area
+// of Gc and f_l / df_l (grown to dim when smaller) until M is formed. After the warps, the CTA's
+// virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
 template <class T, class GT, int L, int AMB, bool PERSIST>
 __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::value) k_soap_bwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
@@ -737,24 +789,30 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
         if (pair_der && gate && gate[sites ? sites[row] : row] == 0.0) return;
         unsigned char *wbase = smem_raw + (size_t)warp * warp_smem;
         const int nmax = P.n_max, dim = P.dim, nout = nmax * NLM;
-        long long *idx = reinterpret_cast<long long *>(wbase);
-        T *cs = reinterpret_cast<T *>(wbase + 256);
-        T *Gc = cs + bwd_c_elems<T>(nout);
-        T *Ms = Gc + P.n_species * NLM * AMB;
+        GroupStage *stage = reinterpret_cast<GroupStage *>(wbase);
+        T *cs = reinterpret_cast<T *>(wbase + sizeof(GroupStage));
         const int MP = P.n_species * AMB, MSP = bwd_m_pitch<T>(nmax, MP);
-        T *fdf = Ms + (L + 1) * MSP;  // [2][L+1][32]: f_l, df_l of each lane's pair
+        T *Ms = cs + bwd_c_elems<T>(nout);
+        T *Gc = Ms + (L + 1) * MSP;
+        T *fdf = Gc + P.n_species * NLM * AMB;  // [2][L+1][32]: f_l, df_l of each lane's pair
+        T *hb = Gc;                             // h [dim] until M is formed
 
         const int site = sites ? sites[row] : row;
         const int my_struct = site_struct ? site_struct[site] : 0;
         const int64_t kb = start[site], ke = start[site + 1];
-        warp_copy_row<T>(cs, c_in + (size_t)row * nout, nout, lane);
+        // c arrives asynchronously (it is first read when Gc is formed)
+        warp_copy_row_async<T>(cs, c_in + (size_t)row * nout, nout, lane);
+        const T nrm = norm_in[row];
         const T *qrow = q_in + (size_t)row * q_ld;
         const GT *grow = g_in + (size_t)row * g_ld;
         T qg = warp_dot_part<T, GT>(qrow, grow, dim, lane);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
-        const T nrm = norm_in[row];
         const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
+        // h = dE/dp = (g - q (q.g)) / |p| into shared memory: independent coalesced loads (the rows
+        // were just read for q.g), so the M entries below are formed at shared-memory latency
+        for (int d = lane; d < dim; d += 32) hb[d] = ((T)grow[d] - qrow[d] * qg) * inv;
+        __syncwarp();
         // M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l], h = dE/dp = (g - q (q.g)) / |p|, stored
         // as rows n' of n_species blocks of AMB columns (radial index n_off[s] + a in column
         // s AMB + a; columns beyond alpha_max stay zero). M_l is symmetric, so the slice of row n'
@@ -776,7 +834,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
             }
             for (int pp = sub; sub < PPW && pp < npair; pp += PPW) {
                 const int np = n + rem, d = pp * (L + 1) + l;
-                const T hv = ((T)grow[d] - qrow[d] * qg) * inv;
+                const T hv = hb[d];
                 const T mv = (n == np) ? (T)2 * hv : (T)1.4142135623730951 * hv;
                 int sn = 0, snp = 0;  // species blocks of n and n'
                 for (int s = 1; s < P.n_species; ++s) {
@@ -793,6 +851,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
                 }
             }
         }
+        cp_async_wait_all();
         __syncwarp();
         // Gc[s][lm][a] = sum_n' M_l[n_off[s] + a][n'] c[n'][lm]: one c value and one padded M row
         // slice per n', accumulated with row FMAs
@@ -825,16 +884,13 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
 
         int64_t scan = kb + 1;
         while (scan < ke) {
-            const int cnt = compact_pairs(P, scan, ke, rjs, nsp, -1, idx, lane);
+            const int cnt = compact_stage(P, scan, ke, rjs, xyz, nsp, -1, stage, lane);
             if (cnt == 0) break;
-            const bool mine = lane < cnt;
-            const int64_t k = mine ? idx[lane] : kb;
-            const bool in_site = k > kb && k < ke;
-            if (mine && !in_site) check_fail(check, kCheckBwdPair, k, site);
-            if (mine && in_site) {
-                const int s = nsp[k] - 1;
-                const double xd0 = xyz[3 * k], xd1 = xyz[3 * k + 1], xd2 = xyz[3 * k + 2];
-                const double rd = rjs[k];
+            if (lane < cnt) {
+                const int64_t k = stage->k[lane];
+                const int s = stage->s[lane];
+                const double xd0 = stage->x[lane], xd1 = stage->y[lane], xd2 = stage->z[lane];
+                const double rd = stage->r[lane];
                 const T r = (T)rd;
                 const T ir = (T)1 / r;
                 const T u0 = (T)xd0 * ir, u1 = (T)xd1 * ir, u2 = (T)xd2 * ir;
@@ -974,8 +1030,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
 inline size_t fwd_warp_bytes(const SoapParams &P, size_t tsz, int astr, int amb)
 {
     const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
-    const size_t area = std::max<size_t>(32 * (size_t)astr, (size_t)P.dim);
-    return 256 + (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
+    const size_t area = tsz == 8 ? (size_t)fwd_area<double>(astr, P.dim) : (size_t)fwd_area<float>(astr, P.dim);
+    return (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
 }
 
 template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
@@ -984,8 +1040,9 @@ template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
     const int nout = P.n_max * (int)nlm;
     const size_t ms = (size_t)(P.l_max + 1) * bwd_m_pitch<T>(P.n_max, P.n_species * amb);
     const size_t fdf = 2 * (size_t)(P.l_max + 1) * 32;
-    return 256 +
-           (sizeof(T) * ((size_t)bwd_c_elems<T>(nout) + (size_t)P.n_species * nlm * amb + ms + fdf) + 15) / 16 * 16;
+    const size_t gf = std::max<size_t>((size_t)P.n_species * nlm * amb + fdf, (size_t)P.dim);  // Gc + f/df, or h
+    static_assert(sizeof(GroupStage) % 16 == 0, "the adjoint's arrays after the stage stay 16-byte aligned");
+    return sizeof(GroupStage) + (sizeof(T) * ((size_t)bwd_c_elems<T>(nout) + ms + gf) + 15) / 16 * 16;
 }
 
 constexpr size_t kMaxDynSmem = 227 * 1024;
