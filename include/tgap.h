@@ -237,6 +237,8 @@ int tgap_system_get_positions(tgap_system *system, double *positions);
 int tgap_system_set_positions(tgap_system *system, const double *positions);
 /* Rebuild the neighbor lists (or only refresh geometry when rebuild == 0). */
 int tgap_system_update(tgap_system *system, int rebuild);
+/* Pairs in the current lists (self entries included). After an MD run has rebuilt the lists on the
+   device this reads the count back (synchronizes the context stream); -1 on a CUDA error. */
 int64_t tgap_system_n_pairs(const tgap_system *system);
 
 /* calculate_e0 (src/gap/calculate_gap_soap.f90:135-169): isolated-atom energies per species

@@ -333,6 +333,54 @@ def test_md_fp64_matches_oracle_verlet(ctx, tg, synth, carbon):
     assert len(pairs) > 1  # the list changed size across rebuilds
 
 
+def test_md_device_rebuild_count_matches_a_host_rebuild(ctx, tg, synth, carbon):
+    """After the first step the MD rebuilds its lists on the device without reading the pair count
+    back; tgap_system_n_pairs then reads it, and it equals the count of a host rebuild at the same
+    positions (the positions the rebuild step started from)."""
+    hyp, m = carbon
+    pos, box, sp, masses = synth.random_packing(128, 2.5, 1.2, seed=71)
+    vel = synth.maxwell_boltzmann(masses, 3000.0, seed=3)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=3, use_graph=True)
+    md.set_velocities(vel)
+    md.run(3)
+    x3 = md.state()["positions"]
+    md.run(1)  # step 3 rebuilds on x3
+    n_dev = system.n_pairs
+    ref = tg.System(ctx, [(x3, box, sp)], 3.7 + 0.3)
+    assert n_dev == ref.n_pairs
+    ref.close()
+    md.close()
+    system.close()
+    model.close()
+
+
+def test_md_pair_capacity_overflow_is_reported(ctx, tg, synth, carbon):
+    """A device-side rebuild that finds more pairs than the arrays reserved (a quarter above the
+    first list) clamps the lists inside the arrays and reports TGAP_ERR_CAPACITY at the next check,
+    with no fault: the atoms are drawn halfway towards the box centre (128 atoms in a 5 A cube,
+    nearly all of them neighbors of each other) before the next rebuild."""
+    hyp, m = carbon
+    pos, box, sp, masses = synth.random_packing(128, 2.5, 1.2, seed=72)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    md = tg.MD(ctx, system, [model], masses, 0.5, rebuild_every=2, use_graph=True)
+    md.set_velocities(np.zeros_like(pos))
+    md.run(2)
+    x = md.state()["positions"]
+    c = 0.5 * np.asarray(box).sum(axis=0)
+    system.set_positions(c + 0.5 * (x - c))
+    with pytest.raises(tg.TgapError) as err:
+        md.run(2)
+        md.state()
+    assert err.value.status == 3  # TGAP_ERR_CAPACITY
+    ctx.synchronize()
+    md.close()
+    system.close()
+    model.close()
+
+
 # ------------------------------------------------------------------------- local properties
 
 def test_local_property_predict_matches_oracle(ctx, synth):

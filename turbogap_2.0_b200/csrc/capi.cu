@@ -265,9 +265,13 @@ int read_device_check(tgap_context *ctx)
                                  "descriptor adjoint: self-slot atom out of range",
                                  "non-finite force",
                                  "neighbor fill past its counted range",
-                                 "Monte Carlo trial capacity exceeded"};
-    const char *w = (h[0] > 0 && h[0] <= kCheckMcOverflow) ? what[h[0]] : "unknown check";
-    return set_error(ctx, h[0] == kCheckNonFinite ? TGAP_ERR_NUMERIC : TGAP_ERR_CUDA,
+                                 "Monte Carlo trial capacity exceeded",
+                                 "device-side list rebuild: more pairs than the reserved capacity"};
+    const char *w = (h[0] > 0 && h[0] <= kCheckPairCapacity) ? what[h[0]] : "unknown check";
+    const int status = h[0] == kCheckNonFinite ? TGAP_ERR_NUMERIC
+                       : h[0] == kCheckPairCapacity ? TGAP_ERR_CAPACITY
+                                                    : TGAP_ERR_CUDA;
+    return set_error(ctx, status,
                      "device check %d (%s): index %d value %d, %d failure(s)", h[0], w, h[1], h[2], h[3]);
 }
 
@@ -856,7 +860,14 @@ extern "C" int tgap_system_destroy(tgap_system *s)
 }
 
 extern "C" int tgap_system_n_atoms(const tgap_system *s) { return s ? s->nb.n_atoms : 0; }
-extern "C" int64_t tgap_system_n_pairs(const tgap_system *s) { return s ? s->nb.n_pairs : 0; }
+extern "C" int64_t tgap_system_n_pairs(const tgap_system *s)
+{
+    if (!s) return 0;
+    // after device-side rebuilds (MD) the count is read back here
+    tgap_system *m = const_cast<tgap_system *>(s);
+    if (m->nb.count_on_device && (activate(m->ctx) || neighbors_sync_count(m->ctx, &m->nb))) return -1;
+    return s->nb.n_pairs;
+}
 
 extern "C" int tgap_system_positions(tgap_system *s, double **d_positions)
 {
@@ -1121,8 +1132,10 @@ extern "C" int tgap_local_property(tgap_context *ctx, tgap_system *s, tgap_model
     if (precision != TGAP_FP64 && precision != TGAP_MIXED) return set_error(ctx, TGAP_ERR_ARGUMENT, "precision");
     const int N = s->nb.n_atoms;
     TGAP_CUDA(ctx, cudaMemsetAsync(d_V, 0, sizeof(double) * N, ctx->stream));
-    if (do_derivatives)
+    if (do_derivatives) {
+        CHECK_RC(neighbors_sync_count(ctx, &s->nb));
         TGAP_CUDA(ctx, cudaMemsetAsync(d_V_der, 0, sizeof(double) * 3 * (size_t)s->nb.n_pairs, ctx->stream));
+    }
     SiteSet *ss = nullptr;
     CHECK_RC(site_set(s, m->central_species, &ss));
     const int n_rows = ss->n_rows;
@@ -1485,6 +1498,20 @@ struct tgap_md {
     cudaGraphExec_t exec_run = nullptr;
     uint64_t run_epoch = 0;
     int64_t run_kernels = 0;
+    // list rebuilds after the first run on the device inside the step graphs, with no read-back
+    // of the pair count (neighbors_rebuild_lists_device): systems without pair/triplet terms,
+    // whose buffers follow the host count
+    bool device_rebuild = false;
+    // a whole rebuild cycle (the rebuild step and the rebuild_every - 1 steps after it) as one graph
+    cudaGraph_t graph_cycle = nullptr;
+    cudaGraphExec_t exec_cycle = nullptr;
+    uint64_t cycle_epoch = 0;
+    int64_t cycle_kernels = 0;
+    // one rebuild step as a graph (when fewer steps than a cycle are asked for)
+    cudaGraph_t graph_rb = nullptr;
+    cudaGraphExec_t exec_rb = nullptr;
+    uint64_t rb_epoch = 0;
+    int64_t rb_kernels = 0;
 };
 
 static int terms_add(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_forces, double *d_e, double *d_f,
@@ -1525,11 +1552,17 @@ static int md_eval(tgap_md *md)
     return TGAP_OK;
 }
 
-// one step after the first: geometry refresh, forces, velocity Verlet
-static int md_step_body(tgap_md *md)
+// one step after the first: geometry refresh, forces, velocity Verlet; with rebuild, new lists on
+// this step's positions first, built on the device (the refresh gives them their species, atom
+// maps and geometry)
+static int md_step_body(tgap_md *md, bool rebuild = false)
 {
     tgap_context *ctx = md->ctx;
-    if (!md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
+    if (rebuild) {
+        CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
+        CHECK_RC(neighbors_rebuild_lists_device(ctx, &md->sys->nb));
+    }
+    if (rebuild || !md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     CHECK_RC(md_eval(md));
     CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
                              md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),
@@ -1670,15 +1703,24 @@ extern "C" int tgap_md_set_terms(tgap_md *md, tgap_terms *t)
         CHECK_RC(upload(ctx, md->sys->d_species, md->sys->host_species.data(), md->sys->host_species.size()));
     md->terms = t;
     md->fused_geom = md_can_fuse_geometry(md);
+    md->device_rebuild = !md->terms;
     // the step graphs change
     if (md->exec) cudaGraphExecDestroy(md->exec);
     if (md->graph) cudaGraphDestroy(md->graph);
     if (md->exec_run) cudaGraphExecDestroy(md->exec_run);
     if (md->graph_run) cudaGraphDestroy(md->graph_run);
+    if (md->exec_cycle) cudaGraphExecDestroy(md->exec_cycle);
+    if (md->graph_cycle) cudaGraphDestroy(md->graph_cycle);
+    if (md->exec_rb) cudaGraphExecDestroy(md->exec_rb);
+    if (md->graph_rb) cudaGraphDestroy(md->graph_rb);
+    md->exec_rb = nullptr;
+    md->graph_rb = nullptr;
     md->exec = nullptr;
     md->graph = nullptr;
     md->exec_run = nullptr;
     md->graph_run = nullptr;
+    md->exec_cycle = nullptr;
+    md->graph_cycle = nullptr;
     return TGAP_OK;
 }
 
@@ -1695,6 +1737,7 @@ extern "C" int tgap_md_create(tgap_context *ctx, tgap_system *sys, int n_models,
     md->models.assign(models, models + n_models);
     md->precision = precision;
     md->fused_geom = md_can_fuse_geometry(md);
+    md->device_rebuild = !md->terms;
     md->rebuild_every = rebuild_every;
     md->use_graph = use_graph;
     md->dt = dt;
@@ -1738,6 +1781,10 @@ extern "C" int tgap_md_destroy(tgap_md *md)
     if (md->graph) cudaGraphDestroy(md->graph);
     if (md->exec_run) cudaGraphExecDestroy(md->exec_run);
     if (md->graph_run) cudaGraphDestroy(md->graph_run);
+    if (md->exec_cycle) cudaGraphExecDestroy(md->exec_cycle);
+    if (md->graph_cycle) cudaGraphDestroy(md->graph_cycle);
+    if (md->exec_rb) cudaGraphExecDestroy(md->exec_rb);
+    if (md->graph_rb) cudaGraphDestroy(md->graph_rb);
     DevBuf *bufs[] = {&md->mass, &md->vel, &md->forces_prev, &md->pos_prev, &md->out};
     for (DevBuf *b : bufs) b->release();
     delete md;
@@ -1753,9 +1800,10 @@ extern "C" int tgap_md_set_velocities(tgap_md *md, const double *v)
     return TGAP_OK;
 }
 
-// Captures n_steps step bodies into one graph (re-captured when an allocation moved a buffer).
+// Captures n_steps step bodies into one graph (re-captured when an allocation moved a buffer); the
+// first of them rebuilds the lists on the device when rebuild_first is set.
 static int md_graph(tgap_md *md, int n_steps, cudaGraph_t *graph, cudaGraphExec_t *exec, uint64_t *epoch,
-                    int64_t *kernels)
+                    int64_t *kernels, bool rebuild_first = false)
 {
     tgap_context *ctx = md->ctx;
     if (*exec && *epoch == g_alloc_epoch.load(std::memory_order_relaxed)) return TGAP_OK;
@@ -1767,7 +1815,7 @@ static int md_graph(tgap_md *md, int n_steps, cudaGraph_t *graph, cudaGraphExec_
     TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
     const int64_t launches = ctx->launches;
     int rc = TGAP_OK;
-    for (int i = 0; i < n_steps && !rc; ++i) rc = md_step_body(md);
+    for (int i = 0; i < n_steps && !rc; ++i) rc = md_step_body(md, rebuild_first && i == 0);
     cudaGraph_t g = nullptr;
     cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
     *kernels = ctx->launches - launches;
@@ -1790,6 +1838,17 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
     CHECK_RC(activate(ctx));
     for (int it = 0; it < n_steps; ++it) {
         const bool rebuild = (md->step % md->rebuild_every) == 0;
+        // a whole rebuild cycle goes out as one graph launch when the lists are rebuilt on the device
+        if (md->use_graph && !md->first && rebuild && md->device_rebuild && n_steps - it >= md->rebuild_every) {
+            CHECK_RC(md_graph(md, md->rebuild_every, &md->graph_cycle, &md->exec_cycle, &md->cycle_epoch,
+                              &md->cycle_kernels, true));
+            TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_cycle, ctx->stream));
+            ctx->launches += md->cycle_kernels;
+            md->sys->nb.count_on_device = true;  // set at capture only: every replay rebuilds
+            md->step += md->rebuild_every;
+            it += md->rebuild_every - 1;
+            continue;
+        }
         // a full run of rebuild-free steps goes out as one graph launch
         const int run = md->rebuild_every - 1;
         if (md->use_graph && !md->first && !rebuild && run > 1 && md->step % md->rebuild_every == 1 &&
@@ -1801,7 +1860,7 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
             it += run - 1;
             continue;
         }
-        if (!md->first && rebuild) {
+        if (!md->first && rebuild && !md->device_rebuild) {
             // new pair lists on the current positions (one host synchronization for the pair
             // count); the step below refreshes the geometry on them like any other step
             CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
@@ -1819,12 +1878,17 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
                                      md->forces_prev.as<double>(), md->mass.as<double>(), md->dt, md->dt,
                                      md->first ? 1 : 0));
             md->first = false;
+        } else if (rebuild && md->device_rebuild && md->use_graph) {
+            CHECK_RC(md_graph(md, 1, &md->graph_rb, &md->exec_rb, &md->rb_epoch, &md->rb_kernels, true));
+            TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_rb, ctx->stream));
+            ctx->launches += md->rb_kernels;
+            md->sys->nb.count_on_device = true;
         } else if (md->use_graph) {
             CHECK_RC(md_graph(md, 1, &md->graph, &md->exec, &md->graph_epoch, &md->graph_kernels));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec, ctx->stream));
             ctx->launches += md->graph_kernels;
         } else {
-            CHECK_RC(md_step_body(md));
+            CHECK_RC(md_step_body(md, rebuild && md->device_rebuild));
         }
         ++md->step;
     }

@@ -251,6 +251,38 @@ __global__ void k_nneigh_from_counts(int n, const int64_t *cnt, int *n_neigh)
     if (g < n) n_neigh[g] = (int)cnt[g];
 }
 
+// Device-side rebuild, one CTA: n_neigh from the list offsets, which stay as they are when the
+// lists fit the reserved pair capacity cap. Longer lists are recorded in the check word and every
+// offset is clamped to cap - 1 (start[i] = min(start[i], cap - 1)): each later pass, the self entry
+// that the descriptor kernels read at start[i] included, stays inside the arrays; the tail sites
+// get no pairs and the fill records the site it cut. The decision is taken once, from start[n],
+// before any offset changes; thread i reading start[i + 1] while another thread clamps it gets
+// the same min(., cap - 1) either way.
+__global__ void k_fit_pairs(int n, int64_t *start, int *n_neigh, int64_t cap, int *check)
+{
+    __shared__ int over;
+    if (threadIdx.x == 0) {
+        over = start[n] > cap;
+        if (over) check_fail(check, kCheckPairCapacity, n, (long long)start[n]);
+    }
+    __syncthreads();
+    const int64_t lim = cap - 1;
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) {
+        int64_t a = start[i];
+        if (i < n) {
+            int64_t b = start[i + 1];
+            if (over) {
+                a = a < lim ? a : lim;
+                b = b < lim ? b : lim;
+            }
+            n_neigh[i] = (int)(b - a);
+        } else if (over) {
+            a = a < lim ? a : lim;
+        }
+        if (over) start[i] = a;
+    }
+}
+
 static int scan_i64(tgap_context *ctx, DevBuf &tmp, const int64_t *in, int64_t *out, int n)
 {
     size_t bytes = 0;
@@ -340,18 +372,15 @@ int make_struct_desc(const double a[3], const double b[3], const double c[3], in
     return TGAP_OK;
 }
 
-int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out)
+// The counting half of a rebuild: cell lists, per-site pair counts and their exclusive scan
+// (start[0..n]). Stream-ordered only.
+static int rebuild_count(tgap_context *ctx, NeighborBatch *nb)
 {
     const int n = nb->n_atoms;
-    if (n <= 0) {
-        *n_pairs_out = 0;
-        return TGAP_OK;
-    }
     const int T = 128;
     const int grid = (n + T - 1) / T;
     const int wgrid = (n + T / 32 - 1) / (T / 32);  // one warp per site
     StructDesc *d_sd = nb->d_structs.as<StructDesc>();
-    StageScope sc(ctx, "neighbors_rebuild");
     // cells
     if (nb->n_cells > 0) {
         TGAP_CUDA(ctx, cudaMemsetAsync(nb->cell_count.ptr, 0, sizeof(int) * (nb->n_cells + 1), ctx->stream));
@@ -374,8 +403,34 @@ int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capaci
                                                       nb->counts.as<int64_t>(), nullptr, nullptr, nullptr);
     TGAP_LAUNCH_CHECK(ctx);
     TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
-    int rc = scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
-    if (rc) return rc;
+    return scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
+}
+
+// The filling half: each warp writes its site's pairs inside [start[g], start[g + 1]).
+static int rebuild_fill(tgap_context *ctx, NeighborBatch *nb)
+{
+    const int n = nb->n_atoms;
+    const int T = 128;
+    const int wgrid = (n + T / 32 - 1) / (T / 32);
+    k_site_pairs<true><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(),
+                                                     nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
+                                                     nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(),
+                                                     nb->list.as<int>(), ctx->d_check);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out)
+{
+    const int n = nb->n_atoms;
+    if (n <= 0) {
+        *n_pairs_out = 0;
+        return TGAP_OK;
+    }
+    const int T = 128;
+    const int grid = (n + T - 1) / T;
+    StageScope sc(ctx, "neighbors_rebuild");
+    if (const int rc = rebuild_count(ctx, nb)) return rc;
     int64_t total = 0;
     TGAP_CUDA(ctx, cudaMemcpyAsync(&total, nb->start.as<int64_t>() + n, sizeof(int64_t), cudaMemcpyDeviceToHost,
                                    ctx->stream));
@@ -384,12 +439,35 @@ int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capaci
     if (capacity >= 0 && total > capacity) return TGAP_ERR_CAPACITY;
     if (nb->ensure_pairs(total)) return set_error(ctx, TGAP_ERR_NOMEM, "pair arrays");
     nb->n_pairs = total;
+    nb->count_on_device = false;
     k_nneigh_from_counts<<<grid, T, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->n_neigh.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
-    k_site_pairs<true><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
-                                                     nb->cell_start.as<int>(), nb->cell_atoms.as<int>(), nullptr,
-                                                     nb->start.as<int64_t>(), nb->list.as<int>(), ctx->d_check);
+    return rebuild_fill(ctx, nb);
+}
+
+int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb)
+{
+    const int n = nb->n_atoms;
+    if (n <= 0) return TGAP_OK;
+    if (!nb->list.ptr) return set_error(ctx, TGAP_ERR_ARGUMENT, "device-side list rebuild before any list was built");
+    StageScope sc(ctx, "neighbors_rebuild");
+    if (const int rc = rebuild_count(ctx, nb)) return rc;
+    k_fit_pairs<<<1, 1024, 0, ctx->stream>>>(n, nb->start.as<int64_t>(), nb->n_neigh.as<int>(), nb->pair_capacity(),
+                                             ctx->d_check);
     TGAP_LAUNCH_CHECK(ctx);
+    nb->count_on_device = true;
+    return rebuild_fill(ctx, nb);
+}
+
+int neighbors_sync_count(tgap_context *ctx, NeighborBatch *nb)
+{
+    if (!nb->count_on_device) return TGAP_OK;
+    int64_t total = 0;
+    TGAP_CUDA(ctx, cudaMemcpyAsync(&total, nb->start.as<int64_t>() + nb->n_atoms, sizeof(int64_t),
+                                   cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    nb->n_pairs = total;
+    nb->count_on_device = false;
     return TGAP_OK;
 }
 
@@ -423,6 +501,7 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
         const int rc = neighbors_rebuild_lists(ctx, nb, capacity, n_pairs_out);
         if (rc) return rc;
     } else {
+        if (const int rc = neighbors_sync_count(ctx, nb)) return rc;
         *n_pairs_out = nb->n_pairs;
     }
     return neighbors_geometry(ctx, nb, with_angles, false);

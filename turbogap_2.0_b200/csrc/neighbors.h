@@ -30,6 +30,9 @@ struct NeighborBatch {
     int n_sc_total = 0;
     int n_cells = 0;
     int64_t n_pairs = 0;
+    // n_pairs is not yet read back: the lists were last rebuilt on the device alone
+    // (neighbors_rebuild_lists_device; neighbors_sync_count reads it)
+    bool count_on_device = false;
     bool replicated = true;  // every supercell is a pure replica of its primitive cell
     std::vector<StructDesc> host_structs;
     DevBuf d_structs;
@@ -47,6 +50,7 @@ struct NeighborBatch {
     DevBuf jatom;           // int [P] folded global atom of the neighbor
     DevBuf scan_tmp;
     int ensure_pairs(int64_t P);
+    int64_t pair_capacity() const { return (int64_t)(list.bytes / sizeof(int)); }
     void release_all()
     {
         DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &atom_cell,
@@ -73,6 +77,13 @@ int neighbors_setup_supercell(tgap_context *ctx, NeighborBatch *nb, int n_sites,
 int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t capacity,
                     int64_t *n_pairs_out, bool with_angles);
 int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out);
+// The same lists rebuilt without a host synchronization (capturable in a graph), inside the pair
+// arrays already reserved (pair_capacity(), a quarter above the count they were sized for): the
+// offsets are clamped below that capacity, and a longer list is recorded in the device check word
+// (kCheckPairCapacity, reported as TGAP_ERR_CAPACITY at the next check). n_pairs is then read
+// back lazily by neighbors_sync_count.
+int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb);
+int neighbors_sync_count(tgap_context *ctx, NeighborBatch *nb);
 // from_positions: form supercell positions from the primitive ones inside the kernel
 int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, bool from_positions);
 // Geometry of the current lists at the current (primitive) positions.

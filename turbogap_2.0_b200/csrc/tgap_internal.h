@@ -153,6 +153,7 @@ enum CheckCode {
     kCheckNonFinite = 5,    // velocity Verlet: non-finite force
     kCheckListOverrun = 6,  // neighbor fill wrote past its counted range
     kCheckMcOverflow = 7,   // Monte Carlo: affected sites or pairs beyond the trial capacity
+    kCheckPairCapacity = 8, // device-side list rebuild: more pairs than the reserved capacity
 };
 
 #ifdef __CUDACC__
