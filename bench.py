@@ -444,13 +444,22 @@ def _e2e(tg, ctx, system, model, masses, vel, pos0, precision, steps):
     for k in range(3):  # warm-up
         force(k)
     x[:] = pos0
+    # velocity Verlet on the host with preallocated arrays (md_utils.f90:486-532)
+    cv = 0.5 * DT / mm
+    cx = 0.5 * DT * DT / mm
+    tmp = np.empty_like(f)
     t0 = time.perf_counter()
     for k in range(steps):
         force(k)
         if k > 0:
-            v += 0.5 * (f + fp) / mm * DT
+            np.add(f, fp, out=tmp)
+            tmp *= cv
+            v += tmp
         fp[:] = f
-        x += v * DT + 0.5 * f / mm * DT * DT
+        np.multiply(v, DT, out=tmp)
+        x += tmp
+        np.multiply(f, cx, out=tmp)
+        x += tmp
     secs = time.perf_counter() - t0
     return dict(value=n * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=8 * 3 * n,
                 d2h_bytes_per_step=8 * (4 * n + 9), steps=steps, precision="mixed" if precision else "fp64")

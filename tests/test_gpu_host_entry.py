@@ -1,0 +1,83 @@
+"""The host-buffer entry tgap_calculate_gap_soap (the calculate_gap_soap surface) against the
+device-pointer path on the same positions: a rebuild of existing lists runs on the device and its
+pair count comes back with the results; without a rebuild the descriptor forward writes the pair
+geometry itself. Each call must equal a fresh system (host-built lists, separate geometry pass)
+evaluated with tgap_compute: bitwise in FP64 up to the order of FP64 atomic additions, and within
+the FP32 accumulation order in the mixed form. A list that outgrows the arrays reserved for it is
+rebuilt on the host and the call repeated, with the same results."""
+import numpy as np
+import pytest
+
+import helpers
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def ctx(tg):
+    import torch
+    assert torch.cuda.is_available()
+    c = tg.Context(0)
+    yield c
+    c.close()
+
+
+def _fresh(ctx, tg, x, box, sp, model, precision):
+    """Energies and forces of a new system at x (lists built on the host) via tgap_compute."""
+    import torch
+    system = tg.System(ctx, [(x, box, sp)], 3.7 + 0.3)
+    n = len(x)
+    e = torch.zeros(n, dtype=torch.float64, device="cuda")
+    f = torch.zeros(3 * n, dtype=torch.float64, device="cuda")
+    v = torch.zeros(9, dtype=torch.float64, device="cuda")
+    torch.cuda.synchronize()
+    system.compute_device([model], precision, e.data_ptr(), f.data_ptr(), v.data_ptr())
+    ctx.synchronize()
+    out = e.cpu().numpy(), f.cpu().numpy().reshape(n, 3), system.n_pairs
+    system.close()
+    return out
+
+
+@pytest.mark.parametrize("precision_name", ["TGAP_FP64", "TGAP_MIXED"])
+def test_host_entry_steps_match_fresh_systems(ctx, tg, synth, precision_name):
+    precision = getattr(tg, precision_name)
+    hyp, m = helpers.carbon_model(synth, 200, seed=17)
+    pos, box, sp, _ = synth.random_packing(300, 2.5, 1.2, seed=18)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    rng = np.random.default_rng(19)
+    x = pos.copy()
+    te, tf = (1e-12, 1e-10) if precision == tg.TGAP_FP64 else (1e-7, 1e-6)
+    for k in range(6):
+        x = x + rng.normal(scale=0.05, size=x.shape)
+        rebuild = k % 2 == 0
+        e, f, _ = system.calculate_gap_soap([model], precision, x, rebuild=rebuild)
+        e_r, f_r, n_r = _fresh(ctx, tg, x, box, sp, model, precision)
+        assert np.max(np.abs(e - e_r)) <= te * max(1.0, np.abs(e_r).max()), k
+        assert np.max(np.abs(f - f_r)) <= tf * max(1.0, np.abs(f_r).max()), k
+        if rebuild:
+            assert system.n_pairs == n_r, k
+    system.close()
+    model.close()
+
+
+def test_host_entry_repeats_a_call_whose_lists_outgrew_their_arrays(ctx, tg, synth):
+    """Atoms drawn halfway towards the box centre: the device-side rebuild finds more pairs than the
+    arrays hold, so the call rebuilds on the host and repeats; the results equal a fresh system's and
+    no device check is left behind."""
+    hyp, m = helpers.carbon_model(synth, 200, seed=17)
+    pos, box, sp, _ = synth.random_packing(128, 2.5, 1.2, seed=20)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    n0 = system.n_pairs
+    c = 0.5 * np.asarray(box).sum(axis=0)
+    x = c + 0.5 * (pos - c)
+    e, f, _ = system.calculate_gap_soap([model], tg.TGAP_FP64, x, rebuild=True)
+    e_r, f_r, n_r = _fresh(ctx, tg, x, box, sp, model, tg.TGAP_FP64)
+    assert n_r > 1.25 * n0 + 256  # beyond the reserved arrays
+    assert system.n_pairs == n_r
+    assert np.max(np.abs(e - e_r)) <= 1e-12 * max(1.0, np.abs(e_r).max())
+    assert np.max(np.abs(f - f_r)) <= 1e-10 * max(1.0, np.abs(f_r).max())
+    ctx.synchronize()  # no device check pending
+    system.close()
+    model.close()

@@ -1298,35 +1298,96 @@ extern "C" int tgap_autotune_set(tgap_context *ctx, const char *key, int value)
     return TGAP_OK;
 }
 
+// The descriptor forward can write each step's pair geometry itself (compute_model's geom) on a
+// pure-replica system whose every site belongs to some model's site set.
+static bool can_fuse_geometry(const tgap_system *s, int n_models, const tgap_model *const *models)
+{
+    if (!s->nb.replicated) return false;
+    std::vector<int> covered;
+    for (int i = 0; i < n_models; ++i) {
+        if (models[i]->central_species == 0) return true;
+        covered.push_back(models[i]->central_species);
+    }
+    for (int sp : s->host_species)
+        if (std::find(covered.begin(), covered.end(), sp) == covered.end()) return false;
+    return true;
+}
+
+// One call of the host-buffer entry. A rebuild of existing lists runs on the device (no host
+// synchronization before the forces); the pair count comes back with the results, and a list that
+// outgrew the reserved arrays is rebuilt on the host and the call repeated (device_rebuild false).
+// Without a rebuild the forward writes the pair geometry itself where it can.
+static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
+                              int precision, const double *positions, int rebuild, bool device_rebuild,
+                              double *energies, double *forces, double *virial)
+{
+    const int N = s->nb.n_atoms, nst = s->nb.n_structures;
+    const size_t out_bytes = sizeof(double) * ((size_t)N + 3 * (size_t)N + 9 * (size_t)nst);
+    if (ctx->pinned[0].ensure(sizeof(double) * 3 * (size_t)N) || ctx->pinned[1].ensure(out_bytes + 16) ||
+        s->scratch_forces.ensure(out_bytes) || s->queue.ensure(sizeof(int) * kQueueInts))
+        return set_error(ctx, TGAP_ERR_NOMEM, "staging buffers");
+    if (n_models <= 0 || !models || 2 * n_models > kQueueInts)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
+    for (int i = 0; i < n_models; ++i)
+        if (!models[i]) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: null model");
+    if (positions) {
+        std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
+        TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
+                                       cudaMemcpyHostToDevice, ctx->stream));
+    }
+    const bool on_device = rebuild && device_rebuild && s->nb.list.ptr && s->nb.n_pairs > 0;
+    bool geom = false;
+    if (on_device) {
+        CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
+        CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
+        CHECK_RC(neighbors_refresh(ctx, &s->nb));
+    } else if (rebuild || !can_fuse_geometry(s, n_models, models)) {
+        CHECK_RC(tgap_system_update(s, rebuild));
+    } else {
+        geom = true;
+    }
+    double *d_e = s->scratch_forces.as<double>();
+    double *d_f = d_e + N;
+    double *d_v = d_f + 3 * (size_t)N;
+    const int do_forces = forces != nullptr || virial != nullptr;
+    // energies, forces and virial are one buffer: one clear, and one for the site counters
+    TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, out_bytes, ctx->stream));
+    TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
+    CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
+                            s->queue.as<int>()));
+    unsigned char *h = ctx->pinned[1].as<unsigned char>();
+    TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+    if (on_device)  // the rebuild's unclamped pair count
+        TGAP_CUDA(ctx, cudaMemcpyAsync(h + out_bytes, s->nb.counts.as<int64_t>() + N, sizeof(int64_t),
+                                       cudaMemcpyDeviceToHost, ctx->stream));
+    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+    if (on_device) {
+        int64_t total = 0;
+        std::memcpy(&total, h + out_bytes, sizeof(int64_t));
+        s->nb.n_pairs = total;
+        s->nb.count_on_device = false;
+        if (total > s->nb.pair_capacity()) {
+            // the device lists were clamped (and this call's results cut short): rebuild on the
+            // host and repeat
+            return calculate_gap_soap(ctx, s, n_models, models, precision, nullptr, 1, false, energies, forces,
+                                      virial);
+        }
+    }
+    const double *hv = reinterpret_cast<const double *>(h);
+    std::memcpy(energies, hv, sizeof(double) * N);
+    if (forces) std::memcpy(forces, hv + N, sizeof(double) * 3 * (size_t)N);
+    if (virial) std::memcpy(virial, hv + 4 * (size_t)N, sizeof(double) * 9 * (size_t)nst);
+    return TGAP_OK;
+}
+
 extern "C" int tgap_calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                                        int precision, const double *positions, int rebuild, double *energies,
                                        double *forces, double *virial)
 {
     CHECK_RC(activate(ctx));
     if (!s || !energies) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad arguments");
-    const int N = s->nb.n_atoms, nst = s->nb.n_structures;
-    const size_t out_bytes = sizeof(double) * ((size_t)N + 3 * (size_t)N + 9 * (size_t)nst);
-    if (ctx->pinned[0].ensure(sizeof(double) * 3 * (size_t)N) || ctx->pinned[1].ensure(out_bytes) ||
-        s->scratch_forces.ensure(out_bytes))
-        return set_error(ctx, TGAP_ERR_NOMEM, "staging buffers");
-    if (positions) {
-        std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
-        TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
-                                       cudaMemcpyHostToDevice, ctx->stream));
-    }
-    CHECK_RC(tgap_system_update(s, rebuild));
-    double *d_e = s->scratch_forces.as<double>();
-    double *d_f = d_e + N;
-    double *d_v = d_f + 3 * (size_t)N;
-    const int do_forces = forces != nullptr || virial != nullptr;
-    CHECK_RC(tgap_compute(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v));
-    TGAP_CUDA(ctx, cudaMemcpyAsync(ctx->pinned[1].ptr, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
-    const double *h = ctx->pinned[1].as<double>();
-    std::memcpy(energies, h, sizeof(double) * N);
-    if (forces) std::memcpy(forces, h + N, sizeof(double) * 3 * (size_t)N);
-    if (virial) std::memcpy(virial, h + 4 * (size_t)N, sizeof(double) * 9 * (size_t)nst);
-    return TGAP_OK;
+    return calculate_gap_soap(ctx, s, n_models, models, precision, positions, rebuild, true, energies, forces,
+                              virial);
 }
 
 extern "C" int tgap_descriptors(tgap_context *ctx, tgap_system *s, const tgap_model *m, int precision,
@@ -1529,15 +1590,7 @@ static int terms_add(tgap_context *ctx, tgap_system *s, tgap_terms *t, int do_fo
 
 static bool md_can_fuse_geometry(const tgap_md *md)
 {
-    if (!md->sys->nb.replicated || md->terms) return false;
-    std::vector<int> covered;
-    for (const tgap_model *m : md->models) {
-        if (m->central_species == 0) return true;
-        covered.push_back(m->central_species);
-    }
-    for (int sp : md->sys->host_species)
-        if (std::find(covered.begin(), covered.end(), sp) == covered.end()) return false;
-    return true;
+    return !md->terms && can_fuse_geometry(md->sys, (int)md->models.size(), md->models.data());
 }
 
 static int md_eval(tgap_md *md)
@@ -1560,7 +1613,7 @@ static int md_step_body(tgap_md *md, bool rebuild = false)
     tgap_context *ctx = md->ctx;
     if (rebuild) {
         CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
-        CHECK_RC(neighbors_rebuild_lists_device(ctx, &md->sys->nb));
+        CHECK_RC(neighbors_rebuild_lists_device(ctx, &md->sys->nb, true));
     }
     if (rebuild || !md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     CHECK_RC(md_eval(md));

@@ -257,11 +257,12 @@ __global__ void k_nneigh_from_counts(int n, const int64_t *cnt, int *n_neigh)
 // that the descriptor kernels read at start[i] included, stays inside the arrays; the tail sites
 // get no pairs and the fill records the site it cut. The decision is taken once, from start[n],
 // before any offset changes; thread i reading start[i + 1] while another thread clamps it gets
-// the same min(., cap - 1) either way.
-__global__ void k_fit_pairs(int n, int64_t *start, int *n_neigh, int64_t cap, int *check)
+// the same min(., cap - 1) either way. The unclamped total is kept in *total.
+__global__ void k_fit_pairs(int n, int64_t *start, int *n_neigh, int64_t cap, int *check, int64_t *total)
 {
     __shared__ int over;
     if (threadIdx.x == 0) {
+        *total = start[n];
         over = start[n] > cap;
         if (over) check_fail(check, kCheckPairCapacity, n, (long long)start[n]);
     }
@@ -406,8 +407,9 @@ static int rebuild_count(tgap_context *ctx, NeighborBatch *nb)
     return scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
 }
 
-// The filling half: each warp writes its site's pairs inside [start[g], start[g + 1]).
-static int rebuild_fill(tgap_context *ctx, NeighborBatch *nb)
+// The filling half: each warp writes its site's pairs inside [start[g], start[g + 1]) (a site cut
+// short is recorded in check when given).
+static int rebuild_fill(tgap_context *ctx, NeighborBatch *nb, int *check)
 {
     const int n = nb->n_atoms;
     const int T = 128;
@@ -415,7 +417,7 @@ static int rebuild_fill(tgap_context *ctx, NeighborBatch *nb)
     k_site_pairs<true><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(),
                                                      nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
                                                      nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(),
-                                                     nb->list.as<int>(), ctx->d_check);
+                                                     nb->list.as<int>(), check);
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }
@@ -442,21 +444,22 @@ int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capaci
     nb->count_on_device = false;
     k_nneigh_from_counts<<<grid, T, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->n_neigh.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
-    return rebuild_fill(ctx, nb);
+    return rebuild_fill(ctx, nb, ctx->d_check);
 }
 
-int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb)
+int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb, bool report)
 {
     const int n = nb->n_atoms;
     if (n <= 0) return TGAP_OK;
     if (!nb->list.ptr) return set_error(ctx, TGAP_ERR_ARGUMENT, "device-side list rebuild before any list was built");
     StageScope sc(ctx, "neighbors_rebuild");
     if (const int rc = rebuild_count(ctx, nb)) return rc;
+    int *check = report ? ctx->d_check : nullptr;
     k_fit_pairs<<<1, 1024, 0, ctx->stream>>>(n, nb->start.as<int64_t>(), nb->n_neigh.as<int>(), nb->pair_capacity(),
-                                             ctx->d_check);
+                                             check, nb->counts.as<int64_t>() + n);
     TGAP_LAUNCH_CHECK(ctx);
     nb->count_on_device = true;
-    return rebuild_fill(ctx, nb);
+    return rebuild_fill(ctx, nb, check);
 }
 
 int neighbors_sync_count(tgap_context *ctx, NeighborBatch *nb)

@@ -79,10 +79,11 @@ int neighbors_build(tgap_context *ctx, NeighborBatch *nb, int rebuild, int64_t c
 int neighbors_rebuild_lists(tgap_context *ctx, NeighborBatch *nb, int64_t capacity, int64_t *n_pairs_out);
 // The same lists rebuilt without a host synchronization (capturable in a graph), inside the pair
 // arrays already reserved (pair_capacity(), a quarter above the count they were sized for): the
-// offsets are clamped below that capacity, and a longer list is recorded in the device check word
-// (kCheckPairCapacity, reported as TGAP_ERR_CAPACITY at the next check). n_pairs is then read
-// back lazily by neighbors_sync_count.
-int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb);
+// offsets are clamped below that capacity, and with report a longer list is recorded in the device
+// check word (kCheckPairCapacity, reported as TGAP_ERR_CAPACITY at the next check); without it the
+// caller compares the count itself: the unclamped total is left in counts[n_atoms]. n_pairs (the
+// pairs the lists hold) is then read back lazily by neighbors_sync_count.
+int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb, bool report);
 int neighbors_sync_count(tgap_context *ctx, NeighborBatch *nb);
 // from_positions: form supercell positions from the primitive ones inside the kernel
 int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, bool from_positions);
