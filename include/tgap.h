@@ -444,7 +444,9 @@ int tgap_mc_screen_log(tgap_mc *mc, int64_t n, double *de_screen, unsigned char 
  * pay for its own evaluation: delayed acceptance saves only the exact energies of the proposals it
  * rejects), the screen is switched off for the rest of the MC object's life (or until
  * tgap_mc_set_screen installs one again). Proposals still take deviate pairs; plain moves use the
- * first. Defaults: 2048, 0.1, 0.002, 0.99. */
+ * first. Defaults: 256, 0.1, 0.002, 0.99 (at a pass rate of 0.998, 256 proposals show at most two
+ * rejections with high probability, so a screen that cannot pay for itself is off within a few
+ * hundred proposals; a useful screen passes far fewer than 99 %). */
 int tgap_mc_screen_fallback(tgap_mc *mc, int64_t window, double min_confirm, double min_pass, double max_pass);
 /* Speculative batch of plain GAP MC (no counterpart in the reference, which judges proposals one
  * at a time): `slots` consecutive proposals (1..16; default 12 mixed, 4 FP64) are evaluated side by side from

@@ -552,7 +552,7 @@ class MC:
         check(self.ctx._L.tgap_mc_screen_log(self.h, n, ptr(des), ptr(st)), self.ctx.h, "tgap_mc_screen_log")
         return des, st
 
-    def screen_fallback(self, window=2048, min_confirm=0.1, min_pass=0.002, max_pass=0.99):
+    def screen_fallback(self, window=256, min_confirm=0.1, min_pass=0.002, max_pass=0.99):
         """Sets when the driver gives up on the screen and continues as plain GAP MC: over each
         window of screen-judged proposals, a pass rate below min_pass or above max_pass (the screen
         settles too few proposals to pay for itself) or an exact-stage confirmation rate below

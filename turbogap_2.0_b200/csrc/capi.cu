@@ -1998,7 +1998,7 @@ struct tgap_mc {
     // learned screen (delayed acceptance); screened: installed (proposals carry deviate pairs),
     // screen_active: used by the step (off after a fallback to plain GAP MC)
     bool screened = false, screen_active = false;
-    int64_t fb_window = 2048;                     // screened proposals per fallback check
+    int64_t fb_window = 256;                      // screened proposals per fallback check
     double fb_min_confirm = 0.1, fb_min_pass = 0.002, fb_max_pass = 0.99;
     long long fb_prop0 = 0, fb_pass0 = 0, fb_conf0 = 0;  // counters at the start of the window
     int64_t fallbacks = 0;
