@@ -444,22 +444,15 @@ def _e2e(tg, ctx, system, model, masses, vel, pos0, precision, steps):
     for k in range(3):  # warm-up
         force(k)
     x[:] = pos0
-    # velocity Verlet on the host with preallocated arrays (md_utils.f90:486-532)
-    cv = 0.5 * DT / mm
-    cx = 0.5 * DT * DT / mm
-    tmp = np.empty_like(f)
+    v = np.ascontiguousarray(v)
+    m_col = np.ascontiguousarray(mm[:, 0])
     t0 = time.perf_counter()
     for k in range(steps):
         force(k)
-        if k > 0:
-            np.add(f, fp, out=tmp)
-            tmp *= cv
-            v += tmp
-        fp[:] = f
-        np.multiply(v, DT, out=tmp)
-        x += tmp
-        np.multiply(f, cx, out=tmp)
-        x += tmp
+        # velocity Verlet on the host (md_utils.f90:486-532), as the reference integrates
+        native.check(L.tgap_velocity_verlet_host(n, native.ptr(x), None, native.ptr(v), native.ptr(f),
+                                                 native.ptr(fp), native.ptr(m_col), DT, DT, int(k == 0)),
+                     ctx.h, "tgap_velocity_verlet_host")
     secs = time.perf_counter() - t0
     return dict(value=n * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=8 * 3 * n,
                 d2h_bytes_per_step=8 * (4 * n + 9), steps=steps, precision="mixed" if precision else "fp64")

@@ -266,6 +266,12 @@ int tgap_system_set_site_range(tgap_system *system, int beg, int end);
 int tgap_velocity_verlet(tgap_context *ctx, int n_sites, double *d_positions, double *d_positions_prev,
                          double *d_velocities, const double *d_forces, double *d_forces_prev,
                          const double *d_masses, double dt, double dt_prev, int first_step);
+/* The same update on host arrays (the arithmetic of tgap_velocity_verlet, one pass over the atoms),
+ * for host-side MD loops around tgap_calculate_gap_soap, where the reference integrates on the host.
+ * positions_prev may be NULL. Non-finite forces return TGAP_ERR_NUMERIC before any array changes. */
+int tgap_velocity_verlet_host(int n_sites, double *positions, double *positions_prev, double *velocities,
+                              const double *forces, double *forces_prev, const double *masses, double dt,
+                              double dt_prev, int first_step);
 
 /* Energies (n_atoms), forces (3 x n_atoms) and virial (9 per structure), device pointers,
  * summed over models, plus each atom's e0 (tgap_system_set_e0; 0 when never set). Overwrites the

@@ -58,6 +58,35 @@ def test_number_of_unit_cells_matches_oracle(tg, orc):
         assert list(idx) == list(orc.number_of_unit_cells(box[0], box[1], box[2], rc))
 
 
+def test_host_velocity_verlet_matches_oracle(tg, orc):
+    """tgap_velocity_verlet_host (host arrays) against the oracle's velocity_verlet
+    (md_utils.f90:486-532) over a first step and two later ones, and its refusal of non-finite
+    forces before touching any array."""
+    from turbogap_b200 import native
+    L = native.lib()
+    rng = np.random.default_rng(3)
+    n = 50
+    m = rng.uniform(1.0, 16.0, n) * 103.6426965268
+    x = rng.normal(size=(n, 3)) * 5.0
+    v = rng.normal(size=(n, 3)) * 0.01
+    xo, vo = x.copy(), v.copy()
+    fp, fpo, xpo = np.zeros((n, 3)), np.zeros((n, 3)), np.zeros((n, 3))
+    xp = np.zeros((n, 3))
+    for k in range(3):
+        f = rng.normal(size=(n, 3))
+        assert L.tgap_velocity_verlet_host(n, native.ptr(x), native.ptr(xp), native.ptr(v), native.ptr(f),
+                                           native.ptr(fp), native.ptr(m), 0.5, 0.5, int(k == 0)) == 0
+        orc.velocity_verlet(xo, xpo, vo, f, fpo, m, 0.5, 0.5, k == 0)
+        assert np.max(np.abs(x - xo)) < 1e-13
+        assert np.max(np.abs(v - vo)) < 1e-15
+        assert np.array_equal(fp, fpo) and np.array_equal(xp, xpo)
+    f[7, 1] = np.nan
+    x0 = x.copy()
+    assert L.tgap_velocity_verlet_host(n, native.ptr(x), None, native.ptr(v), native.ptr(f), native.ptr(fp),
+                                       native.ptr(m), 0.5, 0.5, 0) == 8  # TGAP_ERR_NUMERIC
+    assert np.array_equal(x, x0)
+
+
 def test_assign_species(tg):
     out = tg.api.assign_species(["Si", "O"], ["O", "Si", "Si", "C", "O"])
     assert list(out) == [2, 1, 1, 0, 2]

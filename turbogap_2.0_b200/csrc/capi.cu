@@ -29,6 +29,10 @@ namespace tgap {
 
 std::atomic<uint64_t> g_alloc_epoch{0};
 
+// Captured graphs (MD steps, host-buffer calls) are re-captured after any change of what they baked
+// in: a buffer that moved, e0, the site range, a launch choice of the autotuner.
+static void graphs_stale() { g_alloc_epoch.fetch_add(1, std::memory_order_relaxed); }
+
 int DevBuf::ensure(size_t n)
 {
     if (n <= bytes && ptr) return 0;
@@ -775,6 +779,17 @@ struct tgap_system {
     DevBuf d_e0;
     // sites evaluated as descriptor centres: atoms [range_beg, range_end) (split_tasks of one rank)
     int range_beg = 0, range_end = -1;
+    // device work of the host-buffer entry as CUDA graphs, one per call configuration
+    struct CallGraph {
+        std::vector<const tgap_model *> models;
+        int precision = 0, flags = 0;
+        bool seen = false;  // ran eagerly once (buffers sized): the next call captures
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        uint64_t epoch = 0;
+        int64_t kernels = 0;
+    };
+    std::vector<CallGraph> call_graphs;
 };
 
 extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
@@ -851,6 +866,10 @@ extern "C" int tgap_system_destroy(tgap_system *s)
     cudaSetDevice(s->ctx->device);
     s->nb.release_all();
     for (auto &ss : s->site_sets) ss.sites.release();
+    for (auto &cg : s->call_graphs) {
+        if (cg.exec) cudaGraphExecDestroy(cg.exec);
+        if (cg.graph) cudaGraphDestroy(cg.graph);
+    }
     DevBuf *bufs[] = {&s->c, &s->q, &s->norm, &s->q_hi, &s->q_lo, &s->e_rows, &s->gw.e_part, &s->gw.G,
                       &s->gw.g, &s->gw.G_hi, &s->gw.G_lo, &s->scratch_forces, &s->d_species, &s->queue,
                       &s->d_e0};
@@ -903,6 +922,7 @@ extern "C" int tgap_system_set_positions(tgap_system *s, const double *positions
 // collect_calculation (mpi_utils.f90:515-545) sums the ranks.
 extern "C" int tgap_system_set_site_range(tgap_system *s, int beg, int end)
 {
+    graphs_stale();
     if (!s) return TGAP_ERR_ARGUMENT;
     const int N = (int)s->host_species.size();
     if (end < 0) end = N;
@@ -930,10 +950,34 @@ extern "C" int tgap_velocity_verlet(tgap_context *ctx, int n_sites, double *d_po
                            d_masses, dt, dt_prev, first_step);
 }
 
+extern "C" int tgap_velocity_verlet_host(int n_sites, double *positions, double *positions_prev, double *velocities,
+                                         const double *forces, double *forces_prev, const double *masses, double dt,
+                                         double dt_prev, int first_step)
+{
+    if (n_sites < 0 || (n_sites > 0 && (!positions || !velocities || !forces || !forces_prev || !masses)))
+        return TGAP_ERR_ARGUMENT;
+    const size_t n3 = 3 * (size_t)n_sites;
+    for (size_t g = 0; g < n3; ++g)
+        if (!std::isfinite(forces[g])) return TGAP_ERR_NUMERIC;
+    for (size_t g = 0; g < n3; ++g) {
+        const double m = masses[g / 3];
+        const double fg = forces[g];
+        double v = velocities[g];
+        if (!first_step) v = v + 0.5 * (fg + forces_prev[g]) / m * dt_prev;
+        velocities[g] = v;
+        const double x = positions[g];
+        if (positions_prev) positions_prev[g] = x;
+        forces_prev[g] = fg;
+        positions[g] = x + v * dt + 0.5 * fg / m * (dt * dt);
+    }
+    return TGAP_OK;
+}
+
 // calculate_e0 (calculate_gap_soap.f90:135-169): every atom gets the e0 of its species (the input
 // file's e0 keyword, read_files.f90:380-385); atoms of no listed species keep 0.
 extern "C" int tgap_system_set_e0(tgap_system *s, int n_species, const double *e0)
 {
+    graphs_stale();
     if (!s || n_species < 0 || (n_species > 0 && !e0)) return TGAP_ERR_ARGUMENT;
     tgap_context *ctx = s->ctx;
     CHECK_RC(activate(ctx));
@@ -1196,6 +1240,7 @@ static double stage_mean_ms(tgap_context *ctx, const std::string &stage)
 extern "C" int tgap_autotune(tgap_context *ctx, tgap_system *s, int n_models, tgap_model *const *models,
                              int precision, int reps)
 {
+    graphs_stale();
     CHECK_RC(activate(ctx));
     if (!s || n_models <= 0 || !models || reps < 1) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_autotune: bad arguments");
     const int N = s->nb.n_atoms;
@@ -1274,6 +1319,7 @@ extern "C" int tgap_autotune_report(tgap_context *ctx, char *buf, int64_t cap, i
 
 extern "C" int tgap_autotune_clear(tgap_context *ctx)
 {
+    graphs_stale();
     if (!ctx) return TGAP_ERR_ARGUMENT;
     ctx->tune.clear();
     ctx->tune_suffix.clear();
@@ -1283,6 +1329,7 @@ extern "C" int tgap_autotune_clear(tgap_context *ctx)
 
 extern "C" int tgap_autotune_set(tgap_context *ctx, const char *key, int value)
 {
+    graphs_stale();
     if (!ctx || !key || !key[0]) return TGAP_ERR_ARGUMENT;
     if (key[0] == '*') {
         const std::string suffix(key + 1);
@@ -1330,36 +1377,91 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
     for (int i = 0; i < n_models; ++i)
         if (!models[i]) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: null model");
-    if (positions) {
-        std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
-        TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
-                                       cudaMemcpyHostToDevice, ctx->stream));
-    }
+    if (positions) std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
     const bool on_device = rebuild && device_rebuild && s->nb.list.ptr && s->nb.n_pairs > 0;
-    bool geom = false;
-    if (on_device) {
-        CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
-        CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
-        CHECK_RC(neighbors_refresh(ctx, &s->nb));
-    } else if (rebuild || !can_fuse_geometry(s, n_models, models)) {
-        CHECK_RC(tgap_system_update(s, rebuild));
-    } else {
-        geom = true;
-    }
-    double *d_e = s->scratch_forces.as<double>();
-    double *d_f = d_e + N;
-    double *d_v = d_f + 3 * (size_t)N;
+    const bool host_rebuild = rebuild && !on_device;
+    const bool geom = !rebuild && can_fuse_geometry(s, n_models, models);
     const int do_forces = forces != nullptr || virial != nullptr;
-    // energies, forces and virial are one buffer: one clear, and one for the site counters
-    TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, out_bytes, ctx->stream));
-    TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
-    CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
-                            s->queue.as<int>()));
     unsigned char *h = ctx->pinned[1].as<unsigned char>();
-    TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
-    if (on_device)  // the rebuild's unclamped pair count
-        TGAP_CUDA(ctx, cudaMemcpyAsync(h + out_bytes, s->nb.counts.as<int64_t>() + N, sizeof(int64_t),
-                                       cudaMemcpyDeviceToHost, ctx->stream));
+    // the device work of the call, stream-ordered; with a host rebuild (a host synchronization for
+    // the pair count) it cannot be captured
+    auto device_work = [&]() -> int {
+        if (positions)
+            TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
+                                           cudaMemcpyHostToDevice, ctx->stream));
+        if (on_device) {
+            CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
+            CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
+            CHECK_RC(neighbors_refresh(ctx, &s->nb));
+        } else if (!geom) {
+            CHECK_RC(tgap_system_update(s, host_rebuild ? 1 : 0));
+        }
+        double *d_e = s->scratch_forces.as<double>();
+        double *d_f = d_e + N;
+        double *d_v = d_f + 3 * (size_t)N;
+        // energies, forces and virial are one buffer: one clear, and one for the site counters
+        TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, out_bytes, ctx->stream));
+        TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
+        CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
+                                s->queue.as<int>()));
+        TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        if (on_device)  // the rebuild's unclamped pair count
+            TGAP_CUDA(ctx, cudaMemcpyAsync(h + out_bytes, s->nb.counts.as<int64_t>() + N, sizeof(int64_t),
+                                           cudaMemcpyDeviceToHost, ctx->stream));
+        return TGAP_OK;
+    };
+    // A configuration (models, precision, rebuild on the device or not, geometry fused or not,
+    // positions given, forces) runs eagerly the first time, which sizes every buffer, and from the
+    // second time as one graph launch. Stage timing and per-launch checks keep the eager path.
+    if (host_rebuild || ctx->timing || ctx->sync_check) {
+        CHECK_RC(device_work());
+    } else {
+        const int flags = (on_device ? 1 : 0) | (geom ? 2 : 0) | (positions ? 4 : 0) | (do_forces ? 8 : 0);
+        tgap_system::CallGraph *cg = nullptr;
+        for (auto &c : s->call_graphs)
+            if (c.precision == precision && c.flags == flags && (int)c.models.size() == n_models &&
+                std::equal(c.models.begin(), c.models.end(), models))
+                cg = &c;
+        if (!cg) {
+            s->call_graphs.emplace_back();
+            cg = &s->call_graphs.back();
+            cg->models.assign(models, models + n_models);
+            cg->precision = precision;
+            cg->flags = flags;
+        }
+        const uint64_t e0 = g_alloc_epoch.load(std::memory_order_relaxed);
+        if (cg->exec && cg->epoch != e0) {  // a buffer moved since the capture
+            cudaGraphExecDestroy(cg->exec);
+            cudaGraphDestroy(cg->graph);
+            cg->exec = nullptr;
+            cg->graph = nullptr;
+        }
+        if (!cg->exec && cg->seen) {
+            TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
+            const int64_t launches = ctx->launches;
+            int rc = device_work();
+            cudaGraph_t g = nullptr;
+            const cudaError_t ce = cudaStreamEndCapture(ctx->stream, &g);
+            cg->kernels = ctx->launches - launches;
+            ctx->launches = launches;
+            if (rc || ce != cudaSuccess || g_alloc_epoch.load(std::memory_order_relaxed) != e0) {
+                if (g) cudaGraphDestroy(g);
+                if (rc) return rc;
+                if (ce != cudaSuccess) return cuda_check(ctx, ce, "call graph capture");
+            } else {
+                cg->graph = g;
+                TGAP_CUDA(ctx, cudaGraphInstantiate(&cg->exec, g, 0));
+                cg->epoch = e0;
+            }
+        }
+        if (cg->exec) {
+            TGAP_CUDA(ctx, cudaGraphLaunch(cg->exec, ctx->stream));
+            ctx->launches += cg->kernels;
+        } else {
+            CHECK_RC(device_work());
+            cg->seen = true;
+        }
+    }
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     if (on_device) {
         int64_t total = 0;

@@ -158,6 +158,18 @@ module tgap_iface
          integer(c_int), value :: n_sites, first_step
          real(c_double), value :: dt, dt_prev
       end function
+
+      ! the same update on host arrays, for a host MD loop around tgap_calculate_gap_soap
+      integer(c_int) function tgap_velocity_verlet_host(n_sites, positions, positions_prev, velocities, &
+                                                        forces, forces_prev, masses, dt, dt_prev, first_step) &
+         bind(C, name="tgap_velocity_verlet_host")
+         import :: c_int, c_double, c_ptr
+         integer(c_int), value :: n_sites, first_step
+         real(c_double), intent(inout) :: positions(3, *), velocities(3, *), forces_prev(3, *)
+         type(c_ptr), value :: positions_prev
+         real(c_double), intent(in) :: forces(3, *), masses(*)
+         real(c_double), value :: dt, dt_prev
+      end function
    end interface
 
 contains
