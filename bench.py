@@ -435,25 +435,31 @@ def _e2e(tg, ctx, system, model, masses, vel, pos0, precision, steps):
     fp = np.zeros((n, 3))
     vir = np.zeros(9)
     arr = (C.c_void_p * 1)(model.h.value)
+    v = np.ascontiguousarray(v)
+    m_col = np.ascontiguousarray(mm[:, 0])
+    # the arrays live for the whole run: their addresses are taken once, and they are registered
+    # with the context as pinned host memory, which the call then reads and writes directly
+    px, pe, pf, pv, pfp, pm, pvir = (native.ptr(a) for a in (x, e, f, v, fp, m_col, vir))
+    for a in (x, e, f, vir):
+        native.check(L.tgap_host_register(ctx.h, native.ptr(a), a.nbytes), ctx.h, "tgap_host_register")
 
     def force(k):
-        st = L.tgap_calculate_gap_soap(ctx.h, system.h, 1, arr, int(precision), native.ptr(x), int(k % REBUILD == 0),
-                                       native.ptr(e), native.ptr(f), native.ptr(vir))
+        st = L.tgap_calculate_gap_soap(ctx.h, system.h, 1, arr, int(precision), px, int(k % REBUILD == 0), pe, pf,
+                                       pvir)
         native.check(st, ctx.h, "tgap_calculate_gap_soap")
 
     for k in range(3):  # warm-up
         force(k)
     x[:] = pos0
-    v = np.ascontiguousarray(v)
-    m_col = np.ascontiguousarray(mm[:, 0])
     t0 = time.perf_counter()
     for k in range(steps):
         force(k)
         # velocity Verlet on the host (md_utils.f90:486-532), as the reference integrates
-        native.check(L.tgap_velocity_verlet_host(n, native.ptr(x), None, native.ptr(v), native.ptr(f),
-                                                 native.ptr(fp), native.ptr(m_col), DT, DT, int(k == 0)),
-                     ctx.h, "tgap_velocity_verlet_host")
+        native.check(L.tgap_velocity_verlet_host(n, px, None, pv, pf, pfp, pm, DT, DT, int(k == 0)), ctx.h,
+                     "tgap_velocity_verlet_host")
     secs = time.perf_counter() - t0
+    for a in (x, e, f, vir):
+        native.check(L.tgap_host_unregister(ctx.h, native.ptr(a)), ctx.h, "tgap_host_unregister")
     return dict(value=n * steps / secs, unit="atom-steps/s", h2d_bytes_per_step=8 * 3 * n,
                 d2h_bytes_per_step=8 * (4 * n + 9), steps=steps, precision="mixed" if precision else "fp64")
 

@@ -54,6 +54,12 @@ typedef struct tgap_context tgap_context;
 
 int tgap_create(int device, tgap_context **ctx);
 int tgap_destroy(tgap_context *ctx);
+/* Page-locks the caller's host memory [ptr, ptr + bytes) (cudaHostRegister) for this context: the
+ * host-buffer entries (tgap_calculate_gap_soap) then copy positions from and results to such arrays
+ * directly instead of through the context's staging buffers. For arrays reused across calls;
+ * unregister before freeing them (unregistering synchronizes the context stream). */
+int tgap_host_register(tgap_context *ctx, void *ptr, size_t bytes);
+int tgap_host_unregister(tgap_context *ctx, void *ptr);
 /* Use an external stream (cudaStream_t) for all later work; NULL restores the own stream. */
 int tgap_set_stream(tgap_context *ctx, void *stream);
 int tgap_synchronize(tgap_context *ctx);
@@ -266,8 +272,9 @@ int tgap_system_set_site_range(tgap_system *system, int beg, int end);
 int tgap_velocity_verlet(tgap_context *ctx, int n_sites, double *d_positions, double *d_positions_prev,
                          double *d_velocities, const double *d_forces, double *d_forces_prev,
                          const double *d_masses, double dt, double dt_prev, int first_step);
-/* The same update on host arrays (the arithmetic of tgap_velocity_verlet, one pass over the atoms),
- * for host-side MD loops around tgap_calculate_gap_soap, where the reference integrates on the host.
+/* The same update on host arrays (one pass over the atoms with one reciprocal mass per atom, so it
+ * agrees with the divided form to an ulp), for host-side MD loops around tgap_calculate_gap_soap,
+ * where the reference integrates on the host.
  * positions_prev may be NULL. Non-finite forces return TGAP_ERR_NUMERIC before any array changes. */
 int tgap_velocity_verlet_host(int n_sites, double *positions, double *positions_prev, double *velocities,
                               const double *forces, double *forces_prev, const double *masses, double dt,

@@ -81,3 +81,42 @@ def test_host_entry_repeats_a_call_whose_lists_outgrew_their_arrays(ctx, tg, syn
     ctx.synchronize()  # no device check pending
     system.close()
     model.close()
+
+
+def test_registered_arrays_give_the_staged_results(ctx, tg, synth):
+    """Positions, energies, forces and virial registered with tgap_host_register are copied to and
+    from directly (in the captured call graphs too); each call equals the same call through the
+    staging buffers to the order of the mixed path's atomic additions."""
+    import ctypes as C
+    from turbogap_b200 import native
+    L = native.lib()
+    hyp, m = helpers.carbon_model(synth, 200, seed=17)
+    pos, box, sp, _ = synth.random_packing(300, 2.5, 1.2, seed=21)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    n = len(pos)
+    arr = (C.c_void_p * 1)(model.h.value)
+    runs = []
+    for registered in (False, True):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+        x, e, f, v = pos.copy(), np.zeros(n), np.zeros((n, 3)), np.zeros(9)
+        if registered:
+            for a in (x, e, f, v):
+                ctx.host_register(a)
+        out = []
+        rng = np.random.default_rng(22)
+        for k in range(6):
+            x += rng.normal(scale=0.03, size=x.shape)
+            st = L.tgap_calculate_gap_soap(ctx.h, system.h, 1, arr, tg.TGAP_MIXED, native.ptr(x), int(k % 2 == 0),
+                                           native.ptr(e), native.ptr(f), native.ptr(v))
+            native.check(st, ctx.h, "calculate")
+            out.append((e.copy(), f.copy(), v.copy()))
+        if registered:
+            for a in (x, e, f, v):
+                ctx.host_unregister(a)
+        runs.append(out)
+        system.close()
+    for (e0, f0, v0), (e1, f1, v1) in zip(*runs):
+        assert np.array_equal(e0, e1) or np.max(np.abs(e0 - e1)) <= 1e-7 * np.abs(e0).max()
+        assert np.max(np.abs(f0 - f1)) <= 1e-6 * max(1.0, np.abs(f0).max())
+        assert np.max(np.abs(v0 - v1)) <= 1e-6 * max(1.0, np.abs(v0).max())
+    model.close()

@@ -66,6 +66,14 @@ class Context:
         work-queue descriptor kernels)."""
         check(self._L.tgap_autotune_set(self.h, key.encode(), int(value)), self.h, "autotune_set")
 
+    def host_register(self, array):
+        """Page-locks a numpy array for this context (tgap_host_register): host-buffer calls then
+        copy to and from it directly. Keep the array alive until host_unregister."""
+        check(self._L.tgap_host_register(self.h, ptr(array), array.nbytes), self.h, "tgap_host_register")
+
+    def host_unregister(self, array):
+        check(self._L.tgap_host_unregister(self.h, ptr(array)), self.h, "tgap_host_unregister")
+
     def autotune_clear(self):
         check(self._L.tgap_autotune_clear(self.h), self.h, "autotune_clear")
 

@@ -234,6 +234,7 @@ extern "C" int tgap_destroy(tgap_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto &b : ctx->scratch) b.release();
     for (auto &b : ctx->pinned) b.release();
+    for (auto &r : ctx->registered) cudaHostUnregister(reinterpret_cast<void *>(r.first));
     for (auto &r : ctx->pending) {
         cudaEventDestroy(r.start);
         cudaEventDestroy(r.stop);
@@ -244,6 +245,38 @@ extern "C" int tgap_destroy(tgap_context *ctx)
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
     return TGAP_OK;
+}
+
+extern "C" int tgap_host_register(tgap_context *ctx, void *ptr, size_t bytes)
+{
+    CHECK_RC(activate(ctx));
+    if (!ptr || bytes == 0) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_host_register: bad arguments");
+    TGAP_CUDA(ctx, cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
+    ctx->registered.emplace_back(reinterpret_cast<uintptr_t>(ptr), bytes);
+    return TGAP_OK;
+}
+
+extern "C" int tgap_host_unregister(tgap_context *ctx, void *ptr)
+{
+    CHECK_RC(activate(ctx));
+    for (size_t i = 0; i < ctx->registered.size(); ++i)
+        if (ctx->registered[i].first == reinterpret_cast<uintptr_t>(ptr)) {
+            TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+            TGAP_CUDA(ctx, cudaHostUnregister(ptr));
+            ctx->registered.erase(ctx->registered.begin() + (long)i);
+            graphs_stale();  // graphs that copy to or from it
+            return TGAP_OK;
+        }
+    return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_host_unregister: not registered");
+}
+
+// [p, p + len) lies inside memory registered with tgap_host_register
+static bool host_registered(const tgap_context *ctx, const void *p, size_t len)
+{
+    const uintptr_t a = reinterpret_cast<uintptr_t>(p);
+    for (const auto &r : ctx->registered)
+        if (a >= r.first && a + len <= r.first + r.second) return true;
+    return false;
 }
 
 extern "C" int tgap_set_stream(tgap_context *ctx, void *stream)
@@ -783,6 +816,7 @@ struct tgap_system {
     struct CallGraph {
         std::vector<const tgap_model *> models;
         int precision = 0, flags = 0;
+        const void *io[4] = {nullptr, nullptr, nullptr, nullptr};
         bool seen = false;  // ran eagerly once (buffers sized): the next call captures
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
@@ -959,16 +993,21 @@ extern "C" int tgap_velocity_verlet_host(int n_sites, double *positions, double 
     const size_t n3 = 3 * (size_t)n_sites;
     for (size_t g = 0; g < n3; ++g)
         if (!std::isfinite(forces[g])) return TGAP_ERR_NUMERIC;
-    for (size_t g = 0; g < n3; ++g) {
-        const double m = masses[g / 3];
-        const double fg = forces[g];
-        double v = velocities[g];
-        if (!first_step) v = v + 0.5 * (fg + forces_prev[g]) / m * dt_prev;
-        velocities[g] = v;
-        const double x = positions[g];
-        if (positions_prev) positions_prev[g] = x;
-        forces_prev[g] = fg;
-        positions[g] = x + v * dt + 0.5 * fg / m * (dt * dt);
+    // one reciprocal mass per atom instead of a division per component (within an ulp of the
+    // divided form)
+    for (int i = 0; i < n_sites; ++i) {
+        const double im = 1.0 / masses[i];
+        const double cv = first_step ? 0.0 : 0.5 * dt_prev * im, cx = 0.5 * (dt * dt) * im;
+        for (int c = 0; c < 3; ++c) {
+            const size_t g = 3 * (size_t)i + c;
+            const double fg = forces[g];
+            const double v = velocities[g] + (fg + forces_prev[g]) * cv;
+            velocities[g] = v;
+            const double x = positions[g];
+            if (positions_prev) positions_prev[g] = x;
+            forces_prev[g] = fg;
+            positions[g] = x + v * dt + fg * cx;
+        }
     }
     return TGAP_OK;
 }
@@ -1377,7 +1416,12 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
     for (int i = 0; i < n_models; ++i)
         if (!models[i]) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: null model");
-    if (positions) std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
+    // registered caller arrays are copied to and from directly, others through the staging buffers
+    const bool direct_in = positions && host_registered(ctx, positions, sizeof(double) * 3 * (size_t)N);
+    const bool direct_out = host_registered(ctx, energies, sizeof(double) * N) &&
+                            (!forces || host_registered(ctx, forces, sizeof(double) * 3 * (size_t)N)) &&
+                            (!virial || host_registered(ctx, virial, sizeof(double) * 9 * (size_t)nst));
+    if (positions && !direct_in) std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
     const bool on_device = rebuild && device_rebuild && s->nb.list.ptr && s->nb.n_pairs > 0;
     const bool host_rebuild = rebuild && !on_device;
     const bool geom = !rebuild && can_fuse_geometry(s, n_models, models);
@@ -1387,8 +1431,8 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     // the pair count) it cannot be captured
     auto device_work = [&]() -> int {
         if (positions)
-            TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, ctx->pinned[0].ptr, sizeof(double) * 3 * (size_t)N,
-                                           cudaMemcpyHostToDevice, ctx->stream));
+            TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, direct_in ? positions : ctx->pinned[0].ptr,
+                                           sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, ctx->stream));
         if (on_device) {
             CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
             CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
@@ -1404,7 +1448,17 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
         CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
                                 s->queue.as<int>()));
-        TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        if (direct_out) {
+            TGAP_CUDA(ctx, cudaMemcpyAsync(energies, d_e, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
+            if (forces)
+                TGAP_CUDA(ctx, cudaMemcpyAsync(forces, d_f, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost,
+                                               ctx->stream));
+            if (virial)
+                TGAP_CUDA(ctx, cudaMemcpyAsync(virial, d_v, sizeof(double) * 9 * (size_t)nst, cudaMemcpyDeviceToHost,
+                                               ctx->stream));
+        } else {
+            TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        }
         if (on_device)  // the rebuild's unclamped pair count
             TGAP_CUDA(ctx, cudaMemcpyAsync(h + out_bytes, s->nb.counts.as<int64_t>() + N, sizeof(int64_t),
                                            cudaMemcpyDeviceToHost, ctx->stream));
@@ -1416,11 +1470,15 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     if (host_rebuild || ctx->timing || ctx->sync_check) {
         CHECK_RC(device_work());
     } else {
-        const int flags = (on_device ? 1 : 0) | (geom ? 2 : 0) | (positions ? 4 : 0) | (do_forces ? 8 : 0);
+        const int flags = (on_device ? 1 : 0) | (geom ? 2 : 0) | (positions ? 4 : 0) | (do_forces ? 8 : 0) |
+                          (direct_in ? 16 : 0) | (direct_out ? 32 : 0);
+        // the caller's arrays are part of a graph that copies to or from them directly
+        const void *io[4] = {direct_in ? positions : nullptr, direct_out ? energies : nullptr,
+                             direct_out ? forces : nullptr, direct_out ? virial : nullptr};
         tgap_system::CallGraph *cg = nullptr;
         for (auto &c : s->call_graphs)
             if (c.precision == precision && c.flags == flags && (int)c.models.size() == n_models &&
-                std::equal(c.models.begin(), c.models.end(), models))
+                std::equal(c.models.begin(), c.models.end(), models) && std::equal(io, io + 4, c.io))
                 cg = &c;
         if (!cg) {
             s->call_graphs.emplace_back();
@@ -1428,6 +1486,7 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
             cg->models.assign(models, models + n_models);
             cg->precision = precision;
             cg->flags = flags;
+            std::copy(io, io + 4, cg->io);
         }
         const uint64_t e0 = g_alloc_epoch.load(std::memory_order_relaxed);
         if (cg->exec && cg->epoch != e0) {  // a buffer moved since the capture
@@ -1475,10 +1534,12 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
                                       virial);
         }
     }
-    const double *hv = reinterpret_cast<const double *>(h);
-    std::memcpy(energies, hv, sizeof(double) * N);
-    if (forces) std::memcpy(forces, hv + N, sizeof(double) * 3 * (size_t)N);
-    if (virial) std::memcpy(virial, hv + 4 * (size_t)N, sizeof(double) * 9 * (size_t)nst);
+    if (!direct_out) {
+        const double *hv = reinterpret_cast<const double *>(h);
+        std::memcpy(energies, hv, sizeof(double) * N);
+        if (forces) std::memcpy(forces, hv + N, sizeof(double) * 3 * (size_t)N);
+        if (virial) std::memcpy(virial, hv + 4 * (size_t)N, sizeof(double) * 9 * (size_t)nst);
+    }
     return TGAP_OK;
 }
 

@@ -71,6 +71,8 @@ struct tgap_context {
     // scratch buffers reused across calls (host-buffer entry points)
     tgap::DevBuf scratch[24];
     tgap::HostBuf pinned[4];
+    // caller arrays page-locked with tgap_host_register: (address, bytes)
+    std::vector<std::pair<uintptr_t, size_t>> registered;
     int *d_flag = nullptr;  // device error flag (bounded waits, overflow)
     int *d_check = nullptr; // device check word: code, index, value, failures (int[4])
     bool sync_check = false;  // TGAP_SYNC_CHECK=1: synchronize and read the check after each launch

@@ -114,6 +114,8 @@ def lib():
         "tgap_system_get_positions": (i32, [vp, vp]),
         "tgap_velocity_verlet": (i32, [vp, i32, vp, vp, vp, vp, vp, vp, dbl, dbl, i32]),
         "tgap_velocity_verlet_host": (i32, [i32, vp, vp, vp, vp, vp, vp, dbl, dbl, i32]),
+        "tgap_host_register": (i32, [vp, vp, C.c_size_t]),
+        "tgap_host_unregister": (i32, [vp, vp]),
         "tgap_compute": (i32, [vp, vp, i32, vp, i32, i32, vp, vp, vp]),
         "tgap_descriptors": (i32, [vp, vp, vp, i32, vp, P(i32)]),
         "tgap_md_create": (i32, [vp, vp, i32, vp, vp, dbl, i32, i32, i32, P(vp)]),
