@@ -36,6 +36,19 @@ module tgap_iface
          type(c_ptr), value :: ctx
       end function
 
+      ! page-lock a host array reused across calls (c_loc of a target array), so the host-buffer
+      ! entries copy to and from it directly
+      integer(c_int) function tgap_host_register(ctx, ptr, bytes) bind(C, name="tgap_host_register")
+         import :: c_int, c_ptr, c_size_t
+         type(c_ptr), value :: ctx, ptr
+         integer(c_size_t), value :: bytes
+      end function
+
+      integer(c_int) function tgap_host_unregister(ctx, ptr) bind(C, name="tgap_host_unregister")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: ctx, ptr
+      end function
+
       type(c_ptr) function tgap_last_error(ctx) bind(C, name="tgap_last_error")
          import :: c_ptr
          type(c_ptr), value :: ctx
