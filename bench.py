@@ -563,17 +563,19 @@ def _mc_screen_leg(tg, torch, ctx, stream, model, n_prop, seed, plain):
     mc.set_screen(w)
     mc.run(atoms[:256], disp[:256], u[:256], logs=False)
     torch.cuda.synchronize()
+    s0 = mc.screen_stats()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    r = mc.run(atoms[256:], disp[256:], u[256:], logs=True)
+    # no per-proposal logs, as in the plain leg; the screen's decisions come from its counters
+    r = mc.run(atoms[256:], disp[256:], u[256:], logs=False)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
-    _, stage = mc.screen_log(n_prop)
     st = mc.state()
     ss = mc.screen_stats()
+    by_screen = (ss["judged"] - s0["judged"]) - (ss["passed"] - s0["passed"])  # rejected at stage 1
     out = dict(moves_per_s=n_prop / (ms * 1e-3), us_per_move=1e3 * ms / n_prop, acceptance=r["accepted"] / n_prop,
-               settled_by_screen=float(np.mean(stage == 1)), exact_evaluations_per_move=float(np.mean(stage == 2)),
+               settled_by_screen=by_screen / n_prop, exact_evaluations_per_move=1.0 - by_screen / n_prop,
                screen_validation_rmse_meV_per_atom=1e3 * rmse, screen_active_at_end=ss["active"],
                fallbacks=ss["fallbacks"], training=dict(
                    snapshots=n_snap, energies=int((~val).sum()), data_s=round(t_data, 1), fit_s=round(t_fit, 2),
