@@ -93,21 +93,36 @@ __device__ __forceinline__ unsigned nb_lanemask_lt()
     return m;
 }
 
+// Width of a site's row in the staging area: the count pass of a linked-cell site with at most this
+// many list entries (self included) also writes them, in list order, into its row, and the fill
+// pass copies the row instead of walking the cells again.
+constexpr int kStageW = 96;
+
 // One warp per site; FILL=false counts the site's pairs, FILL=true writes them in the
 // reference order. Linked-cell path: lane c < 27 owns neighbor cell c of the z -> y -> x
 // traversal (c = 9 dz + 3 dy + dx), walks its members in decreasing index, and a warp scan
 // of the per-cell counts gives each lane its offset in the site's list. Brute-force path:
 // the warp strides over the supercell in ascending order and compacts with a ballot.
+// With stage (int [n_atoms][kStageW]) and staged (int [n_atoms]) given, the count pass stages the
+// rows that fit (the second walk of the cells reads what the first just brought into L1) and
+// marks them; the fill pass copies a marked row to its place in the list (bounded by the site's
+// offsets) and walks the cells only for the other sites.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int *site_struct,
                                                     const StructDesc *sd, const double *pos_sc,
                                                     const int *cell_start, const int *cell_atoms,
                                                     int64_t *counts, const int64_t *start, int *list,
-                                                    int *check)
+                                                    int *check, int *stage, int *staged)
 {
     const int lane = threadIdx.x & 31;
     const int g = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (g >= n_atoms_total) return;
+    if (FILL && staged && staged[g]) {
+        const int64_t b = start[g], len = start[g + 1] - b;
+        const int *row = stage + (size_t)g * kStageW;
+        for (int j = lane; j < len && j < kStageW; j += 32) list[b + j] = row[j];
+        return;
+    }
     const StructDesc &S = sd[site_struct[g]];
     const int i = g - S.atom_off + 1;  // 1-based local site
     const double *pi = pos_sc + 3 * (size_t)(S.sc_off + i - 1);
@@ -155,6 +170,22 @@ __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int
         if (!FILL) {
             const int total = __shfl_sync(0xffffffffu, incl, 31);
             if (lane == 0) counts[g] = 1 + total;
+            if (stage) {
+                const bool fits = 1 + total <= kStageW;
+                if (fits) {
+                    int *row = stage + (size_t)g * kStageW;
+                    if (lane == 0) row[0] = i;
+                    int w = 1 + (incl - cnt);
+                    for (int t = t0; t < t1; ++t) {
+                        const int k = cell_atoms[t];
+                        if (k == i) continue;
+                        double dist[3], d;
+                        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
+                        if (d < rc) row[w++] = k;
+                    }
+                }
+                if (lane == 0) staged[g] = fits ? 1 : 0;
+            }
         } else {
             int64_t w = w0 + 1 + (incl - cnt);
             for (int t = t0; t < t1; ++t) {
@@ -180,7 +211,10 @@ __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int
             w += __popc(m);
             n += __popc(m);
         }
-        if (!FILL && lane == 0) counts[g] = n;
+        if (!FILL && lane == 0) {
+            counts[g] = n;
+            if (staged) staged[g] = 0;
+        }
     }
 }
 
@@ -399,9 +433,13 @@ static int rebuild_count(tgap_context *ctx, NeighborBatch *nb)
             nb->n_cells, nb->cell_start.as<int>(), nb->cell_tmp.as<int>(), nb->cell_atoms.as<int>());
         TGAP_LAUNCH_CHECK(ctx);
     }
+    // the staging rows (sized with the batch; no allocation once a list exists)
+    if (nb->stage.ensure(sizeof(int) * (size_t)n * kStageW) || nb->staged.ensure(sizeof(int) * (size_t)n))
+        return set_error(ctx, TGAP_ERR_NOMEM, "pair staging rows");
     k_site_pairs<false><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), d_sd, nb->pos_sc.as<double>(),
                                                       nb->cell_start.as<int>(), nb->cell_atoms.as<int>(),
-                                                      nb->counts.as<int64_t>(), nullptr, nullptr, nullptr);
+                                                      nb->counts.as<int64_t>(), nullptr, nullptr, nullptr,
+                                                      nb->stage.as<int>(), nb->staged.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
     TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
     return scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
@@ -417,7 +455,8 @@ static int rebuild_fill(tgap_context *ctx, NeighborBatch *nb, int *check)
     k_site_pairs<true><<<wgrid, T, 0, ctx->stream>>>(n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(),
                                                      nb->pos_sc.as<double>(), nb->cell_start.as<int>(),
                                                      nb->cell_atoms.as<int>(), nullptr, nb->start.as<int64_t>(),
-                                                     nb->list.as<int>(), check);
+                                                     nb->list.as<int>(), check, nb->stage.as<int>(),
+                                                     nb->staged.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

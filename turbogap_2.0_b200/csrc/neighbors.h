@@ -49,6 +49,7 @@ struct NeighborBatch {
     DevBuf nspecies;        // int [P] species channel of the neighbor
     DevBuf jatom;           // int [P] folded global atom of the neighbor
     DevBuf scan_tmp;
+    DevBuf stage, staged;   // int [n_atoms][96] list rows staged by the count pass, int [n_atoms] flags
     int ensure_pairs(int64_t P);
     int64_t pair_capacity() const { return (int64_t)(list.bytes / sizeof(int)); }
     void release_all()
@@ -56,7 +57,7 @@ struct NeighborBatch {
         DevBuf *bufs[] = {&d_structs, &positions, &pos_sc, &species_sc, &site_struct, &atom_cell,
                           &cell_count, &cell_start, &cell_cursor, &cell_atoms, &cell_tmp, &counts, &start,
                           &n_neigh, &list, &rjs, &xyz, &thetas, &phis, &nspecies, &jatom,
-                          &scan_tmp};
+                          &scan_tmp, &stage, &staged};
         for (DevBuf *b : bufs) b->release();
     }
 };

@@ -541,7 +541,8 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         const int site = sites ? sites[row] : row;
         const int64_t kb = start[site], ke = start[site + 1];
         // the central atom's weights, loaded now and added to l = 0 of its own species block at the end
-        const int s_self = nsp[kb] - 1;
+        // (a site with no list entries at all, which the list's capacity clamp can leave, has none)
+        const int s_self = ke > kb ? nsp[kb] - 1 : -1;
         const bool has_central = s_self >= 0 && s_self < P.n_species && lane < P.alpha_max[s_self];
         const T cen = has_central ? central[P.n_off[s_self] + lane] : (T)0;
         if (geo.pos) {
@@ -951,7 +952,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
 #pragma unroll 8
             for (int q = 0; q < 32; ++q) csum += col[9 * q];
         }
-        if (lane < 3) {
+        if (lane < 3 && ke > kb) {  // the self entry (absent only in a list the capacity clamp cut)
             const double fv = csum;
             if (pair_der) {
                 pair_der[3 * kb + lane] = -fv;  // dq_i/dr_i = -sum_j dq_i/dr_j
