@@ -465,27 +465,20 @@ int pair_forces_from_der(tgap_context *ctx, int n_sites, const int64_t *d_start,
 constexpr size_t kNoAllocPartials = (size_t)1 << 20;
 static __device__ __align__(256) double g_noalloc_e_part[kNoAllocPartials];
 
-// Device address of the scratch array on device `dev`, looked up once per device with that
-// device current (the symbol name is only a host-side handle; kernels must be given the address
-// cudaGetSymbolAddress returns). The address stays valid for the life of the device's primary
-// context; a cudaDeviceReset ends that context, and with it the address cached here.
+// Device address of the scratch array on the current device `dev` (the symbol name is only a
+// host-side handle; kernels must be given the address cudaGetSymbolAddress returns). Looked up on
+// every call: the lookup allocates nothing, and a cached address would outlive a cudaDeviceReset.
 static int noalloc_scratch(int dev, double **out)
 {
-    static std::mutex mu;
-    static double *addr[64] = {nullptr};
-    if (dev < 0 || dev >= 64) return TGAP_ERR_CUDA;
-    std::lock_guard<std::mutex> lock(mu);
-    if (!addr[dev]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_e_part);
-        if (e != cudaSuccess || !p) {
-            if (e != cudaSuccess) cudaGetLastError();  // this call's own error, reported below
-            return thread_error(TGAP_ERR_CUDA, "tgap_soap_energies_noalloc: cudaGetSymbolAddress: %s",
-                                cudaGetErrorString(e));
-        }
-        addr[dev] = static_cast<double *>(p);
+    if (dev < 0) return TGAP_ERR_CUDA;
+    void *p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_e_part);
+    if (e != cudaSuccess || !p) {
+        if (e != cudaSuccess) cudaGetLastError();  // this call's own error, reported below
+        return thread_error(TGAP_ERR_CUDA, "tgap_soap_energies_noalloc: cudaGetSymbolAddress: %s",
+                            cudaGetErrorString(e));
     }
-    *out = addr[dev];
+    *out = static_cast<double *>(p);
     return TGAP_OK;
 }
 
