@@ -1424,7 +1424,7 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     if (positions && !direct_in) std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
     const bool on_device = rebuild && device_rebuild && s->nb.list.ptr && s->nb.n_pairs > 0;
     const bool host_rebuild = rebuild && !on_device;
-    const bool geom = !rebuild && can_fuse_geometry(s, n_models, models);
+    const bool geom = !host_rebuild && can_fuse_geometry(s, n_models, models);
     const int do_forces = forces != nullptr || virial != nullptr;
     unsigned char *h = ctx->pinned[1].as<unsigned char>();
     // the device work of the call, stream-ordered; with a host rebuild (a host synchronization for
@@ -1436,7 +1436,8 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         if (on_device) {
             CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
             CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
-            CHECK_RC(neighbors_refresh(ctx, &s->nb));
+            // the geometry comes from the forward where it can
+            CHECK_RC(geom ? neighbors_maps(ctx, &s->nb) : neighbors_refresh(ctx, &s->nb));
         } else if (!geom) {
             CHECK_RC(tgap_system_update(s, host_rebuild ? 1 : 0));
         }
@@ -1777,8 +1778,11 @@ static int md_step_body(tgap_md *md, bool rebuild = false)
     if (rebuild) {
         CHECK_RC(neighbors_sync_positions(ctx, &md->sys->nb));
         CHECK_RC(neighbors_rebuild_lists_device(ctx, &md->sys->nb, true));
+        // the new lists' species and atom maps; their geometry comes from the forward when fused
+        CHECK_RC(md->fused_geom ? neighbors_maps(ctx, &md->sys->nb) : neighbors_refresh(ctx, &md->sys->nb));
+    } else if (!md->fused_geom) {
+        CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     }
-    if (rebuild || !md->fused_geom) CHECK_RC(neighbors_refresh(ctx, &md->sys->nb));
     CHECK_RC(md_eval(md));
     CHECK_RC(velocity_verlet(ctx, md->sys->nb.n_atoms, md->sys->nb.positions.as<double>(),
                              md->pos_prev.as<double>(), md->vel.as<double>(), md->forces.as<double>(),

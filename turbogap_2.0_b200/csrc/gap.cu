@@ -9,7 +9,6 @@
 // derivative matrix G = zeta delta^2 alpha o K^(zeta-1), which is the A operand of the
 // second GEMM g = G Qs. Both are "NT" products (row-major operands, K contiguous).
 #include <cmath>
-#include <mutex>
 
 #include "gap_kernels.h"
 

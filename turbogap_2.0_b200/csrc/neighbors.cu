@@ -220,7 +220,8 @@ __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int
 
 // Geometry of every pair (neighbors_interface.f90:467-510); angles only when requested. With
 // FROM_POS the supercell positions are formed from the primitive ones on the fly (no replicate
-// pass; only for batches whose supercells are pure replicas).
+// pass; only for batches whose supercells are pure replicas). With rjs null only the per-pair
+// species and atom maps are written (the descriptor forward writes the geometry itself).
 template <bool FROM_POS>
 __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const StructDesc *sd,
                                 const double *pos_sc, const double *pos, const int *species_sc,
@@ -243,6 +244,7 @@ __global__ void k_pair_geometry(int n_atoms_total, const int *site_struct, const
         int j = list[k];
         if (jatom) jatom[k] = S.atom_off + (j - 1) % S.n;
         if (nspecies) nspecies[k] = species_sc[S.sc_off + j - 1];
+        if (!rjs) continue;
         if (k == b) {
             rjs[k] = 0.0;
             xyz[3 * k] = xyz[3 * k + 1] = xyz[3 * k + 2] = 0.0;
@@ -525,6 +527,21 @@ int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, b
         nb->positions.as<double>(), nb->species_sc.as<int>(), nb->start.as<int64_t>(), nb->list.as<int>(),
         nb->rjs.as<double>(), nb->xyz.as<double>(), with_angles ? nb->thetas.as<double>() : nullptr,
         with_angles ? nb->phis.as<double>() : nullptr, nb->nspecies.as<int>(), nb->jatom.as<int>());
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
+int neighbors_maps(tgap_context *ctx, NeighborBatch *nb)
+{
+    const int n = nb->n_atoms;
+    if (n <= 0) return TGAP_OK;
+    const int T = 128;
+    StageScope sc(ctx, "neighbors_maps");
+    k_pair_geometry<false><<<(n + T / 32 - 1) / (T / 32), T, 0, ctx->stream>>>(
+        n, nb->site_struct.as<int>(), nb->d_structs.as<StructDesc>(), nb->pos_sc.as<double>(), nullptr,
+        nb->species_sc.as<int>(),
+        nb->start.as<int64_t>(), nb->list.as<int>(), nullptr, nullptr, nullptr, nullptr, nb->nspecies.as<int>(),
+        nb->jatom.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
     return TGAP_OK;
 }

@@ -90,6 +90,9 @@ int neighbors_sync_count(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_geometry(tgap_context *ctx, NeighborBatch *nb, bool with_angles, bool from_positions);
 // Geometry of the current lists at the current (primitive) positions.
 int neighbors_refresh(tgap_context *ctx, NeighborBatch *nb);
+// Only the per-pair species and atom maps of the current lists (after a rebuild whose geometry the
+// descriptor forward writes).
+int neighbors_maps(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_set_counts(tgap_context *ctx, NeighborBatch *nb);
 int neighbors_sync_positions(tgap_context *ctx, NeighborBatch *nb);
 
