@@ -148,8 +148,9 @@ int sync_check_launch(tgap_context *ctx);
 // Codes of the device check word.
 enum CheckCode {
     kCheckNone = 0,
-    kCheckFwdPair = 1,      // descriptor forward: compacted pair outside its site
-    kCheckBwdPair = 2,      // adjoint: compacted pair outside its site
+    kCheckFwdPair = 1,      // descriptor forward: compacted pair outside its site (not raised since
+                            // the compaction stages only the site's own pairs; the code stays reserved)
+    kCheckBwdPair = 2,      // adjoint: the same (reserved)
     kCheckBwdAtom = 3,      // adjoint: neighbor atom index out of range
     kCheckSelfAtom = 4,     // adjoint: self-slot atom index out of range
     kCheckNonFinite = 5,    // velocity Verlet: non-finite force
