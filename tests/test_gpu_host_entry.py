@@ -120,3 +120,29 @@ def test_registered_arrays_give_the_staged_results(ctx, tg, synth):
         assert np.max(np.abs(f0 - f1)) <= 1e-6 * max(1.0, np.abs(f0).max())
         assert np.max(np.abs(v0 - v1)) <= 1e-6 * max(1.0, np.abs(v0).max())
     model.close()
+
+
+def test_call_graphs_follow_e0_and_site_range_changes(ctx, tg, synth):
+    """The host-buffer entry replays captured graphs from its third call on; e0 (tgap_system_set_e0)
+    and the site range (tgap_system_set_site_range) set afterwards still apply: each atom's energy
+    moves by its e0, and a range leaves the energies outside it at zero and its own unchanged."""
+    hyp, m = helpers.carbon_model(synth, 200, seed=17)
+    pos, box, sp, _ = synth.random_packing(256, 2.5, 1.2, seed=23)
+    n = len(pos)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+    for _ in range(3):  # eager, captured, replayed
+        e, f, _ = system.calculate_gap_soap([model], tg.TGAP_FP64, pos, rebuild=False)
+    system.set_e0([-1.25])
+    e1, f1, _ = system.calculate_gap_soap([model], tg.TGAP_FP64, pos, rebuild=False)
+    assert np.max(np.abs(e1 - (e - 1.25))) < 1e-12
+    assert np.max(np.abs(f1 - f)) < 1e-12
+    system.set_site_range(0, n // 2)
+    e2, _, _ = system.calculate_gap_soap([model], tg.TGAP_FP64, pos, rebuild=False)
+    assert np.all(e2[n // 2:] == 0.0)
+    assert np.max(np.abs(e2[:n // 2] - e1[:n // 2])) < 1e-12
+    system.set_site_range(0)
+    e3, _, _ = system.calculate_gap_soap([model], tg.TGAP_FP64, pos, rebuild=False)
+    assert np.max(np.abs(e3 - e1)) < 1e-12
+    system.close()
+    model.close()

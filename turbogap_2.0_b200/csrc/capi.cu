@@ -817,7 +817,8 @@ struct tgap_system {
         std::vector<const tgap_model *> models;
         int precision = 0, flags = 0;
         const void *io[4] = {nullptr, nullptr, nullptr, nullptr};
-        bool seen = false;  // ran eagerly once (buffers sized): the next call captures
+        bool seen = false;  // ran eagerly once at seen_epoch (buffers sized): the next call captures
+        uint64_t seen_epoch = 0;
         cudaGraph_t graph = nullptr;
         cudaGraphExec_t exec = nullptr;
         uint64_t epoch = 0;
@@ -1490,11 +1491,14 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
             std::copy(io, io + 4, cg->io);
         }
         const uint64_t e0 = g_alloc_epoch.load(std::memory_order_relaxed);
-        if (cg->exec && cg->epoch != e0) {  // a buffer moved since the capture
-            cudaGraphExecDestroy(cg->exec);
-            cudaGraphDestroy(cg->graph);
+        if (cg->epoch != e0) {
+            // something the graph baked in changed (or nothing was captured yet): run eagerly once
+            // more, which rebuilds host-side state such as site sets, before capturing again
+            if (cg->exec) cudaGraphExecDestroy(cg->exec);
+            if (cg->graph) cudaGraphDestroy(cg->graph);
             cg->exec = nullptr;
             cg->graph = nullptr;
+            if (cg->seen && cg->seen_epoch != e0) cg->seen = false;
         }
         if (!cg->exec && cg->seen) {
             TGAP_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeRelaxed));
@@ -1520,6 +1524,7 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         } else {
             CHECK_RC(device_work());
             cg->seen = true;
+            cg->seen_epoch = g_alloc_epoch.load(std::memory_order_relaxed);
         }
     }
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
