@@ -356,6 +356,33 @@ def test_md_device_rebuild_count_matches_a_host_rebuild(ctx, tg, synth, carbon):
     model.close()
 
 
+def test_md_graphs_follow_an_e0_set_between_runs(ctx, tg, synth, carbon):
+    """e0 set between two md.run calls makes the captured step graphs stale: the next step runs
+    eagerly and the graphs are captured again. The trajectory equals that of an MD with e0 set from
+    the start (e0 moves no force), and so does the potential energy once both carry it."""
+    hyp, m = carbon
+    pos, box, sp, masses = synth.random_packing(128, 2.5, 1.2, seed=73)
+    vel = synth.maxwell_boltzmann(masses, 1000.0, seed=4)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    out = []
+    for late in (False, True):
+        system = tg.System(ctx, [(pos, box, sp)], 3.7 + 0.3)
+        if not late:
+            system.set_e0([-2.5])
+        md = tg.MD(ctx, system, [model], masses, 1.0, rebuild_every=5, use_graph=True)
+        md.set_velocities(vel)
+        md.run(12)
+        if late:
+            system.set_e0([-2.5])
+        md.run(13)
+        out.append(md.state())
+        md.close()
+        system.close()
+    assert np.max(np.abs(out[0]["positions"] - out[1]["positions"])) < 1e-9
+    assert abs(out[0]["e_pot"] - out[1]["e_pot"]) < 1e-8
+    model.close()
+
+
 def test_md_pair_capacity_overflow_is_reported(ctx, tg, synth, carbon):
     """A device-side rebuild that finds more pairs than the arrays reserved (a quarter above the
     first list) clamps the lists inside the arrays and reports TGAP_ERR_CAPACITY at the next check,

@@ -1732,6 +1732,7 @@ struct tgap_md {
     // of the pair count (neighbors_rebuild_lists_device): systems without pair/triplet terms,
     // whose buffers follow the host count
     bool device_rebuild = false;
+    uint64_t settled_epoch = 0;  // graph epoch at the last eager step (graphs are captured only at it)
     // a whole rebuild cycle (the rebuild step and the rebuild_every - 1 steps after it) as one graph
     cudaGraph_t graph_cycle = nullptr;
     cudaGraphExec_t exec_cycle = nullptr;
@@ -2063,8 +2064,13 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
     CHECK_RC(activate(ctx));
     for (int it = 0; it < n_steps; ++it) {
         const bool rebuild = (md->step % md->rebuild_every) == 0;
+        // after any change that makes the captured graphs stale, one step runs eagerly (it rebuilds
+        // host-side state such as site sets, which cannot happen inside a capture) before graphs
+        // are captured again
+        const bool graphs = md->use_graph && !md->first &&
+                            md->settled_epoch == g_alloc_epoch.load(std::memory_order_relaxed);
         // a whole rebuild cycle goes out as one graph launch when the lists are rebuilt on the device
-        if (md->use_graph && !md->first && rebuild && md->device_rebuild && n_steps - it >= md->rebuild_every) {
+        if (graphs && rebuild && md->device_rebuild && n_steps - it >= md->rebuild_every) {
             CHECK_RC(md_graph(md, md->rebuild_every, &md->graph_cycle, &md->exec_cycle, &md->cycle_epoch,
                               &md->cycle_kernels, true));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_cycle, ctx->stream));
@@ -2076,8 +2082,7 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
         }
         // a full run of rebuild-free steps goes out as one graph launch
         const int run = md->rebuild_every - 1;
-        if (md->use_graph && !md->first && !rebuild && run > 1 && md->step % md->rebuild_every == 1 &&
-            n_steps - it >= run) {
+        if (graphs && !rebuild && run > 1 && md->step % md->rebuild_every == 1 && n_steps - it >= run) {
             CHECK_RC(md_graph(md, run, &md->graph_run, &md->exec_run, &md->run_epoch, &md->run_kernels));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_run, ctx->stream));
             ctx->launches += md->run_kernels;
@@ -2103,17 +2108,19 @@ extern "C" int tgap_md_run(tgap_md *md, int n_steps)
                                      md->forces_prev.as<double>(), md->mass.as<double>(), md->dt, md->dt,
                                      md->first ? 1 : 0));
             md->first = false;
-        } else if (rebuild && md->device_rebuild && md->use_graph) {
+            md->settled_epoch = g_alloc_epoch.load(std::memory_order_relaxed);
+        } else if (graphs && rebuild && md->device_rebuild) {
             CHECK_RC(md_graph(md, 1, &md->graph_rb, &md->exec_rb, &md->rb_epoch, &md->rb_kernels, true));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec_rb, ctx->stream));
             ctx->launches += md->rb_kernels;
             md->sys->nb.count_on_device = true;
-        } else if (md->use_graph) {
+        } else if (graphs) {
             CHECK_RC(md_graph(md, 1, &md->graph, &md->exec, &md->graph_epoch, &md->graph_kernels));
             TGAP_CUDA(ctx, cudaGraphLaunch(md->exec, ctx->stream));
             ctx->launches += md->graph_kernels;
         } else {
             CHECK_RC(md_step_body(md, rebuild && md->device_rebuild));
+            md->settled_epoch = g_alloc_epoch.load(std::memory_order_relaxed);
         }
         ++md->step;
     }
