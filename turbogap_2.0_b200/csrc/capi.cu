@@ -1413,8 +1413,7 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     if (ctx->pinned[0].ensure(sizeof(double) * 3 * (size_t)N) || ctx->pinned[1].ensure(out_bytes + 16) ||
         s->scratch_forces.ensure(out_bytes) || s->queue.ensure(sizeof(int) * kQueueInts))
         return set_error(ctx, TGAP_ERR_NOMEM, "staging buffers");
-    if (n_models <= 0 || !models || 2 * n_models > kQueueInts)
-        return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
+    if (n_models <= 0 || !models) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
     for (int i = 0; i < n_models; ++i)
         if (!models[i]) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: null model");
     // registered caller arrays are copied to and from directly, others through the staging buffers
@@ -1447,9 +1446,11 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         double *d_v = d_f + 3 * (size_t)N;
         // energies, forces and virial are one buffer: one clear, and one for the site counters
         TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, out_bytes, ctx->stream));
-        TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
+        // (more models than the counters cover: the descriptor launches without the work queue)
+        const bool counters = 2 * n_models <= kQueueInts;
+        if (counters) TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
         CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
-                                s->queue.as<int>()));
+                                counters ? s->queue.as<int>() : nullptr));
         if (direct_out) {
             TGAP_CUDA(ctx, cudaMemcpyAsync(energies, d_e, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
             if (forces)
