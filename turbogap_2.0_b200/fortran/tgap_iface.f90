@@ -145,6 +145,51 @@ module tgap_iface
          real(c_double) :: V(*), V_der(3, *)
       end function
 
+      ! resident models and structures (calculate_gap_soap.f90:171 on device-resident state)
+      integer(c_int) function tgap_model_create(ctx, hypers, central_species, n_sparse, alphas, Qs, delta, &
+                                                zeta, model) bind(C, name="tgap_model_create")
+         import :: c_int, c_ptr, c_double, tgap_soap_hypers
+         type(c_ptr), value :: ctx
+         type(tgap_soap_hypers), intent(in) :: hypers
+         integer(c_int), value :: central_species, n_sparse
+         real(c_double), intent(in) :: alphas(*), Qs(*)
+         real(c_double), value :: delta, zeta
+         type(c_ptr), intent(out) :: model
+      end function
+
+      integer(c_int) function tgap_model_destroy(model) bind(C, name="tgap_model_destroy")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: model
+      end function
+
+      integer(c_int) function tgap_system_create(ctx, n_structures, offsets, positions, boxes, species, &
+                                                 rcut_max, system) bind(C, name="tgap_system_create")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx
+         integer(c_int), value :: n_structures
+         integer(c_int), intent(in) :: offsets(*), species(*)
+         real(c_double), intent(in) :: positions(3, *), boxes(9, *)
+         real(c_double), value :: rcut_max
+         type(c_ptr), intent(out) :: system
+      end function
+
+      integer(c_int) function tgap_system_destroy(system) bind(C, name="tgap_system_destroy")
+         import :: c_int, c_ptr
+         type(c_ptr), value :: system
+      end function
+
+      ! one host-buffer evaluation of a host MD step: positions (c_loc, or c_null_ptr to keep the
+      ! resident ones) in, energies, forces and virial out; rebuild = 1 on list-rebuild steps
+      integer(c_int) function tgap_calculate_gap_soap(ctx, system, n_models, models, precision, positions, &
+                                                      rebuild, energies, forces, virial) &
+         bind(C, name="tgap_calculate_gap_soap")
+         import :: c_int, c_ptr, c_double
+         type(c_ptr), value :: ctx, system, positions
+         integer(c_int), value :: n_models, precision, rebuild
+         type(c_ptr), intent(in) :: models(*)
+         real(c_double), intent(out) :: energies(*), forces(3, *), virial(9, *)
+      end function
+
       ! calculate_e0 (calculate_gap_soap.f90:135-169) on a resident system: species_info%e0(1:n_species)
       integer(c_int) function tgap_system_set_e0(system, n_species, e0) bind(C, name="tgap_system_set_e0")
          import :: c_int, c_ptr, c_double
