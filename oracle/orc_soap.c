@@ -411,6 +411,7 @@ void orc_angular(const orc_soap_hypers *h, int s, double r, const double u[3], d
 
 int orc_soap_dim(const orc_soap_hypers *h)
 {
+    if (h->n_compress > 0) return h->dim_out;
     int nmax = 0;
     for (int s = 0; s < h->n_species; ++s) nmax += h->alpha_max[s];
     return nmax * (nmax + 1) / 2 * (h->l_max + 1);
@@ -430,6 +431,12 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
     }
     if (L > ORC_MAX_L) return 1;
     const int D = nmax * (nmax + 1) / 2 * (L + 1);
+    /* output length: the compressed one when P is given (entries outside the ranges are refused) */
+    const int cmp = h->n_compress > 0;
+    const int Dout = cmp ? h->dim_out : D;
+    for (int e = 0; cmp && e < h->n_compress; ++e)
+        if (h->compress_P_i[e] < 1 || h->compress_P_i[e] > Dout || h->compress_P_j[e] < 1 || h->compress_P_j[e] > D)
+            return 1;
     radial_table *tb = make_tables(h);
     for (int s = 0; s < ns; ++s)
         if (tb[s].n <= 0) {
@@ -448,6 +455,8 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
         double *dc = (double *)malloc(sizeof(double) * 3 * (size_t)nmax * nlm);
         double *p = (double *)malloc(sizeof(double) * (size_t)D);
         double *dp = (double *)malloc(sizeof(double) * 3 * (size_t)D);
+        double *pc = (double *)malloc(sizeof(double) * (size_t)Dout);
+        double *dpc = (double *)malloc(sizeof(double) * 3 * (size_t)Dout);
         double *A = (double *)malloc(sizeof(double) * (size_t)nlm);
         double *dA = (double *)malloc(sizeof(double) * 3 * (size_t)nlm);
 #pragma omp for schedule(dynamic, 4)
@@ -489,15 +498,24 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
                         ++cnt;
                     }
                 }
+            if (cmp) {
+                /* P p in the order the entries are given, and its norm */
+                memset(pc, 0, sizeof(double) * (size_t)Dout);
+                for (int e = 0; e < h->n_compress; ++e)
+                    pc[h->compress_P_i[e] - 1] += h->compress_P_el[e] * p[h->compress_P_j[e] - 1];
+                nrm2 = 0.0;
+                for (int d = 0; d < Dout; ++d) nrm2 += pc[d] * pc[d];
+            }
+            const double *pv = cmp ? pc : p;
             double nrm = sqrt(nrm2);
-            double *q = soap + (size_t)i * D;
-            for (int d = 0; d < D; ++d) q[d] = nrm > 0.0 ? p[d] / nrm : 0.0;
+            double *q = soap + (size_t)i * Dout;
+            for (int d = 0; d < Dout; ++d) q[d] = nrm > 0.0 ? pv[d] / nrm : 0.0;
             if (!soap_cart_der) continue;
             /* derivatives: one pair at a time (non-self), self slot = -sum */
-            double *self_der = soap_cart_der + (size_t)start[i] * D * 3;
-            memset(self_der, 0, sizeof(double) * 3 * (size_t)D);
+            double *self_der = soap_cart_der + (size_t)start[i] * Dout * 3;
+            memset(self_der, 0, sizeof(double) * 3 * (size_t)Dout);
             for (int64_t k = start[i] + 1; k < start[i + 1]; ++k) {
-                double *out = soap_cart_der + (size_t)k * D * 3;
+                double *out = soap_cart_der + (size_t)k * Dout * 3;
                 memset(dc, 0, sizeof(double) * 3 * (size_t)nmax * nlm);
                 int any = 0;
                 double r = rjs[k];
@@ -516,7 +534,7 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
                     any = 1;
                 }
                 if (!any || nrm == 0.0) {
-                    memset(out, 0, sizeof(double) * 3 * (size_t)D);
+                    memset(out, 0, sizeof(double) * 3 * (size_t)Dout);
                     continue;
                 }
                 cnt = 0;
@@ -534,14 +552,25 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
                             }
                             for (int x = 0; x < 3; ++x) {
                                 dp[3 * cnt + x] = mult * acc[x];
-                                qdp[x] += q[cnt] * dp[3 * cnt + x];
+                                if (!cmp) qdp[x] += q[cnt] * dp[3 * cnt + x];
                             }
                             ++cnt;
                         }
                     }
-                for (int d = 0; d < D; ++d)
+                const double *dpv = dp;
+                if (cmp) {
+                    memset(dpc, 0, sizeof(double) * 3 * (size_t)Dout);
+                    for (int e = 0; e < h->n_compress; ++e)
+                        for (int x = 0; x < 3; ++x)
+                            dpc[3 * (h->compress_P_i[e] - 1) + x] +=
+                                h->compress_P_el[e] * dp[3 * (h->compress_P_j[e] - 1) + x];
+                    for (int d = 0; d < Dout; ++d)
+                        for (int x = 0; x < 3; ++x) qdp[x] += q[d] * dpc[3 * d + x];
+                    dpv = dpc;
+                }
+                for (int d = 0; d < Dout; ++d)
                     for (int x = 0; x < 3; ++x) {
-                        double v = (dp[3 * d + x] - q[d] * qdp[x]) / nrm;
+                        double v = (dpv[3 * d + x] - q[d] * qdp[x]) / nrm;
                         out[3 * d + x] = v;
                         self_der[3 * d + x] -= v;
                     }
@@ -551,6 +580,8 @@ int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh, int 
         free(dc);
         free(p);
         free(dp);
+        free(pc);
+        free(dpc);
         free(A);
         free(dA);
     }

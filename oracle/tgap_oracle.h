@@ -83,9 +83,19 @@ typedef struct {
     const double *amplitude_scaling;
     const double *central_weight;
     int radial_enhancement;             /* 0, 1 or 2 */
+    /* SOAP compression (read_gap.f90:489-559, the P_transformation of file_compress_soap): the
+     * descriptor is P p / |P p| with p the uncompressed power spectrum and P sparse, given as
+     * n_compress entries (compress_P_i, compress_P_j 1-based, compress_P_el) and dim_out rows;
+     * n_compress = 0: no compression. */
+    int n_compress;
+    int dim_out;
+    const int *compress_P_i;
+    const int *compress_P_j;
+    const double *compress_P_el;
 } orc_soap_hypers;
 
-/* Length of the (uncompressed) descriptor: n_max (n_max+1)/2 (l_max+1), n_max = sum alpha_max. */
+/* Length of the descriptor: dim_out with compression, else n_max (n_max+1)/2 (l_max+1),
+ * n_max = sum alpha_max. */
 int orc_soap_dim(const orc_soap_hypers *h);
 
 /* Quadrature tables for one species channel (exposed for the known-answer tests).
@@ -106,7 +116,7 @@ void orc_radial(const orc_soap_hypers *h, int s, double r, int central, double *
 void orc_angular(const orc_soap_hypers *h, int s, double r, const double u[3], double *A,
                  double *dA);
 
-/* get_soap (gap_interface.f90:301-306 argument order, compression off).
+/* get_soap (gap_interface.f90:301-306 argument order; compression as the hypers give it).
  * mask is n_atom_pairs x n_species (column-major, nonzero = neighbor belongs to channel).
  * soap: D x n_sites (normalised). soap_cart_der: 3 x D x n_atom_pairs, or NULL. */
 int orc_get_soap(const orc_soap_hypers *h, int n_sites, const int *n_neigh,

@@ -35,6 +35,11 @@ class _Hypers(C.Structure):
         ("amplitude_scaling", C.POINTER(C.c_double)),
         ("central_weight", C.POINTER(C.c_double)),
         ("radial_enhancement", C.c_int),
+        ("n_compress", C.c_int),
+        ("dim_out", C.c_int),
+        ("compress_P_i", C.POINTER(C.c_int)),
+        ("compress_P_j", C.POINTER(C.c_int)),
+        ("compress_P_el", C.POINTER(C.c_double)),
     ]
 
 
@@ -117,6 +122,16 @@ class Hypers:
             v = np.ascontiguousarray(np.broadcast_to(np.asarray(sp[k], dtype=np.float64), (ns,)))
             self.arrays[k] = v
             setattr(self.s, k, v.ctypes.data_as(C.POINTER(C.c_double)))
+        # SOAP compression: sp["compress"] = (P_i, P_j, P_el, dim_out), 1-based indices
+        if sp.get("compress") is not None:
+            pi, pj, pel, dim_out = sp["compress"]
+            for k, v, t in (("compress_P_i", pi, np.int32), ("compress_P_j", pj, np.int32),
+                            ("compress_P_el", pel, np.float64)):
+                a = np.ascontiguousarray(v, dtype=t)
+                self.arrays[k] = a
+                setattr(self.s, k, a.ctypes.data_as(C.POINTER(C.c_int if t is np.int32 else C.c_double)))
+            self.s.n_compress = len(self.arrays["compress_P_i"])
+            self.s.dim_out = int(dim_out)
 
     @property
     def ref(self):

@@ -249,6 +249,60 @@ def test_soap_cart_der_finite_difference(orc, synth):
                 assert np.allclose((qp - qm) / (2 * h), der[k, :, x], atol=2e-8)
 
 
+def _compress_np(q, der, pi, pj, pel, dim_out):
+    """q_c = P q / |P q| and dq_c = (I - q_c q_c^T) P dq / |P q| from the uncompressed normalised
+    descriptor (the normalisation of p cancels: P p / |P p| = P q / |P q|)."""
+    P = np.zeros((dim_out, q.shape[1]))
+    np.add.at(P, (np.asarray(pi) - 1, np.asarray(pj) - 1), pel)
+    pq = q @ P.T
+    nr = np.linalg.norm(pq, axis=1)
+    qc = pq / nr[:, None]
+    return P, qc, nr
+
+
+def test_soap_compression_matches_the_projection(orc, synth):
+    """The oracle's compression (the P_transformation of read_gap.f90:489-559: q = P p / |P p|)
+    against the same projection applied to its uncompressed output, for the identity, a selection
+    of components (the old index-list format) and a random sparse P with repeated rows; the
+    compressed derivatives against finite differences of the compressed descriptor."""
+    rng = np.random.default_rng(12)
+    X = rng.normal(size=(6, 3)) * 1.2
+    hyp = synth.carbon_hypers()
+    H, nb, q, der = _isolated(orc, synth, X, hyp)
+    D = q.shape[1]
+    start = np.concatenate([[0], np.cumsum(nb["n_neigh"])])
+    sel = np.sort(rng.choice(D, 120, replace=False)) + 1
+    nnz = 400
+    cases = [(np.arange(1, D + 1), np.arange(1, D + 1), np.ones(D), D),
+             (np.arange(1, 121), sel, np.ones(120), 120),
+             (rng.integers(1, 91, nnz), rng.integers(1, D + 1, nnz), rng.normal(size=nnz), 90)]
+    for pi, pj, pel, dim_out in cases:
+        hc = dict(hyp, compress=(pi, pj, pel, dim_out))
+        _, _, qc, derc = _isolated(orc, synth, X, hc)
+        P, qref, nr = _compress_np(q, der, pi, pj, pel, dim_out)
+        assert qc.shape == (len(X), dim_out)
+        assert np.max(np.abs(qc - qref)) < 1e-13
+        for i in range(len(X)):
+            for k in range(start[i], start[i + 1]):
+                pd = P @ der[k]  # (dim_out, 3)
+                ref = (pd - np.outer(qref[i], qref[i] @ pd)) / nr[i]
+                assert np.max(np.abs(derc[k] - ref)) < 1e-11, (dim_out, i, k)
+    # finite differences of the random compression
+    pi, pj, pel, dim_out = cases[2]
+    hc = dict(hyp, compress=(pi, pj, pel, dim_out))
+    _, _, qc, derc = _isolated(orc, synth, X, hc)
+    h = 1e-6
+    for i, k in ((0, start[0] + 1), (3, start[3] + 2)):
+        j = nb["neighbors_list"][k] - 1
+        for x in range(3):
+            Xp, Xm = X.copy(), X.copy()
+            Xp[j, x] += h
+            Xm[j, x] -= h
+            qp = _isolated(orc, synth, Xp, hc)[2][i]
+            qm = _isolated(orc, synth, Xm, hc)[2][i]
+            assert np.allclose((qp - qm) / (2 * h), derc[k, :, x], atol=2e-8)
+
+
 # ------------------------------------------------------------------ GAP and dynamics
 
 def test_gap_forces_virial_fd_and_invariance(orc, synth):
