@@ -224,6 +224,17 @@ typedef struct tgap_system tgap_system;
 int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
                       int n_sparse, const double *alphas, const double *Qs, double delta,
                       double zeta, tgap_model **model);
+/* The same with SOAP compression (read_gap.f90:489-559, the P_transformation of a
+ * file_compress_soap): the descriptor is P p / |P p|, p the uncompressed power spectrum in the
+ * component order of tgap_get_soap (n <= n', then l) and P a sparse dim_out x dim matrix given as
+ * P_nonzero entries (P_i in 1..dim_out, P_j in 1..dim, 1-based; entries of one row or column are
+ * summed in the order given). Qs: dim_out x n_sparse. The old index-list format is P_i = i,
+ * P_el = 1. A compress_mode recipe (soap_turbo's get_compress_indices, not in the reference
+ * sources) is not available. */
+int tgap_model_create_compressed(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
+                                 int n_sparse, const double *alphas, const double *Qs, double delta,
+                                 double zeta, int dim_out, int P_nonzero, const int *P_i, const int *P_j,
+                                 const double *P_el, tgap_model **model);
 int tgap_model_destroy(tgap_model *model);
 int tgap_model_dim(const tgap_model *model);
 

@@ -278,14 +278,26 @@ def assign_species(species_types, names):
 class Model:
     """One soap_turbo GAP model resident on the device (tgap_model)."""
 
-    def __init__(self, ctx, hypers, Qs, alphas, delta=1.0, zeta=4.0, central_species=0):
+    def __init__(self, ctx, hypers, Qs, alphas, delta=1.0, zeta=4.0, central_species=0, compress=None):
+        """compress: SOAP compression (P_i, P_j, P_el, dim_out), 1-based entries of P
+        (tgap_model_create_compressed); Qs then has dim_out columns."""
         self.ctx = ctx
         self.hypers = dict(hypers)
         hs, keep = N.make_hypers(hypers)
         Qs = _f64(Qs)
         h = C.c_void_p()
-        check(ctx._L.tgap_model_create(ctx.h, C.byref(hs), int(central_species), Qs.shape[0], ptr(_f64(alphas)),
-                                       ptr(Qs), float(delta), float(zeta), C.byref(h)), ctx.h, "tgap_model_create")
+        if compress is None:
+            check(ctx._L.tgap_model_create(ctx.h, C.byref(hs), int(central_species), Qs.shape[0],
+                                           ptr(_f64(alphas)), ptr(Qs), float(delta), float(zeta), C.byref(h)),
+                  ctx.h, "tgap_model_create")
+        else:
+            pi = np.ascontiguousarray(compress[0], np.int32)
+            pj = np.ascontiguousarray(compress[1], np.int32)
+            pel = _f64(compress[2])
+            check(ctx._L.tgap_model_create_compressed(ctx.h, C.byref(hs), int(central_species), Qs.shape[0],
+                                                      ptr(_f64(alphas)), ptr(Qs), float(delta), float(zeta),
+                                                      int(compress[3]), len(pi), ptr(pi), ptr(pj), ptr(pel),
+                                                      C.byref(h)), ctx.h, "tgap_model_create_compressed")
         del keep
         self.h = h
         self.dim = int(ctx._L.tgap_model_dim(h))

@@ -542,6 +542,62 @@ static void release_soap(DeviceSoap *ds)
     ds->tq32.release();
     ds->central32.release();
     ds->rtab.release();
+    ds->cmp_i.release();
+    ds->cmp_f64.release();
+    ds->cmp_f32.release();
+}
+
+// The compression P (entries P_i, P_j 1-based, values P_el) of a model's descriptor on the device:
+// CSR by output component and CSC by power-spectrum component, each in the given entry order.
+static int upload_compression(tgap_context *ctx, DeviceSoap *ds, int dim_out, int nnz, const int *P_i,
+                              const int *P_j, const double *P_el)
+{
+    const int dim = ds->p.dim;
+    if (dim_out <= 0 || nnz <= 0 || !P_i || !P_j || !P_el)
+        return set_error(ctx, TGAP_ERR_ARGUMENT, "compression: bad arguments");
+    for (int e = 0; e < nnz; ++e)
+        if (P_i[e] < 1 || P_i[e] > dim_out || P_j[e] < 1 || P_j[e] > dim)
+            return set_error(ctx, TGAP_ERR_ARGUMENT, "compression entry %d (%d, %d) outside %d x %d", e, P_i[e],
+                             P_j[e], dim_out, dim);
+    std::vector<int> row(dim_out + 1, 0), col(dim + 1, 0), rcol(nnz), crow(nnz);
+    std::vector<double> rval(nnz), cval(nnz);
+    for (int e = 0; e < nnz; ++e) {
+        ++row[P_i[e]];
+        ++col[P_j[e]];
+    }
+    for (int r = 0; r < dim_out; ++r) row[r + 1] += row[r];
+    for (int c = 0; c < dim; ++c) col[c + 1] += col[c];
+    std::vector<int> rfill(row.begin(), row.end() - 1), cfill(col.begin(), col.end() - 1);
+    for (int e = 0; e < nnz; ++e) {
+        const int r = P_i[e] - 1, c = P_j[e] - 1;
+        rcol[rfill[r]] = c;
+        rval[rfill[r]++] = P_el[e];
+        crow[cfill[c]] = r;
+        cval[cfill[c]++] = P_el[e];
+    }
+    // one int buffer [row | rcol | col | crow], one FP64 and one FP32 buffer [rval | cval]
+    std::vector<int> ib;
+    ib.insert(ib.end(), row.begin(), row.end());
+    ib.insert(ib.end(), rcol.begin(), rcol.end());
+    ib.insert(ib.end(), col.begin(), col.end());
+    ib.insert(ib.end(), crow.begin(), crow.end());
+    std::vector<double> db(rval);
+    db.insert(db.end(), cval.begin(), cval.end());
+    std::vector<float> fb(db.begin(), db.end());
+    CHECK_RC(upload(ctx, ds->cmp_i, ib.data(), ib.size()));
+    CHECK_RC(upload(ctx, ds->cmp_f64, db.data(), db.size()));
+    CHECK_RC(upload(ctx, ds->cmp_f32, fb.data(), fb.size()));
+    const int *i0 = ds->cmp_i.as<int>();
+    ds->p.dim_out = dim_out;
+    ds->p.cmp_row = i0;
+    ds->p.cmp_rcol = i0 + dim_out + 1;
+    ds->p.cmp_col = i0 + dim_out + 1 + nnz;
+    ds->p.cmp_crow = i0 + dim_out + 1 + nnz + dim + 1;
+    ds->p.cmp_rval = ds->cmp_f64.as<double>();
+    ds->p.cmp_cval = ds->cmp_f64.as<double>() + nnz;
+    ds->p.cmp_rval32 = ds->cmp_f32.as<float>();
+    ds->p.cmp_cval32 = ds->cmp_f32.as<float>() + nnz;
+    return TGAP_OK;
 }
 
 extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh, int n_species,
@@ -827,9 +883,9 @@ struct tgap_system {
     std::vector<CallGraph> call_graphs;
 };
 
-extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
-                                 int n_sparse, const double *alphas, const double *Qs, double delta,
-                                 double zeta, tgap_model **out)
+static int model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species, int n_sparse,
+                        const double *alphas, const double *Qs, double delta, double zeta, int dim_out,
+                        int P_nonzero, const int *P_i, const int *P_j, const double *P_el, tgap_model **out)
 {
     CHECK_RC(activate(ctx));
     if (!hypers || n_sparse <= 0 || !alphas || !Qs || !out)
@@ -838,9 +894,10 @@ extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hype
     m->ctx = ctx;
     m->central_species = central_species;
     int rc = prepare_soap(ctx, hypers, &m->soap);
+    if (!rc && P_nonzero > 0) rc = upload_compression(ctx, &m->soap, dim_out, P_nonzero, P_i, P_j, P_el);
     if (!rc) {
         m->gap.n_sparse = n_sparse;
-        m->gap.dim = m->soap.p.dim;
+        m->gap.dim = m->soap.p.dim_out;  // the descriptor's length, compressed or not
         m->gap.delta = delta;
         m->gap.zeta = zeta;
         rc = upload(ctx, m->gap.Qs, Qs, (size_t)n_sparse * m->gap.dim);
@@ -857,6 +914,24 @@ extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hype
     }
     *out = m;
     return TGAP_OK;
+}
+
+extern "C" int tgap_model_create(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
+                                 int n_sparse, const double *alphas, const double *Qs, double delta,
+                                 double zeta, tgap_model **out)
+{
+    return model_create(ctx, hypers, central_species, n_sparse, alphas, Qs, delta, zeta, 0, 0, nullptr, nullptr,
+                        nullptr, out);
+}
+
+extern "C" int tgap_model_create_compressed(tgap_context *ctx, const tgap_soap_hypers *hypers, int central_species,
+                                            int n_sparse, const double *alphas, const double *Qs, double delta,
+                                            double zeta, int dim_out, int P_nonzero, const int *P_i,
+                                            const int *P_j, const double *P_el, tgap_model **out)
+{
+    if (P_nonzero <= 0) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_model_create_compressed: no entries");
+    return model_create(ctx, hypers, central_species, n_sparse, alphas, Qs, delta, zeta, dim_out, P_nonzero, P_i,
+                        P_j, P_el, out);
 }
 
 extern "C" int tgap_model_destroy(tgap_model *m)

@@ -494,11 +494,19 @@ template <int NLM> struct AStride {
 
 // ----------------------------------------------------------------------------- forward
 
-// Elements of the forward's middle area: the angular rows [32][astr], the power spectrum [dim] and
-// the group stage, whichever is largest, rounded to 16 bytes.
-template <class T> __host__ __device__ constexpr int fwd_area(int astr, int dim)
+// Values of the compression P in the kernel's precision: by rows (the forward) or by columns.
+template <class T> __device__ __forceinline__ const T *cmp_vals(const SoapParams &P, bool by_rows)
 {
-    const int a = 32 * astr > dim ? 32 * astr : dim;
+    if constexpr (std::is_same<T, float>::value) return by_rows ? P.cmp_rval32 : P.cmp_cval32;
+    else return by_rows ? P.cmp_rval : P.cmp_cval;
+}
+
+// Elements of the forward's middle area: the angular rows [32][astr], the power spectrum [dim] (and
+// its compression P p [dim_c] after it, dim_c = 0 without compression) and the group stage,
+// whichever is largest, rounded to 16 bytes.
+template <class T> __host__ __device__ constexpr int fwd_area(int astr, int dim, int dim_c)
+{
+    const int a = 32 * astr > dim + dim_c ? 32 * astr : dim + dim_c;
     const int g = (int)((sizeof(GroupStage) + sizeof(T) - 1) / sizeof(T));
     const int m = a > g ? a : g;
     return (m + (int)(16 / sizeof(T)) - 1) / (int)(16 / sizeof(T)) * (int)(16 / sizeof(T));
@@ -536,7 +544,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         T *Rs = reinterpret_cast<T *>(wbase);
         T *As = Rs + 32 * AMB;
         GroupStage *stage = reinterpret_cast<GroupStage *>(As);
-        T *cs = As + fwd_area<T>(ASTR, dim);
+        T *cs = As + fwd_area<T>(ASTR, dim, P.cmp_row ? P.dim_out : 0);
 
         const int site = sites ? sites[row] : row;
         const int64_t kb = start[site], ke = start[site + 1];
@@ -650,6 +658,24 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
                 part += v * v;
             }
         }
+        // with compression the descriptor is P p / |P p|: P p in the area after the power spectrum,
+        // each row summed in the order its entries were given
+        const T *qsrc = ps;
+        int dq = dim;
+        if (P.cmp_row) {
+            __syncwarp();
+            T *pcs = ps + dim;
+            const T *val = cmp_vals<T>(P, true);
+            part = 0;
+            for (int r = lane; r < P.dim_out; r += 32) {
+                T acc = 0;
+                for (int e = P.cmp_row[r]; e < P.cmp_row[r + 1]; ++e) acc += val[e] * ps[P.cmp_rcol[e]];
+                pcs[r] = acc;
+                part += acc * acc;
+            }
+            qsrc = pcs;
+            dq = P.dim_out;
+        }
     #pragma unroll
         for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
         const T nrm = t_sqrt<T>(part);
@@ -664,7 +690,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
             for (int d = 4 * lane; vec && d < q_ld; d += 128) {
                 float v[4];
     #pragma unroll
-                for (int e = 0; e < 4; ++e) v[e] = d + e < dim ? (float)(ps[d + e] * inv) : 0.0f;
+                for (int e = 0; e < 4; ++e) v[e] = d + e < dq ? (float)(qsrc[d + e] * inv) : 0.0f;
                 const size_t o = (size_t)row * q_ld + d;
                 *reinterpret_cast<float4 *>(q_out + o) = make_float4(v[0], v[1], v[2], v[3]);
                 if (g_clear) *reinterpret_cast<float4 *>(g_clear + o) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -687,7 +713,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         if (g_clear)
             for (int d = lane; d < q_ld; d += 32) g_clear[(size_t)row * q_ld + d] = 0.0f;
         for (int d = lane; d < q_ld; d += 32) {
-            const T qv = d < dim ? ps[d] * inv : (T)0;
+            const T qv = d < dq ? qsrc[d] * inv : (T)0;
             q_out[(size_t)row * q_ld + d] = qv;
             if (SPLIT) {
                 const float qf = (float)qv;
@@ -806,14 +832,27 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
         const T nrm = norm_in[row];
         const T *qrow = q_in + (size_t)row * q_ld;
         const GT *grow = g_in + (size_t)row * g_ld;
-        T qg = warp_dot_part<T, GT>(qrow, grow, dim, lane);
+        const int dq = P.dim_out;  // length of q and dE/dq (dim without compression)
+        T qg = warp_dot_part<T, GT>(qrow, grow, dq, lane);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
         const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
         // h = dE/dp = (g - q (q.g)) / |p| into shared memory: independent coalesced loads (the rows
-        // were just read for q.g), so the M entries below are formed at shared-memory latency
-        for (int d = lane; d < dim; d += 32) hb[d] = ((T)grow[d] - qrow[d] * qg) * inv;
+        // were just read for q.g), so the M entries below are formed at shared-memory latency. With
+        // compression this is dE/d(P p), placed after h, and h = P^T of it, each column summed in the
+        // order its entries were given
+        T *hc = P.cmp_row ? hb + dim : hb;
+        for (int d = lane; d < dq; d += 32) hc[d] = ((T)grow[d] - qrow[d] * qg) * inv;
         __syncwarp();
+        if (P.cmp_row) {
+            const T *val = cmp_vals<T>(P, false);
+            for (int j = lane; j < dim; j += 32) {
+                T acc = 0;
+                for (int e = P.cmp_col[j]; e < P.cmp_col[j + 1]; ++e) acc += val[e] * hc[P.cmp_crow[e]];
+                hb[j] = acc;
+            }
+            __syncwarp();
+        }
         // M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l], h = dE/dp = (g - q (q.g)) / |p|, stored
         // as rows n' of n_species blocks of AMB columns (radial index n_off[s] + a in column
         // s AMB + a; columns beyond alpha_max stay zero). M_l is symmetric, so the slice of row n'
@@ -1031,7 +1070,9 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
 inline size_t fwd_warp_bytes(const SoapParams &P, size_t tsz, int astr, int amb)
 {
     const size_t nlm = (size_t)(P.l_max + 1) * (P.l_max + 1);
-    const size_t area = tsz == 8 ? (size_t)fwd_area<double>(astr, P.dim) : (size_t)fwd_area<float>(astr, P.dim);
+    const int dc = P.cmp_row ? P.dim_out : 0;
+    const size_t area =
+        tsz == 8 ? (size_t)fwd_area<double>(astr, P.dim, dc) : (size_t)fwd_area<float>(astr, P.dim, dc);
     return (tsz * (32 * (size_t)amb + area + (size_t)P.n_max * nlm) + 15) / 16 * 16;
 }
 
@@ -1041,7 +1082,9 @@ template <class T> inline size_t bwd_warp_bytes(const SoapParams &P, int amb)
     const int nout = P.n_max * (int)nlm;
     const size_t ms = (size_t)(P.l_max + 1) * bwd_m_pitch<T>(P.n_max, P.n_species * amb);
     const size_t fdf = 2 * (size_t)(P.l_max + 1) * 32;
-    const size_t gf = std::max<size_t>((size_t)P.n_species * nlm * amb + fdf, (size_t)P.dim);  // Gc + f/df, or h
+    // Gc + f/df, or h (and the compressed dE/dp after it)
+    const size_t gf = std::max<size_t>((size_t)P.n_species * nlm * amb + fdf,
+                                       (size_t)P.dim + (P.cmp_row ? (size_t)P.dim_out : 0));
     static_assert(sizeof(GroupStage) % 16 == 0, "the adjoint's arrays after the stage stay 16-byte aligned");
     return sizeof(GroupStage) + (sizeof(T) * ((size_t)bwd_c_elems<T>(nout) + ms + gf) + 15) / 16 * 16;
 }

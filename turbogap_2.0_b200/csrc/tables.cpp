@@ -180,6 +180,10 @@ int make_soap_params(const tgap_soap_hypers *h, SoapParams *p, std::string *why)
     }
     p->n_max = nmax;
     p->dim = nmax * (nmax + 1) / 2 * (h->l_max + 1);
+    p->dim_out = p->dim;
+    p->cmp_row = p->cmp_rcol = p->cmp_col = p->cmp_crow = nullptr;
+    p->cmp_rval = p->cmp_cval = nullptr;
+    p->cmp_rval32 = p->cmp_cval32 = nullptr;
     for (int s = 0; s < h->n_species; ++s) p->tab_scale[s] = (double)kTabIntervals / p->rcut_hard[s];
     p->am_pad = up4(p->max_alpha);
     return TGAP_OK;

@@ -224,6 +224,14 @@ struct SoapParams {
     double sigma_t[kMaxSpecies], sigma_t_scaling[kMaxSpecies];
     double amplitude_scaling[kMaxSpecies], central_weight[kMaxSpecies];
     double rcut_max;
+    // SOAP compression (read_gap.f90:489-559): q = P p / |P p|, P sparse (dim_out x dim); without it
+    // dim_out = dim and the pointers are null. P by rows (output components, for the forward) and by
+    // columns (power-spectrum components, for the adjoint's P^T), each in the order given.
+    int dim_out;
+    const int *cmp_row, *cmp_rcol;  // row offsets [dim_out + 1], column of each entry
+    const int *cmp_col, *cmp_crow;  // column offsets [dim + 1], row of each entry
+    const double *cmp_rval, *cmp_cval;
+    const float *cmp_rval32, *cmp_cval32;
 };
 
 // Host-side tables: quadrature node positions, weighted orthonormal basis values
@@ -246,6 +254,7 @@ struct DeviceSoap {
     float *xq_f = nullptr, *tq_f = nullptr, *central_f = nullptr;  // single-precision copies
     DevBuf xq32, tq32, central32;
     DevBuf rtab;  // float4 [n_species][kTabIntervals][am_pad]: cubic Hermite radial table
+    DevBuf cmp_i, cmp_f64, cmp_f32;  // compression: offsets and indices (int), values (FP64, FP32)
 };
 int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, DeviceSoap *d);
 

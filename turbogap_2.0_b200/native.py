@@ -100,6 +100,8 @@ def lib():
                                     i32, i32, vp, vp, vp, vp]),
         "tgap_assign_species": (i32, [i32, C.c_char_p, i32, C.c_char_p, vp]),
         "tgap_model_create": (i32, [vp, P(SoapHypers), i32, i32, vp, vp, dbl, dbl, P(vp)]),
+        "tgap_model_create_compressed": (i32, [vp, P(SoapHypers), i32, i32, vp, vp, dbl, dbl, i32, i32, vp, vp, vp,
+                                               P(vp)]),
         "tgap_model_destroy": (i32, [vp]),
         "tgap_model_dim": (i32, [vp]),
         "tgap_system_create": (i32, [vp, i32, vp, vp, vp, vp, dbl, P(vp)]),
