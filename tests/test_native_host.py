@@ -232,6 +232,32 @@ def test_gap_file_reader(tg, tmp_path):
     assert g["rcut_max"] == 4.5
 
 
+def test_gap_file_compression(tg, tmp_path):
+    """SOAP compression in a model file (read_gap.f90:489-559): a P_transformation block and the
+    older index-list format give (P_i, P_j, P_el, dim_out); compress_mode without a file is refused
+    when the model is loaded (its recipe is not in the reference sources)."""
+    gf = tg.gap_file
+    (tmp_path / "p.dat").write_text("4 2 3 5\nP_transformation\n1 3 0.5\n2 7 1.0\n1 9 -2.0\n5 1 1.0\n"
+                                    "end_transformation\n")
+    pi, pj, pel, d = gf.read_compress_file(str(tmp_path / "p.dat"), 2)
+    assert d == 5 and list(pi) == [1, 2, 1, 5] and list(pj) == [3, 7, 9, 1] and list(pel) == [0.5, 1.0, -2.0, 1.0]
+    (tmp_path / "old.dat").write_text("8 3 3\n4\n9\n12\n")
+    pi, pj, pel, d = gf.read_compress_file(str(tmp_path / "old.dat"), 1)
+    assert d == 3 and list(pi) == [1, 2, 3] and list(pj) == [4, 9, 12] and list(pel) == [1.0, 1.0, 1.0]
+    (tmp_path / "p1.dat").write_text("8 8 5\nP_transformation\n1 3 0.5\n2 7 1.0\n1 9 -2.0\n5 1 1.0\n"
+                                     "end_transformation\n")
+    gap = tmp_path / "c.gap"
+    gap.write_text("gap_beg soap_turbo\nn_species = 1\nspecies = C\nrcut = 3.7\nn_max = 8\nl_max = 8\n"
+                   "atom_sigma_r = 0.5\natom_sigma_t = 0.5\ncompress_soap = .true.\n"
+                   "file_compress_soap = p1.dat\ngap_end\n")
+    g = gf.read_gap(str(gap), base_dir=str(tmp_path))
+    s = g["soap_turbo"][0]
+    assert s["compress_soap"] and s["compress"][3] == 5 and list(s["compress"][1]) == [3, 7, 9, 1]
+    gap.write_text(gap.read_text().replace("file_compress_soap = p1.dat", "compress_mode = trivial"))
+    g = gf.read_gap(str(gap), base_dir=str(tmp_path))
+    assert g["soap_turbo"][0]["compress"] is None and g["soap_turbo"][0]["compress_mode"] == "trivial"
+
+
 def test_extended_xyz_read_and_round_trip(tg, tmp_path):
     """An extended-XYZ frame as TurboGAP files hold them (case-insensitive keys, quoted Lattice,
     Properties with a column to skip, fix flags and masses), then a write/read round trip of two

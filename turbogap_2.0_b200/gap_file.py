@@ -11,7 +11,10 @@ layouts follow the reference:
     amplitude_scaling 1, central_weight 1, global_scaling 1, zeta 2, delta 1, l_max 8,
     central_species 0; `buffer` is the soft-cutoff width, so rcut_soft = rcut - buffer (rcut when
     the buffer is 0) (:424-432). alphas file: one value per sparse point; desc file: n_sparse x dim
-    values, one per record, descriptor index fastest (:810-827).
+    values, one per record, descriptor index fastest (:810-827). With compress_soap the
+    descriptor is P p / |P p|: file_compress_soap holds P (a P_transformation block or the older
+    index list, :489-529) and dim is its length; a compress_mode recipe without a file is soap_turbo
+    code that the reference sources do not hold, so such a model is refused when loaded.
   * distance_2b / angle_3b: delta 1, sigma 1, buffer 0.5 (not read from the file), kernel_type
     "exp"; alphas file: `alpha cutoff` per sparse point; desc file: 1 (2b) or 3 (3b) values per
     sparse point, one per record (:828-872).
@@ -57,6 +60,32 @@ def _records(path):
         if tok:
             out.append(tok)
     return out
+
+
+def read_compress_file(path, n_species):
+    """SOAP compression file (read_gap.f90:489-529): a first record of n_species + 2 integers, the
+    last the compressed length; then either a `P_transformation` block of `P_i P_j P_el` records up
+    to `end_transformation`, or (the older format) one record per compressed component holding the
+    1-based index of the power-spectrum component it keeps (P_i = i, P_el = 1). Returns
+    (P_i, P_j, P_el, dim_out)."""
+    lines = [ln for ln in _lines(path)]
+    head = _tokens(lines[0])
+    if len(head) < n_species + 2:
+        raise ValueError(f"{path}: the first record needs {n_species + 2} integers")
+    dim_out = int(float(head[n_species + 1]))
+    rest = [_tokens(ln) for ln in lines[1:]]
+    rest = [t for t in rest if t]
+    if rest and rest[0][0] == "P_transformation":
+        pi, pj, pel = [], [], []
+        for t in rest[1:]:
+            if t[0] == "end_transformation":
+                break
+            pi.append(int(float(t[0])))
+            pj.append(int(float(t[1])))
+            pel.append(float(t[2]))
+        return np.array(pi, np.int32), np.array(pj, np.int32), np.array(pel), dim_out
+    pj = np.array([int(float(t[0])) for t in rest[:dim_out]], np.int32)
+    return np.arange(1, dim_out + 1, dtype=np.int32), pj, np.ones(dim_out), dim_out
 
 
 def read_alphas_and_descriptors(file_desc, file_alphas, descriptor_type):
@@ -155,7 +184,8 @@ def _soap_block(recs, path_of):
                amplitude_scaling=[1.0] * ns, central_weight=[1.0] * ns, global_scaling=[1.0] * ns,
                alpha_max=[8] * ns, l_max=8, radial_enhancement=0, species=[""] * ns)
     out = dict(zeta=2.0, delta=1.0, central_species=0, basis="poly3", scaling_mode="polynomial",
-               compress_soap=False, file_alphas=None, file_desc=None, local_properties=[])
+               compress_soap=False, file_compress=None, compress_mode=None, compress=None, file_alphas=None,
+               file_desc=None, local_properties=[])
     lp = dict(n=0, labels=[], desc=[], alphas=[], zetas=[], deltas=[], v0s=[])
     for tok in recs:
         k, v = tok[0], _values(tok)
@@ -178,6 +208,10 @@ def _soap_block(recs, path_of):
             out[k] = v[0]
         elif k == "compress_soap":
             out["compress_soap"] = _bool(v[0])
+        elif k == "file_compress_soap":
+            out["file_compress"] = None if v[0] == "none" else v[0]
+        elif k == "compress_mode":
+            out["compress_mode"] = None if v[0] == "none" else v[0]
         elif k == "alphas_sparse":
             out["file_alphas"] = v[0]
         elif k == "desc_sparse":
@@ -202,6 +236,14 @@ def _soap_block(recs, path_of):
     # the "buffer" is the width of the soft-cutoff region (:424-432)
     hyp["rcut_soft"] = [h if b == 0.0 else h - b for h, b in zip(hyp["rcut_hard"], hyp["rcut_soft"])]
     out["hypers"] = hyp
+    if out["compress_soap"]:
+        # a compression file takes priority over compress_mode (:489-491)
+        if out["file_compress"]:
+            out["compress"] = read_compress_file(path_of(out["file_compress"]), ns)
+        elif out["compress_mode"]:
+            out["compress"] = None  # a soap_turbo recipe (get_compress_indices), resolved on loading
+        else:
+            raise ValueError("compress_soap without file_compress_soap or compress_mode (read_gap.f90:545-548)")
     if out["file_alphas"] and out["file_desc"]:
         out.update(read_alphas_and_descriptors(path_of(out["file_desc"]), path_of(out["file_alphas"]), "soap_turbo"))
     for j in range(lp["n"]):
@@ -288,12 +330,13 @@ def load_soap_models(ctx, gap, precision_ready=True):
     from .api import Model
     models = []
     for m in gap["soap_turbo"]:
-        if m["compress_soap"]:
-            raise NotImplementedError("compressed SOAP models are not supported on this path")
+        if m["compress_soap"] and m["compress"] is None:
+            raise NotImplementedError(f"compress_mode {m['compress_mode']}: its recipe (soap_turbo's "
+                                      "get_compress_indices) is not in the reference sources; give a file_compress_soap")
         if m["basis"] != "poly3":
             raise NotImplementedError(f"basis {m['basis']} is not supported on this path")
         models.append(Model(ctx, m["hypers"], m["Qs"], m["alphas"], m["delta"], m["zeta"],
-                            central_species=m["central_species"]))
+                            central_species=m["central_species"], compress=m["compress"] if m["compress_soap"] else None))
     return models
 
 
