@@ -107,8 +107,10 @@ int tgap_build_neighbors(tgap_context *ctx, int n_sites, int n_sites_supercell,
  *  mask                 n_atom_pairs x n_species, nonzero = neighbor belongs to the channel
  *  basis                "poly3" (poly3gauss: TGAP_ERR_UNSUPPORTED)
  *  scaling_mode         "polynomial"
- *  compress_soap        must be 0 (compression: TGAP_ERR_UNSUPPORTED)
- *  soap                 out, n_soap x n_sites (normalised q)
+ *  compress_soap        with compress_P_* (1-based entries): the descriptor is P p / |P p|
+ *                       (read_gap.f90:489-559), n_soap = the largest P_i
+ *  soap                 out, n_soap x n_sites (normalised q; n_soap the descriptor length,
+ *                       the compressed one with compress_soap)
  *  soap_cart_der        out, 3 x n_soap x n_atom_pairs (dq_i/dr_j; self slot = -sum), or NULL
  *                       when do_derivatives == 0 */
 int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh, int n_species,

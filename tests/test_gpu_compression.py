@@ -83,3 +83,27 @@ def test_identity_compression_equals_the_uncompressed_model(ctx, tg, synth):
     system.close()
     plain.close()
     comp.close()
+
+
+def test_get_soap_with_compression_matches_oracle(ctx, tg, synth):
+    """tgap_get_soap (the get_soap surface) with compress_soap: the compressed descriptor and its
+    Cartesian derivatives against the oracle's compression at the parity bars of get_soap."""
+    import oracle_lib as orc
+    hyp = synth.carbon_hypers()
+    pos, box, sp = synth.diamond_supercell(2, seed=33)
+    rc = max(hyp["rcut_hard"])
+    idx = orc.number_of_unit_cells(*box, rc)
+    small = bool(np.any(idx > 1))
+    pos_sc, sp_sc, a, b, c = orc.set_supercell(pos, sp, idx, *box)
+    nb = orc.build_neighbors(pos_sc, len(pos), a, b, c, rc, sp_sc, small)
+    mask = (nb["neighbor_species"] == 1)[:, None]
+    rng = np.random.default_rng(5)
+    D = synth.soap_dim(hyp)
+    comp = (rng.integers(1, 81, 300), rng.integers(1, D + 1, 300), rng.normal(size=300))
+    comp = (np.concatenate([comp[0], [80]]), np.concatenate([comp[1], [1]]), np.concatenate([comp[2], [1.0]]))
+    q_o, d_o = orc.get_soap(orc.Hypers(dict(hyp, compress=comp + (80,))), nb["n_neigh"], mask, nb["rjs"],
+                            nb["thetas"], nb["phis"])
+    q_g, d_g = ctx.get_soap(hyp, nb["n_neigh"], mask, nb["rjs"], nb["thetas"], nb["phis"], compress=comp)
+    assert q_g.shape == q_o.shape == (len(pos), 80)
+    assert np.max(np.abs(q_g - q_o)) < 1e-12
+    assert np.max(np.abs(d_g - d_o)) < 1e-10

@@ -136,9 +136,10 @@ class Context:
         return dict(n_neigh=nn, neighbors_list=nl, rjs=rjs, xyz=xyz, thetas=th, phis=ph, neighbor_species=nsp)
 
     def get_soap(self, hypers, n_neigh, mask, rjs, thetas, phis, do_derivatives=True, basis="poly3",
-                 scaling_mode="polynomial"):
+                 scaling_mode="polynomial", compress=None):
         """soap_turbo get_soap. mask: (P, n_species) bool. Returns soap (n_sites, D) and,
-        when do_derivatives, soap_cart_der (P, D, 3)."""
+        when do_derivatives, soap_cart_der (P, D, 3). compress: (P_i, P_j, P_el[, dim_out]) 1-based
+        entries of the compression (D is then the largest P_i)."""
         nn = _i32(n_neigh)
         n_sites = nn.shape[0]
         rjs = _f64(rjs)
@@ -147,6 +148,11 @@ class Context:
         m = np.ascontiguousarray(np.asarray(mask, dtype=np.uint8).reshape(P, ns).T)
         nmax = int(np.sum(hypers["alpha_max"]))
         D = nmax * (nmax + 1) // 2 * (int(hypers["l_max"]) + 1)
+        cp = None
+        if compress is not None:
+            cp = (np.ascontiguousarray(compress[0], np.int32), np.ascontiguousarray(compress[1], np.int32),
+                  _f64(compress[2]))
+            D = int(cp[0].max())
         soap = np.zeros((n_sites, D))
         der = np.zeros((P, D, 3)) if do_derivatives else None
         hv = {k: _f64(np.broadcast_to(np.asarray(hypers[k], float), (ns,))) for k in N.HYPER_KEYS}
@@ -157,7 +163,9 @@ class Context:
             ptr(hv["global_scaling"]), ptr(hv["atom_sigma_r"]), ptr(hv["atom_sigma_r_scaling"]),
             ptr(hv["atom_sigma_t"]), ptr(hv["atom_sigma_t_scaling"]), ptr(hv["amplitude_scaling"]),
             int(hypers.get("radial_enhancement", 0)), ptr(hv["central_weight"]), basis.encode(),
-            scaling_mode.encode(), int(do_derivatives), 0, 0, None, None, None, ptr(soap), ptr(der)),
+            scaling_mode.encode(), int(do_derivatives), int(cp is not None), 0 if cp is None else len(cp[0]),
+            None if cp is None else ptr(cp[0]), None if cp is None else ptr(cp[1]),
+            None if cp is None else ptr(cp[2]), ptr(soap), ptr(der)),
             self.h, "tgap_get_soap")
         return soap, der
 

@@ -615,10 +615,6 @@ extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh,
 {
     CHECK_RC(activate(ctx));
     (void)species;
-    (void)compress_P_nonzero;
-    (void)compress_P_i;
-    (void)compress_P_j;
-    (void)compress_P_el;
     if (n_sites < 0 || n_atom_pairs < n_sites || !n_neigh || !mask || !rjs || !thetas || !phis || !soap)
         return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_get_soap: bad arguments");
     if (basis && std::strncmp(basis, "poly3", 5) == 0 && std::strncmp(basis, "poly3gauss", 10) == 0)
@@ -627,7 +623,6 @@ extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh,
         return set_error(ctx, TGAP_ERR_UNSUPPORTED, "basis must be poly3");
     if (scaling_mode && std::strncmp(scaling_mode, "polynomial", 10) != 0)
         return set_error(ctx, TGAP_ERR_UNSUPPORTED, "scaling_mode must be polynomial");
-    if (compress_soap) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "SOAP compression is not implemented");
     if (species_multiplicity)
         for (int i = 0; i < n_sites; ++i)
             if (species_multiplicity[i] > 1)
@@ -677,14 +672,31 @@ extern "C" int tgap_get_soap(tgap_context *ctx, int n_sites, const int *n_neigh,
     o.q = S[5].ptr;
     o.norm = S[6].ptr;
     o.q_ld = P.dim;
+    const bool der = do_derivatives && soap_cart_der;
     CHECK_RC(soap_forward(ctx, ds, pv, nullptr, n_sites, TGAP_FP64, o));
-    CHECK_RC(download(ctx, soap, S[5], (size_t)n_sites * P.dim));
-    if (do_derivatives && soap_cart_der) {
+    if (der) {
         if (S[7].ensure(sizeof(double) * 3 * (size_t)P.dim * np + 8))
             return set_error(ctx, TGAP_ERR_NOMEM, "soap_cart_der (%zu bytes)",
                              sizeof(double) * 3 * (size_t)P.dim * np);
         CHECK_RC(tgap::soap_cart_der(ctx, ds, pv, nullptr, n_sites, o, S[7].as<double>()));
-        CHECK_RC(download(ctx, soap_cart_der, S[7], 3 * (size_t)P.dim * np));
+    }
+    if (!compress_soap) {
+        CHECK_RC(download(ctx, soap, S[5], (size_t)n_sites * P.dim));
+        if (der) CHECK_RC(download(ctx, soap_cart_der, S[7], 3 * (size_t)P.dim * np));
+    } else {
+        // the compression (soap is then n_soap = dim_out x n_sites): the uncompressed q and
+        // derivatives above mapped by P (the launches above already hold the uncompressed params)
+        int dim_out = 0;
+        for (int e = 0; e < compress_P_nonzero; ++e) dim_out = std::max(dim_out, compress_P_i ? compress_P_i[e] : 0);
+        CHECK_RC(upload_compression(ctx, &ds, dim_out, compress_P_nonzero, compress_P_i, compress_P_j, compress_P_el));
+        if (S[8].ensure(sizeof(double) * (size_t)n_sites * dim_out + 8) ||
+            (der && S[9].ensure(sizeof(double) * 3 * (size_t)dim_out * np + 8)))
+            return set_error(ctx, TGAP_ERR_NOMEM, "compressed descriptor");
+        CHECK_RC(soap_compress_rows(ctx, ds, n_sites, S[0].as<int64_t>(), S[5].as<double>(),
+                                    der ? S[7].as<double>() : nullptr, S[8].as<double>(),
+                                    der ? S[9].as<double>() : nullptr));
+        CHECK_RC(download(ctx, soap, S[8], (size_t)n_sites * dim_out));
+        if (der) CHECK_RC(download(ctx, soap_cart_der, S[9], 3 * (size_t)dim_out * np));
     }
     TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
     return TGAP_OK;

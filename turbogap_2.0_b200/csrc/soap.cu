@@ -440,6 +440,84 @@ int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, c
     return TGAP_OK;
 }
 
+// One CTA per site: q_c = P q / |P q| from the normalised uncompressed q (the normalisation of p
+// cancels: P p / |P p| = P q / |P q|) and, for each of the site's pairs, the derivative of that
+// map, dq_c = (P dq - q_c (q_c . P dq)) / |P q| (linear in dq, so the self slot stays minus the sum
+// of the others). Rows of P are summed in the order their entries were given.
+__global__ void __launch_bounds__(128) k_compress_rows(int n_sites, int dim, int dim_out, const int *__restrict__ row,
+                                                       const int *__restrict__ col, const double *__restrict__ val,
+                                                       const int64_t *__restrict__ start, const double *__restrict__ q,
+                                                       const double *__restrict__ der, double *__restrict__ qc_out,
+                                                       double *__restrict__ derc)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double *qc = reinterpret_cast<double *>(smem_raw);  // [dim_out]
+    double *vb = qc + dim_out;                           // [dim_out][3]
+    double *red = vb + 3 * dim_out;                      // [4][4]: per-warp partial sums
+    const int i = blockIdx.x, t = threadIdx.x, lane = t & 31, w = t >> 5;
+    if (i >= n_sites) return;
+    const double *qi = q + (size_t)i * dim;
+    // the block's sum of (up to) three values, in a fixed order
+    auto block_sum3 = [&](double a[3]) {
+#pragma unroll
+        for (int x = 0; x < 3; ++x)
+            for (int o = 16; o > 0; o >>= 1) a[x] += __shfl_xor_sync(0xffffffffu, a[x], o);
+        __syncthreads();
+        if (lane == 0)
+            for (int x = 0; x < 3; ++x) red[4 * w + x] = a[x];
+        __syncthreads();
+        for (int x = 0; x < 3; ++x) a[x] = red[x] + red[4 + x] + red[8 + x] + red[12 + x];
+    };
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int r = t; r < dim_out; r += blockDim.x) {
+        double acc = 0.0;
+        for (int e = row[r]; e < row[r + 1]; ++e) acc += val[e] * qi[col[e]];
+        qc[r] = acc;
+        s[0] += acc * acc;
+    }
+    block_sum3(s);
+    const double nr = sqrt(s[0]), inv = nr > 0.0 ? 1.0 / nr : 0.0;
+    for (int r = t; r < dim_out; r += blockDim.x) {
+        qc[r] *= inv;
+        qc_out[(size_t)i * dim_out + r] = qc[r];
+    }
+    __syncthreads();
+    if (!der) return;
+    for (int64_t k = start[i]; k < start[i + 1]; ++k) {
+        const double *dk = der + (size_t)k * dim * 3;
+        double a[3] = {0.0, 0.0, 0.0};
+        for (int r = t; r < dim_out; r += blockDim.x) {
+            double v[3] = {0.0, 0.0, 0.0};
+            for (int e = row[r]; e < row[r + 1]; ++e)
+                for (int x = 0; x < 3; ++x) v[x] += val[e] * dk[3 * col[e] + x];
+            for (int x = 0; x < 3; ++x) {
+                vb[3 * r + x] = v[x];
+                a[x] += qc[r] * v[x];
+            }
+        }
+        block_sum3(a);
+        double *out = derc + (size_t)k * dim_out * 3;
+        for (int r = t; r < dim_out; r += blockDim.x)
+            for (int x = 0; x < 3; ++x) out[3 * r + x] = (vb[3 * r + x] - qc[r] * a[x]) * inv;
+        __syncthreads();
+    }
+}
+
+int soap_compress_rows(tgap_context *ctx, const DeviceSoap &ds, int n_sites, const int64_t *d_start,
+                       const double *d_q, const double *d_der, double *d_qc, double *d_derc)
+{
+    if (n_sites <= 0) return TGAP_OK;
+    const int dim_out = ds.p.dim_out;
+    const size_t sm = sizeof(double) * (4 * (size_t)dim_out + 16);
+    if (sm > 227 * 1024) return set_error(ctx, TGAP_ERR_UNSUPPORTED, "compressed length %d too large", dim_out);
+    StageScope sc(ctx, "soap_compress_f64");
+    TGAP_CUDA(ctx, cudaFuncSetAttribute(k_compress_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_compress_rows<<<n_sites, 128, sm, ctx->stream>>>(n_sites, ds.p.dim, dim_out, ds.p.cmp_row, ds.p.cmp_rcol,
+                                                       ds.p.cmp_rval, d_start, d_q, d_der, d_qc, d_derc);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
 int upload_soap(tgap_context *ctx, const SoapParams &p, const SoapTables &t, DeviceSoap *d)
 {
     d->p = p;

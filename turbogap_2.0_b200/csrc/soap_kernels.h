@@ -38,5 +38,10 @@ int soap_bwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  double *d_virial);
 int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, const SoapOut &o, double *d_der);
+// SOAP compression of n_sites normalised uncompressed rows q (and, with der, their per-pair
+// derivatives [pair][dim][3]); P by rows in ds.p (CSR). Writes q_c [site][dim_out] and
+// der_c [pair][dim_out][3].
+int soap_compress_rows(tgap_context *ctx, const DeviceSoap &ds, int n_sites, const int64_t *d_start,
+                       const double *d_q, const double *d_der, double *d_qc, double *d_derc);
 
 }  // namespace tgap
