@@ -157,6 +157,21 @@ module tgap_iface
          type(c_ptr), intent(out) :: model
       end function
 
+      ! a model read with compress_soap (read_gap.f90:489-559): compress_P_* as read_gap_hypers fills them
+      integer(c_int) function tgap_model_create_compressed(ctx, hypers, central_species, n_sparse, alphas, &
+                                                           Qs, delta, zeta, dim_out, P_nonzero, P_i, P_j, &
+                                                           P_el, model) &
+         bind(C, name="tgap_model_create_compressed")
+         import :: c_int, c_ptr, c_double, tgap_soap_hypers
+         type(c_ptr), value :: ctx
+         type(tgap_soap_hypers), intent(in) :: hypers
+         integer(c_int), value :: central_species, n_sparse, dim_out, P_nonzero
+         real(c_double), intent(in) :: alphas(*), Qs(*), P_el(*)
+         integer(c_int), intent(in) :: P_i(*), P_j(*)
+         real(c_double), value :: delta, zeta
+         type(c_ptr), intent(out) :: model
+      end function
+
       integer(c_int) function tgap_model_destroy(model) bind(C, name="tgap_model_destroy")
          import :: c_int, c_ptr
          type(c_ptr), value :: model
