@@ -30,6 +30,10 @@ SOURCES = [
     ("soap_fwd_f64.cu", []),
     ("soap_bwd_f32.cu", []),
     ("soap_bwd_f64.cu", []),
+    ("soap_fwd_f32_cmp.cu", []),
+    ("soap_fwd_f64_cmp.cu", []),
+    ("soap_bwd_f32_cmp.cu", []),
+    ("soap_bwd_f64_cmp.cu", []),
     ("gap.cu", []),
     ("gemm_tc.cu", []),
     ("md.cu", []),

@@ -386,8 +386,10 @@ int soap_forward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 {
     if (n_rows <= 0) return TGAP_OK;
     StageScope sc(ctx, precision == TGAP_FP64 ? "soap_forward_f64" : "soap_forward_f32");
-    if (precision == TGAP_FP64) return soap_fwd_f64(ctx, ds, pv, d_sites, n_rows, o);
-    return soap_fwd_f32(ctx, ds, pv, d_sites, n_rows, o);
+    const bool cmp = ds.p.cmp_row != nullptr;
+    if (precision == TGAP_FP64)
+        return (cmp ? soap_fwd_f64_cmp : soap_fwd_f64)(ctx, ds, pv, d_sites, n_rows, o);
+    return (cmp ? soap_fwd_f32_cmp : soap_fwd_f32)(ctx, ds, pv, d_sites, n_rows, o);
 }
 
 int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
@@ -396,9 +398,12 @@ int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, c
 {
     if (n_rows <= 0) return TGAP_OK;
     StageScope sc(ctx, precision == TGAP_FP64 ? "soap_backward_f64" : "soap_backward_f32");
+    const bool cmp = ds.p.cmp_row != nullptr;
     if (precision == TGAP_FP64)
-        return soap_bwd_f64(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
-    return soap_bwd_f32(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, g_is_double, site_struct, d_forces, d_virial);
+        return (cmp ? soap_bwd_f64_cmp : soap_bwd_f64)(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct,
+                                                       d_forces, d_virial);
+    return (cmp ? soap_bwd_f32_cmp : soap_bwd_f32)(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, g_is_double,
+                                                   site_struct, d_forces, d_virial);
 }
 
 // Cubic Hermite coefficients of R_n on interval i of species s from FP64 quadrature values and

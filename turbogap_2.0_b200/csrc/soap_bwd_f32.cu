@@ -8,8 +8,10 @@ int soap_bwd_f32(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  double *d_forces, double *d_virial)
 {
     if (g_is_double)
-        return launch_bwd<float, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
-    return launch_bwd<float, float>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+        return launch_bwd<float, double, false>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces,
+                                                d_virial);
+    return launch_bwd<float, float, false>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces,
+                                           d_virial);
 }
 
 }  // namespace tgap

@@ -7,7 +7,8 @@ int soap_bwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
                  const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                  double *d_virial)
 {
-    return launch_bwd<double, double>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+    return launch_bwd<double, double, false>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces,
+                                             d_virial);
 }
 
 }  // namespace tgap

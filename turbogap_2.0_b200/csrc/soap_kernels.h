@@ -25,17 +25,28 @@ int soap_backward(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, c
                   int n_rows, int precision, const SoapOut &o, const void *d_g, int g_ld,
                   int g_is_double, const int *site_struct, double *d_forces, double *d_virial);
 // Per-precision instantiations of the warp kernels (soap_fwd_f32.cu, soap_fwd_f64.cu,
-// soap_bwd_f32.cu, soap_bwd_f64.cu).
-int soap_fwd_f32(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
-                 SoapOut &o);
-int soap_fwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
-                 SoapOut &o);
+// soap_bwd_f32.cu, soap_bwd_f64.cu) and of their compressed-descriptor forms (the *_cmp.cu files,
+// for a model whose ds.p.cmp_row is set; the uncompressed kernels carry no compression code).
+#define TGAP_SOAP_FWD_DECL(name)                                                                          \
+    int name(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows, \
+             SoapOut &o);
+TGAP_SOAP_FWD_DECL(soap_fwd_f32)
+TGAP_SOAP_FWD_DECL(soap_fwd_f64)
+TGAP_SOAP_FWD_DECL(soap_fwd_f32_cmp)
+TGAP_SOAP_FWD_DECL(soap_fwd_f64_cmp)
+#undef TGAP_SOAP_FWD_DECL
 int soap_bwd_f32(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                  const SoapOut &o, const void *d_g, int g_ld, int g_is_double, const int *site_struct,
                  double *d_forces, double *d_virial);
+int soap_bwd_f32_cmp(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                     const SoapOut &o, const void *d_g, int g_ld, int g_is_double, const int *site_struct,
+                     double *d_forces, double *d_virial);
 int soap_bwd_f64(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                  const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                  double *d_virial);
+int soap_bwd_f64_cmp(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
+                     const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
+                     double *d_virial);
 int soap_cart_der(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites,
                   int n_rows, const SoapOut &o, double *d_der);
 // SOAP compression of n_sites normalised uncompressed rows q (and, with der, their per-pair

@@ -521,7 +521,7 @@ template <class T, bool PERSIST> struct FwdMinCtas {
     static constexpr int value = std::is_same<T, float>::value ? 4 : 0;
 };
 
-template <class T, int L, int AMB, bool SPLIT, bool PERSIST>
+template <class T, int L, int AMB, bool SPLIT, bool PERSIST, bool CMP>
 __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::value) k_soap_fwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
     const T *__restrict__ tq, const float4 *__restrict__ rtab, const T *__restrict__ central,
@@ -544,7 +544,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         T *Rs = reinterpret_cast<T *>(wbase);
         T *As = Rs + 32 * AMB;
         GroupStage *stage = reinterpret_cast<GroupStage *>(As);
-        T *cs = As + fwd_area<T>(ASTR, dim, P.cmp_row ? P.dim_out : 0);
+        T *cs = As + fwd_area<T>(ASTR, dim, CMP ? P.dim_out : 0);
 
         const int site = sites ? sites[row] : row;
         const int64_t kb = start[site], ke = start[site + 1];
@@ -662,7 +662,7 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, FwdMinCtas<T, PERSIST>::val
         // each row summed in the order its entries were given
         const T *qsrc = ps;
         int dq = dim;
-        if (P.cmp_row) {
+        if constexpr (CMP) {
             __syncwarp();
             T *pcs = ps + dim;
             const T *val = cmp_vals<T>(P, true);
@@ -787,7 +787,7 @@ template <class T, bool PERSIST> struct BwdMinCtas {
 // zero beyond alpha_max), f_l / df_l of each lane's pair [2][L+1][32]; h [dim] occupies the area
 // of Gc and f_l / df_l (grown to dim when smaller) until M is formed. After the warps, the CTA's
 // virial partials [kWarpsPerCta][6] and structure ids [kWarpsPerCta].
-template <class T, class GT, int L, int AMB, bool PERSIST>
+template <class T, class GT, int L, int AMB, bool PERSIST, bool CMP>
 __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::value) k_soap_bwd_warp(
     const __grid_constant__ SoapParams P, const __grid_constant__ YlmConst Yc, const T *__restrict__ xq,
     const T *__restrict__ tq, const float4 *__restrict__ rtab, const int *__restrict__ sites, int n_rows,
@@ -832,27 +832,33 @@ __global__ void __launch_bounds__(32 * kWarpsPerCta, BwdMinCtas<T, PERSIST>::val
         const T nrm = norm_in[row];
         const T *qrow = q_in + (size_t)row * q_ld;
         const GT *grow = g_in + (size_t)row * g_ld;
-        const int dq = P.dim_out;  // length of q and dE/dq (dim without compression)
-        T qg = warp_dot_part<T, GT>(qrow, grow, dq, lane);
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
-        const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
         // h = dE/dp = (g - q (q.g)) / |p| into shared memory: independent coalesced loads (the rows
         // were just read for q.g), so the M entries below are formed at shared-memory latency. With
-        // compression this is dE/d(P p), placed after h, and h = P^T of it, each column summed in the
-        // order its entries were given
-        T *hc = P.cmp_row ? hb + dim : hb;
-        for (int d = lane; d < dq; d += 32) hc[d] = ((T)grow[d] - qrow[d] * qg) * inv;
-        __syncwarp();
-        if (P.cmp_row) {
+        // compression q and g have dim_out entries and this is dE/d(P p), placed after h, and h = P^T
+        // of it, each column summed in the order its entries were given
+        if constexpr (!CMP) {
+            T qg = warp_dot_part<T, GT>(qrow, grow, dim, lane);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
+            const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
+            for (int d = lane; d < dim; d += 32) hb[d] = ((T)grow[d] - qrow[d] * qg) * inv;
+        } else {
+            const int dq = P.dim_out;
+            T qg = warp_dot_part<T, GT>(qrow, grow, dq, lane);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) qg += __shfl_xor_sync(0xffffffffu, qg, o);
+            const T inv = nrm > (T)0 ? (T)1 / nrm : (T)0;
+            T *hc = hb + dim;
+            for (int d = lane; d < dq; d += 32) hc[d] = ((T)grow[d] - qrow[d] * qg) * inv;
+            __syncwarp();
             const T *val = cmp_vals<T>(P, false);
             for (int j = lane; j < dim; j += 32) {
                 T acc = 0;
                 for (int e = P.cmp_col[j]; e < P.cmp_col[j + 1]; ++e) acc += val[e] * hc[P.cmp_crow[e]];
                 hb[j] = acc;
             }
-            __syncwarp();
         }
+        __syncwarp();
         // M_l[n][n'] = (2 if n == n' else sqrt 2) h[n n' l], h = dE/dp = (g - q (q.g)) / |p|, stored
         // as rows n' of n_species blocks of AMB columns (radial index n_off[s] + a in column
         // s AMB + a; columns beyond alpha_max stay zero). M_l is symmetric, so the slice of row n'
@@ -1093,12 +1099,13 @@ constexpr size_t kMaxDynSmem = 227 * 1024;
 
 // Autotuner key of a descriptor launch (sites per CTA): kernel, precision, l_max, radial block,
 // bf16 split, and the row count rounded up to a power of two.
-inline std::string warps_key(const char *kind, bool f64, int L, int amb, bool split, int n_rows)
+inline std::string warps_key(const char *kind, bool f64, int L, int amb, bool split, int n_rows, bool cmp)
 {
     int b = 1;
     while (b < n_rows) b <<= 1;
     char k[96];
-    std::snprintf(k, sizeof(k), "soap_%s/%s/l%d/a%d/s%d/rows%d", kind, f64 ? "f64" : "f32", L, amb, (int)split, b);
+    std::snprintf(k, sizeof(k), "soap_%s/%s/l%d/a%d/s%d/rows%d%s", kind, f64 ? "f64" : "f32", L, amb, (int)split, b,
+                  cmp ? "/cmp" : "");
     return k;
 }
 
@@ -1144,7 +1151,7 @@ template <class T> inline const T *soap_tab(const DevBuf &d64, const DevBuf &d32
     return std::is_same<T, double>::value ? (const T *)d64.ptr : (const T *)d32.ptr;
 }
 
-template <class T, bool SPLIT, int L, int AMB>
+template <class T, bool SPLIT, bool CMP, int L, int AMB>
 int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                  SoapOut &o)
 {
@@ -1153,13 +1160,13 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     const int nw_max = (int)std::min<size_t>(kWarpsPerCta, kMaxDynSmem / wb);
     if (nw_max < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor forward needs %zu bytes of shared memory", wb);
     const bool f64 = std::is_same<T, double>::value;
-    const int nw = tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows), f64 ? "soap_forward_f64" : "soap_forward_f32",
-                         warp_candidates(nw_max), nw_max);
+    const std::string key = warps_key("fwd", f64, L, AMB, SPLIT, n_rows, CMP);
+    const int nw = tuned(ctx, key, f64 ? "soap_forward_f64" : "soap_forward_f32", warp_candidates(nw_max), nw_max);
     const bool persist =
-        pv.queue && tuned(ctx, warps_key("fwd", f64, L, AMB, SPLIT, n_rows) + "/persist",
+        pv.queue && tuned(ctx, key + "/persist",
                           f64 ? "soap_forward_f64" : "soap_forward_f32", {0, 1}, f64 ? 0 : 1);
     const size_t sm = wb * nw;
-    auto kern = persist ? k_soap_fwd_warp<T, L, AMB, SPLIT, true> : k_soap_fwd_warp<T, L, AMB, SPLIT, false>;
+    auto kern = persist ? k_soap_fwd_warp<T, L, AMB, SPLIT, true, CMP> : k_soap_fwd_warp<T, L, AMB, SPLIT, false, CMP>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = site_grid((const void *)kern, nw, sm, n_rows, persist);
     TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
@@ -1171,7 +1178,7 @@ int launch_fwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     return TGAP_OK;
 }
 
-template <class T, class GT, int L, int AMB>
+template <class T, class GT, bool CMP, int L, int AMB>
 int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                  const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                  double *d_virial)
@@ -1181,13 +1188,13 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
     const int nw_max = (int)std::min<size_t>(kWarpsPerCta, (kMaxDynSmem - tail) / wb);
     if (nw_max < 1) return set_error(ctx, TGAP_ERR_HYPERS, "descriptor adjoint needs %zu bytes of shared memory", wb);
     const bool f64 = std::is_same<T, double>::value;
-    const int nw = tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows), f64 ? "soap_backward_f64" : "soap_backward_f32",
-                         warp_candidates(nw_max), nw_max);
+    const std::string key = warps_key("bwd", f64, L, AMB, false, n_rows, CMP);
+    const int nw = tuned(ctx, key, f64 ? "soap_backward_f64" : "soap_backward_f32", warp_candidates(nw_max), nw_max);
     const bool persist =
-        pv.queue && tuned(ctx, warps_key("bwd", f64, L, AMB, false, n_rows) + "/persist",
+        pv.queue && tuned(ctx, key + "/persist",
                           f64 ? "soap_backward_f64" : "soap_backward_f32", {0, 1}, f64 ? 0 : 1);
     const size_t sm = wb * nw + tail;
-    auto kern = persist ? k_soap_bwd_warp<T, GT, L, AMB, true> : k_soap_bwd_warp<T, GT, L, AMB, false>;
+    auto kern = persist ? k_soap_bwd_warp<T, GT, L, AMB, true, CMP> : k_soap_bwd_warp<T, GT, L, AMB, false, CMP>;
     TGAP_CUDA(ctx, cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
     const int grid = site_grid((const void *)kern, nw, sm, n_rows, persist);
     TGAP_CUDA(ctx, launch_pdl(kern, dim3(grid), dim3(32 * nw), sm, ctx->stream, ds.p, ylm_host_constants(),
@@ -1203,20 +1210,20 @@ int launch_bwd_l(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, co
 static_assert(kMaxL == 10, "TGAP_FOR_EACH_L lists l_max = 0..10");
 static_assert(kMaxAlpha <= 16, "radial blocks are instantiated for alpha_max <= 8 and <= 16");
 
-template <class T, bool SPLIT, int AMB>
+template <class T, bool SPLIT, bool CMP, int AMB>
 int launch_fwd_amb(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                    SoapOut &o)
 {
     switch (ds.p.l_max) {
 #define TGAP_CASE(l) \
-    case l: return launch_fwd_l<T, SPLIT, l, AMB>(ctx, ds, pv, d_sites, n_rows, o);
+    case l: return launch_fwd_l<T, SPLIT, CMP, l, AMB>(ctx, ds, pv, d_sites, n_rows, o);
         TGAP_FOR_EACH_L(TGAP_CASE)
 #undef TGAP_CASE
     }
     return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
 }
 
-template <class T, class GT, int AMB>
+template <class T, class GT, bool CMP, int AMB>
 int launch_bwd_amb(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                    const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                    double *d_virial)
@@ -1224,30 +1231,34 @@ int launch_bwd_amb(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, 
     switch (ds.p.l_max) {
 #define TGAP_CASE(l)                                                                                          \
     case l:                                                                                                   \
-        return launch_bwd_l<T, GT, l, AMB>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, \
-                                           d_virial);
+        return launch_bwd_l<T, GT, CMP, l, AMB>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, \
+                                                d_forces, d_virial);
         TGAP_FOR_EACH_L(TGAP_CASE)
 #undef TGAP_CASE
     }
     return set_error(ctx, TGAP_ERR_HYPERS, "l_max %d out of range", ds.p.l_max);
 }
 
-template <class T, bool SPLIT>
+// CMP: the model's descriptor is compressed (ds.p.cmp_row set); the compressed kernels are
+// instantiated in translation units of their own.
+template <class T, bool SPLIT, bool CMP>
 int launch_fwd(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                SoapOut &o)
 {
-    if (ds.p.max_alpha <= 8) return launch_fwd_amb<T, SPLIT, 8>(ctx, ds, pv, d_sites, n_rows, o);
-    return launch_fwd_amb<T, SPLIT, 16>(ctx, ds, pv, d_sites, n_rows, o);
+    if (ds.p.max_alpha <= 8) return launch_fwd_amb<T, SPLIT, CMP, 8>(ctx, ds, pv, d_sites, n_rows, o);
+    return launch_fwd_amb<T, SPLIT, CMP, 16>(ctx, ds, pv, d_sites, n_rows, o);
 }
 
-template <class T, class GT>
+template <class T, class GT, bool CMP>
 int launch_bwd(tgap_context *ctx, const DeviceSoap &ds, const PairView &pv, const int *d_sites, int n_rows,
                const SoapOut &o, const void *d_g, int g_ld, const int *site_struct, double *d_forces,
                double *d_virial)
 {
     if (ds.p.max_alpha <= 8)
-        return launch_bwd_amb<T, GT, 8>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
-    return launch_bwd_amb<T, GT, 16>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces, d_virial);
+        return launch_bwd_amb<T, GT, CMP, 8>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces,
+                                             d_virial);
+    return launch_bwd_amb<T, GT, CMP, 16>(ctx, ds, pv, d_sites, n_rows, o, d_g, g_ld, site_struct, d_forces,
+                                          d_virial);
 }
 
 }  // namespace tgap
