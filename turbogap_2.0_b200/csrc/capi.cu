@@ -70,6 +70,12 @@ int HostBuf::ensure(size_t n)
         ptr = nullptr;
         return 1;
     }
+    if (cudaHostGetDevicePointer(&dev, ptr, 0) != cudaSuccess) {
+        cudaGetLastError();
+        cudaFreeHost(ptr);
+        ptr = dev = nullptr;
+        return 1;
+    }
     bytes = n < 256 ? 256 : n;
     return 0;
 }
@@ -77,7 +83,7 @@ int HostBuf::ensure(size_t n)
 void HostBuf::release()
 {
     if (ptr) cudaFreeHost(ptr);
-    ptr = nullptr;
+    ptr = dev = nullptr;
     bytes = 0;
 }
 
@@ -234,7 +240,7 @@ extern "C" int tgap_destroy(tgap_context *ctx)
     cudaStreamSynchronize(ctx->stream);
     for (auto &b : ctx->scratch) b.release();
     for (auto &b : ctx->pinned) b.release();
-    for (auto &r : ctx->registered) cudaHostUnregister(reinterpret_cast<void *>(r.first));
+    for (auto &r : ctx->registered) cudaHostUnregister(reinterpret_cast<void *>(r.host));
     for (auto &r : ctx->pending) {
         cudaEventDestroy(r.start);
         cudaEventDestroy(r.stop);
@@ -251,8 +257,14 @@ extern "C" int tgap_host_register(tgap_context *ctx, void *ptr, size_t bytes)
 {
     CHECK_RC(activate(ctx));
     if (!ptr || bytes == 0) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_host_register: bad arguments");
-    TGAP_CUDA(ctx, cudaHostRegister(ptr, bytes, cudaHostRegisterDefault));
-    ctx->registered.emplace_back(reinterpret_cast<uintptr_t>(ptr), bytes);
+    TGAP_CUDA(ctx, cudaHostRegister(ptr, bytes, cudaHostRegisterMapped));
+    void *dev = nullptr;
+    const cudaError_t e = cudaHostGetDevicePointer(&dev, ptr, 0);
+    if (e != cudaSuccess) {
+        cudaHostUnregister(ptr);
+        return cuda_check(ctx, e, "cudaHostGetDevicePointer");
+    }
+    ctx->registered.push_back({reinterpret_cast<uintptr_t>(ptr), bytes, reinterpret_cast<uintptr_t>(dev)});
     return TGAP_OK;
 }
 
@@ -260,7 +272,7 @@ extern "C" int tgap_host_unregister(tgap_context *ctx, void *ptr)
 {
     CHECK_RC(activate(ctx));
     for (size_t i = 0; i < ctx->registered.size(); ++i)
-        if (ctx->registered[i].first == reinterpret_cast<uintptr_t>(ptr)) {
+        if (ctx->registered[i].host == reinterpret_cast<uintptr_t>(ptr)) {
             TGAP_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
             TGAP_CUDA(ctx, cudaHostUnregister(ptr));
             ctx->registered.erase(ctx->registered.begin() + (long)i);
@@ -270,14 +282,51 @@ extern "C" int tgap_host_unregister(tgap_context *ctx, void *ptr)
     return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_host_unregister: not registered");
 }
 
-// [p, p + len) lies inside memory registered with tgap_host_register
-static bool host_registered(const tgap_context *ctx, const void *p, size_t len)
+// The device address of [p, p + len) when it lies inside memory registered with
+// tgap_host_register, else null.
+static void *host_registered(const tgap_context *ctx, const void *p, size_t len)
 {
     const uintptr_t a = reinterpret_cast<uintptr_t>(p);
     for (const auto &r : ctx->registered)
-        if (a >= r.first && a + len <= r.first + r.second) return true;
-    return false;
+        if (a >= r.host && a + len <= r.host + r.bytes) return reinterpret_cast<void *>(r.dev + (a - r.host));
+    return nullptr;
 }
+
+// Up to four 8-byte word arrays copied in one launch between device memory and mapped host memory
+// (the caller's registered arrays or the pinned staging buffers), and up to two word arrays
+// cleared: in a call graph one kernel costs less than a copy or memset node per array.
+struct WordCopy {
+    const unsigned long long *src[4];
+    unsigned long long *dst[4];
+    long long n[4];
+    unsigned long long *zero[2];
+    long long nz[2];
+};
+
+__global__ void k_copy_words(WordCopy c)
+{
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+        for (long long i = t; i < c.n[a]; i += stride) c.dst[a][i] = c.src[a][i];
+#pragma unroll
+    for (int a = 0; a < 2; ++a)
+        for (long long i = t; i < c.nz[a]; i += stride) c.zero[a][i] = 0ull;
+}
+
+static int copy_words(tgap_context *ctx, const WordCopy &c)
+{
+    long long most = 0;
+    for (int a = 0; a < 4; ++a) most = std::max(most, c.n[a]);
+    for (int a = 0; a < 2; ++a) most = std::max(most, c.nz[a]);
+    if (most == 0) return TGAP_OK;
+    const int grid = (int)std::min<long long>((most + 255) / 256, 2 * 148);
+    k_copy_words<<<grid, 256, 0, ctx->stream>>>(c);
+    TGAP_LAUNCH_CHECK(ctx);
+    return TGAP_OK;
+}
+
 
 extern "C" int tgap_set_stream(tgap_context *ctx, void *stream)
 {
@@ -1079,13 +1128,44 @@ extern "C" int tgap_velocity_verlet_host(int n_sites, double *positions, double 
     if (n_sites < 0 || (n_sites > 0 && (!positions || !velocities || !forces || !forces_prev || !masses)))
         return TGAP_ERR_ARGUMENT;
     const size_t n3 = 3 * (size_t)n_sites;
-    for (size_t g = 0; g < n3; ++g)
-        if (!std::isfinite(forces[g])) return TGAP_ERR_NUMERIC;
+    // non-finite forces: an exponent field of all ones, as one branch-free pass
+    uint64_t bad = 0;
+    for (size_t g = 0; g < n3; ++g) {
+        uint64_t b;
+        std::memcpy(&b, forces + g, sizeof(b));
+        bad |= (uint64_t)(((b >> 52) & 0x7ff) == 0x7ff);
+    }
+    if (bad) return TGAP_ERR_NUMERIC;
     // one reciprocal mass per atom instead of a division per component (within an ulp of the
-    // divided form)
-    for (int i = 0; i < n_sites; ++i) {
+    // divided form); atoms in pairs, whose six components are three 2-wide vectors
+    typedef double v2d __attribute__((vector_size(16)));
+    const auto ld = [](const double *p) {
+        v2d v;
+        std::memcpy(&v, p, sizeof(v));
+        return v;
+    };
+    const auto st = [](double *p, v2d v) { std::memcpy(p, &v, sizeof(v)); };
+    const double hv = first_step ? 0.0 : 0.5 * dt_prev, hx = 0.5 * (dt * dt);
+    const v2d vdt = {dt, dt};
+    int i = 0;
+    for (; i + 1 < n_sites; i += 2) {
+        const double im0 = 1.0 / masses[i], im1 = 1.0 / masses[i + 1];
+        const double cv0 = hv * im0, cv1 = hv * im1, cx0 = hx * im0, cx1 = hx * im1;
+        const v2d cv[3] = {{cv0, cv0}, {cv0, cv1}, {cv1, cv1}}, cx[3] = {{cx0, cx0}, {cx0, cx1}, {cx1, cx1}};
+        for (int k = 0; k < 3; ++k) {
+            const size_t g = 3 * (size_t)i + 2 * k;
+            const v2d fg = ld(forces + g);
+            const v2d v = ld(velocities + g) + (fg + ld(forces_prev + g)) * cv[k];
+            st(velocities + g, v);
+            const v2d x = ld(positions + g);
+            if (positions_prev) st(positions_prev + g, x);
+            st(forces_prev + g, fg);
+            st(positions + g, x + v * vdt + fg * cx[k]);
+        }
+    }
+    for (; i < n_sites; ++i) {
         const double im = 1.0 / masses[i];
-        const double cv = first_step ? 0.0 : 0.5 * dt_prev * im, cx = 0.5 * (dt * dt) * im;
+        const double cv = hv * im, cx = hx * im;
         for (int c = 0; c < 3; ++c) {
             const size_t g = 3 * (size_t)i + c;
             const double fg = forces[g];
@@ -1503,12 +1583,25 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     if (n_models <= 0 || !models) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: bad model list");
     for (int i = 0; i < n_models; ++i)
         if (!models[i]) return set_error(ctx, TGAP_ERR_ARGUMENT, "tgap_calculate_gap_soap: null model");
-    // registered caller arrays are copied to and from directly, others through the staging buffers
-    const bool direct_in = positions && host_registered(ctx, positions, sizeof(double) * 3 * (size_t)N);
-    const bool direct_out = host_registered(ctx, energies, sizeof(double) * N) &&
-                            (!forces || host_registered(ctx, forces, sizeof(double) * 3 * (size_t)N)) &&
-                            (!virial || host_registered(ctx, virial, sizeof(double) * 9 * (size_t)nst));
-    if (positions && !direct_in) std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
+    // registered caller arrays are read and written directly, others through the staging buffers;
+    // either way by a copy kernel over their device addresses
+    void *in_dev = positions ? host_registered(ctx, positions, sizeof(double) * 3 * (size_t)N) : nullptr;
+    void *out_dev[3] = {host_registered(ctx, energies, sizeof(double) * N),
+                        forces ? host_registered(ctx, forces, sizeof(double) * 3 * (size_t)N) : nullptr,
+                        virial ? host_registered(ctx, virial, sizeof(double) * 9 * (size_t)nst) : nullptr};
+    const bool direct_in = in_dev != nullptr;
+    const bool direct_out = out_dev[0] && (!forces || out_dev[1]) && (!virial || out_dev[2]);
+    if (positions && !direct_in) {
+        std::memcpy(ctx->pinned[0].ptr, positions, sizeof(double) * 3 * (size_t)N);
+        in_dev = ctx->pinned[0].dev;
+    }
+    void *stage_dev = ctx->pinned[1].dev;  // the output staging buffer: energies, forces, virial, pair count
+    if (!direct_out) {
+        double *st = static_cast<double *>(stage_dev);
+        out_dev[0] = st;
+        out_dev[1] = st + N;
+        out_dev[2] = st + 4 * (size_t)N;
+    }
     const bool on_device = rebuild && device_rebuild && s->nb.list.ptr && s->nb.n_pairs > 0;
     const bool host_rebuild = rebuild && !on_device;
     const bool geom = !host_rebuild && can_fuse_geometry(s, n_models, models);
@@ -1517,9 +1610,26 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
     // the device work of the call, stream-ordered; with a host rebuild (a host synchronization for
     // the pair count) it cannot be captured
     auto device_work = [&]() -> int {
-        if (positions)
-            TGAP_CUDA(ctx, cudaMemcpyAsync(s->nb.positions.ptr, direct_in ? positions : ctx->pinned[0].ptr,
-                                           sizeof(double) * 3 * (size_t)N, cudaMemcpyHostToDevice, ctx->stream));
+        double *d_e = s->scratch_forces.as<double>();
+        double *d_f = d_e + N;
+        double *d_v = d_f + 3 * (size_t)N;
+        // (more models than the counters cover: the descriptor launches without the work queue)
+        const bool counters = 2 * n_models <= kQueueInts;
+        {
+            // the positions in; energies, forces and virial (one buffer) and the site counters cleared
+            WordCopy in{};
+            if (positions) {
+                in.src[0] = static_cast<const unsigned long long *>(in_dev);
+                in.dst[0] = s->nb.positions.as<unsigned long long>();
+                in.n[0] = 3 * (long long)N;
+            }
+            in.zero[0] = reinterpret_cast<unsigned long long *>(d_e);
+            in.nz[0] = (long long)(out_bytes / sizeof(unsigned long long));
+            static_assert(kQueueInts % 2 == 0, "the site counters clear as 8-byte words");
+            in.zero[1] = s->queue.as<unsigned long long>();
+            in.nz[1] = counters ? kQueueInts / 2 : 0;
+            CHECK_RC(copy_words(ctx, in));
+        }
         if (on_device) {
             CHECK_RC(neighbors_sync_positions(ctx, &s->nb));
             CHECK_RC(neighbors_rebuild_lists_device(ctx, &s->nb, false));
@@ -1528,30 +1638,23 @@ static int calculate_gap_soap(tgap_context *ctx, tgap_system *s, int n_models, t
         } else if (!geom) {
             CHECK_RC(tgap_system_update(s, host_rebuild ? 1 : 0));
         }
-        double *d_e = s->scratch_forces.as<double>();
-        double *d_f = d_e + N;
-        double *d_v = d_f + 3 * (size_t)N;
-        // energies, forces and virial are one buffer: one clear, and one for the site counters
-        TGAP_CUDA(ctx, cudaMemsetAsync(d_e, 0, out_bytes, ctx->stream));
-        // (more models than the counters cover: the descriptor launches without the work queue)
-        const bool counters = 2 * n_models <= kQueueInts;
-        if (counters) TGAP_CUDA(ctx, cudaMemsetAsync(s->queue.ptr, 0, sizeof(int) * kQueueInts, ctx->stream));
         CHECK_RC(compute_models(ctx, s, n_models, models, precision, do_forces, d_e, d_f, d_v, geom, true,
                                 counters ? s->queue.as<int>() : nullptr));
-        if (direct_out) {
-            TGAP_CUDA(ctx, cudaMemcpyAsync(energies, d_e, sizeof(double) * N, cudaMemcpyDeviceToHost, ctx->stream));
-            if (forces)
-                TGAP_CUDA(ctx, cudaMemcpyAsync(forces, d_f, sizeof(double) * 3 * (size_t)N, cudaMemcpyDeviceToHost,
-                                               ctx->stream));
-            if (virial)
-                TGAP_CUDA(ctx, cudaMemcpyAsync(virial, d_v, sizeof(double) * 9 * (size_t)nst, cudaMemcpyDeviceToHost,
-                                               ctx->stream));
-        } else {
-            TGAP_CUDA(ctx, cudaMemcpyAsync(h, d_e, out_bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        // energies, forces, virial and (after a rebuild) the unclamped pair count, in one launch
+        WordCopy out{};
+        const double *src[3] = {d_e, d_f, d_v};
+        const long long len[3] = {N, forces ? 3 * (long long)N : 0, virial ? 9 * (long long)nst : 0};
+        for (int a = 0; a < 3; ++a) {
+            out.src[a] = reinterpret_cast<const unsigned long long *>(src[a]);
+            out.dst[a] = static_cast<unsigned long long *>(out_dev[a]);
+            out.n[a] = out_dev[a] ? len[a] : 0;
         }
-        if (on_device)  // the rebuild's unclamped pair count
-            TGAP_CUDA(ctx, cudaMemcpyAsync(h + out_bytes, s->nb.counts.as<int64_t>() + N, sizeof(int64_t),
-                                           cudaMemcpyDeviceToHost, ctx->stream));
+        if (on_device) {
+            out.src[3] = reinterpret_cast<const unsigned long long *>(s->nb.counts.as<int64_t>() + N);
+            out.dst[3] = reinterpret_cast<unsigned long long *>(static_cast<unsigned char *>(stage_dev) + out_bytes);
+            out.n[3] = 1;
+        }
+        CHECK_RC(copy_words(ctx, out));
         return TGAP_OK;
     };
     // A configuration (models, precision, rebuild on the device or not, geometry fused or not,

@@ -47,6 +47,7 @@ struct DevBuf {
 // Pinned host staging buffer.
 struct HostBuf {
     void *ptr = nullptr;
+    void *dev = nullptr;  // its address in the device's address space (pinned memory is mapped)
     size_t bytes = 0;
     int ensure(size_t n);
     void release();
@@ -71,8 +72,13 @@ struct tgap_context {
     // scratch buffers reused across calls (host-buffer entry points)
     tgap::DevBuf scratch[24];
     tgap::HostBuf pinned[4];
-    // caller arrays page-locked with tgap_host_register: (address, bytes)
-    std::vector<std::pair<uintptr_t, size_t>> registered;
+    // caller arrays page-locked (and mapped) with tgap_host_register
+    struct HostRegion {
+        uintptr_t host;
+        size_t bytes;
+        uintptr_t dev;  // its address in the device's address space
+    };
+    std::vector<HostRegion> registered;
     int *d_flag = nullptr;  // device error flag (bounded waits, overflow)
     int *d_check = nullptr; // device check word: code, index, value, failures (int[4])
     bool sync_check = false;  // TGAP_SYNC_CHECK=1: synchronize and read the check after each launch
