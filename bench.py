@@ -448,7 +448,9 @@ def _e2e(tg, ctx, system, model, masses, vel, pos0, precision, steps):
                                        pvir)
         native.check(st, ctx.h, "tgap_calculate_gap_soap")
 
-    for k in range(3):  # warm-up
+    # warm-up: both call configurations (with and without the list rebuild) run eagerly once and
+    # are captured as graphs, as in any MD loop after its first two rebuild intervals
+    for k in range(2 * REBUILD + 2):
         force(k)
     x[:] = pos0
     t0 = time.perf_counter()
