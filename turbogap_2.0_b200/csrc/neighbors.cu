@@ -99,14 +99,14 @@ __device__ __forceinline__ unsigned nb_lanemask_lt()
 constexpr int kStageW = 96;
 
 // One warp per site; FILL=false counts the site's pairs, FILL=true writes them in the
-// reference order. Linked-cell path: lane c < 27 owns neighbor cell c of the z -> y -> x
-// traversal (c = 9 dz + 3 dy + dx), walks its members in decreasing index, and a warp scan
-// of the per-cell counts gives each lane its offset in the site's list. Brute-force path:
-// the warp strides over the supercell in ascending order and compacts with a ballot.
-// With stage (int [n_atoms][kStageW]) and staged (int [n_atoms]) given, the count pass stages the
-// rows that fit (the second walk of the cells reads what the first just brought into L1) and
-// marks them; the fill pass copies a marked row to its place in the list (bounded by the site's
-// offsets) and walks the cells only for the other sites.
+// reference order. Linked-cell path: lane c < 27 finds neighbor cell c of the z -> y -> x
+// traversal (c = 9 dz + 3 dy + dx) and its member range (members in decreasing index); a warp
+// scan of the ranges' lengths lays the 27 cells' candidates end to end, and the warp tests them
+// 32 at a time, each accepted pair placed by a ballot prefix, which keeps the cell-by-cell order.
+// Brute-force path: the warp strides over the supercell in ascending order and compacts with a
+// ballot. With stage (int [n_atoms][kStageW]) and staged (int [n_atoms]) given, the count pass
+// also writes the rows that fit and marks them; the fill pass copies a marked row to its place in
+// the list (bounded by the site's offsets) and walks the cells only for the other sites.
 template <bool FILL>
 __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int *site_struct,
                                                     const StructDesc *sd, const double *pos_sc,
@@ -152,49 +152,51 @@ __global__ void __launch_bounds__(128) k_site_pairs(int n_atoms_total, const int
             if (!skip)
                 c = S.cell_off + i_modulo(i3 - 1, mx) + i_modulo(j3 - 1, my) * mx + i_modulo(k3 - 1, mz) * mx * my;
         }
-        const int t0 = c >= 0 ? cell_start[c] : 0, t1 = c >= 0 ? cell_start[c + 1] : 0;
-        int cnt = 0;
-        for (int t = t0; t < t1; ++t) {
-            const int k = cell_atoms[t];
-            if (k == i) continue;
-            double dist[3], d;
-            get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
-            if (d < rc) ++cnt;
-        }
-        int incl = cnt;
+        const int t0 = c >= 0 ? cell_start[c] : 0, nc = c >= 0 ? cell_start[c + 1] - t0 : 0;
+        // the candidates of the 27 cells in traversal order (cell by lane, then the cell's sorted
+        // atoms) are walked 32 at a time: lane u takes candidate b + u, the accepted ones keep their
+        // order through a ballot, so the list comes out as a cell-by-cell walk would write it
+        int incl = nc;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int v = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += v;
         }
-        if (!FILL) {
-            const int total = __shfl_sync(0xffffffffu, incl, 31);
-            if (lane == 0) counts[g] = 1 + total;
-            if (stage) {
-                const bool fits = 1 + total <= kStageW;
-                if (fits) {
-                    int *row = stage + (size_t)g * kStageW;
-                    if (lane == 0) row[0] = i;
-                    int w = 1 + (incl - cnt);
-                    for (int t = t0; t < t1; ++t) {
-                        const int k = cell_atoms[t];
-                        if (k == i) continue;
-                        double dist[3], d;
-                        get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
-                        if (d < rc) row[w++] = k;
-                    }
+        const int total = __shfl_sync(0xffffffffu, incl, 31);
+        int *row = !FILL && stage ? stage + (size_t)g * kStageW : nullptr;
+        if (row && lane == 0) row[0] = i;
+        int acc = 0;  // pairs accepted so far (the self entry not counted)
+        for (int b = 0; b < total; b += 32) {
+            const int u = b + lane;
+            // the cell holding candidate u: the first lane whose inclusive count exceeds u
+            int L = 0;
+#pragma unroll
+            for (int st = 16; st > 0; st >>= 1)
+                if (__shfl_sync(0xffffffffu, incl, L + st - 1) <= u) L += st;
+            const int base = __shfl_sync(0xffffffffu, t0, L) - __shfl_sync(0xffffffffu, incl - nc, L);
+            bool ok = false;
+            int k = 0;
+            if (u < total) {
+                k = cell_atoms[base + u];
+                if (k != i) {
+                    double dist[3], d;
+                    get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
+                    ok = d < rc;
                 }
-                if (lane == 0) staged[g] = fits ? 1 : 0;
             }
-        } else {
-            int64_t w = w0 + 1 + (incl - cnt);
-            for (int t = t0; t < t1; ++t) {
-                const int k = cell_atoms[t];
-                if (k == i) continue;
-                double dist[3], d;
-                get_distance_dev(pi, pos_sc + 3 * (size_t)(S.sc_off + k - 1), S, dist, &d);
-                if (d < rc) put(w++, k);
+            const unsigned m = __ballot_sync(0xffffffffu, ok);
+            const int w = 1 + acc + __popc(m & nb_lanemask_lt());
+            if (ok) {
+                if (FILL)
+                    put(w0 + w, k);
+                else if (row && w < kStageW)
+                    row[w] = k;
             }
+            acc += __popc(m);
+        }
+        if (!FILL && lane == 0) {
+            counts[g] = 1 + acc;
+            if (staged) staged[g] = row && 1 + acc <= kStageW ? 1 : 0;
         }
     } else {
         int64_t w = w0 + 1, n = 1;
