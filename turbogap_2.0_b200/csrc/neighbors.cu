@@ -322,6 +322,49 @@ __global__ void k_fit_pairs(int n, int64_t *start, int *n_neigh, int64_t cap, in
     }
 }
 
+// Systems up to this many sites take the list offsets and the capacity fit from one launch.
+constexpr int kScanFitMax = 32768;
+
+// The small-system form of the offset scan and k_fit_pairs in one CTA: start[0, n] = the exclusive
+// sum of the per-site counts (start[n] the total, also kept in *total), then the same capacity fit.
+// Thread t scans the contiguous chunk [t per, (t + 1) per) of the sites.
+__global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *counts, int64_t *start, int *n_neigh,
+                                                         int64_t cap, int *check, int64_t *total)
+{
+    __shared__ int64_t part[1024];
+    __shared__ int over;
+    const int T = blockDim.x, t = threadIdx.x;
+    const int per = (n + T - 1) / T;
+    const int b = min(n, t * per), e = min(n, b + per);
+    int64_t sum = 0;
+    for (int i = b; i < e; ++i) sum += counts[i];
+    part[t] = sum;
+    __syncthreads();
+    for (int o = 1; o < T; o <<= 1) {
+        const int64_t v = t >= o ? part[t - o] : 0;
+        __syncthreads();
+        part[t] += v;
+        __syncthreads();
+    }
+    const int64_t tot = part[T - 1];
+    if (t == 0) {
+        *total = tot;
+        over = tot > cap;
+        if (over) check_fail(check, kCheckPairCapacity, n, (long long)tot);
+    }
+    __syncthreads();
+    const int64_t lim = cap - 1;
+    int64_t a = part[t] - sum;
+    for (int i = b; i < e; ++i) {
+        const int64_t z = a + counts[i];
+        const int64_t a2 = over && a > lim ? lim : a, z2 = over && z > lim ? lim : z;
+        start[i] = a2;
+        n_neigh[i] = (int)(z2 - a2);
+        a = z;
+    }
+    if (t == T - 1) start[n] = over && tot > lim ? lim : tot;
+}
+
 static int scan_i64(tgap_context *ctx, DevBuf &tmp, const int64_t *in, int64_t *out, int n)
 {
     size_t bytes = 0;
@@ -413,7 +456,8 @@ int make_struct_desc(const double a[3], const double b[3], const double c[3], in
 
 // The counting half of a rebuild: cell lists, per-site pair counts and their exclusive scan
 // (start[0..n]). Stream-ordered only.
-static int rebuild_count(tgap_context *ctx, NeighborBatch *nb)
+// scan = false leaves the offsets to the caller (counts only).
+static int rebuild_count(tgap_context *ctx, NeighborBatch *nb, bool scan = true)
 {
     const int n = nb->n_atoms;
     const int T = 128;
@@ -445,6 +489,7 @@ static int rebuild_count(tgap_context *ctx, NeighborBatch *nb)
                                                       nb->counts.as<int64_t>(), nullptr, nullptr, nullptr,
                                                       nb->stage.as<int>(), nb->staged.as<int>());
     TGAP_LAUNCH_CHECK(ctx);
+    if (!scan) return TGAP_OK;
     TGAP_CUDA(ctx, cudaMemsetAsync(nb->counts.as<int64_t>() + n, 0, sizeof(int64_t), ctx->stream));
     return scan_i64(ctx, nb->scan_tmp, nb->counts.as<int64_t>(), nb->start.as<int64_t>(), n + 1);
 }
@@ -496,10 +541,16 @@ int neighbors_rebuild_lists_device(tgap_context *ctx, NeighborBatch *nb, bool re
     if (n <= 0) return TGAP_OK;
     if (!nb->list.ptr) return set_error(ctx, TGAP_ERR_ARGUMENT, "device-side list rebuild before any list was built");
     StageScope sc(ctx, "neighbors_rebuild");
-    if (const int rc = rebuild_count(ctx, nb)) return rc;
+    const bool small = n <= kScanFitMax;
+    if (const int rc = rebuild_count(ctx, nb, !small)) return rc;
     int *check = report ? ctx->d_check : nullptr;
-    k_fit_pairs<<<1, 1024, 0, ctx->stream>>>(n, nb->start.as<int64_t>(), nb->n_neigh.as<int>(), nb->pair_capacity(),
-                                             check, nb->counts.as<int64_t>() + n);
+    if (small)
+        k_scan_fit_pairs<<<1, 1024, 0, ctx->stream>>>(n, nb->counts.as<int64_t>(), nb->start.as<int64_t>(),
+                                                      nb->n_neigh.as<int>(), nb->pair_capacity(), check,
+                                                      nb->counts.as<int64_t>() + n);
+    else
+        k_fit_pairs<<<1, 1024, 0, ctx->stream>>>(n, nb->start.as<int64_t>(), nb->n_neigh.as<int>(),
+                                                 nb->pair_capacity(), check, nb->counts.as<int64_t>() + n);
     TGAP_LAUNCH_CHECK(ctx);
     nb->count_on_device = true;
     return rebuild_fill(ctx, nb, check);
