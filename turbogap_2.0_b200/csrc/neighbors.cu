@@ -323,30 +323,52 @@ __global__ void k_fit_pairs(int n, int64_t *start, int *n_neigh, int64_t cap, in
 }
 
 // Systems up to this many sites take the list offsets and the capacity fit from one launch.
-constexpr int kScanFitMax = 32768;
+constexpr int kScanFitMax = 16384;
 
-// The small-system form of the offset scan and k_fit_pairs in one CTA: start[0, n] = the exclusive
-// sum of the per-site counts (start[n] the total, also kept in *total), then the same capacity fit.
-// Thread t scans the contiguous chunk [t per, (t + 1) per) of the sites.
+// The small-system form of the offset scan and k_fit_pairs in one CTA of 1024 threads: start[0, n] =
+// the exclusive sum of the per-site counts (start[n] the total, also kept in *total), then the same
+// capacity fit. The counts are read in rounds of 1024 consecutive sites (all rounds' loads issued
+// first), each round scanned across the block and carried into the next.
 __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *counts, int64_t *start, int *n_neigh,
                                                          int64_t cap, int *check, int64_t *total)
 {
-    __shared__ int64_t part[1024];
+    constexpr int R = kScanFitMax / 1024;
+    __shared__ int64_t wsum[32];
     __shared__ int over;
-    const int T = blockDim.x, t = threadIdx.x;
-    const int per = (n + T - 1) / T;
-    const int b = min(n, t * per), e = min(n, b + per);
-    int64_t sum = 0;
-    for (int i = b; i < e; ++i) sum += counts[i];
-    part[t] = sum;
-    __syncthreads();
-    for (int o = 1; o < T; o <<= 1) {
-        const int64_t v = t >= o ? part[t - o] : 0;
+    const int t = threadIdx.x, lane = t & 31, w = t >> 5;
+    const int rounds = (n + 1023) / 1024;
+    int64_t v[R];
+#pragma unroll
+    for (int k = 0; k < R; ++k) v[k] = k < rounds && k * 1024 + t < n ? counts[k * 1024 + t] : 0;
+    // inclusive prefix within each round, the rounds' totals carried forward
+    int64_t carry = 0;
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        if (k >= rounds) break;
+        int64_t x = v[k];
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int64_t y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) wsum[w] = x;
         __syncthreads();
-        part[t] += v;
+        if (w == 0) {
+            int64_t z = wsum[lane];
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int64_t y = __shfl_up_sync(0xffffffffu, z, o);
+                if (lane >= o) z += y;
+            }
+            wsum[lane] = z;
+        }
         __syncthreads();
+        const int64_t incl = carry + (w > 0 ? wsum[w - 1] : 0) + x;
+        carry += wsum[31];
+        v[k] = incl - v[k];  // exclusive prefix of site k * 1024 + t
+        __syncthreads();     // wsum is rewritten by the next round
     }
-    const int64_t tot = part[T - 1];
+    const int64_t tot = carry;
     if (t == 0) {
         *total = tot;
         over = tot > cap;
@@ -354,15 +376,16 @@ __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *c
     }
     __syncthreads();
     const int64_t lim = cap - 1;
-    int64_t a = part[t] - sum;
-    for (int i = b; i < e; ++i) {
-        const int64_t z = a + counts[i];
+#pragma unroll
+    for (int k = 0; k < R; ++k) {
+        const int i = k * 1024 + t;
+        if (k >= rounds || i >= n) break;
+        const int64_t a = v[k], z = a + counts[i];
         const int64_t a2 = over && a > lim ? lim : a, z2 = over && z > lim ? lim : z;
         start[i] = a2;
         n_neigh[i] = (int)(z2 - a2);
-        a = z;
     }
-    if (t == T - 1) start[n] = over && tot > lim ? lim : tot;
+    if (t == 0) start[n] = over && tot > lim ? lim : tot;
 }
 
 static int scan_i64(tgap_context *ctx, DevBuf &tmp, const int64_t *in, int64_t *out, int n)
