@@ -54,10 +54,11 @@ typedef struct tgap_context tgap_context;
 
 int tgap_create(int device, tgap_context **ctx);
 int tgap_destroy(tgap_context *ctx);
-/* Page-locks the caller's host memory [ptr, ptr + bytes) (cudaHostRegister) for this context: the
- * host-buffer entries (tgap_calculate_gap_soap) then copy positions from and results to such arrays
- * directly instead of through the context's staging buffers. For arrays reused across calls;
- * unregister before freeing them (unregistering synchronizes the context stream). */
+/* Page-locks and maps the caller's host memory [ptr, ptr + bytes) (cudaHostRegister, mapped) for this
+ * context: the host-buffer entries (tgap_calculate_gap_soap) then read positions from and write
+ * results to such arrays directly, by a copy kernel over their device addresses, instead of through
+ * the context's staging buffers. For arrays reused across calls; unregister before freeing them
+ * (unregistering synchronizes the context stream). */
 int tgap_host_register(tgap_context *ctx, void *ptr, size_t bytes);
 int tgap_host_unregister(tgap_context *ctx, void *ptr);
 /* Use an external stream (cudaStream_t) for all later work; NULL restores the own stream. */
