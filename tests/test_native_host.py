@@ -6,6 +6,7 @@ import os
 import re
 
 import numpy as np
+import pytest
 
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
@@ -58,14 +59,15 @@ def test_number_of_unit_cells_matches_oracle(tg, orc):
         assert list(idx) == list(orc.number_of_unit_cells(box[0], box[1], box[2], rc))
 
 
-def test_host_velocity_verlet_matches_oracle(tg, orc):
+@pytest.mark.parametrize("n", [50, 51, 1])
+def test_host_velocity_verlet_matches_oracle(tg, orc, n):
     """tgap_velocity_verlet_host (host arrays) against the oracle's velocity_verlet
     (md_utils.f90:486-532) over a first step and two later ones, and its refusal of non-finite
-    forces before touching any array."""
+    forces before touching any array; atom counts that fill the pairs of atoms exactly and that
+    leave one atom for the scalar tail."""
     from turbogap_b200 import native
     L = native.lib()
     rng = np.random.default_rng(3)
-    n = 50
     m = rng.uniform(1.0, 16.0, n) * 103.6426965268
     x = rng.normal(size=(n, 3)) * 5.0
     v = rng.normal(size=(n, 3)) * 0.01
@@ -80,7 +82,7 @@ def test_host_velocity_verlet_matches_oracle(tg, orc):
         assert np.max(np.abs(x - xo)) < 1e-13
         assert np.max(np.abs(v - vo)) < 1e-15
         assert np.array_equal(fp, fpo) and np.array_equal(xp, xpo)
-    f[7, 1] = np.nan
+    f[min(7, n - 1), 1] = np.nan
     x0 = x.copy()
     assert L.tgap_velocity_verlet_host(n, native.ptr(x), None, native.ptr(v), native.ptr(f), native.ptr(fp),
                                        native.ptr(m), 0.5, 0.5, 0) == 8  # TGAP_ERR_NUMERIC
