@@ -56,17 +56,24 @@ def _nb_compare(nb_g, nb_o):
     assert np.allclose(nb_g["phis"], nb_o["phis"], rtol=0, atol=1e-14)
 
 
-@pytest.mark.parametrize("case", ["diamond_m2", "packing_m4", "packing_large"])
+@pytest.mark.parametrize("case", ["diamond_m2", "packing_m4", "packing_large", "packing_dense"])
 def test_neighbors_cell_path_bit_exact(ctx, synth, case):
+    """The linked-cell list against the oracle's, bit for bit; packing_dense (rcut 7 A: 3 cells a
+    side of ~74 atoms, ~180 pairs a site) has cells longer than a warp and rows longer than the
+    staging width, so the count pass walks several 32-candidate steps per cell and the fill pass
+    walks the cells again."""
     if case == "diamond_m2":
         pos, box, sp = synth.diamond_supercell(3, seed=7)
         rc = 3.7
     elif case == "packing_m4":
         pos, box, sp, _ = synth.random_packing(500, 2.5, 1.2, seed=8)
         rc = 4.0
-    else:
+    elif case == "packing_large":
         pos, box, sp, _ = synth.random_packing(4096, 2.5, 1.2, seed=9)
         rc = 4.0
+    else:
+        pos, box, sp, _ = synth.random_packing(2000, 2.5, 1.2, seed=13)
+        rc = 7.0
     nb_o = orc.build_neighbors(pos, len(pos), *box, rc, sp, False)
     nb_g = ctx.build_neighbors_list(pos, len(pos), *box, rc, sp, box_small=False)
     _nb_compare(nb_g, nb_o)
