@@ -295,9 +295,11 @@ def test_mc_rejects_moves_beyond_the_skin(ctx, tg, synth, carbon):
 
 
 def test_mc_speculative_batch_matches_one_at_a_time(ctx, tg, synth, carbon):
-    """Batches of 1, 5 and 16 proposals give the same decisions, the same dE (FP64, bitwise: a
-    row's energy does not depend on the rows beside it) and the same final positions; on a box
-    several cutoffs wide a batch settles more than one proposal on average."""
+    """Batches of 1, 5 and 16 proposals give the same decisions and the same final positions
+    (bitwise), and the same dE to rounding: a batch settles proposals past a deferred one, so a list
+    rebuild can fall between other moves than one at a time, and the rebuilt lists sum the FP64
+    descriptors in another order. On a box several cutoffs wide a batch settles more than one
+    proposal on average."""
     hyp, m = carbon
     pos, box, sp, _ = synth.random_packing(1000, 2.0, 1.2, seed=60)
     model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
@@ -316,7 +318,7 @@ def test_mc_speculative_batch_matches_one_at_a_time(ctx, tg, synth, carbon):
     for B in (5, 16):
         out, st, bs = runs[B]
         assert np.array_equal(out["accept"], ref_out["accept"]), B
-        assert np.array_equal(out["de"], ref_out["de"]), B
+        assert np.max(np.abs(out["de"] - ref_out["de"])) < 1e-12, B
         assert np.array_equal(st["positions"], ref_st["positions"]), B
         assert st["accepted"] == ref_st["accepted"]
         assert bs["settled"] == 300
@@ -325,8 +327,9 @@ def test_mc_speculative_batch_matches_one_at_a_time(ctx, tg, synth, carbon):
 
 def test_screened_batch_equals_one_at_a_time(ctx, tg, synth, carbon):
     """Delayed acceptance inside the speculative batch (12 slots judged by the screen from the
-    state before the batch, exact GAP row tiles of rejected slots skipped, in-order settlement)
-    makes the same decisions and ends at the same positions as one proposal at a time."""
+    state before the batch, exact GAP row tiles of rejected slots skipped, settlement in proposal
+    order past deferred slots) makes the same decisions and ends at the same positions as one
+    proposal at a time."""
     hyp, m = carbon
     pos, box, sp, _ = synth.random_packing(64, 2.0, 1.2, seed=110)
     model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
@@ -353,7 +356,9 @@ def test_screened_batch_equals_one_at_a_time(ctx, tg, synth, carbon):
     assert np.array_equal(o1["accept"], o12["accept"])
     assert np.max(np.abs(d1 - d12)) < 1e-5  # same screen energies (FP32 rows, FP64 sums)
     ex = s1 == 2
-    assert np.max(np.abs(o1["de"][ex] - o12["de"][ex])) < 1e-9
+    # exact dE to the mixed path's rounding: a list rebuild can fall between other moves when the
+    # batch settles past a deferred slot, and the FP32 descriptors then sum in another order
+    assert np.max(np.abs(o1["de"][ex] - o12["de"][ex])) < 1e-6
     assert np.array_equal(st1["positions"], st12["positions"])
     assert bs["settled"] == n  # every proposal was settled by the speculative batch
     model.close()

@@ -2710,15 +2710,19 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
     CHECK_RC(mc_read_state(mc, &h));
     const long long acc0 = h.accepted;
     CHECK_RC(mc_begin(ctx, mc->st.as<McDev>(), n));
-    long long rebuilt_at = -1;  // proposal index of the last rebuild
+    long long rebuilt_at = -1;  // proposals settled at the last rebuild
     for (;;) {
         CHECK_RC(mc_read_state(mc, &h));
+        // every proposal below next is settled except the deferred ones
+        const long long settled_now = h.next - h.n_pend;
         if (h.status == kMcNeedRebuild) {
-            // fresh lists always admit a move below the skin; a second request for the same
-            // proposal means the state is inconsistent, not that another rebuild would help
-            if (rebuilt_at == h.next)
-                return set_error(ctx, TGAP_ERR_NUMERIC, "proposal %lld still needs a list rebuild after one", h.next);
-            rebuilt_at = h.next;
+            // fresh lists always admit the first unsettled move (below the skin); a second request
+            // with nothing settled in between means the state is inconsistent, not that another
+            // rebuild would help
+            if (rebuilt_at == settled_now)
+                return set_error(ctx, TGAP_ERR_NUMERIC, "proposal %lld still needs a list rebuild after one",
+                                 h.n_pend > 0 ? h.pend[0] : h.next);
+            rebuilt_at = settled_now;
             // lists at the current positions; the cached site energies stay valid
             NeighborBatch &nb = mc->sys->nb;
             CHECK_RC(neighbors_sync_positions(ctx, &nb));
@@ -2730,7 +2734,7 @@ extern "C" int tgap_mc_run(tgap_mc *mc, int64_t n, const int *atoms, const doubl
             ++mc->rebuilds;
             continue;
         }
-        if (h.status == kMcDone || h.next >= n) break;
+        if (h.status == kMcDone || (h.next >= n && h.n_pend == 0)) break;
         mc_screen_check(mc, h);
         if (mc->use_graph) {
             if (!mc->exec || mc->graph_epoch != g_alloc_epoch.load(std::memory_order_relaxed)) {

@@ -278,6 +278,7 @@ __global__ void k_mc_accept(McDev *st, int n_models, const int *__restrict__ sit
 __global__ void k_mc_begin(McDev *st, long long n_prop)
 {
     st->next = 0;
+    st->n_pend = 0;
     st->n_prop = n_prop;
     if (st->status != kMcNeedRebuild) st->status = kMcRunning;
 }
@@ -294,8 +295,9 @@ __global__ void k_mc_lists_rebuilt(McDev *st, double *dacc, int n)
 
 // ----------------------------------------------------------------------------- speculative batch
 
-// Block b (one warp) selects the affected sites of proposal next + b from the state before the
-// batch; mark[b N + atom] holds the stamp of the last batch whose slot b took the atom.
+// Block b (one warp) selects the affected sites of slot b's proposal (the deferred ones first, then
+// next, next + 1, ...) from the state before the batch; mark[b N + atom] holds the stamp of the last
+// batch whose slot b took the atom.
 __global__ void k_mc_select_batch(McDev *st, const int64_t *__restrict__ start, const int *__restrict__ list,
                                   const int *__restrict__ jatom, const int *__restrict__ site_struct,
                                   const StructDesc *__restrict__ sd, const double *__restrict__ pos,
@@ -309,8 +311,9 @@ __global__ void k_mc_select_batch(McDev *st, const int64_t *__restrict__ start, 
     if (lane == 0) {
         int flag = 1;
         if (st->status == kMcRunning) {
-            const long long k = st->next + b;
+            const long long k = b < st->n_pend ? st->pend[b] : st->next + (b - st->n_pend);
             if (k < st->n_prop) {
+                st->slot_prop[b] = k;
                 const int a = prop_atom[k];
                 const double d0 = prop_disp[3 * k], d1 = prop_disp[3 * k + 1], d2 = prop_disp[3 * k + 2];
                 const double dn = sqrt(d0 * d0 + d1 * d1 + d2 * d2);
@@ -444,7 +447,11 @@ __global__ void k_mc_trial_geometry_batch(const McDev *st, int n_models, const i
     }
 }
 
-// One warp: settles the batch's proposals in order (see mc_select_batch for the validity rule).
+// One warp: settles the batch's proposals in proposal order. A slot's energies stay valid unless an
+// accepted earlier slot of the batch moved an atom within 2 rc + |d_i| + |d_b| of it; such a slot is
+// deferred to the next batch, and so is every later slot within that range of a deferred one (its
+// move could change the deferred proposal's energies), so each proposal is decided from the state
+// that settling them one at a time gives it: the chain is the one-at-a-time chain.
 __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restrict__ sites, int cap, int B,
                                    const double *__restrict__ etrial, double *__restrict__ ecache, int n_atoms,
                                    double *__restrict__ pos, double *__restrict__ dacc,
@@ -454,23 +461,24 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
                                    const float *__restrict__ es_trial, float *__restrict__ es_cache)
 {
     const int lane = threadIdx.x & 31;
-    __shared__ int acc_slot[kMcMaxBatch];
+    __shared__ int acc_slot[kMcMaxBatch], def_slot[kMcMaxBatch];
     if (st->status != kMcRunning) return;
-    long long k = st->next;
-    int n_acc = 0, settled = 0;
-    for (int b = 0; b < B; ++b) {
+    int n_acc = 0, n_def = 0, settled = 0;
+    int b = 0;
+    for (; b < B; ++b) {
         const int flag = st->slot_flag[b];
         if (flag == 1) break;
         if (flag == 2) {
             if (lane == 0) st->status = kMcNeedRebuild;
             break;
         }
+        const long long k = st->slot_prop[b];
         const int a = st->slot_atom[b];
         const double dn = st->slot_dn[b];
-        // valid unless an accepted earlier slot moved an atom within 2 rc + |d_i| + |d_b|
+        // blocked by an accepted or a deferred earlier slot within 2 rc + |d_i| + |d_b|
         bool conflict = false;
-        if (lane < n_acc) {
-            const int i = acc_slot[lane];
+        if (lane < n_acc + n_def) {
+            const int i = lane < n_acc ? acc_slot[lane] : def_slot[lane - n_acc];
             const int ai = st->slot_atom[i];
             if (ai == a) {
                 conflict = true;
@@ -487,7 +495,12 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
                 }
             }
         }
-        if (__any_sync(0xffffffffu, conflict)) break;
+        if (__any_sync(0xffffffffu, conflict)) {
+            if (lane == 0) def_slot[n_def] = b;
+            ++n_def;
+            __syncwarp();
+            continue;
+        }
         if (st->maxD + dacc[a] + dn >= skin) {
             if (lane == 0) st->status = kMcNeedRebuild;
             break;
@@ -505,7 +518,6 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
                     if (logs.stage) logs.stage[k] = 1;
                 }
                 __syncwarp();
-                ++k;
                 ++settled;
                 continue;
             }
@@ -558,11 +570,30 @@ __global__ void k_mc_resolve_batch(McDev *st, int n_models, const int *__restric
             ++n_acc;
         }
         __syncwarp();
-        ++k;
         ++settled;
     }
     if (lane == 0) {
-        st->next = k;
+        // unsettled: the deferred slots and every slot from b on that holds a proposal, in order
+        long long pend[kMcMaxBatch];
+        int np = 0;
+        long long top = st->next;  // one past the largest proposal of the batch
+        for (int i = 0; i < n_def; ++i) pend[np++] = st->slot_prop[def_slot[i]];
+        for (int i = 0; i < B; ++i)
+            if (st->slot_flag[i] != 1) {
+                if (i >= b) pend[np++] = st->slot_prop[i];
+                if (st->slot_prop[i] + 1 > top) top = st->slot_prop[i] + 1;
+            }
+        // a run of consecutive proposals ending at top is the plain state next = its first
+        bool run = true;
+        for (int i = 0; i < np; ++i) run = run && pend[i] == top - np + i;
+        if (run) {
+            st->next = top - np;
+            st->n_pend = 0;
+        } else {
+            st->next = top;
+            st->n_pend = np;
+            for (int i = 0; i < np; ++i) st->pend[i] = pend[i];
+        }
         st->serial += 1;
         st->batches += 1;
         st->batch_resolved += settled;
@@ -608,8 +639,8 @@ int mc_resolve_batch(tgap_context *ctx, McDev *d_st, const NeighborBatch &nb, in
 }
 
 // Warp b: slot b's screen energy change over its model-0 rows in a fixed reduction order and the
-// stage-1 test against u1 of proposal next + b (the proposal the slot holds if the batch settles
-// that far; a slot the batch does not reach is evaluated again in the next batch). Then one thread
+// stage-1 test against u1 of the slot's proposal (a slot the batch does not settle is evaluated
+// again in the next batch). Then one thread
 // per row tile of 128 trial rows: the tile is needed when a passing slot's rows fall into it.
 __global__ void k_mc_screen_batch(McDev *st, const int *__restrict__ sites, int cap, int B,
                                   const float *__restrict__ es_trial, const float *__restrict__ es_cache,
@@ -630,7 +661,7 @@ __global__ void k_mc_screen_batch(McDev *st, const int *__restrict__ sites, int 
             for (int o = 16; o > 0; o >>= 1) des += __shfl_xor_sync(0xffffffffu, des, o);
             double p = exp(-des / (mc_kb() * temperature));
             p = p < 1.0 ? p : 1.0;
-            pass = p > prop_u[2 * (st->next + b)] ? 1 : 0;
+            pass = p > prop_u[2 * st->slot_prop[b]] ? 1 : 0;
         }
         if (lane == 0) {
             st->slot_des[b] = des;

@@ -32,8 +32,12 @@ struct McDev {
     long long s_prop;    // proposals judged by the screen since creation (stage 1)
     long long s_pass;    // of those, passed on to the exact stage
     long long s_conf;    // of those, accepted by the exact stage
-    // speculative batch (plain GAP MC): slot b holds proposal next + b, evaluated from the state
-    // before the batch
+    // speculative batch (plain GAP MC): slot b holds proposal slot_prop[b], evaluated from the state
+    // before the batch: first the deferred proposals pend[0, n_pend) (in order, all below next), then
+    // next, next + 1, ... With n_pend = 0 the unsettled proposals are next, next + 1, ...
+    int n_pend;
+    long long pend[kMcMaxBatch];
+    long long slot_prop[kMcMaxBatch];
     int slot_flag[kMcMaxBatch];  // 0 evaluated, 1 no proposal left, 2 needs a list rebuild
     int slot_atom[kMcMaxBatch];
     double slot_old[kMcMaxBatch][3], slot_new[kMcMaxBatch][3], slot_dn[kMcMaxBatch];
