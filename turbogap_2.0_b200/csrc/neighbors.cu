@@ -366,7 +366,7 @@ __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *c
         const int64_t incl = carry + (w > 0 ? wsum[w - 1] : 0) + x;
         carry += wsum[31];
         v[k] = incl - v[k];  // exclusive prefix of site k * 1024 + t
-        __syncthreads();     // wsum is rewritten by the next round
+        __syncthreads();     // wsum is rewritten for the next 1024 sites
     }
     const int64_t tot = carry;
     if (t == 0) {
