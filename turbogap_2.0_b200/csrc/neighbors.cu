@@ -327,8 +327,8 @@ constexpr int kScanFitMax = 16384;
 
 // The small-system form of the offset scan and k_fit_pairs in one CTA of 1024 threads: start[0, n] =
 // the exclusive sum of the per-site counts (start[n] the total, also kept in *total), then the same
-// capacity fit. The counts are read in rounds of 1024 consecutive sites (all rounds' loads issued
-// first), each round scanned across the block and carried into the next.
+// capacity fit. The counts are read in chunks of 1024 consecutive sites (all chunks' loads issued
+// first), each chunk scanned across the block and carried into the next.
 __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *counts, int64_t *start, int *n_neigh,
                                                          int64_t cap, int *check, int64_t *total)
 {
@@ -336,15 +336,15 @@ __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *c
     __shared__ int64_t wsum[32];
     __shared__ int over;
     const int t = threadIdx.x, lane = t & 31, w = t >> 5;
-    const int rounds = (n + 1023) / 1024;
+    const int chunks = (n + 1023) / 1024;
     int64_t v[R];
 #pragma unroll
-    for (int k = 0; k < R; ++k) v[k] = k < rounds && k * 1024 + t < n ? counts[k * 1024 + t] : 0;
-    // inclusive prefix within each round, the rounds' totals carried forward
+    for (int k = 0; k < R; ++k) v[k] = k < chunks && k * 1024 + t < n ? counts[k * 1024 + t] : 0;
+    // inclusive prefix within each chunk, the chunks' totals carried forward
     int64_t carry = 0;
 #pragma unroll
     for (int k = 0; k < R; ++k) {
-        if (k >= rounds) break;
+        if (k >= chunks) break;
         int64_t x = v[k];
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
@@ -379,7 +379,7 @@ __global__ void __launch_bounds__(1024) k_scan_fit_pairs(int n, const int64_t *c
 #pragma unroll
     for (int k = 0; k < R; ++k) {
         const int i = k * 1024 + t;
-        if (k >= rounds || i >= n) break;
+        if (k >= chunks || i >= n) break;
         const int64_t a = v[k], z = a + counts[i];
         const int64_t a2 = over && a > lim ? lim : a, z2 = over && z > lim ? lim : z;
         start[i] = a2;
