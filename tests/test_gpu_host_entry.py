@@ -146,3 +146,29 @@ def test_call_graphs_follow_e0_and_site_range_changes(ctx, tg, synth):
     assert np.max(np.abs(e3 - e1)) < 1e-12
     system.close()
     model.close()
+
+
+def test_call_graphs_follow_staging_growth(ctx, tg, synth):
+    """A larger system on the same context grows the pinned staging buffers that a smaller system's
+    captured call graph reads and writes; the smaller system's next call runs with the new buffers
+    and gives the results it gave before, and the larger one equals a fresh system."""
+    hyp, m = helpers.carbon_model(synth, 200, seed=17)
+    model = tg.Model(ctx, hyp, m["Qs"], m["alphas"], 1.0, 4.0)
+    pa, ba, sa, _ = synth.random_packing(128, 2.5, 1.2, seed=24)
+    pb, bb, sb, _ = synth.random_packing(640, 2.5, 1.2, seed=25)
+    sys_a = tg.System(ctx, [(pa, ba, sa)], 3.7 + 0.3)
+    sys_b = tg.System(ctx, [(pb, bb, sb)], 3.7 + 0.3)
+    for _ in range(3):  # eager, captured, replayed
+        ea, fa, _ = sys_a.calculate_gap_soap([model], tg.TGAP_FP64, pa, rebuild=False)
+    eb, fb, _ = sys_b.calculate_gap_soap([model], tg.TGAP_FP64, pb, rebuild=False)
+    for _ in range(3):
+        ea2, fa2, _ = sys_a.calculate_gap_soap([model], tg.TGAP_FP64, pa, rebuild=False)
+        # the same to the order of the FP64 force atomics
+        assert np.max(np.abs(ea2 - ea)) <= 1e-12 * max(1.0, np.abs(ea).max())
+        assert np.max(np.abs(fa2 - fa)) <= 1e-12 * max(1.0, np.abs(fa).max())
+    eb_r, fb_r, _ = _fresh(ctx, tg, pb, bb, sb, model, tg.TGAP_FP64)
+    assert np.max(np.abs(eb - eb_r)) <= 1e-12 * max(1.0, np.abs(eb_r).max())
+    assert np.max(np.abs(fb - fb_r)) <= 1e-10 * max(1.0, np.abs(fb_r).max())
+    sys_a.close()
+    sys_b.close()
+    model.close()

@@ -62,6 +62,8 @@ void DevBuf::release()
 int HostBuf::ensure(size_t n)
 {
     if (n <= bytes && ptr) return 0;
+    // captured call graphs read and write the staging buffers through their device addresses
+    g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
     if (ptr) cudaFreeHost(ptr);
     ptr = nullptr;
     bytes = 0;
@@ -82,6 +84,7 @@ int HostBuf::ensure(size_t n)
 
 void HostBuf::release()
 {
+    if (ptr) g_alloc_epoch.fetch_add(1, std::memory_order_relaxed);
     if (ptr) cudaFreeHost(ptr);
     ptr = dev = nullptr;
     bytes = 0;
